@@ -1,0 +1,382 @@
+#!/usr/bin/env python3
+"""Benchmark of the coupled LBM / phase-field step on B200.
+
+Workload: the two-phase Allen-Cahn bubble case at 256^3 (D3Q19 MRT
+pressure/velocity lattice + D3Q19 conservative Allen-Cahn lattice, 24 seeded
+bubbles, periodic x/y, walls in z).  A "step" is one loop of the coupled step
+over the whole domain.  MLUPS = lattice cells x steps / s / 1e6.
+
+Arms
+  default           the sm_100a library (libmkb200.so) through its C ABI
+  --impl reference  the reference method's CPU implementation (the FP64
+                    OpenMP restatement in oracle/, since the reference's own
+                    solver is a closed Windows DLL), all host threads
+
+Under torchrun (N > 1) every rank runs an independent replica of the case on
+its own GPU (the case is one domain; "scaling": "weak"); the time is the max
+over ranks and the value sums all ranks' cells.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS, %HBM roofline: LBM+phase-field 256^3, FP16-store vs FP32 plain"
+WORKLOAD = "multiphase Allen-Cahn bubbles 256^3, D3Q19 MRT + D3Q19 AC, 24 bubbles, seed 0xB200"
+
+
+def _measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _ncu_traffic():
+    """Per-cell DRAM bytes of the dominant kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    out = {}
+    try:
+        with open(path) as f:
+            for line in f:
+                line = line.strip()
+                if not line or line.startswith("#"):
+                    continue
+                k, v = line.split("=", 1)
+                out[k.strip()] = float(v)
+    except Exception:
+        pass
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        smax.append(float(parts[2]))
+                    except ValueError:
+                        continue
+                    for nm, val in zip(names, parts[5:9]):
+                        if val.lower() == "active":
+                            reasons.add(nm)
+        except Exception:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _case_path(precision: str, n: int) -> str:
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import cases
+    d = os.path.join(tempfile.gettempdir(), "mkb200_bench")
+    return cases.write(cases.multiphase_bubbles(n=n, precision=precision, loops=10000),
+                       os.path.join(d, f"bubbles_{n}_{precision}.xml"))
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_ours(args):
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, case_params, initial_field
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
+
+    ws, rank, local = _dist()
+    lib = A.load()
+    st = lib.mk_set_device(local)
+    if st != A.MK_OK:
+        raise A.MkError(st, lib.mk_last_global_error().decode())
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.size
+    K, W = args.steps, args.warmup
+    results = {}
+    prec_list = [args.precision] + [p for p in ("fp32", "fp16", "bf16") if p != args.precision]
+    if args.no_variants:
+        prec_list = prec_list[:1]
+    peak, peak_kind = _measured_peak()
+    main = None
+    for prec in prec_list:
+        params = case_params(_case_path(prec, n))
+        s = Solver(params=params)
+        s.advance(W, graph=True)
+        s.sync()
+        barrier()
+        clk = Clocks(local)
+        with clk:
+            ms = s.time_advance(K, graph=True)
+        ms = max_over_ranks(ms)
+        cells = params.ncell()
+        mlups = cells * K * ws / (ms * 1e-3) / 1e6
+        bpc = s.bytes_per_cell()
+        # dominant kernel, timed live with CUDA events on the library's stream
+        prof = s.profile(min(K, 50), "collide")
+        prof_phi = s.profile(min(K, 50), "phi")
+        fluid = s.fluid_cells()
+        launches = min(K, 50)
+        t_launch = prof["kernel_ms"] / launches * 1e-3
+        S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
+        phi_b = 8 if prec == "fp64" else 4
+        collide_bytes = fluid * (2 * 38 * S + phi_b)
+        achieved = collide_bytes / t_launch / 1e9
+        step_gbs = bpc * cells * K / (ms * 1e-3) / 1e9
+        d = s.diagnostics(raise_on_divergence=False)
+        results[prec] = {
+            "mlups": mlups, "ms_per_step": ms / K, "bytes_per_cell": bpc, "step_gbs": step_gbs,
+            "step_frac": step_gbs / peak, "collide_ms": prof["kernel_ms"] / launches,
+            "phi_ms": prof_phi["kernel_ms"] / launches, "collide_gbs": achieved, "collide_frac": achieved / peak,
+            "collide_bytes_per_launch": collide_bytes, "clocks": clk.summary(), "n_bad": d["n_bad"],
+            "launches_per_step": s.launches_per_step(),
+        }
+        if prec == args.precision:
+            main = (params, s)
+        else:
+            s.close()
+    params, s = main
+    r = results[args.precision]
+
+    # end to end through the C ABI: pinned host phi -> device, K loops, phi -> pinned host
+    cells = params.ncell()
+    nbytes = cells * 4
+    hp_in, hp_out = A.C.c_void_p(), A.C.c_void_p()
+    lib.mk_host_alloc(nbytes, A.C.byref(hp_in))
+    lib.mk_host_alloc(nbytes, A.C.byref(hp_out))
+    phi_in = np.ctypeslib.as_array((A.C.c_float * cells).from_address(hp_in.value))
+    phi_out = np.ctypeslib.as_array((A.C.c_float * cells).from_address(hp_out.value))
+    phi_in[:] = initial_field(params, "phi").ravel().astype(np.float32)
+    fptr = phi_in.ctypes.data_as(A.C.POINTER(A.C.c_float))
+    # warm the staging buffers once
+    lib.mk_set_state_f32(s.handle, fptr, None, None)
+    lib.mk_get_field(s.handle, A.MK_FIELD_PHI, A.MK_DTYPE_F32, hp_out, nbytes)
+    barrier()
+    t0 = time.perf_counter()
+    stt = lib.mk_set_state_f32(s.handle, fptr, None, None)
+    stt |= lib.mk_advance_graph(s.handle, K)
+    stt |= lib.mk_get_field(s.handle, A.MK_FIELD_PHI, A.MK_DTYPE_F32, hp_out, nbytes)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s)
+    if stt != 0:
+        raise A.MkError(stt, lib.mk_last_error(s.handle).decode())
+    e2e_mlups = cells * K * ws / e2e_s / 1e6
+    phi_ok = bool(np.isfinite(phi_out).all())
+    lib.mk_host_free(hp_in)
+    lib.mk_host_free(hp_out)
+    s.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(n, budget_s=args.cpu_budget)
+
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    traffic = _ncu_traffic()
+    tkey = f"collide_{args.precision}_bytes_per_cell"
+    traffic_launch = traffic[tkey] * params.ncell() if tkey in traffic else None
+    line = {
+        "metric": METRIC,
+        "value": round(r["mlups"], 1),
+        "unit": "MLUPS",
+        "n_gpus": ws,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(r["ms_per_step"], 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded bubble case, splitmix64 seed 0xB200)",
+        "config": {"workload": WORKLOAD, "cells": params.ncell(), "storage": args.precision,
+                   "collision": "MRT(g) + BGK(h)", "streaming": "AA in place",
+                   "l2": "inputs larger than L2 (%.2f GB resident populations)" % (
+                       r["bytes_per_cell"] * params.ncell() / 2 / 1e9),
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+        "roofline": {"bound": "hbm", "kernel": "k_mp_collide", "achieved": round(r["collide_gbs"], 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(r["collide_frac"], 4),
+                     "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": r["collide_bytes_per_launch"],
+                     "traffic": traffic_launch,
+                     "step_bytes_per_cell": r["bytes_per_cell"], "step_gbs": round(r["step_gbs"], 1),
+                     "step_frac": round(r["step_frac"], 4)},
+        "variants": {k: {"mlups": round(v["mlups"], 1), "ms_per_step": round(v["ms_per_step"], 4),
+                         "collide_frac": round(v["collide_frac"], 4), "step_frac": round(v["step_frac"], 4),
+                         "bytes_per_cell": v["bytes_per_cell"], "n_bad": v["n_bad"],
+                         "speedup_vs_fp32": round(v["mlups"] / results["fp32"]["mlups"], 3)
+                         if "fp32" in results else None}
+                     for k, v in results.items()},
+        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": nbytes / K,
+                "d2h_bytes_per_step": nbytes / K, "seconds": round(e2e_s, 4), "phi_finite": phi_ok,
+                "path": "mk_set_state_f32 (pinned) + mk_advance_graph + mk_get_field f32 (pinned)"},
+        "gpu_launches": K * r["launches_per_step"],
+        "clocks": r["clocks"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(n: int, budget_s: float = 20.0):
+    """Time the FP64 OpenMP oracle on the host cores on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import Oracle, load as load_oracle
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import case_params, initial_field
+
+    lib = load_oracle()
+    params = case_params(_case_path("fp64", n))
+    phi = initial_field(params, "phi")
+    o = Oracle(params, phi=phi)
+    t0 = time.perf_counter()
+    o.advance(1)
+    t1 = time.perf_counter() - t0
+    steps = max(1, min(20, int(budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    o.advance(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    cells = params.ncell()
+    return {"value": round(cells * steps / dt / 1e6, 2), "unit": "MLUPS", "cores": int(lib.orc_get_threads()),
+            "kind": "port", "sample": f"{steps} loops of the {n}^3 case after 1 untimed loop (FP64 oracle)",
+            "seconds": round(dt, 2)}
+
+
+def run_reference(args):
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import Oracle, load as load_oracle
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import case_params, initial_field
+
+    lib = load_oracle()
+    n = args.size
+    params = case_params(_case_path("fp64", n))
+    o = Oracle(params, phi=initial_field(params, "phi"))
+    t0 = time.perf_counter()
+    o.advance(1)  # one untimed warm-up loop
+    t1 = time.perf_counter() - t0
+    # each step is one full loop; the number of timed loops is capped so the
+    # whole run stays within the budget
+    steps = max(1, min(args.steps, int(args.ref_budget / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    o.advance(steps)
+    dt = time.perf_counter() - t0
+    cells = params.ncell()
+    mlups = cells * steps / dt / 1e6
+    cores = int(lib.orc_get_threads())
+    line = {
+        "metric": METRIC, "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws, "steps": steps, "warmup": 1,
+        "ms_per_step": round(dt / steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubble case, splitmix64 seed 0xB200)",
+        "config": {"workload": WORKLOAD, "cells": cells, "storage": "fp64", "parallelism": f"{cores} host threads"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": cores, "kind": "port",
+                         "sample": f"{steps} loops of the {n}^3 case (requested {args.steps}); the reference's own "
+                                   f"solver is a closed Windows DLL, so this is the FP64 OpenMP restatement"},
+        "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--ref-budget", type=float, default=120.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,287 @@
+/*
+ * mkb200.h — C ABI of the B200 coupled lattice-Boltzmann / phase-field step.
+ *
+ * This is the drop-in boundary for MaterKit's solver path.  The reference
+ * exposes a C++ class API from a Windows DLL (MaterKit/inc/MaterKit.h:28-35,
+ * MK_API = __declspec(dllexport)); its lifecycle is
+ *
+ *   mkSpace(xml)                      MaterKit/inc/mkSpace.h:36
+ *   solver(space), solver.reset(xml)  MaterKit/inc/mkFluidsLBM.h:35-38
+ *   readParameters(loops,frames,xml)  MaterKit/inc/mkFunction.h:62
+ *   solver.initialize(xml)            MaterKit/inc/mkFluidsMRT.h:39
+ *   solver.initialize_geometry()      MaterKit/inc/mkFluidsMRT.h:40
+ *   per loop: propagate()/relaxation*()/bdy*()   (MaterKit/MaterKit.cpp:204-237)
+ *   write_vtkfile(loops), check_variables(...)   (MaterKit/inc/mkFluidsMRT.h:48,
+ *                                                  MaterKit/inc/mkFluidsLBM.h:55)
+ *
+ * Every entry point here returns mk_status; no C++ exception crosses the ABI
+ * (the reference throws mkIOError from MaterKit/xml/mkTINYXMLIO.hh:40).  All
+ * arguments are plain pointers and sizes.  A handle owns its device memory and
+ * one CUDA stream; it is thread-compatible (one host thread at a time).
+ *
+ * Field arrays exchanged through this header are dense, x fastest:
+ *   index = x + nx * (y + ny * z).
+ */
+#ifndef MKB200_H
+#define MKB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MKB200_ABI_VERSION 1
+
+/* Status codes.  Replace the exception family of
+ * MaterKit/inc/mkRunTimeDiagnostics.h:59-117 (mkIOError, mkMemoryError, ...). */
+typedef enum mk_status {
+  MK_OK = 0,
+  MK_ERR_XML = 1,      /* unreadable XML or a tag with a malformed value */
+  MK_ERR_ARG = 2,      /* invalid argument / unsupported combination      */
+  MK_ERR_CUDA = 3,     /* CUDA runtime error (message in mk_last_error)   */
+  MK_ERR_DIVERGED = 4, /* NaN/Inf or non-positive density detected        */
+  MK_ERR_TIMEOUT = 5,  /* a bounded device wait gave up                   */
+  MK_ERR_OOM = 6,      /* device or host allocation failed                */
+  MK_ERR_IO = 7,       /* file could not be written / read                */
+  MK_ERR_STATE = 8,    /* call not valid in the handle's current state    */
+  MK_ERR_NODEVICE = 9  /* no CUDA device (the library has no CPU fallback) */
+} mk_status;
+
+/* Which solver path a case runs.  In the reference the driver picks this by
+ * calling one run_* function (MaterKit/MaterKit.cpp:23-34). */
+typedef enum mk_model {
+  MK_MODEL_FLOW = 0,             /* single-phase flow, run_flow_Poiseuille (MaterKit.cpp:244-288) */
+  MK_MODEL_MULTIPHASE = 1,       /* Allen-Cahn two-phase flow, run_flow_multiphase (:290-331)     */
+  MK_MODEL_THERMAL_DENDRITE = 2, /* phase field + thermal ADE, run_thermal_dendrite (:743-788)    */
+  MK_MODEL_SOLUTAL_DENDRITE = 3  /* phase field + solutal ADE, run_solutal_dendrite (:633-687)    */
+} mk_model;
+
+/* Population storage precision.  Collision arithmetic is FP64 for MK_PREC_FP64
+ * and FP32 otherwise.  FP16/BF16 store the deviation from the rest state
+ * ("shifted storage"). */
+typedef enum mk_precision {
+  MK_PREC_FP64 = 0,
+  MK_PREC_FP32 = 1,
+  MK_PREC_FP16 = 2,
+  MK_PREC_BF16 = 3
+} mk_precision;
+
+/* Collision operators of mkNode (MaterKit/inc/mkNode.h:74-87). */
+typedef enum mk_collision {
+  MK_COLL_BGK = 0,
+  MK_COLL_TRT = 1,
+  MK_COLL_MRT = 2
+} mk_collision;
+
+/* Velocity sets.  The reference's lattice class is MaterKit/inc/mkLattice.h:26-100. */
+typedef enum mk_lattice {
+  MK_D3Q7 = 7,
+  MK_D3Q19 = 19,
+  MK_D3Q27 = 27
+} mk_lattice;
+
+/* Boundary kind per axis. */
+typedef enum mk_bc {
+  MK_BC_PERIODIC = 0, /* periodic wrap, as mkFluidsLBM::neighbor (mkFluidsLBM.h:82)      */
+  MK_BC_WALLS = 1,    /* cells 0 and n-1 are solid walls; half-way bounce-back          */
+  MK_BC_CLOSED = 2    /* all cells fluid; the domain faces bounce back (zero flux)      */
+} mk_bc;
+
+/* Node flags, values of MaterKit/inc/mkGlobalDefs.h:140-145. */
+#define MK_FLAG_FLUID 0
+#define MK_FLAG_INTER 1
+#define MK_FLAG_SOLID 2
+#define MK_FLAG_WALLS 3
+
+typedef enum mk_field {
+  MK_FIELD_RHO = 0,      /* density                                          */
+  MK_FIELD_UX = 1,       /* velocity x                                       */
+  MK_FIELD_UY = 2,
+  MK_FIELD_UZ = 3,
+  MK_FIELD_T = 4,        /* dimensionless temperature u = (T - Tm)/(L/cp)    */
+  MK_FIELD_C = 5,        /* solute: supersaturation U of the dilute alloy    */
+  MK_FIELD_PHI = 6,      /* order parameter                                  */
+  MK_FIELD_FLAG = 7,     /* node flag (as double)                            */
+  MK_FIELD_PRESSURE = 8, /* normalised pressure p* (multiphase)              */
+  MK_FIELD_DPHI = 9,     /* phi(n) - phi(n-1), the latent-heat driver        */
+  MK_FIELD_GRAIN = 10    /* grain id (seed index)                            */
+} mk_field;
+
+typedef enum mk_dtype {
+  MK_DTYPE_F64 = 0,
+  MK_DTYPE_F32 = 1
+} mk_dtype;
+
+#define MK_MAX_OBJECTS 64
+
+/* Every resolved number of a case, in lattice units.  Filled from the
+ * BoltzTechs XML (tags listed in DESIGN.md) plus the optional <b200> block. */
+typedef struct mk_params {
+  int32_t model;      /* mk_model */
+  int32_t lattice;    /* flow lattice (D3Q19/D3Q27); scalar lattices are D3Q7 */
+  int32_t collision;  /* mk_collision of the flow lattice */
+  int32_t precision;  /* mk_precision */
+  int32_t nx, ny, nz; /* MeshXYZ */
+  int32_t bc[3];      /* mk_bc per axis */
+  int32_t max_loops;  /* output/numLoops */
+  int32_t max_frames; /* output/numFrames */
+
+  /* single-phase flow */
+  double rho0;        /* initial density */
+  double u0[3];       /* initial velocity */
+  double tau;         /* BGK tau, TRT tau+, MRT shear tau */
+  double magic;       /* TRT Lambda = (tau+ - 1/2)(tau- - 1/2) */
+  double force[3];    /* body force density (flow) or gravity acceleration (multiphase) */
+
+  /* two-phase Allen-Cahn flow */
+  double rho_l, rho_g;   /* densities of phi = 1 and phi = 0 */
+  double tau_l, tau_g;   /* flow relaxation times of the two fluids */
+  double sigma;          /* surface tension */
+  double width;          /* interface width W */
+  double mobility;       /* Allen-Cahn mobility M */
+  double contact_angle;  /* degrees, at solid walls */
+
+  /* phase field (dendrites) */
+  double eps4;        /* 4-fold anisotropy strength */
+  double W0;          /* interface width */
+  double tau0;        /* relaxation time of the phase field */
+  double lambda;      /* coupling constant */
+  double delta;       /* dimensionless undercooling (u0 = -delta) / supersaturation */
+  double D;           /* thermal or solutal diffusivity (liquid) */
+  double D_s;         /* solutal diffusivity in the solid */
+  double k_part;      /* partition coefficient */
+  double at_coef;     /* anti-trapping coefficient (1/(2 sqrt 2) for the standard current) */
+
+  /* seeds (dendrites) or bubbles (multiphase) */
+  int32_t n_objects;
+  int32_t _pad0;
+  double obj_center[MK_MAX_OBJECTS][3];
+  double obj_angle[MK_MAX_OBJECTS][3];  /* degrees, rotate order ZYX */
+  double obj_radius[MK_MAX_OBJECTS];
+  uint64_t rng_seed;
+} mk_params;
+
+/* Optional overrides at creation; a negative value keeps the XML/default. */
+typedef struct mk_options {
+  int32_t model;
+  int32_t precision;
+  int32_t collision;
+  int32_t lattice;
+  double magic;
+  int32_t device;
+  int32_t block_x;    /* launch shape override (0 = tuned default) */
+  int32_t block_y;
+} mk_options;
+
+/* FP64 global sums (K6).  Replaces check_variables (mkFluidsLBM.h:55). */
+typedef struct mk_diag {
+  int64_t step;
+  double mass;         /* sum of density over fluid cells          */
+  double momentum[3];  /* sum of rho*u                             */
+  double phi_sum;      /* sum of phi                               */
+  double solid_frac;   /* fraction of fluid cells with phi > 0 (dendrite) or phi < 1/2 (multiphase gas) */
+  double heat;         /* sum of T (+ latent part)                 */
+  double solute;       /* sum of solute                            */
+  double max_speed;    /* max |u|                                  */
+  int32_t n_bad;       /* NaN/Inf/non-positive density cells       */
+  int32_t _pad;
+} mk_diag;
+
+typedef struct mk_handle mk_handle;
+
+/* Library / ABI. */
+int32_t mk_abi_version(void);
+/* Select the CUDA device of handles created afterwards by this host thread. */
+mk_status mk_set_device(int32_t device);
+const char* mk_version_string(void);
+/* Last error of a failed call that had no handle (e.g. mk_create_from_xml). */
+const char* mk_last_global_error(void);
+
+/* readParameters(maxLoops, maxFrame, xml) — MaterKit/inc/mkFunction.h:62.
+ * Reads output/numLoops and output/numFrames. */
+mk_status mk_read_parameters(const char* xml_path, int32_t* max_loops, int32_t* max_frames);
+
+/* Resolve a case to its parameters without touching a GPU
+ * (= mkSpace(xml) + reset + read_parameters, MaterKit/inc/mkFluidsLBM.h:37,42). */
+mk_status mk_case_params(const char* xml_path, const mk_options* opt, mk_params* out);
+
+/* Host-side initial state of a case (= initialize + initialize_geometry,
+ * MaterKit/inc/mkFluidsMRT.h:39-40).  Writes ncells doubles. */
+mk_status mk_case_initial_field(const mk_params* p, int32_t field, double* out, size_t ncells);
+
+/* Create a solver on the GPU from a BoltzTechs XML case.
+ * = mkSpace(xml) + solver(space) + reset(xml) + initialize(xml) + initialize_geometry(). */
+mk_status mk_create_from_xml(const char* xml_path, const mk_options* opt, mk_handle** out);
+/* Same, from already-resolved parameters. */
+mk_status mk_create(const mk_params* p, mk_handle** out);
+mk_status mk_destroy(mk_handle* h);
+const char* mk_last_error(const mk_handle* h);
+
+mk_status mk_get_params(const mk_handle* h, mk_params* out);
+int64_t mk_get_step(const mk_handle* h);
+
+/* Advance n loops of the coupled step (propagate + relaxation of every field in
+ * the reference's per-loop order).  Asynchronous on the handle's stream. */
+mk_status mk_advance(mk_handle* h, int64_t nsteps);
+/* Capture the per-loop launches in a CUDA graph and replay it n times. */
+mk_status mk_advance_graph(mk_handle* h, int64_t nsteps);
+mk_status mk_sync(mk_handle* h);
+/* The handle's cudaStream_t, for event timing by the caller. */
+mk_status mk_get_stream(mk_handle* h, void** stream);
+
+/* Copy a macroscopic field to host memory (synchronous). */
+mk_status mk_get_field(mk_handle* h, int32_t field, int32_t dtype, void* host_dst, size_t bytes);
+/* Replace the state by the equilibrium of host-provided macroscopic fields
+ * (phi, and rho/u/T/C where the model has them).  Any pointer may be NULL to
+ * keep the case's initial field.  Resets the step counter to 0. */
+mk_status mk_set_state(mk_handle* h, const double* phi, const double* temp, const double* conc,
+                       const double* rho, const double* ux, const double* uy, const double* uz);
+/* Same from FP32 host buffers (pinned memory is used directly). */
+mk_status mk_set_state_f32(mk_handle* h, const float* phi, const float* temp, const float* conc);
+
+/* Legacy VTK RECTILINEAR_GRID writer in the reference's format
+ * (MaterKit/src/mkFluidsUser.cpp:714-947); file <dir>/fluid_t<loops>.vtk. */
+mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir);
+
+/* FP64 conservation sums and the divergence watchdog. */
+mk_status mk_diagnostics(mk_handle* h, mk_diag* out);
+
+/* Binary checkpoint: populations, phi, step and a parameter hash. */
+mk_status mk_checkpoint(mk_handle* h, const char* path);
+mk_status mk_restore(mk_handle* h, const char* path);
+
+/* Timing of one kernel of the step (CUDA events on the handle's stream):
+ * runs `launches` steps and returns the summed device time of the kernel
+ * named `kernel` ("collide", "phi", ...), and the total step time. */
+mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel,
+                           double* kernel_ms, double* step_ms, int64_t* kernel_launches);
+
+/* Advance n loops bracketed by CUDA events on the handle's stream; returns the
+ * device time in milliseconds (synchronises at the end). */
+mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, double* ms);
+
+/* Page-locked host buffers for end-to-end transfers (cudaHostAlloc). */
+mk_status mk_host_alloc(size_t bytes, void** out);
+mk_status mk_host_free(void* p);
+
+/* Algorithmic bytes per cell per step of the handle's configuration. */
+double mk_bytes_per_cell(const mk_handle* h);
+int64_t mk_fluid_cells(const mk_handle* h);
+/* Number of kernel launches one step issues. */
+int32_t mk_launches_per_step(const mk_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* MKB200_H */

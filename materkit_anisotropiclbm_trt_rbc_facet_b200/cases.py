@@ -1,0 +1,94 @@
+"""BoltzTechs XML cases of the five benchmark configurations.
+
+Each case is a complete BoltzTechs file (the tag set of
+MaterKit/BoltzTechs - thermal.xml and BoltzTechs - multiPhaseFlow.xml) plus a
+``<b200>`` element with the lattice-unit values the configuration names.  The
+generators take overrides so tests run the same case at reduced size.
+"""
+from __future__ import annotations
+
+import os
+
+_HEADER = """<?xml version="1.0" encoding="utf-8"?>
+<MaterKit>
+  <calcMode> <dendrite> {dendrite} </dendrite> <flowField> {flow} </flowField> </calcMode>
+  <output> <numLoops> {loops} </numLoops> <numFrames> {frames} </numFrames> </output>
+  <geometry> <MeshXYZ> {nx} {ny} {nz} </MeshXYZ> <Gravity> 0.0 0.0 0.0 </Gravity> </geometry>
+  <numerics> <mk_dx> 1.0 </mk_dx> <mk_dt> 1.0 </mk_dt> <stepSize> -1.0 </stepSize>
+    <omega_f> -1.0 </omega_f> <omega_g> -1.0 </omega_g> <omega_h> -1.0 </omega_h> </numerics>
+"""
+
+
+def poiseuille(nx=64, ny=32, nz=32, loops=2000, precision="fp64", collision="TRT", lattice="D3Q19",
+               tau=0.8, magic=0.1875, force=1e-6) -> str:
+    """Config 1: 3D Poiseuille channel, D3Q19 TRT, walls at y = 0 and y = ny-1."""
+    return _HEADER.format(dendrite="false", flow="true", loops=loops, frames=min(loops, 100), nx=nx, ny=ny, nz=nz) + f"""
+  <flow> <acceleration> {force} 0.0 0.0 </acceleration> <velocityInlet> 0 0 0 </velocityInlet> </flow>
+  <b200>
+    <model> flow </model> <lattice> {lattice} </lattice> <collision> {collision} </collision>
+    <precision> {precision} </precision> <boundary> periodic walls periodic </boundary>
+    <tau> {tau} </tau> <magic> {magic} </magic> <rho0> 1.0 </rho0> <force> {force} 0.0 0.0 </force>
+  </b200>
+</MaterKit>
+"""
+
+
+def thermal_dendrite(n=128, loops=5000, precision="fp32", eps4=0.05, W0=1.5, lam=10.0, delta=0.55, D=0.1,
+                     radius=8.0, tau0=None, center=None) -> str:
+    """Config 2: D3Q7 thermal lattice + anisotropic phase field, one centred seed."""
+    c = center if center is not None else ((n - 1) / 2.0,) * 3
+    t0 = f"<tau0> {tau0} </tau0>" if tau0 else ""
+    return _HEADER.format(dendrite="true", flow="false", loops=loops, frames=min(loops, 100), nx=n, ny=n, nz=n) + f"""
+  <phasechange>
+    <d0> 0.138486 </d0> <lambda> {lam} </lambda> <anisotropy> {eps4} </anisotropy> <W0> 1.0 </W0> <t0> 1.0 </t0>
+    <seed> <number> 1 </number> <center> {c[0]} {c[1]} {c[2]} </center> <angle> 0 0 0 </angle>
+      <radius> {radius} </radius> </seed>
+  </phasechange>
+  <temperature> <iniValue> {-delta} </iniValue> <undercooling> {delta} </undercooling>
+    <alphaFluid> {D} </alphaFluid> <alphaSolid> {D} </alphaSolid> <beta> 0.0 </beta> </temperature>
+  <b200>
+    <model> thermal_dendrite </model> <precision> {precision} </precision>
+    <boundary> closed closed closed </boundary>
+    <eps4> {eps4} </eps4> <W0> {W0} </W0> <lambda> {lam} </lambda> <delta> {delta} </delta>
+    <diffusivity> {D} </diffusivity> {t0}
+  </b200>
+</MaterKit>
+"""
+
+
+def multiphase_bubbles(n=256, nz=None, loops=10000, precision="fp32", bubbles=24, rmin=8.0, rmax=16.0,
+                       seed=0xB200, width=4.0, sigma=1e-3, rho_ratio=10.0, nu_ratio=10.0, tau_l=0.8,
+                       mobility=0.05, gz=-1e-6, contact_angle=90.0) -> str:
+    """Config 3 (headline): 256^3 D3Q19 MRT + D3Q19 conservative Allen-Cahn, 24 bubbles.
+
+    Liquid (phi = 1) density 1, gas density 1/rho_ratio; liquid kinematic
+    viscosity nu_l = (tau_l - 1/2)/3, gas nu_l / nu_ratio.
+    """
+    nz = n if nz is None else nz
+    nu_l = (tau_l - 0.5) / 3.0
+    tau_g = 3.0 * nu_l / nu_ratio + 0.5
+    return _HEADER.format(dendrite="false", flow="true", loops=loops, frames=min(loops, 100), nx=n, ny=n, nz=nz) + f"""
+  <multiphases>
+    <fluidDense> <kinematicViscosity> {nu_l} </kinematicViscosity> <density> 1.0 </density> </fluidDense>
+    <fluidRare> <kinematicViscosity> {nu_l / nu_ratio} </kinematicViscosity> <density> {1.0 / rho_ratio} </density> </fluidRare>
+    <force> 0.0 0.0 0.0 </force> <W0> {width} </W0> <Mobility> {mobility} </Mobility> <sigma> {sigma} </sigma>
+    <contactAngle> {contact_angle} </contactAngle>
+  </multiphases>
+  <b200>
+    <model> multiphase </model> <collision> MRT </collision> <precision> {precision} </precision>
+    <boundary> periodic periodic walls </boundary>
+    <rhoL> 1.0 </rhoL> <rhoG> {1.0 / rho_ratio} </rhoG> <tauL> {tau_l} </tauL> <tauG> {tau_g} </tauG>
+    <sigma> {sigma} </sigma> <width> {width} </width> <mobility> {mobility} </mobility>
+    <contactAngle> {contact_angle} </contactAngle> <force> 0.0 0.0 {gz} </force>
+    <random> <bubbles> {bubbles} </bubbles> <radiusMin> {rmin} </radiusMin> <radiusMax> {rmax} </radiusMax>
+      <gap> {2 * width} </gap> <seed> {hex(seed)} </seed> </random>
+  </b200>
+</MaterKit>
+"""
+
+
+def write(text: str, path: str) -> str:
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        f.write(text)
+    return path

@@ -1,0 +1,253 @@
+// mk_device.cuh — lattice tables, storage traits and geometry shared by the
+// sm_100a kernels.
+//
+// Memory layout in HBM: structure of arrays, one plane per population,
+// A[q * stride + cell] with cell = x + nx (y + ny z) and stride rounded up to
+// a multiple of 64 cells, so every population plane starts 256-byte aligned.
+// Streaming is in place with the AA pattern (Bailey et al. 2009): an even
+// loop reads and writes only the cell's own slots (A[i][c] in, A[inv i][c]
+// out); an odd loop reads A[inv i][c - e_i] and writes A[i][c + e_i].  Each
+// population is therefore read once and written once per loop, and no second
+// population array exists.  Half-way bounce-back (MaterKit/src/mkFluidsUser.cpp:
+// 77-97 streams with bounce-back in the same sweep) folds into the odd loop's
+// addressing: a link to a non-fluid neighbour reads/writes the cell's own
+// opposite slot instead.
+#ifndef MK_DEVICE_CUH
+#define MK_DEVICE_CUH
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace mkd {
+
+// ------------------------------------------------------------- lattices
+// Direction order identical to the oracle and the public header docs:
+// rest, +-x, +-y, +-z, xy/xz/yz edges, 8 corners; opposite directions adjacent.
+__host__ __device__ constexpr int ex(int i) {
+  constexpr int t[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+  return t[i];
+}
+__host__ __device__ constexpr int ey(int i) {
+  constexpr int t[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+  return t[i];
+}
+__host__ __device__ constexpr int ez(int i) {
+  constexpr int t[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+  return t[i];
+}
+__host__ __device__ constexpr int inv(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+
+template <int Q>
+__host__ __device__ constexpr double wq(int i) {
+  return Q == 7 ? (i == 0 ? 0.25 : 0.125)
+                : (Q == 19 ? (i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0))
+                           : (i == 0 ? 8.0 / 27.0 : (i <= 6 ? 2.0 / 27.0 : (i <= 18 ? 1.0 / 54.0 : 1.0 / 216.0))));
+}
+
+// d'Humieres 2002 D3Q19 moment matrix entry M[k][i] (integer valued).
+__host__ __device__ constexpr int mrt_m(int k, int i) {
+  const int x = ex(i), y = ey(i), z = ez(i);
+  const int e2 = x * x + y * y + z * z;
+  switch (k) {
+    case 0: return 1;
+    case 1: return 19 * e2 - 30;
+    case 2: return (21 * e2 * e2 - 53 * e2 + 24) / 2;
+    case 3: return x;
+    case 4: return (5 * e2 - 9) * x;
+    case 5: return y;
+    case 6: return (5 * e2 - 9) * y;
+    case 7: return z;
+    case 8: return (5 * e2 - 9) * z;
+    case 9: return 3 * x * x - e2;
+    case 10: return (3 * e2 - 5) * (3 * x * x - e2);
+    case 11: return y * y - z * z;
+    case 12: return (3 * e2 - 5) * (y * y - z * z);
+    case 13: return x * y;
+    case 14: return y * z;
+    case 15: return x * z;
+    case 16: return (y * y - z * z) * x;
+    case 17: return (z * z - x * x) * y;
+    default: return (x * x - y * y) * z;
+  }
+}
+__host__ __device__ constexpr int mrt_norm(int k) {
+  int s = 0;
+  for (int i = 0; i < 19; ++i) s += mrt_m(k, i) * mrt_m(k, i);
+  return s;
+}
+// Fixed rates; the shear rows (9, 11, 13, 14, 15) take the runtime rate.
+__host__ __device__ constexpr double mrt_rate(int k) {
+  return k == 1 ? 1.19 : (k == 2 ? 1.4 : ((k == 4 || k == 6 || k == 8) ? 1.2 : ((k == 10 || k == 12) ? 1.4 : (k >= 16 ? 1.98 : 1.0))));
+}
+__host__ __device__ constexpr bool mrt_is_shear(int k) { return k == 9 || k == 11 || k == 13 || k == 14 || k == 15; }
+
+// f -= Mi [ S M (f - feq) - (I - S/2) M F ]   (all loops unrolled; M is
+// integer so the compiler folds every zero).
+template <class T>
+__device__ __forceinline__ void mrt19_collide(T (&f)[19], const T (&feq)[19], const T (&F)[19], T s_nu) {
+  T d[19];
+#pragma unroll
+  for (int k = 0; k < 19; ++k) {
+    T mn = T(0), mf = T(0);
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+      if (mrt_m(k, i) != 0) {
+        mn += T(mrt_m(k, i)) * (f[i] - feq[i]);
+        mf += T(mrt_m(k, i)) * F[i];
+      }
+    }
+    const T s = mrt_is_shear(k) ? s_nu : T(mrt_rate(k));
+    d[k] = (s * mn - (T(1) - T(0.5) * s) * mf) * T(1.0 / mrt_norm(k));
+  }
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < 19; ++k)
+      if (mrt_m(k, i) != 0) acc += T(mrt_m(k, i)) * d[k];
+    f[i] -= acc;
+  }
+}
+
+// -------------------------------------------------------- storage traits
+// FP64/FP32 store populations as they are.  FP16/BF16 store the shifted,
+// weight-normalised deviation (f_i / w_i - ref), which keeps every plane in
+// the normal range of the 16-bit format; arithmetic stays FP32.
+template <class S>
+struct Stor;
+template <>
+struct Stor<double> {
+  typedef double T;
+  static constexpr int bytes = 8;
+  __device__ __forceinline__ static double ld(const double* p, double, double) { return *p; }
+  __device__ __forceinline__ static void st(double* p, double v, double, double) { *p = v; }
+};
+template <>
+struct Stor<float> {
+  typedef float T;
+  static constexpr int bytes = 4;
+  __device__ __forceinline__ static float ld(const float* p, float, float) { return *p; }
+  __device__ __forceinline__ static void st(float* p, float v, float, float) { *p = v; }
+};
+template <>
+struct Stor<__half> {
+  typedef float T;
+  static constexpr int bytes = 2;
+  __device__ __forceinline__ static float ld(const __half* p, float w, float ref) { return w * (ref + __half2float(*p)); }
+  __device__ __forceinline__ static void st(__half* p, float v, float w, float ref) {
+    *p = __float2half_rn(v * (1.0f / w) - ref);
+  }
+};
+template <>
+struct Stor<__nv_bfloat16> {
+  typedef float T;
+  static constexpr int bytes = 2;
+  __device__ __forceinline__ static float ld(const __nv_bfloat16* p, float w, float ref) {
+    return w * (ref + __bfloat162float(*p));
+  }
+  __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float w, float ref) {
+    *p = __float2bfloat16_rn(v * (1.0f / w) - ref);
+  }
+};
+
+// -------------------------------------------------------------- geometry
+// Boundary kinds per axis: 0 periodic, 1 walls (cells 0 and n-1 solid),
+// 2 closed faces (all cells fluid, the faces bounce back).
+struct Geom {
+  int nx, ny, nz;
+  int bc0, bc1, bc2;
+  int64_t stride;  // population plane stride (cells)
+
+  __device__ __forceinline__ bool fluid(int x, int y, int z) const {
+    if (bc0 == 1 && (x == 0 || x == nx - 1)) return false;
+    if (bc1 == 1 && (y == 0 || y == ny - 1)) return false;
+    if (bc2 == 1 && (z == 0 || z == nz - 1)) return false;
+    return true;
+  }
+  __device__ __forceinline__ int64_t idx(int x, int y, int z) const {
+    return (int64_t)x + (int64_t)nx * ((int64_t)y + (int64_t)ny * z);
+  }
+  // Neighbour index along (dx,dy,dz); false when it is non-fluid or outside a
+  // closed face.  Periodic axes wrap (mkFluidsLBM::neighbor, mkFluidsLBM.h:82).
+  __device__ __forceinline__ bool nbr(int x, int y, int z, int dx, int dy, int dz, int64_t& out) const {
+    int cx = x + dx, cy = y + dy, cz = z + dz;
+    if (dx != 0) {
+      if (cx < 0 || cx >= nx) {
+        if (bc0 != 0) return false;
+        cx = cx < 0 ? cx + nx : cx - nx;
+      }
+      if (bc0 == 1 && (cx == 0 || cx == nx - 1)) return false;
+    }
+    if (dy != 0) {
+      if (cy < 0 || cy >= ny) {
+        if (bc1 != 0) return false;
+        cy = cy < 0 ? cy + ny : cy - ny;
+      }
+      if (bc1 == 1 && (cy == 0 || cy == ny - 1)) return false;
+    }
+    if (dz != 0) {
+      if (cz < 0 || cz >= nz) {
+        if (bc2 != 0) return false;
+        cz = cz < 0 ? cz + nz : cz - nz;
+      }
+      if (bc2 == 1 && (cz == 0 || cz == nz - 1)) return false;
+    }
+    out = idx(cx, cy, cz);
+    return true;
+  }
+};
+
+// Load the pre-collision population i of cell (x,y,z) at the given AA parity.
+template <class S, int Q>
+__device__ __forceinline__ typename Stor<S>::T load_in(const S* __restrict__ A, const Geom& g, int parity, int x,
+                                                        int y, int z, int64_t c, int i, float ref) {
+  typedef typename Stor<S>::T T;
+  const T w = T(wq<Q>(i));
+  if (parity == 0) return Stor<S>::ld(A + (int64_t)i * g.stride + c, w, ref);
+  int64_t s;
+  if (g.nbr(x, y, z, -ex(i), -ey(i), -ez(i), s)) return Stor<S>::ld(A + (int64_t)inv(i) * g.stride + s, w, ref);
+  return Stor<S>::ld(A + (int64_t)i * g.stride + c, w, ref);
+}
+
+// Store the post-collision population i of cell (x,y,z) at the given parity.
+template <class S, int Q>
+__device__ __forceinline__ void store_out(S* __restrict__ A, const Geom& g, int parity, int x, int y, int z, int64_t c,
+                                          int i, typename Stor<S>::T v, float ref) {
+  typedef typename Stor<S>::T T;
+  const T w = T(wq<Q>(i));
+  if (parity == 0) {
+    Stor<S>::st(A + (int64_t)inv(i) * g.stride + c, v, w, ref);
+    return;
+  }
+  int64_t d;
+  if (g.nbr(x, y, z, ex(i), ey(i), ez(i), d))
+    Stor<S>::st(A + (int64_t)i * g.stride + d, v, w, ref);
+  else
+    Stor<S>::st(A + (int64_t)inv(i) * g.stride + c, v, w, ref);
+}
+
+// Post-collision population i of a cell in the layout left after `steps_done`
+// loops (used by field output and checkpoints).
+template <class S, int Q>
+__device__ __forceinline__ typename Stor<S>::T load_out(const S* __restrict__ A, const Geom& g, int64_t steps_done,
+                                                         int x, int y, int z, int64_t c, int i, float ref) {
+  typedef typename Stor<S>::T T;
+  const T w = T(wq<Q>(i));
+  if (steps_done & 1) return Stor<S>::ld(A + (int64_t)inv(i) * g.stride + c, w, ref);
+  int64_t d;
+  if (g.nbr(x, y, z, ex(i), ey(i), ez(i), d)) return Stor<S>::ld(A + (int64_t)i * g.stride + d, w, ref);
+  return Stor<S>::ld(A + (int64_t)inv(i) * g.stride + c, w, ref);
+}
+
+// Inverse of load_out: place post-collision population i so that the next
+// loop (parity = steps_done & 1) reads it as the streamed value.
+template <class S, int Q>
+__device__ __forceinline__ void store_out_layout(S* __restrict__ A, const Geom& g, int64_t steps_done, int x, int y,
+                                                 int z, int64_t c, int i, typename Stor<S>::T v, float ref) {
+  store_out<S, Q>(A, g, (int)((steps_done + 1) & 1), x, y, z, c, i, v, ref);
+}
+
+}  // namespace mkd
+
+#endif

@@ -1,0 +1,93 @@
+// mk_engine.hpp — internal interface between the C ABI (mk_api.cpp) and the
+// kernels (mk_kernels.cu).  Not installed; no torch types anywhere.
+#ifndef MK_ENGINE_HPP
+#define MK_ENGINE_HPP
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/mkb200.h"
+
+namespace mke {
+
+// Number of FP64 diagnostic accumulators.
+enum {
+  DG_MASS = 0,
+  DG_MX,
+  DG_MY,
+  DG_MZ,
+  DG_PHI,
+  DG_SOLID,
+  DG_HEAT,
+  DG_SOLUTE,
+  DG_MAXU,
+  DG_BAD,
+  DG_FLUID,
+  DG_N
+};
+
+struct Engine {
+  mk_params p;
+  int nx, ny, nz;
+  int64_t ncell;
+  int64_t stride;     // population plane stride in cells
+  int elem;           // bytes per stored population
+  int phi_elem;       // bytes per phi / temperature value (8 for FP64, else 4)
+  int Q0, Q1;         // populations of lattice 0 and 1 (0 if absent)
+  int64_t step;       // completed loops
+  int phi_cur;        // dendrites: index of the current phi buffer
+  cudaStream_t stream;
+  int device;
+  int block_x, block_y;
+  // device buffers
+  void* pop0;
+  void* pop1;
+  void* phi[2];
+  void* temp;
+  double* seeds;      // n_objects * 12 doubles: centre (3), rotation (9, row-major, columns = crystal axes)
+  double* partial;    // diagnostics scratch, DG_N doubles per block
+  int partial_blocks;
+  double* dsum;       // DG_N doubles
+  double* field;      // ncell doubles (field output staging)
+  float* field32;     // ncell floats (FP32 field output staging, allocated on first use)
+  float* stage32;     // 2 * ncell floats (FP32 state upload staging, allocated on first use)
+  // launch counters
+  int64_t launches;
+};
+
+// Allocate and zero device buffers for p.  Returns cudaSuccess or an error.
+cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x, int block_y, std::string& err);
+void engine_free(Engine& e);
+
+// Initialise populations, phi and T/U from host macroscopic fields (ncell
+// doubles each; NULL uses the value the case defines as uniform default).
+cudaError_t engine_set_state(Engine& e, const double* phi, const double* temp, const double* rho, const double* ux,
+                             const double* uy, const double* uz);
+
+// Same from FP32 host arrays (phi and T/U; NULL keeps the uniform default).
+cudaError_t engine_set_state_f32(Engine& e, const float* phi, const float* temp);
+
+// Field as FP32 into e.field32 (device).
+cudaError_t engine_field_f32(Engine& e, int field);
+
+// One loop.  When `ev` is non-null, ev[2k], ev[2k+1] bracket the k-th kernel.
+cudaError_t engine_step(Engine& e, cudaEvent_t* ev);
+int engine_kernels_per_step(const Engine& e);
+const char* engine_kernel_name(const Engine& e, int k);
+
+// Compute a macroscopic field of the current state into e.field (device).
+cudaError_t engine_field(Engine& e, int field);
+
+// FP64 diagnostics (two-pass reduction into e.dsum); host copy in out[DG_N].
+cudaError_t engine_diag(Engine& e, double* out);
+
+// Raw state for checkpoints: populations in their storage format.
+size_t engine_pop_bytes(const Engine& e, int which);
+
+double engine_bytes_per_cell(const Engine& e);
+
+}  // namespace mke
+
+#endif

@@ -1,0 +1,1183 @@
+// mk_kernels.cu — sm_100a kernels of the coupled step and their launchers.
+//
+// K1 k_flow          fused collide + AA stream, D3Q19/D3Q27, BGK/TRT/MRT, Guo
+//                    forcing, half-way bounce-back           (mkFluidsLBM::propagate/
+//                    relaxation, mkFluidsLBM.h:47-49; mkNode::collision_*, mkNode.h:74-87)
+// K4 k_mp_phi        phi = sum h of the streamed Allen-Cahn populations
+//    k_mp_collide    MRT pressure/velocity lattice + conservative Allen-Cahn lattice,
+//                    surface tension, gravity, wetting       (mkFluidsMultiphase::propagate/
+//                    relaxation, mkFluidsMultiphase.h:52-57; getEquPDFsLiang/PhiLiang, mkNode.h:38-40)
+// K3 k_pf_phi        phi = sum g of the streamed phase-field populations
+// K2/K3 k_dend_collide  anisotropic phase field + D3Q7 thermal ADE with latent heat
+//                    (mkPhaseField::relaxation_anisotropy_thermal, mkPhaseField.h:46;
+//                    mkThermalField::propagate/relaxation, mkThermalField.h:33-34)
+// K6 k_diag_*        FP64 warp-shuffle reductions (check_variables, mkFluidsLBM.h:55)
+//
+// All kernels are HBM-bound stencils: one thread per cell, x fastest, so a
+// warp touches 32 consecutive cells of every population plane.  No tensor
+// cores: the step is not a contraction.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mk_device.cuh"
+#include "mk_engine.hpp"
+
+using namespace mkd;
+
+namespace {
+
+template <class S>
+struct PhiOf {
+  typedef float type;
+};
+template <>
+struct PhiOf<double> {
+  typedef double type;
+};
+
+// Reference values of the shifted 16-bit storage (f_i / w_i - ref).
+struct Refs {
+  float r0, r1;
+};
+
+// ================================================================ FLOW (K1)
+template <class T>
+struct FlowK {
+  T om, om_m, Fx, Fy, Fz;
+  float ref;
+};
+
+template <class S, int Q, int COLL, int PARITY>
+__global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, const FlowK<typename Stor<S>::T> k) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int64_t c = g.idx(x, y, z);
+  T f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = load_in<S, Q>(A, g, PARITY, x, y, z, c, i, k.ref);
+  T rho = T(0), jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    rho += f[i];
+    if (ex(i)) jx += T(ex(i)) * f[i];
+    if (ey(i)) jy += T(ey(i)) * f[i];
+    if (ez(i)) jz += T(ez(i)) * f[i];
+  }
+  const T ux = (jx + T(0.5) * k.Fx) / rho;
+  const T uy = (jy + T(0.5) * k.Fy) / rho;
+  const T uz = (jz + T(0.5) * k.Fz) / rho;
+  const T uu = ux * ux + uy * uy + uz * uz;
+  const T uF = ux * k.Fx + uy * k.Fy + uz * k.Fz;
+  T feq[Q], Fi[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const T w = T(wq<Q>(i));
+    const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
+    const T eF = T(ex(i)) * k.Fx + T(ey(i)) * k.Fy + T(ez(i)) * k.Fz;
+    feq[i] = rho * (w * (T(1) + T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu));
+    Fi[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF);
+  }
+  if (COLL == MK_COLL_BGK) {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] += -k.om * (f[i] - feq[i]) + (T(1) - T(0.5) * k.om) * Fi[i];
+  } else if (COLL == MK_COLL_TRT) {
+    T fo[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const int j = inv(i);
+      const T fp = T(0.5) * (f[i] + f[j]), fm = T(0.5) * (f[i] - f[j]);
+      const T ep = T(0.5) * (feq[i] + feq[j]), em = T(0.5) * (feq[i] - feq[j]);
+      const T Fp = T(0.5) * (Fi[i] + Fi[j]), Fm = T(0.5) * (Fi[i] - Fi[j]);
+      fo[i] = f[i] - k.om * (fp - ep) - k.om_m * (fm - em) + (T(1) - T(0.5) * k.om) * Fp +
+              (T(1) - T(0.5) * k.om_m) * Fm;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = fo[i];
+  } else {
+    if constexpr (Q == 19) mrt19_collide<T>(f, feq, Fi, k.om);
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) store_out<S, Q>(A, g, PARITY, x, y, z, c, i, f[i], k.ref);
+}
+
+// ========================================================= MULTIPHASE (K4)
+template <class T>
+struct MpK {
+  T beta, kappa, om_h, coef_wet, inv_w4, rho_l, rho_g, tau_l, tau_g, gx, gy, gz;
+  float ref_g, ref_h;
+};
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, P* __restrict__ phi, const Geom g, float ref_h) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int64_t c = g.idx(x, y, z);
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < 19; ++i) s += load_in<S, 19>(H, g, PARITY, x, y, z, c, i, ref_h);
+  phi[c] = P(s);
+}
+
+// Density, phi gradient and total force of a fluid cell (shared by the
+// collision and by field output so both see identical values).
+template <class T, class P>
+__device__ __forceinline__ void mp_force(const P* __restrict__ phi, const Geom& g, int x, int y, int z, int64_t c,
+                                         const MpK<T>& k, T pstar, T& ph, T& rho, T (&gp)[3], T (&F)[3]) {
+  ph = T(phi[c]);
+  const T wall = ph + k.coef_wet * ph * (T(1) - ph);
+  T gx = T(0), gy = T(0), gz = T(0), l = T(0);
+#pragma unroll
+  for (int i = 1; i < 19; ++i) {
+    int64_t j;
+    const T fn = g.nbr(x, y, z, ex(i), ey(i), ez(i), j) ? T(__ldg(phi + j)) : wall;
+    const T w = T(wq<19>(i));
+    if (ex(i)) gx += (w * T(ex(i))) * fn;
+    if (ey(i)) gy += (w * T(ey(i))) * fn;
+    if (ez(i)) gz += (w * T(ez(i))) * fn;
+    l += w * (fn - ph);
+  }
+  gp[0] = T(3) * gx;
+  gp[1] = T(3) * gy;
+  gp[2] = T(3) * gz;
+  const T lap = T(6) * l;
+  const T drho = k.rho_l - k.rho_g;
+  rho = k.rho_g + ph * drho;
+  const T mu = T(4) * k.beta * ph * (ph - T(1)) * (ph - T(0.5)) - k.kappa * lap;
+  const T pg = pstar * (T(1) / T(3)) * drho;
+  F[0] = mu * gp[0] + rho * k.gx - pg * gp[0];
+  F[1] = mu * gp[1] + rho * k.gy - pg * gp[1];
+  F[2] = mu * gp[2] + rho * k.gz - pg * gp[2];
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mp_collide(S* __restrict__ G, S* __restrict__ H, const P* __restrict__ phi,
+                                                    const Geom g, const MpK<typename Stor<S>::T> k) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int64_t c = g.idx(x, y, z);
+  T gp_[19], h[19];
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    gp_[i] = load_in<S, 19>(G, g, PARITY, x, y, z, c, i, k.ref_g);
+    h[i] = load_in<S, 19>(H, g, PARITY, x, y, z, c, i, k.ref_h);
+  }
+  T pstar = T(0), jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    pstar += gp_[i];
+    if (ex(i)) jx += T(ex(i)) * gp_[i];
+    if (ey(i)) jy += T(ey(i)) * gp_[i];
+    if (ez(i)) jz += T(ez(i)) * gp_[i];
+  }
+  T ph, rho, gphi[3], F[3];
+  mp_force<T, P>(phi, g, x, y, z, c, k, pstar, ph, rho, gphi, F);
+  const T ux = jx + F[0] / (T(2) * rho);
+  const T uy = jy + F[1] / (T(2) * rho);
+  const T uz = jz + F[2] / (T(2) * rho);
+  const T uu = ux * ux + uy * uy + uz * uz;
+  const T uF = ux * F[0] + uy * F[1] + uz * F[2];
+  const T tau = k.tau_g + ph * (k.tau_l - k.tau_g);
+  const T gn = sqrt(gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2]);
+  const T inv_gn = T(1) / (gn + T(1e-12));
+  const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
+  const T lam = k.inv_w4 * ph * (T(1) - ph);
+  const T irho = T(1) / rho;
+  T geq[19], Fb[19];
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    const T w = T(wq<19>(i));
+    const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
+    const T eF = T(ex(i)) * F[0] + T(ey(i)) * F[1] + T(ez(i)) * F[2];
+    const T en = T(ex(i)) * nx_ + T(ey(i)) * ny_ + T(ez(i)) * nz_;
+    const T poly = T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu;
+    geq[i] = w * (pstar + poly);
+    Fb[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF) * irho;
+    const T heq = ph * (w * (T(1) + poly));
+    h[i] += -k.om_h * (h[i] - heq) + (T(1) - T(0.5) * k.om_h) * w * lam * en;
+  }
+  mrt19_collide<T>(gp_, geq, Fb, T(1) / tau);
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    store_out<S, 19>(G, g, PARITY, x, y, z, c, i, gp_[i], k.ref_g);
+    store_out<S, 19>(H, g, PARITY, x, y, z, c, i, h[i], k.ref_h);
+  }
+}
+
+// ========================================================== DENDRITE (K2/K3)
+template <class T>
+struct DendK {
+  T om_g, om_t, inv_tau0, lambda, eps4;
+  int nobj;
+  float ref_g, ref_t;
+};
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P* __restrict__ phi_old,
+                                                P* __restrict__ phi_new, const Geom g, float ref_g) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  if (!g.fluid(x, y, z)) {
+    phi_new[c] = phi_old[c];
+    return;
+  }
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) s += load_in<S, 7>(G, g, PARITY, x, y, z, c, i, ref_g);
+  phi_new[c] = P(s);
+}
+
+// Nearest seed (ties to the lower index), in FP64 like the oracle.
+__device__ __forceinline__ int nearest_seed(const double* __restrict__ seeds, int nobj, int x, int y, int z) {
+  int best = 0;
+  double bd = 1e300;
+  for (int k = 0; k < nobj; ++k) {
+    const double dx = x - __ldg(seeds + 12 * k + 0), dy = y - __ldg(seeds + 12 * k + 1),
+                 dz = z - __ldg(seeds + 12 * k + 2);
+    const double d = dx * dx + dy * dy + dz * dz;
+    if (d < bd) {
+      bd = d;
+      best = k;
+    }
+  }
+  return best;
+}
+
+// a(n) and the lab-frame anisotropy vector N of Karma-Rappel 4-fold
+// anisotropy (mkPhaseField::anisotropy, mkPhaseField.h:61).
+template <class T>
+__device__ __forceinline__ void anisotropy(const double* __restrict__ Rm, T eps4, const T (&gr)[3], T& a, T (&N)[3]) {
+  T R[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) R[q] = T(__ldg(Rm + q));
+  const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+  const T inv = T(1) / (gn + T(1e-12));
+  const T nl0 = gr[0] * inv, nl1 = gr[1] * inv, nl2 = gr[2] * inv;
+  T nc[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) nc[q] = R[0 * 3 + q] * nl0 + R[1 * 3 + q] * nl1 + R[2 * 3 + q] * nl2;
+  const T s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
+  a = T(1) - T(3) * eps4 + T(4) * eps4 * s4;
+  T Nc[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) Nc[q] = gn * a * T(16) * eps4 * (nc[q] * nc[q] * nc[q] - nc[q] * s4);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) N[q] = R[q * 3 + 0] * Nc[0] + R[q * 3 + 1] * Nc[1] + R[q * 3 + 2] * Nc[2];
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256)
+    k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
+                   P* __restrict__ temp, const double* __restrict__ seeds, const Geom g,
+                   const DendK<typename Stor<S>::T> k) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int64_t c = g.idx(x, y, z);
+  const T ph = T(phi_new[c]);
+  T gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll
+  for (int i = 1; i < 19; ++i) {
+    int64_t j;
+    const T fn = g.nbr(x, y, z, ex(i), ey(i), ez(i), j) ? T(__ldg(phi_new + j)) : ph;
+    const T w = T(wq<19>(i));
+    if (ex(i)) gx += (w * T(ex(i))) * fn;
+    if (ey(i)) gy += (w * T(ey(i))) * fn;
+    if (ez(i)) gz += (w * T(ez(i))) * fn;
+  }
+  const T gr[3] = {T(3) * gx, T(3) * gy, T(3) * gz};
+  const int gid = k.nobj > 1 ? nearest_seed(seeds, k.nobj, x, y, z) : 0;
+  T a, N[3];
+  anisotropy<T>(seeds + 12 * gid + 3, k.eps4, gr, a, N);
+  const T dphi = ph - T(phi_old[c]);
+  const T u_old = T(temp[c]);
+  const T one_m = T(1) - ph * ph;
+  const T src = (ph - ph * ph * ph - k.lambda * u_old * one_m * one_m) * k.inv_tau0 + (T(1) - a * a) * dphi;
+  const T cs2 = T(0.25);
+  const T B0 = -cs2 * ((a * a - T(1)) * gr[0] + N[0]);
+  const T B1 = -cs2 * ((a * a - T(1)) * gr[1] + N[1]);
+  const T B2 = -cs2 * ((a * a - T(1)) * gr[2] + N[2]);
+  const T fo = (T(1) - T(0.5) * k.om_g) / cs2;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    const T w = T(wq<7>(i));
+    const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
+    const T gi = load_in<S, 7>(G, g, PARITY, x, y, z, c, i, k.ref_g);
+    const T go = gi - k.om_g * (gi - w * ph) + fo * w * eB + w * src;
+    store_out<S, 7>(G, g, PARITY, x, y, z, c, i, go, k.ref_g);
+  }
+  // thermal lattice: relaxation with latent heat (1/2) dphi
+  T t[7];
+  T Tn = T(0);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    t[i] = load_in<S, 7>(Tp, g, PARITY, x, y, z, c, i, k.ref_t);
+    Tn += t[i];
+  }
+  const T lat = T(0.5) * dphi;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    const T w = T(wq<7>(i));
+    const T to = t[i] - k.om_t * (t[i] - w * Tn) + w * lat;
+    store_out<S, 7>(Tp, g, PARITY, x, y, z, c, i, to, k.ref_t);
+  }
+  temp[c] = P(Tn);
+}
+
+// ===================================================================== INIT
+template <class S, int Q>
+__device__ __forceinline__ void put_eq(S* A, const Geom& g, int x, int y, int z, int64_t c, double base_scale,
+                                       double ux, double uy, double uz, double p_extra, float ref) {
+  // population_i = base_scale * w (1 + 3eu + 4.5eu^2 - 1.5u^2) + w p_extra
+  typedef typename Stor<S>::T T;
+  const double uu = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const double w = wq<Q>(i);
+    const double eu = ex(i) * ux + ey(i) * uy + ez(i) * uz;
+    const double v = base_scale * (w * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu)) + w * p_extra;
+    store_out_layout<S, Q>(A, g, 0, x, y, z, c, i, T(v), ref);
+  }
+}
+
+template <class S, class InT>
+__global__ void k_init(int model, int Q0, S* A0, S* A1, typename PhiOf<S>::type* phi0,
+                       typename PhiOf<S>::type* phi1, typename PhiOf<S>::type* temp, const InT* __restrict__ in_phi,
+                       const InT* __restrict__ in_t, const InT* __restrict__ in_rho,
+                       const InT* __restrict__ in_u, double d_rho, double d_ux, double d_uy, double d_uz,
+                       double d_t, const Geom g, int64_t ncell, Refs refs) {
+  typedef typename PhiOf<S>::type P;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  const double ph = in_phi ? in_phi[c] : 0.0;
+  const double ux = in_u ? in_u[c] : d_ux, uy = in_u ? in_u[ncell + c] : d_uy, uz = in_u ? in_u[2 * ncell + c] : d_uz;
+  if (phi0) phi0[c] = P(ph);
+  if (phi1) phi1[c] = P(ph);
+  const double tv = in_t ? in_t[c] : d_t;
+  if (temp) temp[c] = P(tv);
+  if (!g.fluid(x, y, z)) return;
+  if (model == MK_MODEL_FLOW) {
+    const double r = in_rho ? in_rho[c] : d_rho;
+    if (Q0 == 19)
+      put_eq<S, 19>(A0, g, x, y, z, c, r, ux, uy, uz, 0.0, refs.r0);
+    else
+      put_eq<S, 27>(A0, g, x, y, z, c, r, ux, uy, uz, 0.0, refs.r0);
+  } else if (model == MK_MODEL_MULTIPHASE) {
+    // g = geq(p* = 0, u) = w (3eu + 4.5eu^2 - 1.5u^2); h = phi w (1 + ...)
+    put_eq<S, 19>(A0, g, x, y, z, c, 1.0, ux, uy, uz, -1.0, refs.r0);
+    put_eq<S, 19>(A1, g, x, y, z, c, ph, ux, uy, uz, 0.0, refs.r1);
+  } else {
+    put_eq<S, 7>(A0, g, x, y, z, c, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
+    put_eq<S, 7>(A1, g, x, y, z, c, tv, 0.0, 0.0, 0.0, 0.0, refs.r1);
+  }
+}
+
+// =================================================================== FIELDS
+template <class S, int Q>
+__global__ void k_field_flow(const S* __restrict__ A, const Geom g, int64_t steps_done, int field, double Fx, double Fy,
+                             double Fz, double rho0, float ref, double* __restrict__ out) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  if (!g.fluid(x, y, z)) {
+    out[c] = field == MK_FIELD_RHO ? rho0 : 0.0;
+    return;
+  }
+  double rho = 0, j[3] = {0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const double f = double(load_out<S, Q>(A, g, steps_done, x, y, z, c, i, ref));
+    rho += f;
+    j[0] += ex(i) * f;
+    j[1] += ey(i) * f;
+    j[2] += ez(i) * f;
+  }
+  const double F[3] = {Fx, Fy, Fz};
+  out[c] = field == MK_FIELD_RHO ? rho : (j[field - MK_FIELD_UX] - 0.5 * F[field - MK_FIELD_UX]) / rho;
+}
+
+template <class S>
+__global__ void k_field_mp(const S* __restrict__ G, const typename PhiOf<S>::type* __restrict__ phi, const Geom g,
+                           int64_t steps_done, int field, const MpK<typename Stor<S>::T> k, double* __restrict__ out) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  if (field == MK_FIELD_RHO) {
+    out[c] = double(k.rho_g) + double(phi[c]) * (double(k.rho_l) - double(k.rho_g));
+    return;
+  }
+  if (!g.fluid(x, y, z)) {
+    out[c] = 0.0;
+    return;
+  }
+  T pstar = T(0), j[3] = {T(0), T(0), T(0)};
+#pragma unroll
+  for (int i = 0; i < 19; ++i) {
+    const T v = load_out<S, 19>(G, g, steps_done, x, y, z, c, i, k.ref_g);
+    pstar += v;
+    j[0] += T(ex(i)) * v;
+    j[1] += T(ey(i)) * v;
+    j[2] += T(ez(i)) * v;
+  }
+  if (field == MK_FIELD_PRESSURE) {
+    out[c] = double(pstar);
+    return;
+  }
+  T ph, rho, gp[3], F[3];
+  mp_force<T, P>(phi, g, x, y, z, c, k, pstar, ph, rho, gp, F);
+  const int a = field - MK_FIELD_UX;
+  out[c] = double(j[a] - F[a] / (T(2) * rho));
+}
+
+template <class P>
+__global__ void k_field_copy(const P* __restrict__ a, const P* __restrict__ b, int64_t n, double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = b ? double(a[i]) - double(b[i]) : double(a[i]);
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, int64_t n, float* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (float)a[i];
+}
+
+__global__ void k_field_geom(const Geom g, int field, const double* __restrict__ seeds, int nobj,
+                             double* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  if (field == MK_FIELD_FLAG)
+    out[c] = g.fluid(x, y, z) ? MK_FLAG_FLUID : MK_FLAG_WALLS;
+  else
+    out[c] = nobj > 0 ? nearest_seed(seeds, nobj, x, y, z) : 0;
+}
+
+// ============================================================ DIAGNOSTICS (K6)
+__device__ __forceinline__ void warp_reduce(double (&v)[mke::DG_N]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < mke::DG_N; ++q) {
+      const double r = __shfl_down_sync(0xffffffffu, v[q], o);
+      v[q] = q == mke::DG_MAXU ? fmax(v[q], r) : v[q] + r;
+    }
+  }
+}
+
+// Block-level reduction of per-thread partials into partial[blockIdx.x].
+__device__ __forceinline__ void block_reduce_store(double (&v)[mke::DG_N], double* __restrict__ partial) {
+  __shared__ double sh[32][mke::DG_N];
+  warp_reduce(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < mke::DG_N; ++q) sh[wid][q] = v[q];
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < mke::DG_N; ++q) v[q] = lane < nw ? sh[lane][q] : (q == mke::DG_MAXU ? 0.0 : 0.0);
+    warp_reduce(v);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < mke::DG_N; ++q) partial[(int64_t)blockIdx.x * mke::DG_N + q] = v[q];
+  }
+}
+
+__device__ __forceinline__ void cell_coords(const Geom& g, int64_t c, int& x, int& y, int& z) {
+  x = (int)(c % g.nx);
+  const int64_t r = c / g.nx;
+  y = (int)(r % g.ny);
+  z = (int)(r / g.ny);
+}
+
+template <class S, int Q>
+__global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, const Geom g, int64_t steps_done, double Fx,
+                                                   double Fy, double Fz, float ref, int64_t n,
+                                                   double* __restrict__ partial) {
+  double v[mke::DG_N];
+#pragma unroll
+  for (int q = 0; q < mke::DG_N; ++q) v[q] = 0.0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_coords(g, c, x, y, z);
+    if (!g.fluid(x, y, z)) continue;
+    double rho = 0, j[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const double f = double(load_out<S, Q>(A, g, steps_done, x, y, z, c, i, ref));
+      rho += f;
+      j[0] += ex(i) * f;
+      j[1] += ey(i) * f;
+      j[2] += ez(i) * f;
+    }
+    const double mx = j[0] - 0.5 * Fx, my = j[1] - 0.5 * Fy, mz = j[2] - 0.5 * Fz;
+    const bool bad = !(rho > 0.0) || !isfinite(rho) || !isfinite(mx) || !isfinite(my) || !isfinite(mz);
+    v[mke::DG_MASS] += rho;
+    v[mke::DG_MX] += mx;
+    v[mke::DG_MY] += my;
+    v[mke::DG_MZ] += mz;
+    v[mke::DG_FLUID] += 1.0;
+    v[mke::DG_BAD] += bad ? 1.0 : 0.0;
+    if (!bad) v[mke::DG_MAXU] = fmax(v[mke::DG_MAXU], sqrt(mx * mx + my * my + mz * mz) / rho);
+  }
+  block_reduce_store(v, partial);
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_diag_mp(const S* __restrict__ G, const typename PhiOf<S>::type* __restrict__ phi,
+                                                 const Geom g, int64_t steps_done, const MpK<typename Stor<S>::T> k,
+                                                 int64_t n, double* __restrict__ partial) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  double v[mke::DG_N];
+#pragma unroll
+  for (int q = 0; q < mke::DG_N; ++q) v[q] = 0.0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_coords(g, c, x, y, z);
+    if (!g.fluid(x, y, z)) continue;
+    T pstar = T(0), j[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+      const T f = load_out<S, 19>(G, g, steps_done, x, y, z, c, i, k.ref_g);
+      pstar += f;
+      j[0] += T(ex(i)) * f;
+      j[1] += T(ey(i)) * f;
+      j[2] += T(ez(i)) * f;
+    }
+    T ph, rho, gp[3], F[3];
+    mp_force<T, P>(phi, g, x, y, z, c, k, pstar, ph, rho, gp, F);
+    double u[3];
+    for (int a = 0; a < 3; ++a) u[a] = double(j[a] - F[a] / (T(2) * rho));
+    const double r = double(rho), p = double(ph);
+    const bool bad = !isfinite(p) || !isfinite(double(pstar)) || !(r > 0.0) || !isfinite(u[0]) || !isfinite(u[1]) ||
+                     !isfinite(u[2]);
+    v[mke::DG_MASS] += r;
+    v[mke::DG_MX] += r * u[0];
+    v[mke::DG_MY] += r * u[1];
+    v[mke::DG_MZ] += r * u[2];
+    v[mke::DG_PHI] += p;
+    v[mke::DG_SOLID] += p < 0.5 ? 1.0 : 0.0;
+    v[mke::DG_FLUID] += 1.0;
+    v[mke::DG_BAD] += bad ? 1.0 : 0.0;
+    if (!bad) v[mke::DG_MAXU] = fmax(v[mke::DG_MAXU], sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+  }
+  block_reduce_store(v, partial);
+}
+
+template <class P>
+__global__ void __launch_bounds__(256) k_diag_dend(const P* __restrict__ phi, const P* __restrict__ phi_prev,
+                                                   const P* __restrict__ temp, const Geom g, int solutal, int64_t n,
+                                                   double* __restrict__ partial) {
+  double v[mke::DG_N];
+#pragma unroll
+  for (int q = 0; q < mke::DG_N; ++q) v[q] = 0.0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_coords(g, c, x, y, z);
+    if (!g.fluid(x, y, z)) continue;
+    const double p = double(phi[c]), pp = double(phi_prev[c]), t = double(temp[c]);
+    const bool bad = !isfinite(p) || !isfinite(t);
+    v[mke::DG_PHI] += p;
+    v[mke::DG_SOLID] += p > 0.0 ? 1.0 : 0.0;
+    if (solutal)
+      v[mke::DG_SOLUTE] += t;
+    else
+      v[mke::DG_HEAT] += t - 0.5 * pp;
+    v[mke::DG_FLUID] += 1.0;
+    v[mke::DG_BAD] += bad ? 1.0 : 0.0;
+  }
+  block_reduce_store(v, partial);
+}
+
+// Second pass: one block sums the partials in a fixed order (deterministic).
+__global__ void k_diag_final(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+  double v[mke::DG_N];
+#pragma unroll
+  for (int q = 0; q < mke::DG_N; ++q) v[q] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < mke::DG_N; ++q) {
+      const double r = partial[(int64_t)b * mke::DG_N + q];
+      v[q] = q == mke::DG_MAXU ? fmax(v[q], r) : v[q] + r;
+    }
+  __shared__ double sh[32][mke::DG_N];
+  warp_reduce(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int q = 0; q < mke::DG_N; ++q) sh[wid][q] = v[q];
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int q = 0; q < mke::DG_N; ++q) v[q] = lane < nw ? sh[lane][q] : 0.0;
+    warp_reduce(v);
+    if (lane == 0)
+      for (int q = 0; q < mke::DG_N; ++q) out[q] = v[q];
+  }
+}
+
+// ================================================================ launchers
+Geom make_geom(const mke::Engine& e) {
+  Geom g;
+  g.nx = e.nx;
+  g.ny = e.ny;
+  g.nz = e.nz;
+  g.bc0 = e.p.bc[0];
+  g.bc1 = e.p.bc[1];
+  g.bc2 = e.p.bc[2];
+  g.stride = e.stride;
+  return g;
+}
+
+void launch_dims(const mke::Engine& e, dim3& grid, dim3& block) {
+  block = dim3(e.block_x, e.block_y, 1);
+  grid = dim3((e.nx + e.block_x - 1) / e.block_x, (e.ny + e.block_y - 1) / e.block_y, e.nz);
+}
+
+// Reference values of the shifted storage per lattice.
+Refs refs_of(const mk_params& p) {
+  Refs r{0.f, 0.f};
+  if (p.model == MK_MODEL_FLOW) {
+    r.r0 = (float)p.rho0;
+  } else if (p.model == MK_MODEL_MULTIPHASE) {
+    r.r0 = 0.f;  // g: rest state 0
+    r.r1 = 1.f;  // h: liquid phi = 1
+  } else {
+    r.r0 = -1.f;               // g: liquid phi = -1
+    r.r1 = (float)(-p.delta);  // t/U: far-field value
+  }
+  return r;
+}
+
+template <class T>
+FlowK<T> flow_coef(const mk_params& p, float ref) {
+  FlowK<T> k;
+  k.om = T(1.0 / p.tau);
+  k.om_m = T(1.0 / (0.5 + p.magic / (p.tau - 0.5)));
+  k.Fx = T(p.force[0]);
+  k.Fy = T(p.force[1]);
+  k.Fz = T(p.force[2]);
+  k.ref = ref;
+  return k;
+}
+
+template <class T>
+MpK<T> mp_coef(const mk_params& p, Refs r) {
+  MpK<T> k;
+  k.beta = T(12.0 * p.sigma / p.width);
+  k.kappa = T(1.5 * p.sigma * p.width);
+  k.om_h = T(1.0 / (3.0 * p.mobility + 0.5));
+  k.coef_wet = T(4.0 * std::cos(p.contact_angle * M_PI / 180.0) / p.width);
+  k.inv_w4 = T(4.0 / p.width);
+  k.rho_l = T(p.rho_l);
+  k.rho_g = T(p.rho_g);
+  k.tau_l = T(p.tau_l);
+  k.tau_g = T(p.tau_g);
+  k.gx = T(p.force[0]);
+  k.gy = T(p.force[1]);
+  k.gz = T(p.force[2]);
+  k.ref_g = r.r0;
+  k.ref_h = r.r1;
+  return k;
+}
+
+template <class T>
+DendK<T> dend_coef(const mk_params& p, Refs r) {
+  DendK<T> k;
+  const double D0 = p.W0 * p.W0 / p.tau0;
+  k.om_g = T(1.0 / (4.0 * D0 + 0.5));
+  k.om_t = T(1.0 / (4.0 * p.D + 0.5));
+  k.inv_tau0 = T(1.0 / p.tau0);
+  k.lambda = T(p.lambda);
+  k.eps4 = T(p.eps4);
+  k.nobj = p.n_objects;
+  k.ref_g = r.r0;
+  k.ref_t = r.r1;
+  return k;
+}
+
+template <class S, int Q, int COLL>
+void launch_flow_t(mke::Engine& e, int parity, dim3 grid, dim3 block) {
+  typedef typename Stor<S>::T T;
+  const Geom g = make_geom(e);
+  const FlowK<T> k = flow_coef<T>(e.p, refs_of(e.p).r0);
+  S* A = (S*)e.pop0;
+  if (parity == 0)
+    k_flow<S, Q, COLL, 0><<<grid, block, 0, e.stream>>>(A, g, k);
+  else
+    k_flow<S, Q, COLL, 1><<<grid, block, 0, e.stream>>>(A, g, k);
+}
+
+template <class S>
+void launch_flow(mke::Engine& e, int parity, dim3 grid, dim3 block) {
+  const int Q = e.p.lattice, C = e.p.collision;
+  if (Q == 19) {
+    if (C == MK_COLL_BGK)
+      launch_flow_t<S, 19, MK_COLL_BGK>(e, parity, grid, block);
+    else if (C == MK_COLL_TRT)
+      launch_flow_t<S, 19, MK_COLL_TRT>(e, parity, grid, block);
+    else
+      launch_flow_t<S, 19, MK_COLL_MRT>(e, parity, grid, block);
+  } else {
+    if (C == MK_COLL_BGK)
+      launch_flow_t<S, 27, MK_COLL_BGK>(e, parity, grid, block);
+    else
+      launch_flow_t<S, 27, MK_COLL_TRT>(e, parity, grid, block);
+  }
+}
+
+template <class S>
+void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  const MpK<T> k = mp_coef<T>(e.p, r);
+  S* G = (S*)e.pop0;
+  S* H = (S*)e.pop1;
+  P* phi = (P*)e.phi[0];
+  if (ev) cudaEventRecord(ev[0], e.stream);
+  if (parity == 0)
+    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, phi, g, r.r1);
+  else
+    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, phi, g, r.r1);
+  if (ev) {
+    cudaEventRecord(ev[1], e.stream);
+    cudaEventRecord(ev[2], e.stream);
+  }
+  if (parity == 0)
+    k_mp_collide<S, P, 0><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+  else
+    k_mp_collide<S, P, 1><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+  if (ev) cudaEventRecord(ev[3], e.stream);
+}
+
+template <class S>
+void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  const DendK<T> k = dend_coef<T>(e.p, r);
+  S* G = (S*)e.pop0;
+  S* Tp = (S*)e.pop1;
+  P* phi_old = (P*)e.phi[e.phi_cur];
+  P* phi_new = (P*)e.phi[1 - e.phi_cur];
+  P* temp = (P*)e.temp;
+  if (ev) cudaEventRecord(ev[0], e.stream);
+  if (parity == 0)
+    k_pf_phi<S, P, 0><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, r.r0);
+  else
+    k_pf_phi<S, P, 1><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, r.r0);
+  if (ev) {
+    cudaEventRecord(ev[1], e.stream);
+    cudaEventRecord(ev[2], e.stream);
+  }
+  if (parity == 0)
+    k_dend_collide<S, P, 0><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+  else
+    k_dend_collide<S, P, 1><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+  if (ev) cudaEventRecord(ev[3], e.stream);
+}
+
+template <class S>
+void step_t(mke::Engine& e, cudaEvent_t* ev) {
+  dim3 grid, block;
+  launch_dims(e, grid, block);
+  const int parity = (int)(e.step & 1);
+  switch (e.p.model) {
+    case MK_MODEL_FLOW:
+      if (ev) cudaEventRecord(ev[0], e.stream);
+      launch_flow<S>(e, parity, grid, block);
+      if (ev) cudaEventRecord(ev[1], e.stream);
+      e.launches += 1;
+      break;
+    case MK_MODEL_MULTIPHASE:
+      launch_mp<S>(e, parity, grid, block, ev);
+      e.launches += 2;
+      break;
+    default:
+      launch_dend<S>(e, parity, grid, block, ev);
+      e.phi_cur = 1 - e.phi_cur;
+      e.launches += 2;
+      break;
+  }
+  e.step += 1;
+}
+
+template <class S, class InT>
+cudaError_t set_state_t(mke::Engine& e, const InT* d_phi, const InT* d_t, const InT* d_rho, const InT* d_u) {
+  typedef typename PhiOf<S>::type P;
+  dim3 grid, block;
+  launch_dims(e, grid, block);
+  const Geom g = make_geom(e);
+  k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, (P*)e.phi[0], (P*)e.phi[1],
+                                          (P*)e.temp, d_phi, d_t, d_rho, d_u, e.p.rho0, e.p.u0[0], e.p.u0[1],
+                                          e.p.u0[2], -e.p.delta, g, e.ncell, refs_of(e.p));
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t field_t(mke::Engine& e, int field) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  dim3 grid, block;
+  launch_dims(e, grid, block);
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  const int m = e.p.model;
+  const int nb = (int)((e.ncell + 255) / 256);
+  if (field == MK_FIELD_FLAG || field == MK_FIELD_GRAIN) {
+    const int nobj = (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE) ? e.p.n_objects : 0;
+    k_field_geom<<<grid, block, 0, e.stream>>>(g, field, e.seeds, nobj, e.field);
+    return cudaGetLastError();
+  }
+  if (field == MK_FIELD_PHI) {
+    k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.phi[e.phi_cur], nullptr, e.ncell, e.field);
+    return cudaGetLastError();
+  }
+  if (m == MK_MODEL_FLOW) {
+    if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ)
+      return cudaErrorInvalidValue;
+    if (e.p.lattice == 19)
+      k_field_flow<S, 19><<<grid, block, 0, e.stream>>>((const S*)e.pop0, g, e.step, field, e.p.force[0],
+                                                        e.p.force[1], e.p.force[2], e.p.rho0, r.r0, e.field);
+    else
+      k_field_flow<S, 27><<<grid, block, 0, e.stream>>>((const S*)e.pop0, g, e.step, field, e.p.force[0],
+                                                        e.p.force[1], e.p.force[2], e.p.rho0, r.r0, e.field);
+    return cudaGetLastError();
+  }
+  if (m == MK_MODEL_MULTIPHASE) {
+    if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ &&
+        field != MK_FIELD_PRESSURE)
+      return cudaErrorInvalidValue;
+    k_field_mp<S><<<grid, block, 0, e.stream>>>((const S*)e.pop0, (const P*)e.phi[0], g, e.step, field,
+                                                mp_coef<T>(e.p, r), e.field);
+    return cudaGetLastError();
+  }
+  if (field == MK_FIELD_T || field == MK_FIELD_C) {
+    if ((field == MK_FIELD_T) != (m == MK_MODEL_THERMAL_DENDRITE)) return cudaErrorInvalidValue;
+    k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.temp, nullptr, e.ncell, e.field);
+    return cudaGetLastError();
+  }
+  if (field == MK_FIELD_DPHI) {
+    k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.phi[e.phi_cur], (const P*)e.phi[1 - e.phi_cur], e.ncell,
+                                              e.field);
+    return cudaGetLastError();
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class S>
+cudaError_t diag_t(mke::Engine& e) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  const int nb = e.partial_blocks;
+  const int m = e.p.model;
+  if (m == MK_MODEL_FLOW) {
+    if (e.p.lattice == 19)
+      k_diag_flow<S, 19><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, g, e.step, e.p.force[0], e.p.force[1],
+                                                   e.p.force[2], r.r0, e.ncell, e.partial);
+    else
+      k_diag_flow<S, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, g, e.step, e.p.force[0], e.p.force[1],
+                                                   e.p.force[2], r.r0, e.ncell, e.partial);
+  } else if (m == MK_MODEL_MULTIPHASE) {
+    k_diag_mp<S><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, (const P*)e.phi[0], g, e.step, mp_coef<T>(e.p, r),
+                                           e.ncell, e.partial);
+  } else {
+    k_diag_dend<P><<<nb, 256, 0, e.stream>>>((const P*)e.phi[e.phi_cur], (const P*)e.phi[1 - e.phi_cur],
+                                             (const P*)e.temp, g, m == MK_MODEL_SOLUTAL_DENDRITE ? 1 : 0, e.ncell,
+                                             e.partial);
+  }
+  k_diag_final<<<1, 256, 0, e.stream>>>(e.partial, nb, e.dsum);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+namespace mke {
+
+static int store_bytes(int prec) { return prec == MK_PREC_FP64 ? 8 : (prec == MK_PREC_FP32 ? 4 : 2); }
+
+cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x, int block_y, std::string& err) {
+  std::memset(&e, 0, sizeof(e));
+  e.p = p;
+  e.nx = p.nx;
+  e.ny = p.ny;
+  e.nz = p.nz;
+  e.ncell = (int64_t)p.nx * p.ny * p.nz;
+  e.stride = (e.ncell + 63) / 64 * 64;
+  e.elem = store_bytes(p.precision);
+  e.phi_elem = p.precision == MK_PREC_FP64 ? 8 : 4;
+  e.device = device;
+  if (p.model == MK_MODEL_FLOW) {
+    e.Q0 = p.lattice;
+    e.Q1 = 0;
+  } else if (p.model == MK_MODEL_MULTIPHASE) {
+    e.Q0 = 19;
+    e.Q1 = 19;
+  } else {
+    e.Q0 = 7;
+    e.Q1 = 7;
+  }
+  // Launch shape: a full warp row along x, rows stacked in y to 256 threads.
+  int bx = block_x > 0 ? block_x : (p.nx >= 128 ? 128 : (p.nx >= 64 ? 64 : 32));
+  int by = block_y > 0 ? block_y : 256 / bx;
+  if (bx * by > 1024 || bx < 1 || by < 1) {
+    err = "invalid block shape";
+    return cudaErrorInvalidValue;
+  }
+  e.block_x = bx;
+  e.block_y = by;
+  cudaError_t st = cudaSetDevice(device);
+  if (st != cudaSuccess) return st;
+  st = cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking);
+  if (st != cudaSuccess) return st;
+  auto alloc = [&](void** ptr, size_t bytes) -> cudaError_t {
+    if (bytes == 0) {
+      *ptr = nullptr;
+      return cudaSuccess;
+    }
+    cudaError_t s = cudaMalloc(ptr, bytes);
+    if (s != cudaSuccess) return s;
+    return cudaMemsetAsync(*ptr, 0, bytes, e.stream);
+  };
+  if ((st = alloc(&e.pop0, (size_t)e.Q0 * e.stride * e.elem)) != cudaSuccess) return st;
+  if ((st = alloc(&e.pop1, (size_t)e.Q1 * e.stride * e.elem)) != cudaSuccess) return st;
+  if ((st = alloc(&e.phi[0], (size_t)e.ncell * e.phi_elem)) != cudaSuccess) return st;
+  const bool dend = p.model == MK_MODEL_THERMAL_DENDRITE || p.model == MK_MODEL_SOLUTAL_DENDRITE;
+  if ((st = alloc(&e.phi[1], dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
+  if (!dend) e.phi[1] = nullptr;
+  if ((st = alloc(&e.temp, dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
+  // seeds: centre + rotation per object (rotation as in the oracle: R = Rz Ry Rx)
+  const int nobj = p.n_objects > 0 ? p.n_objects : 1;
+  std::vector<double> sd((size_t)12 * nobj, 0.0);
+  for (int k = 0; k < nobj; ++k) {
+    double* s = &sd[12 * k];
+    if (k < p.n_objects) {
+      s[0] = p.obj_center[k][0];
+      s[1] = p.obj_center[k][1];
+      s[2] = p.obj_center[k][2];
+    }
+    const double d2r = M_PI / 180.0;
+    const double ax = (k < p.n_objects ? p.obj_angle[k][0] : 0) * d2r, ay = (k < p.n_objects ? p.obj_angle[k][1] : 0) * d2r,
+                 az = (k < p.n_objects ? p.obj_angle[k][2] : 0) * d2r;
+    const double cx = std::cos(ax), sx = std::sin(ax), cy = std::cos(ay), sy = std::sin(ay), cz = std::cos(az),
+                 sz = std::sin(az);
+    double* R = s + 3;
+    R[0] = cz * cy;
+    R[1] = cz * sy * sx - sz * cx;
+    R[2] = cz * sy * cx + sz * sx;
+    R[3] = sz * cy;
+    R[4] = sz * sy * sx + cz * cx;
+    R[5] = sz * sy * cx - cz * sx;
+    R[6] = -sy;
+    R[7] = cy * sx;
+    R[8] = cy * cx;
+  }
+  if ((st = cudaMalloc((void**)&e.seeds, sd.size() * sizeof(double))) != cudaSuccess) return st;
+  if ((st = cudaMemcpyAsync(e.seeds, sd.data(), sd.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream)) !=
+      cudaSuccess)
+    return st;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  e.partial_blocks = sms * 8;
+  if ((st = cudaMalloc((void**)&e.partial, (size_t)e.partial_blocks * DG_N * sizeof(double))) != cudaSuccess)
+    return st;
+  if ((st = cudaMalloc((void**)&e.dsum, DG_N * sizeof(double))) != cudaSuccess) return st;
+  if ((st = cudaMalloc((void**)&e.field, (size_t)e.ncell * sizeof(double))) != cudaSuccess) return st;
+  // host-side copy of sd must outlive the async copy
+  st = cudaStreamSynchronize(e.stream);
+  return st;
+}
+
+void engine_free(Engine& e) {
+  if (e.stream) cudaStreamSynchronize(e.stream);
+  void* ptrs[] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.seeds, e.partial, e.dsum, e.field, e.field32,
+                  e.stage32};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (e.stream) cudaStreamDestroy(e.stream);
+  std::memset(&e, 0, sizeof(e));
+}
+
+cudaError_t engine_set_state(Engine& e, const double* phi, const double* temp, const double* rho, const double* ux,
+                             const double* uy, const double* uz) {
+  // Stage host fields in one device buffer: phi | T | rho | ux uy uz.
+  const size_t n = (size_t)e.ncell;
+  double* d = nullptr;
+  cudaError_t st = cudaMalloc((void**)&d, 6 * n * sizeof(double));
+  if (st != cudaSuccess) return st;
+  const double* src[6] = {phi, temp, rho, ux, uy, uz};
+  for (int q = 0; q < 6; ++q)
+    if (src[q] && (st = cudaMemcpyAsync(d + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice, e.stream)) !=
+                      cudaSuccess) {
+      cudaFree(d);
+      return st;
+    }
+  const bool has_u = ux && uy && uz;
+  const double* dphi = phi ? d : nullptr;
+  const double* dt = temp ? d + n : nullptr;
+  const double* drho = rho ? d + 2 * n : nullptr;
+  const double* du = has_u ? d + 3 * n : nullptr;
+  e.step = 0;
+  e.phi_cur = 0;
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      st = set_state_t<double, double>(e, dphi, dt, drho, du);
+      break;
+    case MK_PREC_FP32:
+      st = set_state_t<float, double>(e, dphi, dt, drho, du);
+      break;
+    case MK_PREC_FP16:
+      st = set_state_t<__half, double>(e, dphi, dt, drho, du);
+      break;
+    default:
+      st = set_state_t<__nv_bfloat16, double>(e, dphi, dt, drho, du);
+      break;
+  }
+  cudaError_t s2 = cudaStreamSynchronize(e.stream);
+  cudaFree(d);
+  return st != cudaSuccess ? st : s2;
+}
+
+cudaError_t engine_set_state_f32(Engine& e, const float* phi, const float* temp) {
+  // Host arrays go straight into a persistent FP32 staging buffer (a pinned
+  // source makes these plain DMA copies), then one init kernel.
+  const size_t n = (size_t)e.ncell;
+  cudaError_t st;
+  if (!e.stage32 && (st = cudaMalloc((void**)&e.stage32, 2 * n * sizeof(float))) != cudaSuccess) return st;
+  if (phi && (st = cudaMemcpyAsync(e.stage32, phi, n * sizeof(float), cudaMemcpyHostToDevice, e.stream)) !=
+                 cudaSuccess)
+    return st;
+  if (temp && (st = cudaMemcpyAsync(e.stage32 + n, temp, n * sizeof(float), cudaMemcpyHostToDevice, e.stream)) !=
+                  cudaSuccess)
+    return st;
+  const float* dphi = phi ? e.stage32 : nullptr;
+  const float* dt = temp ? e.stage32 + n : nullptr;
+  e.step = 0;
+  e.phi_cur = 0;
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      return set_state_t<double, float>(e, dphi, dt, nullptr, nullptr);
+    case MK_PREC_FP32:
+      return set_state_t<float, float>(e, dphi, dt, nullptr, nullptr);
+    case MK_PREC_FP16:
+      return set_state_t<__half, float>(e, dphi, dt, nullptr, nullptr);
+    default:
+      return set_state_t<__nv_bfloat16, float>(e, dphi, dt, nullptr, nullptr);
+  }
+}
+
+cudaError_t engine_field_f32(Engine& e, int field) {
+  cudaError_t st = engine_field(e, field);
+  if (st != cudaSuccess) return st;
+  if (!e.field32 && (st = cudaMalloc((void**)&e.field32, (size_t)e.ncell * sizeof(float))) != cudaSuccess) return st;
+  const int nb = (int)((e.ncell + 255) / 256);
+  k_to_f32<<<nb, 256, 0, e.stream>>>(e.field, e.ncell, e.field32);
+  return cudaGetLastError();
+}
+
+cudaError_t engine_step(Engine& e, cudaEvent_t* ev) {
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      step_t<double>(e, ev);
+      break;
+    case MK_PREC_FP32:
+      step_t<float>(e, ev);
+      break;
+    case MK_PREC_FP16:
+      step_t<__half>(e, ev);
+      break;
+    default:
+      step_t<__nv_bfloat16>(e, ev);
+      break;
+  }
+  return cudaGetLastError();
+}
+
+int engine_kernels_per_step(const Engine& e) { return e.p.model == MK_MODEL_FLOW ? 1 : 2; }
+
+const char* engine_kernel_name(const Engine& e, int k) {
+  if (e.p.model == MK_MODEL_FLOW) return "collide";
+  return k == 0 ? "phi" : "collide";
+}
+
+cudaError_t engine_field(Engine& e, int field) {
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      return field_t<double>(e, field);
+    case MK_PREC_FP32:
+      return field_t<float>(e, field);
+    case MK_PREC_FP16:
+      return field_t<__half>(e, field);
+    default:
+      return field_t<__nv_bfloat16>(e, field);
+  }
+}
+
+cudaError_t engine_diag(Engine& e, double* out) {
+  cudaError_t st;
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      st = diag_t<double>(e);
+      break;
+    case MK_PREC_FP32:
+      st = diag_t<float>(e);
+      break;
+    case MK_PREC_FP16:
+      st = diag_t<__half>(e);
+      break;
+    default:
+      st = diag_t<__nv_bfloat16>(e);
+      break;
+  }
+  if (st != cudaSuccess) return st;
+  st = cudaMemcpyAsync(out, e.dsum, DG_N * sizeof(double), cudaMemcpyDeviceToHost, e.stream);
+  if (st != cudaSuccess) return st;
+  return cudaStreamSynchronize(e.stream);
+}
+
+size_t engine_pop_bytes(const Engine& e, int which) {
+  return (size_t)(which == 0 ? e.Q0 : e.Q1) * e.stride * e.elem;
+}
+
+double engine_bytes_per_cell(const Engine& e) {
+  // Compulsory traffic: every population read once and written once; phi
+  // written once and read once where a model has it.
+  const double S = e.elem;
+  const double phi = e.p.model == MK_MODEL_FLOW ? 0.0 : 2.0 * e.phi_elem;
+  return 2.0 * (e.Q0 + e.Q1) * S + phi;
+}
+
+}  // namespace mke

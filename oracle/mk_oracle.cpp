@@ -1,0 +1,682 @@
+// mk_oracle.cpp — TEST INFRASTRUCTURE ONLY (see mk_oracle.hpp for the model
+// definitions and the parity status).  FP64, OpenMP, SoA, two-array pull
+// streaming: propagate writes the post-stream ("hlp") populations from the
+// neighbours' post-collision ("out") populations, then relaxation writes
+// "out" again — the order of MaterKit/src/mkFluidsUser.cpp:68-299.
+#include "mk_oracle.hpp"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------- lattices
+// Velocity set of MaterKit/inc/mkLattice.h:33-35 (e, c, inv), in 3D.
+const int E27[27][3] = {
+    {0, 0, 0},   {1, 0, 0},   {-1, 0, 0},  {0, 1, 0},   {0, -1, 0},  {0, 0, 1},  {0, 0, -1},
+    {1, 1, 0},   {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0},  {1, 0, 1},   {-1, 0, -1}, {1, 0, -1},
+    {-1, 0, 1},  {0, 1, 1},   {0, -1, -1}, {0, 1, -1},  {0, -1, 1},  {1, 1, 1},  {-1, -1, -1},
+    {1, 1, -1},  {-1, -1, 1}, {1, -1, 1},  {-1, 1, -1}, {-1, 1, 1},  {1, -1, -1}};
+
+inline int inv_dir(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+
+double weight(int Q, int i) {
+  if (Q == 7) return i == 0 ? 0.25 : 0.125;
+  if (Q == 19) {
+    if (i == 0) return 1.0 / 3.0;
+    if (i <= 6) return 1.0 / 18.0;
+    return 1.0 / 36.0;
+  }
+  // D3Q27
+  if (i == 0) return 8.0 / 27.0;
+  if (i <= 6) return 2.0 / 27.0;
+  if (i <= 18) return 1.0 / 54.0;
+  return 1.0 / 216.0;
+}
+
+// d'Humieres et al. (2002) orthogonal D3Q19 moment basis, the "M" of
+// MaterKit/inc/mkLattice.h:89 for the 3D lattice.
+struct Mrt19 {
+  double M[19][19];
+  double inv_norm[19];
+  Mrt19() {
+    for (int i = 0; i < 19; ++i) {
+      const double ex = E27[i][0], ey = E27[i][1], ez = E27[i][2];
+      const double e2 = ex * ex + ey * ey + ez * ez;
+      M[0][i] = 1.0;
+      M[1][i] = 19.0 * e2 - 30.0;
+      M[2][i] = (21.0 * e2 * e2 - 53.0 * e2 + 24.0) / 2.0;
+      M[3][i] = ex;
+      M[4][i] = (5.0 * e2 - 9.0) * ex;
+      M[5][i] = ey;
+      M[6][i] = (5.0 * e2 - 9.0) * ey;
+      M[7][i] = ez;
+      M[8][i] = (5.0 * e2 - 9.0) * ez;
+      M[9][i] = 3.0 * ex * ex - e2;
+      M[10][i] = (3.0 * e2 - 5.0) * (3.0 * ex * ex - e2);
+      M[11][i] = ey * ey - ez * ez;
+      M[12][i] = (3.0 * e2 - 5.0) * (ey * ey - ez * ez);
+      M[13][i] = ex * ey;
+      M[14][i] = ey * ez;
+      M[15][i] = ex * ez;
+      M[16][i] = (ey * ey - ez * ez) * ex;
+      M[17][i] = (ez * ez - ex * ex) * ey;
+      M[18][i] = (ex * ex - ey * ey) * ez;
+    }
+    for (int k = 0; k < 19; ++k) {
+      double n = 0;
+      for (int i = 0; i < 19; ++i) n += M[k][i] * M[k][i];
+      inv_norm[k] = 1.0 / n;
+    }
+  }
+};
+const Mrt19 MRT;
+
+// Relaxation rates; index 9,11,13,14,15 carry the shear rate.
+void mrt_rates(double s_nu, double S[19]) {
+  for (int k = 0; k < 19; ++k) S[k] = 1.0;
+  S[1] = 1.19;
+  S[2] = 1.4;
+  S[4] = S[6] = S[8] = 1.2;
+  S[10] = S[12] = 1.4;
+  S[16] = S[17] = S[18] = 1.98;
+  S[9] = S[11] = S[13] = S[14] = S[15] = s_nu;
+}
+
+// f* = f - Mi [ S (M(f - feq)) - (I - S/2) M F ]
+void mrt_collide(double* f, const double* feq, const double* F, double s_nu) {
+  double S[19];
+  mrt_rates(s_nu, S);
+  double d[19], fneq[19];
+  for (int i = 0; i < 19; ++i) fneq[i] = f[i] - feq[i];
+  for (int k = 0; k < 19; ++k) {
+    double mn = 0, mf = 0;
+    for (int i = 0; i < 19; ++i) {
+      mn += MRT.M[k][i] * fneq[i];
+      mf += MRT.M[k][i] * F[i];
+    }
+    d[k] = (S[k] * mn - (1.0 - 0.5 * S[k]) * mf) * MRT.inv_norm[k];
+  }
+  for (int i = 0; i < 19; ++i) {
+    double s = 0;
+    for (int k = 0; k < 19; ++k) s += MRT.M[k][i] * d[k];
+    f[i] -= s;
+  }
+}
+
+inline double feq2(double w, double eu, double uu) { return w * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu); }
+
+// Rotation "rotate-order ZYX" of the seed angles (BoltzTechs - thermal.xml:71-75):
+// R = Rz(az) Ry(ay) Rx(ax), angles in degrees.  Columns are the crystal axes.
+void rotation_zyx(const double ang_deg[3], double R[3][3]) {
+  const double d2r = M_PI / 180.0;
+  const double ax = ang_deg[0] * d2r, ay = ang_deg[1] * d2r, az = ang_deg[2] * d2r;
+  const double cx = cos(ax), sx = sin(ax), cy = cos(ay), sy = sin(ay), cz = cos(az), sz = sin(az);
+  // Rz*Ry*Rx
+  R[0][0] = cz * cy;
+  R[0][1] = cz * sy * sx - sz * cx;
+  R[0][2] = cz * sy * cx + sz * sx;
+  R[1][0] = sz * cy;
+  R[1][1] = sz * sy * sx + cz * cx;
+  R[1][2] = sz * sy * cx - cz * sx;
+  R[2][0] = -sy;
+  R[2][1] = cy * sx;
+  R[2][2] = cy * cx;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ state
+struct orc_state {
+  mk_params p;
+  int nx, ny, nz;
+  int64_t n;
+  int64_t step;
+  int Qf;  // populations of lattice 0 (flow / phase field)
+  int Qs;  // populations of lattice 1 (AC h / thermal / solutal), 0 if none
+  std::vector<uint8_t> flag;
+  std::vector<double> f_out, f_hlp;  // lattice 0, [q][cell]
+  std::vector<double> s_out, s_hlp;  // lattice 1
+  std::vector<double> phi, phi_prev, temp, conc, conc_prev;
+  std::vector<int> grain;
+  std::vector<double> rot;  // 9 per object (R, columns = crystal axes)
+};
+
+namespace {
+
+inline int64_t cidx(const orc_state* s, int x, int y, int z) {
+  return (int64_t)x + (int64_t)s->nx * ((int64_t)y + (int64_t)s->ny * z);
+}
+
+// Neighbour of (x,y,z) along (dx,dy,dz), or -1 when it is solid or outside a
+// closed face.  Periodic axes wrap like mkFluidsLBM::neighbor (mkFluidsLBM.h:82).
+inline int64_t nbr(const orc_state* s, int x, int y, int z, int dx, int dy, int dz) {
+  int c[3] = {x + dx, y + dy, z + dz};
+  const int n[3] = {s->nx, s->ny, s->nz};
+  for (int a = 0; a < 3; ++a) {
+    if (c[a] < 0 || c[a] >= n[a]) {
+      if (s->p.bc[a] == MK_BC_PERIODIC)
+        c[a] = (c[a] + n[a]) % n[a];
+      else
+        return -1;
+    }
+  }
+  int64_t j = cidx(s, c[0], c[1], c[2]);
+  return s->flag[j] == MK_FLAG_FLUID ? j : -1;
+}
+
+// Propagate with half-way bounce-back: hlp_i(x) = out_i(x - e_i), or
+// out_inv(i)(x) when x - e_i is not fluid (MaterKit/src/mkFluidsUser.cpp:77-97).
+void propagate(const orc_state* s, int Q, const std::vector<double>& out, std::vector<double>& hlp) {
+  const int64_t n = s->n;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int64_t c = cidx(s, x, y, z);
+        if (s->flag[c] != MK_FLAG_FLUID) continue;
+        for (int i = 0; i < Q; ++i) {
+          const int64_t src = nbr(s, x, y, z, -E27[i][0], -E27[i][1], -E27[i][2]);
+          hlp[(int64_t)i * n + c] = src >= 0 ? out[(int64_t)i * n + src] : out[(int64_t)inv_dir(i) * n + c];
+        }
+      }
+}
+
+// Isotropic gradient and Laplacian of a scalar with D3Q19 weights.  `wall`
+// gives the value substituted at a non-fluid neighbour.
+template <class WallFn>
+void grad_lap(const orc_state* s, const std::vector<double>& f, int x, int y, int z, WallFn wall, double g[3],
+              double* lap) {
+  const int64_t c = cidx(s, x, y, z);
+  const double f0 = f[c];
+  g[0] = g[1] = g[2] = 0;
+  double l = 0;
+  for (int i = 1; i < 19; ++i) {
+    const int64_t j = nbr(s, x, y, z, E27[i][0], E27[i][1], E27[i][2]);
+    const double fn = j >= 0 ? f[j] : wall(f0);
+    const double w = weight(19, i);
+    g[0] += w * E27[i][0] * fn;
+    g[1] += w * E27[i][1] * fn;
+    g[2] += w * E27[i][2] * fn;
+    l += w * (fn - f0);
+  }
+  g[0] *= 3.0;
+  g[1] *= 3.0;
+  g[2] *= 3.0;
+  *lap = 6.0 * l;
+}
+
+// ------------------------------------------------------------ FLOW model
+void flow_force(const orc_state* s, double F[3]) {
+  F[0] = s->p.force[0];
+  F[1] = s->p.force[1];
+  F[2] = s->p.force[2];
+}
+
+void flow_step(orc_state* s) {
+  const int Q = s->Qf;
+  const int64_t n = s->n;
+  propagate(s, Q, s->f_out, s->f_hlp);
+  double F[3];
+  flow_force(s, F);
+  const double tau = s->p.tau;
+  const double om = 1.0 / tau;
+  const double tau_m = 0.5 + s->p.magic / (tau - 0.5);
+  const double om_m = 1.0 / tau_m;
+  const int coll = s->p.collision;
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    double f[27], feq[27], Fi[27];
+    double rho = 0, j[3] = {0, 0, 0};
+    for (int i = 0; i < Q; ++i) {
+      f[i] = s->f_hlp[(int64_t)i * n + c];
+      rho += f[i];
+      j[0] += E27[i][0] * f[i];
+      j[1] += E27[i][1] * f[i];
+      j[2] += E27[i][2] * f[i];
+    }
+    double u[3];
+    for (int a = 0; a < 3; ++a) u[a] = (j[a] + 0.5 * F[a]) / rho;
+    const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const double uF = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
+    for (int i = 0; i < Q; ++i) {
+      const double w = weight(Q, i);
+      const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+      const double eF = E27[i][0] * F[0] + E27[i][1] * F[1] + E27[i][2] * F[2];
+      feq[i] = rho * feq2(w, eu, uu);
+      Fi[i] = w * (3.0 * eF + 9.0 * eu * eF - 3.0 * uF);
+    }
+    if (coll == MK_COLL_BGK) {
+      for (int i = 0; i < Q; ++i) f[i] += -om * (f[i] - feq[i]) + (1.0 - 0.5 * om) * Fi[i];
+    } else if (coll == MK_COLL_TRT) {
+      double fo[27];
+      for (int i = 0; i < Q; ++i) {
+        const int k = inv_dir(i);
+        const double fp = 0.5 * (f[i] + f[k]), fm = 0.5 * (f[i] - f[k]);
+        const double ep = 0.5 * (feq[i] + feq[k]), em = 0.5 * (feq[i] - feq[k]);
+        const double Fp = 0.5 * (Fi[i] + Fi[k]), Fm = 0.5 * (Fi[i] - Fi[k]);
+        fo[i] = f[i] - om * (fp - ep) - om_m * (fm - em) + (1.0 - 0.5 * om) * Fp + (1.0 - 0.5 * om_m) * Fm;
+      }
+      for (int i = 0; i < Q; ++i) f[i] = fo[i];
+    } else {
+      mrt_collide(f, feq, Fi, om);
+    }
+    for (int i = 0; i < Q; ++i) s->f_out[(int64_t)i * n + c] = f[i];
+  }
+}
+
+// --------------------------------------------------------- MULTIPHASE model
+struct MpConst {
+  double beta, kappa, tau_h, om_h, cos_t, W;
+};
+
+MpConst mp_const(const mk_params& p) {
+  MpConst k;
+  k.beta = 12.0 * p.sigma / p.width;
+  k.kappa = 1.5 * p.sigma * p.width;
+  k.tau_h = 3.0 * p.mobility + 0.5;
+  k.om_h = 1.0 / k.tau_h;
+  k.cos_t = cos(p.contact_angle * M_PI / 180.0);
+  k.W = p.width;
+  return k;
+}
+
+// Force, density and phi gradient of a fluid cell at the stored phi.
+struct MpLocal {
+  double phi, rho, gphi[3], F[3];
+};
+
+MpLocal mp_local(const orc_state* s, const MpConst& k, int x, int y, int z, double pstar) {
+  MpLocal L;
+  const int64_t c = cidx(s, x, y, z);
+  L.phi = s->phi[c];
+  const double coef = 4.0 * k.cos_t / k.W;
+  double lap;
+  grad_lap(
+      s, s->phi, x, y, z, [&](double p0) { return p0 + coef * p0 * (1.0 - p0); }, L.gphi, &lap);
+  const mk_params& p = s->p;
+  const double drho = p.rho_l - p.rho_g;
+  L.rho = p.rho_g + L.phi * drho;
+  const double mu = 4.0 * k.beta * L.phi * (L.phi - 1.0) * (L.phi - 0.5) - k.kappa * lap;
+  for (int a = 0; a < 3; ++a)
+    L.F[a] = mu * L.gphi[a] + L.rho * p.force[a] - pstar * (1.0 / 3.0) * drho * L.gphi[a];
+  return L;
+}
+
+void mp_step(orc_state* s) {
+  const int64_t n = s->n;
+  propagate(s, 19, s->f_out, s->f_hlp);  // g (pressure / velocity)
+  propagate(s, 19, s->s_out, s->s_hlp);  // h (Allen-Cahn)
+  // phi = sum h over all fluid cells before any gradient is taken.
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    double ph = 0;
+    for (int i = 0; i < 19; ++i) ph += s->s_hlp[(int64_t)i * n + c];
+    s->phi[c] = ph;
+  }
+  const MpConst k = mp_const(s->p);
+  const mk_params& p = s->p;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int64_t c = cidx(s, x, y, z);
+        if (s->flag[c] != MK_FLAG_FLUID) continue;
+        double g[19], h[19], geq[19], Fb[19];
+        double pstar = 0, j[3] = {0, 0, 0};
+        for (int i = 0; i < 19; ++i) {
+          g[i] = s->f_hlp[(int64_t)i * n + c];
+          h[i] = s->s_hlp[(int64_t)i * n + c];
+          pstar += g[i];
+          j[0] += E27[i][0] * g[i];
+          j[1] += E27[i][1] * g[i];
+          j[2] += E27[i][2] * g[i];
+        }
+        const MpLocal L = mp_local(s, k, x, y, z, pstar);
+        double u[3];
+        for (int a = 0; a < 3; ++a) u[a] = j[a] + L.F[a] / (2.0 * L.rho);
+        const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        const double uF = u[0] * L.F[0] + u[1] * L.F[1] + u[2] * L.F[2];
+        const double tau = p.tau_g + L.phi * (p.tau_l - p.tau_g);
+        const double gn = sqrt(L.gphi[0] * L.gphi[0] + L.gphi[1] * L.gphi[1] + L.gphi[2] * L.gphi[2]);
+        double nrm[3];
+        for (int a = 0; a < 3; ++a) nrm[a] = L.gphi[a] / (gn + 1e-12);
+        const double lam = 4.0 * L.phi * (1.0 - L.phi) / k.W;
+        for (int i = 0; i < 19; ++i) {
+          const double w = weight(19, i);
+          const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+          const double eF = E27[i][0] * L.F[0] + E27[i][1] * L.F[1] + E27[i][2] * L.F[2];
+          const double en = E27[i][0] * nrm[0] + E27[i][1] * nrm[1] + E27[i][2] * nrm[2];
+          geq[i] = w * (pstar + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
+          Fb[i] = w * (3.0 * eF + 9.0 * eu * eF - 3.0 * uF) / L.rho;
+          const double heq = L.phi * feq2(w, eu, uu);
+          h[i] += -k.om_h * (h[i] - heq) + (1.0 - 0.5 * k.om_h) * w * lam * en;
+        }
+        mrt_collide(g, geq, Fb, 1.0 / tau);
+        for (int i = 0; i < 19; ++i) {
+          s->f_out[(int64_t)i * n + c] = g[i];
+          s->s_out[(int64_t)i * n + c] = h[i];
+        }
+      }
+}
+
+// ------------------------------------------------------ DENDRITE models
+// Nearest-seed grain of a cell (ties to the lower index).
+int nearest_seed(const mk_params& p, double x, double y, double z) {
+  int best = 0;
+  double bd = 1e300;
+  for (int k = 0; k < p.n_objects; ++k) {
+    const double dx = x - p.obj_center[k][0], dy = y - p.obj_center[k][1], dz = z - p.obj_center[k][2];
+    const double d = dx * dx + dy * dy + dz * dz;
+    if (d < bd) {
+      bd = d;
+      best = k;
+    }
+  }
+  return best;
+}
+
+// Anisotropy of a cell: returns a(n) and the lab-frame vector N, from the
+// lab gradient and the grain's rotation (columns = crystal axes).
+void anisotropy(const double* R, double eps4, const double g[3], double* a_out, double N[3]) {
+  const double gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  const double inv = 1.0 / (gn + 1e-12);
+  const double nl[3] = {g[0] * inv, g[1] * inv, g[2] * inv};
+  double nc[3];
+  for (int a = 0; a < 3; ++a) nc[a] = R[0 * 3 + a] * nl[0] + R[1 * 3 + a] * nl[1] + R[2 * 3 + a] * nl[2];
+  const double s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
+  const double a = 1.0 - 3.0 * eps4 + 4.0 * eps4 * s4;
+  double Nc[3];
+  for (int k = 0; k < 3; ++k) Nc[k] = gn * a * 16.0 * eps4 * (nc[k] * nc[k] * nc[k] - nc[k] * s4);
+  for (int a2 = 0; a2 < 3; ++a2) N[a2] = R[a2 * 3 + 0] * Nc[0] + R[a2 * 3 + 1] * Nc[1] + R[a2 * 3 + 2] * Nc[2];
+  *a_out = a;
+}
+
+void thermal_dendrite_step(orc_state* s) {
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  // 1. phase-field propagate, phi^n = sum g (MaterKit/src/mkFluidsUser.cpp:147-172).
+  propagate(s, 7, s->f_out, s->f_hlp);
+  std::swap(s->phi_prev, s->phi);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) {
+      s->phi[c] = s->phi_prev[c];
+      continue;
+    }
+    double ph = 0;
+    for (int i = 0; i < 7; ++i) ph += s->f_hlp[(int64_t)i * n + c];
+    s->phi[c] = ph;
+  }
+  // 2. phase-field relaxation with anisotropy and thermal coupling.
+  const double D0 = p.W0 * p.W0 / p.tau0;
+  const double om_g = 1.0 / (4.0 * D0 + 0.5);
+  const double cs2 = 0.25;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int64_t c = cidx(s, x, y, z);
+        if (s->flag[c] != MK_FLAG_FLUID) continue;
+        double gr[3], lap;
+        grad_lap(
+            s, s->phi, x, y, z, [](double p0) { return p0; }, gr, &lap);
+        double a, N[3];
+        anisotropy(&s->rot[9 * s->grain[c]], p.eps4, gr, &a, N);
+        const double ph = s->phi[c];
+        const double dphi = ph - s->phi_prev[c];
+        const double one_m = 1.0 - ph * ph;
+        const double src = (ph - ph * ph * ph - p.lambda * s->temp[c] * one_m * one_m) / p.tau0 + (1.0 - a * a) * dphi;
+        double B[3];
+        for (int k = 0; k < 3; ++k) B[k] = -cs2 * ((a * a - 1.0) * gr[k] + N[k]);
+        for (int i = 0; i < 7; ++i) {
+          const double w = weight(7, i);
+          const double eB = E27[i][0] * B[0] + E27[i][1] * B[1] + E27[i][2] * B[2];
+          const double gi = s->f_hlp[(int64_t)i * n + c];
+          s->f_out[(int64_t)i * n + c] = gi - om_g * (gi - w * ph) + (1.0 - 0.5 * om_g) * w * eB / cs2 + w * src;
+        }
+      }
+  // 3. thermal propagate + relaxation with latent heat (1/2) dphi.
+  propagate(s, 7, s->s_out, s->s_hlp);
+  const double om_t = 1.0 / (4.0 * p.D + 0.5);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    double T = 0;
+    for (int i = 0; i < 7; ++i) T += s->s_hlp[(int64_t)i * n + c];
+    const double lat = 0.5 * (s->phi[c] - s->phi_prev[c]);
+    for (int i = 0; i < 7; ++i) {
+      const double w = weight(7, i);
+      const double ti = s->s_hlp[(int64_t)i * n + c];
+      s->s_out[(int64_t)i * n + c] = ti - om_t * (ti - w * T) + w * lat;
+    }
+    s->temp[c] = T;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C API
+static int g_threads = 0;
+
+extern "C" void orc_set_threads(int n) {
+  g_threads = n;
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#endif
+}
+
+extern "C" int orc_get_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const double* T0, const double* C0,
+                                 const double* rho0, const double* ux0, const double* uy0, const double* uz0) {
+  orc_state* s = new orc_state();
+  s->p = *p;
+  s->nx = p->nx;
+  s->ny = p->ny;
+  s->nz = p->nz;
+  s->n = (int64_t)p->nx * p->ny * p->nz;
+  s->step = 0;
+  const int64_t n = s->n;
+  s->flag.assign(n, MK_FLAG_FLUID);
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int c3[3] = {x, y, z};
+        const int n3[3] = {s->nx, s->ny, s->nz};
+        for (int a = 0; a < 3; ++a)
+          if (p->bc[a] == MK_BC_WALLS && (c3[a] == 0 || c3[a] == n3[a] - 1)) s->flag[cidx(s, x, y, z)] = MK_FLAG_WALLS;
+      }
+  s->phi.assign(n, 0.0);
+  if (phi0) std::memcpy(s->phi.data(), phi0, n * sizeof(double));
+  s->phi_prev = s->phi;
+  s->grain.assign(n, 0);
+  s->rot.assign(9 * (size_t)(p->n_objects > 0 ? p->n_objects : 1), 0.0);
+  s->rot[0] = s->rot[4] = s->rot[8] = 1.0;
+  for (int k = 0; k < p->n_objects; ++k) {
+    double R[3][3];
+    rotation_zyx(p->obj_angle[k], R);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) s->rot[9 * k + 3 * a + b] = R[a][b];
+  }
+  if (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE) {
+    for (int z = 0; z < s->nz; ++z)
+      for (int y = 0; y < s->ny; ++y)
+        for (int x = 0; x < s->nx; ++x) s->grain[cidx(s, x, y, z)] = nearest_seed(*p, x, y, z);
+  }
+
+  if (p->model == MK_MODEL_FLOW) {
+    s->Qf = p->lattice;
+    s->Qs = 0;
+    const int Q = s->Qf;
+    s->f_out.assign((size_t)Q * n, 0.0);
+    s->f_hlp.assign((size_t)Q * n, 0.0);
+    for (int64_t c = 0; c < n; ++c) {
+      const double r = rho0 ? rho0[c] : p->rho0;
+      const double u[3] = {ux0 ? ux0[c] : p->u0[0], uy0 ? uy0[c] : p->u0[1], uz0 ? uz0[c] : p->u0[2]};
+      const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+      for (int i = 0; i < Q; ++i) {
+        const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+        s->f_out[(int64_t)i * n + c] = r * feq2(weight(Q, i), eu, uu);
+      }
+    }
+  } else if (p->model == MK_MODEL_MULTIPHASE) {
+    s->Qf = 19;
+    s->Qs = 19;
+    s->f_out.assign((size_t)19 * n, 0.0);  // g = geq(p* = 0, u = 0) = 0
+    s->f_hlp.assign((size_t)19 * n, 0.0);
+    s->s_out.assign((size_t)19 * n, 0.0);
+    s->s_hlp.assign((size_t)19 * n, 0.0);
+    for (int64_t c = 0; c < n; ++c)
+      for (int i = 0; i < 19; ++i) s->s_out[(int64_t)i * n + c] = weight(19, i) * s->phi[c];
+  } else {
+    s->Qf = 7;
+    s->Qs = 7;
+    s->temp.assign(n, -p->delta);
+    if (p->model == MK_MODEL_THERMAL_DENDRITE && T0) std::memcpy(s->temp.data(), T0, n * sizeof(double));
+    if (p->model == MK_MODEL_SOLUTAL_DENDRITE && C0) std::memcpy(s->temp.data(), C0, n * sizeof(double));
+    s->f_out.assign((size_t)7 * n, 0.0);
+    s->f_hlp.assign((size_t)7 * n, 0.0);
+    s->s_out.assign((size_t)7 * n, 0.0);
+    s->s_hlp.assign((size_t)7 * n, 0.0);
+    for (int64_t c = 0; c < n; ++c)
+      for (int i = 0; i < 7; ++i) {
+        s->f_out[(int64_t)i * n + c] = weight(7, i) * s->phi[c];
+        s->s_out[(int64_t)i * n + c] = weight(7, i) * s->temp[c];
+      }
+  }
+  return s;
+}
+
+extern "C" void orc_destroy(orc_state* s) { delete s; }
+
+extern "C" int64_t orc_step(const orc_state* s) { return s->step; }
+
+extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
+  for (int64_t t = 0; t < nsteps; ++t) {
+    switch (s->p.model) {
+      case MK_MODEL_FLOW:
+        flow_step(s);
+        break;
+      case MK_MODEL_MULTIPHASE:
+        mp_step(s);
+        break;
+      case MK_MODEL_THERMAL_DENDRITE:
+        thermal_dendrite_step(s);
+        break;
+      default:
+        return;
+    }
+    s->step++;
+  }
+}
+
+extern "C" int orc_get_populations(const orc_state* s, int which, double* out) {
+  const std::vector<double>& v = which == 0 ? s->f_out : s->s_out;
+  if (v.empty()) return 1;
+  std::memcpy(out, v.data(), v.size() * sizeof(double));
+  return 0;
+}
+
+extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  if (field == MK_FIELD_FLAG) {
+    for (int64_t c = 0; c < n; ++c) out[c] = s->flag[c];
+    return 0;
+  }
+  if (field == MK_FIELD_GRAIN) {
+    for (int64_t c = 0; c < n; ++c) out[c] = s->grain[c];
+    return 0;
+  }
+  if (field == MK_FIELD_PHI) {
+    std::memcpy(out, s->phi.data(), n * sizeof(double));
+    return 0;
+  }
+  if (p.model == MK_MODEL_FLOW) {
+    if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ) return 1;
+    double F[3];
+    flow_force(s, F);
+    const int Q = s->Qf;
+    for (int64_t c = 0; c < n; ++c) {
+      if (s->flag[c] != MK_FLAG_FLUID) {
+        out[c] = field == MK_FIELD_RHO ? p.rho0 : 0.0;
+        continue;
+      }
+      double rho = 0, j[3] = {0, 0, 0};
+      for (int i = 0; i < Q; ++i) {
+        const double f = s->f_out[(int64_t)i * n + c];
+        rho += f;
+        j[0] += E27[i][0] * f;
+        j[1] += E27[i][1] * f;
+        j[2] += E27[i][2] * f;
+      }
+      if (field == MK_FIELD_RHO)
+        out[c] = rho;
+      else {
+        const int a = field - MK_FIELD_UX;
+        out[c] = (j[a] - 0.5 * F[a]) / rho;
+      }
+    }
+    return 0;
+  }
+  if (p.model == MK_MODEL_MULTIPHASE) {
+    if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ &&
+        field != MK_FIELD_PRESSURE)
+      return 1;
+    const MpConst k = mp_const(p);
+    for (int z = 0; z < s->nz; ++z)
+      for (int y = 0; y < s->ny; ++y)
+        for (int x = 0; x < s->nx; ++x) {
+          const int64_t c = cidx(s, x, y, z);
+          if (field == MK_FIELD_RHO) {
+            out[c] = p.rho_g + s->phi[c] * (p.rho_l - p.rho_g);
+            continue;
+          }
+          if (s->flag[c] != MK_FLAG_FLUID) {
+            out[c] = 0.0;
+            continue;
+          }
+          double pstar = 0, j[3] = {0, 0, 0};
+          for (int i = 0; i < 19; ++i) {
+            const double g = s->f_out[(int64_t)i * n + c];
+            pstar += g;
+            j[0] += E27[i][0] * g;
+            j[1] += E27[i][1] * g;
+            j[2] += E27[i][2] * g;
+          }
+          if (field == MK_FIELD_PRESSURE) {
+            out[c] = pstar;
+            continue;
+          }
+          const MpLocal L = mp_local(s, k, x, y, z, pstar);
+          const int a = field - MK_FIELD_UX;
+          out[c] = j[a] - L.F[a] / (2.0 * L.rho);
+        }
+    return 0;
+  }
+  // dendrites
+  if (field == MK_FIELD_T || field == MK_FIELD_C) {
+    if ((field == MK_FIELD_T) != (p.model == MK_MODEL_THERMAL_DENDRITE)) return 1;
+    std::memcpy(out, s->temp.data(), n * sizeof(double));
+    return 0;
+  }
+  if (field == MK_FIELD_DPHI) {
+    for (int64_t c = 0; c < n; ++c) out[c] = s->phi[c] - s->phi_prev[c];
+    return 0;
+  }
+  return 1;
+}

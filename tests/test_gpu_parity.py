@@ -1,0 +1,173 @@
+"""GPU (sm_100a library, through the C ABI) vs the FP64 CPU oracle.
+
+FP64 storage must match the oracle to 1e-10 relative L2 per field (the
+tolerance of the FP64 mode); FP32 to 1e-5; the 16-bit shifted storage states
+its own bounds.  Steps 1, 2 and 3 are checked separately because the in-place
+AA streaming alternates its addressing between even and odd loops.
+"""
+import numpy as np
+import pytest
+
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params, initial_field
+from _oracle import Oracle, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+
+
+def _pair(casedir, name, text, **opt):
+    p = case_params(cases.write(text, f"{casedir}/{name}.xml"), **opt)
+    s = Solver(params=p)
+    o = Oracle(p, phi=initial_field(p, "phi"), T=initial_field(p, "T"), Cc=initial_field(p, "C"))
+    return p, s, o
+
+
+def _fluid(p):
+    return initial_field(p, "flag") == 0
+
+
+def _compare(s, o, fields, tol, mask=None):
+    errs = {}
+    for f in fields:
+        errs[f] = rel_l2(s.field(f), o.field(f), mask)
+    bad = {k: v for k, v in errs.items() if not v <= tol}
+    assert not bad, f"step {s.step}: {errs}"
+    return errs
+
+
+FLOW_FIELDS = ["rho", "ux", "uy", "uz"]
+
+
+@pytest.mark.parametrize("coll,lat", [("TRT", "D3Q19"), ("BGK", "D3Q19"), ("MRT", "D3Q19"), ("TRT", "D3Q27"),
+                                      ("BGK", "D3Q27")])
+def test_flow_fp64_steps_123(casedir, coll, lat):
+    p, s, o = _pair(casedir, f"flow_{coll}_{lat}",
+                    cases.poiseuille(nx=9, ny=7, nz=5, loops=10, collision=coll, lattice=lat, force=1e-4))
+    m = _fluid(p)
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, FLOW_FIELDS, FP64_TOL, m)
+    s.advance(40)
+    o.advance(40)
+    _compare(s, o, FLOW_FIELDS, FP64_TOL, m)
+
+
+def test_flow_config1_full_fp64(casedir):
+    # Config 1 at its full size and step count: 64x32x32, D3Q19 TRT, 2000 loops.
+    p, s, o = _pair(casedir, "config1", cases.poiseuille())
+    s.advance(2000)
+    o.advance(2000)
+    errs = _compare(s, o, FLOW_FIELDS, FP64_TOL, _fluid(p))
+    assert s.step == 2000
+
+
+def test_flow_fp32(casedir):
+    p, s, o = _pair(casedir, "flow32", cases.poiseuille(nx=16, ny=12, nz=8, loops=10, precision="fp32",
+                                                        force=1e-5))
+    s.advance(200)
+    o.advance(200)
+    _compare(s, o, ["rho"], 1e-6, _fluid(p))
+    _compare(s, o, ["ux"], 1e-4, _fluid(p))
+
+
+def _mp_case(precision="fp64", n=32, bubbles=2, **kw):
+    return cases.multiphase_bubbles(n=n, nz=n, bubbles=bubbles, rmin=4, rmax=6, width=3.0, gz=-1e-5,
+                                    precision=precision, loops=10, **kw)
+
+
+MP_FIELDS = ["phi", "rho", "pressure", "ux", "uy", "uz"]
+
+
+def test_multiphase_fp64_steps(casedir):
+    p, s, o = _pair(casedir, "mp64", _mp_case())
+    m = _fluid(p)
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, MP_FIELDS, FP64_TOL, m)
+    s.advance(97)
+    o.advance(97)
+    _compare(s, o, MP_FIELDS, FP64_TOL, m)
+
+
+def test_multiphase_fp64_wetting(casedir):
+    p, s, o = _pair(casedir, "mp64w", _mp_case(contact_angle=60.0))
+    s.advance(50)
+    o.advance(50)
+    _compare(s, o, MP_FIELDS, FP64_TOL, _fluid(p))
+
+
+def test_multiphase_fp32(casedir):
+    p, s, o = _pair(casedir, "mp32", _mp_case("fp32"))
+    s.advance(100)
+    o.advance(100)
+    _compare(s, o, ["phi", "rho"], 1e-5, _fluid(p))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp16", 5e-3), ("bf16", 3e-2)])
+def test_multiphase_shifted_16bit(casedir, prec, tol):
+    p, s, o = _pair(casedir, f"mp_{prec}", _mp_case(prec))
+    s.advance(100)
+    o.advance(100)
+    _compare(s, o, ["phi"], tol, _fluid(p))
+
+
+def _dend_case(precision="fp64", n=24, **kw):
+    return cases.thermal_dendrite(n=n, loops=10, precision=precision, radius=4.0, **kw)
+
+
+DEND_FIELDS = ["phi", "T", "dphi"]
+
+
+def test_dendrite_fp64_steps(casedir):
+    p, s, o = _pair(casedir, "dend64", _dend_case())
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, DEND_FIELDS, FP64_TOL)
+    s.advance(150)
+    o.advance(150)
+    _compare(s, o, DEND_FIELDS, FP64_TOL)
+
+
+def test_dendrite_fp32(casedir):
+    p, s, o = _pair(casedir, "dend32", _dend_case("fp32"))
+    s.advance(150)
+    o.advance(150)
+    _compare(s, o, ["phi", "T"], 1e-5)
+
+
+def test_graph_matches_eager(casedir):
+    p = case_params(cases.write(_mp_case("fp32"), f"{casedir}/g.xml"))
+    a, b = Solver(params=p), Solver(params=p)
+    a.advance(11)
+    b.advance(11, graph=True)
+    for f in ["phi", "ux", "pressure"]:
+        assert np.array_equal(a.field(f), b.field(f))
+
+
+def test_checkpoint_roundtrip(casedir, tmp_path):
+    p = case_params(cases.write(_dend_case("fp32"), f"{casedir}/ck.xml"))
+    a = Solver(params=p)
+    a.advance(7)
+    a.checkpoint(str(tmp_path / "ck.bin"))
+    a.advance(9)
+    b = Solver(params=p)
+    b.restore(str(tmp_path / "ck.bin"))
+    assert b.step == 7
+    b.advance(9)
+    for f in ["phi", "T", "dphi"]:
+        assert np.array_equal(a.field(f), b.field(f))
+
+
+def test_diagnostics_conservation_fp64(casedir):
+    p = case_params(cases.write(_mp_case(), f"{casedir}/diag.xml"))
+    s = Solver(params=p)
+    d0 = s.diagnostics()
+    s.advance(100)
+    d1 = s.diagnostics()
+    assert abs(d1["phi_sum"] - d0["phi_sum"]) / d0["phi_sum"] < 1e-12
+    assert d1["n_bad"] == 0
+    assert 0.0 < d1["solid_frac"] < 0.5

@@ -1,0 +1,148 @@
+"""Known-answer pins of the FP64 CPU oracle.
+
+The reference solver (a closed Windows DLL) cannot run here, so the oracle is
+pinned by analytic solutions and exact invariants of the method instead.
+"""
+import numpy as np
+import pytest
+
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import cases, case_params, initial_field
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
+from _oracle import Oracle
+
+
+def _params(casedir, name, text, **opt):
+    return case_params(cases.write(text, f"{casedir}/{name}.xml"), **opt)
+
+
+def test_poiseuille_trt_magic_exact(casedir):
+    # TRT with Lambda = 3/16 and half-way bounce-back reproduces the parabola
+    # to round-off (walls at y = 1/2 and y = ny - 3/2).
+    p = _params(casedir, "pois_kat", cases.poiseuille(nx=3, ny=12, nz=3, loops=1, tau=0.8, magic=3 / 16,
+                                                       force=1e-6))
+    o = Oracle(p)
+    o.advance(30000)
+    ux = o.field("ux")[1, :, 1]
+    nu = (p.tau - 0.5) / 3.0
+    H = p.ny - 2
+    y = np.arange(p.ny, dtype=np.float64)
+    exact = p.force[0] / (2 * nu) * (y - 0.5) * (H + 0.5 - y)
+    fl = slice(1, p.ny - 1)
+    err = np.max(np.abs(ux[fl] - exact[fl])) / np.max(exact[fl])
+    assert err < 1e-10, err
+
+
+@pytest.mark.parametrize("coll", ["BGK", "MRT"])
+def test_poiseuille_other_collisions_converge(casedir, coll):
+    # BGK/MRT carry the known tau-dependent wall slip; the profile is still
+    # parabolic to O(1e-2) at tau = 0.8.
+    p = _params(casedir, f"pois_{coll}", cases.poiseuille(nx=3, ny=12, nz=3, loops=1, collision=coll, force=1e-6))
+    o = Oracle(p)
+    o.advance(20000)
+    ux = o.field("ux")[1, :, 1]
+    nu = (p.tau - 0.5) / 3.0
+    H = p.ny - 2
+    y = np.arange(p.ny, dtype=np.float64)
+    exact = p.force[0] / (2 * nu) * (y - 0.5) * (H + 0.5 - y)
+    fl = slice(1, p.ny - 1)
+    assert np.max(np.abs(ux[fl] - exact[fl])) / np.max(exact[fl]) < 2e-2
+
+
+def test_flow_mass_conservation(casedir):
+    p = _params(casedir, "pois_mass", cases.poiseuille(nx=8, ny=10, nz=6, loops=1, force=1e-5, lattice="D3Q27"))
+    o = Oracle(p)
+    fl = initial_field(p, "flag") == 0
+    m0 = o.field("rho")[fl].sum()
+    o.advance(300)
+    m1 = o.field("rho")[fl].sum()
+    assert abs(m1 - m0) / m0 < 1e-13
+
+
+def _mp(casedir, name, **kw):
+    return _params(casedir, name, cases.multiphase_bubbles(**kw))
+
+
+def test_multiphase_phi_conservation(casedir):
+    p = _mp(casedir, "mp_cons", n=32, nz=32, bubbles=2, rmin=4, rmax=5, width=3.0, gz=-1e-5, loops=1)
+    phi0 = initial_field(p, "phi")
+    o = Oracle(p, phi=phi0)
+    fl = initial_field(p, "flag") == 0
+    s0 = o.field("phi")[fl].sum()
+    o.advance(200)
+    s1 = o.field("phi")[fl].sum()
+    assert abs(s1 - s0) / s0 < 1e-12
+    assert np.all(np.isfinite(o.field("ux")))
+
+
+def test_multiphase_flat_interface_stays_tanh(casedir):
+    # Gas slab (phi = 0) between two flat interfaces, periodic everywhere:
+    # the equilibrium profile 1/2 (1 + tanh(2 d / W)) is (almost) steady.
+    p = _mp(casedir, "mp_flat", n=4, nz=48, bubbles=0, width=4.0, gz=0.0, loops=1)
+    p.bc[2] = A.MK_BC_PERIODIC
+    z = np.arange(p.nz, dtype=np.float64)
+    W = p.width
+    prof = 0.5 * (1 + np.tanh(2 * (np.abs(z - 23.5) - 10.0) / W))
+    phi0 = np.broadcast_to(prof[:, None, None], (p.nz, p.ny, p.nx)).copy()
+    o = Oracle(p, phi=phi0)
+    o.advance(400)
+    phi = o.field("phi")[:, 1, 1]
+    # the discrete equilibrium sits within 1e-2 of the continuous tanh ...
+    assert np.max(np.abs(phi - prof)) < 1e-2
+    # ... and is steady
+    o.advance(400)
+    assert np.max(np.abs(o.field("phi")[:, 1, 1] - phi)) < 5e-4
+    assert np.max(np.abs(o.field("uz"))) < 1e-5
+
+
+def test_thermal_diffusion_variance_rate(casedir):
+    # No seed: phi = -1 everywhere, so T obeys pure D3Q7 diffusion; the
+    # variance of a Gaussian grows by 2 D per step along each axis.
+    n = 40
+    p = _params(casedir, "diff", cases.thermal_dendrite(n=n, loops=1, D=0.1, delta=0.0))
+    p.n_objects = 0
+    c = (n - 1) / 2
+    zz, yy, xx = np.meshgrid(*(np.arange(n, dtype=np.float64),) * 3, indexing="ij")
+    r2 = (xx - c) ** 2 + (yy - c) ** 2 + (zz - c) ** 2
+    T0 = 1e-3 * np.exp(-r2 / (2 * 2.0 ** 2))
+    phi0 = -np.ones_like(T0)
+    o = Oracle(p, phi=phi0, T=T0)
+
+    def var_x(T):
+        return float(((xx - c) ** 2 * T).sum() / T.sum())
+
+    o.advance(20)
+    v1 = var_x(o.field("T"))
+    o.advance(40)
+    v2 = var_x(o.field("T"))
+    rate = (v2 - v1) / 40
+    assert abs(rate - 2 * p.D) / (2 * p.D) < 2e-3, rate
+
+
+def test_thermal_dendrite_cubic_symmetry(casedir):
+    n = 25
+    p = _params(casedir, "sym", cases.thermal_dendrite(n=n, loops=1, radius=4.0))
+    o = Oracle(p, phi=initial_field(p, "phi"))
+    o.advance(120)
+    phi = o.field("phi")
+    assert np.max(np.abs(phi - phi.transpose(0, 2, 1))) < 1e-12
+    assert np.max(np.abs(phi - phi.transpose(2, 1, 0))) < 1e-12
+    assert np.max(np.abs(phi - phi[::-1, :, :])) < 1e-12
+    # the seed has grown (undercooled melt)
+    assert (phi > 0).sum() > (initial_field(p, "phi") > 0).sum()
+
+
+def test_thermal_dendrite_enthalpy_conserved(casedir):
+    # sum(T - phi_prev/2) is invariant in a closed box.
+    n = 20
+    p = _params(casedir, "enth", cases.thermal_dendrite(n=n, loops=1, radius=4.0))
+    o = Oracle(p, phi=initial_field(p, "phi"))
+
+    def H():
+        phi = o.field("phi")
+        dphi = o.field("dphi")
+        return float((o.field("T") - 0.5 * (phi - dphi)).sum())
+
+    o.advance(2)
+    h0 = H()
+    o.advance(150)
+    assert abs(H() - h0) / abs(h0) < 1e-12
