@@ -178,6 +178,7 @@ def run_ours(args):
     for prec in prec_list:
         params = case_params(_case_path(prec, n))
         s = Solver(params=params)
+        tune = s.autotune(4)
         s.advance(W, graph=True)
         s.sync()
         barrier()
@@ -205,7 +206,7 @@ def run_ours(args):
             "step_frac": step_gbs / peak, "collide_ms": prof["kernel_ms"] / launches,
             "phi_ms": prof_phi["kernel_ms"] / launches, "collide_gbs": achieved, "collide_frac": achieved / peak,
             "collide_bytes_per_launch": collide_bytes, "clocks": clk.summary(), "n_bad": d["n_bad"],
-            "launches_per_step": s.launches_per_step(),
+            "launches_per_step": s.launches_per_step(), "tune": tune,
         }
         if prec == args.precision:
             main = (params, s)
@@ -282,6 +283,8 @@ def run_ours(args):
         "variants": {k: {"mlups": round(v["mlups"], 1), "ms_per_step": round(v["ms_per_step"], 4),
                          "collide_frac": round(v["collide_frac"], 4), "step_frac": round(v["step_frac"], 4),
                          "bytes_per_cell": v["bytes_per_cell"], "n_bad": v["n_bad"],
+                         "collide_ms": round(v["collide_ms"], 4), "phi_ms": round(v["phi_ms"], 4),
+                         "tuned": {"block": list(v["tune"]["block"]), "minb": v["tune"]["minb"]},
                          "speedup_vs_fp32": round(v["mlups"] / results["fp32"]["mlups"], 3)
                          if "fp32" in results else None}
                      for k, v in results.items()},

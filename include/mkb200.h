@@ -266,6 +266,13 @@ mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel,
  * device time in milliseconds (synchronises at the end). */
 mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, double* ms);
 
+/* Launch-shape autotuner: times `trial_steps` loops of each candidate block
+ * shape and occupancy variant of the step's kernels on a saved copy of the
+ * state (restored afterwards, so the simulation is unchanged) and keeps the
+ * fastest.  Outputs may be NULL. */
+mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32_t* block_y, int32_t* minb,
+                      double* ms_per_step);
+
 /* Page-locked host buffers for end-to-end transfers (cudaHostAlloc). */
 mk_status mk_host_alloc(size_t bytes, void** out);
 mk_status mk_host_free(void* p);

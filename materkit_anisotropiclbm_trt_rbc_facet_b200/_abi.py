@@ -118,6 +118,7 @@ PROTOTYPES = {
     "mk_restore": (C.c_int, [H, C.c_char_p]),
     "mk_profile_steps": (C.c_int, [H, C.c_int64, C.c_char_p, P(C.c_double), P(C.c_double), P(C.c_int64)]),
     "mk_time_advance": (C.c_int, [H, C.c_int64, C.c_int32, P(C.c_double)]),
+    "mk_autotune": (C.c_int, [H, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_double)]),
     "mk_host_alloc": (C.c_int, [C.c_size_t, P(C.c_void_p)]),
     "mk_host_free": (C.c_int, [C.c_void_p]),
     "mk_bytes_per_cell": (C.c_double, [H]),

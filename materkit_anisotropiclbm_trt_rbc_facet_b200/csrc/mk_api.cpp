@@ -133,12 +133,14 @@ mk_status mk_create(const mk_params* p, mk_handle** out) {
   }
   // initial state (initialize + initialize_geometry)
   const size_t n = (size_t)h->e.ncell;
-  std::vector<double> phi(n), temp(n), rho(n);
-  mkc::initial_field(p, MK_FIELD_PHI, phi.data(), n, err);
-  mkc::initial_field(p, MK_FIELD_T, temp.data(), n, err);
-  mkc::initial_field(p, MK_FIELD_RHO, rho.data(), n, err);
-  st = mke::engine_set_state(h->e, phi.data(), temp.data(), p->model == MK_MODEL_FLOW ? rho.data() : nullptr,
-                             nullptr, nullptr, nullptr);
+  const bool flow = p->model == MK_MODEL_FLOW;
+  const bool dend = p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE;
+  std::vector<double> phi(flow ? 0 : n), temp(dend ? n : 0), rho(flow ? n : 0);
+  if (!flow) mkc::initial_field(p, MK_FIELD_PHI, phi.data(), n, err);
+  if (dend) mkc::initial_field(p, MK_FIELD_T, temp.data(), n, err);
+  if (flow) mkc::initial_field(p, MK_FIELD_RHO, rho.data(), n, err);
+  st = mke::engine_set_state(h->e, flow ? nullptr : phi.data(), dend ? temp.data() : nullptr,
+                             flow ? rho.data() : nullptr, nullptr, nullptr, nullptr);
   if (st != cudaSuccess) {
     mk_status r = cuda_fail(h, st, "initialise");
     mke::engine_free(h->e);
@@ -561,6 +563,25 @@ mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, doubl
   if (s != MK_OK) return s;
   if (st != cudaSuccess) return cuda_fail(h, st, "time_advance");
   *ms = f;
+  return MK_OK;
+}
+
+mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32_t* block_y, int32_t* minb,
+                      double* ms_per_step) {
+  if (!h || trial_steps < 1) return MK_ERR_ARG;
+  mke::TuneResult r;
+  cudaError_t st = mke::engine_autotune(h->e, trial_steps, &r);
+  if (st != cudaSuccess) return cuda_fail(h, st, "autotune");
+  // captured graphs hold the old launch shape
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  if (block_x) *block_x = r.block_x;
+  if (block_y) *block_y = r.block_y;
+  if (minb) *minb = r.minb;
+  if (ms_per_step) *ms_per_step = r.ms_per_step;
   return MK_OK;
 }
 

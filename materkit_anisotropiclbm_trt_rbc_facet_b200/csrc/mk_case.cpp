@@ -201,9 +201,10 @@ mk_status validate_params(const mk_params* p, std::string& err) {
     err = "MeshXYZ must be positive";
     return MK_ERR_ARG;
   }
+  // cell indices inside a population plane are 32-bit on the device
   const double cells = (double)p->nx * p->ny * p->nz;
-  if (cells > 4.0e9) {
-    err = "domain too large";
+  if (cells >= 2147483647.0 - 64.0) {
+    err = "domain too large (at most 2^31 - 65 cells)";
     return MK_ERR_ARG;
   }
   for (int a = 0; a < 3; ++a) {
@@ -529,6 +530,26 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
   return MK_OK;
 }
 
+// Gas bubbles (phi = 0) in liquid (phi = 1): phi = min_k 1/2 (1 + tanh(2 (d_k - R_k)/W)),
+// d_k with the minimum image on periodic axes.  Beyond d - R = 10 W the
+// double-precision tanh is exactly 1, so those bubbles are skipped.
+static double bubble_phi(const mk_params* p, const double pos[3], const int n3[3]) {
+  double ph = 1.0;
+  for (int k = 0; k < p->n_objects; ++k) {
+    double d2 = 0;
+    for (int a = 0; a < 3; ++a) {
+      double d = std::fabs(pos[a] - p->obj_center[k][a]);
+      if (p->bc[a] == MK_BC_PERIODIC && d > 0.5 * n3[a]) d = n3[a] - d;
+      d2 += d * d;
+    }
+    const double far = p->obj_radius[k] + 10.0 * p->width;
+    if (d2 > far * far) continue;
+    const double ph_k = 0.5 * (1.0 + std::tanh(2.0 * (std::sqrt(d2) - p->obj_radius[k]) / p->width));
+    if (ph_k < ph) ph = ph_k;
+  }
+  return ph;
+}
+
 mk_status initial_field(const mk_params* p, int field, double* out, size_t ncells, std::string& err) {
   const size_t n = (size_t)p->nx * p->ny * p->nz;
   if (ncells < n) {
@@ -547,24 +568,9 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
             v = is_fluid(p, x, y, z) ? MK_FLAG_FLUID : MK_FLAG_WALLS;
             break;
           case MK_FIELD_RHO:
-            if (p->model == MK_MODEL_FLOW)
-              v = p->rho0;
-            else {
-              double ph = 1.0;
-              std::string e2;
-              // density of the multiphase initial state follows phi
-              for (int k = 0; k < p->n_objects; ++k) {
-                double d2 = 0;
-                for (int a = 0; a < 3; ++a) {
-                  double d = std::fabs(pos[a] - p->obj_center[k][a]);
-                  if (p->bc[a] == MK_BC_PERIODIC && d > 0.5 * n3[a]) d = n3[a] - d;
-                  d2 += d * d;
-                }
-                const double ph_k = 0.5 * (1.0 + std::tanh(2.0 * (std::sqrt(d2) - p->obj_radius[k]) / p->width));
-                if (ph_k < ph) ph = ph_k;
-              }
-              v = p->model == MK_MODEL_MULTIPHASE ? p->rho_g + ph * (p->rho_l - p->rho_g) : p->rho0;
-            }
+            // the multiphase density follows phi
+            v = p->model == MK_MODEL_MULTIPHASE ? p->rho_g + bubble_phi(p, pos, n3) * (p->rho_l - p->rho_g)
+                                                : p->rho0;
             break;
           case MK_FIELD_UX:
           case MK_FIELD_UY:
@@ -598,19 +604,7 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
           }
           case MK_FIELD_PHI:
             if (p->model == MK_MODEL_MULTIPHASE) {
-              // gas bubbles (phi = 0) in liquid (phi = 1): 1/2 (1 + tanh(2 (d - R)/W))
-              double ph = 1.0;
-              for (int k = 0; k < p->n_objects; ++k) {
-                double d2 = 0;
-                for (int a = 0; a < 3; ++a) {
-                  double d = std::fabs(pos[a] - p->obj_center[k][a]);
-                  if (p->bc[a] == MK_BC_PERIODIC && d > 0.5 * n3[a]) d = n3[a] - d;
-                  d2 += d * d;
-                }
-                const double ph_k = 0.5 * (1.0 + std::tanh(2.0 * (std::sqrt(d2) - p->obj_radius[k]) / p->width));
-                if (ph_k < ph) ph = ph_k;
-              }
-              v = ph;
+              v = bubble_phi(p, pos, n3);
             } else if (p->model == MK_MODEL_FLOW) {
               v = 0.0;
             } else {

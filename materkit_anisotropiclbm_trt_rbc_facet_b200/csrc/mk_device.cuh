@@ -19,6 +19,8 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace mkd {
 
 // ------------------------------------------------------------- lattices
@@ -82,10 +84,141 @@ __host__ __device__ constexpr double mrt_rate(int k) {
 }
 __host__ __device__ constexpr bool mrt_is_shear(int k) { return k == 9 || k == 11 || k == 13 || k == 14 || k == 15; }
 
+// ---- moment-space MRT with analytic equilibria -------------------------
+// For an equilibrium  f_eq,i = w_i [a0 + 3 e_i.b + 4.5 (e_i e_i):Q]  and a
+// Guo force term  F_i = s_F w_i [3 e_i.F + 9 (e_i.u)(e_i.F) - 3 u.F]  the
+// moments M f_eq and M F are linear in (a0, b, Q) and (F, u F) with the
+// integer tables below (weights scaled by 36).  Everything is evaluated at
+// compile time, so one collision costs the pair-split transform M f, 19
+// relaxations and the pair-split back-transform.
+__host__ __device__ constexpr int w36(int i) { return i == 0 ? 12 : (i <= 6 ? 2 : 1); }
+__host__ __device__ constexpr int mrt_a36(int k) {
+  int s = 0;
+  for (int i = 0; i < 19; ++i) s += mrt_m(k, i) * w36(i);
+  return s;
+}
+__host__ __device__ constexpr int mrt_b36(int k, int a) {
+  int s = 0;
+  for (int i = 0; i < 19; ++i) s += mrt_m(k, i) * w36(i) * (a == 0 ? ex(i) : (a == 1 ? ey(i) : ez(i)));
+  return s;
+}
+__host__ __device__ constexpr int mrt_c36(int k, int a, int b) {
+  int s = 0;
+  for (int i = 0; i < 19; ++i)
+    s += mrt_m(k, i) * w36(i) * (a == 0 ? ex(i) : (a == 1 ? ey(i) : ez(i))) *
+         (b == 0 ? ex(i) : (b == 1 ? ey(i) : ez(i)));
+  return s;
+}
+__host__ __device__ constexpr bool mrt_even(int k) { return k <= 2 || (k >= 9 && k <= 15); }
+
+template <int K>
+struct MrtRow {
+  static constexpr int a = mrt_a36(K);
+  static constexpr int bx = mrt_b36(K, 0), by = mrt_b36(K, 1), bz = mrt_b36(K, 2);
+  static constexpr int cxx = mrt_c36(K, 0, 0), cyy = mrt_c36(K, 1, 1), czz = mrt_c36(K, 2, 2);
+  static constexpr int cxy = mrt_c36(K, 0, 1), cxz = mrt_c36(K, 0, 2), cyz = mrt_c36(K, 1, 2);
+  static constexpr int norm = mrt_norm(K);
+};
+
+template <class T>
+struct MrtIn {
+  T a0, bx, by, bz;                 // equilibrium: a0 and the vector b
+  T qxx, qyy, qzz, qxy, qxz, qyz;   // equilibrium: symmetric tensor Q (full off-diagonal value)
+  T Fx, Fy, Fz, ux, uy, uz, sF;     // force, velocity of the force term, scale
+  T s_nu;                           // shear rate
+};
+
+// d_K = (s_K (m_K - meq_K) - (1 - s_K/2) mF_K) / |M_K|^2
+template <class T, int K>
+__host__ __device__ __forceinline__ T mrt_relax(T mk, const MrtIn<T>& q) {
+  typedef MrtRow<K> R;
+  constexpr double c = 1.0 / 36.0;
+  T meq = T(0), mf = T(0);
+  if constexpr (R::a != 0) meq += T(R::a * c) * q.a0;
+  if constexpr (R::bx != 0) meq += T(3.0 * R::bx * c) * q.bx;
+  if constexpr (R::by != 0) meq += T(3.0 * R::by * c) * q.by;
+  if constexpr (R::bz != 0) meq += T(3.0 * R::bz * c) * q.bz;
+  if constexpr (R::cxx != 0) meq += T(4.5 * R::cxx * c) * q.qxx;
+  if constexpr (R::cyy != 0) meq += T(4.5 * R::cyy * c) * q.qyy;
+  if constexpr (R::czz != 0) meq += T(4.5 * R::czz * c) * q.qzz;
+  if constexpr (R::cxy != 0) meq += T(9.0 * R::cxy * c) * q.qxy;
+  if constexpr (R::cxz != 0) meq += T(9.0 * R::cxz * c) * q.qxz;
+  if constexpr (R::cyz != 0) meq += T(9.0 * R::cyz * c) * q.qyz;
+  // force moments: 3 B.F + 9 u.C.F - 3 A u.F
+  if constexpr (R::bx != 0) mf += T(3.0 * R::bx * c) * q.Fx;
+  if constexpr (R::by != 0) mf += T(3.0 * R::by * c) * q.Fy;
+  if constexpr (R::bz != 0) mf += T(3.0 * R::bz * c) * q.Fz;
+  if constexpr (R::cxx != 0) mf += T(9.0 * R::cxx * c) * (q.ux * q.Fx);
+  if constexpr (R::cyy != 0) mf += T(9.0 * R::cyy * c) * (q.uy * q.Fy);
+  if constexpr (R::czz != 0) mf += T(9.0 * R::czz * c) * (q.uz * q.Fz);
+  if constexpr (R::cxy != 0) mf += T(9.0 * R::cxy * c) * (q.ux * q.Fy + q.uy * q.Fx);
+  if constexpr (R::cxz != 0) mf += T(9.0 * R::cxz * c) * (q.ux * q.Fz + q.uz * q.Fx);
+  if constexpr (R::cyz != 0) mf += T(9.0 * R::cyz * c) * (q.uy * q.Fz + q.uz * q.Fy);
+  if constexpr (R::a != 0) mf -= T(3.0 * R::a * c) * (q.ux * q.Fx + q.uy * q.Fy + q.uz * q.Fz);
+  const T s = mrt_is_shear(K) ? q.s_nu : T(mrt_rate(K));
+  return (s * (mk - meq) - (T(1) - T(0.5) * s) * (q.sF * mf)) * T(1.0 / R::norm);
+}
+
+template <class T, int... Ks>
+__host__ __device__ __forceinline__ void mrt_relax_all(const T (&m)[19], T (&d)[19], const MrtIn<T>& q,
+                                              std::integer_sequence<int, Ks...>) {
+  ((d[Ks] = mrt_relax<T, Ks>(m[Ks], q)), ...);
+}
+
+// In-place D3Q19 MRT collision in moment space (pair-split transforms).
+template <class T>
+__host__ __device__ __forceinline__ void mrt19_collide_moments(T (&f)[19], const MrtIn<T>& q) {
+  T s[10], a[10];
+  s[0] = f[0];
+  a[0] = T(0);
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    s[p] = f[2 * p - 1] + f[2 * p];
+    a[p] = f[2 * p - 1] - f[2 * p];
+  }
+  T m[19];
+#pragma unroll
+  for (int k = 0; k < 19; ++k) {
+    T acc = T(0);
+    if (mrt_even(k)) {
+      if (mrt_m(k, 0) != 0) acc += T(mrt_m(k, 0)) * s[0];
+#pragma unroll
+      for (int p = 1; p <= 9; ++p)
+        if (mrt_m(k, 2 * p - 1) != 0) acc += T(mrt_m(k, 2 * p - 1)) * s[p];
+    } else {
+#pragma unroll
+      for (int p = 1; p <= 9; ++p)
+        if (mrt_m(k, 2 * p - 1) != 0) acc += T(mrt_m(k, 2 * p - 1)) * a[p];
+    }
+    m[k] = acc;
+  }
+  T d[19];
+  mrt_relax_all<T>(m, d, q, std::make_integer_sequence<int, 19>{});
+  T d0 = T(0);
+#pragma unroll
+  for (int k = 0; k < 19; ++k)
+    if (mrt_even(k) && mrt_m(k, 0) != 0) d0 += T(mrt_m(k, 0)) * d[k];
+  f[0] -= d0;
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    T E = T(0), O = T(0);
+#pragma unroll
+    for (int k = 0; k < 19; ++k) {
+      if (mrt_m(k, 2 * p - 1) == 0) continue;
+      if (mrt_even(k))
+        E += T(mrt_m(k, 2 * p - 1)) * d[k];
+      else
+        O += T(mrt_m(k, 2 * p - 1)) * d[k];
+    }
+    f[2 * p - 1] -= E + O;
+    f[2 * p] -= E - O;
+  }
+}
+
 // f -= Mi [ S M (f - feq) - (I - S/2) M F ]   (all loops unrolled; M is
 // integer so the compiler folds every zero).
 template <class T>
-__device__ __forceinline__ void mrt19_collide(T (&f)[19], const T (&feq)[19], const T (&F)[19], T s_nu) {
+__host__ __device__ __forceinline__ void mrt19_collide(T (&f)[19], const T (&feq)[19], const T (&F)[19], T s_nu) {
   T d[19];
 #pragma unroll
   for (int k = 0; k < 19; ++k) {
@@ -197,6 +330,81 @@ struct Geom {
     return true;
   }
 };
+
+// Neighbourhood of one cell, resolved once per thread: per axis the three
+// candidate coordinates (already multiplied by the axis stride) and whether
+// each is fluid; a 27-bit mask answers "is neighbour (dx,dy,dz) fluid".
+// Cell indices are 32-bit (domains are limited to < 2^31 cells); only the
+// population-plane offset i * stride is 64-bit.
+struct Nbr {
+  int ox[3], oy[3], oz[3];
+  unsigned ok;
+
+  __device__ __forceinline__ static void axis(int n, int bc, int c, int mul, int (&o)[3], bool (&v)[3]) {
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      int cc = c + d;
+      bool valid = true;
+      if (cc < 0 || cc >= n) {
+        if (bc == 0) {
+          cc = cc < 0 ? cc + n : cc - n;
+        } else {
+          valid = false;
+          cc = c;
+        }
+      }
+      if (bc == 1 && (cc == 0 || cc == n - 1)) valid = false;
+      o[d + 1] = cc * mul;
+      v[d + 1] = valid;
+    }
+  }
+
+  __device__ __forceinline__ Nbr(const Geom& g, int x, int y, int z) {
+    bool vx[3], vy[3], vz[3];
+    axis(g.nx, g.bc0, x, 1, ox, vx);
+    axis(g.ny, g.bc1, y, g.nx, oy, vy);
+    axis(g.nz, g.bc2, z, g.nx * g.ny, oz, vz);
+    ok = 0u;
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx)
+          if (vx[dx] && vy[dy] && vz[dz]) ok |= 1u << (dx + 3 * dy + 9 * dz);
+  }
+  __device__ __forceinline__ int idx(int dx, int dy, int dz) const { return ox[dx + 1] + oy[dy + 1] + oz[dz + 1]; }
+  __device__ __forceinline__ bool fluid(int dx, int dy, int dz) const {
+    return (ok >> ((dx + 1) + 3 * (dy + 1) + 9 * (dz + 1))) & 1u;
+  }
+};
+
+// Pre-collision population i of the cell at `c` (= nb.idx(0,0,0)).
+template <class S, int Q>
+__device__ __forceinline__ typename Stor<S>::T ld_in(const S* __restrict__ A, int64_t stride, const Nbr& nb,
+                                                      int parity, int c, int i, float ref) {
+  typedef typename Stor<S>::T T;
+  const T w = T(wq<Q>(i));
+  if (parity == 0) return Stor<S>::ld(A + (int64_t)i * stride + c, w, ref);
+  if (nb.fluid(-ex(i), -ey(i), -ez(i)))
+    return Stor<S>::ld(A + (int64_t)inv(i) * stride + nb.idx(-ex(i), -ey(i), -ez(i)), w, ref);
+  return Stor<S>::ld(A + (int64_t)i * stride + c, w, ref);
+}
+
+// Store post-collision population i of the cell at `c`.
+template <class S, int Q>
+__device__ __forceinline__ void st_out(S* __restrict__ A, int64_t stride, const Nbr& nb, int parity, int c, int i,
+                                       typename Stor<S>::T v, float ref) {
+  typedef typename Stor<S>::T T;
+  const T w = T(wq<Q>(i));
+  if (parity == 0) {
+    Stor<S>::st(A + (int64_t)inv(i) * stride + c, v, w, ref);
+  } else if (nb.fluid(ex(i), ey(i), ez(i))) {
+    Stor<S>::st(A + (int64_t)i * stride + nb.idx(ex(i), ey(i), ez(i)), v, w, ref);
+  } else {
+    Stor<S>::st(A + (int64_t)inv(i) * stride + c, v, w, ref);
+  }
+}
 
 // Load the pre-collision population i of cell (x,y,z) at the given AA parity.
 template <class S, int Q>

