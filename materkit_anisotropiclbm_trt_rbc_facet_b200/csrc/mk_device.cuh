@@ -244,43 +244,44 @@ __host__ __device__ __forceinline__ void mrt19_collide(T (&f)[19], const T (&feq
 }
 
 // -------------------------------------------------------- storage traits
-// FP64/FP32 store populations as they are.  FP16/BF16 store the shifted,
-// weight-normalised deviation (f_i / w_i - ref), which keeps every plane in
-// the normal range of the 16-bit format; arithmetic stays FP32.
+// Every lattice is held as its deviation from the rest state,
+//   f'_i = f_i - w_i ref      (ref = rho0, phi = 1, phi = -1, u = -Delta, ...),
+// and the kernels do their arithmetic on f' (moments of f' plus the rest
+// value; equilibria minus w_i ref).  Near rest the deviation is small, so FP32
+// keeps the digits of the velocity moments that raw f_i ~ w_i would round
+// away, and the 16-bit formats hold f'_i / w_i, a plane-independent O(1)
+// quantity inside the normal range of FP16.  FP64 and FP32 store f', FP16 and
+// BF16 store f'/w; collision arithmetic is FP64 or FP32.
 template <class S>
 struct Stor;
 template <>
 struct Stor<double> {
   typedef double T;
   static constexpr int bytes = 8;
-  __device__ __forceinline__ static double ld(const double* p, double, double) { return *p; }
-  __device__ __forceinline__ static void st(double* p, double v, double, double) { *p = v; }
+  __device__ __forceinline__ static double ld(const double* p, double) { return *p; }
+  __device__ __forceinline__ static void st(double* p, double v, double) { *p = v; }
 };
 template <>
 struct Stor<float> {
   typedef float T;
   static constexpr int bytes = 4;
-  __device__ __forceinline__ static float ld(const float* p, float, float) { return *p; }
-  __device__ __forceinline__ static void st(float* p, float v, float, float) { *p = v; }
+  __device__ __forceinline__ static float ld(const float* p, float) { return *p; }
+  __device__ __forceinline__ static void st(float* p, float v, float) { *p = v; }
 };
 template <>
 struct Stor<__half> {
   typedef float T;
   static constexpr int bytes = 2;
-  __device__ __forceinline__ static float ld(const __half* p, float w, float ref) { return w * (ref + __half2float(*p)); }
-  __device__ __forceinline__ static void st(__half* p, float v, float w, float ref) {
-    *p = __float2half_rn(v * (1.0f / w) - ref);
-  }
+  __device__ __forceinline__ static float ld(const __half* p, float w) { return w * __half2float(*p); }
+  __device__ __forceinline__ static void st(__half* p, float v, float w) { *p = __float2half_rn(v * (1.0f / w)); }
 };
 template <>
 struct Stor<__nv_bfloat16> {
   typedef float T;
   static constexpr int bytes = 2;
-  __device__ __forceinline__ static float ld(const __nv_bfloat16* p, float w, float ref) {
-    return w * (ref + __bfloat162float(*p));
-  }
-  __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float w, float ref) {
-    *p = __float2bfloat16_rn(v * (1.0f / w) - ref);
+  __device__ __forceinline__ static float ld(const __nv_bfloat16* p, float w) { return w * __bfloat162float(*p); }
+  __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float w) {
+    *p = __float2bfloat16_rn(v * (1.0f / w));
   }
 };
 
@@ -379,81 +380,55 @@ struct Nbr {
   }
 };
 
-// Pre-collision population i of the cell at `c` (= nb.idx(0,0,0)).
+// Element offset of the slot population i of the cell at `c` is read from
+// (pre-collision) at the given AA parity.  The bounce-back alternative is a
+// select, not a branch, so every access is one load or store.
+template <int Q>
+__device__ __forceinline__ int64_t off_in(int64_t stride, const Nbr& nb, int parity, int c, int i) {
+  if (parity == 0) return (int64_t)i * stride + c;
+  const bool f = nb.fluid(-ex(i), -ey(i), -ez(i));
+  const int cell = f ? nb.idx(-ex(i), -ey(i), -ez(i)) : c;
+  return (int64_t)(f ? inv(i) : i) * stride + cell;
+}
+
+// Element offset of the slot the post-collision population i is written to.
+template <int Q>
+__device__ __forceinline__ int64_t off_out(int64_t stride, const Nbr& nb, int parity, int c, int i) {
+  if (parity == 0) return (int64_t)inv(i) * stride + c;
+  const bool f = nb.fluid(ex(i), ey(i), ez(i));
+  const int cell = f ? nb.idx(ex(i), ey(i), ez(i)) : c;
+  return (int64_t)(f ? i : inv(i)) * stride + cell;
+}
+
+// Pre-collision deviation f'_i of the cell at `c` (= nb.idx(0,0,0)).
 template <class S, int Q>
 __device__ __forceinline__ typename Stor<S>::T ld_in(const S* __restrict__ A, int64_t stride, const Nbr& nb,
-                                                      int parity, int c, int i, float ref) {
-  typedef typename Stor<S>::T T;
-  const T w = T(wq<Q>(i));
-  if (parity == 0) return Stor<S>::ld(A + (int64_t)i * stride + c, w, ref);
-  if (nb.fluid(-ex(i), -ey(i), -ez(i)))
-    return Stor<S>::ld(A + (int64_t)inv(i) * stride + nb.idx(-ex(i), -ey(i), -ez(i)), w, ref);
-  return Stor<S>::ld(A + (int64_t)i * stride + c, w, ref);
+                                                      int parity, int c, int i) {
+  return Stor<S>::ld(A + off_in<Q>(stride, nb, parity, c, i), typename Stor<S>::T(wq<Q>(i)));
 }
 
-// Store post-collision population i of the cell at `c`.
+// Store the post-collision deviation f'_i of the cell at `c`.
 template <class S, int Q>
 __device__ __forceinline__ void st_out(S* __restrict__ A, int64_t stride, const Nbr& nb, int parity, int c, int i,
-                                       typename Stor<S>::T v, float ref) {
-  typedef typename Stor<S>::T T;
-  const T w = T(wq<Q>(i));
-  if (parity == 0) {
-    Stor<S>::st(A + (int64_t)inv(i) * stride + c, v, w, ref);
-  } else if (nb.fluid(ex(i), ey(i), ez(i))) {
-    Stor<S>::st(A + (int64_t)i * stride + nb.idx(ex(i), ey(i), ez(i)), v, w, ref);
-  } else {
-    Stor<S>::st(A + (int64_t)inv(i) * stride + c, v, w, ref);
-  }
+                                       typename Stor<S>::T v) {
+  Stor<S>::st(A + off_out<Q>(stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
 }
 
-// Load the pre-collision population i of cell (x,y,z) at the given AA parity.
+// Post-collision deviation f'_i of a cell in the layout left after
+// `steps_done` loops (field output, diagnostics): the slot the last loop
+// wrote it to.
 template <class S, int Q>
-__device__ __forceinline__ typename Stor<S>::T load_in(const S* __restrict__ A, const Geom& g, int parity, int x,
-                                                        int y, int z, int64_t c, int i, float ref) {
-  typedef typename Stor<S>::T T;
-  const T w = T(wq<Q>(i));
-  if (parity == 0) return Stor<S>::ld(A + (int64_t)i * g.stride + c, w, ref);
-  int64_t s;
-  if (g.nbr(x, y, z, -ex(i), -ey(i), -ez(i), s)) return Stor<S>::ld(A + (int64_t)inv(i) * g.stride + s, w, ref);
-  return Stor<S>::ld(A + (int64_t)i * g.stride + c, w, ref);
+__device__ __forceinline__ typename Stor<S>::T ld_out(const S* __restrict__ A, int64_t stride, const Nbr& nb,
+                                                       int64_t steps_done, int c, int i) {
+  return Stor<S>::ld(A + off_out<Q>(stride, nb, (int)((steps_done + 1) & 1), c, i), typename Stor<S>::T(wq<Q>(i)));
 }
 
-// Store the post-collision population i of cell (x,y,z) at the given parity.
+// Inverse of ld_out: place a post-collision deviation so that the next loop
+// (parity = steps_done & 1) reads it as the streamed value.
 template <class S, int Q>
-__device__ __forceinline__ void store_out(S* __restrict__ A, const Geom& g, int parity, int x, int y, int z, int64_t c,
-                                          int i, typename Stor<S>::T v, float ref) {
-  typedef typename Stor<S>::T T;
-  const T w = T(wq<Q>(i));
-  if (parity == 0) {
-    Stor<S>::st(A + (int64_t)inv(i) * g.stride + c, v, w, ref);
-    return;
-  }
-  int64_t d;
-  if (g.nbr(x, y, z, ex(i), ey(i), ez(i), d))
-    Stor<S>::st(A + (int64_t)i * g.stride + d, v, w, ref);
-  else
-    Stor<S>::st(A + (int64_t)inv(i) * g.stride + c, v, w, ref);
-}
-
-// Post-collision population i of a cell in the layout left after `steps_done`
-// loops (used by field output and checkpoints).
-template <class S, int Q>
-__device__ __forceinline__ typename Stor<S>::T load_out(const S* __restrict__ A, const Geom& g, int64_t steps_done,
-                                                         int x, int y, int z, int64_t c, int i, float ref) {
-  typedef typename Stor<S>::T T;
-  const T w = T(wq<Q>(i));
-  if (steps_done & 1) return Stor<S>::ld(A + (int64_t)inv(i) * g.stride + c, w, ref);
-  int64_t d;
-  if (g.nbr(x, y, z, ex(i), ey(i), ez(i), d)) return Stor<S>::ld(A + (int64_t)i * g.stride + d, w, ref);
-  return Stor<S>::ld(A + (int64_t)inv(i) * g.stride + c, w, ref);
-}
-
-// Inverse of load_out: place post-collision population i so that the next
-// loop (parity = steps_done & 1) reads it as the streamed value.
-template <class S, int Q>
-__device__ __forceinline__ void store_out_layout(S* __restrict__ A, const Geom& g, int64_t steps_done, int x, int y,
-                                                 int z, int64_t c, int i, typename Stor<S>::T v, float ref) {
-  store_out<S, Q>(A, g, (int)((steps_done + 1) & 1), x, y, z, c, i, v, ref);
+__device__ __forceinline__ void st_layout(S* __restrict__ A, int64_t stride, const Nbr& nb, int64_t steps_done, int c,
+                                          int i, typename Stor<S>::T v) {
+  Stor<S>::st(A + off_out<Q>(stride, nb, (int)((steps_done + 1) & 1), c, i), v, typename Stor<S>::T(wq<Q>(i)));
 }
 
 }  // namespace mkd

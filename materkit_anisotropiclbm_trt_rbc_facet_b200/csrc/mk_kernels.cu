@@ -36,16 +36,16 @@ struct PhiOf<double> {
   typedef double type;
 };
 
-// Reference values of the shifted 16-bit storage (f_i / w_i - ref).
+// Rest values of the two lattices: populations are held as f_i - w_i ref.
 struct Refs {
-  float r0, r1;
+  double r0, r1;
 };
 
 // ================================================================ FLOW (K1)
 template <class T>
 struct FlowK {
   T om, om_m, Fx, Fy, Fz;
-  float ref;
+  T ref;  // rho0
 };
 
 template <class S, int Q, int COLL, int PARITY>
@@ -57,24 +57,25 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   const Nbr nb(g, x, y, z);
   const int c = nb.idx(0, 0, 0);
-  T f[Q];
+  T f[Q];  // deviations f_i - w_i rho0
 #pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(A, g.stride, nb, PARITY, c, i, k.ref);
-  T rho = T(0), jx = T(0), jy = T(0), jz = T(0);
+  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(A, g.stride, nb, PARITY, c, i);
+  T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    rho += f[i];
+    drho += f[i];
     if (ex(i)) jx += T(ex(i)) * f[i];
     if (ey(i)) jy += T(ey(i)) * f[i];
     if (ez(i)) jz += T(ez(i)) * f[i];
   }
+  const T rho = k.ref + drho;
   const T ux = (jx + T(0.5) * k.Fx) / rho;
   const T uy = (jy + T(0.5) * k.Fy) / rho;
   const T uz = (jz + T(0.5) * k.Fz) / rho;
   const T uu = ux * ux + uy * uy + uz * uz;
   if constexpr (COLL == MK_COLL_MRT && Q == 19) {
-    MrtIn<T> q;
-    q.a0 = rho * (T(1) - T(1.5) * uu);
+    MrtIn<T> q;  // equilibrium deviation: w [drho + rho (3eu + 4.5(eu)^2 - 1.5u^2)]
+    q.a0 = drho - T(1.5) * rho * uu;
     q.bx = rho * ux;
     q.by = rho * uy;
     q.bz = rho * uz;
@@ -94,17 +95,17 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
     q.s_nu = k.om;
     mrt19_collide_moments<T>(f, q);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i], k.ref);
+    for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i]);
     return;
   }
   const T uF = ux * k.Fx + uy * k.Fy + uz * k.Fz;
-  T feq[Q], Fi[Q];
+  T feq[Q], Fi[Q];  // equilibrium deviations and Guo force terms
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const T w = T(wq<Q>(i));
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
     const T eF = T(ex(i)) * k.Fx + T(ey(i)) * k.Fy + T(ez(i)) * k.Fz;
-    feq[i] = rho * (w * (T(1) + T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu));
+    feq[i] = w * (drho + rho * (T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu));
     Fi[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF);
   }
   if (COLL == MK_COLL_BGK) {
@@ -125,18 +126,21 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
     for (int i = 0; i < Q; ++i) f[i] = fo[i];
   }
 #pragma unroll
-  for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i], k.ref);
+  for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i]);
 }
 
 // ========================================================= MULTIPHASE (K4)
+// The pressure lattice g rests at 0 (p* = 0, u = 0), so its deviation is g
+// itself; the Allen-Cahn lattice h rests at the liquid, h_i = w_i (phi = 1).
 template <class T>
 struct MpK {
   T beta, kappa, om_h, coef_wet, inv_w4, rho_l, rho_g, tau_l, tau_g, gx, gy, gz;
-  float ref_g, ref_h;
+  T ref_h;  // 1
 };
 
 template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, P* __restrict__ phi, const Geom g, float ref_h) {
+__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, P* __restrict__ phi, const Geom g,
+                                                typename Stor<S>::T ref_h) {
   typedef typename Stor<S>::T T;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -146,8 +150,8 @@ __global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, P* __re
   const int c = nb.idx(0, 0, 0);
   T s = T(0);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) s += ld_in<S, 19>(H, g.stride, nb, PARITY, c, i, ref_h);
-  phi[c] = P(s);
+  for (int i = 0; i < 19; ++i) s += ld_in<S, 19>(H, g.stride, nb, PARITY, c, i);
+  phi[c] = P(ref_h + s);
 }
 
 // Density, phi gradient and total force of a fluid cell (shared by the
@@ -198,11 +202,11 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   const Nbr nb(g, x, y, z);
   const int c = nb.idx(0, 0, 0);
-  T gp_[19], h[19];
+  T gp_[19], h[19];  // g, and the deviations h_i - w_i
 #pragma unroll
-  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, g.stride, nb, PARITY, c, i, k.ref_g);
+  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, g.stride, nb, PARITY, c, i);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) h[i] = ld_in<S, 19>(H, g.stride, nb, PARITY, c, i, k.ref_h);
+  for (int i = 0; i < 19; ++i) h[i] = ld_in<S, 19>(H, g.stride, nb, PARITY, c, i);
   T pstar = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
   for (int i = 0; i < 19; ++i) {
@@ -222,14 +226,16 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   const T inv_gn = T(1) / (gn + T(1e-12));
   const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
   const T lam = k.inv_w4 * ph * (T(1) - ph);
-  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair
+  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair, on the
+  // deviations: heq_i - w_i = w_i [(phi - 1) + phi (3eu + 4.5(eu)^2 - 1.5u^2)]
   const T om_h = k.om_h;
   const T src = (T(1) - T(0.5) * om_h) * lam;
+  const T dph = ph - k.ref_h;
   {
     const T w = T(wq<19>(0));
     const T h0 = h[0];
-    const T heq = ph * (w * (T(1) - T(1.5) * uu));
-    st_out<S, 19>(H, g.stride, nb, PARITY, c, 0, h0 - om_h * (h0 - heq), k.ref_h);
+    const T heq = w * (dph - T(1.5) * ph * uu);
+    st_out<S, 19>(H, g.stride, nb, PARITY, c, 0, h0 - om_h * (h0 - heq));
   }
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
@@ -239,11 +245,11 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
     const T hj = h[j];
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
     const T en = T(ex(i)) * nx_ + T(ey(i)) * ny_ + T(ez(i)) * nz_;
-    const T even = ph * (w * (T(1) + T(4.5) * eu * eu - T(1.5) * uu));
+    const T even = w * (dph + ph * (T(4.5) * eu * eu - T(1.5) * uu));
     const T odd = ph * (w * (T(3) * eu));
     const T s = src * w * en;
-    st_out<S, 19>(H, g.stride, nb, PARITY, c, i, hi - om_h * (hi - (even + odd)) + s, k.ref_h);
-    st_out<S, 19>(H, g.stride, nb, PARITY, c, j, hj - om_h * (hj - (even - odd)) - s, k.ref_h);
+    st_out<S, 19>(H, g.stride, nb, PARITY, c, i, hi - om_h * (hi - (even + odd)) + s);
+    st_out<S, 19>(H, g.stride, nb, PARITY, c, j, hj - om_h * (hj - (even - odd)) - s);
   }
   // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
   MrtIn<T> q;
@@ -267,20 +273,22 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   q.s_nu = T(1) / (k.tau_g + ph * (k.tau_l - k.tau_g));
   mrt19_collide_moments<T>(gp_, q);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) st_out<S, 19>(G, g.stride, nb, PARITY, c, i, gp_[i], k.ref_g);
+  for (int i = 0; i < 19; ++i) st_out<S, 19>(G, g.stride, nb, PARITY, c, i, gp_[i]);
 }
 
 // ========================================================== DENDRITE (K2/K3)
+// Both D3Q7 lattices are held as deviations from the far-field liquid:
+// g_i - w_i ref_g (ref_g = -1) and t_i - w_i ref_t (ref_t = -Delta).
 template <class T>
 struct DendK {
   T om_g, om_t, inv_tau0, lambda, eps4;
   int nobj;
-  float ref_g, ref_t;
+  T ref_g, ref_t;
 };
 
 template <class S, class P, int PARITY>
 __global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P* __restrict__ phi_old,
-                                                P* __restrict__ phi_new, const Geom g, float ref_g) {
+                                                P* __restrict__ phi_new, const Geom g, typename Stor<S>::T ref_g) {
   typedef typename Stor<S>::T T;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -295,8 +303,8 @@ __global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P
   const int c = nb.idx(0, 0, 0);
   T s = T(0);
 #pragma unroll
-  for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, g.stride, nb, PARITY, c, i, ref_g);
-  phi_new[c] = P(s);
+  for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, g.stride, nb, PARITY, c, i);
+  phi_new[c] = P(ref_g + s);
 }
 
 // Nearest seed (ties to the lower index), in FP64 like the oracle.
@@ -375,45 +383,47 @@ __global__ void __launch_bounds__(256)
   // phase-field lattice, all seven loaded before any store (in-place safety)
   T gv[7];
 #pragma unroll
-  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, g.stride, nb, PARITY, c, i, k.ref_g);
+  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, g.stride, nb, PARITY, c, i);
+  const T dph = ph - k.ref_g;
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
     const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
-    const T go = gv[i] - k.om_g * (gv[i] - w * ph) + fo * w * eB + w * src;
-    st_out<S, 7>(G, g.stride, nb, PARITY, c, i, go, k.ref_g);
+    const T go = gv[i] - k.om_g * (gv[i] - w * dph) + fo * w * eB + w * src;
+    st_out<S, 7>(G, g.stride, nb, PARITY, c, i, go);
   }
   // thermal lattice: relaxation with latent heat (1/2) dphi
   T t[7];
-  T Tn = T(0);
+  T dT = T(0);
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
-    t[i] = ld_in<S, 7>(Tp, g.stride, nb, PARITY, c, i, k.ref_t);
-    Tn += t[i];
+    t[i] = ld_in<S, 7>(Tp, g.stride, nb, PARITY, c, i);
+    dT += t[i];
   }
   const T lat = T(0.5) * dphi;
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
-    const T to = t[i] - k.om_t * (t[i] - w * Tn) + w * lat;
-    st_out<S, 7>(Tp, g.stride, nb, PARITY, c, i, to, k.ref_t);
+    const T to = t[i] - k.om_t * (t[i] - w * dT) + w * lat;
+    st_out<S, 7>(Tp, g.stride, nb, PARITY, c, i, to);
   }
-  temp[c] = P(Tn);
+  temp[c] = P(k.ref_t + dT);
 }
 
 // ===================================================================== INIT
+// Stores the deviation of  f_i = base_scale w (1 + 3eu + 4.5eu^2 - 1.5u^2) + w p_extra
+// from w ref, placed as the post-collision state of loop 0.
 template <class S, int Q>
-__device__ __forceinline__ void put_eq(S* A, const Geom& g, int x, int y, int z, int64_t c, double base_scale,
-                                       double ux, double uy, double uz, double p_extra, float ref) {
-  // population_i = base_scale * w (1 + 3eu + 4.5eu^2 - 1.5u^2) + w p_extra
+__device__ __forceinline__ void put_eq(S* A, const Geom& g, const Nbr& nb, int c, double base_scale, double ux,
+                                       double uy, double uz, double p_extra, double ref) {
   typedef typename Stor<S>::T T;
   const double uu = ux * ux + uy * uy + uz * uz;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const double w = wq<Q>(i);
     const double eu = ex(i) * ux + ey(i) * uy + ez(i) * uz;
-    const double v = base_scale * (w * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu)) + w * p_extra;
-    store_out_layout<S, Q>(A, g, 0, x, y, z, c, i, T(v), ref);
+    const double v = w * ((base_scale - ref + p_extra) + base_scale * (3.0 * eu + 4.5 * eu * eu - 1.5 * uu));
+    st_layout<S, Q>(A, g.stride, nb, 0, c, i, T(v));
   }
 }
 
@@ -436,27 +446,28 @@ __global__ void k_init(int model, int Q0, S* A0, S* A1, typename PhiOf<S>::type*
   const double tv = in_t ? in_t[c] : d_t;
   if (temp) temp[c] = P(tv);
   if (!g.fluid(x, y, z)) return;
+  const Nbr nb(g, x, y, z);
+  const int ci = (int)c;
   if (model == MK_MODEL_FLOW) {
     const double r = in_rho ? in_rho[c] : d_rho;
     if (Q0 == 19)
-      put_eq<S, 19>(A0, g, x, y, z, c, r, ux, uy, uz, 0.0, refs.r0);
+      put_eq<S, 19>(A0, g, nb, ci, r, ux, uy, uz, 0.0, refs.r0);
     else
-      put_eq<S, 27>(A0, g, x, y, z, c, r, ux, uy, uz, 0.0, refs.r0);
+      put_eq<S, 27>(A0, g, nb, ci, r, ux, uy, uz, 0.0, refs.r0);
   } else if (model == MK_MODEL_MULTIPHASE) {
     // g = geq(p* = 0, u) = w (3eu + 4.5eu^2 - 1.5u^2); h = phi w (1 + ...)
-    put_eq<S, 19>(A0, g, x, y, z, c, 1.0, ux, uy, uz, -1.0, refs.r0);
-    put_eq<S, 19>(A1, g, x, y, z, c, ph, ux, uy, uz, 0.0, refs.r1);
+    put_eq<S, 19>(A0, g, nb, ci, 1.0, ux, uy, uz, -1.0, refs.r0);
+    put_eq<S, 19>(A1, g, nb, ci, ph, ux, uy, uz, 0.0, refs.r1);
   } else {
-    put_eq<S, 7>(A0, g, x, y, z, c, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
-    put_eq<S, 7>(A1, g, x, y, z, c, tv, 0.0, 0.0, 0.0, 0.0, refs.r1);
+    put_eq<S, 7>(A0, g, nb, ci, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
+    put_eq<S, 7>(A1, g, nb, ci, tv, 0.0, 0.0, 0.0, 0.0, refs.r1);
   }
 }
 
 // =================================================================== FIELDS
 template <class S, int Q>
 __global__ void k_field_flow(const S* __restrict__ A, const Geom g, int64_t steps_done, int field, double Fx, double Fy,
-                             double Fz, double rho0, float ref, double* __restrict__ out) {
-  typedef typename Stor<S>::T T;
+                             double Fz, double rho0, double* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
@@ -466,15 +477,17 @@ __global__ void k_field_flow(const S* __restrict__ A, const Geom g, int64_t step
     out[c] = field == MK_FIELD_RHO ? rho0 : 0.0;
     return;
   }
-  double rho = 0, j[3] = {0, 0, 0};
+  const Nbr nb(g, x, y, z);
+  double drho = 0, j[3] = {0, 0, 0};
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    const double f = double(load_out<S, Q>(A, g, steps_done, x, y, z, c, i, ref));
-    rho += f;
+    const double f = double(ld_out<S, Q>(A, g.stride, nb, steps_done, (int)c, i));
+    drho += f;
     j[0] += ex(i) * f;
     j[1] += ey(i) * f;
     j[2] += ez(i) * f;
   }
+  const double rho = rho0 + drho;
   const double F[3] = {Fx, Fy, Fz};
   out[c] = field == MK_FIELD_RHO ? rho : (j[field - MK_FIELD_UX] - 0.5 * F[field - MK_FIELD_UX]) / rho;
 }
@@ -497,10 +510,11 @@ __global__ void k_field_mp(const S* __restrict__ G, const typename PhiOf<S>::typ
     out[c] = 0.0;
     return;
   }
+  const Nbr nb(g, x, y, z);
   T pstar = T(0), j[3] = {T(0), T(0), T(0)};
 #pragma unroll
   for (int i = 0; i < 19; ++i) {
-    const T v = load_out<S, 19>(G, g, steps_done, x, y, z, c, i, k.ref_g);
+    const T v = ld_out<S, 19>(G, g.stride, nb, steps_done, (int)c, i);
     pstar += v;
     j[0] += T(ex(i)) * v;
     j[1] += T(ey(i)) * v;
@@ -511,7 +525,6 @@ __global__ void k_field_mp(const S* __restrict__ G, const typename PhiOf<S>::typ
     return;
   }
   T ph, rho, gp[3], F[3];
-  const Nbr nb(g, x, y, z);
   mp_force<T, P>(phi, nb, (int)c, k, pstar, ph, rho, gp, F);
   const int a = field - MK_FIELD_UX;
   out[c] = double(j[a] - F[a] / (T(2) * rho));
@@ -583,7 +596,7 @@ __device__ __forceinline__ void cell_coords(const Geom& g, int64_t c, int& x, in
 
 template <class S, int Q>
 __global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, const Geom g, int64_t steps_done, double Fx,
-                                                   double Fy, double Fz, float ref, int64_t n,
+                                                   double Fy, double Fz, double rho0, int64_t n,
                                                    double* __restrict__ partial) {
   double v[mke::DG_N];
 #pragma unroll
@@ -592,15 +605,17 @@ __global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, cons
     int x, y, z;
     cell_coords(g, c, x, y, z);
     if (!g.fluid(x, y, z)) continue;
-    double rho = 0, j[3] = {0, 0, 0};
+    const Nbr nb(g, x, y, z);
+    double drho = 0, j[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const double f = double(load_out<S, Q>(A, g, steps_done, x, y, z, c, i, ref));
-      rho += f;
+      const double f = double(ld_out<S, Q>(A, g.stride, nb, steps_done, (int)c, i));
+      drho += f;
       j[0] += ex(i) * f;
       j[1] += ey(i) * f;
       j[2] += ez(i) * f;
     }
+    const double rho = rho0 + drho;
     const double mx = j[0] - 0.5 * Fx, my = j[1] - 0.5 * Fy, mz = j[2] - 0.5 * Fz;
     const bool bad = !(rho > 0.0) || !isfinite(rho) || !isfinite(mx) || !isfinite(my) || !isfinite(mz);
     v[mke::DG_MASS] += rho;
@@ -627,17 +642,17 @@ __global__ void __launch_bounds__(256) k_diag_mp(const S* __restrict__ G, const 
     int x, y, z;
     cell_coords(g, c, x, y, z);
     if (!g.fluid(x, y, z)) continue;
+    const Nbr nb(g, x, y, z);
     T pstar = T(0), j[3] = {T(0), T(0), T(0)};
 #pragma unroll
     for (int i = 0; i < 19; ++i) {
-      const T f = load_out<S, 19>(G, g, steps_done, x, y, z, c, i, k.ref_g);
+      const T f = ld_out<S, 19>(G, g.stride, nb, steps_done, (int)c, i);
       pstar += f;
       j[0] += T(ex(i)) * f;
       j[1] += T(ey(i)) * f;
       j[2] += T(ez(i)) * f;
     }
     T ph, rho, gp[3], F[3];
-    const Nbr nb(g, x, y, z);
     mp_force<T, P>(phi, nb, (int)c, k, pstar, ph, rho, gp, F);
     double u[3];
     for (int a = 0; a < 3; ++a) u[a] = double(j[a] - F[a] / (T(2) * rho));
@@ -726,30 +741,30 @@ void launch_dims(const mke::Engine& e, dim3& grid, dim3& block) {
   grid = dim3((e.nx + e.block_x - 1) / e.block_x, (e.ny + e.block_y - 1) / e.block_y, e.nz);
 }
 
-// Reference values of the shifted storage per lattice.
+// Rest values of the lattices (populations are held as f_i - w_i ref).
 Refs refs_of(const mk_params& p) {
-  Refs r{0.f, 0.f};
+  Refs r{0.0, 0.0};
   if (p.model == MK_MODEL_FLOW) {
-    r.r0 = (float)p.rho0;
+    r.r0 = p.rho0;
   } else if (p.model == MK_MODEL_MULTIPHASE) {
-    r.r0 = 0.f;  // g: rest state 0
-    r.r1 = 1.f;  // h: liquid phi = 1
+    r.r0 = 0.0;  // g: rest state p* = 0, u = 0
+    r.r1 = 1.0;  // h: liquid phi = 1
   } else {
-    r.r0 = -1.f;               // g: liquid phi = -1
-    r.r1 = (float)(-p.delta);  // t/U: far-field value
+    r.r0 = -1.0;      // g: liquid phi = -1
+    r.r1 = -p.delta;  // t/U: far-field value
   }
   return r;
 }
 
 template <class T>
-FlowK<T> flow_coef(const mk_params& p, float ref) {
+FlowK<T> flow_coef(const mk_params& p, double ref) {
   FlowK<T> k;
   k.om = T(1.0 / p.tau);
   k.om_m = T(1.0 / (0.5 + p.magic / (p.tau - 0.5)));
   k.Fx = T(p.force[0]);
   k.Fy = T(p.force[1]);
   k.Fz = T(p.force[2]);
-  k.ref = ref;
+  k.ref = T(ref);
   return k;
 }
 
@@ -768,8 +783,7 @@ MpK<T> mp_coef(const mk_params& p, Refs r) {
   k.gx = T(p.force[0]);
   k.gy = T(p.force[1]);
   k.gz = T(p.force[2]);
-  k.ref_g = r.r0;
-  k.ref_h = r.r1;
+  k.ref_h = T(r.r1);
   return k;
 }
 
@@ -783,8 +797,8 @@ DendK<T> dend_coef(const mk_params& p, Refs r) {
   k.lambda = T(p.lambda);
   k.eps4 = T(p.eps4);
   k.nobj = p.n_objects;
-  k.ref_g = r.r0;
-  k.ref_t = r.r1;
+  k.ref_g = T(r.r0);
+  k.ref_t = T(r.r1);
   return k;
 }
 
@@ -830,9 +844,9 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   P* phi = (P*)e.phi[0];
   if (ev) cudaEventRecord(ev[0], e.stream);
   if (parity == 0)
-    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, phi, g, r.r1);
+    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, phi, g, T(r.r1));
   else
-    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, phi, g, r.r1);
+    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, phi, g, T(r.r1));
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
@@ -865,9 +879,9 @@ void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t*
   P* temp = (P*)e.temp;
   if (ev) cudaEventRecord(ev[0], e.stream);
   if (parity == 0)
-    k_pf_phi<S, P, 0><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, r.r0);
+    k_pf_phi<S, P, 0><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, T(r.r0));
   else
-    k_pf_phi<S, P, 1><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, r.r0);
+    k_pf_phi<S, P, 1><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, T(r.r0));
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
@@ -940,10 +954,10 @@ cudaError_t field_t(mke::Engine& e, int field) {
       return cudaErrorInvalidValue;
     if (e.p.lattice == 19)
       k_field_flow<S, 19><<<grid, block, 0, e.stream>>>((const S*)e.pop0, g, e.step, field, e.p.force[0],
-                                                        e.p.force[1], e.p.force[2], e.p.rho0, r.r0, e.field);
+                                                        e.p.force[1], e.p.force[2], e.p.rho0, e.field);
     else
       k_field_flow<S, 27><<<grid, block, 0, e.stream>>>((const S*)e.pop0, g, e.step, field, e.p.force[0],
-                                                        e.p.force[1], e.p.force[2], e.p.rho0, r.r0, e.field);
+                                                        e.p.force[1], e.p.force[2], e.p.rho0, e.field);
     return cudaGetLastError();
   }
   if (m == MK_MODEL_MULTIPHASE) {
@@ -978,10 +992,10 @@ cudaError_t diag_t(mke::Engine& e) {
   if (m == MK_MODEL_FLOW) {
     if (e.p.lattice == 19)
       k_diag_flow<S, 19><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, g, e.step, e.p.force[0], e.p.force[1],
-                                                   e.p.force[2], r.r0, e.ncell, e.partial);
+                                                   e.p.force[2], e.p.rho0, e.ncell, e.partial);
     else
       k_diag_flow<S, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, g, e.step, e.p.force[0], e.p.force[1],
-                                                   e.p.force[2], r.r0, e.ncell, e.partial);
+                                                   e.p.force[2], e.p.rho0, e.ncell, e.partial);
   } else if (m == MK_MODEL_MULTIPHASE) {
     k_diag_mp<S><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, (const P*)e.phi[0], g, e.step, mp_coef<T>(e.p, r),
                                            e.ncell, e.partial);
@@ -1270,16 +1284,17 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
-  const int bxs[4] = {32, 64, 128, 256};
+  // 64-, 128- and 256-thread blocks, a warp-multiple row along x
+  const int shapes[9][2] = {{32, 2}, {64, 1}, {32, 4}, {64, 2}, {128, 1}, {32, 8}, {64, 4}, {128, 2}, {256, 1}};
   const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 2 : 1;
   double best = 1e300;
   int bbx = bx0, bby = by0, bmb = mb0, ncand = 0;
-  for (int bi = 0; bi < 4 && st == cudaSuccess; ++bi) {
-    const int bx = bxs[bi];
+  for (int si = 0; si < 9 && st == cudaSuccess; ++si) {
+    const int bx = shapes[si][0];
     if (bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
     for (int mb = 1; mb <= nmb && st == cudaSuccess; ++mb) {
       e.block_x = bx;
-      e.block_y = 256 / bx;
+      e.block_y = shapes[si][1];
       e.minb = nmb == 2 ? mb : mb0;
       engine_step(e, nullptr);  // warm-up of this shape
       cudaEventRecord(t0, e.stream);
