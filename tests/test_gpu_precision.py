@@ -1,0 +1,51 @@
+"""Reduced-precision storage over a long run, against the FP64 path.
+
+The FP64 device path equals the CPU oracle to 1e-10 (test_gpu_parity); over
+10,000 loops the oracle is too slow, so the reduced-precision runs are measured
+against the FP64 device run of the same case.  Each line states the phi
+relative L2 error and the drift of the conserved phi sum.
+"""
+import numpy as np
+import pytest
+
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, case_params, cases, initial_field
+from _oracle import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 10000
+
+
+def _case(prec):
+    return cases.multiphase_bubbles(n=64, nz=64, bubbles=6, rmin=6.0, rmax=10.0, width=4.0, gz=-1e-6,
+                                    precision=prec, loops=STEPS)
+
+
+@pytest.fixture(scope="module")
+def fp64_run(tmp_path_factory):
+    d = tmp_path_factory.mktemp("prec")
+    p = case_params(cases.write(_case("fp64"), str(d / "p64.xml")))
+    s = Solver(params=p)
+    d0 = s.diagnostics()
+    s.advance(STEPS, graph=True)
+    return p, s.field("phi"), d0, s.diagnostics(), str(d)
+
+
+# phi relative L2 bounds after 10k loops, set about 2x above the measured
+# errors (FP32 2.6e-4, FP16 8.2e-3, BF16 4.4e-2) so a regression shows; the
+# 1e-3 goal for FP16 is not met yet.
+@pytest.mark.parametrize("prec,bound", [("fp32", 6e-4), ("fp16", 2e-2), ("bf16", 1e-1)])
+def test_shifted_storage_accuracy_10k(fp64_run, prec, bound):
+    p64, phi64, d0_64, d1_64, d = fp64_run
+    p = case_params(cases.write(_case(prec), f"{d}/p_{prec}.xml"))
+    s = Solver(params=p)
+    d0 = s.diagnostics()
+    s.advance(STEPS, graph=True)
+    d1 = s.diagnostics()
+    fl = initial_field(p, "flag") == 0
+    err = rel_l2(s.field("phi"), phi64, fl)
+    drift = abs(d1["phi_sum"] - d0["phi_sum"]) / d0["phi_sum"]
+    print(f"{prec}: phi rel L2 vs FP64 after {STEPS} loops = {err:.3e}, phi-sum drift = {drift:.3e}, "
+          f"FP64 drift = {abs(d1_64['phi_sum'] - d0_64['phi_sum']) / d0_64['phi_sum']:.3e}")
+    assert d1["n_bad"] == 0
+    assert err <= bound, err
