@@ -277,6 +277,25 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
 mk_status mk_host_alloc(size_t bytes, void** out);
 mk_status mk_host_free(void* p);
 
+/* Allocation-free FP64 statistics of a device-resident FP32 field.
+ * No counterpart in the reference (its solver has no device code); it is the
+ * diagnostics reduction for callers that may not call cudaMalloc, such as a
+ * host code whose own pool owns the device memory.  Needs no handle.
+ *   d_field: n floats in device memory; d_out: 5 doubles in device memory,
+ *   {sum, sum of squares, min, max, count of non-finite values} (the first
+ *   four over the finite values).  Asynchronous on `stream` (NULL = legacy
+ *   default stream).
+ * The block partials live in a fixed 80 KiB device array inside the library,
+ * so n is limited to MK_NOALLOC_MAX_CELLS (larger n: MK_ERR_ARG, message in
+ * mk_noalloc_last_error).  Every call on a device shares that array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on a device looks up the array's address and should come before
+ * any stream capture.  Calls no allocating routine. */
+#define MK_NOALLOC_MAX_BLOCKS 2048
+#define MK_NOALLOC_MAX_CELLS ((int64_t)MK_NOALLOC_MAX_BLOCKS * 256 * 64)
+mk_status mk_field_stats_noalloc(const float* d_field, int64_t n, double* d_out, void* stream);
+const char* mk_noalloc_last_error(void);
+
 /* Algorithmic bytes per cell per step of the handle's configuration. */
 double mk_bytes_per_cell(const mk_handle* h);
 int64_t mk_fluid_cells(const mk_handle* h);

@@ -25,6 +25,7 @@ MK_BC_PERIODIC, MK_BC_WALLS, MK_BC_CLOSED = range(3)
  MK_FIELD_PRESSURE, MK_FIELD_DPHI, MK_FIELD_GRAIN) = range(11)
 MK_DTYPE_F64, MK_DTYPE_F32 = 0, 1
 MK_MAX_OBJECTS = 64
+MK_NOALLOC_MAX_CELLS = 2048 * 256 * 64
 
 PRECISIONS = {"fp64": MK_PREC_FP64, "fp32": MK_PREC_FP32, "fp16": MK_PREC_FP16, "bf16": MK_PREC_BF16}
 MODELS = {"flow": MK_MODEL_FLOW, "multiphase": MK_MODEL_MULTIPHASE, "thermal_dendrite": MK_MODEL_THERMAL_DENDRITE,
@@ -121,6 +122,8 @@ PROTOTYPES = {
     "mk_autotune": (C.c_int, [H, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_double)]),
     "mk_host_alloc": (C.c_int, [C.c_size_t, P(C.c_void_p)]),
     "mk_host_free": (C.c_int, [C.c_void_p]),
+    "mk_field_stats_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "mk_noalloc_last_error": (C.c_char_p, []),
     "mk_bytes_per_cell": (C.c_double, [H]),
     "mk_fluid_cells": (C.c_int64, [H]),
     "mk_launches_per_step": (C.c_int32, [H]),
