@@ -197,7 +197,8 @@ def run_ours(args):
         t_launch = prof["kernel_ms"] / launches * 1e-3
         S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
         phi_b = 8 if prec == "fp64" else 4
-        collide_bytes = fluid * (2 * 38 * S + phi_b)
+        # 16-bit storage keeps the Allen-Cahn rest population in FP32 (+2 B each way)
+        collide_bytes = fluid * (2 * 38 * S + phi_b + (4 if S == 2 else 0))
         achieved = collide_bytes / t_launch / 1e9
         step_gbs = bpc * cells * K / (ms * 1e-3) / 1e9
         d = s.diagnostics(raise_on_divergence=False)

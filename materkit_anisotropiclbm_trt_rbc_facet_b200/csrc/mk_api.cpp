@@ -446,6 +446,7 @@ mk_status mk_checkpoint(mk_handle* h, const char* path) {
   dump(e.phi[0], bp);
   dump(e.phi[1], e.phi[1] ? bp : 0);
   dump(e.temp, e.temp ? bp : 0);
+  dump(e.rest1, e.rest1 ? (uint64_t)e.ncell * sizeof(float) : 0);
   fclose(f);
   if (!ok) {
     h->err = std::string("checkpoint write failed: ") + path;
@@ -496,6 +497,7 @@ mk_status mk_restore(mk_handle* h, const char* path) {
   load(e.phi[0], bp);
   load(e.phi[1], e.phi[1] ? bp : 0);
   load(e.temp, e.temp ? bp : 0);
+  load(e.rest1, e.rest1 ? (uint64_t)e.ncell * sizeof(float) : 0);
   fclose(f);
   if (!ok) {
     h->err = "checkpoint truncated";

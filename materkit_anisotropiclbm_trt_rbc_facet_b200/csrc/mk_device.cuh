@@ -215,6 +215,85 @@ __host__ __device__ __forceinline__ void mrt19_collide_moments(T (&f)[19], const
   }
 }
 
+// The same collision with the two transforms written out in the pair-split
+// basis, sharing partial sums (face sum, edge sum, the x/y/z edge fluxes), so
+// the forward transform is ~45 additions and the back transform ~60.  Pairs:
+// p = 1..3 the +-x, +-y, +-z faces; p = 4..9 the xy(+,+), xy(+,-), xz(+,+),
+// xz(+,-), yz(+,+), yz(+,-) edges (direction 2p-1, opposite 2p).
+template <class T>
+__host__ __device__ __forceinline__ void mrt19_collide_fact(T (&f)[19], const MrtIn<T>& q) {
+  T s[10], a[10];
+  s[0] = f[0];
+  a[0] = T(0);
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    s[p] = f[2 * p - 1] + f[2 * p];
+    a[p] = f[2 * p - 1] - f[2 * p];
+  }
+  T m[19];
+  const T Sf = s[1] + s[2] + s[3];
+  const T Se = (s[4] + s[5]) + (s[6] + s[7]) + (s[8] + s[9]);
+  m[0] = s[0] + Sf + Se;
+  m[1] = T(-30) * s[0] - T(11) * Sf + T(8) * Se;
+  m[2] = T(12) * s[0] - T(4) * Sf + Se;
+  const T t9 = T(2) * s[1] - s[2] - s[3];
+  const T u9 = (s[4] + s[5]) + (s[6] + s[7]) - T(2) * (s[8] + s[9]);
+  m[9] = t9 + u9;
+  m[10] = T(-2) * t9 + u9;
+  const T t11 = s[2] - s[3];
+  const T u11 = (s[4] + s[5]) - (s[6] + s[7]);
+  m[11] = t11 + u11;
+  m[12] = T(-2) * t11 + u11;
+  m[13] = s[4] - s[5];
+  m[14] = s[8] - s[9];
+  m[15] = s[6] - s[7];
+  const T Ax = (a[4] + a[5]) + (a[6] + a[7]);
+  const T Ay = (a[4] - a[5]) + (a[8] + a[9]);
+  const T Az = (a[6] - a[7]) + (a[8] - a[9]);
+  m[3] = a[1] + Ax;
+  m[4] = T(-4) * a[1] + Ax;
+  m[5] = a[2] + Ay;
+  m[6] = T(-4) * a[2] + Ay;
+  m[7] = a[3] + Az;
+  m[8] = T(-4) * a[3] + Az;
+  m[16] = (a[4] + a[5]) - (a[6] + a[7]);
+  m[17] = (a[5] - a[4]) + (a[8] + a[9]);
+  m[18] = (a[6] - a[7]) - (a[8] - a[9]);
+  T d[19];
+  mrt_relax_all<T>(m, d, q, std::make_integer_sequence<int, 19>{});
+  // back transform f -= M^T d, even part E and odd part O per pair
+  f[0] -= d[0] - T(30) * d[1] + T(12) * d[2];
+  const T cf = d[0] - T(11) * d[1] - T(4) * d[2];
+  const T ce = d[0] + T(8) * d[1] + d[2];
+  const T g9 = d[9] + d[10];
+  const T h11 = d[11] + d[12];
+  T E[10], O[10];
+  E[1] = cf + T(2) * d[9] - T(4) * d[10];
+  E[2] = cf - d[9] + T(2) * d[10] + d[11] - T(2) * d[12];
+  E[3] = cf - d[9] + T(2) * d[10] - d[11] + T(2) * d[12];
+  E[4] = ce + g9 + h11 + d[13];
+  E[5] = ce + g9 + h11 - d[13];
+  E[6] = ce + g9 - h11 + d[15];
+  E[7] = ce + g9 - h11 - d[15];
+  E[8] = ce - T(2) * g9 + d[14];
+  E[9] = ce - T(2) * g9 - d[14];
+  const T jx = d[3] + d[4], jy = d[5] + d[6], jz = d[7] + d[8];
+  O[1] = d[3] - T(4) * d[4];
+  O[2] = d[5] - T(4) * d[6];
+  O[3] = d[7] - T(4) * d[8];
+  O[4] = jx + jy + d[16] - d[17];
+  O[5] = jx - jy + d[16] + d[17];
+  O[6] = jx + jz - d[16] + d[18];
+  O[7] = jx - jz - d[16] - d[18];
+  O[8] = jy + jz + d[17] - d[18];
+  O[9] = jy - jz + d[17] + d[18];
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    f[2 * p - 1] -= E[p] + O[p];
+    f[2 * p] -= E[p] - O[p];
+  }
+}
+
 // f -= Mi [ S M (f - feq) - (I - S/2) M F ]   (all loops unrolled; M is
 // integer so the compiler folds every zero).
 template <class T>
@@ -252,6 +331,8 @@ __host__ __device__ __forceinline__ void mrt19_collide(T (&f)[19], const T (&feq
 // away, and the 16-bit formats hold f'_i / w_i, a plane-independent O(1)
 // quantity inside the normal range of FP16.  FP64 and FP32 store f', FP16 and
 // BF16 store f'/w; collision arithmetic is FP64 or FP32.
+// st_rt stores like st and returns the value a later ld will see (used to
+// carry the 16-bit rounding residual into an FP32 rest population).
 template <class S>
 struct Stor;
 template <>
@@ -260,6 +341,10 @@ struct Stor<double> {
   static constexpr int bytes = 8;
   __device__ __forceinline__ static double ld(const double* p, double) { return *p; }
   __device__ __forceinline__ static void st(double* p, double v, double) { *p = v; }
+  __device__ __forceinline__ static double st_rt(double* p, double v, double) {
+    *p = v;
+    return v;
+  }
 };
 template <>
 struct Stor<float> {
@@ -267,6 +352,10 @@ struct Stor<float> {
   static constexpr int bytes = 4;
   __device__ __forceinline__ static float ld(const float* p, float) { return *p; }
   __device__ __forceinline__ static void st(float* p, float v, float) { *p = v; }
+  __device__ __forceinline__ static float st_rt(float* p, float v, float) {
+    *p = v;
+    return v;
+  }
 };
 template <>
 struct Stor<__half> {
@@ -274,6 +363,11 @@ struct Stor<__half> {
   static constexpr int bytes = 2;
   __device__ __forceinline__ static float ld(const __half* p, float w) { return w * __half2float(*p); }
   __device__ __forceinline__ static void st(__half* p, float v, float w) { *p = __float2half_rn(v * (1.0f / w)); }
+  __device__ __forceinline__ static float st_rt(__half* p, float v, float w) {
+    const __half h = __float2half_rn(v * (1.0f / w));
+    *p = h;
+    return w * __half2float(h);
+  }
 };
 template <>
 struct Stor<__nv_bfloat16> {
@@ -282,6 +376,11 @@ struct Stor<__nv_bfloat16> {
   __device__ __forceinline__ static float ld(const __nv_bfloat16* p, float w) { return w * __bfloat162float(*p); }
   __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float w) {
     *p = __float2bfloat16_rn(v * (1.0f / w));
+  }
+  __device__ __forceinline__ static float st_rt(__nv_bfloat16* p, float v, float w) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v * (1.0f / w));
+    *p = h;
+    return w * __bfloat162float(h);
   }
 };
 
@@ -380,6 +479,48 @@ struct Nbr {
   }
 };
 
+// Addressing of a cell whose y and z neighbours are all fluid and need no
+// periodic wrap (every row of the domain interior, so a warp — one row
+// segment — takes this path as a whole).  x neighbours come from two
+// wrap-aware offsets; no fluid tests, no selects.
+struct Fast {
+  int c, xm, xp, nx, nxy;
+  __device__ __forceinline__ int xo(int d) const { return d < 0 ? xm : (d > 0 ? xp : 0); }
+  __device__ __forceinline__ int idx(int dx, int dy, int dz) const { return c + xo(dx) + dy * nx + dz * nxy; }
+};
+
+// Whether (x,y,z) may use Fast: y, z strictly inside the fluid span of their
+// axis, x inside it or on a periodic axis.
+__device__ __forceinline__ bool fast_cell(const Geom& g, int x, int y, int z) {
+  auto inside = [](int c, int n, int bc) {
+    const int lo = bc == 1 ? 2 : 1;
+    const int hi = bc == 1 ? n - 3 : n - 2;
+    return c >= lo && c <= hi;
+  };
+  return inside(y, g.ny, g.bc1) && inside(z, g.nz, g.bc2) && (g.bc0 == 0 ? g.nx >= 3 : inside(x, g.nx, g.bc0));
+}
+
+__device__ __forceinline__ Fast make_fast(const Geom& g, int x, int y, int z) {
+  Fast f;
+  f.nx = g.nx;
+  f.nxy = g.nx * g.ny;
+  f.c = x + g.nx * (y + g.ny * z);
+  f.xm = x == 0 ? g.nx - 1 : -1;
+  f.xp = x == g.nx - 1 ? -(g.nx - 1) : 1;
+  return f;
+}
+
+template <int Q>
+__device__ __forceinline__ int64_t off_in(int64_t stride, const Fast& fa, int parity, int, int i) {
+  if (parity == 0) return (int64_t)i * stride + fa.c;
+  return (int64_t)inv(i) * stride + fa.idx(-ex(i), -ey(i), -ez(i));
+}
+template <int Q>
+__device__ __forceinline__ int64_t off_out(int64_t stride, const Fast& fa, int parity, int, int i) {
+  if (parity == 0) return (int64_t)inv(i) * stride + fa.c;
+  return (int64_t)i * stride + fa.idx(ex(i), ey(i), ez(i));
+}
+
 // Element offset of the slot population i of the cell at `c` is read from
 // (pre-collision) at the given AA parity.  The bounce-back alternative is a
 // select, not a branch, so every access is one load or store.
@@ -400,19 +541,33 @@ __device__ __forceinline__ int64_t off_out(int64_t stride, const Nbr& nb, int pa
   return (int64_t)(f ? i : inv(i)) * stride + cell;
 }
 
-// Pre-collision deviation f'_i of the cell at `c` (= nb.idx(0,0,0)).
-template <class S, int Q>
-__device__ __forceinline__ typename Stor<S>::T ld_in(const S* __restrict__ A, int64_t stride, const Nbr& nb,
+// Pre-collision deviation f'_i of the cell at `c` (= nb.idx(0,0,0)); `nb` is
+// a general neighbourhood (Nbr) or an interior-row one (Fast).
+template <class S, int Q, class NB>
+__device__ __forceinline__ typename Stor<S>::T ld_in(const S* __restrict__ A, int64_t stride, const NB& nb,
                                                       int parity, int c, int i) {
   return Stor<S>::ld(A + off_in<Q>(stride, nb, parity, c, i), typename Stor<S>::T(wq<Q>(i)));
 }
 
 // Store the post-collision deviation f'_i of the cell at `c`.
-template <class S, int Q>
-__device__ __forceinline__ void st_out(S* __restrict__ A, int64_t stride, const Nbr& nb, int parity, int c, int i,
+template <class S, int Q, class NB>
+__device__ __forceinline__ void st_out(S* __restrict__ A, int64_t stride, const NB& nb, int parity, int c, int i,
                                        typename Stor<S>::T v) {
   Stor<S>::st(A + off_out<Q>(stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
 }
+
+// Store and return the value a later load will see.
+template <class S, int Q, class NB>
+__device__ __forceinline__ typename Stor<S>::T st_out_rt(S* __restrict__ A, int64_t stride, const NB& nb, int parity,
+                                                          int c, int i, typename Stor<S>::T v) {
+  return Stor<S>::st_rt(A + off_out<Q>(stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
+}
+
+// Neighbour queries common to both neighbourhood kinds.
+__device__ __forceinline__ bool nb_fluid(const Nbr& nb, int dx, int dy, int dz) { return nb.fluid(dx, dy, dz); }
+__device__ __forceinline__ bool nb_fluid(const Fast&, int, int, int) { return true; }
+__device__ __forceinline__ int nb_idx(const Nbr& nb, int dx, int dy, int dz) { return nb.idx(dx, dy, dz); }
+__device__ __forceinline__ int nb_idx(const Fast& fa, int dx, int dy, int dz) { return fa.idx(dx, dy, dz); }
 
 // Post-collision deviation f'_i of a cell in the layout left after
 // `steps_done` loops (field output, diagnostics): the slot the last loop

@@ -45,6 +45,7 @@ struct Engine {
   // device buffers
   void* pop0;
   void* pop1;
+  float* rest1;       // FP32 rest population of lattice 1 (multiphase h) with 16-bit storage, else null
   void* phi[2];
   void* temp;
   double* seeds;      // n_objects * 12 doubles: centre (3), rotation (9, row-major, columns = crystal axes)

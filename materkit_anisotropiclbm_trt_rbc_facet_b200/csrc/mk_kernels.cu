@@ -138,33 +138,52 @@ struct MpK {
   T ref_h;  // 1
 };
 
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, P* __restrict__ phi, const Geom g,
-                                                typename Stor<S>::T ref_h) {
+// With 16-bit storage the Allen-Cahn rest population h_0 (always stored at
+// its own cell, in both AA parities) lives in an FP32 plane H0 and absorbs the
+// rounding residual of the cell's 18 moving populations, so sum(h) — the
+// conserved phase volume — is kept to FP32 rounding.
+template <class S>
+struct Rest32 {
+  static constexpr bool on = Stor<S>::bytes == 2;
+};
+
+template <class S, class P, int PARITY, class NB>
+__device__ __forceinline__ void mp_phi_cell(const S* __restrict__ H, const float* __restrict__ H0, P* __restrict__ phi,
+                                            int64_t stride, const NB& nb, int c, typename Stor<S>::T ref_h) {
   typedef typename Stor<S>::T T;
+  T s = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
+#pragma unroll
+  for (int i = 1; i < 19; ++i) s += ld_in<S, 19>(H, stride, nb, PARITY, c, i);
+  phi[c] = P(ref_h + s);
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const float* __restrict__ H0,
+                                                P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const Nbr nb(g, x, y, z);
-  const int c = nb.idx(0, 0, 0);
-  T s = T(0);
-#pragma unroll
-  for (int i = 0; i < 19; ++i) s += ld_in<S, 19>(H, g.stride, nb, PARITY, c, i);
-  phi[c] = P(ref_h + s);
+  if (fast_cell(g, x, y, z)) {
+    const Fast fa = make_fast(g, x, y, z);
+    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, ref_h);
+  } else {
+    const Nbr nb(g, x, y, z);
+    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), ref_h);
+  }
 }
 
 // Density, phi gradient and total force of a fluid cell (shared by the
 // collision and by field output so both see identical values).
-template <class T, class P>
-__device__ __forceinline__ void mp_force(const P* __restrict__ phi, const Nbr& nb, int c, const MpK<T>& k, T pstar,
+template <class T, class P, class NB>
+__device__ __forceinline__ void mp_force(const P* __restrict__ phi, const NB& nb, int c, const MpK<T>& k, T pstar,
                                          T& ph, T& rho, T (&gp)[3], T (&F)[3]) {
   ph = T(phi[c]);
   const T wall = ph + k.coef_wet * ph * (T(1) - ph);
   T gx = T(0), gy = T(0), gz = T(0), l = T(0);
 #pragma unroll
   for (int i = 1; i < 19; ++i) {
-    const T fn = nb.fluid(ex(i), ey(i), ez(i)) ? T(__ldg(phi + nb.idx(ex(i), ey(i), ez(i)))) : wall;
+    const T fn = nb_fluid(nb, ex(i), ey(i), ez(i)) ? T(__ldg(phi + nb_idx(nb, ex(i), ey(i), ez(i)))) : wall;
     const T w = T(wq<19>(i));
     if (ex(i)) gx += (w * T(ex(i))) * fn;
     if (ey(i)) gy += (w * T(ey(i))) * fn;
@@ -188,25 +207,18 @@ __device__ __forceinline__ void mp_force(const P* __restrict__ phi, const Nbr& n
 // before any store: the loads are the latency the kernel must hide, and a
 // store into the same array in between would stop the compiler from hoisting
 // the later loads (in place, on odd loops a direction's result goes to the
-// slot its opposite direction is read from).  MINB is the occupancy hint
-// (resident 256-thread blocks per SM): 1 keeps every value in registers, 2
-// doubles the warps per SM at the price of a few spills; the autotuner picks.
-template <class S, class P, int PARITY, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
-                                                          const P* __restrict__ phi, const Geom g,
-                                                          const MpK<typename Stor<S>::T> k) {
+// slot its opposite direction is read from).
+template <class S, class P, int PARITY, class NB>
+__device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                                const P* __restrict__ phi, const int64_t stride, const NB& nb,
+                                                const int c, const MpK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const Nbr nb(g, x, y, z);
-  const int c = nb.idx(0, 0, 0);
   T gp_[19], h[19];  // g, and the deviations h_i - w_i
 #pragma unroll
-  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, g.stride, nb, PARITY, c, i);
+  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, stride, nb, PARITY, c, i);
+  h[0] = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) h[i] = ld_in<S, 19>(H, g.stride, nb, PARITY, c, i);
+  for (int i = 1; i < 19; ++i) h[i] = ld_in<S, 19>(H, stride, nb, PARITY, c, i);
   T pstar = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
   for (int i = 0; i < 19; ++i) {
@@ -216,7 +228,7 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
     if (ez(i)) jz += T(ez(i)) * gp_[i];
   }
   T ph, rho, gphi[3], F[3];
-  mp_force<T, P>(phi, nb, c, k, pstar, ph, rho, gphi, F);
+  mp_force<T, P, NB>(phi, nb, c, k, pstar, ph, rho, gphi, F);
   const T irho = T(1) / rho;
   const T ux = jx + T(0.5) * F[0] * irho;
   const T uy = jy + T(0.5) * F[1] * irho;
@@ -231,12 +243,7 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   const T om_h = k.om_h;
   const T src = (T(1) - T(0.5) * om_h) * lam;
   const T dph = ph - k.ref_h;
-  {
-    const T w = T(wq<19>(0));
-    const T h0 = h[0];
-    const T heq = w * (dph - T(1.5) * ph * uu);
-    st_out<S, 19>(H, g.stride, nb, PARITY, c, 0, h0 - om_h * (h0 - heq));
-  }
+  T resid = T(0);  // what the 16-bit stores rounded away (Rest32 only)
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
     const int i = 2 * p - 1, j = 2 * p;
@@ -248,8 +255,25 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
     const T even = w * (dph + ph * (T(4.5) * eu * eu - T(1.5) * uu));
     const T odd = ph * (w * (T(3) * eu));
     const T s = src * w * en;
-    st_out<S, 19>(H, g.stride, nb, PARITY, c, i, hi - om_h * (hi - (even + odd)) + s);
-    st_out<S, 19>(H, g.stride, nb, PARITY, c, j, hj - om_h * (hj - (even - odd)) - s);
+    const T vi = hi - om_h * (hi - (even + odd)) + s;
+    const T vj = hj - om_h * (hj - (even - odd)) - s;
+    if constexpr (Rest32<S>::on) {
+      resid += (vi - st_out_rt<S, 19>(H, stride, nb, PARITY, c, i, vi)) +
+               (vj - st_out_rt<S, 19>(H, stride, nb, PARITY, c, j, vj));
+    } else {
+      st_out<S, 19>(H, stride, nb, PARITY, c, i, vi);
+      st_out<S, 19>(H, stride, nb, PARITY, c, j, vj);
+    }
+  }
+  {
+    const T w = T(wq<19>(0));
+    const T h0 = h[0];
+    const T heq = w * (dph - T(1.5) * ph * uu);
+    const T v0 = h0 - om_h * (h0 - heq);
+    if constexpr (Rest32<S>::on)
+      H0[c] = float(v0 + resid);
+    else
+      st_out<S, 19>(H, stride, nb, PARITY, c, 0, v0);
   }
   // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
   MrtIn<T> q;
@@ -271,9 +295,29 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   q.uz = uz;
   q.sF = irho;
   q.s_nu = T(1) / (k.tau_g + ph * (k.tau_l - k.tau_g));
-  mrt19_collide_moments<T>(gp_, q);
+  mrt19_collide_fact<T>(gp_, q);
 #pragma unroll
-  for (int i = 0; i < 19; ++i) st_out<S, 19>(G, g.stride, nb, PARITY, c, i, gp_[i]);
+  for (int i = 0; i < 19; ++i) st_out<S, 19>(G, stride, nb, PARITY, c, i, gp_[i]);
+}
+
+// MINB is the occupancy hint (resident 256-thread blocks per SM): 1 keeps
+// every value in registers, 2 doubles the warps per SM at the price of a few
+// spills; the autotuner picks.  Interior rows take the Fast addressing.
+template <class S, class P, int PARITY, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
+                                                          float* __restrict__ H0, const P* __restrict__ phi,
+                                                          const Geom g, const MpK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  if (fast_cell(g, x, y, z)) {
+    const Fast fa = make_fast(g, x, y, z);
+    mp_collide_cell<S, P, PARITY>(G, H, H0, phi, g.stride, fa, fa.c, k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    mp_collide_cell<S, P, PARITY>(G, H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), k);
+  }
 }
 
 // ========================================================== DENDRITE (K2/K3)
@@ -428,7 +472,7 @@ __device__ __forceinline__ void put_eq(S* A, const Geom& g, const Nbr& nb, int c
 }
 
 template <class S, class InT>
-__global__ void k_init(int model, int Q0, S* A0, S* A1, typename PhiOf<S>::type* phi0,
+__global__ void k_init(int model, int Q0, S* A0, S* A1, float* H0, typename PhiOf<S>::type* phi0,
                        typename PhiOf<S>::type* phi1, typename PhiOf<S>::type* temp, const InT* __restrict__ in_phi,
                        const InT* __restrict__ in_t, const InT* __restrict__ in_rho,
                        const InT* __restrict__ in_u, double d_rho, double d_ux, double d_uy, double d_uz,
@@ -458,6 +502,7 @@ __global__ void k_init(int model, int Q0, S* A0, S* A1, typename PhiOf<S>::type*
     // g = geq(p* = 0, u) = w (3eu + 4.5eu^2 - 1.5u^2); h = phi w (1 + ...)
     put_eq<S, 19>(A0, g, nb, ci, 1.0, ux, uy, uz, -1.0, refs.r0);
     put_eq<S, 19>(A1, g, nb, ci, ph, ux, uy, uz, 0.0, refs.r1);
+    if (H0) H0[c] = float(wq<19>(0) * ((ph - refs.r1) - 1.5 * ph * (ux * ux + uy * uy + uz * uz)));
   } else {
     put_eq<S, 7>(A0, g, nb, ci, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
     put_eq<S, 7>(A1, g, nb, ci, tv, 0.0, 0.0, 0.0, 0.0, refs.r1);
@@ -844,23 +889,23 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   P* phi = (P*)e.phi[0];
   if (ev) cudaEventRecord(ev[0], e.stream);
   if (parity == 0)
-    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, phi, g, T(r.r1));
+    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
   else
-    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, phi, g, T(r.r1));
+    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
   }
   if (e.minb == 1) {
     if (parity == 0)
-      k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+      k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
     else
-      k_mp_collide<S, P, 1, 1><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+      k_mp_collide<S, P, 1, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
   } else {
     if (parity == 0)
-      k_mp_collide<S, P, 0, 2><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+      k_mp_collide<S, P, 0, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
     else
-      k_mp_collide<S, P, 1, 2><<<grid, block, 0, e.stream>>>(G, H, phi, g, k);
+      k_mp_collide<S, P, 1, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
   }
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
@@ -924,7 +969,8 @@ cudaError_t set_state_t(mke::Engine& e, const InT* d_phi, const InT* d_t, const 
   dim3 grid, block;
   launch_dims(e, grid, block);
   const Geom g = make_geom(e);
-  k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, (P*)e.phi[0], (P*)e.phi[1],
+  k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, e.rest1, (P*)e.phi[0],
+                                               (P*)e.phi[1],
                                           (P*)e.temp, d_phi, d_t, d_rho, d_u, e.p.rho0, e.p.u0[0], e.p.u0[1],
                                           e.p.u0[2], -e.p.delta, g, e.ncell, refs_of(e.p));
   return cudaGetLastError();
@@ -1060,6 +1106,11 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   };
   if ((st = alloc(&e.pop0, (size_t)e.Q0 * e.stride * e.elem)) != cudaSuccess) return st;
   if ((st = alloc(&e.pop1, (size_t)e.Q1 * e.stride * e.elem)) != cudaSuccess) return st;
+  if (p.model == MK_MODEL_MULTIPHASE && e.elem == 2) {
+    if ((st = alloc((void**)&e.rest1, (size_t)e.ncell * sizeof(float))) != cudaSuccess) return st;
+  } else {
+    e.rest1 = nullptr;
+  }
   if ((st = alloc(&e.phi[0], (size_t)e.ncell * e.phi_elem)) != cudaSuccess) return st;
   const bool dend = p.model == MK_MODEL_THERMAL_DENDRITE || p.model == MK_MODEL_SOLUTAL_DENDRITE;
   if ((st = alloc(&e.phi[1], dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
@@ -1109,8 +1160,8 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
-  void* ptrs[] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.seeds, e.partial, e.dsum, e.field, e.field32,
-                  e.stage32};
+  void* ptrs[] = {e.pop0, e.pop1, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.partial, e.dsum, e.field,
+                  e.field32, e.stage32};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (e.stream) cudaStreamDestroy(e.stream);
@@ -1257,8 +1308,9 @@ cudaError_t engine_diag(Engine& e, double* out) {
 cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   if (trial_steps < 1) trial_steps = 1;
   const size_t b0 = engine_pop_bytes(e, 0), b1 = engine_pop_bytes(e, 1), bp = (size_t)e.ncell * e.phi_elem;
-  void* const bufs[5] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp};
-  const size_t sizes[5] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0};
+  void* const bufs[6] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.rest1};
+  const size_t sizes[6] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0,
+                           e.rest1 ? (size_t)e.ncell * sizeof(float) : 0};
   size_t total = 0;
   for (size_t s : sizes) total += s;
   char* save = nullptr;
@@ -1266,7 +1318,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   if (st != cudaSuccess) return st;
   auto copy = [&](bool to_save) -> cudaError_t {
     size_t off = 0;
-    for (int q = 0; q < 5; ++q) {
+    for (int q = 0; q < 6; ++q) {
       if (!sizes[q]) continue;
       cudaError_t s2 = to_save ? cudaMemcpyAsync(save + off, bufs[q], sizes[q], cudaMemcpyDeviceToDevice, e.stream)
                                : cudaMemcpyAsync(bufs[q], save + off, sizes[q], cudaMemcpyDeviceToDevice, e.stream);
@@ -1343,9 +1395,11 @@ size_t engine_pop_bytes(const Engine& e, int which) {
 double engine_bytes_per_cell(const Engine& e) {
   // Compulsory traffic: every population read once and written once; phi
   // written once and read once where a model has it.
+  // An FP32 rest plane (16-bit multiphase storage) moves 4 B instead of 2 B.
   const double S = e.elem;
   const double phi = e.p.model == MK_MODEL_FLOW ? 0.0 : 2.0 * e.phi_elem;
-  return 2.0 * (e.Q0 + e.Q1) * S + phi;
+  const double rest = e.rest1 ? 2.0 * (4.0 - S) : 0.0;
+  return 2.0 * (e.Q0 + e.Q1) * S + phi + rest;
 }
 
 }  // namespace mke

@@ -31,10 +31,10 @@ def fp64_run(tmp_path_factory):
     return p, s.field("phi"), d0, s.diagnostics(), str(d)
 
 
-# phi relative L2 bounds after 10k loops, set about 2x above the measured
-# errors (FP32 2.6e-4, FP16 8.2e-3, BF16 4.4e-2) so a regression shows; the
-# 1e-3 goal for FP16 is not met yet.
-@pytest.mark.parametrize("prec,bound", [("fp32", 6e-4), ("fp16", 2e-2), ("bf16", 1e-1)])
+# phi relative L2 bounds after 10k loops: 1e-3 is the goal for the shifted
+# 16-bit storage (measured FP32 2.5e-4, FP16 3.0e-4, BF16 6.7e-4 with the FP32
+# rest population carrying the rounding residual).
+@pytest.mark.parametrize("prec,bound", [("fp32", 6e-4), ("fp16", 1e-3), ("bf16", 1.5e-3)])
 def test_shifted_storage_accuracy_10k(fp64_run, prec, bound):
     p64, phi64, d0_64, d1_64, d = fp64_run
     p = case_params(cases.write(_case(prec), f"{d}/p_{prec}.xml"))
