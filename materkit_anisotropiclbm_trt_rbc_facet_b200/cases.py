@@ -56,6 +56,39 @@ def thermal_dendrite(n=128, loops=5000, precision="fp32", eps4=0.05, W0=1.5, lam
 """
 
 
+def solutal_dendrite(n=64, ny=None, nz=None, loops=3000, precision="fp32", eps4=0.04, W0=1.5, lam=10.0,
+                     delta=0.55, D=0.1, D_s=1e-4, k=0.15, seeds=None, tau0=None) -> str:
+    """Config 4 element: D3Q7 solutal lattice + anisotropic phase field, closed faces.
+
+    `seeds` is a list of (center xyz, angles xyz in degrees, radius); default one
+    centred seed of radius 6.
+    """
+    ny = n if ny is None else ny
+    nz = n if nz is None else nz
+    if seeds is None:
+        seeds = [(((n - 1) / 2.0, (ny - 1) / 2.0, (nz - 1) / 2.0), (0.0, 0.0, 0.0), 6.0)]
+    cen = " ".join(f"{c[0]} {c[1]} {c[2]}" for c, _, _ in seeds)
+    ang = " ".join(f"{a[0]} {a[1]} {a[2]}" for _, a, _ in seeds)
+    rad = " ".join(f"{r}" for _, _, r in seeds)
+    t0 = f"<tau0> {tau0} </tau0>" if tau0 else ""
+    return _HEADER.format(dendrite="true", flow="false", loops=loops, frames=min(loops, 100), nx=n, ny=ny, nz=nz) + f"""
+  <phasechange>
+    <d0> 0.2762 </d0> <lambda> {lam} </lambda> <anisotropy> {eps4} </anisotropy> <W0> 1.0 </W0> <t0> 1.0 </t0>
+  </phasechange>
+  <composition> <number> 1 </number> <diffFluid> {D} </diffFluid> <diffSolid> {D_s} </diffSolid>
+    <iniValue> {-delta} </iniValue> <partition> {k} </partition> </composition>
+  <b200>
+    <model> solutal_dendrite </model> <precision> {precision} </precision>
+    <boundary> closed closed closed </boundary>
+    <eps4> {eps4} </eps4> <W0> {W0} </W0> <lambda> {lam} </lambda> <delta> {delta} </delta>
+    <diffusivity> {D} </diffusivity> <diffSolid> {D_s} </diffSolid> <partition> {k} </partition> {t0}
+    <objects> <number> {len(seeds)} </number> <center> {cen} </center> <angle> {ang} </angle>
+      <radius> {rad} </radius> </objects>
+  </b200>
+</MaterKit>
+"""
+
+
 def multiphase_bubbles(n=256, nz=None, loops=10000, precision="fp32", bubbles=24, rmin=8.0, rmax=16.0,
                        seed=0xB200, width=4.0, sigma=1e-3, rho_ratio=10.0, nu_ratio=10.0, tau_l=0.8,
                        mobility=0.05, gz=-1e-6, contact_angle=90.0) -> str:

@@ -328,6 +328,7 @@ struct DendK {
   T om_g, om_t, inv_tau0, lambda, eps4;
   int nobj;
   T ref_g, ref_t;
+  T k_part, D_l, D_s, at_w0;  // solutal lattice
 };
 
 template <class S, class P, int PARITY>
@@ -389,23 +390,21 @@ __device__ __forceinline__ void anisotropy(const double* __restrict__ Rm, T eps4
   for (int q = 0; q < 3; ++q) N[q] = R[q * 3 + 0] * Nc[0] + R[q * 3 + 1] * Nc[1] + R[q * 3 + 2] * Nc[2];
 }
 
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256)
-    k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
-                   P* __restrict__ temp, const double* __restrict__ seeds, const Geom g,
-                   const DendK<typename Stor<S>::T> k) {
+// One loop of a dendrite cell: the phase-field lattice, then the thermal
+// (SOL = false) or solutal (SOL = true) lattice.  `seeds` is the grain table
+// of the cell's domain.
+template <class S, class P, int PARITY, bool SOL, class NB>
+__device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
+                                          const P* __restrict__ phi_old, P* __restrict__ temp,
+                                          const double* __restrict__ seeds, const int64_t stride, const NB& nb,
+                                          const int c, const int x, const int y, const int z,
+                                          const DendK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const Nbr nb(g, x, y, z);
-  const int c = nb.idx(0, 0, 0);
   const T ph = T(phi_new[c]);
   T gx = T(0), gy = T(0), gz = T(0);
 #pragma unroll
   for (int i = 1; i < 19; ++i) {
-    const T fn = nb.fluid(ex(i), ey(i), ez(i)) ? T(__ldg(phi_new + nb.idx(ex(i), ey(i), ez(i)))) : ph;
+    const T fn = nb_fluid(nb, ex(i), ey(i), ez(i)) ? T(__ldg(phi_new + nb_idx(nb, ex(i), ey(i), ez(i)))) : ph;
     const T w = T(wq<19>(i));
     if (ex(i)) gx += (w * T(ex(i))) * fn;
     if (ey(i)) gy += (w * T(ey(i))) * fn;
@@ -427,31 +426,79 @@ __global__ void __launch_bounds__(256)
   // phase-field lattice, all seven loaded before any store (in-place safety)
   T gv[7];
 #pragma unroll
-  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, g.stride, nb, PARITY, c, i);
+  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, stride, nb, PARITY, c, i);
   const T dph = ph - k.ref_g;
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
     const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
     const T go = gv[i] - k.om_g * (gv[i] - w * dph) + fo * w * eB + w * src;
-    st_out<S, 7>(G, g.stride, nb, PARITY, c, i, go);
+    st_out<S, 7>(G, stride, nb, PARITY, c, i, go);
   }
-  // thermal lattice: relaxation with latent heat (1/2) dphi
   T t[7];
   T dT = T(0);
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
-    t[i] = ld_in<S, 7>(Tp, g.stride, nb, PARITY, c, i);
+    t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
     dT += t[i];
   }
-  const T lat = T(0.5) * dphi;
+  if constexpr (SOL) {
+    // solutal lattice (TRT): capacity c(phi) applied to D(phi), the
+    // anti-trapping current (first moment of the equilibrium) and the
+    // rejection source; pair sums relax to equilibrium with rate 1, pair
+    // differences with omega(phi)
+    const T U = k.ref_t + dT;
+    const T km = T(1) - k.k_part;
+    const T cap = (T(1) + k.k_part - km * ph) * T(0.5);
+    const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+    const T fj = -k.at_w0 * (T(1) + km * U) * dphi / ((gn + T(1e-6)) * cap);
+    const T D = (k.D_l * (T(1) - ph) * T(0.5) + k.D_s * (T(1) + ph) * T(0.5)) / cap;
+    const T om = T(1) / (T(4) * D + T(0.5));
+    const T su = T(0.5) * (T(1) + km * U) * dphi / cap;
+    {
+      const T w0 = T(wq<7>(0));
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
+    }
 #pragma unroll
-  for (int i = 0; i < 7; ++i) {
-    const T w = T(wq<7>(i));
-    const T to = t[i] - k.om_t * (t[i] - w * dT) + w * lat;
-    st_out<S, 7>(Tp, g.stride, nb, PARITY, c, i, to);
+    for (int i = 1; i < 7; i += 2) {
+      const int j = i + 1;
+      const T w = T(wq<7>(i));
+      const T ej = fj * (T(ex(i)) * gr[0] + T(ey(i)) * gr[1] + T(ez(i)) * gr[2]);
+      const T sym = w * dT;
+      const T am = T(0.5) * (t[i] - t[j]);
+      const T am_new = am - om * (am - w * T(4) * ej);
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
+    }
+  } else {
+    // thermal lattice: relaxation with latent heat (1/2) dphi
+    const T lat = T(0.5) * dphi;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      const T w = T(wq<7>(i));
+      const T to = t[i] - k.om_t * (t[i] - w * dT) + w * lat;
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
+    }
   }
   temp[c] = P(k.ref_t + dT);
+}
+
+template <class S, class P, int PARITY, bool SOL>
+__global__ void __launch_bounds__(256)
+    k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
+                   P* __restrict__ temp, const double* __restrict__ seeds, const Geom g,
+                   const DendK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  if (fast_cell(g, x, y, z)) {
+    const Fast fa = make_fast(g, x, y, z);
+    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, seeds, g.stride, fa, fa.c, x, y, z, k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, seeds, g.stride, nb, nb.idx(0, 0, 0), x, y, z, k);
+  }
 }
 
 // ===================================================================== INIT
@@ -844,6 +891,10 @@ DendK<T> dend_coef(const mk_params& p, Refs r) {
   k.nobj = p.n_objects;
   k.ref_g = T(r.r0);
   k.ref_t = T(r.r1);
+  k.k_part = T(p.k_part);
+  k.D_l = T(p.D);
+  k.D_s = T(p.D_s);
+  k.at_w0 = T(p.at_coef * p.W0);
   return k;
 }
 
@@ -931,10 +982,18 @@ void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t*
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
   }
-  if (parity == 0)
-    k_dend_collide<S, P, 0><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
-  else
-    k_dend_collide<S, P, 1><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+  const bool sol = e.p.model == MK_MODEL_SOLUTAL_DENDRITE;
+  if (parity == 0) {
+    if (sol)
+      k_dend_collide<S, P, 0, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+    else
+      k_dend_collide<S, P, 0, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+  } else {
+    if (sol)
+      k_dend_collide<S, P, 1, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+    else
+      k_dend_collide<S, P, 1, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+  }
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
 

@@ -443,8 +443,57 @@ void thermal_dendrite_step(orc_state* s) {
           s->f_out[(int64_t)i * n + c] = gi - om_g * (gi - w * ph) + (1.0 - 0.5 * om_g) * w * eB / cs2 + w * src;
         }
       }
-  // 3. thermal propagate + relaxation with latent heat (1/2) dphi.
   propagate(s, 7, s->s_out, s->s_hlp);
+  if (p.model == MK_MODEL_SOLUTAL_DENDRITE) {
+    // 3'. solutal propagate + relaxation: variable diffusivity, anti-trapping
+    // current in the equilibrium's first moment, rejection and lagged capacity.
+    const double k = p.k_part;
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < s->nz; ++z)
+      for (int y = 0; y < s->ny; ++y)
+        for (int x = 0; x < s->nx; ++x) {
+          const int64_t c = cidx(s, x, y, z);
+          if (s->flag[c] != MK_FLAG_FLUID) continue;
+          double U = 0;
+          for (int i = 0; i < 7; ++i) U += s->s_hlp[(int64_t)i * n + c];
+          const double ph = s->phi[c];
+          const double dphi = ph - s->phi_prev[c];
+          double gr[3], lap;
+          grad_lap(
+              s, s->phi, x, y, z, [](double p0) { return p0; }, gr, &lap);
+          // capacity c(phi) applied by dividing the local diffusivity, the
+          // anti-trapping flux and the rejection source
+          const double cap = (1.0 + k - (1.0 - k) * ph) * 0.5;
+          const double gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+          // the current is linear in n, so its normal is regularised at 1e-6
+          // (not 1e-12) to keep rounding noise where grad phi vanishes out of it
+          const double f = -p.at_coef * p.W0 * (1.0 + (1.0 - k) * U) * dphi / ((gn + 1e-6) * cap);
+          const double jat[3] = {f * gr[0], f * gr[1], f * gr[2]};
+          const double D = (p.D * (1.0 - ph) * 0.5 + p.D_s * (1.0 + ph) * 0.5) / cap;
+          const double om = 1.0 / (4.0 * D + 0.5);
+          const double src = 0.5 * (1.0 + (1.0 - k) * U) * dphi / cap;
+          // TRT: the antisymmetric part relaxes with omega(phi) (sets D), the
+          // symmetric part with 1 (the rest population and the pair sums go
+          // straight to equilibrium, which keeps the lattice stable where
+          // D(phi) -> D_s makes omega approach 2).
+          double t[7];
+          for (int i = 0; i < 7; ++i) t[i] = s->s_hlp[(int64_t)i * n + c];
+          s->s_out[c] = weight(7, 0) * U + weight(7, 0) * src;
+          for (int i = 1; i < 7; i += 2) {
+            const int j = i + 1;
+            const double w = weight(7, i);
+            const double ej = E27[i][0] * jat[0] + E27[i][1] * jat[1] + E27[i][2] * jat[2];
+            const double sym = w * U;             // (t_i + t_j)/2 after relaxation with rate 1
+            const double am = 0.5 * (t[i] - t[j]);  // antisymmetric part
+            const double am_new = am - om * (am - w * 4.0 * ej);
+            s->s_out[(int64_t)i * n + c] = sym + am_new + w * src;
+            s->s_out[(int64_t)j * n + c] = sym - am_new + w * src;
+          }
+          s->temp[c] = U;
+        }
+    return;
+  }
+  // 3. thermal propagate + relaxation with latent heat (1/2) dphi.
   const double om_t = 1.0 / (4.0 * p.D + 0.5);
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < n; ++c) {
@@ -575,7 +624,8 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
         mp_step(s);
         break;
       case MK_MODEL_THERMAL_DENDRITE:
-        thermal_dendrite_step(s);
+      case MK_MODEL_SOLUTAL_DENDRITE:
+        thermal_dendrite_step(s);  // the second lattice follows p.model
         break;
       default:
         return;

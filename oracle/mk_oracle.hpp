@@ -68,7 +68,21 @@
 //   t* = t - omega_T (t - w u) + w (phi^n - phi^(n-1))/2
 //   The phase-field relaxation at loop n uses u from the previous thermal relaxation.
 //
-// SOLUTAL DENDRITE: see mk_oracle_solutal section of mk_oracle.cpp.
+// SOLUTAL DENDRITE (mkPhaseField::relaxation_anisotropy_solute(loops), mkPhaseField.h:48;
+// mkSolutalField::propagate/relaxation/ATcurrent, mkSolutalField.h:35-37,65; dilute
+// binary alloy of Karma, PRL 87 115701 (2001), phi = +1 solid, U supersaturation):
+//   tau0 a^2 dphi/dt = W0^2 div(a^2 grad phi + N) + phi - phi^3 - lam U (1-phi^2)^2
+//   c(phi) dU/dt = div(D(phi) grad U - j_at) + (1/2)(1 + (1-k)U) dphi/dt
+//   c(phi) = (1 + k - (1-k) phi)/2, D(phi) = D (1-phi)/2 + D_s (1+phi)/2,
+//   j_at = -at W0 (1 + (1-k)U) (dphi/dt) n,  at = 1/(2 sqrt 2) (<antiTrapping>)
+//   phase field: the thermal-dendrite g-lattice with u -> U.
+//   The capacity is applied locally: c dU/dt = div(...) + R is advanced as
+//   dU/dt = div((D/c) grad U - j_at/c) + R/c (the grad(1/c) cross terms, nonzero only
+//   inside the interface, are dropped).  U-lattice (D3Q7), TRT: pair sums relax to
+//   equilibrium with rate 1, pair differences with omega(phi) = 1/(4 D(phi)/c(phi) + 1/2):
+//   t0* = w0 U + w0 S,  t_i,j* = w U +- [a - omega (a - w 4 e_i.j_at/c)] + w S,
+//   a = (t_i - t_j)/2,  S = (1/2)(1 + (1-k)U) dphi / c(phi),
+//   U = sum t (post-stream), phi, dphi of this loop, n = grad phi/(|grad phi| + 1e-6).
 // ---------------------------------------------------------------------------
 #ifndef MK_ORACLE_HPP
 #define MK_ORACLE_HPP

@@ -203,3 +203,31 @@ def test_diagnostics_conservation_fp64(casedir):
     assert abs(d1["phi_sum"] - d0["phi_sum"]) / d0["phi_sum"] < 1e-12
     assert d1["n_bad"] == 0
     assert 0.0 < d1["solid_frac"] < 0.5
+
+
+def _sol_case(precision="fp64", n=24, **kw):
+    return cases.solutal_dendrite(n=n, loops=10, precision=precision,
+                                  seeds=[((11.3, 12.1, 10.7), (10.0, 20.0, 30.0), 4.0),
+                                         ((4.0, 5.0, 17.0), (0.0, 45.0, 0.0), 2.5)], **kw)
+
+
+SOL_FIELDS = ["phi", "C", "dphi"]
+
+
+def test_solutal_fp64_steps(casedir):
+    p, s, o = _pair(casedir, "sol64", _sol_case())
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, SOL_FIELDS, FP64_TOL)
+    s.advance(150)
+    o.advance(150)
+    _compare(s, o, SOL_FIELDS, FP64_TOL)
+    assert np.array_equal(s.field("grain"), o.field("grain"))
+
+
+def test_solutal_fp32(casedir):
+    p, s, o = _pair(casedir, "sol32", _sol_case("fp32"))
+    s.advance(150)
+    o.advance(150)
+    _compare(s, o, ["phi", "C"], 1e-5)

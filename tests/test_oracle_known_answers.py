@@ -146,3 +146,43 @@ def test_thermal_dendrite_enthalpy_conserved(casedir):
     h0 = H()
     o.advance(150)
     assert abs(H() - h0) / abs(h0) < 1e-12
+
+
+def test_solutal_no_seed_is_pure_diffusion(casedir):
+    # No seed: phi = -1 (liquid, capacity 1, D = D_l), so U diffuses with
+    # variance growth 2 D_l per step and the total is conserved.
+    n = 40
+    p = _params(casedir, "sol_diff", cases.solutal_dendrite(n=n, loops=1, D=0.1, delta=0.0))
+    p.n_objects = 0
+    c = (n - 1) / 2
+    zz, yy, xx = np.meshgrid(*(np.arange(n, dtype=np.float64),) * 3, indexing="ij")
+    U0 = 1e-3 * np.exp(-((xx - c) ** 2 + (yy - c) ** 2 + (zz - c) ** 2) / (2 * 2.0 ** 2))
+    o = Oracle(p, phi=-np.ones_like(U0), Cc=U0)
+
+    def var_x(U):
+        return float(((xx - c) ** 2 * U).sum() / U.sum())
+
+    o.advance(20)
+    v1, s1 = var_x(o.field("C")), o.field("C").sum()
+    o.advance(40)
+    v2, s2 = var_x(o.field("C")), o.field("C").sum()
+    assert abs((v2 - v1) / 40 - 2 * p.D) / (2 * p.D) < 2e-3
+    assert abs(s2 - s1) / abs(s1) < 1e-12
+
+
+def test_solutal_seed_grows_rejects_solute_symmetrically(casedir):
+    # seed centred between cells: no cell sits where grad phi vanishes
+    n = 24
+    p = _params(casedir, "sol_seed", cases.solutal_dendrite(n=n, loops=1, seeds=[((11.5, 11.5, 11.5), (0, 0, 0),
+                                                                                    4.0)]))
+    o = Oracle(p, phi=initial_field(p, "phi"))
+    U0 = o.field("C").copy()
+    o.advance(150)
+    phi, U = o.field("phi"), o.field("C")
+    assert (phi > 0).sum() > (initial_field(p, "phi") > 0).sum()
+    # solute is rejected into the liquid ahead of the interface: U rises above the far field there
+    liquid = phi < -0.5
+    assert U[liquid].max() > U0.max() + 1e-3
+    assert np.max(np.abs(phi - phi.transpose(0, 2, 1))) < 1e-12
+    assert np.max(np.abs(phi - phi.transpose(2, 1, 0))) < 1e-12
+    assert np.max(np.abs(U - U.transpose(2, 1, 0))) < 1e-12
