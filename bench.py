@@ -1,10 +1,16 @@
 #!/usr/bin/env python3
 """Benchmark of the coupled LBM / phase-field step on B200.
 
-Workload: the two-phase Allen-Cahn bubble case at 256^3 (D3Q19 MRT
-pressure/velocity lattice + D3Q19 conservative Allen-Cahn lattice, 24 seeded
-bubbles, periodic x/y, walls in z).  A "step" is one loop of the coupled step
-over the whole domain.  MLUPS = lattice cells x steps / s / 1e6.
+Workloads (--workload)
+  bubbles   (default, the headline) the two-phase Allen-Cahn bubble case at
+            256^3 (D3Q19 MRT pressure/velocity lattice + D3Q19 conservative
+            Allen-Cahn lattice, 24 seeded bubbles, periodic x/y, walls in z)
+  dendrite  thermal dendrite at 128^3 (anisotropic phase field + D3Q7
+            thermal lattice, one centred seed)
+  ensemble  48 seeded solutal dendrite domains (edges 48-128) packed into
+            one lattice, BF16 storage, persistent launches + CUDA graph
+A "step" is one loop of the coupled step over every cell of the workload.
+MLUPS = lattice cells x steps / s / 1e6.
 
 Arms
   default           the sm_100a library (libmkb200.so) through its C ABI
@@ -33,7 +39,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS, %HBM roofline: LBM+phase-field 256^3, FP16-store vs FP32 plain"
-WORKLOAD = "multiphase Allen-Cahn bubbles 256^3, D3Q19 MRT + D3Q19 AC, 24 bubbles, seed 0xB200"
+WORKLOADS = {
+    "bubbles": {"workload": "multiphase Allen-Cahn bubbles {n}^3, D3Q19 MRT + D3Q19 AC, 24 bubbles, seed 0xB200",
+                "metric": METRIC, "size": 256, "precision": "fp32", "kernel": "k_mp_collide", "collision": "MRT(g) + BGK(h)",
+                "data": "synthetic (seeded bubble case, splitmix64 seed 0xB200)"},
+    "dendrite": {"workload": "thermal dendrite {n}^3, anisotropic phase field (D3Q7) + D3Q7 thermal, one seed",
+                 "metric": "MLUPS, %HBM roofline: thermal dendrite 128^3 (phase field + D3Q7 thermal)",
+                 "size": 128, "precision": "fp32", "kernel": "k_dend_collide", "collision": "BGK(g) + BGK(T)",
+                 "data": "synthetic (centred seed, eps4 0.05, undercooling 0.55)"},
+    "ensemble": {"workload": "solutal dendrite ensemble: 48 domains, edges 48-128, 1-6 seeds each, seed 0xE45E",
+                 "metric": "MLUPS aggregate, %HBM roofline: 48-domain solutal dendrite ensemble, BF16, "
+                           "persistent + graph",
+                 "size": 0, "precision": "bf16", "kernel": "k_ens_collide", "collision": "BGK(g) + TRT(U)",
+                 "data": "synthetic (splitmix64 ensemble generator, seed 0xE45E)"},
+}
+ENSEMBLE_SEED = 0xE45E
+ENSEMBLE_DOMAINS = 48
 
 
 def _measured_peak():
@@ -123,11 +144,30 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def _case_path(precision: str, n: int) -> str:
+def _case_path(precision: str, n: int, workload: str = "bubbles") -> str:
     from materkit_anisotropiclbm_trt_rbc_facet_b200 import cases
     d = os.path.join(tempfile.gettempdir(), "mkb200_bench")
-    return cases.write(cases.multiphase_bubbles(n=n, precision=precision, loops=10000),
-                       os.path.join(d, f"bubbles_{n}_{precision}.xml"))
+    if workload == "dendrite":
+        text = cases.thermal_dendrite(n=n, precision=precision, loops=5000)
+    else:
+        text = cases.multiphase_bubbles(n=n, precision=precision, loops=10000)
+    return cases.write(text, os.path.join(d, f"{workload}_{n}_{precision}.xml"))
+
+
+def _collide_bytes(workload: str, prec: str, cells: int) -> int:
+    """Algorithmic DRAM bytes of one launch of the dominant kernel.
+
+    bubbles:  g and h (19 + 19 populations) read and written, phi read once,
+              plus the FP32 Allen-Cahn rest population (read + write) with
+              16-bit storage.
+    dendrite / ensemble: phase-field and T/U lattices (7 + 7) read and
+              written, phi(t+1) and phi(t) read, T/U read and written.
+    """
+    S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
+    P = 8 if prec == "fp64" else 4
+    if workload == "bubbles":
+        return cells * (2 * 38 * S + P + (4 if S == 2 else 0))
+    return cells * (28 * S + 4 * P)
 
 
 def _dist():
@@ -168,6 +208,7 @@ def run_ours(args):
         return float(t.item())
 
     n = args.size
+    wl = WORKLOADS[args.workload]
     K, W = args.steps, args.warmup
     results = {}
     prec_list = [args.precision] + [p for p in ("fp32", "fp16", "bf16") if p != args.precision]
@@ -176,7 +217,7 @@ def run_ours(args):
     peak, peak_kind = _measured_peak()
     main = None
     for prec in prec_list:
-        params = case_params(_case_path(prec, n))
+        params = case_params(_case_path(prec, n, args.workload))
         s = Solver(params=params)
         tune = s.autotune(4)
         s.advance(W, graph=True)
@@ -195,10 +236,7 @@ def run_ours(args):
         fluid = s.fluid_cells()
         launches = min(K, 50)
         t_launch = prof["kernel_ms"] / launches * 1e-3
-        S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
-        phi_b = 8 if prec == "fp64" else 4
-        # 16-bit storage keeps the Allen-Cahn rest population in FP32 (+2 B each way)
-        collide_bytes = fluid * (2 * 38 * S + phi_b + (4 if S == 2 else 0))
+        collide_bytes = _collide_bytes(args.workload, prec, fluid)
         achieved = collide_bytes / t_launch / 1e9
         step_gbs = bpc * cells * K / (ms * 1e-3) / 1e9
         d = s.diagnostics(raise_on_divergence=False)
@@ -246,7 +284,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(n, budget_s=args.cpu_budget)
+        cpu = cpu_baseline(n, budget_s=args.cpu_budget, workload=args.workload)
 
     if pg is not None:
         pg.barrier()
@@ -254,10 +292,10 @@ def run_ours(args):
     if rank != 0:
         return
     traffic = _ncu_traffic()
-    tkey = f"collide_{args.precision}_bytes_per_cell"
+    tkey = f"{args.workload}_collide_{args.precision}_bytes_per_cell"
     traffic_launch = traffic[tkey] * params.ncell() if tkey in traffic else None
     line = {
-        "metric": METRIC,
+        "metric": wl["metric"],
         "value": round(r["mlups"], 1),
         "unit": "MLUPS",
         "n_gpus": ws,
@@ -268,13 +306,13 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded bubble case, splitmix64 seed 0xB200)",
-        "config": {"workload": WORKLOAD, "cells": params.ncell(), "storage": args.precision,
-                   "collision": "MRT(g) + BGK(h)", "streaming": "AA in place",
+        "data": wl["data"],
+        "config": {"workload": wl["workload"].format(n=n), "cells": params.ncell(), "storage": args.precision,
+                   "collision": wl["collision"], "streaming": "AA in place",
                    "l2": "inputs larger than L2 (%.2f GB resident populations)" % (
                        r["bytes_per_cell"] * params.ncell() / 2 / 1e9),
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
-        "roofline": {"bound": "hbm", "kernel": "k_mp_collide", "achieved": round(r["collide_gbs"], 1),
+        "roofline": {"bound": "hbm", "kernel": wl["kernel"], "achieved": round(r["collide_gbs"], 1),
                      "peak": peak, "unit": "GB/s", "frac": round(r["collide_frac"], 4),
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": r["collide_bytes_per_launch"],
@@ -299,16 +337,162 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(n: int, budget_s: float = 20.0):
+def run_ensemble(args):
+    """The packed solutal dendrite ensemble: every rank runs the whole ensemble
+    (replicas; the domains are independent, so a multi-GPU job would give each
+    rank its own ensemble seed)."""
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import Ensemble, ensemble_params
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
+
+    ws, rank, local = _dist()
+    lib = A.load()
+    st = lib.mk_set_device(local)
+    if st != A.MK_OK:
+        raise A.MkError(st, lib.mk_last_global_error().decode())
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    wl = WORKLOADS["ensemble"]
+    K, W = args.steps, args.warmup
+    nd = args.domains
+    peak, peak_kind = _measured_peak()
+    prec_list = [args.precision] + [p for p in ("bf16", "fp16", "fp32") if p != args.precision]
+    if args.no_variants:
+        prec_list = prec_list[:1]
+    results = {}
+    for prec in prec_list:
+        ps = ensemble_params(ENSEMBLE_SEED + rank, nd, prec)
+        e = Ensemble(ps)
+        e.advance(W)
+        if pg is not None:
+            pg.barrier()
+        clk = Clocks(local)
+        l0 = e.launches
+        with clk:
+            ms = e.time_advance(K)
+        launches = e.launches - l0
+        ms = max_over_ranks(ms)
+        cells = e.cells
+        nprof = min(K, 50)
+        prof = e.profile(nprof, "collide")
+        prof_phi = e.profile(nprof, "phi")
+        t_launch = prof["kernel_ms"] / nprof * 1e-3
+        cb = _collide_bytes("ensemble", prec, cells)
+        S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
+        P = 8 if prec == "fp64" else 4
+        step_bytes = cells * (35 * S + 5 * P)
+        bad = 0
+        for d in range(nd):
+            bad += int((~np.isfinite(e.field(d, "phi", np.float32))).sum())
+        results[prec] = {"mlups": cells * K * ws / (ms * 1e-3) / 1e6, "ms_per_step": ms / K, "cells": cells,
+                         "collide_ms": prof["kernel_ms"] / nprof, "phi_ms": prof_phi["kernel_ms"] / nprof,
+                         "collide_gbs": cb / t_launch / 1e9, "collide_frac": cb / t_launch / 1e9 / peak,
+                         "collide_bytes_per_launch": cb, "step_bytes_per_cell": step_bytes / cells,
+                         "step_gbs": step_bytes * K / (ms * 1e-3) / 1e9, "clocks": clk.summary(),
+                         "launches": launches, "n_bad": bad}
+        results[prec]["step_frac"] = results[prec]["step_gbs"] / peak
+        e.close()
+    r = results[args.precision]
+
+    # end to end through the C ABI: host parameters -> packed device state
+    # (initial fields uploaded), K loops, phi of every domain back to the host
+    ps = ensemble_params(ENSEMBLE_SEED + rank, nd, args.precision)
+    cells = sum(p.ncell() for p in ps)
+    if pg is not None:
+        pg.barrier()
+    t0 = time.perf_counter()
+    e = Ensemble(ps)
+    e.advance(K)
+    phis = [e.field(d, "phi", np.float32) for d in range(nd)]
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    phi_ok = all(bool(np.isfinite(x).all()) for x in phis)
+    e.close()
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(0, budget_s=args.cpu_budget, workload="ensemble")
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    traffic = _ncu_traffic()
+    tkey = f"ensemble_collide_{args.precision}_bytes_per_cell"
+    line = {
+        "metric": wl["metric"], "value": round(r["mlups"], 1), "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": round(r["ms_per_step"], 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32"}.get(args.precision, "f32"),
+        "data": wl["data"],
+        "config": {"workload": wl["workload"], "domains": nd, "cells": r["cells"], "storage": args.precision,
+                   "collision": wl["collision"], "streaming": "AA in place",
+                   "l2": "inputs larger than L2 (%.2f GB resident state)" % (
+                       r["step_bytes_per_cell"] * r["cells"] / 2 / 1e9),
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+        "roofline": {"bound": "hbm", "kernel": wl["kernel"], "achieved": round(r["collide_gbs"], 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(r["collide_frac"], 4), "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": r["collide_bytes_per_launch"],
+                     "traffic": traffic[tkey] * r["cells"] if tkey in traffic else None,
+                     "step_bytes_per_cell": r["step_bytes_per_cell"], "step_gbs": round(r["step_gbs"], 1),
+                     "step_frac": round(r["step_frac"], 4)},
+        "variants": {k: {"mlups": round(v["mlups"], 1), "ms_per_step": round(v["ms_per_step"], 4),
+                         "collide_ms": round(v["collide_ms"], 4), "phi_ms": round(v["phi_ms"], 4),
+                         "collide_frac": round(v["collide_frac"], 4), "step_frac": round(v["step_frac"], 4),
+                         "n_bad": v["n_bad"]} for k, v in results.items()},
+        "e2e": {"value": round(cells * K * ws / e2e_s / 1e6, 1), "unit": "MLUPS",
+                "h2d_bytes_per_step": cells * 16 / K, "d2h_bytes_per_step": cells * 4 / K,
+                "seconds": round(e2e_s, 4), "phi_finite": phi_ok,
+                "path": "mk_ensemble_create (host initial fields, FP64) + mk_ensemble_advance + "
+                        "mk_ensemble_get_field f32 per domain"},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _oracle_case(workload: str, n: int):
+    """FP64 parameters and initial fields of the workload's CPU sample (the
+    ensemble's sample is its first domain)."""
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import case_params, ensemble_params, initial_field
+    if workload == "ensemble":
+        params = ensemble_params(ENSEMBLE_SEED, 1, "fp64")[0]
+    else:
+        params = case_params(_case_path("fp64", n, workload))
+    dend = workload != "bubbles"
+    fields = {"phi": initial_field(params, "phi")}
+    if dend:
+        fields["T"] = initial_field(params, "T")
+        fields["Cc"] = initial_field(params, "C")
+    return params, fields
+
+
+def _sample_name(workload: str, n: int) -> str:
+    if workload == "ensemble":
+        return "domain 0 of the ensemble"
+    return f"the {n}^3 case"
+
+
+def cpu_baseline(n: int, budget_s: float = 20.0, workload: str = "bubbles"):
     """Time the FP64 OpenMP oracle on the host cores on a bounded sample of the workload."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from _oracle import Oracle, load as load_oracle
-    from materkit_anisotropiclbm_trt_rbc_facet_b200 import case_params, initial_field
 
     lib = load_oracle()
-    params = case_params(_case_path("fp64", n))
-    phi = initial_field(params, "phi")
-    o = Oracle(params, phi=phi)
+    params, fields = _oracle_case(workload, n)
+    o = Oracle(params, **fields)
     t0 = time.perf_counter()
     o.advance(1)
     t1 = time.perf_counter() - t0
@@ -319,7 +503,8 @@ def cpu_baseline(n: int, budget_s: float = 20.0):
     o.close()
     cells = params.ncell()
     return {"value": round(cells * steps / dt / 1e6, 2), "unit": "MLUPS", "cores": int(lib.orc_get_threads()),
-            "kind": "port", "sample": f"{steps} loops of the {n}^3 case after 1 untimed loop (FP64 oracle)",
+            "kind": "port",
+            "sample": f"{steps} loops of {_sample_name(workload, n)} after 1 untimed loop (FP64 oracle)",
             "seconds": round(dt, 2)}
 
 
@@ -329,12 +514,12 @@ def run_reference(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from _oracle import Oracle, load as load_oracle
-    from materkit_anisotropiclbm_trt_rbc_facet_b200 import case_params, initial_field
 
     lib = load_oracle()
     n = args.size
-    params = case_params(_case_path("fp64", n))
-    o = Oracle(params, phi=initial_field(params, "phi"))
+    wl = WORKLOADS[args.workload]
+    params, fields = _oracle_case(args.workload, n)
+    o = Oracle(params, **fields)
     t0 = time.perf_counter()
     o.advance(1)  # one untimed warm-up loop
     t1 = time.perf_counter() - t0
@@ -348,13 +533,15 @@ def run_reference(args):
     mlups = cells * steps / dt / 1e6
     cores = int(lib.orc_get_threads())
     line = {
-        "metric": METRIC, "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws, "steps": steps, "warmup": 1,
+        "metric": wl["metric"], "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws, "steps": steps, "warmup": 1,
         "ms_per_step": round(dt / steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubble case, splitmix64 seed 0xB200)",
-        "config": {"workload": WORKLOAD, "cells": cells, "storage": "fp64", "parallelism": f"{cores} host threads"},
+        "vs_baseline": None, "dtype": "f64", "data": wl["data"],
+        "config": {"workload": wl["workload"].format(n=n), "cells": cells, "storage": "fp64",
+                   "parallelism": f"{cores} host threads"},
         "impl": "reference",
         "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": cores, "kind": "port",
-                         "sample": f"{steps} loops of the {n}^3 case (requested {args.steps}); the reference's own "
+                         "sample": f"{steps} loops of {_sample_name(args.workload, n)} (requested {args.steps}); "
+                                   f"the reference's own "
                                    f"solver is a closed Windows DLL, so this is the FP64 OpenMP restatement"},
         "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -367,8 +554,10 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "bf16", "fp64"])
-    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--workload", default="bubbles", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default=None, choices=["fp32", "fp16", "bf16", "fp64"])
+    ap.add_argument("--size", type=int, default=None)
+    ap.add_argument("--domains", type=int, default=ENSEMBLE_DOMAINS)
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
@@ -376,8 +565,15 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    wl = WORKLOADS[args.workload]
+    if args.precision is None:
+        args.precision = wl["precision"]
+    if args.size is None:
+        args.size = wl["size"]
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
     else:
         run_ours(args)
 

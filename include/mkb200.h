@@ -277,6 +277,35 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
 mk_status mk_host_alloc(size_t bytes, void** out);
 mk_status mk_host_free(void* p);
 
+/* ---- Ensembles: many dendrite domains advanced together ----------------
+ * Batches unevenly sized domains (seed, anisotropy and undercooling sweeps of
+ * run_solutal_dendrite / run_thermal_dendrite, MaterKit.cpp:633-687, 743-788)
+ * into one packed cell index: every loop is two persistent launches over all
+ * domains, and mk_ensemble_advance replays them as a CUDA graph.  All domains
+ * share the model and the storage precision; each cell count must be a
+ * multiple of 256. */
+typedef struct mk_ensemble mk_ensemble;
+
+/* Seeded generator of the solutal ensemble: n cubes with edges from
+ * {48, 64, 80, 96, 128}, eps4 ~ U[0.02, 0.06], 1-6 seeds of radius U[4, 8]
+ * with uniformly random orientations; k = 0.15, D_l = 0.1, D_s = 1e-4. */
+mk_status mk_ensemble_case_params(uint64_t seed, int32_t n_domains, int32_t precision, mk_params* out);
+mk_status mk_ensemble_create(const mk_params* params, int32_t n_domains, mk_ensemble** out);
+mk_status mk_ensemble_destroy(mk_ensemble* e);
+const char* mk_ensemble_last_error(const mk_ensemble* e);
+mk_status mk_ensemble_advance(mk_ensemble* e, int64_t nsteps);
+mk_status mk_ensemble_time_advance(mk_ensemble* e, int64_t nsteps, double* ms);
+mk_status mk_ensemble_get_field(mk_ensemble* e, int32_t domain, int32_t field, int32_t dtype, void* host_dst,
+                                size_t bytes);
+/* Device time of one of the two launches of a loop ("phi" or "collide"),
+ * summed over `nsteps` eager loops, and the total time of those loops. */
+mk_status mk_ensemble_profile_steps(mk_ensemble* e, int64_t nsteps, const char* kernel, double* kernel_ms,
+                                    double* step_ms);
+/* Kernel launches issued so far (two per loop). */
+int64_t mk_ensemble_launches(const mk_ensemble* e);
+int64_t mk_ensemble_cells(const mk_ensemble* e);
+int64_t mk_ensemble_step(const mk_ensemble* e);
+
 /* Allocation-free FP64 statistics of a device-resident FP32 field.
  * No counterpart in the reference (its solver has no device code); it is the
  * diagnostics reduction for callers that may not call cudaMalloc, such as a

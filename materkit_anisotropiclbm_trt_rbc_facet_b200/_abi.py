@@ -122,6 +122,17 @@ PROTOTYPES = {
     "mk_autotune": (C.c_int, [H, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_double)]),
     "mk_host_alloc": (C.c_int, [C.c_size_t, P(C.c_void_p)]),
     "mk_host_free": (C.c_int, [C.c_void_p]),
+    "mk_ensemble_case_params": (C.c_int, [C.c_uint64, C.c_int32, C.c_int32, P(MkParams)]),
+    "mk_ensemble_create": (C.c_int, [P(MkParams), C.c_int32, P(H)]),
+    "mk_ensemble_destroy": (C.c_int, [H]),
+    "mk_ensemble_last_error": (C.c_char_p, [H]),
+    "mk_ensemble_advance": (C.c_int, [H, C.c_int64]),
+    "mk_ensemble_time_advance": (C.c_int, [H, C.c_int64, P(C.c_double)]),
+    "mk_ensemble_get_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),
+    "mk_ensemble_profile_steps": (C.c_int, [H, C.c_int64, C.c_char_p, P(C.c_double), P(C.c_double)]),
+    "mk_ensemble_launches": (C.c_int64, [H]),
+    "mk_ensemble_cells": (C.c_int64, [H]),
+    "mk_ensemble_step": (C.c_int64, [H]),
     "mk_field_stats_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "mk_noalloc_last_error": (C.c_char_p, []),
     "mk_bytes_per_cell": (C.c_double, [H]),

@@ -70,6 +70,10 @@ mk_status copy_field(mk_handle* h, int field, std::vector<double>& out) {
 
 }  // namespace
 
+namespace mke {
+void set_global_error(const std::string& m) { g_err = m; }
+}  // namespace mke
+
 extern "C" {
 
 int32_t mk_abi_version(void) { return MKB200_ABI_VERSION; }

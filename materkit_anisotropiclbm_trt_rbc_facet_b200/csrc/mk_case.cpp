@@ -631,6 +631,54 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
   return MK_OK;
 }
 
+mk_status ensemble_case(unsigned long long seed, int n, int precision, mk_params* out, std::string& err) {
+  if (n < 1 || n > 4096) {
+    err = "ensemble size out of range";
+    return MK_ERR_ARG;
+  }
+  SplitMix64 rng(seed);
+  const int edges[5] = {48, 64, 80, 96, 128};
+  for (int d = 0; d < n; ++d) {
+    mk_params p;
+    default_params(&p);
+    p.model = MK_MODEL_SOLUTAL_DENDRITE;
+    p.precision = precision;
+    const int L = edges[rng.next() % 5];
+    p.nx = p.ny = p.nz = L;
+    p.bc[0] = p.bc[1] = p.bc[2] = MK_BC_CLOSED;
+    p.max_loops = 3000;
+    p.eps4 = 0.02 + 0.04 * rng.uniform();
+    p.k_part = 0.15;
+    p.D = 0.1;
+    p.D_s = 1e-4;
+    p.W0 = 1.5;
+    p.lambda = 10.0;
+    p.delta = 0.55;
+    p.tau0 = 0.6267 * p.lambda * p.W0 * p.W0 / p.D;
+    p.n_objects = 1 + (int)(rng.next() % 6);
+    for (int s = 0; s < p.n_objects; ++s) {
+      const double R = 4.0 + 4.0 * rng.uniform();
+      for (int a = 0; a < 3; ++a) p.obj_center[s][a] = (R + 2.0) + (L - 1 - 2.0 * (R + 2.0)) * rng.uniform();
+      p.obj_radius[s] = R;
+      // uniformly random orientation (Shoemake's uniform quaternion) as ZYX angles
+      const double u1 = rng.uniform(), u2 = rng.uniform(), u3 = rng.uniform();
+      const double qx = std::sqrt(1 - u1) * std::sin(2 * M_PI * u2), qy = std::sqrt(1 - u1) * std::cos(2 * M_PI * u2);
+      const double qz = std::sqrt(u1) * std::sin(2 * M_PI * u3), qw = std::sqrt(u1) * std::cos(2 * M_PI * u3);
+      const double R00 = 1 - 2 * (qy * qy + qz * qz), R10 = 2 * (qx * qy + qz * qw), R20 = 2 * (qx * qz - qy * qw);
+      const double R21 = 2 * (qy * qz + qx * qw), R22 = 1 - 2 * (qx * qx + qy * qy);
+      const double r2d = 180.0 / M_PI;
+      p.obj_angle[s][0] = std::atan2(R21, R22) * r2d;
+      p.obj_angle[s][1] = -std::asin(std::max(-1.0, std::min(1.0, R20))) * r2d;
+      p.obj_angle[s][2] = std::atan2(R10, R00) * r2d;
+    }
+    p.rng_seed = seed;
+    mk_status st = validate_params(&p, err);
+    if (st != MK_OK) return st;
+    out[d] = p;
+  }
+  return MK_OK;
+}
+
 unsigned long long params_hash(const mk_params* p) {
   // FNV-1a over the bytes of the parameter block (precision excluded so a
   // checkpoint can be restored at another storage precision).

@@ -53,6 +53,9 @@ inline bool is_fluid(const mk_params* p, int x, int y, int z) {
   return true;
 }
 
+// Seeded solutal ensemble (config 4): n domain parameter sets.
+mk_status ensemble_case(unsigned long long seed, int n, int precision, mk_params* out, std::string& err);
+
 // A stable hash of the parameters (checkpoint compatibility).
 unsigned long long params_hash(const mk_params* p);
 

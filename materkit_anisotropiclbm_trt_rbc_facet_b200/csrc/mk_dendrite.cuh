@@ -1,0 +1,242 @@
+// mk_dendrite.cuh — phase-field + thermal / solutal cell update of one loop,
+// shared by the single-domain kernels (mk_kernels.cu) and the packed
+// multi-domain ensemble (mk_ensemble.cu).
+#ifndef MK_DENDRITE_CUH
+#define MK_DENDRITE_CUH
+
+#include "mk_device.cuh"
+#include "../../include/mkb200.h"
+
+namespace mkd {
+
+// ========================================================== DENDRITE (K2/K3)
+// Both D3Q7 lattices are held as deviations from the far-field liquid:
+// g_i - w_i ref_g (ref_g = -1) and t_i - w_i ref_t (ref_t = -Delta).
+template <class T>
+struct DendK {
+  T om_g, om_t, inv_tau0, lambda, eps4;
+  int nobj;
+  T ref_g, ref_t;
+  T k_part, D_l, D_s, at_w0;  // solutal lattice
+};
+
+// phi of a streamed cell: the sum of its seven phase-field populations.
+template <class S, class P, int PARITY, class NB>
+__device__ __forceinline__ void pf_phi_cell(const S* __restrict__ G, P* __restrict__ phi_new, const int64_t stride,
+                                            const NB& nb, const int c, const typename Stor<S>::T ref_g) {
+  typedef typename Stor<S>::T T;
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, stride, nb, PARITY, c, i);
+  phi_new[c] = P(ref_g + s);
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P* __restrict__ phi_old,
+                                                P* __restrict__ phi_new, const Geom g, typename Stor<S>::T ref_g) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  if (!g.fluid(x, y, z)) {
+    const int64_t c = g.idx(x, y, z);
+    phi_new[c] = phi_old[c];
+    return;
+  }
+  if (fastw_cell(g, x, y, z)) {
+    const FastW fa = make_fastw(g, x, y, z);
+    pf_phi_cell<S, P, PARITY>(G, phi_new, g.stride, fa, fa.c, ref_g);
+  } else {
+    const Nbr nb(g, x, y, z);
+    pf_phi_cell<S, P, PARITY>(G, phi_new, g.stride, nb, nb.idx(0, 0, 0), ref_g);
+  }
+}
+
+// Nearest seed (ties to the lower index), in FP64 like the oracle.
+__device__ __forceinline__ int nearest_seed(const double* __restrict__ seeds, int nobj, int x, int y, int z) {
+  int best = 0;
+  double bd = 1e300;
+  for (int k = 0; k < nobj; ++k) {
+    const double dx = x - __ldg(seeds + 12 * k + 0), dy = y - __ldg(seeds + 12 * k + 1),
+                 dz = z - __ldg(seeds + 12 * k + 2);
+    const double d = dx * dx + dy * dy + dz * dz;
+    if (d < bd) {
+      bd = d;
+      best = k;
+    }
+  }
+  return best;
+}
+
+// a(n) and the lab-frame anisotropy vector N of Karma-Rappel 4-fold
+// anisotropy (mkPhaseField::anisotropy, mkPhaseField.h:61).
+// `Rm` is the grain's rotation (row-major, columns = crystal axes) in the
+// arithmetic type.
+template <class T>
+__device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, T eps4, const T (&gr)[3], T& a, T (&N)[3]) {
+  T R[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) R[q] = __ldg(Rm + q);
+  const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+  const T inv = T(1) / (gn + T(1e-12));
+  const T nl0 = gr[0] * inv, nl1 = gr[1] * inv, nl2 = gr[2] * inv;
+  T nc[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) nc[q] = R[0 * 3 + q] * nl0 + R[1 * 3 + q] * nl1 + R[2 * 3 + q] * nl2;
+  const T s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
+  a = T(1) - T(3) * eps4 + T(4) * eps4 * s4;
+  T Nc[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) Nc[q] = gn * a * T(16) * eps4 * (nc[q] * nc[q] * nc[q] - nc[q] * s4);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) N[q] = R[q * 3 + 0] * Nc[0] + R[q * 3 + 1] * Nc[1] + R[q * 3 + 2] * Nc[2];
+}
+
+// One loop of a dendrite cell: the phase-field lattice, then the thermal
+// (SOL = false) or solutal (SOL = true) lattice.  `grain` is the per-cell
+// grain index (read only with more than one grain), `rot` the rotations of
+// the cell's domain, 9 values per grain.
+template <class S, class P, int PARITY, bool SOL, class NB>
+__device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
+                                          const P* __restrict__ phi_old, P* __restrict__ temp,
+                                          const unsigned char* __restrict__ grain,
+                                          const typename Stor<S>::T* __restrict__ rot, const int64_t stride,
+                                          const NB& nb, const int c, const DendK<typename Stor<S>::T>& k) {
+  typedef typename Stor<S>::T T;
+  const T ph = T(phi_new[c]);
+  T gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll
+  for (int i = 1; i < 19; ++i) {
+    const T fn = nb_fluid(nb, ex(i), ey(i), ez(i)) ? T(__ldg(phi_new + nb_idx(nb, ex(i), ey(i), ez(i)))) : ph;
+    const T w = T(wq<19>(i));
+    if (ex(i)) gx += (w * T(ex(i))) * fn;
+    if (ey(i)) gy += (w * T(ey(i))) * fn;
+    if (ez(i)) gz += (w * T(ez(i))) * fn;
+  }
+  const T gr[3] = {T(3) * gx, T(3) * gy, T(3) * gz};
+  const int gid = k.nobj > 1 ? (int)__ldg(grain + c) : 0;
+  T a, N[3];
+  anisotropy<T>(rot + 9 * gid, k.eps4, gr, a, N);
+  const T dphi = ph - T(phi_old[c]);
+  const T u_old = T(temp[c]);
+  const T one_m = T(1) - ph * ph;
+  const T src = (ph - ph * ph * ph - k.lambda * u_old * one_m * one_m) * k.inv_tau0 + (T(1) - a * a) * dphi;
+  const T cs2 = T(0.25);
+  const T B0 = -cs2 * ((a * a - T(1)) * gr[0] + N[0]);
+  const T B1 = -cs2 * ((a * a - T(1)) * gr[1] + N[1]);
+  const T B2 = -cs2 * ((a * a - T(1)) * gr[2] + N[2]);
+  const T fo = (T(1) - T(0.5) * k.om_g) / cs2;
+  // phase-field lattice, all seven loaded before any store (in-place safety)
+  T gv[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, stride, nb, PARITY, c, i);
+  const T dph = ph - k.ref_g;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    const T w = T(wq<7>(i));
+    const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
+    const T go = gv[i] - k.om_g * (gv[i] - w * dph) + fo * w * eB + w * src;
+    st_out<S, 7>(G, stride, nb, PARITY, c, i, go);
+  }
+  T t[7];
+  T dT = T(0);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
+    dT += t[i];
+  }
+  if constexpr (SOL) {
+    // solutal lattice (TRT): capacity c(phi) applied to D(phi), the
+    // anti-trapping current (first moment of the equilibrium) and the
+    // rejection source; pair sums relax to equilibrium with rate 1, pair
+    // differences with omega(phi)
+    const T U = k.ref_t + dT;
+    const T km = T(1) - k.k_part;
+    const T cap = (T(1) + k.k_part - km * ph) * T(0.5);
+    const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+    const T fj = -k.at_w0 * (T(1) + km * U) * dphi / ((gn + T(1e-6)) * cap);
+    const T D = (k.D_l * (T(1) - ph) * T(0.5) + k.D_s * (T(1) + ph) * T(0.5)) / cap;
+    const T om = T(1) / (T(4) * D + T(0.5));
+    const T su = T(0.5) * (T(1) + km * U) * dphi / cap;
+    {
+      const T w0 = T(wq<7>(0));
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
+    }
+#pragma unroll
+    for (int i = 1; i < 7; i += 2) {
+      const int j = i + 1;
+      const T w = T(wq<7>(i));
+      const T ej = fj * (T(ex(i)) * gr[0] + T(ey(i)) * gr[1] + T(ez(i)) * gr[2]);
+      const T sym = w * dT;
+      const T am = T(0.5) * (t[i] - t[j]);
+      const T am_new = am - om * (am - w * T(4) * ej);
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
+    }
+  } else {
+    // thermal lattice: relaxation with latent heat (1/2) dphi
+    const T lat = T(0.5) * dphi;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      const T w = T(wq<7>(i));
+      const T to = t[i] - k.om_t * (t[i] - w * dT) + w * lat;
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
+    }
+  }
+  temp[c] = P(k.ref_t + dT);
+}
+
+template <class S, class P, int PARITY, bool SOL>
+__global__ void __launch_bounds__(256)
+    k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
+                   P* __restrict__ temp, const unsigned char* __restrict__ grain,
+                   const typename Stor<S>::T* __restrict__ rot, const Geom g, const DendK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  if (fastw_cell(g, x, y, z)) {
+    const FastW fa = make_fastw(g, x, y, z);
+    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, fa.c, k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, nb.idx(0, 0, 0), k);
+  }
+}
+
+// Per-cell grain index: the nearest seed in FP64, ties to the lower index
+// (computed once; the seeds do not move).
+static __global__ void k_grain_map(const Geom g, const double* __restrict__ seeds, int nobj, int base,
+                            unsigned char* __restrict__ grain) {
+  const int n = g.nx * g.ny * g.nz;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int z = i / (g.nx * g.ny), r = i - z * g.nx * g.ny, y = r / g.nx, x = r - y * g.nx;
+    grain[base + i] = (unsigned char)(nobj > 1 ? nearest_seed(seeds, nobj, x, y, z) : 0);
+  }
+}
+
+
+// Kernel coefficients of a dendrite case (host side).
+template <class T>
+inline DendK<T> dend_params(const mk_params& p, double ref_g, double ref_t) {
+  DendK<T> k;
+  const double D0 = p.W0 * p.W0 / p.tau0;
+  k.om_g = T(1.0 / (4.0 * D0 + 0.5));
+  k.om_t = T(1.0 / (4.0 * p.D + 0.5));
+  k.inv_tau0 = T(1.0 / p.tau0);
+  k.lambda = T(p.lambda);
+  k.eps4 = T(p.eps4);
+  k.nobj = p.n_objects;
+  k.ref_g = T(ref_g);
+  k.ref_t = T(ref_t);
+  k.k_part = T(p.k_part);
+  k.D_l = T(p.D);
+  k.D_s = T(p.D_s);
+  k.at_w0 = T(p.at_coef * p.W0);
+  return k;
+}
+
+}  // namespace mkd
+
+#endif

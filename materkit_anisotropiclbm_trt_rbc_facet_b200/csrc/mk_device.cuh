@@ -439,6 +439,7 @@ struct Geom {
 struct Nbr {
   int ox[3], oy[3], oz[3];
   unsigned ok;
+  int base = 0;  // offset of the domain inside a packed multi-domain index
 
   __device__ __forceinline__ static void axis(int n, int bc, int c, int mul, int (&o)[3], bool (&v)[3]) {
 #pragma unroll
@@ -473,7 +474,9 @@ struct Nbr {
         for (int dx = 0; dx < 3; ++dx)
           if (vx[dx] && vy[dy] && vz[dz]) ok |= 1u << (dx + 3 * dy + 9 * dz);
   }
-  __device__ __forceinline__ int idx(int dx, int dy, int dz) const { return ox[dx + 1] + oy[dy + 1] + oz[dz + 1]; }
+  __device__ __forceinline__ int idx(int dx, int dy, int dz) const {
+    return base + ox[dx + 1] + oy[dy + 1] + oz[dz + 1];
+  }
   __device__ __forceinline__ bool fluid(int dx, int dy, int dz) const {
     return (ok >> ((dx + 1) + 3 * (dy + 1) + 9 * (dz + 1))) & 1u;
   }
@@ -508,6 +511,61 @@ __device__ __forceinline__ Fast make_fast(const Geom& g, int x, int y, int z) {
   f.xm = x == 0 ? g.nx - 1 : -1;
   f.xp = x == g.nx - 1 ? -(g.nx - 1) : 1;
   return f;
+}
+
+// Interior-row addressing for domains whose x faces are closed or walled:
+// as Fast, plus the validity of the two x neighbours, so the cells at the
+// ends of a row stay on the same code path as the rest of their warp (the
+// bounce-back select is emitted only for directions with ex != 0).
+struct FastW : Fast {
+  bool okm, okp;  // x-1 / x+1 neighbour is fluid
+};
+
+// Whether (x,y,z) may use FastW: y and z strictly inside the fluid span of
+// their axis (x is free).
+__device__ __forceinline__ bool fastw_cell(const Geom& g, int, int y, int z) {
+  auto inside = [](int c, int n, int bc) {
+    const int lo = bc == 1 ? 2 : 1;
+    const int hi = bc == 1 ? n - 3 : n - 2;
+    return c >= lo && c <= hi;
+  };
+  return inside(y, g.ny, g.bc1) && inside(z, g.nz, g.bc2);
+}
+
+__device__ __forceinline__ FastW make_fastw(const Geom& g, int x, int y, int z) {
+  FastW f;
+  f.nx = g.nx;
+  f.nxy = g.nx * g.ny;
+  f.c = x + g.nx * (y + g.ny * z);
+  if (g.bc0 == 0) {
+    f.xm = x == 0 ? g.nx - 1 : -1;
+    f.xp = x == g.nx - 1 ? -(g.nx - 1) : 1;
+    f.okm = f.okp = true;
+  } else {
+    const int lo = g.bc0 == 1 ? 1 : 0, hi = g.bc0 == 1 ? g.nx - 2 : g.nx - 1;
+    f.xm = -1;
+    f.xp = 1;
+    f.okm = x - 1 >= lo;
+    f.okp = x + 1 <= hi;
+  }
+  return f;
+}
+
+__device__ __forceinline__ bool fastw_fluid(const FastW& fa, int dx) { return dx < 0 ? fa.okm : (dx > 0 ? fa.okp : true); }
+
+template <int Q>
+__device__ __forceinline__ int64_t off_in(int64_t stride, const FastW& fa, int parity, int, int i) {
+  if (parity == 0) return (int64_t)i * stride + fa.c;
+  if (ex(i) == 0) return (int64_t)inv(i) * stride + fa.idx(-ex(i), -ey(i), -ez(i));
+  const bool f = fastw_fluid(fa, -ex(i));
+  return (int64_t)(f ? inv(i) : i) * stride + (f ? fa.idx(-ex(i), -ey(i), -ez(i)) : fa.c);
+}
+template <int Q>
+__device__ __forceinline__ int64_t off_out(int64_t stride, const FastW& fa, int parity, int, int i) {
+  if (parity == 0) return (int64_t)inv(i) * stride + fa.c;
+  if (ex(i) == 0) return (int64_t)i * stride + fa.idx(ex(i), ey(i), ez(i));
+  const bool f = fastw_fluid(fa, ex(i));
+  return (int64_t)(f ? i : inv(i)) * stride + (f ? fa.idx(ex(i), ey(i), ez(i)) : fa.c);
 }
 
 template <int Q>
@@ -568,6 +626,8 @@ __device__ __forceinline__ bool nb_fluid(const Nbr& nb, int dx, int dy, int dz) 
 __device__ __forceinline__ bool nb_fluid(const Fast&, int, int, int) { return true; }
 __device__ __forceinline__ int nb_idx(const Nbr& nb, int dx, int dy, int dz) { return nb.idx(dx, dy, dz); }
 __device__ __forceinline__ int nb_idx(const Fast& fa, int dx, int dy, int dz) { return fa.idx(dx, dy, dz); }
+__device__ __forceinline__ bool nb_fluid(const FastW& fa, int dx, int, int) { return fastw_fluid(fa, dx); }
+__device__ __forceinline__ int nb_idx(const FastW& fa, int dx, int dy, int dz) { return fa.idx(dx, dy, dz); }
 
 // Post-collision deviation f'_i of a cell in the layout left after
 // `steps_done` loops (field output, diagnostics): the slot the last loop
@@ -585,6 +645,33 @@ __device__ __forceinline__ void st_layout(S* __restrict__ A, int64_t stride, con
                                           int i, typename Stor<S>::T v) {
   Stor<S>::st(A + off_out<Q>(stride, nb, (int)((steps_done + 1) & 1), c, i), v, typename Stor<S>::T(wq<Q>(i)));
 }
+
+// Equilibrium placement of the initial state.
+// Stores the deviation of  f_i = base_scale w (1 + 3eu + 4.5eu^2 - 1.5u^2) + w p_extra
+// from w ref, placed as the post-collision state of loop 0.
+template <class S, int Q>
+__device__ __forceinline__ void put_eq(S* A, const Geom& g, const Nbr& nb, int c, double base_scale, double ux,
+                                       double uy, double uz, double p_extra, double ref) {
+  typedef typename Stor<S>::T T;
+  const double uu = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const double w = wq<Q>(i);
+    const double eu = ex(i) * ux + ey(i) * uy + ez(i) * uz;
+    const double v = w * ((base_scale - ref + p_extra) + base_scale * (3.0 * eu + 4.5 * eu * eu - 1.5 * uu));
+    st_layout<S, Q>(A, g.stride, nb, 0, c, i, T(v));
+  }
+}
+
+// Storage type of phi and the scalar fields: FP64 with FP64 populations, else FP32.
+template <class S>
+struct PhiOf {
+  typedef float type;
+};
+template <>
+struct PhiOf<double> {
+  typedef double type;
+};
 
 }  // namespace mkd
 

@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/mkb200.h"
 
@@ -49,6 +50,8 @@ struct Engine {
   void* phi[2];
   void* temp;
   double* seeds;      // n_objects * 12 doubles: centre (3), rotation (9, row-major, columns = crystal axes)
+  void* rot;          // the rotations alone in the arithmetic type (double for FP64, else float)
+  unsigned char* grain;  // per-cell nearest-seed index (dendrites with more than one seed), else null
   double* partial;    // diagnostics scratch, DG_N doubles per block
   int partial_blocks;
   double* dsum;       // DG_N doubles
@@ -58,6 +61,13 @@ struct Engine {
   // launch counters
   int64_t launches;
 };
+
+// Message returned by mk_last_global_error on this thread.
+void set_global_error(const std::string& m);
+
+// Grain table of a dendrite case: 12 doubles per object (centre, then the
+// row-major rotation whose columns are the crystal axes).
+void seed_table(const mk_params& p, std::vector<double>& sd);
 
 // Allocate and zero device buffers for p.  Returns cudaSuccess or an error.
 cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x, int block_y, std::string& err);

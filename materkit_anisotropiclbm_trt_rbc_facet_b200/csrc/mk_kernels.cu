@@ -16,6 +16,7 @@
 // All kernels are HBM-bound stencils: one thread per cell, x fastest, so a
 // warp touches 32 consecutive cells of every population plane.  No tensor
 // cores: the step is not a contraction.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -26,15 +27,6 @@
 using namespace mkd;
 
 namespace {
-
-template <class S>
-struct PhiOf {
-  typedef float type;
-};
-template <>
-struct PhiOf<double> {
-  typedef double type;
-};
 
 // Rest values of the two lattices: populations are held as f_i - w_i ref.
 struct Refs {
@@ -320,204 +312,13 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   }
 }
 
-// ========================================================== DENDRITE (K2/K3)
-// Both D3Q7 lattices are held as deviations from the far-field liquid:
-// g_i - w_i ref_g (ref_g = -1) and t_i - w_i ref_t (ref_t = -Delta).
-template <class T>
-struct DendK {
-  T om_g, om_t, inv_tau0, lambda, eps4;
-  int nobj;
-  T ref_g, ref_t;
-  T k_part, D_l, D_s, at_w0;  // solutal lattice
-};
+}  // namespace
 
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P* __restrict__ phi_old,
-                                                P* __restrict__ phi_new, const Geom g, typename Stor<S>::T ref_g) {
-  typedef typename Stor<S>::T T;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny) return;
-  if (!g.fluid(x, y, z)) {
-    const int64_t c = g.idx(x, y, z);
-    phi_new[c] = phi_old[c];
-    return;
-  }
-  const Nbr nb(g, x, y, z);
-  const int c = nb.idx(0, 0, 0);
-  T s = T(0);
-#pragma unroll
-  for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, g.stride, nb, PARITY, c, i);
-  phi_new[c] = P(ref_g + s);
-}
+#include "mk_dendrite.cuh"
 
-// Nearest seed (ties to the lower index), in FP64 like the oracle.
-__device__ __forceinline__ int nearest_seed(const double* __restrict__ seeds, int nobj, int x, int y, int z) {
-  int best = 0;
-  double bd = 1e300;
-  for (int k = 0; k < nobj; ++k) {
-    const double dx = x - __ldg(seeds + 12 * k + 0), dy = y - __ldg(seeds + 12 * k + 1),
-                 dz = z - __ldg(seeds + 12 * k + 2);
-    const double d = dx * dx + dy * dy + dz * dz;
-    if (d < bd) {
-      bd = d;
-      best = k;
-    }
-  }
-  return best;
-}
-
-// a(n) and the lab-frame anisotropy vector N of Karma-Rappel 4-fold
-// anisotropy (mkPhaseField::anisotropy, mkPhaseField.h:61).
-template <class T>
-__device__ __forceinline__ void anisotropy(const double* __restrict__ Rm, T eps4, const T (&gr)[3], T& a, T (&N)[3]) {
-  T R[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) R[q] = T(__ldg(Rm + q));
-  const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
-  const T inv = T(1) / (gn + T(1e-12));
-  const T nl0 = gr[0] * inv, nl1 = gr[1] * inv, nl2 = gr[2] * inv;
-  T nc[3];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) nc[q] = R[0 * 3 + q] * nl0 + R[1 * 3 + q] * nl1 + R[2 * 3 + q] * nl2;
-  const T s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
-  a = T(1) - T(3) * eps4 + T(4) * eps4 * s4;
-  T Nc[3];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) Nc[q] = gn * a * T(16) * eps4 * (nc[q] * nc[q] * nc[q] - nc[q] * s4);
-#pragma unroll
-  for (int q = 0; q < 3; ++q) N[q] = R[q * 3 + 0] * Nc[0] + R[q * 3 + 1] * Nc[1] + R[q * 3 + 2] * Nc[2];
-}
-
-// One loop of a dendrite cell: the phase-field lattice, then the thermal
-// (SOL = false) or solutal (SOL = true) lattice.  `seeds` is the grain table
-// of the cell's domain.
-template <class S, class P, int PARITY, bool SOL, class NB>
-__device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
-                                          const P* __restrict__ phi_old, P* __restrict__ temp,
-                                          const double* __restrict__ seeds, const int64_t stride, const NB& nb,
-                                          const int c, const int x, const int y, const int z,
-                                          const DendK<typename Stor<S>::T>& k) {
-  typedef typename Stor<S>::T T;
-  const T ph = T(phi_new[c]);
-  T gx = T(0), gy = T(0), gz = T(0);
-#pragma unroll
-  for (int i = 1; i < 19; ++i) {
-    const T fn = nb_fluid(nb, ex(i), ey(i), ez(i)) ? T(__ldg(phi_new + nb_idx(nb, ex(i), ey(i), ez(i)))) : ph;
-    const T w = T(wq<19>(i));
-    if (ex(i)) gx += (w * T(ex(i))) * fn;
-    if (ey(i)) gy += (w * T(ey(i))) * fn;
-    if (ez(i)) gz += (w * T(ez(i))) * fn;
-  }
-  const T gr[3] = {T(3) * gx, T(3) * gy, T(3) * gz};
-  const int gid = k.nobj > 1 ? nearest_seed(seeds, k.nobj, x, y, z) : 0;
-  T a, N[3];
-  anisotropy<T>(seeds + 12 * gid + 3, k.eps4, gr, a, N);
-  const T dphi = ph - T(phi_old[c]);
-  const T u_old = T(temp[c]);
-  const T one_m = T(1) - ph * ph;
-  const T src = (ph - ph * ph * ph - k.lambda * u_old * one_m * one_m) * k.inv_tau0 + (T(1) - a * a) * dphi;
-  const T cs2 = T(0.25);
-  const T B0 = -cs2 * ((a * a - T(1)) * gr[0] + N[0]);
-  const T B1 = -cs2 * ((a * a - T(1)) * gr[1] + N[1]);
-  const T B2 = -cs2 * ((a * a - T(1)) * gr[2] + N[2]);
-  const T fo = (T(1) - T(0.5) * k.om_g) / cs2;
-  // phase-field lattice, all seven loaded before any store (in-place safety)
-  T gv[7];
-#pragma unroll
-  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, stride, nb, PARITY, c, i);
-  const T dph = ph - k.ref_g;
-#pragma unroll
-  for (int i = 0; i < 7; ++i) {
-    const T w = T(wq<7>(i));
-    const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
-    const T go = gv[i] - k.om_g * (gv[i] - w * dph) + fo * w * eB + w * src;
-    st_out<S, 7>(G, stride, nb, PARITY, c, i, go);
-  }
-  T t[7];
-  T dT = T(0);
-#pragma unroll
-  for (int i = 0; i < 7; ++i) {
-    t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
-    dT += t[i];
-  }
-  if constexpr (SOL) {
-    // solutal lattice (TRT): capacity c(phi) applied to D(phi), the
-    // anti-trapping current (first moment of the equilibrium) and the
-    // rejection source; pair sums relax to equilibrium with rate 1, pair
-    // differences with omega(phi)
-    const T U = k.ref_t + dT;
-    const T km = T(1) - k.k_part;
-    const T cap = (T(1) + k.k_part - km * ph) * T(0.5);
-    const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
-    const T fj = -k.at_w0 * (T(1) + km * U) * dphi / ((gn + T(1e-6)) * cap);
-    const T D = (k.D_l * (T(1) - ph) * T(0.5) + k.D_s * (T(1) + ph) * T(0.5)) / cap;
-    const T om = T(1) / (T(4) * D + T(0.5));
-    const T su = T(0.5) * (T(1) + km * U) * dphi / cap;
-    {
-      const T w0 = T(wq<7>(0));
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
-    }
-#pragma unroll
-    for (int i = 1; i < 7; i += 2) {
-      const int j = i + 1;
-      const T w = T(wq<7>(i));
-      const T ej = fj * (T(ex(i)) * gr[0] + T(ey(i)) * gr[1] + T(ez(i)) * gr[2]);
-      const T sym = w * dT;
-      const T am = T(0.5) * (t[i] - t[j]);
-      const T am_new = am - om * (am - w * T(4) * ej);
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
-    }
-  } else {
-    // thermal lattice: relaxation with latent heat (1/2) dphi
-    const T lat = T(0.5) * dphi;
-#pragma unroll
-    for (int i = 0; i < 7; ++i) {
-      const T w = T(wq<7>(i));
-      const T to = t[i] - k.om_t * (t[i] - w * dT) + w * lat;
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
-    }
-  }
-  temp[c] = P(k.ref_t + dT);
-}
-
-template <class S, class P, int PARITY, bool SOL>
-__global__ void __launch_bounds__(256)
-    k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
-                   P* __restrict__ temp, const double* __restrict__ seeds, const Geom g,
-                   const DendK<typename Stor<S>::T> k) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  if (fast_cell(g, x, y, z)) {
-    const Fast fa = make_fast(g, x, y, z);
-    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, seeds, g.stride, fa, fa.c, x, y, z, k);
-  } else {
-    const Nbr nb(g, x, y, z);
-    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, seeds, g.stride, nb, nb.idx(0, 0, 0), x, y, z, k);
-  }
-}
+namespace {
 
 // ===================================================================== INIT
-// Stores the deviation of  f_i = base_scale w (1 + 3eu + 4.5eu^2 - 1.5u^2) + w p_extra
-// from w ref, placed as the post-collision state of loop 0.
-template <class S, int Q>
-__device__ __forceinline__ void put_eq(S* A, const Geom& g, const Nbr& nb, int c, double base_scale, double ux,
-                                       double uy, double uz, double p_extra, double ref) {
-  typedef typename Stor<S>::T T;
-  const double uu = ux * ux + uy * uy + uz * uz;
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const double w = wq<Q>(i);
-    const double eu = ex(i) * ux + ey(i) * uy + ez(i) * uz;
-    const double v = w * ((base_scale - ref + p_extra) + base_scale * (3.0 * eu + 4.5 * eu * eu - 1.5 * uu));
-    st_layout<S, Q>(A, g.stride, nb, 0, c, i, T(v));
-  }
-}
-
 template <class S, class InT>
 __global__ void k_init(int model, int Q0, S* A0, S* A1, float* H0, typename PhiOf<S>::type* phi0,
                        typename PhiOf<S>::type* phi1, typename PhiOf<S>::type* temp, const InT* __restrict__ in_phi,
@@ -881,21 +682,7 @@ MpK<T> mp_coef(const mk_params& p, Refs r) {
 
 template <class T>
 DendK<T> dend_coef(const mk_params& p, Refs r) {
-  DendK<T> k;
-  const double D0 = p.W0 * p.W0 / p.tau0;
-  k.om_g = T(1.0 / (4.0 * D0 + 0.5));
-  k.om_t = T(1.0 / (4.0 * p.D + 0.5));
-  k.inv_tau0 = T(1.0 / p.tau0);
-  k.lambda = T(p.lambda);
-  k.eps4 = T(p.eps4);
-  k.nobj = p.n_objects;
-  k.ref_g = T(r.r0);
-  k.ref_t = T(r.r1);
-  k.k_part = T(p.k_part);
-  k.D_l = T(p.D);
-  k.D_s = T(p.D_s);
-  k.at_w0 = T(p.at_coef * p.W0);
-  return k;
+  return dend_params<T>(p, r.r0, r.r1);
 }
 
 template <class S, int Q, int COLL>
@@ -985,14 +772,18 @@ void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t*
   const bool sol = e.p.model == MK_MODEL_SOLUTAL_DENDRITE;
   if (parity == 0) {
     if (sol)
-      k_dend_collide<S, P, 0, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+      k_dend_collide<S, P, 0, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
+                                                                   (const T*)e.rot, g, k);
     else
-      k_dend_collide<S, P, 0, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+      k_dend_collide<S, P, 0, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
+                                                                   (const T*)e.rot, g, k);
   } else {
     if (sol)
-      k_dend_collide<S, P, 1, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+      k_dend_collide<S, P, 1, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
+                                                                   (const T*)e.rot, g, k);
     else
-      k_dend_collide<S, P, 1, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.seeds, g, k);
+      k_dend_collide<S, P, 1, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
+                                                                   (const T*)e.rot, g, k);
   }
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
@@ -1119,6 +910,36 @@ namespace mke {
 
 static int store_bytes(int prec) { return prec == MK_PREC_FP64 ? 8 : (prec == MK_PREC_FP32 ? 4 : 2); }
 
+// Grain table: centre + rotation per object (R = Rz Ry Rx of the ZYX angles in
+// degrees, as in the oracle); one identity entry when there are none.
+void seed_table(const mk_params& p, std::vector<double>& sd) {
+  const int nobj = p.n_objects > 0 ? p.n_objects : 1;
+  sd.assign((size_t)12 * nobj, 0.0);
+  for (int k = 0; k < nobj; ++k) {
+    double* s = &sd[12 * k];
+    if (k < p.n_objects) {
+      s[0] = p.obj_center[k][0];
+      s[1] = p.obj_center[k][1];
+      s[2] = p.obj_center[k][2];
+    }
+    const double d2r = M_PI / 180.0;
+    const double ax = (k < p.n_objects ? p.obj_angle[k][0] : 0) * d2r, ay = (k < p.n_objects ? p.obj_angle[k][1] : 0) * d2r,
+                 az = (k < p.n_objects ? p.obj_angle[k][2] : 0) * d2r;
+    const double cx = std::cos(ax), sx = std::sin(ax), cy = std::cos(ay), sy = std::sin(ay), cz = std::cos(az),
+                 sz = std::sin(az);
+    double* R = s + 3;
+    R[0] = cz * cy;
+    R[1] = cz * sy * sx - sz * cx;
+    R[2] = cz * sy * cx + sz * sx;
+    R[3] = sz * cy;
+    R[4] = sz * sy * sx + cz * cx;
+    R[5] = sz * sy * cx - cz * sx;
+    R[6] = -sy;
+    R[7] = cy * sx;
+    R[8] = cy * cx;
+  }
+}
+
 cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x, int block_y, std::string& err) {
   std::memset(&e, 0, sizeof(e));
   e.p = p;
@@ -1175,36 +996,41 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   if ((st = alloc(&e.phi[1], dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (!dend) e.phi[1] = nullptr;
   if ((st = alloc(&e.temp, dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
-  // seeds: centre + rotation per object (rotation as in the oracle: R = Rz Ry Rx)
-  const int nobj = p.n_objects > 0 ? p.n_objects : 1;
-  std::vector<double> sd((size_t)12 * nobj, 0.0);
-  for (int k = 0; k < nobj; ++k) {
-    double* s = &sd[12 * k];
-    if (k < p.n_objects) {
-      s[0] = p.obj_center[k][0];
-      s[1] = p.obj_center[k][1];
-      s[2] = p.obj_center[k][2];
-    }
-    const double d2r = M_PI / 180.0;
-    const double ax = (k < p.n_objects ? p.obj_angle[k][0] : 0) * d2r, ay = (k < p.n_objects ? p.obj_angle[k][1] : 0) * d2r,
-                 az = (k < p.n_objects ? p.obj_angle[k][2] : 0) * d2r;
-    const double cx = std::cos(ax), sx = std::sin(ax), cy = std::cos(ay), sy = std::sin(ay), cz = std::cos(az),
-                 sz = std::sin(az);
-    double* R = s + 3;
-    R[0] = cz * cy;
-    R[1] = cz * sy * sx - sz * cx;
-    R[2] = cz * sy * cx + sz * sx;
-    R[3] = sz * cy;
-    R[4] = sz * sy * sx + cz * cx;
-    R[5] = sz * sy * cx - cz * sx;
-    R[6] = -sy;
-    R[7] = cy * sx;
-    R[8] = cy * cx;
-  }
+  std::vector<double> sd;
+  seed_table(p, sd);
   if ((st = cudaMalloc((void**)&e.seeds, sd.size() * sizeof(double))) != cudaSuccess) return st;
   if ((st = cudaMemcpyAsync(e.seeds, sd.data(), sd.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream)) !=
       cudaSuccess)
     return st;
+  // rotations in the arithmetic type (9 per grain) and the per-cell grain map
+  const int nrot = (int)(sd.size() / 12);
+  std::vector<double> rd((size_t)9 * nrot);
+  std::vector<float> rf((size_t)9 * nrot);
+  for (int k = 0; k < nrot; ++k)
+    for (int q = 0; q < 9; ++q) {
+      rd[9 * k + q] = sd[12 * k + 3 + q];
+      rf[9 * k + q] = (float)sd[12 * k + 3 + q];
+    }
+  const bool rot64 = p.precision == MK_PREC_FP64;
+  const size_t rbytes = rot64 ? rd.size() * sizeof(double) : rf.size() * sizeof(float);
+  if ((st = cudaMalloc(&e.rot, rbytes)) != cudaSuccess) return st;
+  if ((st = cudaMemcpyAsync(e.rot, rot64 ? (const void*)rd.data() : (const void*)rf.data(), rbytes,
+                            cudaMemcpyHostToDevice, e.stream)) != cudaSuccess)
+    return st;
+  if (dend && p.n_objects > 1) {
+    if ((st = cudaMalloc((void**)&e.grain, (size_t)e.ncell)) != cudaSuccess) return st;
+    Geom g;
+    g.nx = p.nx;
+    g.ny = p.ny;
+    g.nz = p.nz;
+    g.bc0 = p.bc[0];
+    g.bc1 = p.bc[1];
+    g.bc2 = p.bc[2];
+    g.stride = e.stride;
+    k_grain_map<<<(int)std::min<int64_t>((e.ncell + 255) / 256, 4096), 256, 0, e.stream>>>(g, e.seeds, p.n_objects, 0,
+                                                                                         e.grain);
+    if ((st = cudaGetLastError()) != cudaSuccess) return st;
+  }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   e.partial_blocks = sms * 8;
@@ -1219,7 +1045,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
-  void* ptrs[] = {e.pop0, e.pop1, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.partial, e.dsum, e.field,
+  void* ptrs[] = {e.pop0, e.pop1, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
                   e.field32, e.stage32};
   for (void* q : ptrs)
     if (q) cudaFree(q);

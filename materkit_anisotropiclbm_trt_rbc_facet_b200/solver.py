@@ -68,6 +68,92 @@ def initial_field(params: A.MkParams, field: str) -> np.ndarray:
     return out.reshape(params.nz, params.ny, params.nx)
 
 
+def ensemble_params(seed: int, n_domains: int, precision: str | int = "bf16") -> list[A.MkParams]:
+    """The seeded solutal ensemble: n cubes with edges from {48, 64, 80, 96, 128},
+    eps4 ~ U[0.02, 0.06], 1-6 randomly oriented seeds (no GPU needed)."""
+    lib = A.load()
+    prec = A.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    arr = (A.MkParams * int(n_domains))()
+    _check(lib.mk_ensemble_case_params(int(seed), int(n_domains), prec, arr))
+    return list(arr)
+
+
+class Ensemble:
+    """Many dendrite domains advanced together in one packed lattice (the
+    ensemble of ``run_solutal_dendrite`` / ``run_thermal_dendrite`` sweeps,
+    MaterKit/MaterKit.cpp:633-687, :743-788).  Every loop is two persistent
+    launches over all domains; ``advance`` replays two loops as a CUDA graph."""
+
+    def __init__(self, params: list[A.MkParams]):
+        self._lib = A.load()
+        self._h = C.c_void_p()
+        self.params = [p for p in params]
+        arr = (A.MkParams * len(self.params))(*self.params)
+        _check(self._lib.mk_ensemble_create(arr, len(self.params), C.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.mk_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, status: int) -> None:
+        if status != A.MK_OK:
+            msg = self._lib.mk_ensemble_last_error(self._h) if self._h else self._lib.mk_last_global_error()
+            raise A.MkError(status, (msg or b"").decode(errors="replace"))
+
+    def __len__(self) -> int:
+        return len(self.params)
+
+    @property
+    def cells(self) -> int:
+        return int(self._lib.mk_ensemble_cells(self._h))
+
+    @property
+    def step(self) -> int:
+        return int(self._lib.mk_ensemble_step(self._h))
+
+    def advance(self, nsteps: int) -> None:
+        self._chk(self._lib.mk_ensemble_advance(self._h, int(nsteps)))
+
+    def time_advance(self, nsteps: int) -> float:
+        ms = C.c_double()
+        self._chk(self._lib.mk_ensemble_time_advance(self._h, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def profile(self, nsteps: int, kernel: str = "collide") -> dict:
+        """Device time of one launch kind over `nsteps` eager loops (CUDA events)."""
+        k, t = C.c_double(), C.c_double()
+        self._chk(self._lib.mk_ensemble_profile_steps(self._h, int(nsteps), kernel.encode(), C.byref(k), C.byref(t)))
+        return {"kernel_ms": k.value, "step_ms": t.value, "launches": int(nsteps)}
+
+    @property
+    def launches(self) -> int:
+        return int(self._lib.mk_ensemble_launches(self._h))
+
+    def field(self, domain: int, name: str, dtype=np.float64) -> np.ndarray:
+        if not 0 <= domain < len(self.params):
+            raise A.MkError(A.MK_ERR_ARG, f"domain index {domain} out of range")
+        p = self.params[domain]
+        dt = np.dtype(dtype)
+        code = A.MK_DTYPE_F64 if dt == np.float64 else A.MK_DTYPE_F32
+        out = np.empty(p.ncell(), dtype=dt)
+        self._chk(self._lib.mk_ensemble_get_field(self._h, int(domain), A.FIELDS[name], code, out.ctypes.data,
+                                                  out.nbytes))
+        return out.reshape(p.nz, p.ny, p.nx)
+
+
 class Solver:
     """One device-resident case (a handle of the C ABI)."""
 
