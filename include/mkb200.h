@@ -93,6 +93,15 @@ typedef enum mk_bc {
   MK_BC_CLOSED = 2    /* all cells fluid; the domain faces bounce back (zero flux)      */
 } mk_bc;
 
+/* Interfacial anisotropy a(n) of the phase field, n the crystal-frame normal
+ * (mkPhaseField::anisotropy / _cbc / _hcp / _facet, mkPhaseField.h:61-64). */
+typedef enum mk_anisotropy {
+  MK_ANISO_CUBIC = 0, /* 1 - 3 e4 + 4 e4 sum n^4                                        */
+  MK_ANISO_CBC = 1,   /* 1 + e4 (sum n^4 - 3/5) + e2 (3 sum n^4 + 66 nx^2 ny^2 nz^2 - 17/7) */
+  MK_ANISO_HCP = 2,   /* 1 + e4 Re (nx + i ny)^6 + e2 (2 nz^2 - 1)                     */
+  MK_ANISO_FACET = 3  /* 1 + e4 (sum sqrt(n^2 + e2^2) - sqrt(1 + e2^2) - 2 e2)          */
+} mk_anisotropy;
+
 /* Node flags, values of MaterKit/inc/mkGlobalDefs.h:140-145. */
 #define MK_FLAG_FLUID 0
 #define MK_FLAG_INTER 1
@@ -160,11 +169,21 @@ typedef struct mk_params {
 
   /* seeds (dendrites) or bubbles (multiphase) */
   int32_t n_objects;
-  int32_t _pad0;
+  int32_t aniso;      /* mk_anisotropy of the phase field (dendrites) */
   double obj_center[MK_MAX_OBJECTS][3];
   double obj_angle[MK_MAX_OBJECTS][3];  /* degrees, rotate order ZYX */
   double obj_radius[MK_MAX_OBJECTS];
   uint64_t rng_seed;
+
+  double eps2;        /* second anisotropy coefficient: cbc eps2, hcp eps_z, facet cusp width */
+
+  /* plates and inlets (convection, flow) */
+  int32_t wall_axis;    /* axis whose two faces are plates with a Dirichlet scalar / wall velocity; -1 none */
+  int32_t inlet;        /* 1: velocity inlet at x = 0, pressure outlet at x = nx - 1 (flow) */
+  double wall_value[2]; /* scalar (T or C) on the low / high plate */
+  double wall_u[2][3];  /* velocity of the low / high plate (flow) */
+  double beta;          /* Boussinesq expansion coefficient: F = -rho0 beta (s - s_ref) g, g = force */
+  double s_ref;         /* reference value of the scalar in the buoyancy */
 } mk_params;
 
 /* Optional overrides at creation; a negative value keeps the XML/default. */

@@ -21,6 +21,8 @@ MK_PREC_FP64, MK_PREC_FP32, MK_PREC_FP16, MK_PREC_BF16 = range(4)
 MK_COLL_BGK, MK_COLL_TRT, MK_COLL_MRT = range(3)
 MK_D3Q7, MK_D3Q19, MK_D3Q27 = 7, 19, 27
 MK_BC_PERIODIC, MK_BC_WALLS, MK_BC_CLOSED = range(3)
+MK_ANISO_CUBIC, MK_ANISO_CBC, MK_ANISO_HCP, MK_ANISO_FACET = range(4)
+ANISOTROPIES = {"cubic": MK_ANISO_CUBIC, "cbc": MK_ANISO_CBC, "hcp": MK_ANISO_HCP, "facet": MK_ANISO_FACET}
 (MK_FIELD_RHO, MK_FIELD_UX, MK_FIELD_UY, MK_FIELD_UZ, MK_FIELD_T, MK_FIELD_C, MK_FIELD_PHI, MK_FIELD_FLAG,
  MK_FIELD_PRESSURE, MK_FIELD_DPHI, MK_FIELD_GRAIN) = range(11)
 MK_DTYPE_F64, MK_DTYPE_F32 = 0, 1
@@ -47,9 +49,12 @@ class MkParams(C.Structure):
         ("eps4", C.c_double), ("W0", C.c_double), ("tau0", C.c_double), ("lambda_", C.c_double),
         ("delta", C.c_double), ("D", C.c_double), ("D_s", C.c_double), ("k_part", C.c_double),
         ("at_coef", C.c_double),
-        ("n_objects", C.c_int32), ("_pad0", C.c_int32),
+        ("n_objects", C.c_int32), ("aniso", C.c_int32),
         ("obj_center", (C.c_double * 3) * MK_MAX_OBJECTS), ("obj_angle", (C.c_double * 3) * MK_MAX_OBJECTS),
         ("obj_radius", C.c_double * MK_MAX_OBJECTS), ("rng_seed", C.c_uint64),
+        ("eps2", C.c_double),
+        ("wall_axis", C.c_int32), ("inlet", C.c_int32), ("wall_value", C.c_double * 2),
+        ("wall_u", (C.c_double * 3) * 2), ("beta", C.c_double), ("s_ref", C.c_double),
     ]
 
     def ncell(self) -> int:

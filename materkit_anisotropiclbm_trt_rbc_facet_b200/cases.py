@@ -34,10 +34,14 @@ def poiseuille(nx=64, ny=32, nz=32, loops=2000, precision="fp64", collision="TRT
 
 
 def thermal_dendrite(n=128, loops=5000, precision="fp32", eps4=0.05, W0=1.5, lam=10.0, delta=0.55, D=0.1,
-                     radius=8.0, tau0=None, center=None) -> str:
-    """Config 2: D3Q7 thermal lattice + anisotropic phase field, one centred seed."""
+                     radius=8.0, tau0=None, center=None, aniso="cubic", eps2=0.0) -> str:
+    """Config 2: D3Q7 thermal lattice + anisotropic phase field, one centred seed.
+
+    `aniso` selects the anisotropy kind (cubic, cbc, hcp, facet) with `eps4`
+    and `eps2` its two coefficients."""
     c = center if center is not None else ((n - 1) / 2.0,) * 3
-    t0 = f"<tau0> {tau0} </tau0>" if tau0 else ""
+    extra = f"<tau0> {tau0} </tau0>" if tau0 else ""
+    extra += f" <anisotropyKind> {aniso} </anisotropyKind> <eps2> {eps2} </eps2>"
     return _HEADER.format(dendrite="true", flow="false", loops=loops, frames=min(loops, 100), nx=n, ny=n, nz=n) + f"""
   <phasechange>
     <d0> 0.138486 </d0> <lambda> {lam} </lambda> <anisotropy> {eps4} </anisotropy> <W0> 1.0 </W0> <t0> 1.0 </t0>
@@ -50,18 +54,18 @@ def thermal_dendrite(n=128, loops=5000, precision="fp32", eps4=0.05, W0=1.5, lam
     <model> thermal_dendrite </model> <precision> {precision} </precision>
     <boundary> closed closed closed </boundary>
     <eps4> {eps4} </eps4> <W0> {W0} </W0> <lambda> {lam} </lambda> <delta> {delta} </delta>
-    <diffusivity> {D} </diffusivity> {t0}
+    <diffusivity> {D} </diffusivity> {extra}
   </b200>
 </MaterKit>
 """
 
 
 def solutal_dendrite(n=64, ny=None, nz=None, loops=3000, precision="fp32", eps4=0.04, W0=1.5, lam=10.0,
-                     delta=0.55, D=0.1, D_s=1e-4, k=0.15, seeds=None, tau0=None) -> str:
+                     delta=0.55, D=0.1, D_s=1e-4, k=0.15, seeds=None, tau0=None, aniso="cubic", eps2=0.0) -> str:
     """Config 4 element: D3Q7 solutal lattice + anisotropic phase field, closed faces.
 
     `seeds` is a list of (center xyz, angles xyz in degrees, radius); default one
-    centred seed of radius 6.
+    centred seed of radius 6.  `aniso` / `eps2` as in thermal_dendrite.
     """
     ny = n if ny is None else ny
     nz = n if nz is None else nz
@@ -71,6 +75,7 @@ def solutal_dendrite(n=64, ny=None, nz=None, loops=3000, precision="fp32", eps4=
     ang = " ".join(f"{a[0]} {a[1]} {a[2]}" for _, a, _ in seeds)
     rad = " ".join(f"{r}" for _, _, r in seeds)
     t0 = f"<tau0> {tau0} </tau0>" if tau0 else ""
+    t0 += f" <anisotropyKind> {aniso} </anisotropyKind> <eps2> {eps2} </eps2>"
     return _HEADER.format(dendrite="true", flow="false", loops=loops, frames=min(loops, 100), nx=n, ny=ny, nz=nz) + f"""
   <phasechange>
     <d0> 0.2762 </d0> <lambda> {lam} </lambda> <anisotropy> {eps4} </anisotropy> <W0> 1.0 </W0> <t0> 1.0 </t0>

@@ -49,6 +49,10 @@ void default_params(mk_params* p) {
   p->at_coef = 1.0 / (2.0 * std::sqrt(2.0));
   p->tau0 = 0.6267 * p->lambda * p->W0 * p->W0 / p->D;
   p->rng_seed = 0;
+  p->aniso = MK_ANISO_CUBIC;
+  p->eps2 = 0.0;
+  p->wall_axis = -1;
+  p->inlet = 0;
 }
 
 void default_options(mk_options* o) {
@@ -263,6 +267,14 @@ mk_status validate_params(const mk_params* p, std::string& err) {
     }
     if (p->n_objects < 0 || p->n_objects > MK_MAX_OBJECTS) {
       err = "bad seed count";
+      return MK_ERR_ARG;
+    }
+    if (p->aniso < MK_ANISO_CUBIC || p->aniso > MK_ANISO_FACET) {
+      err = "unknown anisotropy kind";
+      return MK_ERR_ARG;
+    }
+    if (p->aniso == MK_ANISO_FACET && !(p->eps2 > 0)) {
+      err = "facet anisotropy needs a positive cusp width (eps2)";
       return MK_ERR_ARG;
     }
   }
@@ -482,8 +494,23 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
         p.bc[a] = bc;
       }
     }
+    if (const mkx::Element* e = b->child("anisotropyKind")) {
+      const std::string t = lower(mkx::trimmed(e->text));
+      if (t == "cubic")
+        p.aniso = MK_ANISO_CUBIC;
+      else if (t == "cbc")
+        p.aniso = MK_ANISO_CBC;
+      else if (t == "hcp")
+        p.aniso = MK_ANISO_HCP;
+      else if (t == "facet")
+        p.aniso = MK_ANISO_FACET;
+      else {
+        err = "<b200><anisotropyKind>: unknown '" + t + "'";
+        return MK_ERR_XML;
+      }
+    }
     std::vector<double> v;
-    bool ok = opt_d(b, "magic", p.magic, err) && opt_d(b, "tau", p.tau, err) && opt_d(b, "rho0", p.rho0, err) &&
+    bool ok = opt_d(b, "eps2", p.eps2, err) && opt_d(b, "magic", p.magic, err) && opt_d(b, "tau", p.tau, err) && opt_d(b, "rho0", p.rho0, err) &&
               opt_d(b, "rhoL", p.rho_l, err) && opt_d(b, "rhoG", p.rho_g, err) && opt_d(b, "tauL", p.tau_l, err) &&
               opt_d(b, "tauG", p.tau_g, err) && opt_d(b, "sigma", p.sigma, err) && opt_d(b, "width", p.width, err) &&
               opt_d(b, "mobility", p.mobility, err) && opt_d(b, "contactAngle", p.contact_angle, err) &&

@@ -14,8 +14,8 @@ namespace mkd {
 // g_i - w_i ref_g (ref_g = -1) and t_i - w_i ref_t (ref_t = -Delta).
 template <class T>
 struct DendK {
-  T om_g, om_t, inv_tau0, lambda, eps4;
-  int nobj;
+  T om_g, om_t, inv_tau0, lambda, eps4, eps2;
+  int nobj, aniso;
   T ref_g, ref_t;
   T k_part, D_l, D_s, at_w0;  // solutal lattice
 };
@@ -69,12 +69,57 @@ __device__ __forceinline__ int nearest_seed(const double* __restrict__ seeds, in
   return best;
 }
 
-// a(n) and the lab-frame anisotropy vector N of Karma-Rappel 4-fold
-// anisotropy (mkPhaseField::anisotropy, mkPhaseField.h:61).
-// `Rm` is the grain's rotation (row-major, columns = crystal axes) in the
-// arithmetic type.
+// a(n) and da/dn of the anisotropy kinds (mk_anisotropy), n the crystal-frame
+// unit normal (mkPhaseField::anisotropy / _cbc / _hcp / _facet,
+// mkPhaseField.h:61-64).  The kind is uniform over a launch, so the switch
+// never diverges.
 template <class T>
-__device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, T eps4, const T (&gr)[3], T& a, T (&N)[3]) {
+__device__ __forceinline__ void aniso_function(int kind, T e4, T e2, const T (&n)[3], T& a, T (&g)[3]) {
+  const T x = n[0], y = n[1], z = n[2];
+  const T x2 = x * x, y2 = y * y, z2 = z * z;
+  switch (kind) {
+    case MK_ANISO_CBC: {
+      const T s4 = x2 * x2 + y2 * y2 + z2 * z2, s6 = x2 * y2 * z2;
+      a = T(1) + e4 * (s4 - T(0.6)) + e2 * (T(3) * s4 + T(66) * s6 - T(17.0 / 7.0));
+      g[0] = T(4) * e4 * x2 * x + e2 * (T(12) * x2 * x + T(132) * x * y2 * z2);
+      g[1] = T(4) * e4 * y2 * y + e2 * (T(12) * y2 * y + T(132) * y * x2 * z2);
+      g[2] = T(4) * e4 * z2 * z + e2 * (T(12) * z2 * z + T(132) * z * x2 * y2);
+      break;
+    }
+    case MK_ANISO_HCP: {
+      const T c6 = x2 * x2 * x2 - T(15) * x2 * x2 * y2 + T(15) * x2 * y2 * y2 - y2 * y2 * y2;
+      a = T(1) + e4 * c6 + e2 * (T(2) * z2 - T(1));
+      g[0] = T(6) * e4 * (x2 * x2 * x - T(10) * x2 * x * y2 + T(5) * x * y2 * y2);
+      g[1] = T(-6) * e4 * (T(5) * x2 * x2 * y - T(10) * x2 * y2 * y + y2 * y2 * y);
+      g[2] = T(4) * e2 * z;
+      break;
+    }
+    case MK_ANISO_FACET: {
+      const T rx = sqrt(x2 + e2 * e2), ry = sqrt(y2 + e2 * e2), rz = sqrt(z2 + e2 * e2);
+      a = T(1) + e4 * (rx + ry + rz - sqrt(T(1) + e2 * e2) - T(2) * e2);
+      g[0] = e4 * x / rx;
+      g[1] = e4 * y / ry;
+      g[2] = e4 * z / rz;
+      break;
+    }
+    default: {
+      const T s4 = x2 * x2 + y2 * y2 + z2 * z2;
+      a = T(1) - T(3) * e4 + T(4) * e4 * s4;
+      g[0] = T(16) * e4 * x2 * x;
+      g[1] = T(16) * e4 * y2 * y;
+      g[2] = T(16) * e4 * z2 * z;
+      break;
+    }
+  }
+}
+
+// a(n) and the lab-frame vector N of the anisotropic flux (Karma-Rappel):
+// N_c = |grad phi| a (da/dn - n (n . da/dn)) in the crystal frame.  `Rm` is
+// the grain's rotation (row-major, columns = crystal axes) in the arithmetic
+// type.
+template <class T>
+__device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T eps4, T eps2, const T (&gr)[3],
+                                           T& a, T (&N)[3]) {
   T R[9];
 #pragma unroll
   for (int q = 0; q < 9; ++q) R[q] = __ldg(Rm + q);
@@ -84,11 +129,12 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, T eps4, con
   T nc[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) nc[q] = R[0 * 3 + q] * nl0 + R[1 * 3 + q] * nl1 + R[2 * 3 + q] * nl2;
-  const T s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
-  a = T(1) - T(3) * eps4 + T(4) * eps4 * s4;
+  T da[3];
+  aniso_function<T>(kind, eps4, eps2, nc, a, da);
+  const T ndg = nc[0] * da[0] + nc[1] * da[1] + nc[2] * da[2];
   T Nc[3];
 #pragma unroll
-  for (int q = 0; q < 3; ++q) Nc[q] = gn * a * T(16) * eps4 * (nc[q] * nc[q] * nc[q] - nc[q] * s4);
+  for (int q = 0; q < 3; ++q) Nc[q] = gn * a * (da[q] - nc[q] * ndg);
 #pragma unroll
   for (int q = 0; q < 3; ++q) N[q] = R[q * 3 + 0] * Nc[0] + R[q * 3 + 1] * Nc[1] + R[q * 3 + 2] * Nc[2];
 }
@@ -117,7 +163,7 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
   const T gr[3] = {T(3) * gx, T(3) * gy, T(3) * gz};
   const int gid = k.nobj > 1 ? (int)__ldg(grain + c) : 0;
   T a, N[3];
-  anisotropy<T>(rot + 9 * gid, k.eps4, gr, a, N);
+  anisotropy<T>(rot + 9 * gid, k.aniso, k.eps4, k.eps2, gr, a, N);
   const T dphi = ph - T(phi_old[c]);
   const T u_old = T(temp[c]);
   const T one_m = T(1) - ph * ph;
@@ -227,7 +273,9 @@ inline DendK<T> dend_params(const mk_params& p, double ref_g, double ref_t) {
   k.inv_tau0 = T(1.0 / p.tau0);
   k.lambda = T(p.lambda);
   k.eps4 = T(p.eps4);
+  k.eps2 = T(p.eps2);
   k.nobj = p.n_objects;
+  k.aniso = p.aniso;
   k.ref_g = T(ref_g);
   k.ref_t = T(ref_t);
   k.k_part = T(p.k_part);

@@ -383,18 +383,73 @@ int nearest_seed(const mk_params& p, double x, double y, double z) {
   return best;
 }
 
-// Anisotropy of a cell: returns a(n) and the lab-frame vector N, from the
+// a(n) and its gradient da/dn of the interfacial anisotropy kinds, n the
+// crystal-frame unit normal (mkPhaseField::anisotropy / _cbc / _hcp / _facet,
+// mkPhaseField.h:61-64; forms of the mk_anisotropy enum in include/mkb200.h):
+//   cubic  Karma & Rappel 1998 four-fold: 1 - 3 e4 + 4 e4 s4, s4 = sum n^4
+//   cbc    two cubic harmonics (Haxhimali et al., Nat. Mater. 5 (2006) 660):
+//          1 + e4 (s4 - 3/5) + e2 (3 s4 + 66 nx^2 ny^2 nz^2 - 17/7)
+//   hcp    six-fold in the basal plane plus a c-axis term:
+//          1 + e4 Re (nx + i ny)^6 + e2 (2 nz^2 - 1)
+//   facet  regularised cusps at the cube directions (the |n_q| faceting form
+//          of Eggleston, McFadden & Voorhees, Physica D 150 (2001) 91):
+//          1 + e4 (sum sqrt(n_q^2 + e2^2) - sqrt(1 + e2^2) - 2 e2)
+void aniso_function(int kind, double e4, double e2, const double n[3], double* a_out, double g[3]) {
+  const double x = n[0], y = n[1], z = n[2];
+  const double x2 = x * x, y2 = y * y, z2 = z * z;
+  double a;
+  switch (kind) {
+    case MK_ANISO_CBC: {
+      const double s4 = x2 * x2 + y2 * y2 + z2 * z2, s6 = x2 * y2 * z2;
+      a = 1.0 + e4 * (s4 - 0.6) + e2 * (3.0 * s4 + 66.0 * s6 - 17.0 / 7.0);
+      g[0] = 4.0 * e4 * x2 * x + e2 * (12.0 * x2 * x + 132.0 * x * y2 * z2);
+      g[1] = 4.0 * e4 * y2 * y + e2 * (12.0 * y2 * y + 132.0 * y * x2 * z2);
+      g[2] = 4.0 * e4 * z2 * z + e2 * (12.0 * z2 * z + 132.0 * z * x2 * y2);
+      break;
+    }
+    case MK_ANISO_HCP: {
+      const double c6 = x2 * x2 * x2 - 15.0 * x2 * x2 * y2 + 15.0 * x2 * y2 * y2 - y2 * y2 * y2;
+      a = 1.0 + e4 * c6 + e2 * (2.0 * z2 - 1.0);
+      g[0] = 6.0 * e4 * (x2 * x2 * x - 10.0 * x2 * x * y2 + 5.0 * x * y2 * y2);
+      g[1] = -6.0 * e4 * (5.0 * x2 * x2 * y - 10.0 * x2 * y2 * y + y2 * y2 * y);
+      g[2] = 4.0 * e2 * z;
+      break;
+    }
+    case MK_ANISO_FACET: {
+      const double rx = sqrt(x2 + e2 * e2), ry = sqrt(y2 + e2 * e2), rz = sqrt(z2 + e2 * e2);
+      a = 1.0 + e4 * (rx + ry + rz - sqrt(1.0 + e2 * e2) - 2.0 * e2);
+      g[0] = e4 * x / rx;
+      g[1] = e4 * y / ry;
+      g[2] = e4 * z / rz;
+      break;
+    }
+    default: {
+      const double s4 = x2 * x2 + y2 * y2 + z2 * z2;
+      a = 1.0 - 3.0 * e4 + 4.0 * e4 * s4;
+      g[0] = 16.0 * e4 * x2 * x;
+      g[1] = 16.0 * e4 * y2 * y;
+      g[2] = 16.0 * e4 * z2 * z;
+      break;
+    }
+  }
+  *a_out = a;
+}
+
+// Anisotropy of a cell: returns a(n) and the lab-frame vector N of the
+// anisotropic flux  div(|grad phi|^2 a da/d(grad phi)),
+// N_c = |grad phi| a (da/dn - n (n . da/dn)) in the crystal frame, from the
 // lab gradient and the grain's rotation (columns = crystal axes).
-void anisotropy(const double* R, double eps4, const double g[3], double* a_out, double N[3]) {
+void anisotropy(const double* R, int kind, double e4, double e2, const double g[3], double* a_out, double N[3]) {
   const double gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
   const double inv = 1.0 / (gn + 1e-12);
   const double nl[3] = {g[0] * inv, g[1] * inv, g[2] * inv};
   double nc[3];
   for (int a = 0; a < 3; ++a) nc[a] = R[0 * 3 + a] * nl[0] + R[1 * 3 + a] * nl[1] + R[2 * 3 + a] * nl[2];
-  const double s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
-  const double a = 1.0 - 3.0 * eps4 + 4.0 * eps4 * s4;
+  double a, da[3];
+  aniso_function(kind, e4, e2, nc, &a, da);
+  const double ndg = nc[0] * da[0] + nc[1] * da[1] + nc[2] * da[2];
   double Nc[3];
-  for (int k = 0; k < 3; ++k) Nc[k] = gn * a * 16.0 * eps4 * (nc[k] * nc[k] * nc[k] - nc[k] * s4);
+  for (int k = 0; k < 3; ++k) Nc[k] = gn * a * (da[k] - nc[k] * ndg);
   for (int a2 = 0; a2 < 3; ++a2) N[a2] = R[a2 * 3 + 0] * Nc[0] + R[a2 * 3 + 1] * Nc[1] + R[a2 * 3 + 2] * Nc[2];
   *a_out = a;
 }
@@ -429,7 +484,7 @@ void thermal_dendrite_step(orc_state* s) {
         grad_lap(
             s, s->phi, x, y, z, [](double p0) { return p0; }, gr, &lap);
         double a, N[3];
-        anisotropy(&s->rot[9 * s->grain[c]], p.eps4, gr, &a, N);
+        anisotropy(&s->rot[9 * s->grain[c]], p.aniso, p.eps4, p.eps2, gr, &a, N);
         const double ph = s->phi[c];
         const double dphi = ph - s->phi_prev[c];
         const double one_m = 1.0 - ph * ph;
@@ -729,4 +784,8 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
     return 0;
   }
   return 1;
+}
+
+extern "C" void orc_anisotropy(int kind, double e4, double e2, const double* n, double* a, double* g) {
+  aniso_function(kind, e4, e2, n, a, g);
 }

@@ -58,8 +58,9 @@
 // Karma-Rappel thin-interface model, Chai et al. IJHMT 122 (2018) 631 source
 // form as in mkFluidsUser.cpp:262-288):
 //   tau0 a^2 dphi/dt = W0^2 div(a^2 grad phi + N) + phi - phi^3 - lam u (1-phi^2)^2
-//   a(n) = 1 - 3 eps4 + 4 eps4 sum n_k^4 (crystal frame),
-//   N_k = |grad phi| a 16 eps4 (n_k^3 - n_k sum n_j^4)
+//   a(n) one of the mk_anisotropy kinds (crystal frame n; cubic:
+//   1 - 3 eps4 + 4 eps4 sum n_k^4), with da/dn its gradient,
+//   N_k = |grad phi| a (da/dn_k - n_k (n . da/dn))   (cubic: |grad phi| a 16 eps4 (n_k^3 - n_k sum n_j^4))
 //   D3Q7 g-lattice: geq = w phi, omega_g = 1/(4 W0^2/tau0 + 1/2),
 //   g* = g - omega_g (g - geq) + (1 - omega_g/2) w (e.B)/cs^2 + w S,
 //   B = -cs^2 [(a^2 - 1) grad phi + N],
@@ -108,6 +109,8 @@ int orc_get_field(const orc_state* s, int field, double* out);
 // Raw post-collision populations of lattice `which` (0 flow/phase, 1 second lattice).
 int orc_get_populations(const orc_state* s, int which, double* out);
 void orc_set_threads(int n);
+// a(n) and da/dn of an anisotropy kind at the crystal-frame unit normal n (tests).
+void orc_anisotropy(int kind, double e4, double e2, const double* n, double* a, double* g);
 int orc_get_threads(void);
 
 #ifdef __cplusplus

@@ -45,6 +45,7 @@ def load() -> C.CDLL:
         lib.orc_get_populations.argtypes = [C.c_void_p, C.c_int, D]
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_get_threads.restype = C.c_int
+        lib.orc_anisotropy.argtypes = [C.c_int, C.c_double, C.c_double, D, D, D]
         _lib = lib
     return _lib
 
@@ -123,3 +124,12 @@ def rel_l2(a, b, mask=None, floor: float = 0.0) -> float:
     if den == 0.0:
         return num
     return num / den
+
+
+def anisotropy(kind: int, e4: float, e2: float, n):
+    """a(n) and da/dn of the oracle's anisotropy kind at the unit normal n."""
+    nn = np.ascontiguousarray(n, dtype=np.float64)
+    a = np.zeros(1)
+    g = np.zeros(3)
+    load().orc_anisotropy(int(kind), float(e4), float(e2), _ptr(nn), _ptr(a), _ptr(g))
+    return float(a[0]), g

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params, initial_field
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
 from _oracle import Oracle, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -224,6 +225,26 @@ def test_solutal_fp64_steps(casedir):
     o.advance(150)
     _compare(s, o, SOL_FIELDS, FP64_TOL)
     assert np.array_equal(s.field("grain"), o.field("grain"))
+
+
+@pytest.mark.parametrize("aniso,e4,e2", [("cbc", 0.03, -0.02), ("hcp", 0.02, 0.03), ("facet", 0.1, 0.05)])
+def test_dendrite_anisotropy_kinds_fp64(casedir, aniso, e4, e2):
+    # two rotated seeds: the kinds are evaluated in each grain's crystal frame
+    # dphi = phi^n - phi^(n-1) is a difference of nearly equal fields: its
+    # relative error is the phi error amplified by |phi| / |dphi| (~1e3), and
+    # the steep facet cusps make the normal's rounding (FMA on the device, none
+    # on the host) visible there, so it is held to 1e-9 instead of 1e-10
+    p, s, o = _pair(casedir, f"aniso_{aniso}", _sol_case(eps4=e4, aniso=aniso, eps2=e2))
+    assert p.aniso == A.ANISOTROPIES[aniso]
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, ["phi", "C"], FP64_TOL)
+        _compare(s, o, ["dphi"], 1e-9)
+    s.advance(60)
+    o.advance(60)
+    _compare(s, o, ["phi", "C"], FP64_TOL)
+    _compare(s, o, ["dphi"], 1e-9)
 
 
 def test_solutal_fp32(casedir):

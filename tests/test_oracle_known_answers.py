@@ -186,3 +186,77 @@ def test_solutal_seed_grows_rejects_solute_symmetrically(casedir):
     assert np.max(np.abs(phi - phi.transpose(0, 2, 1))) < 1e-12
     assert np.max(np.abs(phi - phi.transpose(2, 1, 0))) < 1e-12
     assert np.max(np.abs(U - U.transpose(2, 1, 0))) < 1e-12
+
+
+# ---------------------------------------------------------------- anisotropy kinds
+from _oracle import anisotropy as orc_aniso  # noqa: E402
+
+KINDS = {"cubic": (A.MK_ANISO_CUBIC, 0.05, 0.0), "cbc": (A.MK_ANISO_CBC, 0.03, -0.02),
+         "hcp": (A.MK_ANISO_HCP, 0.02, 0.03), "facet": (A.MK_ANISO_FACET, 0.1, 0.05)}
+
+
+@pytest.mark.parametrize("name", sorted(KINDS))
+def test_anisotropy_gradient_matches_finite_differences(name):
+    kind, e4, e2 = KINDS[name]
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        n = rng.normal(size=3)
+        n /= np.linalg.norm(n)
+        a, g = orc_aniso(kind, e4, e2, n)
+        h = 1e-6
+        for q in range(3):
+            dp, dm = n.copy(), n.copy()
+            dp[q] += h
+            dm[q] -= h
+            fd = (orc_aniso(kind, e4, e2, dp)[0] - orc_aniso(kind, e4, e2, dm)[0]) / (2 * h)
+            assert abs(fd - g[q]) < 1e-8, (name, n, q, fd, g[q])
+
+
+def test_anisotropy_values_at_special_directions():
+    e4, e2 = 0.04, 0.03
+    s = 1 / np.sqrt(3)
+    # cubic: a(100) = 1 + e4, a(111) = 1 - 5 e4 / 3
+    assert orc_aniso(A.MK_ANISO_CUBIC, e4, 0, [1, 0, 0])[0] == pytest.approx(1 + e4, abs=1e-15)
+    assert orc_aniso(A.MK_ANISO_CUBIC, e4, 0, [s, s, s])[0] == pytest.approx(1 - 5 * e4 / 3, abs=1e-15)
+    # cbc: the harmonics average to zero over the sphere; a(100) = 1 + 0.4 e4 + 4/7 e2
+    assert orc_aniso(A.MK_ANISO_CBC, e4, e2, [1, 0, 0])[0] == pytest.approx(1 + 0.4 * e4 + 4 / 7 * e2, abs=1e-15)
+    # hcp: six-fold in the basal plane, a(c axis) = 1 + e2
+    c, sn = np.cos(np.pi / 6), np.sin(np.pi / 6)
+    assert orc_aniso(A.MK_ANISO_HCP, e4, e2, [1, 0, 0])[0] == pytest.approx(1 + e4 - e2, abs=1e-15)
+    assert orc_aniso(A.MK_ANISO_HCP, e4, e2, [c, sn, 0])[0] == pytest.approx(1 - e4 - e2, abs=1e-14)
+    assert orc_aniso(A.MK_ANISO_HCP, e4, e2, [0, 0, 1])[0] == pytest.approx(1 + e2, abs=1e-15)
+    for k in range(6):
+        t = k * np.pi / 3 + 0.2
+        assert orc_aniso(A.MK_ANISO_HCP, e4, e2, [np.cos(t), np.sin(t), 0])[0] == pytest.approx(
+            orc_aniso(A.MK_ANISO_HCP, e4, e2, [np.cos(0.2), np.sin(0.2), 0])[0], abs=1e-14)
+    # facet: cusp minimum a = 1 at the cube directions, larger elsewhere
+    assert orc_aniso(A.MK_ANISO_FACET, 0.1, 0.05, [0, 1, 0])[0] == pytest.approx(1.0, abs=1e-15)
+    assert orc_aniso(A.MK_ANISO_FACET, 0.1, 0.05, [s, s, s])[0] > 1.05
+
+
+@pytest.mark.parametrize("name", ["cbc", "facet"])
+def test_cubic_kinds_keep_cubic_symmetry(casedir, name):
+    kind, e4, e2 = KINDS[name]
+    n = 21
+    p = _params(casedir, f"sym_{name}", cases.thermal_dendrite(n=n, loops=1, radius=4.0, eps4=e4, aniso=name,
+                                                               eps2=e2))
+    assert p.aniso == kind
+    o = Oracle(p, phi=initial_field(p, "phi"))
+    o.advance(80)
+    phi = o.field("phi")
+    assert np.max(np.abs(phi - phi.transpose(0, 2, 1))) < 1e-12
+    assert np.max(np.abs(phi - phi.transpose(2, 1, 0))) < 1e-12
+    assert (phi > 0).sum() > (initial_field(p, "phi") > 0).sum()
+
+
+def test_hcp_keeps_its_mirror_symmetries_and_differs_from_cubic(casedir):
+    n = 21
+    p = _params(casedir, "sym_hcp", cases.thermal_dendrite(n=n, loops=1, radius=4.0, eps4=0.03, aniso="hcp",
+                                                           eps2=0.02))
+    o = Oracle(p, phi=initial_field(p, "phi"))
+    o.advance(80)
+    phi = o.field("phi")
+    for ax in range(3):
+        assert np.max(np.abs(phi - np.flip(phi, axis=ax))) < 1e-12
+    # six-fold in the basal (x, y) plane: not symmetric under x <-> y, unlike a cubic crystal
+    assert np.max(np.abs(phi - phi.transpose(0, 2, 1))) > 1e-6
