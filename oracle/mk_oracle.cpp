@@ -789,3 +789,285 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
 extern "C" void orc_anisotropy(int kind, double e4, double e2, const double* n, double* a, double* g) {
   aniso_function(kind, e4, e2, n, a, g);
 }
+
+// ------------------------------------------------------------------ ADJOINT
+// Discrete adjoint of the thermal dendrite loop (thermal_dendrite_step),
+// reverse mode over stored states.  The state at the start of loop n is
+// Y = (F = f_out, S = s_out, P = phi (= phi^(n-1)), U = temp (= u^n)); the loss
+// is a function of P after the last loop.
+namespace {
+
+// d2a/dn2 and the derivatives of a and da/dn with respect to e4, for the
+// kinds of aniso_function.
+void aniso_second(int kind, double e4, double e2, const double n[3], double H[3][3], double* a_e4,
+                  double da_e4[3]) {
+  const double x = n[0], y = n[1], z = n[2];
+  const double x2 = x * x, y2 = y * y, z2 = z * z;
+  for (int q = 0; q < 3; ++q)
+    for (int r = 0; r < 3; ++r) H[q][r] = 0.0;
+  switch (kind) {
+    case MK_ANISO_CBC: {
+      const double s4 = x2 * x2 + y2 * y2 + z2 * z2;
+      H[0][0] = 12.0 * e4 * x2 + e2 * (36.0 * x2 + 132.0 * y2 * z2);
+      H[1][1] = 12.0 * e4 * y2 + e2 * (36.0 * y2 + 132.0 * x2 * z2);
+      H[2][2] = 12.0 * e4 * z2 + e2 * (36.0 * z2 + 132.0 * x2 * y2);
+      H[0][1] = H[1][0] = 264.0 * e2 * x * y * z2;
+      H[0][2] = H[2][0] = 264.0 * e2 * x * z * y2;
+      H[1][2] = H[2][1] = 264.0 * e2 * y * z * x2;
+      *a_e4 = s4 - 0.6;
+      da_e4[0] = 4.0 * x2 * x;
+      da_e4[1] = 4.0 * y2 * y;
+      da_e4[2] = 4.0 * z2 * z;
+      break;
+    }
+    case MK_ANISO_HCP: {
+      const double h00 = 6.0 * e4 * (5.0 * x2 * x2 - 30.0 * x2 * y2 + 5.0 * y2 * y2);
+      H[0][0] = h00;
+      H[1][1] = -h00;
+      H[0][1] = H[1][0] = 6.0 * e4 * (-20.0 * x2 * x * y + 20.0 * x * y2 * y);
+      H[2][2] = 4.0 * e2;
+      *a_e4 = x2 * x2 * x2 - 15.0 * x2 * x2 * y2 + 15.0 * x2 * y2 * y2 - y2 * y2 * y2;
+      da_e4[0] = 6.0 * (x2 * x2 * x - 10.0 * x2 * x * y2 + 5.0 * x * y2 * y2);
+      da_e4[1] = -6.0 * (5.0 * x2 * x2 * y - 10.0 * x2 * y2 * y + y2 * y2 * y);
+      da_e4[2] = 0.0;
+      break;
+    }
+    case MK_ANISO_FACET: {
+      const double r[3] = {sqrt(x2 + e2 * e2), sqrt(y2 + e2 * e2), sqrt(z2 + e2 * e2)};
+      for (int q = 0; q < 3; ++q) {
+        H[q][q] = e4 * e2 * e2 / (r[q] * r[q] * r[q]);
+        da_e4[q] = n[q] / r[q];
+      }
+      *a_e4 = r[0] + r[1] + r[2] - sqrt(1.0 + e2 * e2) - 2.0 * e2;
+      break;
+    }
+    default: {
+      H[0][0] = 48.0 * e4 * x2;
+      H[1][1] = 48.0 * e4 * y2;
+      H[2][2] = 48.0 * e4 * z2;
+      *a_e4 = -3.0 + 4.0 * (x2 * x2 + y2 * y2 + z2 * z2);
+      da_e4[0] = 16.0 * x2 * x;
+      da_e4[1] = 16.0 * y2 * y;
+      da_e4[2] = 16.0 * z2 * z;
+      break;
+    }
+  }
+}
+
+// Reverse of anisotropy(): from the adjoints ab of a and Nb of N, adds the
+// adjoint of the lab gradient to gb and that of e4 to *e4b.
+void anisotropy_vjp(const double* R, int kind, double e4, double e2, const double g[3], double ab, const double Nb[3],
+                    double gb[3], double* e4b) {
+  const double gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  const double inv = 1.0 / (gn + 1e-12);
+  const double nl[3] = {g[0] * inv, g[1] * inv, g[2] * inv};
+  double nc[3];
+  for (int q = 0; q < 3; ++q) nc[q] = R[0 * 3 + q] * nl[0] + R[1 * 3 + q] * nl[1] + R[2 * 3 + q] * nl[2];
+  double a, da[3];
+  aniso_function(kind, e4, e2, nc, &a, da);
+  const double ndg = nc[0] * da[0] + nc[1] * da[1] + nc[2] * da[2];
+  // N = R Nc, Nc = gn a (da - nc ndg)
+  double Ncb[3];
+  for (int q = 0; q < 3; ++q) Ncb[q] = R[0 * 3 + q] * Nb[0] + R[1 * 3 + q] * Nb[1] + R[2 * 3 + q] * Nb[2];
+  double ct = 0, cn = 0;
+  for (int q = 0; q < 3; ++q) {
+    ct += Ncb[q] * (da[q] - nc[q] * ndg);
+    cn += Ncb[q] * nc[q];
+  }
+  double gnb = a * ct;
+  const double abt = ab + gn * ct;
+  double dab[3], ncb[3];
+  const double ndgb = -gn * a * cn;
+  for (int q = 0; q < 3; ++q) {
+    dab[q] = gn * a * Ncb[q] + ndgb * nc[q];
+    ncb[q] = -gn * a * Ncb[q] * ndg + ndgb * da[q];
+  }
+  // (a, da) = f(nc)
+  double H[3][3], a_e4, da_e4[3];
+  aniso_second(kind, e4, e2, nc, H, &a_e4, da_e4);
+  for (int q = 0; q < 3; ++q) ncb[q] += abt * da[q] + H[q][0] * dab[0] + H[q][1] * dab[1] + H[q][2] * dab[2];
+  *e4b += abt * a_e4 + dab[0] * da_e4[0] + dab[1] * da_e4[1] + dab[2] * da_e4[2];
+  // nc = R^T nl
+  double nlb[3];
+  for (int r = 0; r < 3; ++r) nlb[r] = R[r * 3 + 0] * ncb[0] + R[r * 3 + 1] * ncb[1] + R[r * 3 + 2] * ncb[2];
+  // nl = g inv, inv = 1/(gn + 1e-12), gn = |g|
+  const double invb = nlb[0] * g[0] + nlb[1] * g[1] + nlb[2] * g[2];
+  for (int q = 0; q < 3; ++q) gb[q] += inv * nlb[q];
+  gnb -= inv * inv * invb;
+  if (gn > 0)
+    for (int q = 0; q < 3; ++q) gb[q] += gnb * g[q] / gn;
+}
+
+// Transpose of propagate(): outb_k(y) = hlpb_k(y + e_k), or hlpb_inv(k)(y)
+// when y + e_k is not fluid.
+void propagate_adjoint(const orc_state* s, int Q, const std::vector<double>& hlpb, std::vector<double>& outb) {
+  const int64_t n = s->n;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int64_t c = cidx(s, x, y, z);
+        for (int i = 0; i < Q; ++i) {
+          if (s->flag[c] != MK_FLAG_FLUID) {
+            outb[(int64_t)i * n + c] = 0.0;
+            continue;
+          }
+          const int64_t d = nbr(s, x, y, z, E27[i][0], E27[i][1], E27[i][2]);
+          outb[(int64_t)i * n + c] = d >= 0 ? hlpb[(int64_t)i * n + d] : hlpb[(int64_t)inv_dir(i) * n + c];
+        }
+      }
+}
+
+struct AdjSnap {
+  std::vector<double> F, S, P, U;
+};
+
+}  // namespace
+
+// Loss L = sum (phi - target)^2 of phi after `steps` loops from the current
+// state, and dL/d eps4, dL/d Delta (a uniform shift of the initial u by
+// -Delta) and dL/d tau_T (omega_T = 1/tau_T; tau0 held fixed).  out = {L,
+// dL/deps4, dL/dDelta, dL/dtau_T}.  Thermal dendrite only; leaves the state
+// advanced by `steps` loops.
+extern "C" int orc_backward(orc_state* s, const double* target, int64_t steps, double* out) {
+  if (s->p.model != MK_MODEL_THERMAL_DENDRITE || steps < 1) return 1;
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  std::vector<AdjSnap> Y((size_t)steps + 1);
+  auto snap = [&](AdjSnap& y) {
+    y.F = s->f_out;
+    y.S = s->s_out;
+    y.P = s->phi;
+    y.U = s->temp;
+  };
+  snap(Y[0]);
+  for (int64_t t = 0; t < steps; ++t) {
+    thermal_dendrite_step(s);
+    s->step++;
+    snap(Y[(size_t)t + 1]);
+  }
+  double loss = 0;
+  std::vector<double> Pb(n), Ub(n, 0.0), Fb(7 * n, 0.0), Sb(7 * n, 0.0);
+  for (int64_t c = 0; c < n; ++c) {
+    const double d = s->phi[c] - target[c];
+    loss += d * d;
+    Pb[c] = 2.0 * d;
+  }
+  const double D0 = p.W0 * p.W0 / p.tau0;
+  const double om_g = 1.0 / (4.0 * D0 + 0.5);
+  const double om_t = 1.0 / (4.0 * p.D + 0.5);
+  const double cs2 = 0.25;
+  const double fo = (1.0 - 0.5 * om_g) / cs2;
+  double e4b = 0, omtb = 0;
+  std::vector<double> fh(7 * n), sh(7 * n), fhb(7 * n), shb(7 * n), phib(n), Pbn(n), Ubn(n), gbar(3 * n);
+  for (int64_t t = steps - 1; t >= 0; --t) {
+    const AdjSnap& y = Y[(size_t)t];
+    const std::vector<double>& phin = Y[(size_t)t + 1].P;  // phi^t
+    propagate(s, 7, y.F, fh);
+    propagate(s, 7, y.S, sh);
+    std::fill(fhb.begin(), fhb.end(), 0.0);
+    std::fill(shb.begin(), shb.end(), 0.0);
+    std::fill(Pbn.begin(), Pbn.end(), 0.0);
+    std::fill(Ubn.begin(), Ubn.end(), 0.0);
+    std::fill(gbar.begin(), gbar.end(), 0.0);
+    for (int64_t c = 0; c < n; ++c) phib[c] = Pb[c];  // the loop's phi^t becomes P
+    double e4_acc = 0, om_acc = 0;
+#pragma omp parallel for schedule(static) reduction(+ : e4_acc, om_acc)
+    for (int z = 0; z < s->nz; ++z)
+      for (int yy = 0; yy < s->ny; ++yy)
+        for (int x = 0; x < s->nx; ++x) {
+          const int64_t c = cidx(s, x, yy, z);
+          if (s->flag[c] != MK_FLAG_FLUID) continue;
+          // thermal relaxation t* = t - om_t (t - w T) + w dphi / 2, U' = T
+          double T = 0, Mt = 0;
+          for (int i = 0; i < 7; ++i) {
+            T += sh[(int64_t)i * n + c];
+            Mt += weight(7, i) * Sb[(int64_t)i * n + c];
+          }
+          for (int i = 0; i < 7; ++i) {
+            const double sbi = Sb[(int64_t)i * n + c];
+            shb[(int64_t)i * n + c] = (1.0 - om_t) * sbi + om_t * Mt + Ub[c];
+            om_acc += sbi * (weight(7, i) * T - sh[(int64_t)i * n + c]);
+          }
+          double dphib = 0.5 * Mt;
+          // phase-field relaxation
+          const double ph = phin[c];
+          const double dphi = ph - y.P[c];
+          const double u = y.U[c];
+          const double one_m = 1.0 - ph * ph;
+          double gr[3], lap;
+          grad_lap(
+              s, phin, x, yy, z, [](double p0) { return p0; }, gr, &lap);
+          const double* R = &s->rot[9 * s->grain[c]];
+          double a, N[3];
+          anisotropy(R, p.aniso, p.eps4, p.eps2, gr, &a, N);
+          double Mg = 0, Vg[3] = {0, 0, 0};
+          for (int i = 0; i < 7; ++i) {
+            const double fb = Fb[(int64_t)i * n + c];
+            const double w = weight(7, i);
+            Mg += w * fb;
+            for (int q = 0; q < 3; ++q) Vg[q] += w * E27[i][q] * fb;
+            fhb[(int64_t)i * n + c] = (1.0 - om_g) * fb;
+          }
+          const double src_phi = (1.0 - 3.0 * ph * ph + 4.0 * p.lambda * u * ph * one_m) / p.tau0;
+          double phb = om_g * Mg + Mg * src_phi;
+          Ubn[c] = -Mg * p.lambda * one_m * one_m / p.tau0;
+          dphib += (1.0 - a * a) * Mg;
+          phb += dphib;
+          Pbn[c] -= dphib;
+          const double beta[3] = {fo * Vg[0], fo * Vg[1], fo * Vg[2]};
+          const double bg = beta[0] * gr[0] + beta[1] * gr[1] + beta[2] * gr[2];
+          const double ab = -cs2 * 2.0 * a * bg - 2.0 * a * dphi * Mg;
+          const double Nb[3] = {-cs2 * beta[0], -cs2 * beta[1], -cs2 * beta[2]};
+          double gb[3] = {-cs2 * (a * a - 1.0) * beta[0], -cs2 * (a * a - 1.0) * beta[1],
+                          -cs2 * (a * a - 1.0) * beta[2]};
+          anisotropy_vjp(R, p.aniso, p.eps4, p.eps2, gr, ab, Nb, gb, &e4_acc);
+          for (int q = 0; q < 3; ++q) gbar[3 * c + q] = gb[q];
+          phib[c] += phb;
+        }
+    e4b += e4_acc;
+    omtb += om_acc;
+    // gr(x) = 3 sum_k w_k e_k phi~(x + e_k), phi~ = phi(x) at a non-fluid neighbour
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < s->nz; ++z)
+      for (int yy = 0; yy < s->ny; ++yy)
+        for (int x = 0; x < s->nx; ++x) {
+          const int64_t c = cidx(s, x, yy, z);
+          if (s->flag[c] != MK_FLAG_FLUID) continue;
+          double acc = 0;
+          for (int k = 1; k < 19; ++k) {
+            const double w3 = 3.0 * weight(19, k);
+            const int64_t src = nbr(s, x, yy, z, -E27[k][0], -E27[k][1], -E27[k][2]);
+            if (src >= 0)
+              acc += w3 * (E27[k][0] * gbar[3 * src] + E27[k][1] * gbar[3 * src + 1] + E27[k][2] * gbar[3 * src + 2]);
+            if (nbr(s, x, yy, z, E27[k][0], E27[k][1], E27[k][2]) < 0)
+              acc += w3 * (E27[k][0] * gbar[3 * c] + E27[k][1] * gbar[3 * c + 1] + E27[k][2] * gbar[3 * c + 2]);
+          }
+          phib[c] += acc;
+        }
+    // phi^t = sum of the streamed g (fluid), a copy of P (elsewhere)
+    for (int64_t c = 0; c < n; ++c) {
+      if (s->flag[c] == MK_FLAG_FLUID) {
+        for (int i = 0; i < 7; ++i) fhb[(int64_t)i * n + c] += phib[c];
+      } else {
+        Pbn[c] += phib[c];
+      }
+    }
+    propagate_adjoint(s, 7, fhb, Fb);
+    propagate_adjoint(s, 7, shb, Sb);
+    Pb.swap(Pbn);
+    Ub.swap(Ubn);
+  }
+  // initial state: S_i = w_i u0, U = u0, u0 = -Delta (fluid cells)
+  double sum_u = 0;
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    for (int i = 0; i < 7; ++i) sum_u += weight(7, i) * Sb[(int64_t)i * n + c];
+    sum_u += Ub[c];
+  }
+  out[0] = loss;
+  out[1] = e4b;
+  out[2] = -sum_u;
+  out[3] = -om_t * om_t * omtb;
+  return 0;
+}

@@ -109,6 +109,10 @@ int orc_get_field(const orc_state* s, int field, double* out);
 // Raw post-collision populations of lattice `which` (0 flow/phase, 1 second lattice).
 int orc_get_populations(const orc_state* s, int which, double* out);
 void orc_set_threads(int n);
+// Discrete adjoint of the thermal dendrite loop: L = sum (phi - target)^2 after
+// `steps` loops from the current state; out = {L, dL/deps4, dL/dDelta,
+// dL/dtau_T}.  Stores every state (small cases).  Returns 0 on success.
+int orc_backward(orc_state* s, const double* target, int64_t steps, double* out);
 // a(n) and da/dn of an anisotropy kind at the crystal-frame unit normal n (tests).
 void orc_anisotropy(int kind, double e4, double e2, const double* n, double* a, double* g);
 int orc_get_threads(void);

@@ -46,6 +46,8 @@ def load() -> C.CDLL:
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_get_threads.restype = C.c_int
         lib.orc_anisotropy.argtypes = [C.c_int, C.c_double, C.c_double, D, D, D]
+        lib.orc_backward.restype = C.c_int
+        lib.orc_backward.argtypes = [C.c_void_p, D, C.c_int64, D]
         _lib = lib
     return _lib
 
@@ -83,6 +85,15 @@ class Oracle:
     @property
     def step(self) -> int:
         return int(self.lib.orc_step(self.h))
+
+    def backward(self, target, steps: int) -> dict:
+        """Discrete adjoint: loss and its gradient after `steps` loops."""
+        t = np.ascontiguousarray(target, dtype=np.float64).ravel()
+        out = np.zeros(4)
+        rc = self.lib.orc_backward(self.h, _ptr(t), int(steps), _ptr(out))
+        if rc != 0:
+            raise RuntimeError("orc_backward failed")
+        return {"loss": out[0], "d_eps4": out[1], "d_delta": out[2], "d_tau_t": out[3]}
 
     def field(self, name: str) -> np.ndarray:
         p = self.params

@@ -260,3 +260,40 @@ def test_hcp_keeps_its_mirror_symmetries_and_differs_from_cubic(casedir):
         assert np.max(np.abs(phi - np.flip(phi, axis=ax))) < 1e-12
     # six-fold in the basal (x, y) plane: not symmetric under x <-> y, unlike a cubic crystal
     assert np.max(np.abs(phi - phi.transpose(0, 2, 1))) > 1e-6
+
+
+# ---------------------------------------------------------------- adjoint
+@pytest.mark.parametrize("aniso", ["cubic", "facet"])
+def test_oracle_adjoint_matches_central_differences(casedir, aniso):
+    # the discrete adjoint is the exact gradient of the discrete loop: central
+    # differences with h = 1e-4 agree to their O(h^2) truncation
+    n, steps, h = 10, 12, 1e-4
+    e2 = 0.03 if aniso != "cubic" else 0.0
+
+    def params(eps4, delta):
+        return _params(casedir, f"adj_{aniso}", cases.thermal_dendrite(n=n, loops=1, radius=3.0, eps4=eps4,
+                                                                        delta=delta, aniso=aniso, eps2=e2))
+
+    def phi_after(p):
+        o = Oracle(p, phi=initial_field(p, "phi"), T=initial_field(p, "T"))
+        o.advance(steps)
+        return o.field("phi")
+
+    target = phi_after(params(0.04, 0.50))
+    p0 = params(0.05, 0.55)
+    g = Oracle(p0, phi=initial_field(p0, "phi"), T=initial_field(p0, "T")).backward(target, steps)
+
+    def loss(p):
+        p.tau0 = p0.tau0  # tau_T and Delta derivatives hold tau0 fixed
+        return float(((phi_after(p) - target) ** 2).sum())
+
+    assert g["loss"] == pytest.approx(loss(params(0.05, 0.55)), rel=1e-13)
+    fd_e = (loss(params(0.05 + h, 0.55)) - loss(params(0.05 - h, 0.55))) / (2 * h)
+    fd_d = (loss(params(0.05, 0.55 + h)) - loss(params(0.05, 0.55 - h))) / (2 * h)
+    pp, pm = params(0.05, 0.55), params(0.05, 0.55)
+    pp.D += h / 4  # tau_T = 4 D + 1/2
+    pm.D -= h / 4
+    fd_t = (loss(pp) - loss(pm)) / (2 * h)
+    assert g["d_eps4"] == pytest.approx(fd_e, rel=1e-6)
+    assert g["d_delta"] == pytest.approx(fd_d, rel=1e-6)
+    assert g["d_tau_t"] == pytest.approx(fd_t, rel=1e-6)
