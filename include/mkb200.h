@@ -296,6 +296,29 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
 mk_status mk_host_alloc(size_t bytes, void** out);
 mk_status mk_host_free(void* p);
 
+/* ---- Gradients: discrete adjoint of the thermal dendrite loop -----------
+ * L = sum over cells of (phi - target)^2, phi after `steps` loops from the
+ * handle's current state.  Reverse mode over the loops the kernels run, with
+ * state checkpoints every `checkpoint_every` loops (<= 0: 100) and each
+ * segment recomputed forward.  Thermal dendrite cases, FP64 or FP32 storage;
+ * the adjoint arithmetic is FP64.  The handle is left at the state after the
+ * forward run (its step advanced by `steps`). */
+typedef struct mk_loss {
+  const double* target_phi; /* host, nx*ny*nz values, x fastest */
+  int64_t steps;
+  int64_t checkpoint_every;
+} mk_loss;
+
+typedef struct mk_grad {
+  double loss;
+  double d_eps4;   /* dL/d eps4 (the first anisotropy coefficient)                */
+  double d_delta;  /* dL/d Delta: the initial u shifted uniformly by -Delta         */
+  double d_tau_t;  /* dL/d tau_T, tau_T = 1/omega_T = 4 D + 1/2 (tau0 held fixed)   */
+  int64_t forward_loops; /* loops run forward: the first pass plus the recomputation */
+} mk_grad;
+
+mk_status mk_backward(mk_handle* h, const mk_loss* loss, mk_grad* out);
+
 /* ---- Ensembles: many dendrite domains advanced together ----------------
  * Batches unevenly sized domains (seed, anisotropy and undercooling sweeps of
  * run_solutal_dendrite / run_thermal_dendrite, MaterKit.cpp:633-687, 743-788)

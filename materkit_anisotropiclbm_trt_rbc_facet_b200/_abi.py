@@ -93,6 +93,15 @@ class MkDiag(C.Structure):
                 "max_speed": self.max_speed, "n_bad": self.n_bad}
 
 
+class MkLoss(C.Structure):
+    _fields_ = [("target_phi", C.POINTER(C.c_double)), ("steps", C.c_int64), ("checkpoint_every", C.c_int64)]
+
+
+class MkGrad(C.Structure):
+    _fields_ = [("loss", C.c_double), ("d_eps4", C.c_double), ("d_delta", C.c_double), ("d_tau_t", C.c_double),
+                ("forward_loops", C.c_int64)]
+
+
 H = C.c_void_p
 P = C.POINTER
 
@@ -127,6 +136,7 @@ PROTOTYPES = {
     "mk_autotune": (C.c_int, [H, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_double)]),
     "mk_host_alloc": (C.c_int, [C.c_size_t, P(C.c_void_p)]),
     "mk_host_free": (C.c_int, [C.c_void_p]),
+    "mk_backward": (C.c_int, [H, P(MkLoss), P(MkGrad)]),
     "mk_ensemble_case_params": (C.c_int, [C.c_uint64, C.c_int32, C.c_int32, P(MkParams)]),
     "mk_ensemble_create": (C.c_int, [P(MkParams), C.c_int32, P(H)]),
     "mk_ensemble_destroy": (C.c_int, [H]),

@@ -591,6 +591,24 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
   return MK_OK;
 }
 
+mk_status mk_backward(mk_handle* h, const mk_loss* loss, mk_grad* out) {
+  if (!h || !loss || !out || !loss->target_phi) return MK_ERR_ARG;
+  std::string err;
+  double r[5] = {0, 0, 0, 0, 0};
+  cudaError_t st = mke::engine_backward(h->e, loss->target_phi, loss->steps, loss->checkpoint_every, r, err);
+  if (st == cudaErrorInvalidValue && !err.empty()) {
+    h->err = err;
+    return MK_ERR_ARG;
+  }
+  if (st != cudaSuccess) return cuda_fail(h, st, "backward");
+  out->loss = r[0];
+  out->d_eps4 = r[1];
+  out->d_delta = r[2];
+  out->d_tau_t = r[3];
+  out->forward_loops = (int64_t)r[4];
+  return MK_OK;
+}
+
 mk_status mk_host_alloc(size_t bytes, void** out) {
   if (!out) return set_global(MK_ERR_ARG, "null argument");
   cudaError_t st = cudaHostAlloc(out, bytes, cudaHostAllocDefault);

@@ -110,6 +110,13 @@ size_t engine_pop_bytes(const Engine& e, int which);
 
 double engine_bytes_per_cell(const Engine& e);
 
+// Discrete adjoint of `steps` thermal dendrite loops from the current state
+// with checkpoints every `every` loops (<= 0: 100).  out = {loss, dL/deps4,
+// dL/dDelta, dL/dtau_T, forward loops run}.  Leaves the state after the
+// forward run.  cudaErrorInvalidValue with `err` set for unsupported cases.
+cudaError_t engine_backward(Engine& e, const double* h_target, int64_t steps, int64_t every, double* out,
+                            std::string& err);
+
 }  // namespace mke
 
 #endif

@@ -282,6 +282,19 @@ class Solver:
         _check(self._lib.mk_time_advance(self._h, int(nsteps), 1 if graph else 0, C.byref(ms)), self._h)
         return ms.value
 
+    def backward(self, target_phi, steps: int, checkpoint_every: int = 100) -> dict:
+        """Discrete adjoint of `steps` thermal dendrite loops from the current
+        state: L = sum (phi - target)^2 and dL/d eps4, dL/d Delta, dL/d tau_T.
+        Leaves the state after the forward run."""
+        t = np.ascontiguousarray(target_phi, dtype=np.float64).ravel()
+        if t.size != self.params.ncell():
+            raise ValueError("target_phi must have one value per cell")
+        loss = A.MkLoss(t.ctypes.data_as(C.POINTER(C.c_double)), int(steps), int(checkpoint_every))
+        g = A.MkGrad()
+        _check(self._lib.mk_backward(self._h, C.byref(loss), C.byref(g)), self._h)
+        return {"loss": g.loss, "d_eps4": g.d_eps4, "d_delta": g.d_delta, "d_tau_t": g.d_tau_t,
+                "forward_loops": g.forward_loops}
+
     def autotune(self, trial_steps: int = 4) -> dict:
         """Pick the fastest launch shape / occupancy variant; the state is left unchanged."""
         bx, by, mb, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()

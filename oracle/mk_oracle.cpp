@@ -854,6 +854,14 @@ void aniso_second(int kind, double e4, double e2, const double n[3], double H[3]
   }
 }
 
+// Below this |grad phi| the normal n = grad phi / (|grad phi| + 1e-12) is
+// rounding noise, and its exact derivative (~1 / (|grad phi| + 1e-12)) makes
+// the adjoint of the (1 - a^2) dphi source grow without bound over long runs
+// (measured: 1e32 after 2000 loops at 96^3, while central differences stay
+// near 3e5).  There the reverse sweep keeps the direct eps4 derivative of a
+// and N and drops their derivative through n.
+const double kAdjGradCut = 1e-8;
+
 // Reverse of anisotropy(): from the adjoints ab of a and Nb of N, adds the
 // adjoint of the lab gradient to gb and that of e4 to *e4b.
 void anisotropy_vjp(const double* R, int kind, double e4, double e2, const double g[3], double ab, const double Nb[3],
@@ -887,6 +895,7 @@ void anisotropy_vjp(const double* R, int kind, double e4, double e2, const doubl
   aniso_second(kind, e4, e2, nc, H, &a_e4, da_e4);
   for (int q = 0; q < 3; ++q) ncb[q] += abt * da[q] + H[q][0] * dab[0] + H[q][1] * dab[1] + H[q][2] * dab[2];
   *e4b += abt * a_e4 + dab[0] * da_e4[0] + dab[1] * da_e4[1] + dab[2] * da_e4[2];
+  if (gn < kAdjGradCut) return;
   // nc = R^T nl
   double nlb[3];
   for (int r = 0; r < 3; ++r) nlb[r] = R[r * 3 + 0] * ncb[0] + R[r * 3 + 1] * ncb[1] + R[r * 3 + 2] * ncb[2];
