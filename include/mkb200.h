@@ -59,7 +59,10 @@ typedef enum mk_model {
   MK_MODEL_FLOW = 0,             /* single-phase flow, run_flow_Poiseuille (MaterKit.cpp:244-288) */
   MK_MODEL_MULTIPHASE = 1,       /* Allen-Cahn two-phase flow, run_flow_multiphase (:290-331)     */
   MK_MODEL_THERMAL_DENDRITE = 2, /* phase field + thermal ADE, run_thermal_dendrite (:743-788)    */
-  MK_MODEL_SOLUTAL_DENDRITE = 3  /* phase field + solutal ADE, run_solutal_dendrite (:633-687)    */
+  MK_MODEL_SOLUTAL_DENDRITE = 3, /* phase field + solutal ADE, run_solutal_dendrite (:633-687)    */
+  MK_MODEL_CONVECTION = 4        /* flow + advected D3Q7 scalar with Boussinesq buoyancy and
+                                    Dirichlet plates: Rayleigh-Benard (bdy_RBC, Thermal_NusseltRBC,
+                                    mkThermalField.h:33-40, mkFluidsLBM.h:59-68)                  */
 } mk_model;
 
 /* Population storage precision.  Collision arithmetic is FP64 for MK_PREC_FP64
@@ -270,6 +273,12 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir);
 
 /* FP64 conservation sums and the divergence watchdog. */
 mk_status mk_diagnostics(mk_handle* h, mk_diag* out);
+
+/* Nusselt number of a convection case (Thermal_NusseltRBC, mkFluidsLBM.h:67):
+ * Nu = 1 + <u_a T> H / (kappa (T_low - T_high)), the volume average over the
+ * fluid cells, a the plate axis, H the layer thickness between the half-way
+ * plates, kappa the scalar diffusivity D.  FP64 reduction. */
+mk_status mk_nusselt(mk_handle* h, double* nu);
 
 /* Binary checkpoint: populations, phi, step and a parameter hash. */
 mk_status mk_checkpoint(mk_handle* h, const char* path);

@@ -125,6 +125,52 @@ def multiphase_bubbles(n=256, nz=None, loops=10000, precision="fp32", bubbles=24
 """
 
 
+def convection(nx=64, ny=3, nz=34, axis="z", Ra=1e4, Pr=0.71, U=0.05, T_hot=1.0, T_cold=0.0, loops=20000,
+               precision="fp64", collision="TRT", lattice="D3Q19", beta=None) -> str:
+    """Rayleigh-Benard convection: hot plate below, cold plate above along `axis`
+    (walls there, periodic elsewhere), gravity g = 1 along -axis.  The free-fall
+    velocity U = sqrt(g beta dT H) sets the Mach number; then
+    nu = U H sqrt(Pr/Ra), kappa = nu/Pr, tau = 3 nu + 1/2, H the layer
+    thickness between the half-way plates.  `beta` overrides the expansion
+    coefficient (0: pure conduction)."""
+    a = "xyz".index(axis)
+    n3 = [nx, ny, nz]
+    H = n3[a] - 2
+    dT = T_hot - T_cold
+    nu = U * H * (Pr / Ra) ** 0.5
+    kappa = nu / Pr
+    tau = 3.0 * nu + 0.5
+    beta = U * U / (dT * H) if beta is None else beta
+    g = [0.0, 0.0, 0.0]
+    g[a] = -1.0
+    bc = ["periodic"] * 3
+    bc[a] = "walls"
+    return _HEADER.format(dendrite="false", flow="true", loops=loops, frames=min(loops, 100), nx=nx, ny=ny, nz=nz) + f"""
+  <b200>
+    <model> convection </model> <lattice> {lattice} </lattice> <collision> {collision} </collision>
+    <precision> {precision} </precision> <boundary> {" ".join(bc)} </boundary>
+    <tau> {tau} </tau> <magic> 0.1875 </magic> <rho0> 1.0 </rho0> <diffusivity> {kappa} </diffusivity>
+    <force> {g[0]} {g[1]} {g[2]} </force> <beta> {beta} </beta> <sRef> {0.5 * (T_hot + T_cold)} </sRef>
+    <wallAxis> {axis} </wallAxis> <wallValue> {T_hot} {T_cold} </wallValue>
+  </b200>
+</MaterKit>
+"""
+
+
+def couette(nx=4, ny=18, nz=4, U=1e-2, loops=20000, precision="fp64", collision="TRT", lattice="D3Q19",
+            tau=0.8) -> str:
+    """Plane Couette flow: plates normal to y, the upper one moving with U along x."""
+    return _HEADER.format(dendrite="false", flow="true", loops=loops, frames=min(loops, 100), nx=nx, ny=ny, nz=nz) + f"""
+  <b200>
+    <model> flow </model> <lattice> {lattice} </lattice> <collision> {collision} </collision>
+    <precision> {precision} </precision> <boundary> periodic walls periodic </boundary>
+    <tau> {tau} </tau> <magic> 0.1875 </magic> <rho0> 1.0 </rho0> <force> 0 0 0 </force>
+    <wallAxis> y </wallAxis> <wallVelocity> 0 0 0 {U} 0 0 </wallVelocity>
+  </b200>
+</MaterKit>
+"""
+
+
 def write(text: str, path: str) -> str:
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
     with open(path, "w") as f:

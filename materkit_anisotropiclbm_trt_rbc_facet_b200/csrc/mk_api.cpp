@@ -137,13 +137,14 @@ mk_status mk_create(const mk_params* p, mk_handle** out) {
   }
   // initial state (initialize + initialize_geometry)
   const size_t n = (size_t)h->e.ncell;
-  const bool flow = p->model == MK_MODEL_FLOW;
-  const bool dend = p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE;
-  std::vector<double> phi(flow ? 0 : n), temp(dend ? n : 0), rho(flow ? n : 0);
+  const bool flow = p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION;
+  const bool scalar = p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
+                      p->model == MK_MODEL_CONVECTION;
+  std::vector<double> phi(flow ? 0 : n), temp(scalar ? n : 0), rho(flow ? n : 0);
   if (!flow) mkc::initial_field(p, MK_FIELD_PHI, phi.data(), n, err);
-  if (dend) mkc::initial_field(p, MK_FIELD_T, temp.data(), n, err);
+  if (scalar) mkc::initial_field(p, MK_FIELD_T, temp.data(), n, err);
   if (flow) mkc::initial_field(p, MK_FIELD_RHO, rho.data(), n, err);
-  st = mke::engine_set_state(h->e, flow ? nullptr : phi.data(), dend ? temp.data() : nullptr,
+  st = mke::engine_set_state(h->e, flow ? nullptr : phi.data(), scalar ? temp.data() : nullptr,
                              flow ? rho.data() : nullptr, nullptr, nullptr, nullptr);
   if (st != cudaSuccess) {
     mk_status r = cuda_fail(h, st, "initialise");
@@ -325,7 +326,7 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   std::vector<double> rho(n, 1.0), grain(n, 0.0), phi(n, 0.0), dphi(n, 0.0), conc(n, 0.0), temp(n, 0.0), ux(n, 0.0),
       uy(n, 0.0), uz(n, 0.0);
   mk_status s;
-  if (m == MK_MODEL_FLOW || m == MK_MODEL_MULTIPHASE) {
+  if (m == MK_MODEL_FLOW || m == MK_MODEL_MULTIPHASE || m == MK_MODEL_CONVECTION) {
     if ((s = copy_field(h, MK_FIELD_RHO, rho)) != MK_OK) return s;
     if ((s = copy_field(h, MK_FIELD_UX, ux)) != MK_OK) return s;
     if ((s = copy_field(h, MK_FIELD_UY, uy)) != MK_OK) return s;
@@ -333,6 +334,7 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   }
   if ((s = copy_field(h, MK_FIELD_GRAIN, grain)) != MK_OK) return s;
   if ((s = copy_field(h, MK_FIELD_PHI, phi)) != MK_OK) return s;
+  if (m == MK_MODEL_CONVECTION && (s = copy_field(h, MK_FIELD_T, temp)) != MK_OK) return s;
   if (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE) {
     if ((s = copy_field(h, MK_FIELD_DPHI, dphi)) != MK_OK) return s;
     if ((s = copy_field(h, m == MK_MODEL_THERMAL_DENDRITE ? MK_FIELD_T : MK_FIELD_C,
@@ -410,6 +412,30 @@ mk_status mk_diagnostics(mk_handle* h, mk_diag* out) {
     h->err = "diverged: non-finite or non-positive state in " + std::to_string(out->n_bad) + " cells";
     return MK_ERR_DIVERGED;
   }
+  return MK_OK;
+}
+
+mk_status mk_nusselt(mk_handle* h, double* nu) {
+  if (!h || !nu) return MK_ERR_ARG;
+  const mk_params& p = h->e.p;
+  if (p.model != MK_MODEL_CONVECTION) {
+    h->err = "Nusselt number: convection cases only";
+    return MK_ERR_ARG;
+  }
+  const double dT = p.wall_value[0] - p.wall_value[1];
+  if (dT == 0.0) {
+    h->err = "Nusselt number: the plates hold the same value";
+    return MK_ERR_ARG;
+  }
+  double v[mke::DG_N];
+  cudaError_t st = mke::engine_diag(h->e, v);
+  if (st != cudaSuccess) return cuda_fail(h, st, "nusselt");
+  const int a = p.wall_axis;
+  const int n3[3] = {p.nx, p.ny, p.nz};
+  const double H = p.bc[a] == MK_BC_WALLS ? n3[a] - 2 : n3[a];
+  // Nu = 1 + <u_a T> H / (kappa dT): the convective part of the heat flux
+  // across the layer over the conductive flux kappa dT / H
+  *nu = 1.0 + (v[mke::DG_FLUX] / v[mke::DG_FLUID]) * H / (p.D * dT);
   return MK_OK;
 }
 

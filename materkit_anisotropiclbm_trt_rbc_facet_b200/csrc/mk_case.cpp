@@ -11,6 +11,7 @@
 // overrides all of the above.
 #include "mk_case.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -222,7 +223,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model < 0 || p->model > 3) {
+  if (p->model < 0 || p->model > 4) {
     err = "unknown model";
     return MK_ERR_ARG;
   }
@@ -230,7 +231,29 @@ mk_status validate_params(const mk_params* p, std::string& err) {
     err = "unknown precision";
     return MK_ERR_ARG;
   }
-  if (p->model == MK_MODEL_FLOW) {
+  if (p->wall_axis < -1 || p->wall_axis > 2) {
+    err = "wall_axis must be -1, 0, 1 or 2";
+    return MK_ERR_ARG;
+  }
+  if (p->wall_axis >= 0 && p->bc[p->wall_axis] != MK_BC_WALLS) {
+    err = "the plate axis must have walled faces";
+    return MK_ERR_ARG;
+  }
+  if (p->wall_axis >= 0 && p->model != MK_MODEL_FLOW && p->model != MK_MODEL_CONVECTION) {
+    err = "plates (wall_axis) apply to the flow and convection models";
+    return MK_ERR_ARG;
+  }
+  if (p->model == MK_MODEL_CONVECTION) {
+    if (!(p->D > 0)) {
+      err = "convection needs a positive scalar diffusivity";
+      return MK_ERR_ARG;
+    }
+    if (p->wall_axis < 0) {
+      err = "convection needs a plate axis (wall_axis)";
+      return MK_ERR_ARG;
+    }
+  }
+  if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) {
     if (p->lattice != MK_D3Q19 && p->lattice != MK_D3Q27) {
       err = "flow lattice must be D3Q19 or D3Q27";
       return MK_ERR_ARG;
@@ -334,6 +357,8 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       model = MK_MODEL_THERMAL_DENDRITE;
     else if (m == "solutal_dendrite" || m == "solutal")
       model = MK_MODEL_SOLUTAL_DENDRITE;
+    else if (m == "convection" || m == "rbc" || m == "rayleigh_benard")
+      model = MK_MODEL_CONVECTION;
     else {
       err = "<b200><model>: unknown model '" + m + "'";
       return MK_ERR_XML;
@@ -351,7 +376,31 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
   // --- physical-unit tags of the shipped cases
   double omega_f = -1;
   if (!opt_d(r, "numerics/omega_f", omega_f, err)) return MK_ERR_XML;
-  if (model == MK_MODEL_FLOW) {
+  if (model == MK_MODEL_CONVECTION) {
+    // Rayleigh-Benard (bdy_RBC, mkFluidsUser.cpp:362-392): gravity from
+    // geometry/Gravity, the expansion coefficient from temperature/beta,
+    // plates normal to y (the reference's bdy_RBC) holding
+    // composition/highValue at y = 0 and composition/lowValue at y = My-1
+    double nu = -1, alpha = -1, beta = 0, hi = 1.0, lo = 0.0;
+    if (!opt_d(r, "phases/fluid/kinematicViscosity", nu, err) || !opt_d(r, "temperature/alphaFluid", alpha, err) ||
+        !opt_d(r, "temperature/beta", beta, err) || !opt_d(r, "composition/highValue", hi, err) ||
+        !opt_d(r, "composition/lowValue", lo, err))
+      return MK_ERR_XML;
+    if (nu > 0) p.tau = 3.0 * nu * dt / (dx * dx) + 0.5;
+    if (omega_f > 0) p.tau = 1.0 / omega_f;
+    if (alpha > 0) p.D = alpha * dt / (dx * dx);
+    p.beta = beta;
+    p.rho0 = 1.0;
+    for (int a = 0; a < 3; ++a) p.force[a] = g_lu[a];
+    p.bc[0] = MK_BC_PERIODIC;
+    p.bc[1] = MK_BC_WALLS;
+    p.bc[2] = MK_BC_PERIODIC;
+    p.wall_axis = 1;
+    p.wall_value[0] = hi;
+    p.wall_value[1] = lo;
+    p.s_ref = 0.5 * (hi + lo);
+    p.collision = MK_COLL_TRT;
+  } else if (model == MK_MODEL_FLOW) {
     double nu = -1, rho = 1.0;
     if (!opt_d(r, "phases/fluid/kinematicViscosity", nu, err)) return MK_ERR_XML;
     if (nu > 0) p.tau = 3.0 * nu * dt / (dx * dx) + 0.5;
@@ -532,6 +581,42 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       if (!opt_v(b, "velocity", v, err)) return MK_ERR_XML;
       for (int a = 0; a < 3; ++a) p.u0[a] = a < (int)v.size() ? v[a] : 0.0;
     }
+    if (const mkx::Element* e = b->child("wallAxis")) {
+      const std::string t = lower(mkx::trimmed(e->text));
+      if (t == "x" || t == "0")
+        p.wall_axis = 0;
+      else if (t == "y" || t == "1")
+        p.wall_axis = 1;
+      else if (t == "z" || t == "2")
+        p.wall_axis = 2;
+      else if (t == "none" || t == "-1")
+        p.wall_axis = -1;
+      else {
+        err = "<b200><wallAxis>: unknown '" + t + "'";
+        return MK_ERR_XML;
+      }
+    }
+    if (b->child("wallValue")) {
+      if (!opt_v(b, "wallValue", v, err)) return MK_ERR_XML;
+      if (v.size() != 2) {
+        err = "<b200><wallValue> needs 2 values (low plate, high plate)";
+        return MK_ERR_XML;
+      }
+      p.wall_value[0] = v[0];
+      p.wall_value[1] = v[1];
+    }
+    if (b->child("wallVelocity")) {
+      if (!opt_v(b, "wallVelocity", v, err)) return MK_ERR_XML;
+      if (v.size() != 6) {
+        err = "<b200><wallVelocity> needs 6 values (low plate xyz, high plate xyz)";
+        return MK_ERR_XML;
+      }
+      for (int a = 0; a < 3; ++a) {
+        p.wall_u[0][a] = v[a];
+        p.wall_u[1][a] = v[3 + a];
+      }
+    }
+    if (!opt_d(b, "beta", p.beta, err) || !opt_d(b, "sRef", p.s_ref, err)) return MK_ERR_XML;
     if (const mkx::Element* o = b->child("objects")) {
       if (!read_seeds(o, &p, err)) return MK_ERR_XML;
     }
@@ -602,11 +687,24 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
           case MK_FIELD_UX:
           case MK_FIELD_UY:
           case MK_FIELD_UZ:
-            v = p->model == MK_MODEL_FLOW ? p->u0[field - MK_FIELD_UX] : 0.0;
+            v = (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) ? p->u0[field - MK_FIELD_UX] : 0.0;
             break;
           case MK_FIELD_T:
           case MK_FIELD_C:
-            v = -p->delta;
+            if (p->model == MK_MODEL_CONVECTION) {
+              // conduction profile between the plates (walls half a cell
+              // outside the fluid span) plus one convection-roll mode of
+              // amplitude 1e-2 (T_low - T_high) along the first other axis
+              const int a = p->wall_axis, b = a == 0 ? 1 : 0;
+              const int lo = p->bc[a] == MK_BC_WALLS ? 1 : 0, hi = p->bc[a] == MK_BC_WALLS ? n3[a] - 2 : n3[a] - 1;
+              const double H = hi - lo + 1;
+              const double sa = std::min(1.0, std::max(0.0, (pos[a] - lo + 0.5) / H));
+              const double dT = p->wall_value[0] - p->wall_value[1];
+              v = p->wall_value[0] - dT * sa +
+                  1e-2 * dT * std::sin(M_PI * sa) * std::cos(2.0 * M_PI * pos[b] / n3[b]);
+            } else {
+              v = -p->delta;
+            }
             break;
           case MK_FIELD_PRESSURE:
           case MK_FIELD_DPHI:
@@ -632,7 +730,7 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
           case MK_FIELD_PHI:
             if (p->model == MK_MODEL_MULTIPHASE) {
               v = bubble_phi(p, pos, n3);
-            } else if (p->model == MK_MODEL_FLOW) {
+            } else if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) {
               v = 0.0;
             } else {
               // solid seeds (phi = +1) in liquid (phi = -1): -tanh((r - R)/(sqrt(2) W0))

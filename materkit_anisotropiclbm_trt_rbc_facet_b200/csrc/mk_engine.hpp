@@ -26,6 +26,7 @@ enum {
   DG_MAXU,
   DG_BAD,
   DG_FLUID,
+  DG_FLUX,  // sum of u_axis T (convection: the convective heat flux across the plates)
   DG_N
 };
 

@@ -40,18 +40,11 @@ struct FlowK {
   T ref;  // rho0
 };
 
-template <class S, int Q, int COLL, int PARITY>
-__global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, const FlowK<typename Stor<S>::T> k) {
-  typedef typename Stor<S>::T T;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const Nbr nb(g, x, y, z);
-  const int c = nb.idx(0, 0, 0);
-  T f[Q];  // deviations f_i - w_i rho0
-#pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(A, g.stride, nb, PARITY, c, i);
+// Moments, velocity (half-force corrected) and collision of one cell's Q
+// deviations f_i - w_i rho0 in place, with the Guo force F.
+template <class T, int Q, int COLL>
+__device__ __forceinline__ void flow_relax(T (&f)[Q], const FlowK<T>& k, const T Fx, const T Fy, const T Fz, T& ux,
+                                           T& uy, T& uz) {
   T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
@@ -61,9 +54,9 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
     if (ez(i)) jz += T(ez(i)) * f[i];
   }
   const T rho = k.ref + drho;
-  const T ux = (jx + T(0.5) * k.Fx) / rho;
-  const T uy = (jy + T(0.5) * k.Fy) / rho;
-  const T uz = (jz + T(0.5) * k.Fz) / rho;
+  ux = (jx + T(0.5) * Fx) / rho;
+  uy = (jy + T(0.5) * Fy) / rho;
+  uz = (jz + T(0.5) * Fz) / rho;
   const T uu = ux * ux + uy * uy + uz * uz;
   if constexpr (COLL == MK_COLL_MRT && Q == 19) {
     MrtIn<T> q;  // equilibrium deviation: w [drho + rho (3eu + 4.5(eu)^2 - 1.5u^2)]
@@ -77,26 +70,24 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
     q.qxy = rho * ux * uy;
     q.qxz = rho * ux * uz;
     q.qyz = rho * uy * uz;
-    q.Fx = k.Fx;
-    q.Fy = k.Fy;
-    q.Fz = k.Fz;
+    q.Fx = Fx;
+    q.Fy = Fy;
+    q.Fz = Fz;
     q.ux = ux;
     q.uy = uy;
     q.uz = uz;
     q.sF = T(1);
     q.s_nu = k.om;
     mrt19_collide_moments<T>(f, q);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i]);
     return;
   }
-  const T uF = ux * k.Fx + uy * k.Fy + uz * k.Fz;
+  const T uF = ux * Fx + uy * Fy + uz * Fz;
   T feq[Q], Fi[Q];  // equilibrium deviations and Guo force terms
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const T w = T(wq<Q>(i));
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
-    const T eF = T(ex(i)) * k.Fx + T(ey(i)) * k.Fy + T(ez(i)) * k.Fz;
+    const T eF = T(ex(i)) * Fx + T(ey(i)) * Fy + T(ez(i)) * Fz;
     feq[i] = w * (drho + rho * (T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu));
     Fi[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF);
   }
@@ -117,8 +108,110 @@ __global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, c
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = fo[i];
   }
+}
+
+template <class S, int Q, int COLL, int PARITY>
+__global__ void __launch_bounds__(256) k_flow(S* __restrict__ A, const Geom g, const FlowK<typename Stor<S>::T> k) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const Nbr nb(g, x, y, z);
+  const int c = nb.idx(0, 0, 0);
+  T f[Q];  // deviations f_i - w_i rho0
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(A, g.stride, nb, PARITY, c, i);
+  T ux, uy, uz;
+  flow_relax<T, Q, COLL>(f, k, k.Fx, k.Fy, k.Fz, ux, uy, uz);
 #pragma unroll
   for (int i = 0; i < Q; ++i) st_out<S, Q>(A, g.stride, nb, PARITY, c, i, f[i]);
+}
+
+// ================================================== CONVECTION (RBC, a3/a7)
+// Flow lattice with the Boussinesq force F = -rho0 beta (T - T_ref) g and a
+// D3Q7 advection-diffusion lattice t_eq = w T (1 + 4 e.u) (mkThermalField
+// relaxation with the flow's velocity), both held as deviations (f - w rho0,
+// t - w T_ref).  Populations bounced at a plate of `axis` get the plate's
+// correction on read: + 6 w rho0 e.u_w for the flow (a moving wall; Couette,
+// bdyCouette), t -> -t + 2 w (T_w - T_ref) for the scalar (Dirichlet anti-
+// bounce-back; bdy_constT / bdy_RBC).  SCALAR = false is the flow model with
+// moving plates and its constant body force.
+template <class T>
+struct ConvK {
+  FlowK<T> f;       // om, om_m, Fx..Fz (flow model body force), ref = rho0
+  T om_t, ref_t;    // scalar relaxation rate and rest value (T_ref)
+  T bg[3];          // -rho0 beta g
+  T tw2[2];         // 2 (T_w - T_ref) of the low / high plate
+  T uw6[2][3];      // 6 rho0 u_w of the low / high plate
+  int axis, lo, hi; // plate axis and the fluid span on it
+};
+
+__device__ __forceinline__ int e_on(int i, int axis) { return axis == 0 ? ex(i) : (axis == 1 ? ey(i) : ez(i)); }
+
+template <class S, int Q, int COLL, int PARITY, bool SCALAR, bool WALLS, class NB>
+__device__ __forceinline__ void conv_cell(S* __restrict__ F, S* __restrict__ Tp, const int64_t stride, const NB& nb,
+                                          const int c, const int coord, const ConvK<typename Stor<S>::T>& k) {
+  typedef typename Stor<S>::T T;
+  T f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    f[i] = ld_in<S, Q>(F, stride, nb, PARITY, c, i);
+    if (WALLS && !nb_fluid(nb, -ex(i), -ey(i), -ez(i))) {
+      const int ea = e_on(i, k.axis);
+      const int p = coord - ea;
+      const int side = ea == 0 ? -1 : (p < k.lo ? 0 : (p > k.hi ? 1 : -1));
+      if (side >= 0)
+        f[i] += T(wq<Q>(i)) * (T(ex(i)) * k.uw6[side][0] + T(ey(i)) * k.uw6[side][1] + T(ez(i)) * k.uw6[side][2]);
+    }
+  }
+  T t[7], dT = T(0);
+  if constexpr (SCALAR) {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
+      if (WALLS && !nb_fluid(nb, -ex(i), -ey(i), -ez(i))) {
+        const int ea = e_on(i, k.axis);
+        const int p = coord - ea;
+        const int side = ea == 0 ? -1 : (p < k.lo ? 0 : (p > k.hi ? 1 : -1));
+        if (side >= 0) t[i] = -t[i] + T(wq<7>(i)) * k.tw2[side];
+      }
+      dT += t[i];
+    }
+  }
+  T ux, uy, uz;
+  if constexpr (SCALAR)
+    flow_relax<T, Q, COLL>(f, k.f, k.bg[0] * dT, k.bg[1] * dT, k.bg[2] * dT, ux, uy, uz);
+  else
+    flow_relax<T, Q, COLL>(f, k.f, k.f.Fx, k.f.Fy, k.f.Fz, ux, uy, uz);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) st_out<S, Q>(F, stride, nb, PARITY, c, i, f[i]);
+  if constexpr (SCALAR) {
+    const T Tabs = k.ref_t + dT;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      const T w = T(wq<7>(i));
+      const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, t[i] - k.om_t * (t[i] - w * (dT + T(4) * Tabs * eu)));
+    }
+  }
+}
+
+template <class S, int Q, int COLL, int PARITY, bool SCALAR>
+__global__ void __launch_bounds__(256)
+    k_conv(S* __restrict__ F, S* __restrict__ Tp, const Geom g, const ConvK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int coord = k.axis == 0 ? x : (k.axis == 1 ? y : z);
+  if (fast_cell(g, x, y, z)) {
+    const Fast fa = make_fast(g, x, y, z);
+    conv_cell<S, Q, COLL, PARITY, SCALAR, false>(F, Tp, g.stride, fa, fa.c, coord, k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    conv_cell<S, Q, COLL, PARITY, SCALAR, true>(F, Tp, g.stride, nb, nb.idx(0, 0, 0), coord, k);
+  }
 }
 
 // ========================================================= MULTIPHASE (K4)
@@ -340,12 +433,21 @@ __global__ void k_init(int model, int Q0, S* A0, S* A1, float* H0, typename PhiO
   if (!g.fluid(x, y, z)) return;
   const Nbr nb(g, x, y, z);
   const int ci = (int)c;
-  if (model == MK_MODEL_FLOW) {
+  if (model == MK_MODEL_FLOW || model == MK_MODEL_CONVECTION) {
     const double r = in_rho ? in_rho[c] : d_rho;
     if (Q0 == 19)
       put_eq<S, 19>(A0, g, nb, ci, r, ux, uy, uz, 0.0, refs.r0);
     else
       put_eq<S, 27>(A0, g, nb, ci, r, ux, uy, uz, 0.0, refs.r0);
+    if (model == MK_MODEL_CONVECTION) {
+      // t_eq = w T (1 + 4 e.u), held as t - w T_ref
+#pragma unroll
+      for (int i = 0; i < 7; ++i) {
+        const double eu = ex(i) * ux + ey(i) * uy + ez(i) * uz;
+        st_layout<S, 7>(A1, g.stride, nb, 0, ci, i,
+                        typename Stor<S>::T(wq<7>(i) * ((tv - refs.r1) + 4.0 * tv * eu)));
+      }
+    }
   } else if (model == MK_MODEL_MULTIPHASE) {
     // g = geq(p* = 0, u) = w (3eu + 4.5eu^2 - 1.5u^2); h = phi w (1 + ...)
     put_eq<S, 19>(A0, g, nb, ci, 1.0, ux, uy, uz, -1.0, refs.r0);
@@ -358,19 +460,45 @@ __global__ void k_init(int model, int Q0, S* A0, S* A1, float* H0, typename PhiO
 }
 
 // =================================================================== FIELDS
+// Buoyancy coefficients of the stored scalar (convection): F = bg (T - T_ref).
+struct Buoy {
+  double bg[3], ref;
+};
+
+// Stored (post-collision) scalar T of a convection cell.
+template <class S>
+__device__ __forceinline__ double conv_T(const S* __restrict__ Tp, const Geom& g, const Nbr& nb, int64_t steps_done,
+                                         int c, double ref) {
+  double t = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) t += double(ld_out<S, 7>(Tp, g.stride, nb, steps_done, c, i));
+  return ref + t;
+}
+
 template <class S, int Q>
-__global__ void k_field_flow(const S* __restrict__ A, const Geom g, int64_t steps_done, int field, double Fx, double Fy,
-                             double Fz, double rho0, double* __restrict__ out) {
+__global__ void k_field_flow(const S* __restrict__ A, const S* __restrict__ Tp, const Buoy bu, const Geom g,
+                             int64_t steps_done, int field, double Fx, double Fy, double Fz, double rho0,
+                             double* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
   const int64_t c = g.idx(x, y, z);
   if (!g.fluid(x, y, z)) {
-    out[c] = field == MK_FIELD_RHO ? rho0 : 0.0;
+    out[c] = field == MK_FIELD_RHO ? rho0 : (field == MK_FIELD_T ? bu.ref : 0.0);
     return;
   }
   const Nbr nb(g, x, y, z);
+  if (Tp) {
+    const double T = conv_T<S>(Tp, g, nb, steps_done, (int)c, bu.ref);
+    if (field == MK_FIELD_T) {
+      out[c] = T;
+      return;
+    }
+    Fx = bu.bg[0] * (T - bu.ref);
+    Fy = bu.bg[1] * (T - bu.ref);
+    Fz = bu.bg[2] * (T - bu.ref);
+  }
   double drho = 0, j[3] = {0, 0, 0};
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
@@ -488,8 +616,9 @@ __device__ __forceinline__ void cell_coords(const Geom& g, int64_t c, int& x, in
 }
 
 template <class S, int Q>
-__global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, const Geom g, int64_t steps_done, double Fx,
-                                                   double Fy, double Fz, double rho0, int64_t n,
+__global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, const S* __restrict__ Tp, const Buoy bu,
+                                                   int axis, const Geom g, int64_t steps_done, double Fx0,
+                                                   double Fy0, double Fz0, double rho0, int64_t n,
                                                    double* __restrict__ partial) {
   double v[mke::DG_N];
 #pragma unroll
@@ -508,9 +637,17 @@ __global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, cons
       j[1] += ey(i) * f;
       j[2] += ez(i) * f;
     }
+    double Fx = Fx0, Fy = Fy0, Fz = Fz0, T = 0;
+    if (Tp) {
+      T = conv_T<S>(Tp, g, nb, steps_done, (int)c, bu.ref);
+      Fx = bu.bg[0] * (T - bu.ref);
+      Fy = bu.bg[1] * (T - bu.ref);
+      Fz = bu.bg[2] * (T - bu.ref);
+    }
     const double rho = rho0 + drho;
     const double mx = j[0] - 0.5 * Fx, my = j[1] - 0.5 * Fy, mz = j[2] - 0.5 * Fz;
-    const bool bad = !(rho > 0.0) || !isfinite(rho) || !isfinite(mx) || !isfinite(my) || !isfinite(mz);
+    const bool bad = !(rho > 0.0) || !isfinite(rho) || !isfinite(mx) || !isfinite(my) || !isfinite(mz) ||
+                     (Tp && !isfinite(T));
     v[mke::DG_MASS] += rho;
     v[mke::DG_MX] += mx;
     v[mke::DG_MY] += my;
@@ -518,6 +655,10 @@ __global__ void __launch_bounds__(256) k_diag_flow(const S* __restrict__ A, cons
     v[mke::DG_FLUID] += 1.0;
     v[mke::DG_BAD] += bad ? 1.0 : 0.0;
     if (!bad) v[mke::DG_MAXU] = fmax(v[mke::DG_MAXU], sqrt(mx * mx + my * my + mz * mz) / rho);
+    if (Tp) {
+      v[mke::DG_HEAT] += T;
+      v[mke::DG_FLUX] += (axis == 0 ? mx : (axis == 1 ? my : mz)) / rho * T;
+    }
   }
   block_reduce_store(v, partial);
 }
@@ -639,6 +780,9 @@ Refs refs_of(const mk_params& p) {
   Refs r{0.0, 0.0};
   if (p.model == MK_MODEL_FLOW) {
     r.r0 = p.rho0;
+  } else if (p.model == MK_MODEL_CONVECTION) {
+    r.r0 = p.rho0;
+    r.r1 = p.s_ref;  // t: the buoyancy reference value
   } else if (p.model == MK_MODEL_MULTIPHASE) {
     r.r0 = 0.0;  // g: rest state p* = 0, u = 0
     r.r1 = 1.0;  // h: liquid phi = 1
@@ -683,6 +827,61 @@ MpK<T> mp_coef(const mk_params& p, Refs r) {
 template <class T>
 DendK<T> dend_coef(const mk_params& p, Refs r) {
   return dend_params<T>(p, r.r0, r.r1);
+}
+
+Buoy buoy_of(const mk_params& p) {
+  Buoy b;
+  for (int a = 0; a < 3; ++a) b.bg[a] = -p.rho0 * p.beta * p.force[a];
+  b.ref = p.s_ref;
+  return b;
+}
+
+template <class T>
+ConvK<T> conv_coef(const mk_params& p) {
+  ConvK<T> k;
+  k.f = flow_coef<T>(p, p.rho0);
+  k.om_t = T(1.0 / (4.0 * p.D + 0.5));
+  k.ref_t = T(p.s_ref);
+  for (int a = 0; a < 3; ++a) k.bg[a] = T(-p.rho0 * p.beta * p.force[a]);
+  const int ax = p.wall_axis >= 0 ? p.wall_axis : 0;
+  const int n3[3] = {p.nx, p.ny, p.nz};
+  k.axis = ax;
+  k.lo = p.bc[ax] == MK_BC_WALLS ? 1 : 0;
+  k.hi = p.bc[ax] == MK_BC_WALLS ? n3[ax] - 2 : n3[ax] - 1;
+  for (int sd = 0; sd < 2; ++sd) {
+    k.tw2[sd] = T(2.0 * (p.wall_value[sd] - p.s_ref));
+    for (int a = 0; a < 3; ++a) k.uw6[sd][a] = T(6.0 * p.rho0 * p.wall_u[sd][a]);
+  }
+  return k;
+}
+
+template <class S, int Q, int COLL, bool SCALAR>
+void launch_conv_t(mke::Engine& e, int parity, dim3 grid, dim3 block) {
+  typedef typename Stor<S>::T T;
+  const Geom g = make_geom(e);
+  const ConvK<T> k = conv_coef<T>(e.p);
+  if (parity == 0)
+    k_conv<S, Q, COLL, 0, SCALAR><<<grid, block, 0, e.stream>>>((S*)e.pop0, (S*)e.pop1, g, k);
+  else
+    k_conv<S, Q, COLL, 1, SCALAR><<<grid, block, 0, e.stream>>>((S*)e.pop0, (S*)e.pop1, g, k);
+}
+
+template <class S, bool SCALAR>
+void launch_conv(mke::Engine& e, int parity, dim3 grid, dim3 block) {
+  const int Q = e.p.lattice, C = e.p.collision;
+  if (Q == 19) {
+    if (C == MK_COLL_BGK)
+      launch_conv_t<S, 19, MK_COLL_BGK, SCALAR>(e, parity, grid, block);
+    else if (C == MK_COLL_TRT)
+      launch_conv_t<S, 19, MK_COLL_TRT, SCALAR>(e, parity, grid, block);
+    else
+      launch_conv_t<S, 19, MK_COLL_MRT, SCALAR>(e, parity, grid, block);
+  } else {
+    if (C == MK_COLL_BGK)
+      launch_conv_t<S, 27, MK_COLL_BGK, SCALAR>(e, parity, grid, block);
+    else
+      launch_conv_t<S, 27, MK_COLL_TRT, SCALAR>(e, parity, grid, block);
+  }
 }
 
 template <class S, int Q, int COLL>
@@ -796,7 +995,16 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
   switch (e.p.model) {
     case MK_MODEL_FLOW:
       if (ev) cudaEventRecord(ev[0], e.stream);
-      launch_flow<S>(e, parity, grid, block);
+      if (e.p.wall_axis >= 0)
+        launch_conv<S, false>(e, parity, grid, block);  // moving plates
+      else
+        launch_flow<S>(e, parity, grid, block);
+      if (ev) cudaEventRecord(ev[1], e.stream);
+      e.launches += 1;
+      break;
+    case MK_MODEL_CONVECTION:
+      if (ev) cudaEventRecord(ev[0], e.stream);
+      launch_conv<S, true>(e, parity, grid, block);
       if (ev) cudaEventRecord(ev[1], e.stream);
       e.launches += 1;
       break;
@@ -822,7 +1030,8 @@ cudaError_t set_state_t(mke::Engine& e, const InT* d_phi, const InT* d_t, const 
   k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, e.rest1, (P*)e.phi[0],
                                                (P*)e.phi[1],
                                           (P*)e.temp, d_phi, d_t, d_rho, d_u, e.p.rho0, e.p.u0[0], e.p.u0[1],
-                                          e.p.u0[2], -e.p.delta, g, e.ncell, refs_of(e.p));
+                                          e.p.u0[2], e.p.model == MK_MODEL_CONVECTION ? e.p.s_ref : -e.p.delta, g,
+                                          e.ncell, refs_of(e.p));
   return cudaGetLastError();
 }
 
@@ -845,14 +1054,18 @@ cudaError_t field_t(mke::Engine& e, int field) {
     k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.phi[e.phi_cur], nullptr, e.ncell, e.field);
     return cudaGetLastError();
   }
-  if (m == MK_MODEL_FLOW) {
-    if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ)
+  if (m == MK_MODEL_FLOW || m == MK_MODEL_CONVECTION) {
+    const bool conv = m == MK_MODEL_CONVECTION;
+    if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ &&
+        !(conv && field == MK_FIELD_T))
       return cudaErrorInvalidValue;
+    const S* Tp = conv ? (const S*)e.pop1 : nullptr;
+    const Buoy bu = buoy_of(e.p);
     if (e.p.lattice == 19)
-      k_field_flow<S, 19><<<grid, block, 0, e.stream>>>((const S*)e.pop0, g, e.step, field, e.p.force[0],
+      k_field_flow<S, 19><<<grid, block, 0, e.stream>>>((const S*)e.pop0, Tp, bu, g, e.step, field, e.p.force[0],
                                                         e.p.force[1], e.p.force[2], e.p.rho0, e.field);
     else
-      k_field_flow<S, 27><<<grid, block, 0, e.stream>>>((const S*)e.pop0, g, e.step, field, e.p.force[0],
+      k_field_flow<S, 27><<<grid, block, 0, e.stream>>>((const S*)e.pop0, Tp, bu, g, e.step, field, e.p.force[0],
                                                         e.p.force[1], e.p.force[2], e.p.rho0, e.field);
     return cudaGetLastError();
   }
@@ -885,13 +1098,16 @@ cudaError_t diag_t(mke::Engine& e) {
   const Refs r = refs_of(e.p);
   const int nb = e.partial_blocks;
   const int m = e.p.model;
-  if (m == MK_MODEL_FLOW) {
+  if (m == MK_MODEL_FLOW || m == MK_MODEL_CONVECTION) {
+    const S* Tp = m == MK_MODEL_CONVECTION ? (const S*)e.pop1 : nullptr;
+    const Buoy bu = buoy_of(e.p);
+    const int ax = e.p.wall_axis >= 0 ? e.p.wall_axis : 0;
     if (e.p.lattice == 19)
-      k_diag_flow<S, 19><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, g, e.step, e.p.force[0], e.p.force[1],
-                                                   e.p.force[2], e.p.rho0, e.ncell, e.partial);
+      k_diag_flow<S, 19><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, Tp, bu, ax, g, e.step, e.p.force[0],
+                                                   e.p.force[1], e.p.force[2], e.p.rho0, e.ncell, e.partial);
     else
-      k_diag_flow<S, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, g, e.step, e.p.force[0], e.p.force[1],
-                                                   e.p.force[2], e.p.rho0, e.ncell, e.partial);
+      k_diag_flow<S, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, Tp, bu, ax, g, e.step, e.p.force[0],
+                                                   e.p.force[1], e.p.force[2], e.p.rho0, e.ncell, e.partial);
   } else if (m == MK_MODEL_MULTIPHASE) {
     k_diag_mp<S><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, (const P*)e.phi[0], g, e.step, mp_coef<T>(e.p, r),
                                            e.ncell, e.partial);
@@ -951,9 +1167,9 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   e.elem = store_bytes(p.precision);
   e.phi_elem = p.precision == MK_PREC_FP64 ? 8 : 4;
   e.device = device;
-  if (p.model == MK_MODEL_FLOW) {
+  if (p.model == MK_MODEL_FLOW || p.model == MK_MODEL_CONVECTION) {
     e.Q0 = p.lattice;
-    e.Q1 = 0;
+    e.Q1 = p.model == MK_MODEL_CONVECTION ? 7 : 0;
   } else if (p.model == MK_MODEL_MULTIPHASE) {
     e.Q0 = 19;
     e.Q1 = 19;
@@ -1148,10 +1364,12 @@ cudaError_t engine_step(Engine& e, cudaEvent_t* ev) {
   return cudaGetLastError();
 }
 
-int engine_kernels_per_step(const Engine& e) { return e.p.model == MK_MODEL_FLOW ? 1 : 2; }
+static bool one_kernel(const Engine& e) { return e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION; }
+
+int engine_kernels_per_step(const Engine& e) { return one_kernel(e) ? 1 : 2; }
 
 const char* engine_kernel_name(const Engine& e, int k) {
-  if (e.p.model == MK_MODEL_FLOW) return "collide";
+  if (one_kernel(e)) return "collide";
   return k == 0 ? "phi" : "collide";
 }
 
@@ -1282,7 +1500,7 @@ double engine_bytes_per_cell(const Engine& e) {
   // written once and read once where a model has it.
   // An FP32 rest plane (16-bit multiphase storage) moves 4 B instead of 2 B.
   const double S = e.elem;
-  const double phi = e.p.model == MK_MODEL_FLOW ? 0.0 : 2.0 * e.phi_elem;
+  const double phi = (e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION) ? 0.0 : 2.0 * e.phi_elem;
   const double rest = e.rest1 ? 2.0 * (4.0 - S) : 0.0;
   return 2.0 * (e.Q0 + e.Q1) * S + phi + rest;
 }

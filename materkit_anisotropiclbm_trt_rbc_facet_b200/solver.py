@@ -282,6 +282,12 @@ class Solver:
         _check(self._lib.mk_time_advance(self._h, int(nsteps), 1 if graph else 0, C.byref(ms)), self._h)
         return ms.value
 
+    def nusselt(self) -> float:
+        """Nusselt number of a convection case (FP64 reduction on the device)."""
+        nu = C.c_double()
+        _check(self._lib.mk_nusselt(self._h, C.byref(nu)), self._h)
+        return nu.value
+
     def backward(self, target_phi, steps: int, checkpoint_every: int = 100) -> dict:
         """Discrete adjoint of `steps` thermal dendrite loops from the current
         state: L = sum (phi - target)^2 and dL/d eps4, dL/d Delta, dL/d tau_T.

@@ -187,6 +187,56 @@ void propagate(const orc_state* s, int Q, const std::vector<double>& out, std::v
       }
 }
 
+// Plate corrections of a bounced population (wall_axis >= 0): the flow sees
+// a wall moving with wall_u (Ladd: + 6 w rho0 e.u_w, bdyCouette /
+// boundary_vel, mkFluidsLBM.h:61-63), a scalar sees the Dirichlet value
+// wall_value (anti-bounce-back -t + 2 w T_w, bdy_constT / bdy_RBC,
+// mkThermalField.h:37-39).  A population is bounced at the low (high) plate
+// when the upwind cell lies below (above) the fluid span of wall_axis.
+enum { kWallFlow = 1, kWallScalar = 2 };
+
+// Plate side (0 low, 1 high) of the upwind cell x - e_i, or -1.
+inline int plate_side(const orc_state* s, int x, int y, int z, int i) {
+  const int a = s->p.wall_axis;
+  if (a < 0 || E27[i][a] == 0) return -1;
+  const int c3[3] = {x, y, z};
+  const int n3[3] = {s->nx, s->ny, s->nz};
+  const int p = c3[a] - E27[i][a];
+  const int lo = s->p.bc[a] == MK_BC_WALLS ? 1 : 0, hi = s->p.bc[a] == MK_BC_WALLS ? n3[a] - 2 : n3[a] - 1;
+  return p < lo ? 0 : (p > hi ? 1 : -1);
+}
+
+void propagate_bc(const orc_state* s, int Q, const std::vector<double>& out, std::vector<double>& hlp, int kind) {
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int64_t c = cidx(s, x, y, z);
+        if (s->flag[c] != MK_FLAG_FLUID) continue;
+        for (int i = 0; i < Q; ++i) {
+          const int64_t src = nbr(s, x, y, z, -E27[i][0], -E27[i][1], -E27[i][2]);
+          if (src >= 0) {
+            hlp[(int64_t)i * n + c] = out[(int64_t)i * n + src];
+            continue;
+          }
+          double v = out[(int64_t)inv_dir(i) * n + c];
+          const int side = plate_side(s, x, y, z, i);
+          if (side >= 0) {
+            const double w = weight(Q, i);
+            if (kind == kWallFlow) {
+              const double* uw = p.wall_u[side];
+              v += 6.0 * w * p.rho0 * (E27[i][0] * uw[0] + E27[i][1] * uw[1] + E27[i][2] * uw[2]);
+            } else {
+              v = -v + 2.0 * w * p.wall_value[side];
+            }
+          }
+          hlp[(int64_t)i * n + c] = v;
+        }
+      }
+}
+
 // Isotropic gradient and Laplacian of a scalar with D3Q19 weights.  `wall`
 // gives the value substituted at a non-fluid neighbour.
 template <class WallFn>
@@ -218,10 +268,48 @@ void flow_force(const orc_state* s, double F[3]) {
   F[2] = s->p.force[2];
 }
 
+// Collision of one cell's Q populations with the Guo force F
+// (mkNode::collision_BGK/TRT/MRT*, mkNode.h:74-87); returns u.
+void flow_collide(int Q, int coll, double om, double om_m, double* f, const double F[3], double u[3]) {
+  double feq[27], Fi[27];
+  double rho = 0, j[3] = {0, 0, 0};
+  for (int i = 0; i < Q; ++i) {
+    rho += f[i];
+    j[0] += E27[i][0] * f[i];
+    j[1] += E27[i][1] * f[i];
+    j[2] += E27[i][2] * f[i];
+  }
+  for (int a = 0; a < 3; ++a) u[a] = (j[a] + 0.5 * F[a]) / rho;
+  const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const double uF = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
+  for (int i = 0; i < Q; ++i) {
+    const double w = weight(Q, i);
+    const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+    const double eF = E27[i][0] * F[0] + E27[i][1] * F[1] + E27[i][2] * F[2];
+    feq[i] = rho * feq2(w, eu, uu);
+    Fi[i] = w * (3.0 * eF + 9.0 * eu * eF - 3.0 * uF);
+  }
+  if (coll == MK_COLL_BGK) {
+    for (int i = 0; i < Q; ++i) f[i] += -om * (f[i] - feq[i]) + (1.0 - 0.5 * om) * Fi[i];
+  } else if (coll == MK_COLL_TRT) {
+    double fo[27];
+    for (int i = 0; i < Q; ++i) {
+      const int k = inv_dir(i);
+      const double fp = 0.5 * (f[i] + f[k]), fm = 0.5 * (f[i] - f[k]);
+      const double ep = 0.5 * (feq[i] + feq[k]), em = 0.5 * (feq[i] - feq[k]);
+      const double Fp = 0.5 * (Fi[i] + Fi[k]), Fm = 0.5 * (Fi[i] - Fi[k]);
+      fo[i] = f[i] - om * (fp - ep) - om_m * (fm - em) + (1.0 - 0.5 * om) * Fp + (1.0 - 0.5 * om_m) * Fm;
+    }
+    for (int i = 0; i < Q; ++i) f[i] = fo[i];
+  } else {
+    mrt_collide(f, feq, Fi, om);
+  }
+}
+
 void flow_step(orc_state* s) {
   const int Q = s->Qf;
   const int64_t n = s->n;
-  propagate(s, Q, s->f_out, s->f_hlp);
+  propagate_bc(s, Q, s->f_out, s->f_hlp, kWallFlow);
   double F[3];
   flow_force(s, F);
   const double tau = s->p.tau;
@@ -232,42 +320,46 @@ void flow_step(orc_state* s) {
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < n; ++c) {
     if (s->flag[c] != MK_FLAG_FLUID) continue;
-    double f[27], feq[27], Fi[27];
-    double rho = 0, j[3] = {0, 0, 0};
-    for (int i = 0; i < Q; ++i) {
-      f[i] = s->f_hlp[(int64_t)i * n + c];
-      rho += f[i];
-      j[0] += E27[i][0] * f[i];
-      j[1] += E27[i][1] * f[i];
-      j[2] += E27[i][2] * f[i];
-    }
-    double u[3];
-    for (int a = 0; a < 3; ++a) u[a] = (j[a] + 0.5 * F[a]) / rho;
-    const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    const double uF = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
-    for (int i = 0; i < Q; ++i) {
-      const double w = weight(Q, i);
-      const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
-      const double eF = E27[i][0] * F[0] + E27[i][1] * F[1] + E27[i][2] * F[2];
-      feq[i] = rho * feq2(w, eu, uu);
-      Fi[i] = w * (3.0 * eF + 9.0 * eu * eF - 3.0 * uF);
-    }
-    if (coll == MK_COLL_BGK) {
-      for (int i = 0; i < Q; ++i) f[i] += -om * (f[i] - feq[i]) + (1.0 - 0.5 * om) * Fi[i];
-    } else if (coll == MK_COLL_TRT) {
-      double fo[27];
-      for (int i = 0; i < Q; ++i) {
-        const int k = inv_dir(i);
-        const double fp = 0.5 * (f[i] + f[k]), fm = 0.5 * (f[i] - f[k]);
-        const double ep = 0.5 * (feq[i] + feq[k]), em = 0.5 * (feq[i] - feq[k]);
-        const double Fp = 0.5 * (Fi[i] + Fi[k]), Fm = 0.5 * (Fi[i] - Fi[k]);
-        fo[i] = f[i] - om * (fp - ep) - om_m * (fm - em) + (1.0 - 0.5 * om) * Fp + (1.0 - 0.5 * om_m) * Fm;
-      }
-      for (int i = 0; i < Q; ++i) f[i] = fo[i];
-    } else {
-      mrt_collide(f, feq, Fi, om);
-    }
+    double f[27], u[3];
+    for (int i = 0; i < Q; ++i) f[i] = s->f_hlp[(int64_t)i * n + c];
+    flow_collide(Q, coll, om, om_m, f, F, u);
     for (int i = 0; i < Q; ++i) s->f_out[(int64_t)i * n + c] = f[i];
+  }
+}
+
+// ------------------------------------------------------ CONVECTION model
+// Rayleigh-Benard / natural convection (bdy_RBC, bdy_constT, mkThermalField
+// relaxation with advection, Thermal_NusseltRBC: mkThermalField.h:33-40,
+// mkFluidsLBM.h:59-68, mkFluidsUser.cpp:362-392): the flow lattice with the
+// Boussinesq force F = -rho0 beta (T - T_ref) g (g = force) and a D3Q7
+// advection-diffusion lattice t_eq = w T (1 + 4 e.u), omega_T = 1/(4 D + 1/2);
+// both streamed with the plate corrections of propagate_bc.
+void convection_step(orc_state* s) {
+  const int Q = s->Qf;
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  propagate_bc(s, Q, s->f_out, s->f_hlp, kWallFlow);
+  propagate_bc(s, 7, s->s_out, s->s_hlp, kWallScalar);
+  const double om = 1.0 / p.tau;
+  const double om_m = 1.0 / (0.5 + p.magic / (p.tau - 0.5));
+  const double om_t = 1.0 / (4.0 * p.D + 0.5);
+  const double bg[3] = {-p.rho0 * p.beta * p.force[0], -p.rho0 * p.beta * p.force[1], -p.rho0 * p.beta * p.force[2]};
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    double T = 0;
+    for (int i = 0; i < 7; ++i) T += s->s_hlp[(int64_t)i * n + c];
+    const double F[3] = {bg[0] * (T - p.s_ref), bg[1] * (T - p.s_ref), bg[2] * (T - p.s_ref)};
+    double f[27], u[3];
+    for (int i = 0; i < Q; ++i) f[i] = s->f_hlp[(int64_t)i * n + c];
+    flow_collide(Q, p.collision, om, om_m, f, F, u);
+    for (int i = 0; i < Q; ++i) s->f_out[(int64_t)i * n + c] = f[i];
+    for (int i = 0; i < 7; ++i) {
+      const double ti = s->s_hlp[(int64_t)i * n + c];
+      const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+      s->s_out[(int64_t)i * n + c] = ti - om_t * (ti - weight(7, i) * T * (1.0 + 4.0 * eu));
+    }
+    s->temp[c] = T;
   }
 }
 
@@ -622,12 +714,19 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
         for (int x = 0; x < s->nx; ++x) s->grain[cidx(s, x, y, z)] = nearest_seed(*p, x, y, z);
   }
 
-  if (p->model == MK_MODEL_FLOW) {
+  if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) {
+    const bool conv = p->model == MK_MODEL_CONVECTION;
     s->Qf = p->lattice;
-    s->Qs = 0;
+    s->Qs = conv ? 7 : 0;
     const int Q = s->Qf;
     s->f_out.assign((size_t)Q * n, 0.0);
     s->f_hlp.assign((size_t)Q * n, 0.0);
+    if (conv) {
+      s->s_out.assign((size_t)7 * n, 0.0);
+      s->s_hlp.assign((size_t)7 * n, 0.0);
+      s->temp.assign(n, p->s_ref);
+      if (T0) std::memcpy(s->temp.data(), T0, n * sizeof(double));
+    }
     for (int64_t c = 0; c < n; ++c) {
       const double r = rho0 ? rho0[c] : p->rho0;
       const double u[3] = {ux0 ? ux0[c] : p->u0[0], uy0 ? uy0[c] : p->u0[1], uz0 ? uz0[c] : p->u0[2]};
@@ -636,6 +735,11 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
         const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
         s->f_out[(int64_t)i * n + c] = r * feq2(weight(Q, i), eu, uu);
       }
+      if (conv)
+        for (int i = 0; i < 7; ++i) {
+          const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+          s->s_out[(int64_t)i * n + c] = weight(7, i) * s->temp[c] * (1.0 + 4.0 * eu);
+        }
     }
   } else if (p->model == MK_MODEL_MULTIPHASE) {
     s->Qf = 19;
@@ -678,6 +782,9 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
       case MK_MODEL_MULTIPHASE:
         mp_step(s);
         break;
+      case MK_MODEL_CONVECTION:
+        convection_step(s);
+        break;
       case MK_MODEL_THERMAL_DENDRITE:
       case MK_MODEL_SOLUTAL_DENDRITE:
         thermal_dendrite_step(s);  // the second lattice follows p.model
@@ -711,7 +818,11 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
     std::memcpy(out, s->phi.data(), n * sizeof(double));
     return 0;
   }
-  if (p.model == MK_MODEL_FLOW) {
+  if (p.model == MK_MODEL_CONVECTION && field == MK_FIELD_T) {
+    std::memcpy(out, s->temp.data(), n * sizeof(double));
+    return 0;
+  }
+  if (p.model == MK_MODEL_FLOW || p.model == MK_MODEL_CONVECTION) {
     if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ) return 1;
     double F[3];
     flow_force(s, F);
@@ -720,6 +831,12 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
       if (s->flag[c] != MK_FLAG_FLUID) {
         out[c] = field == MK_FIELD_RHO ? p.rho0 : 0.0;
         continue;
+      }
+      if (p.model == MK_MODEL_CONVECTION) {
+        // the buoyancy of the stored (post-collision) scalar
+        double T = 0;
+        for (int i = 0; i < 7; ++i) T += s->s_out[(int64_t)i * n + c];
+        for (int a = 0; a < 3; ++a) F[a] = -p.rho0 * p.beta * p.force[a] * (T - p.s_ref);
       }
       double rho = 0, j[3] = {0, 0, 0};
       for (int i = 0; i < Q; ++i) {

@@ -255,3 +255,50 @@ def test_solutal_fp32(casedir):
     s.advance(150)
     o.advance(150)
     _compare(s, o, ["phi", "C"], 3e-5)
+
+
+# ---------------------------------------------------------------- convection and plates
+CONV_FIELDS = ["rho", "ux", "uy", "uz", "T"]
+
+
+@pytest.mark.parametrize("coll,lat,axis", [("TRT", "D3Q19", "z"), ("BGK", "D3Q19", "z"), ("MRT", "D3Q19", "z"),
+                                           ("TRT", "D3Q27", "z"), ("TRT", "D3Q19", "x"), ("BGK", "D3Q19", "y")])
+def test_convection_fp64_steps(casedir, coll, lat, axis):
+    n3 = {"z": (20, 5, 12), "x": (12, 5, 20), "y": (20, 12, 5)}[axis]
+    p, s, o = _pair(casedir, f"conv_{coll}_{lat}_{axis}",
+                    cases.convection(nx=n3[0], ny=n3[1], nz=n3[2], axis=axis, Ra=2e4, collision=coll, lattice=lat))
+    mask = _fluid(p)
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, CONV_FIELDS, FP64_TOL, mask)
+    s.advance(300, graph=True)
+    o.advance(300)
+    _compare(s, o, CONV_FIELDS, FP64_TOL, mask)
+    # the device Nusselt reduction against the oracle's fields
+    a = "xyz".index(axis)
+    H = (n3[a] - 2)
+    u = o.field(["ux", "uy", "uz"][a])
+    nu_o = 1.0 + (u * o.field("T"))[mask].mean() * H / (p.D * (p.wall_value[0] - p.wall_value[1]))
+    assert s.nusselt() == pytest.approx(nu_o, rel=1e-9, abs=1e-12)
+
+
+def test_convection_fp32(casedir):
+    p, s, o = _pair(casedir, "conv32", cases.convection(nx=20, ny=5, nz=12, Ra=2e4, precision="fp32"))
+    s.advance(300)
+    o.advance(300)
+    _compare(s, o, ["rho", "T"], 1e-5, _fluid(p))
+    _compare(s, o, ["ux", "uy", "uz"], 1e-4, _fluid(p))
+
+
+@pytest.mark.parametrize("coll", ["TRT", "BGK", "MRT"])
+def test_couette_fp64(casedir, coll):
+    p, s, o = _pair(casedir, f"couette_{coll}", cases.couette(nx=6, ny=12, nz=5, U=2e-2, collision=coll))
+    mask = _fluid(p)
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        _compare(s, o, FLOW_FIELDS, FP64_TOL, mask)
+    s.advance(400)
+    o.advance(400)
+    _compare(s, o, FLOW_FIELDS, FP64_TOL, mask)

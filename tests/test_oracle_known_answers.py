@@ -297,3 +297,63 @@ def test_oracle_adjoint_matches_central_differences(casedir, aniso):
     assert g["d_eps4"] == pytest.approx(fd_e, rel=1e-6)
     assert g["d_delta"] == pytest.approx(fd_d, rel=1e-6)
     assert g["d_tau_t"] == pytest.approx(fd_t, rel=1e-6)
+
+
+# ---------------------------------------------------------------- plates and convection
+def test_couette_linear_profile_exact(casedir):
+    # moving upper plate, half-way walls at y = 1/2 and y = ny - 3/2: the
+    # steady linear profile is exact for the lattice
+    U = 1e-2
+    p = _params(casedir, "couette", cases.couette(nx=3, ny=14, nz=3, U=U))
+    o = Oracle(p)
+    o.advance(30000)
+    ux = o.field("ux")[1, :, 1]
+    H = p.ny - 2
+    y = np.arange(p.ny, dtype=np.float64)
+    exact = U * (y - 0.5) / H
+    fl = slice(1, p.ny - 1)
+    assert np.max(np.abs(ux[fl] - exact[fl])) < 1e-9 * U
+
+
+def test_conduction_between_plates_is_linear_and_nu_is_one(casedir):
+    # no buoyancy: the plates impose a linear profile (exact for the D3Q7
+    # anti-bounce-back), no flow, Nu = 1
+    p = _params(casedir, "cond", cases.convection(nx=8, ny=3, nz=12, Ra=1e3, beta=0.0))
+    o = Oracle(p, T=initial_field(p, "T"))
+    o.advance(8000)
+    T = o.field("T")[:, 1, 3]
+    H = p.nz - 2
+    z = np.arange(p.nz, dtype=np.float64)
+    exact = 1.0 - (z - 0.5) / H
+    fl = slice(1, p.nz - 1)
+    assert np.max(np.abs(T[fl] - exact[fl])) < 1e-9
+    assert np.max(np.abs(o.field("uz"))) < 1e-12
+
+
+def _nusselt(o, p):
+    T, uz = o.field("T"), o.field("uz")
+    fl = initial_field(p, "flag") == 0
+    H = p.nz - 2
+    return 1.0 + (uz * T)[fl].mean() * H / (p.D * (p.wall_value[0] - p.wall_value[1]))
+
+
+def test_rbc_below_onset_decays_to_conduction(casedir):
+    # Ra = 1000 < 1708 (the rigid-rigid critical value): the seeded roll decays
+    # (what stays is the O(Ma^2) hydrostatic compressibility residue)
+    p = _params(casedir, "rbc_sub", cases.convection(nx=24, ny=3, nz=14, Ra=1000.0))
+    o = Oracle(p, T=initial_field(p, "T"))
+    o.advance(8000)
+    assert abs(_nusselt(o, p) - 1.0) < 1e-3
+    assert np.max(np.abs(o.field("uz"))) < 2e-5
+
+
+def test_rbc_above_onset_convects(casedir):
+    # Ra = 1e4, Pr = 0.71, laterally periodic layer of aspect ratio 2 (one
+    # roll pair near the critical wavelength): steady rolls.  The periodic-
+    # layer value is Nu ~ 2.66 (Clever & Busse 1974, alpha ~ 3.1); this
+    # lattice gives 2.72 at H = 12 and 2.67 at H = 24 (converging).
+    p = _params(casedir, "rbc_sup", cases.convection(nx=24, ny=3, nz=14, Ra=1e4))
+    o = Oracle(p, T=initial_field(p, "T"))
+    o.advance(25000)
+    nu = _nusselt(o, p)
+    assert 2.6 < nu < 2.8, nu
