@@ -220,8 +220,10 @@ __host__ __device__ __forceinline__ void mrt19_collide_moments(T (&f)[19], const
 // the forward transform is ~45 additions and the back transform ~60.  Pairs:
 // p = 1..3 the +-x, +-y, +-z faces; p = 4..9 the xy(+,+), xy(+,-), xz(+,+),
 // xz(+,-), yz(+,+), yz(+,-) edges (direction 2p-1, opposite 2p).
+// The 19 moments m = M f of the d'Humieres basis by pair-split sums (m[0]
+// is sum f, m[3], m[5], m[7] the three momentum components).
 template <class T>
-__host__ __device__ __forceinline__ void mrt19_collide_fact(T (&f)[19], const MrtIn<T>& q) {
+__host__ __device__ __forceinline__ void mrt19_moments(const T (&f)[19], T (&m)[19]) {
   T s[10], a[10];
   s[0] = f[0];
   a[0] = T(0);
@@ -230,7 +232,6 @@ __host__ __device__ __forceinline__ void mrt19_collide_fact(T (&f)[19], const Mr
     s[p] = f[2 * p - 1] + f[2 * p];
     a[p] = f[2 * p - 1] - f[2 * p];
   }
-  T m[19];
   const T Sf = s[1] + s[2] + s[3];
   const T Se = (s[4] + s[5]) + (s[6] + s[7]) + (s[8] + s[9]);
   m[0] = s[0] + Sf + Se;
@@ -259,6 +260,11 @@ __host__ __device__ __forceinline__ void mrt19_collide_fact(T (&f)[19], const Mr
   m[16] = (a[4] + a[5]) - (a[6] + a[7]);
   m[17] = (a[5] - a[4]) + (a[8] + a[9]);
   m[18] = (a[6] - a[7]) - (a[8] - a[9]);
+}
+
+// f -= M^T d with d the relaxed, force-corrected moment updates of m.
+template <class T>
+__host__ __device__ __forceinline__ void mrt19_relax_back(T (&f)[19], const T (&m)[19], const MrtIn<T>& q) {
   T d[19];
   mrt_relax_all<T>(m, d, q, std::make_integer_sequence<int, 19>{});
   // back transform f -= M^T d, even part E and odd part O per pair
@@ -292,6 +298,14 @@ __host__ __device__ __forceinline__ void mrt19_collide_fact(T (&f)[19], const Mr
     f[2 * p - 1] -= E[p] + O[p];
     f[2 * p] -= E[p] - O[p];
   }
+}
+
+// In-place D3Q19 MRT collision in moment space (pair-split transforms).
+template <class T>
+__host__ __device__ __forceinline__ void mrt19_collide_fact(T (&f)[19], const MrtIn<T>& q) {
+  T m[19];
+  mrt19_moments<T>(f, m);
+  mrt19_relax_back<T>(f, m, q);
 }
 
 // f -= Mi [ S M (f - feq) - (I - S/2) M F ]   (all loops unrolled; M is
@@ -339,6 +353,9 @@ template <>
 struct Stor<double> {
   typedef double T;
   static constexpr int bytes = 8;
+  static constexpr bool scaled = false;
+  __device__ __forceinline__ static double ldr(const double* p) { return *p; }
+  __device__ __forceinline__ static void str(double* p, double v) { *p = v; }
   __device__ __forceinline__ static double ld(const double* p, double) { return *p; }
   __device__ __forceinline__ static void st(double* p, double v, double) { *p = v; }
   __device__ __forceinline__ static double st_rt(double* p, double v, double) {
@@ -350,6 +367,9 @@ template <>
 struct Stor<float> {
   typedef float T;
   static constexpr int bytes = 4;
+  static constexpr bool scaled = false;
+  __device__ __forceinline__ static float ldr(const float* p) { return *p; }
+  __device__ __forceinline__ static void str(float* p, float v) { *p = v; }
   __device__ __forceinline__ static float ld(const float* p, float) { return *p; }
   __device__ __forceinline__ static void st(float* p, float v, float) { *p = v; }
   __device__ __forceinline__ static float st_rt(float* p, float v, float) {
@@ -361,6 +381,15 @@ template <>
 struct Stor<__half> {
   typedef float T;
   static constexpr int bytes = 2;
+  static constexpr bool scaled = true;  // stores f'/w
+  __device__ __forceinline__ static float ldr(const __half* p) { return __half2float(*p); }
+  __device__ __forceinline__ static void str(__half* p, float v) { *p = __float2half_rn(v); }
+  // store and return what a later ldr reads
+  __device__ __forceinline__ static float str_rt(__half* p, float v) {
+    const __half h = __float2half_rn(v);
+    *p = h;
+    return __half2float(h);
+  }
   __device__ __forceinline__ static float ld(const __half* p, float w) { return w * __half2float(*p); }
   __device__ __forceinline__ static void st(__half* p, float v, float w) { *p = __float2half_rn(v * (1.0f / w)); }
   __device__ __forceinline__ static float st_rt(__half* p, float v, float w) {
@@ -373,6 +402,14 @@ template <>
 struct Stor<__nv_bfloat16> {
   typedef float T;
   static constexpr int bytes = 2;
+  static constexpr bool scaled = true;  // stores f'/w
+  __device__ __forceinline__ static float ldr(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+  __device__ __forceinline__ static void str(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+  __device__ __forceinline__ static float str_rt(__nv_bfloat16* p, float v) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    *p = h;
+    return __bfloat162float(h);
+  }
   __device__ __forceinline__ static float ld(const __nv_bfloat16* p, float w) { return w * __bfloat162float(*p); }
   __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float w) {
     *p = __float2bfloat16_rn(v * (1.0f / w));
@@ -605,6 +642,32 @@ template <class S, int Q, class NB>
 __device__ __forceinline__ typename Stor<S>::T ld_in(const S* __restrict__ A, int64_t stride, const NB& nb,
                                                       int parity, int c, int i) {
   return Stor<S>::ld(A + off_in<Q>(stride, nb, parity, c, i), typename Stor<S>::T(wq<Q>(i)));
+}
+
+// Bring the slot that population i of the cell at `c` is read from into L2
+// (no register, no wait), for a load that comes later in the thread.
+template <class S, int Q, class NB>
+__device__ __forceinline__ void pf_in(const S* __restrict__ A, int64_t stride, const NB& nb, int parity, int c, int i) {
+  const S* p = A + off_in<Q>(stride, nb, parity, c, i);
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// The stored value itself: f'_i, or f'_i / w_i for the 16-bit formats
+// (Stor<S>::scaled), for arithmetic that works in the stored units.
+template <class S, int Q, class NB>
+__device__ __forceinline__ typename Stor<S>::T ld_in_raw(const S* __restrict__ A, int64_t stride, const NB& nb,
+                                                          int parity, int c, int i) {
+  return Stor<S>::ldr(A + off_in<Q>(stride, nb, parity, c, i));
+}
+template <class S, int Q, class NB>
+__device__ __forceinline__ void st_out_raw(S* __restrict__ A, int64_t stride, const NB& nb, int parity, int c, int i,
+                                           typename Stor<S>::T v) {
+  Stor<S>::str(A + off_out<Q>(stride, nb, parity, c, i), v);
+}
+template <class S, int Q, class NB>
+__device__ __forceinline__ typename Stor<S>::T st_out_raw_rt(S* __restrict__ A, int64_t stride, const NB& nb,
+                                                              int parity, int c, int i, typename Stor<S>::T v) {
+  return Stor<S>::str_rt(A + off_out<Q>(stride, nb, parity, c, i), v);
 }
 
 // Store the post-collision deviation f'_i of the cell at `c`.

@@ -298,20 +298,17 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
                                                 const P* __restrict__ phi, const int64_t stride, const NB& nb,
                                                 const int c, const MpK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
-  T gp_[19], h[19];  // g, and the deviations h_i - w_i
+  // the Allen-Cahn slots go to L2 now and are loaded once the pressure
+  // lattice is stored, so the two lattices' populations are never live
+  // together (register pressure sets the occupancy of this kernel)
+#pragma unroll
+  for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
+  T gp_[19];  // g (rests at 0)
 #pragma unroll
   for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, stride, nb, PARITY, c, i);
-  h[0] = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
-#pragma unroll
-  for (int i = 1; i < 19; ++i) h[i] = ld_in<S, 19>(H, stride, nb, PARITY, c, i);
-  T pstar = T(0), jx = T(0), jy = T(0), jz = T(0);
-#pragma unroll
-  for (int i = 0; i < 19; ++i) {
-    pstar += gp_[i];
-    if (ex(i)) jx += T(ex(i)) * gp_[i];
-    if (ey(i)) jy += T(ey(i)) * gp_[i];
-    if (ez(i)) jz += T(ez(i)) * gp_[i];
-  }
+  T m[19];  // MRT moments: m[0] = p*, (m[3], m[5], m[7]) = j
+  mrt19_moments<T>(gp_, m);
+  const T pstar = m[0], jx = m[3], jy = m[5], jz = m[7];
   T ph, rho, gphi[3], F[3];
   mp_force<T, P, NB>(phi, nb, c, k, pstar, ph, rho, gphi, F);
   const T irho = T(1) / rho;
@@ -319,35 +316,71 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
   const T uy = jy + T(0.5) * F[1] * irho;
   const T uz = jz + T(0.5) * F[2] * irho;
   const T uu = ux * ux + uy * uy + uz * uz;
+  // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
+  {
+    MrtIn<T> q;
+    q.a0 = pstar - T(1.5) * uu;
+    q.bx = ux;
+    q.by = uy;
+    q.bz = uz;
+    q.qxx = ux * ux;
+    q.qyy = uy * uy;
+    q.qzz = uz * uz;
+    q.qxy = ux * uy;
+    q.qxz = ux * uz;
+    q.qyz = uy * uz;
+    q.Fx = F[0];
+    q.Fy = F[1];
+    q.Fz = F[2];
+    q.ux = ux;
+    q.uy = uy;
+    q.uz = uz;
+    q.sF = irho;
+    q.s_nu = T(1) / (k.tau_g + ph * (k.tau_l - k.tau_g));
+    mrt19_relax_back<T>(gp_, m, q);
+#pragma unroll
+    for (int i = 0; i < 19; ++i) st_out<S, 19>(G, stride, nb, PARITY, c, i, gp_[i]);
+  }
   const T gn = sqrt(gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2]);
   const T inv_gn = T(1) / (gn + T(1e-12));
   const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
   const T lam = k.inv_w4 * ph * (T(1) - ph);
-  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair, on the
-  // deviations: heq_i - w_i = w_i [(phi - 1) + phi (3eu + 4.5(eu)^2 - 1.5u^2)]
+  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair, in the
+  // stored units (h' = h - w, or h'/w for 16-bit storage, sig = w or 1):
+  //   h*' = (1 - om) h' + sig [om (X_even +- X_odd) +- Y],
+  //   heq_i - w_i = w_i [X_even + X_odd], X_even = (phi - 1) + phi (4.5(eu)^2 - 1.5u^2),
+  //   X_odd = 3 phi eu, the sharpening flux w_i Y = w_i (1 - om/2) lam (e.n)
+  constexpr bool SC = Stor<S>::scaled;
+  T h[19];
+  h[0] = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
+#pragma unroll
+  for (int i = 1; i < 19; ++i) h[i] = ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
   const T om_h = k.om_h;
+  const T one_om = T(1) - om_h;
   const T src = (T(1) - T(0.5) * om_h) * lam;
   const T dph = ph - k.ref_h;
-  T resid = T(0);  // what the 16-bit stores rounded away (Rest32 only)
+  T res_a = T(0), res_d = T(0);  // what the 16-bit stores rounded away, per weight class (Rest32 only)
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
     const int i = 2 * p - 1, j = 2 * p;
-    const T w = T(wq<19>(i));
-    const T hi = h[i];
-    const T hj = h[j];
+    const T sig = SC ? T(1) : T(wq<19>(i));
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
     const T en = T(ex(i)) * nx_ + T(ey(i)) * ny_ + T(ez(i)) * nz_;
-    const T even = w * (dph + ph * (T(4.5) * eu * eu - T(1.5) * uu));
-    const T odd = ph * (w * (T(3) * eu));
-    const T s = src * w * en;
-    const T vi = hi - om_h * (hi - (even + odd)) + s;
-    const T vj = hj - om_h * (hj - (even - odd)) - s;
+    const T xe = dph + ph * (T(4.5) * eu * eu - T(1.5) * uu);
+    const T xo = ph * (T(3) * eu);
+    const T y = src * en;
+    const T vi = one_om * h[i] + sig * (om_h * (xe + xo) + y);
+    const T vj = one_om * h[j] + sig * (om_h * (xe - xo) - y);
     if constexpr (Rest32<S>::on) {
-      resid += (vi - st_out_rt<S, 19>(H, stride, nb, PARITY, c, i, vi)) +
-               (vj - st_out_rt<S, 19>(H, stride, nb, PARITY, c, j, vj));
+      const T r = (vi - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, i, vi)) +
+                  (vj - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, j, vj));
+      if (p <= 3)
+        res_a += r;
+      else
+        res_d += r;
     } else {
-      st_out<S, 19>(H, stride, nb, PARITY, c, i, vi);
-      st_out<S, 19>(H, stride, nb, PARITY, c, j, vj);
+      st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, vi);
+      st_out_raw<S, 19>(H, stride, nb, PARITY, c, j, vj);
     }
   }
   {
@@ -356,33 +389,10 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
     const T heq = w * (dph - T(1.5) * ph * uu);
     const T v0 = h0 - om_h * (h0 - heq);
     if constexpr (Rest32<S>::on)
-      H0[c] = float(v0 + resid);
+      H0[c] = float(v0 + (T(wq<19>(1)) * res_a + T(wq<19>(7)) * res_d));
     else
       st_out<S, 19>(H, stride, nb, PARITY, c, 0, v0);
   }
-  // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
-  MrtIn<T> q;
-  q.a0 = pstar - T(1.5) * uu;
-  q.bx = ux;
-  q.by = uy;
-  q.bz = uz;
-  q.qxx = ux * ux;
-  q.qyy = uy * uy;
-  q.qzz = uz * uz;
-  q.qxy = ux * uy;
-  q.qxz = ux * uz;
-  q.qyz = uy * uz;
-  q.Fx = F[0];
-  q.Fy = F[1];
-  q.Fz = F[2];
-  q.ux = ux;
-  q.uy = uy;
-  q.uz = uz;
-  q.sF = irho;
-  q.s_nu = T(1) / (k.tau_g + ph * (k.tau_l - k.tau_g));
-  mrt19_collide_fact<T>(gp_, q);
-#pragma unroll
-  for (int i = 0; i < 19; ++i) st_out<S, 19>(G, stride, nb, PARITY, c, i, gp_[i]);
 }
 
 // MINB is the occupancy hint (resident 256-thread blocks per SM): 1 keeps
