@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "mk_device.cuh"
@@ -360,6 +361,55 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
   const T src = (T(1) - T(0.5) * om_h) * lam;
   const T dph = ph - k.ref_h;
   T res_a = T(0), res_d = T(0);  // what the 16-bit stores rounded away, per weight class (Rest32 only)
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32 arithmetic: two pairs per packed instruction, the pairs of equal
+    // weight grouped (+-x with +-y, then the four diagonal planes two by
+    // two); the +-z pair goes alone
+    auto store = [&](int i, float v, bool axis) {
+      if constexpr (Rest32<S>::on) {
+        const float r = v - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, i, v);
+        if (axis)
+          res_a += r;
+        else
+          res_d += r;
+      } else {
+        st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, v);
+      }
+    };
+    const float2 b_ph = bc2(ph), b_dph = bc2(dph), b_uu = bc2(-1.5f * uu), b_one_om = bc2(one_om);
+    const float2 b_om = bc2(om_h), b_3phom = bc2(3.0f * ph * om_h), b_src = bc2(src), b_m1 = bc2(-1.0f);
+    auto group = [&](int p, int q, float2 eu, float2 en, float sg) {
+      const float2 t = fma2(bc2(4.5f), mul2(eu, eu), b_uu);
+      const float2 E = mul2(b_om, fma2(b_ph, t, b_dph));          // om X_even
+      const float2 Pq = fma2(b_3phom, eu, mul2(b_src, en));       // om X_odd + Y
+      float2 a = add2(E, Pq), b = fma2(Pq, b_m1, E);
+      if (!SC) {
+        a = mul2(bc2(sg), a);
+        b = mul2(bc2(sg), b);
+      }
+      const float2 hi = make_float2(h[2 * p - 1], h[2 * q - 1]), hj = make_float2(h[2 * p], h[2 * q]);
+      const float2 vi = fma2(b_one_om, hi, a), vj = fma2(b_one_om, hj, b);
+      const bool ax = p <= 3;
+      store(2 * p - 1, vi.x, ax);
+      store(2 * p, vj.x, ax);
+      store(2 * q - 1, vi.y, ax);
+      store(2 * q, vj.y, ax);
+    };
+    const float wa = float(wq<19>(1)), wd = float(wq<19>(7));
+    group(1, 2, make_float2(ux, uy), make_float2(nx_, ny_), wa);
+    group(4, 5, make_float2(ux + uy, ux - uy), make_float2(nx_ + ny_, nx_ - ny_), wd);
+    group(6, 7, make_float2(ux + uz, ux - uz), make_float2(nx_ + nz_, nx_ - nz_), wd);
+    group(8, 9, make_float2(uy + uz, uy - uz), make_float2(ny_ + nz_, ny_ - nz_), wd);
+    {
+      // +-z alone
+      const float sg = SC ? 1.0f : wa;
+      const float eu = uz, en = nz_;
+      const float E = om_h * (dph + ph * (4.5f * eu * eu - 1.5f * uu));
+      const float Pq = 3.0f * ph * om_h * eu + src * en;
+      store(5, one_om * h[5] + sg * (E + Pq), true);
+      store(6, one_om * h[6] + sg * (E - Pq), true);
+    }
+  } else {
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
     const int i = 2 * p - 1, j = 2 * p;
@@ -382,6 +432,7 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
       st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, vi);
       st_out_raw<S, 19>(H, stride, nb, PARITY, c, j, vj);
     }
+  }
   }
   {
     const T w = T(wq<19>(0));
