@@ -117,7 +117,9 @@ __device__ __forceinline__ void aniso_function(int kind, T e4, T e2, const T (&n
 // N_c = |grad phi| a (da/dn - n (n . da/dn)) in the crystal frame.  `Rm` is
 // the grain's rotation (row-major, columns = crystal axes) in the arithmetic
 // type.
-template <class T>
+// GEN = false compiles the four-fold cubic kind alone (the form of the
+// reference's default anisotropy()); GEN = true takes any kind at run time.
+template <class T, bool GEN = true>
 __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T eps4, T eps2, const T (&gr)[3],
                                            T& a, T (&N)[3]) {
   T R[9];
@@ -129,12 +131,21 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T
   T nc[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) nc[q] = R[0 * 3 + q] * nl0 + R[1 * 3 + q] * nl1 + R[2 * 3 + q] * nl2;
-  T da[3];
-  aniso_function<T>(kind, eps4, eps2, nc, a, da);
-  const T ndg = nc[0] * da[0] + nc[1] * da[1] + nc[2] * da[2];
   T Nc[3];
+  if constexpr (!GEN) {
+    (void)kind;
+    (void)eps2;
+    const T s4 = nc[0] * nc[0] * nc[0] * nc[0] + nc[1] * nc[1] * nc[1] * nc[1] + nc[2] * nc[2] * nc[2] * nc[2];
+    a = T(1) - T(3) * eps4 + T(4) * eps4 * s4;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) Nc[q] = gn * a * (da[q] - nc[q] * ndg);
+    for (int q = 0; q < 3; ++q) Nc[q] = gn * a * T(16) * eps4 * (nc[q] * nc[q] * nc[q] - nc[q] * s4);
+  } else {
+    T da[3];
+    aniso_function<T>(kind, eps4, eps2, nc, a, da);
+    const T ndg = nc[0] * da[0] + nc[1] * da[1] + nc[2] * da[2];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) Nc[q] = gn * a * (da[q] - nc[q] * ndg);
+  }
 #pragma unroll
   for (int q = 0; q < 3; ++q) N[q] = R[q * 3 + 0] * Nc[0] + R[q * 3 + 1] * Nc[1] + R[q * 3 + 2] * Nc[2];
 }
@@ -143,7 +154,7 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T
 // (SOL = false) or solutal (SOL = true) lattice.  `grain` is the per-cell
 // grain index (read only with more than one grain), `rot` the rotations of
 // the cell's domain, 9 values per grain.
-template <class S, class P, int PARITY, bool SOL, class NB>
+template <class S, class P, int PARITY, bool SOL, bool GEN, class NB>
 __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
                                           const P* __restrict__ phi_old, P* __restrict__ temp,
                                           const unsigned char* __restrict__ grain,
@@ -163,7 +174,7 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
   const T gr[3] = {T(3) * gx, T(3) * gy, T(3) * gz};
   const int gid = k.nobj > 1 ? (int)__ldg(grain + c) : 0;
   T a, N[3];
-  anisotropy<T>(rot + 9 * gid, k.aniso, k.eps4, k.eps2, gr, a, N);
+  anisotropy<T, GEN>(rot + 9 * gid, k.aniso, k.eps4, k.eps2, gr, a, N);
   const T dphi = ph - T(phi_old[c]);
   const T u_old = T(temp[c]);
   const T one_m = T(1) - ph * ph;
@@ -233,7 +244,7 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
   temp[c] = P(k.ref_t + dT);
 }
 
-template <class S, class P, int PARITY, bool SOL>
+template <class S, class P, int PARITY, bool SOL, bool GEN>
 __global__ void __launch_bounds__(256)
     k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
                    P* __restrict__ temp, const unsigned char* __restrict__ grain,
@@ -244,10 +255,10 @@ __global__ void __launch_bounds__(256)
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   if (fastw_cell(g, x, y, z)) {
     const FastW fa = make_fastw(g, x, y, z);
-    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, fa.c, k);
+    dend_cell<S, P, PARITY, SOL, GEN>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, fa.c, k);
   } else {
     const Nbr nb(g, x, y, z);
-    dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, nb.idx(0, 0, 0), k);
+    dend_cell<S, P, PARITY, SOL, GEN>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, nb.idx(0, 0, 0), k);
   }
 }
 

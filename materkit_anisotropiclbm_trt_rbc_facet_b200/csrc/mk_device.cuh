@@ -645,67 +645,19 @@ __device__ __forceinline__ int64_t off_out(int64_t stride, const Nbr& nb, int pa
   return (int64_t)(f ? i : inv(i)) * stride + cell;
 }
 
-// Address of a population: the plane base (a multiple of the stride, the
-// same for every thread) plus a 32-bit cell index, so each access costs one
-// wide multiply-add instead of 64-bit index arithmetic.
-template <class S>
-__device__ __forceinline__ S* plane_at(S* A, int64_t stride, int slot, int cell) {
-  return (A + (int64_t)slot * stride) + cell;
-}
-
-// Address the pre-collision population i of the cell at `c` is read from.
-template <class S, int Q>
-__device__ __forceinline__ S* p_in(S* A, int64_t stride, const Fast& fa, int parity, int, int i) {
-  if (parity == 0) return plane_at(A, stride, i, fa.c);
-  return plane_at(A, stride, inv(i), fa.idx(-ex(i), -ey(i), -ez(i)));
-}
-template <class S, int Q>
-__device__ __forceinline__ S* p_in(S* A, int64_t stride, const FastW& fa, int parity, int, int i) {
-  if (parity == 0) return plane_at(A, stride, i, fa.c);
-  if (ex(i) == 0) return plane_at(A, stride, inv(i), fa.idx(-ex(i), -ey(i), -ez(i)));
-  return fastw_fluid(fa, -ex(i)) ? plane_at(A, stride, inv(i), fa.idx(-ex(i), -ey(i), -ez(i)))
-                                 : plane_at(A, stride, i, fa.c);
-}
-template <class S, int Q>
-__device__ __forceinline__ S* p_in(S* A, int64_t stride, const Nbr& nb, int parity, int c, int i) {
-  if (parity == 0) return plane_at(A, stride, i, c);
-  return nb.fluid(-ex(i), -ey(i), -ez(i)) ? plane_at(A, stride, inv(i), nb.idx(-ex(i), -ey(i), -ez(i)))
-                                          : plane_at(A, stride, i, c);
-}
-
-// Address the post-collision population i of the cell at `c` is written to.
-template <class S, int Q>
-__device__ __forceinline__ S* p_out(S* A, int64_t stride, const Fast& fa, int parity, int, int i) {
-  if (parity == 0) return plane_at(A, stride, inv(i), fa.c);
-  return plane_at(A, stride, i, fa.idx(ex(i), ey(i), ez(i)));
-}
-template <class S, int Q>
-__device__ __forceinline__ S* p_out(S* A, int64_t stride, const FastW& fa, int parity, int, int i) {
-  if (parity == 0) return plane_at(A, stride, inv(i), fa.c);
-  if (ex(i) == 0) return plane_at(A, stride, i, fa.idx(ex(i), ey(i), ez(i)));
-  return fastw_fluid(fa, ex(i)) ? plane_at(A, stride, i, fa.idx(ex(i), ey(i), ez(i)))
-                                : plane_at(A, stride, inv(i), fa.c);
-}
-template <class S, int Q>
-__device__ __forceinline__ S* p_out(S* A, int64_t stride, const Nbr& nb, int parity, int c, int i) {
-  if (parity == 0) return plane_at(A, stride, inv(i), c);
-  return nb.fluid(ex(i), ey(i), ez(i)) ? plane_at(A, stride, i, nb.idx(ex(i), ey(i), ez(i)))
-                                       : plane_at(A, stride, inv(i), c);
-}
-
 // Pre-collision deviation f'_i of the cell at `c` (= nb.idx(0,0,0)); `nb` is
 // a general neighbourhood (Nbr) or an interior-row one (Fast).
 template <class S, int Q, class NB>
 __device__ __forceinline__ typename Stor<S>::T ld_in(const S* __restrict__ A, int64_t stride, const NB& nb,
                                                       int parity, int c, int i) {
-  return Stor<S>::ld(p_in<const S, Q>(A, stride, nb, parity, c, i), typename Stor<S>::T(wq<Q>(i)));
+  return Stor<S>::ld(A + off_in<Q>(stride, nb, parity, c, i), typename Stor<S>::T(wq<Q>(i)));
 }
 
 // Bring the slot that population i of the cell at `c` is read from into L2
 // (no register, no wait), for a load that comes later in the thread.
 template <class S, int Q, class NB>
 __device__ __forceinline__ void pf_in(const S* __restrict__ A, int64_t stride, const NB& nb, int parity, int c, int i) {
-  const S* p = p_in<const S, Q>(A, stride, nb, parity, c, i);
+  const S* p = A + off_in<Q>(stride, nb, parity, c, i);
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
@@ -714,31 +666,31 @@ __device__ __forceinline__ void pf_in(const S* __restrict__ A, int64_t stride, c
 template <class S, int Q, class NB>
 __device__ __forceinline__ typename Stor<S>::T ld_in_raw(const S* __restrict__ A, int64_t stride, const NB& nb,
                                                           int parity, int c, int i) {
-  return Stor<S>::ldr(p_in<const S, Q>(A, stride, nb, parity, c, i));
+  return Stor<S>::ldr(A + off_in<Q>(stride, nb, parity, c, i));
 }
 template <class S, int Q, class NB>
 __device__ __forceinline__ void st_out_raw(S* __restrict__ A, int64_t stride, const NB& nb, int parity, int c, int i,
                                            typename Stor<S>::T v) {
-  Stor<S>::str(p_out<S, Q>(A, stride, nb, parity, c, i), v);
+  Stor<S>::str(A + off_out<Q>(stride, nb, parity, c, i), v);
 }
 template <class S, int Q, class NB>
 __device__ __forceinline__ typename Stor<S>::T st_out_raw_rt(S* __restrict__ A, int64_t stride, const NB& nb,
                                                               int parity, int c, int i, typename Stor<S>::T v) {
-  return Stor<S>::str_rt(p_out<S, Q>(A, stride, nb, parity, c, i), v);
+  return Stor<S>::str_rt(A + off_out<Q>(stride, nb, parity, c, i), v);
 }
 
 // Store the post-collision deviation f'_i of the cell at `c`.
 template <class S, int Q, class NB>
 __device__ __forceinline__ void st_out(S* __restrict__ A, int64_t stride, const NB& nb, int parity, int c, int i,
                                        typename Stor<S>::T v) {
-  Stor<S>::st(p_out<S, Q>(A, stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
+  Stor<S>::st(A + off_out<Q>(stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
 }
 
 // Store and return the value a later load will see.
 template <class S, int Q, class NB>
 __device__ __forceinline__ typename Stor<S>::T st_out_rt(S* __restrict__ A, int64_t stride, const NB& nb, int parity,
                                                           int c, int i, typename Stor<S>::T v) {
-  return Stor<S>::st_rt(p_out<S, Q>(A, stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
+  return Stor<S>::st_rt(A + off_out<Q>(stride, nb, parity, c, i), v, typename Stor<S>::T(wq<Q>(i)));
 }
 
 // Neighbour queries common to both neighbourhood kinds.

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(TILE)
 
 // Four resident 256-thread blocks per SM (64 registers) for the 32-bit and
 // 16-bit variants; the FP64 one keeps its registers.
-template <class S, class P, int PARITY, bool SOL>
+template <class S, class P, int PARITY, bool SOL, bool GEN>
 __global__ void __launch_bounds__(TILE, sizeof(typename Stor<S>::T) == 8 ? 2 : 4)
     k_ens_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
                   const P* __restrict__ phi_old, P* __restrict__ temp, const unsigned char* __restrict__ grain,
@@ -116,11 +116,12 @@ __global__ void __launch_bounds__(TILE, sizeof(typename Stor<S>::T) == 8 ? 2 : 4
     if (fastw_cell(di.g, x, y, z)) {
       FastW fa = make_fastw(di.g, x, y, z);
       fa.c += di.off;
-      dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, grain, rd, di.g.stride, fa, fa.c, k);
+      dend_cell<S, P, PARITY, SOL, GEN>(G, Tp, phi_new, phi_old, temp, grain, rd, di.g.stride, fa, fa.c, k);
     } else {
       Nbr nb(di.g, x, y, z);
       nb.base = di.off;
-      dend_cell<S, P, PARITY, SOL>(G, Tp, phi_new, phi_old, temp, grain, rd, di.g.stride, nb, nb.idx(0, 0, 0), k);
+      dend_cell<S, P, PARITY, SOL, GEN>(G, Tp, phi_new, phi_old, temp, grain, rd, di.g.stride, nb, nb.idx(0, 0, 0),
+                                        k);
     }
   }
 }
@@ -184,6 +185,7 @@ struct mk_ensemble {
   int ntiles = 0;
   int device = 0, sms = 148;
   int grid_phi[2] = {1, 1}, grid_col[2] = {1, 1};  // persistent launch sizes per parity
+  bool gen_aniso = false;  // some domain has a non-cubic anisotropy kind
   cudaStream_t stream = nullptr;
   void* pop0 = nullptr;
   void* pop1 = nullptr;
@@ -231,7 +233,7 @@ int persistent_grid(const mk_ensemble& e, K kernel) {
 
 // One loop.  When `ev` is non-null, ev[0..1] bracket the phi launch and
 // ev[2..3] the collide launch.
-template <class S, bool SOL>
+template <class S, bool SOL, bool GEN>
 void loop_t(mk_ensemble& e, cudaEvent_t* ev) {
   typedef typename Stor<S>::T T;
   typedef typename PhiOf<S>::type P;
@@ -254,11 +256,11 @@ void loop_t(mk_ensemble& e, cudaEvent_t* ev) {
     cudaEventRecord(ev[2], e.stream);
   }
   if (parity == 0)
-    k_ens_collide<S, P, 0, SOL><<<e.grid_col[0], TILE, 0, e.stream>>>(G, Tp, phi_new, phi_old, (P*)e.temp, e.grain,
+    k_ens_collide<S, P, 0, SOL, GEN><<<e.grid_col[0], TILE, 0, e.stream>>>(G, Tp, phi_new, phi_old, (P*)e.temp, e.grain,
                                                                        (const T*)e.rot, e.dom, kd, e.tile_dom,
                                                                        e.ntiles);
   else
-    k_ens_collide<S, P, 1, SOL><<<e.grid_col[1], TILE, 0, e.stream>>>(G, Tp, phi_new, phi_old, (P*)e.temp, e.grain,
+    k_ens_collide<S, P, 1, SOL, GEN><<<e.grid_col[1], TILE, 0, e.stream>>>(G, Tp, phi_new, phi_old, (P*)e.temp, e.grain,
                                                                        (const T*)e.rot, e.dom, kd, e.tile_dom,
                                                                        e.ntiles);
   if (ev) cudaEventRecord(ev[3], e.stream);
@@ -269,10 +271,18 @@ void loop_t(mk_ensemble& e, cudaEvent_t* ev) {
 
 template <class S>
 void loop_s(mk_ensemble& e, cudaEvent_t* ev) {
-  if (e.model == MK_MODEL_SOLUTAL_DENDRITE)
-    loop_t<S, true>(e, ev);
-  else
-    loop_t<S, false>(e, ev);
+  const bool sol = e.model == MK_MODEL_SOLUTAL_DENDRITE;
+  if (e.gen_aniso) {
+    if (sol)
+      loop_t<S, true, true>(e, ev);
+    else
+      loop_t<S, false, true>(e, ev);
+  } else {
+    if (sol)
+      loop_t<S, true, false>(e, ev);
+    else
+      loop_t<S, false, false>(e, ev);
+  }
 }
 
 void ens_loop(mk_ensemble& e, cudaEvent_t* ev = nullptr) {
@@ -299,8 +309,16 @@ void size_grids(mk_ensemble& e) {
   // each parity has its own register footprint, hence its own resident count
   e.grid_phi[0] = persistent_grid(e, k_ens_phi<S, P, 0>);
   e.grid_phi[1] = persistent_grid(e, k_ens_phi<S, P, 1>);
-  e.grid_col[0] = sol ? persistent_grid(e, k_ens_collide<S, P, 0, true>) : persistent_grid(e, k_ens_collide<S, P, 0, false>);
-  e.grid_col[1] = sol ? persistent_grid(e, k_ens_collide<S, P, 1, true>) : persistent_grid(e, k_ens_collide<S, P, 1, false>);
+  for (int par = 0; par < 2; ++par) {
+    int g;
+    if (e.gen_aniso)
+      g = sol ? persistent_grid(e, par ? k_ens_collide<S, P, 1, true, true> : k_ens_collide<S, P, 0, true, true>)
+              : persistent_grid(e, par ? k_ens_collide<S, P, 1, false, true> : k_ens_collide<S, P, 0, false, true>);
+    else
+      g = sol ? persistent_grid(e, par ? k_ens_collide<S, P, 1, true, false> : k_ens_collide<S, P, 0, true, false>)
+              : persistent_grid(e, par ? k_ens_collide<S, P, 1, false, false> : k_ens_collide<S, P, 0, false, false>);
+    e.grid_col[par] = g;
+  }
 }
 
 // Per-domain coefficients and the rotations, in the arithmetic type.
@@ -490,6 +508,7 @@ mk_status mk_ensemble_create(const mk_params* params, int32_t n_domains, mk_ense
   e->model = params[0].model;
   e->precision = params[0].precision;
   e->elem = store_bytes(e->precision);
+  for (int d = 0; d < n_domains; ++d) e->gen_aniso = e->gen_aniso || params[d].aniso != MK_ANISO_CUBIC;
   e->phi_elem = e->precision == MK_PREC_FP64 ? 8 : 4;
   cudaGetDevice(&e->device);
   cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device);

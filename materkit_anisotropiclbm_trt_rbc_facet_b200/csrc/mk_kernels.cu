@@ -1030,21 +1030,22 @@ void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t*
     cudaEventRecord(ev[2], e.stream);
   }
   const bool sol = e.p.model == MK_MODEL_SOLUTAL_DENDRITE;
+  const bool gen = e.p.aniso != MK_ANISO_CUBIC;
+#define MK_DEND(PAR, SOL, GEN)                                                                              \
+  k_dend_collide<S, P, PAR, SOL, GEN><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain, \
+                                                                    (const T*)e.rot, g, k)
   if (parity == 0) {
     if (sol)
-      k_dend_collide<S, P, 0, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
-                                                                   (const T*)e.rot, g, k);
+      gen ? MK_DEND(0, true, true) : MK_DEND(0, true, false);
     else
-      k_dend_collide<S, P, 0, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
-                                                                   (const T*)e.rot, g, k);
+      gen ? MK_DEND(0, false, true) : MK_DEND(0, false, false);
   } else {
     if (sol)
-      k_dend_collide<S, P, 1, true><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
-                                                                   (const T*)e.rot, g, k);
+      gen ? MK_DEND(1, true, true) : MK_DEND(1, true, false);
     else
-      k_dend_collide<S, P, 1, false><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain,
-                                                                   (const T*)e.rot, g, k);
+      gen ? MK_DEND(1, false, true) : MK_DEND(1, false, false);
   }
+#undef MK_DEND
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
 
