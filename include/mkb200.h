@@ -60,9 +60,12 @@ typedef enum mk_model {
   MK_MODEL_MULTIPHASE = 1,       /* Allen-Cahn two-phase flow, run_flow_multiphase (:290-331)     */
   MK_MODEL_THERMAL_DENDRITE = 2, /* phase field + thermal ADE, run_thermal_dendrite (:743-788)    */
   MK_MODEL_SOLUTAL_DENDRITE = 3, /* phase field + solutal ADE, run_solutal_dendrite (:633-687)    */
-  MK_MODEL_CONVECTION = 4        /* flow + advected D3Q7 scalar with Boussinesq buoyancy and
+  MK_MODEL_CONVECTION = 4,       /* flow + advected D3Q7 scalar with Boussinesq buoyancy and
                                     Dirichlet plates: Rayleigh-Benard (bdy_RBC, Thermal_NusseltRBC,
                                     mkThermalField.h:33-40, mkFluidsLBM.h:59-68)                  */
+  MK_MODEL_FLOW_DENDRITE = 5     /* thermal dendrite growing in a flow: porous bounce-back of the
+                                    flow by the solid fraction, thermal lattice advected, inflow /
+                                    outflow faces, run_flow_thermal_dendrite (MaterKit.cpp:467-527) */
 } mk_model;
 
 /* Population storage precision.  Collision arithmetic is FP64 for MK_PREC_FP64

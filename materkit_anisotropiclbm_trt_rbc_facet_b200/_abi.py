@@ -16,7 +16,8 @@ MK_OK, MK_ERR_XML, MK_ERR_ARG, MK_ERR_CUDA, MK_ERR_DIVERGED, MK_ERR_TIMEOUT, MK_
 STATUS_NAMES = {0: "MK_OK", 1: "MK_ERR_XML", 2: "MK_ERR_ARG", 3: "MK_ERR_CUDA", 4: "MK_ERR_DIVERGED",
                 5: "MK_ERR_TIMEOUT", 6: "MK_ERR_OOM", 7: "MK_ERR_IO", 8: "MK_ERR_STATE", 9: "MK_ERR_NODEVICE"}
 
-MK_MODEL_FLOW, MK_MODEL_MULTIPHASE, MK_MODEL_THERMAL_DENDRITE, MK_MODEL_SOLUTAL_DENDRITE, MK_MODEL_CONVECTION = range(5)
+(MK_MODEL_FLOW, MK_MODEL_MULTIPHASE, MK_MODEL_THERMAL_DENDRITE, MK_MODEL_SOLUTAL_DENDRITE, MK_MODEL_CONVECTION,
+ MK_MODEL_FLOW_DENDRITE) = range(6)
 MK_PREC_FP64, MK_PREC_FP32, MK_PREC_FP16, MK_PREC_BF16 = range(4)
 MK_COLL_BGK, MK_COLL_TRT, MK_COLL_MRT = range(3)
 MK_D3Q7, MK_D3Q19, MK_D3Q27 = 7, 19, 27
@@ -26,12 +27,14 @@ ANISOTROPIES = {"cubic": MK_ANISO_CUBIC, "cbc": MK_ANISO_CBC, "hcp": MK_ANISO_HC
 (MK_FIELD_RHO, MK_FIELD_UX, MK_FIELD_UY, MK_FIELD_UZ, MK_FIELD_T, MK_FIELD_C, MK_FIELD_PHI, MK_FIELD_FLAG,
  MK_FIELD_PRESSURE, MK_FIELD_DPHI, MK_FIELD_GRAIN) = range(11)
 MK_DTYPE_F64, MK_DTYPE_F32 = 0, 1
+MK_FLAG_FLUID, MK_FLAG_INTER, MK_FLAG_SOLID, MK_FLAG_WALLS = range(4)
 MK_MAX_OBJECTS = 64
 MK_NOALLOC_MAX_CELLS = 2048 * 256 * 64
 
 PRECISIONS = {"fp64": MK_PREC_FP64, "fp32": MK_PREC_FP32, "fp16": MK_PREC_FP16, "bf16": MK_PREC_BF16}
 MODELS = {"flow": MK_MODEL_FLOW, "multiphase": MK_MODEL_MULTIPHASE, "thermal_dendrite": MK_MODEL_THERMAL_DENDRITE,
-          "solutal_dendrite": MK_MODEL_SOLUTAL_DENDRITE, "convection": MK_MODEL_CONVECTION}
+          "solutal_dendrite": MK_MODEL_SOLUTAL_DENDRITE, "convection": MK_MODEL_CONVECTION,
+          "flow_dendrite": MK_MODEL_FLOW_DENDRITE}
 FIELDS = {"rho": MK_FIELD_RHO, "ux": MK_FIELD_UX, "uy": MK_FIELD_UY, "uz": MK_FIELD_UZ, "T": MK_FIELD_T,
           "C": MK_FIELD_C, "phi": MK_FIELD_PHI, "flag": MK_FIELD_FLAG, "pressure": MK_FIELD_PRESSURE,
           "dphi": MK_FIELD_DPHI, "grain": MK_FIELD_GRAIN}

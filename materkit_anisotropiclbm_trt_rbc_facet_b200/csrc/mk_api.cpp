@@ -139,7 +139,7 @@ mk_status mk_create(const mk_params* p, mk_handle** out) {
   const size_t n = (size_t)h->e.ncell;
   const bool flow = p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION;
   const bool scalar = p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
-                      p->model == MK_MODEL_CONVECTION;
+                      p->model == MK_MODEL_CONVECTION || p->model == MK_MODEL_FLOW_DENDRITE;
   std::vector<double> phi(flow ? 0 : n), temp(scalar ? n : 0), rho(flow ? n : 0);
   if (!flow) mkc::initial_field(p, MK_FIELD_PHI, phi.data(), n, err);
   if (scalar) mkc::initial_field(p, MK_FIELD_T, temp.data(), n, err);
@@ -326,7 +326,7 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   std::vector<double> rho(n, 1.0), grain(n, 0.0), phi(n, 0.0), dphi(n, 0.0), conc(n, 0.0), temp(n, 0.0), ux(n, 0.0),
       uy(n, 0.0), uz(n, 0.0);
   mk_status s;
-  if (m == MK_MODEL_FLOW || m == MK_MODEL_MULTIPHASE || m == MK_MODEL_CONVECTION) {
+  if (m == MK_MODEL_FLOW || m == MK_MODEL_MULTIPHASE || m == MK_MODEL_CONVECTION || m == MK_MODEL_FLOW_DENDRITE) {
     if ((s = copy_field(h, MK_FIELD_RHO, rho)) != MK_OK) return s;
     if ((s = copy_field(h, MK_FIELD_UX, ux)) != MK_OK) return s;
     if ((s = copy_field(h, MK_FIELD_UY, uy)) != MK_OK) return s;
@@ -335,11 +335,10 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   if ((s = copy_field(h, MK_FIELD_GRAIN, grain)) != MK_OK) return s;
   if ((s = copy_field(h, MK_FIELD_PHI, phi)) != MK_OK) return s;
   if (m == MK_MODEL_CONVECTION && (s = copy_field(h, MK_FIELD_T, temp)) != MK_OK) return s;
-  if (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE) {
+  if (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE) {
+    const bool th = m != MK_MODEL_SOLUTAL_DENDRITE;
     if ((s = copy_field(h, MK_FIELD_DPHI, dphi)) != MK_OK) return s;
-    if ((s = copy_field(h, m == MK_MODEL_THERMAL_DENDRITE ? MK_FIELD_T : MK_FIELD_C,
-                        m == MK_MODEL_THERMAL_DENDRITE ? temp : conc)) != MK_OK)
-      return s;
+    if ((s = copy_field(h, th ? MK_FIELD_T : MK_FIELD_C, th ? temp : conc)) != MK_OK) return s;
   }
   std::ostringstream fn;
   fn << dir << "/fluid_t" << loops << ".vtk";
@@ -440,7 +439,9 @@ mk_status mk_nusselt(mk_handle* h, double* nu) {
 }
 
 // Checkpoint layout: magic, version, params hash, step, phi_cur, precision,
-// byte counts, then raw population planes, phi buffers and T/U.
+// byte counts, then raw population planes, phi buffers and T/U, the FP32 rest
+// plane (16-bit multiphase) and the flow lattice of the flow + dendrite model
+// (sizes implied by the parameters the hash covers).
 static const char kMagic[8] = {'M', 'K', 'B', '2', '0', '0', 'C', 'K'};
 
 mk_status mk_checkpoint(mk_handle* h, const char* path) {
@@ -477,6 +478,7 @@ mk_status mk_checkpoint(mk_handle* h, const char* path) {
   dump(e.phi[1], e.phi[1] ? bp : 0);
   dump(e.temp, e.temp ? bp : 0);
   dump(e.rest1, e.rest1 ? (uint64_t)e.ncell * sizeof(float) : 0);
+  dump(e.pop2, mke::engine_pop_bytes(e, 2));
   fclose(f);
   if (!ok) {
     h->err = std::string("checkpoint write failed: ") + path;
@@ -528,6 +530,7 @@ mk_status mk_restore(mk_handle* h, const char* path) {
   load(e.phi[1], e.phi[1] ? bp : 0);
   load(e.temp, e.temp ? bp : 0);
   load(e.rest1, e.rest1 ? (uint64_t)e.ncell * sizeof(float) : 0);
+  load(e.pop2, mke::engine_pop_bytes(e, 2));
   fclose(f);
   if (!ok) {
     h->err = "checkpoint truncated";
@@ -550,20 +553,21 @@ mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel, dou
     h->err = std::string("no kernel named ") + kernel;
     return MK_ERR_ARG;
   }
-  std::vector<cudaEvent_t> ev((size_t)nsteps * 4);
+  const size_t per = (size_t)2 * kps;
+  std::vector<cudaEvent_t> ev((size_t)nsteps * per);
   for (auto& x : ev) cudaEventCreate(&x);
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, e.stream);
-  for (int64_t s = 0; s < nsteps; ++s) mke::engine_step(e, &ev[(size_t)s * 4]);
+  for (int64_t s = 0; s < nsteps; ++s) mke::engine_step(e, &ev[(size_t)s * per]);
   cudaEventRecord(t1, e.stream);
   cudaError_t st = cudaEventSynchronize(t1);
   double kt = 0;
   if (st == cudaSuccess) {
     for (int64_t s = 0; s < nsteps; ++s) {
       float ms = 0;
-      cudaEventElapsedTime(&ms, ev[(size_t)s * 4 + 2 * slot], ev[(size_t)s * 4 + 2 * slot + 1]);
+      cudaEventElapsedTime(&ms, ev[(size_t)s * per + 2 * slot], ev[(size_t)s * per + 2 * slot + 1]);
       kt += ms;
     }
     float tot = 0;

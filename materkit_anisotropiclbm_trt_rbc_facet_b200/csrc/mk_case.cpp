@@ -223,7 +223,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model < 0 || p->model > 4) {
+  if (p->model < 0 || p->model > 5) {
     err = "unknown model";
     return MK_ERR_ARG;
   }
@@ -253,7 +253,21 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) {
+  if (p->inlet) {
+    if (p->model != MK_MODEL_FLOW && p->model != MK_MODEL_FLOW_DENDRITE) {
+      err = "inflow / outflow faces apply to the flow and flow + dendrite models";
+      return MK_ERR_ARG;
+    }
+    if (p->bc[0] != MK_BC_CLOSED || p->nx < 3) {
+      err = "inflow / outflow faces need closed x faces and at least 3 cells along x";
+      return MK_ERR_ARG;
+    }
+    if (p->wall_axis == 0) {
+      err = "inflow / outflow faces and plates on x exclude each other";
+      return MK_ERR_ARG;
+    }
+  }
+  if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION || p->model == MK_MODEL_FLOW_DENDRITE) {
     if (p->lattice != MK_D3Q19 && p->lattice != MK_D3Q27) {
       err = "flow lattice must be D3Q19 or D3Q27";
       return MK_ERR_ARG;
@@ -283,7 +297,9 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       err = "multiphase parameters out of range (tau > 1/2, densities, W, M > 0)";
       return MK_ERR_ARG;
     }
-  } else {
+  }
+  if (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
+      p->model == MK_MODEL_FLOW_DENDRITE) {
     if (!(p->W0 > 0 && p->tau0 > 0 && p->D > 0)) {
       err = "phase-field parameters out of range (W0, tau0, D > 0)";
       return MK_ERR_ARG;
@@ -359,6 +375,8 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       model = MK_MODEL_SOLUTAL_DENDRITE;
     else if (m == "convection" || m == "rbc" || m == "rayleigh_benard")
       model = MK_MODEL_CONVECTION;
+    else if (m == "flow_dendrite" || m == "flow_thermal_dendrite")
+      model = MK_MODEL_FLOW_DENDRITE;
     else {
       err = "<b200><model>: unknown model '" + m + "'";
       return MK_ERR_XML;
@@ -366,10 +384,14 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
   }
   if (opt && opt->model >= 0) model = opt->model;
   if (model < 0) {
-    bool dendrite = false;
+    // calcMode as the reference's driver reads it: a dendrite in a flow
+    // (run_flow_thermal_dendrite), a dendrite alone, or a flow alone
+    bool dendrite = false, flowfield = false;
     if (const mkx::Element* e = r->path("calcMode/dendrite"))
       if (!mkx::read_bool(e, dendrite, err)) return MK_ERR_XML;
-    model = dendrite ? MK_MODEL_THERMAL_DENDRITE : MK_MODEL_FLOW;
+    if (const mkx::Element* e = r->path("calcMode/flowField"))
+      if (!mkx::read_bool(e, flowfield, err)) return MK_ERR_XML;
+    model = dendrite ? (flowfield ? MK_MODEL_FLOW_DENDRITE : MK_MODEL_THERMAL_DENDRITE) : MK_MODEL_FLOW;
   }
   p.model = model;
 
@@ -458,7 +480,7 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       p.lambda = lam;
     else if (d0 > 0)
       p.lambda = 0.8839 * W0 / d0;
-    if (model == MK_MODEL_THERMAL_DENDRITE) {
+    if (model == MK_MODEL_THERMAL_DENDRITE || model == MK_MODEL_FLOW_DENDRITE) {
       if (!opt_d(r, "temperature/alphaFluid", alpha, err) || !opt_d(r, "temperature/undercooling", under, err) ||
           !opt_d(r, "temperature/iniValue", ini, err))
         return MK_ERR_XML;
@@ -475,6 +497,25 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       if (iv < 1e299) p.delta = -iv;
     }
     p.bc[0] = p.bc[1] = p.bc[2] = MK_BC_CLOSED;
+    if (model == MK_MODEL_FLOW_DENDRITE) {
+      // the melt flows in at x = 0 with flow/velocityInlet and out at
+      // x = nx - 1 (boundary_vel, mkFluidsUser.cpp:455-617); periodic across
+      double nu = -1;
+      std::vector<double> vin, acc;
+      if (!opt_d(r, "phases/fluid/kinematicViscosity", nu, err) || !opt_v(r, "flow/velocityInlet", vin, err) ||
+          !opt_v(r, "flow/acceleration", acc, err))
+        return MK_ERR_XML;
+      if (nu > 0) p.tau = 3.0 * nu * dt / (dx * dx) + 0.5;
+      if (omega_f > 0) p.tau = 1.0 / omega_f;
+      for (int a = 0; a < 3; ++a) {
+        p.u0[a] = a < (int)vin.size() ? vin[a] * dt / dx : 0.0;
+        p.force[a] = (a < (int)acc.size() ? acc[a] : 0.0) + g_lu[a];
+      }
+      p.rho0 = 1.0;
+      p.inlet = 1;
+      p.bc[1] = p.bc[2] = MK_BC_PERIODIC;
+      p.collision = MK_COLL_TRT;
+    }
     if (!read_seeds(r->path("phasechange/seed"), &p, err)) return MK_ERR_XML;
   }
 
@@ -617,6 +658,11 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       }
     }
     if (!opt_d(b, "beta", p.beta, err) || !opt_d(b, "sRef", p.s_ref, err)) return MK_ERR_XML;
+    {
+      double inl = p.inlet;
+      if (!opt_d(b, "inlet", inl, err)) return MK_ERR_XML;
+      p.inlet = inl != 0.0 ? 1 : 0;
+    }
     if (const mkx::Element* o = b->child("objects")) {
       if (!read_seeds(o, &p, err)) return MK_ERR_XML;
     }
@@ -662,6 +708,22 @@ static double bubble_phi(const mk_params* p, const double pos[3], const int n3[3
   return ph;
 }
 
+// Solid seeds (phi = +1) in liquid (phi = -1): the largest of
+// -tanh((r_k - R_k)/(sqrt(2) W0)) over the seeds.
+static double seed_phi(const mk_params* p, const double pos[3]) {
+  double ph = -1.0;
+  for (int k = 0; k < p->n_objects; ++k) {
+    double d2 = 0;
+    for (int a = 0; a < 3; ++a) {
+      const double d = pos[a] - p->obj_center[k][a];
+      d2 += d * d;
+    }
+    const double ph_k = -std::tanh((std::sqrt(d2) - p->obj_radius[k]) / (std::sqrt(2.0) * p->W0));
+    if (ph_k > ph) ph = ph_k;
+  }
+  return ph;
+}
+
 mk_status initial_field(const mk_params* p, int field, double* out, size_t ncells, std::string& err) {
   const size_t n = (size_t)p->nx * p->ny * p->nz;
   if (ncells < n) {
@@ -687,7 +749,13 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
           case MK_FIELD_UX:
           case MK_FIELD_UY:
           case MK_FIELD_UZ:
-            v = (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) ? p->u0[field - MK_FIELD_UX] : 0.0;
+            if (p->model == MK_MODEL_FLOW_DENDRITE) {
+              // u0 scaled by the liquid fraction of the seeded phi
+              const double ns = std::min(1.0, std::max(0.0, 0.5 * (1.0 + seed_phi(p, pos))));
+              v = (1.0 - ns) * p->u0[field - MK_FIELD_UX];
+            } else {
+              v = (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) ? p->u0[field - MK_FIELD_UX] : 0.0;
+            }
             break;
           case MK_FIELD_T:
           case MK_FIELD_C:
@@ -724,7 +792,10 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
                 best = k;
               }
             }
-            v = (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE) ? best : 0;
+            v = (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
+                 p->model == MK_MODEL_FLOW_DENDRITE)
+                    ? best
+                    : 0;
             break;
           }
           case MK_FIELD_PHI:
@@ -733,18 +804,7 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
             } else if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) {
               v = 0.0;
             } else {
-              // solid seeds (phi = +1) in liquid (phi = -1): -tanh((r - R)/(sqrt(2) W0))
-              double ph = -1.0;
-              for (int k = 0; k < p->n_objects; ++k) {
-                double d2 = 0;
-                for (int a = 0; a < 3; ++a) {
-                  const double d = pos[a] - p->obj_center[k][a];
-                  d2 += d * d;
-                }
-                const double ph_k = -std::tanh((std::sqrt(d2) - p->obj_radius[k]) / (std::sqrt(2.0) * p->W0));
-                if (ph_k > ph) ph = ph_k;
-              }
-              v = ph;
+              v = seed_phi(p, pos);
             }
             break;
           default:

@@ -153,13 +153,17 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T
 // One loop of a dendrite cell: the phase-field lattice, then the thermal
 // (SOL = false) or solutal (SOL = true) lattice.  `grain` is the per-cell
 // grain index (read only with more than one grain), `rot` the rotations of
-// the cell's domain, 9 values per grain.
-template <class S, class P, int PARITY, bool SOL, bool GEN, class NB>
+// the cell's domain, 9 values per grain.  ADV = true advects the thermal
+// equilibrium with the flow velocity (vx, vy, vz): t_eq = w T (1 + 4 e.u)
+// (mkThermalField::relaxation with a flow lattice, getTEquPDFs).
+template <class S, class P, int PARITY, bool SOL, bool GEN, class NB, bool ADV = false>
 __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
                                           const P* __restrict__ phi_old, P* __restrict__ temp,
                                           const unsigned char* __restrict__ grain,
                                           const typename Stor<S>::T* __restrict__ rot, const int64_t stride,
-                                          const NB& nb, const int c, const DendK<typename Stor<S>::T>& k) {
+                                          const NB& nb, const int c, const DendK<typename Stor<S>::T>& k,
+                                          typename Stor<S>::T vx = 0, typename Stor<S>::T vy = 0,
+                                          typename Stor<S>::T vz = 0) {
   typedef typename Stor<S>::T T;
   const T ph = T(phi_new[c]);
   T gx = T(0), gy = T(0), gz = T(0);
@@ -237,7 +241,12 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
       const T w = T(wq<7>(i));
-      const T to = t[i] - k.om_t * (t[i] - w * dT) + w * lat;
+      T eq = dT;
+      if constexpr (ADV) {
+        const T eu = T(ex(i)) * vx + T(ey(i)) * vy + T(ez(i)) * vz;
+        if (i > 0) eq += T(4) * (k.ref_t + dT) * eu;
+      }
+      const T to = t[i] - k.om_t * (t[i] - w * eq) + w * lat;
       st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
     }
   }

@@ -38,6 +38,7 @@ struct Engine {
   int elem;           // bytes per stored population
   int phi_elem;       // bytes per phi / temperature value (8 for FP64, else 4)
   int Q0, Q1;         // populations of lattice 0 and 1 (0 if absent)
+  int Q2;             // populations of lattice 2: the flow of the flow + dendrite model, else 0
   int64_t step;       // completed loops
   int phi_cur;        // dendrites: index of the current phi buffer
   cudaStream_t stream;
@@ -47,6 +48,9 @@ struct Engine {
   // device buffers
   void* pop0;
   void* pop1;
+  void* pop2;         // flow lattice of the flow + dendrite model (deviations f - w rho0)
+  void* face_u;       // flow + dendrite with inflow/outflow: collision velocity of the planes x = 1 and
+                      // x = nx - 2 (2 x 3 x ny nz values, phi type), read by the boundary kernel
   float* rest1;       // FP32 rest population of lattice 1 (multiphase h) with 16-bit storage, else null
   void* phi[2];
   void* temp;

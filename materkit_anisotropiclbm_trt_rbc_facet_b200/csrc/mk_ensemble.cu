@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mkb200.h"
@@ -548,12 +549,21 @@ mk_status mk_ensemble_create(const mk_params* params, int32_t n_domains, mk_ense
     for (int64_t t = e->off[d] / TILE; t < (e->off[d] + c) / TILE; ++t) tile_dom[t] = d;
   }
   // initial fields (mkSpace + initialize of every domain), packed
+  // (independent per domain: host threads take domains in turn)
   std::vector<double> h_init((size_t)2 * off);
-  for (int d = 0; d < n_domains; ++d) {
-    const size_t c = (size_t)params[d].nx * params[d].ny * params[d].nz;
-    std::string err;
-    mkc::initial_field(&params[d], MK_FIELD_PHI, h_init.data() + e->off[d], c, err);
-    mkc::initial_field(&params[d], MK_FIELD_T, h_init.data() + off + e->off[d], c, err);
+  {
+    const int nth = std::max(1, std::min<int>(n_domains, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; ++t)
+      pool.emplace_back([&, t]() {
+        for (int d = t; d < n_domains; d += nth) {
+          const size_t c = (size_t)params[d].nx * params[d].ny * params[d].nz;
+          std::string err;
+          mkc::initial_field(&params[d], MK_FIELD_PHI, h_init.data() + e->off[d], c, err);
+          mkc::initial_field(&params[d], MK_FIELD_T, h_init.data() + off + e->off[d], c, err);
+        }
+      });
+    for (std::thread& th : pool) th.join();
   }
   double* d_init = nullptr;
   auto fail = [&](cudaError_t s, const char* where) {

@@ -472,9 +472,184 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
 
 namespace {
 
+// ============================================== FLOW + DENDRITE (a1/a7/a8)
+// run_flow_thermal_dendrite (MaterKit.cpp:467-527): per loop the flow lattice
+// with the partially saturated porous bounce-back (mkFluidsMRT::propagate_PBB
+// and relaxation), the phase field, the thermal lattice advected by the flow,
+// then the inflow/outflow faces (bdyVelocity, bdy_flowin).  The porous
+// bounce-back follows Noble & Torczynski (Int. J. Mod. Phys. C 9 (1998)
+// 1189): with the solid fraction n_s = clamp((1 + phi)/2) of the previous
+// loop and B = n_s (tau - 1/2) / ((1 - n_s) + (tau - 1/2)),
+//   f* = f_coll + B (Omega_s - (f_coll - f)),
+//   Omega_s = f_inv(i) - f_i + feq_i(rho, 0) - feq_inv(i)(rho, u).
+template <class T>
+struct FdK {
+  FlowK<T> f;     // flow lattice coefficients (ref = rho0)
+  T half;         // tau - 1/2
+  T u0[3];        // inflow velocity
+  T ref_g, ref_t; // rest values of the phase-field and thermal lattices (-1, -Delta)
+  int inlet;      // 1: inflow at x = 0, outflow at x = nx - 1
+};
+
+template <class S, class P, int Q, int COLL, int PARITY, bool GEN, class NB>
+__device__ __forceinline__ void fd_cell(S* __restrict__ W, S* __restrict__ G, S* __restrict__ Tp,
+                                        const P* __restrict__ phi_new, const P* __restrict__ phi_old,
+                                        P* __restrict__ temp, P* __restrict__ face_u,
+                                        const unsigned char* __restrict__ grain,
+                                        const typename Stor<S>::T* __restrict__ rot, const Geom& g, const NB& nb,
+                                        const int c, const int x, const int yz, const DendK<typename Stor<S>::T>& kd,
+                                        const FdK<typename Stor<S>::T>& k) {
+  typedef typename Stor<S>::T T;
+  T ux, uy, uz;
+  {
+    T f[Q], fc[Q];  // deviations f_i - w_i rho0 before and after the fluid collision
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      f[i] = ld_in<S, Q>(W, g.stride, nb, PARITY, c, i);
+      fc[i] = f[i];
+    }
+    flow_relax<T, Q, COLL>(fc, k.f, k.f.Fx, k.f.Fy, k.f.Fz, ux, uy, uz);
+    const T ns = fmin(T(1), fmax(T(0), T(0.5) * (T(1) + T(phi_old[c]))));
+    if (ns > T(0)) {
+      const T B = ns * k.half / ((T(1) - ns) + k.half);
+      T drho = T(0);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) drho += f[i];
+      const T rho = k.f.ref + drho;
+      const T uu = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        const T w = T(wq<Q>(i));
+        const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
+        // rho w - feq_inv(i)(rho, u) with e_inv(i).u = -e_i.u
+        const T om_s = f[inv(i)] - f[i] - rho * w * (T(-3) * eu + T(4.5) * eu * eu - T(1.5) * uu);
+        fc[i] += B * (om_s - (fc[i] - f[i]));
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) st_out<S, Q>(W, g.stride, nb, PARITY, c, i, fc[i]);
+  }
+  if (k.inlet) {
+    const int plane = g.ny * g.nz;
+    if (x == 1) {
+      face_u[yz] = P(ux);
+      face_u[plane + yz] = P(uy);
+      face_u[2 * plane + yz] = P(uz);
+    }
+    if (x == g.nx - 2) {
+      face_u[3 * plane + yz] = P(ux);
+      face_u[4 * plane + yz] = P(uy);
+      face_u[5 * plane + yz] = P(uz);
+    }
+  }
+  dend_cell<S, P, PARITY, false, GEN, NB, true>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, kd, ux,
+                                                uy, uz);
+}
+
+template <class S, class P, int Q, int COLL, int PARITY, bool GEN>
+__global__ void __launch_bounds__(256)
+    k_fd_collide(S* __restrict__ W, S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
+                 const P* __restrict__ phi_old, P* __restrict__ temp, P* __restrict__ face_u,
+                 const unsigned char* __restrict__ grain, const typename Stor<S>::T* __restrict__ rot, const Geom g,
+                 const DendK<typename Stor<S>::T> kd, const FdK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int yz = y + g.ny * z;
+  if (fastw_cell(g, x, y, z)) {
+    const FastW fa = make_fastw(g, x, y, z);
+    fd_cell<S, P, Q, COLL, PARITY, GEN>(W, G, Tp, phi_new, phi_old, temp, face_u, grain, rot, g, fa, fa.c, x, yz, kd,
+                                        k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    fd_cell<S, P, Q, COLL, PARITY, GEN>(W, G, Tp, phi_new, phi_old, temp, face_u, grain, rot, g, nb, nb.idx(0, 0, 0),
+                                        x, yz, kd, k);
+  }
+}
+
+// Non-equilibrium extrapolation of the x faces after the loop's collisions
+// (boundary_vel, mkFluidsUser.cpp:455-617; bdy_flowin): with n the inner
+// neighbour of the face cell b,
+//   flow      f(b) = f(n) + feq(rho_b, u_b) - feq(rho_n, u_n)
+//   phase     g(b) = g(n) + w (phi_b - phi_n)
+//   thermal   t(b) = t(n) + w T_b (1 + 4 e.u_b) - w T_n (1 + 4 e.u_n)
+// inflow (x = 0): u_b = u0, rho_b = rho_n, phi_b = -1, T_b = -Delta;
+// outflow (x = nx - 1): rho_b = rho0, u_b = u_n, phi_b = phi_n, T_b = T_n;
+// the face cell's temperature becomes T_b.
+// rho_n, u_n, phi_n, T_n are moments of the post-collision populations of n,
+// except the thermal u_n, the collision velocity of n (face_u).  One thread
+// per face cell; each writes only its own cell's outgoing slots and reads only
+// those of x = 1 / x = nx - 2, so no two threads touch one slot.
+template <class S, class P, int Q>
+__global__ void __launch_bounds__(128)
+    k_fd_nee(S* __restrict__ W, S* __restrict__ G, S* __restrict__ Tp, P* __restrict__ temp,
+             const P* __restrict__ face_u, const Geom g, int64_t steps_done, const FdK<typename Stor<S>::T> k) {
+  typedef typename Stor<S>::T T;
+  const int plane = g.ny * g.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * plane) return;
+  const int side = t >= plane ? 1 : 0;
+  const int yz = t - side * plane;
+  const int y = yz % g.ny, z = yz / g.ny;
+  const int xb = side == 0 ? 0 : g.nx - 1, xn = side == 0 ? 1 : g.nx - 2;
+  if (!g.fluid(xb, y, z) || !g.fluid(xn, y, z)) return;
+  const Nbr nbb(g, xb, y, z), nbn(g, xn, y, z);
+  const int cb = nbb.idx(0, 0, 0), cn = nbn.idx(0, 0, 0);
+  // flow lattice
+  T fn[Q];
+  T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    fn[i] = ld_out<S, Q>(W, g.stride, nbn, steps_done, cn, i);
+    drho += fn[i];
+    if (ex(i)) jx += T(ex(i)) * fn[i];
+    if (ey(i)) jy += T(ey(i)) * fn[i];
+    if (ez(i)) jz += T(ez(i)) * fn[i];
+  }
+  const T rn = k.f.ref + drho;
+  const T un[3] = {jx / rn, jy / rn, jz / rn};
+  const T ub[3] = {side == 0 ? k.u0[0] : un[0], side == 0 ? k.u0[1] : un[1], side == 0 ? k.u0[2] : un[2]};
+  const T rb = side == 0 ? rn : k.f.ref;
+  const T uun = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
+  const T uub = ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const T w = T(wq<Q>(i));
+    const T eun = T(ex(i)) * un[0] + T(ey(i)) * un[1] + T(ez(i)) * un[2];
+    const T eub = T(ex(i)) * ub[0] + T(ey(i)) * ub[1] + T(ez(i)) * ub[2];
+    const T d = w * ((rb - rn) + rb * (T(3) * eub + T(4.5) * eub * eub - T(1.5) * uub) -
+                     rn * (T(3) * eun + T(4.5) * eun * eun - T(1.5) * uun));
+    st_layout<S, Q>(W, g.stride, nbb, steps_done, cb, i, fn[i] + d);
+  }
+  // phase-field and thermal lattices
+  T gn[7], tn[7], sg = T(0), st = T(0);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    gn[i] = ld_out<S, 7>(G, g.stride, nbn, steps_done, cn, i);
+    tn[i] = ld_out<S, 7>(Tp, g.stride, nbn, steps_done, cn, i);
+    sg += gn[i];
+    st += tn[i];
+  }
+  const T phn = k.ref_g + sg, Tn = k.ref_t + st;
+  const T phb = side == 0 ? T(-1) : phn, Tb = side == 0 ? k.ref_t : Tn;
+  const P* fu = face_u + 3 * side * plane;
+  const T vn[3] = {T(fu[yz]), T(fu[plane + yz]), T(fu[2 * plane + yz])};
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    const T w = T(wq<7>(i));
+    const T evn = T(ex(i)) * vn[0] + T(ey(i)) * vn[1] + T(ez(i)) * vn[2];
+    const T evb = T(ex(i)) * ub[0] + T(ey(i)) * ub[1] + T(ez(i)) * ub[2];
+    st_layout<S, 7>(G, g.stride, nbb, steps_done, cb, i, gn[i] + w * (phb - phn));
+    st_layout<S, 7>(Tp, g.stride, nbb, steps_done, cb, i,
+                    tn[i] + w * (Tb * (T(1) + T(4) * evb) - Tn * (T(1) + T(4) * evn)));
+  }
+  temp[cb] = P(Tb);
+}
+
 // ===================================================================== INIT
 template <class S, class InT>
-__global__ void k_init(int model, int Q0, S* A0, S* A1, float* H0, typename PhiOf<S>::type* phi0,
+__global__ void k_init(int model, int Q0, S* A0, S* A1, S* A2, int Q2, float* H0, typename PhiOf<S>::type* phi0,
                        typename PhiOf<S>::type* phi1, typename PhiOf<S>::type* temp, const InT* __restrict__ in_phi,
                        const InT* __restrict__ in_t, const InT* __restrict__ in_rho,
                        const InT* __restrict__ in_u, double d_rho, double d_ux, double d_uy, double d_uz,
@@ -514,6 +689,23 @@ __global__ void k_init(int model, int Q0, S* A0, S* A1, float* H0, typename PhiO
     put_eq<S, 19>(A0, g, nb, ci, 1.0, ux, uy, uz, -1.0, refs.r0);
     put_eq<S, 19>(A1, g, nb, ci, ph, ux, uy, uz, 0.0, refs.r1);
     if (H0) H0[c] = float(wq<19>(0) * ((ph - refs.r1) - 1.5 * ph * (ux * ux + uy * uy + uz * uz)));
+  } else if (model == MK_MODEL_FLOW_DENDRITE) {
+    // the flow starts at rho0 with u0 scaled by the liquid fraction (unless
+    // given); the thermal equilibrium carries the same velocity
+    const double ns = fmin(1.0, fmax(0.0, 0.5 * (1.0 + ph)));
+    const double vx = in_u ? ux : (1.0 - ns) * d_ux, vy = in_u ? uy : (1.0 - ns) * d_uy,
+                 vz = in_u ? uz : (1.0 - ns) * d_uz;
+    const double r = in_rho ? in_rho[c] : d_rho;
+    put_eq<S, 7>(A0, g, nb, ci, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      const double eu = ex(i) * vx + ey(i) * vy + ez(i) * vz;
+      st_layout<S, 7>(A1, g.stride, nb, 0, ci, i, typename Stor<S>::T(wq<7>(i) * ((tv - refs.r1) + 4.0 * tv * eu)));
+    }
+    if (Q2 == 19)
+      put_eq<S, 19>(A2, g, nb, ci, r, vx, vy, vz, 0.0, d_rho);
+    else
+      put_eq<S, 27>(A2, g, nb, ci, r, vx, vy, vz, 0.0, d_rho);
   } else {
     put_eq<S, 7>(A0, g, nb, ci, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
     put_eq<S, 7>(A1, g, nb, ci, tv, 0.0, 0.0, 0.0, 0.0, refs.r1);
@@ -635,6 +827,18 @@ __global__ void k_field_geom(const Geom g, int field, const double* __restrict__
     out[c] = g.fluid(x, y, z) ? MK_FLAG_FLUID : MK_FLAG_WALLS;
   else
     out[c] = nobj > 0 ? nearest_seed(seeds, nobj, x, y, z) : 0;
+}
+
+// Cell flags of the flow + dendrite model (reset_flags, mkPhaseField.h:37):
+// solid where phi > 0, walls where the geometry has them, else fluid.
+template <class P>
+__global__ void k_field_fdflag(const Geom g, const P* __restrict__ phi, double* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  out[c] = !g.fluid(x, y, z) ? MK_FLAG_WALLS : (double(phi[c]) > 0.0 ? MK_FLAG_SOLID : MK_FLAG_FLUID);
 }
 
 // ============================================================ DIAGNOSTICS (K6)
@@ -763,6 +967,49 @@ __global__ void __launch_bounds__(256) k_diag_mp(const S* __restrict__ G, const 
     v[mke::DG_FLUID] += 1.0;
     v[mke::DG_BAD] += bad ? 1.0 : 0.0;
     if (!bad) v[mke::DG_MAXU] = fmax(v[mke::DG_MAXU], sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+  }
+  block_reduce_store(v, partial);
+}
+
+// Flow + dendrite: the flow lattice's mass, momentum and speed with the phase
+// field's and the thermal lattice's sums.
+template <class S, class P, int Q>
+__global__ void __launch_bounds__(256) k_diag_fd(const S* __restrict__ W, const P* __restrict__ phi,
+                                                 const P* __restrict__ phi_prev, const P* __restrict__ temp,
+                                                 const Geom g, int64_t steps_done, double Fx, double Fy, double Fz,
+                                                 double rho0, int64_t n, double* __restrict__ partial) {
+  double v[mke::DG_N];
+#pragma unroll
+  for (int q = 0; q < mke::DG_N; ++q) v[q] = 0.0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_coords(g, c, x, y, z);
+    if (!g.fluid(x, y, z)) continue;
+    const Nbr nb(g, x, y, z);
+    double drho = 0, j[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const double f = double(ld_out<S, Q>(W, g.stride, nb, steps_done, (int)c, i));
+      drho += f;
+      j[0] += ex(i) * f;
+      j[1] += ey(i) * f;
+      j[2] += ez(i) * f;
+    }
+    const double rho = rho0 + drho;
+    const double mx = j[0] - 0.5 * Fx, my = j[1] - 0.5 * Fy, mz = j[2] - 0.5 * Fz;
+    const double p = double(phi[c]), pp = double(phi_prev[c]), t = double(temp[c]);
+    const bool bad = !(rho > 0.0) || !isfinite(rho) || !isfinite(mx) || !isfinite(my) || !isfinite(mz) ||
+                     !isfinite(p) || !isfinite(t);
+    v[mke::DG_MASS] += rho;
+    v[mke::DG_MX] += mx;
+    v[mke::DG_MY] += my;
+    v[mke::DG_MZ] += mz;
+    v[mke::DG_PHI] += p;
+    v[mke::DG_SOLID] += p > 0.0 ? 1.0 : 0.0;
+    v[mke::DG_HEAT] += t - 0.5 * pp;
+    v[mke::DG_FLUID] += 1.0;
+    v[mke::DG_BAD] += bad ? 1.0 : 0.0;
+    if (!bad) v[mke::DG_MAXU] = fmax(v[mke::DG_MAXU], sqrt(mx * mx + my * my + mz * mz) / rho);
   }
   block_reduce_store(v, partial);
 }
@@ -1049,6 +1296,96 @@ void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t*
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
 
+template <class T>
+FdK<T> fd_coef(const mk_params& p, Refs r) {
+  FdK<T> k;
+  k.f = flow_coef<T>(p, p.rho0);
+  k.half = T(p.tau - 0.5);
+  for (int a = 0; a < 3; ++a) k.u0[a] = T(p.u0[a]);
+  k.ref_g = T(r.r0);
+  k.ref_t = T(r.r1);
+  k.inlet = p.inlet ? 1 : 0;
+  return k;
+}
+
+template <class S, int Q, int COLL, int PARITY>
+void launch_fd_collide(mke::Engine& e, dim3 grid, dim3 block, bool gen) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  const DendK<T> kd = dend_coef<T>(e.p, r);
+  const FdK<T> k = fd_coef<T>(e.p, r);
+  P* phi_old = (P*)e.phi[e.phi_cur];
+  P* phi_new = (P*)e.phi[1 - e.phi_cur];
+  if (gen)
+    k_fd_collide<S, P, Q, COLL, PARITY, true><<<grid, block, 0, e.stream>>>(
+        (S*)e.pop2, (S*)e.pop0, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, (P*)e.face_u, e.grain, (const T*)e.rot, g,
+        kd, k);
+  else
+    k_fd_collide<S, P, Q, COLL, PARITY, false><<<grid, block, 0, e.stream>>>(
+        (S*)e.pop2, (S*)e.pop0, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, (P*)e.face_u, e.grain, (const T*)e.rot, g,
+        kd, k);
+}
+
+template <class S, int Q, int COLL>
+void launch_fd_q(mke::Engine& e, int parity, dim3 grid, dim3 block) {
+  const bool gen = e.p.aniso != MK_ANISO_CUBIC;
+  if (parity == 0)
+    launch_fd_collide<S, Q, COLL, 0>(e, grid, block, gen);
+  else
+    launch_fd_collide<S, Q, COLL, 1>(e, grid, block, gen);
+}
+
+// Flow + dendrite loop: phi of the streamed phase field, the fused flow /
+// phase-field / thermal collision, then the inflow/outflow faces.
+template <class S>
+void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  S* G = (S*)e.pop0;
+  P* phi_old = (P*)e.phi[e.phi_cur];
+  P* phi_new = (P*)e.phi[1 - e.phi_cur];
+  if (ev) cudaEventRecord(ev[0], e.stream);
+  if (parity == 0)
+    k_pf_phi<S, P, 0><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, T(r.r0));
+  else
+    k_pf_phi<S, P, 1><<<grid, block, 0, e.stream>>>(G, phi_old, phi_new, g, T(r.r0));
+  if (ev) {
+    cudaEventRecord(ev[1], e.stream);
+    cudaEventRecord(ev[2], e.stream);
+  }
+  const int Q = e.p.lattice, C = e.p.collision;
+  if (Q == 19) {
+    if (C == MK_COLL_BGK)
+      launch_fd_q<S, 19, MK_COLL_BGK>(e, parity, grid, block);
+    else if (C == MK_COLL_TRT)
+      launch_fd_q<S, 19, MK_COLL_TRT>(e, parity, grid, block);
+    else
+      launch_fd_q<S, 19, MK_COLL_MRT>(e, parity, grid, block);
+  } else {
+    if (C == MK_COLL_BGK)
+      launch_fd_q<S, 27, MK_COLL_BGK>(e, parity, grid, block);
+    else
+      launch_fd_q<S, 27, MK_COLL_TRT>(e, parity, grid, block);
+  }
+  if (ev) cudaEventRecord(ev[3], e.stream);
+  if (e.p.inlet) {
+    if (ev) cudaEventRecord(ev[4], e.stream);
+    const FdK<T> k = fd_coef<T>(e.p, r);
+    const int nt = 2 * e.ny * e.nz;
+    if (Q == 19)
+      k_fd_nee<S, P, 19><<<(nt + 127) / 128, 128, 0, e.stream>>>((S*)e.pop2, G, (S*)e.pop1, (P*)e.temp, (const P*)e.face_u, g,
+                                                                 e.step + 1, k);
+    else
+      k_fd_nee<S, P, 27><<<(nt + 127) / 128, 128, 0, e.stream>>>((S*)e.pop2, G, (S*)e.pop1, (P*)e.temp, (const P*)e.face_u, g,
+                                                                 e.step + 1, k);
+    if (ev) cudaEventRecord(ev[5], e.stream);
+  }
+}
+
 template <class S>
 void step_t(mke::Engine& e, cudaEvent_t* ev) {
   dim3 grid, block;
@@ -1074,6 +1411,11 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
       launch_mp<S>(e, parity, grid, block, ev);
       e.launches += 2;
       break;
+    case MK_MODEL_FLOW_DENDRITE:
+      launch_fd<S>(e, parity, grid, block, ev);
+      e.phi_cur = 1 - e.phi_cur;
+      e.launches += e.p.inlet ? 3 : 2;
+      break;
     default:
       launch_dend<S>(e, parity, grid, block, ev);
       e.phi_cur = 1 - e.phi_cur;
@@ -1089,7 +1431,8 @@ cudaError_t set_state_t(mke::Engine& e, const InT* d_phi, const InT* d_t, const 
   dim3 grid, block;
   launch_dims(e, grid, block);
   const Geom g = make_geom(e);
-  k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, e.rest1, (P*)e.phi[0],
+  k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, (S*)e.pop2, e.Q2, e.rest1,
+                                               (P*)e.phi[0],
                                                (P*)e.phi[1],
                                           (P*)e.temp, d_phi, d_t, d_rho, d_u, e.p.rho0, e.p.u0[0], e.p.u0[1],
                                           e.p.u0[2], e.p.model == MK_MODEL_CONVECTION ? e.p.s_ref : -e.p.delta, g,
@@ -1107,8 +1450,13 @@ cudaError_t field_t(mke::Engine& e, int field) {
   const Refs r = refs_of(e.p);
   const int m = e.p.model;
   const int nb = (int)((e.ncell + 255) / 256);
+  if (field == MK_FIELD_FLAG && m == MK_MODEL_FLOW_DENDRITE) {
+    k_field_fdflag<P><<<grid, block, 0, e.stream>>>(g, (const P*)e.phi[e.phi_cur], e.field);
+    return cudaGetLastError();
+  }
   if (field == MK_FIELD_FLAG || field == MK_FIELD_GRAIN) {
-    const int nobj = (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE) ? e.p.n_objects : 0;
+    const int nobj = (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE ||
+                      m == MK_MODEL_FLOW_DENDRITE) ? e.p.n_objects : 0;
     k_field_geom<<<grid, block, 0, e.stream>>>(g, field, e.seeds, nobj, e.field);
     return cudaGetLastError();
   }
@@ -1131,6 +1479,17 @@ cudaError_t field_t(mke::Engine& e, int field) {
                                                         e.p.force[1], e.p.force[2], e.p.rho0, e.field);
     return cudaGetLastError();
   }
+  if (m == MK_MODEL_FLOW_DENDRITE &&
+      (field == MK_FIELD_RHO || field == MK_FIELD_UX || field == MK_FIELD_UY || field == MK_FIELD_UZ)) {
+    const Buoy bu = buoy_of(e.p);
+    if (e.Q2 == 19)
+      k_field_flow<S, 19><<<grid, block, 0, e.stream>>>((const S*)e.pop2, nullptr, bu, g, e.step, field, e.p.force[0],
+                                                        e.p.force[1], e.p.force[2], e.p.rho0, e.field);
+    else
+      k_field_flow<S, 27><<<grid, block, 0, e.stream>>>((const S*)e.pop2, nullptr, bu, g, e.step, field, e.p.force[0],
+                                                        e.p.force[1], e.p.force[2], e.p.rho0, e.field);
+    return cudaGetLastError();
+  }
   if (m == MK_MODEL_MULTIPHASE) {
     if (field != MK_FIELD_RHO && field != MK_FIELD_UX && field != MK_FIELD_UY && field != MK_FIELD_UZ &&
         field != MK_FIELD_PRESSURE)
@@ -1140,7 +1499,8 @@ cudaError_t field_t(mke::Engine& e, int field) {
     return cudaGetLastError();
   }
   if (field == MK_FIELD_T || field == MK_FIELD_C) {
-    if ((field == MK_FIELD_T) != (m == MK_MODEL_THERMAL_DENDRITE)) return cudaErrorInvalidValue;
+    if ((field == MK_FIELD_T) != (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE))
+      return cudaErrorInvalidValue;
     k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.temp, nullptr, e.ncell, e.field);
     return cudaGetLastError();
   }
@@ -1170,6 +1530,17 @@ cudaError_t diag_t(mke::Engine& e) {
     else
       k_diag_flow<S, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, Tp, bu, ax, g, e.step, e.p.force[0],
                                                    e.p.force[1], e.p.force[2], e.p.rho0, e.ncell, e.partial);
+  } else if (m == MK_MODEL_FLOW_DENDRITE) {
+    const P* ph = (const P*)e.phi[e.phi_cur];
+    const P* pp = (const P*)e.phi[1 - e.phi_cur];
+    if (e.Q2 == 19)
+      k_diag_fd<S, P, 19><<<nb, 256, 0, e.stream>>>((const S*)e.pop2, ph, pp, (const P*)e.temp, g, e.step,
+                                                    e.p.force[0], e.p.force[1], e.p.force[2], e.p.rho0, e.ncell,
+                                                    e.partial);
+    else
+      k_diag_fd<S, P, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop2, ph, pp, (const P*)e.temp, g, e.step,
+                                                    e.p.force[0], e.p.force[1], e.p.force[2], e.p.rho0, e.ncell,
+                                                    e.partial);
   } else if (m == MK_MODEL_MULTIPHASE) {
     k_diag_mp<S><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, (const P*)e.phi[0], g, e.step, mp_coef<T>(e.p, r),
                                            e.ncell, e.partial);
@@ -1239,6 +1610,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     e.Q0 = 7;
     e.Q1 = 7;
   }
+  e.Q2 = p.model == MK_MODEL_FLOW_DENDRITE ? p.lattice : 0;
   // Launch shape: a full warp row along x, rows stacked in y to 256 threads.
   int bx = block_x > 0 ? block_x : (p.nx >= 128 ? 128 : (p.nx >= 64 ? 64 : 32));
   int by = block_y > 0 ? block_y : 256 / bx;
@@ -1264,13 +1636,17 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   };
   if ((st = alloc(&e.pop0, (size_t)e.Q0 * e.stride * e.elem)) != cudaSuccess) return st;
   if ((st = alloc(&e.pop1, (size_t)e.Q1 * e.stride * e.elem)) != cudaSuccess) return st;
+  if ((st = alloc(&e.pop2, (size_t)e.Q2 * e.stride * e.elem)) != cudaSuccess) return st;
+  const bool faces = p.model == MK_MODEL_FLOW_DENDRITE && p.inlet;
+  if ((st = alloc(&e.face_u, faces ? (size_t)6 * p.ny * p.nz * e.phi_elem : 0)) != cudaSuccess) return st;
   if (p.model == MK_MODEL_MULTIPHASE && e.elem == 2) {
     if ((st = alloc((void**)&e.rest1, (size_t)e.ncell * sizeof(float))) != cudaSuccess) return st;
   } else {
     e.rest1 = nullptr;
   }
   if ((st = alloc(&e.phi[0], (size_t)e.ncell * e.phi_elem)) != cudaSuccess) return st;
-  const bool dend = p.model == MK_MODEL_THERMAL_DENDRITE || p.model == MK_MODEL_SOLUTAL_DENDRITE;
+  const bool dend = p.model == MK_MODEL_THERMAL_DENDRITE || p.model == MK_MODEL_SOLUTAL_DENDRITE ||
+                    p.model == MK_MODEL_FLOW_DENDRITE;
   if ((st = alloc(&e.phi[1], dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (!dend) e.phi[1] = nullptr;
   if ((st = alloc(&e.temp, dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
@@ -1323,7 +1699,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
-  void* ptrs[] = {e.pop0, e.pop1, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
+  void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.face_u, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
                   e.field32, e.stage32};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -1428,11 +1804,14 @@ cudaError_t engine_step(Engine& e, cudaEvent_t* ev) {
 
 static bool one_kernel(const Engine& e) { return e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION; }
 
-int engine_kernels_per_step(const Engine& e) { return one_kernel(e) ? 1 : 2; }
+int engine_kernels_per_step(const Engine& e) {
+  if (e.p.model == MK_MODEL_FLOW_DENDRITE) return e.p.inlet ? 3 : 2;
+  return one_kernel(e) ? 1 : 2;
+}
 
 const char* engine_kernel_name(const Engine& e, int k) {
   if (one_kernel(e)) return "collide";
-  return k == 0 ? "phi" : "collide";
+  return k == 0 ? "phi" : (k == 1 ? "collide" : "boundary");
 }
 
 cudaError_t engine_field(Engine& e, int field) {
@@ -1472,10 +1851,11 @@ cudaError_t engine_diag(Engine& e, double* out) {
 
 cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   if (trial_steps < 1) trial_steps = 1;
-  const size_t b0 = engine_pop_bytes(e, 0), b1 = engine_pop_bytes(e, 1), bp = (size_t)e.ncell * e.phi_elem;
-  void* const bufs[6] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.rest1};
-  const size_t sizes[6] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0,
-                           e.rest1 ? (size_t)e.ncell * sizeof(float) : 0};
+  const size_t b0 = engine_pop_bytes(e, 0), b1 = engine_pop_bytes(e, 1), b2 = engine_pop_bytes(e, 2),
+               bp = (size_t)e.ncell * e.phi_elem;
+  void* const bufs[7] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.rest1, e.pop2};
+  const size_t sizes[7] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0,
+                           e.rest1 ? (size_t)e.ncell * sizeof(float) : 0, b2};
   size_t total = 0;
   for (size_t s : sizes) total += s;
   char* save = nullptr;
@@ -1483,7 +1863,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   if (st != cudaSuccess) return st;
   auto copy = [&](bool to_save) -> cudaError_t {
     size_t off = 0;
-    for (int q = 0; q < 6; ++q) {
+    for (int q = 0; q < 7; ++q) {
       if (!sizes[q]) continue;
       cudaError_t s2 = to_save ? cudaMemcpyAsync(save + off, bufs[q], sizes[q], cudaMemcpyDeviceToDevice, e.stream)
                                : cudaMemcpyAsync(bufs[q], save + off, sizes[q], cudaMemcpyDeviceToDevice, e.stream);
@@ -1554,7 +1934,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
 }
 
 size_t engine_pop_bytes(const Engine& e, int which) {
-  return (size_t)(which == 0 ? e.Q0 : e.Q1) * e.stride * e.elem;
+  return (size_t)(which == 0 ? e.Q0 : (which == 1 ? e.Q1 : e.Q2)) * e.stride * e.elem;
 }
 
 double engine_bytes_per_cell(const Engine& e) {
@@ -1564,7 +1944,7 @@ double engine_bytes_per_cell(const Engine& e) {
   const double S = e.elem;
   const double phi = (e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION) ? 0.0 : 2.0 * e.phi_elem;
   const double rest = e.rest1 ? 2.0 * (4.0 - S) : 0.0;
-  return 2.0 * (e.Q0 + e.Q1) * S + phi + rest;
+  return 2.0 * (e.Q0 + e.Q1 + e.Q2) * S + phi + rest;
 }
 
 }  // namespace mke

@@ -143,6 +143,9 @@ struct orc_state {
   std::vector<double> f_out, f_hlp;  // lattice 0, [q][cell]
   std::vector<double> s_out, s_hlp;  // lattice 1
   std::vector<double> phi, phi_prev, temp, conc, conc_prev;
+  int Qw = 0;                        // flow lattice of the flow + dendrite model, 0 if none
+  std::vector<double> w_out, w_hlp;  // its populations
+  std::vector<double> vel;           // its velocity, 3 per cell (advects the thermal lattice)
   std::vector<int> grain;
   std::vector<double> rot;  // 9 per object (R, columns = crystal axes)
 };
@@ -640,8 +643,10 @@ void thermal_dendrite_step(orc_state* s) {
         }
     return;
   }
-  // 3. thermal propagate + relaxation with latent heat (1/2) dphi.
+  // 3. thermal propagate + relaxation with latent heat (1/2) dphi; with a
+  // flow lattice the equilibrium is advected, w T (1 + 4 e.u) (getTEquPDFs).
   const double om_t = 1.0 / (4.0 * p.D + 0.5);
+  const bool adv = !s->vel.empty();
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < n; ++c) {
     if (s->flag[c] != MK_FLAG_FLUID) continue;
@@ -650,11 +655,125 @@ void thermal_dendrite_step(orc_state* s) {
     const double lat = 0.5 * (s->phi[c] - s->phi_prev[c]);
     for (int i = 0; i < 7; ++i) {
       const double w = weight(7, i);
+      const double eu = adv ? E27[i][0] * s->vel[3 * c] + E27[i][1] * s->vel[3 * c + 1] + E27[i][2] * s->vel[3 * c + 2]
+                            : 0.0;
       const double ti = s->s_hlp[(int64_t)i * n + c];
-      s->s_out[(int64_t)i * n + c] = ti - om_t * (ti - w * T) + w * lat;
+      s->s_out[(int64_t)i * n + c] = ti - om_t * (ti - w * T * (1.0 + 4.0 * eu)) + w * lat;
     }
     s->temp[c] = T;
   }
+}
+
+// ------------------------------------------------ FLOW + DENDRITE model
+// run_flow_thermal_dendrite (MaterKit.cpp:467-527): per loop the flow
+// (mkFluidsMRT::propagate_PBB, relaxation, bdyVelocity), then the phase field
+// and the thermal lattice (advected by the flow's velocity, bdy_flowin).  The
+// porous bounce-back is the partially saturated method of Noble & Torczynski
+// (Int. J. Mod. Phys. C 9 (1998) 1189): with the solid fraction
+// n_s = clamp((1 + phi)/2) of the previous loop and B = n_s (tau - 1/2) /
+// ((1 - n_s) + (tau - 1/2)),
+//   f* = f + (1 - B) (f_coll - f) + B (f_inv(i) - f_i + feq_i(rho, 0) - feq_inv(i)(rho, u)).
+// The x faces carry the non-equilibrium extrapolation of boundary_vel
+// (mkFluidsUser.cpp:455-617): f(b) = f(n) + feq(rho_b, u_b) - feq(rho_n, u_n)
+// with n the inner neighbour; inflow at x = 0 (u_b = u0, rho_b = rho_n,
+// T_b = -Delta, phi_b = -1), outflow at x = nx - 1 (rho_b = rho0, u_b = u_n,
+// T_b = T_n, phi_b = phi_n); the face cell's temperature becomes T_b.
+void flow_dendrite_nee(orc_state* s, bool flow_lattice);
+
+void flow_dendrite_flow(orc_state* s) {
+  const int Q = s->Qw;
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  propagate(s, Q, s->w_out, s->w_hlp);
+  const double om = 1.0 / p.tau;
+  const double om_m = 1.0 / (0.5 + p.magic / (p.tau - 0.5));
+  const double F[3] = {p.force[0], p.force[1], p.force[2]};
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    double f[27], fc[27], u[3];
+    double rho = 0;
+    for (int i = 0; i < Q; ++i) {
+      f[i] = s->w_hlp[(int64_t)i * n + c];
+      fc[i] = f[i];
+      rho += f[i];
+    }
+    flow_collide(Q, p.collision, om, om_m, fc, F, u);
+    const double ns = std::min(1.0, std::max(0.0, 0.5 * (1.0 + s->phi[c])));
+    const double B = ns * (p.tau - 0.5) / ((1.0 - ns) + (p.tau - 0.5));
+    const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    for (int i = 0; i < Q; ++i) {
+      const int k = inv_dir(i);
+      const double w = weight(Q, i);
+      const double euk = E27[k][0] * u[0] + E27[k][1] * u[1] + E27[k][2] * u[2];
+      const double omega_s = f[k] - f[i] + rho * w - rho * feq2(w, euk, uu);
+      s->w_out[(int64_t)i * n + c] = f[i] + (1.0 - B) * (fc[i] - f[i]) + B * omega_s;
+    }
+    for (int a = 0; a < 3; ++a) s->vel[3 * c + a] = u[a];
+  }
+  flow_dendrite_nee(s, true);
+}
+
+void flow_dendrite_nee(orc_state* s, bool flow_lattice) {
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  if (!p.inlet) return;
+  for (int side = 0; side < 2; ++side) {
+    const int xb = side == 0 ? 0 : s->nx - 1, xn = side == 0 ? 1 : s->nx - 2;
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < s->nz; ++z)
+      for (int y = 0; y < s->ny; ++y) {
+        const int64_t b = cidx(s, xb, y, z), nn = cidx(s, xn, y, z);
+        if (s->flag[b] != MK_FLAG_FLUID || s->flag[nn] != MK_FLAG_FLUID) continue;
+        if (flow_lattice) {
+          const int Q = s->Qw;
+          double rho = 0, j[3] = {0, 0, 0};
+          for (int i = 0; i < Q; ++i) {
+            const double v = s->w_out[(int64_t)i * n + nn];
+            rho += v;
+            for (int a = 0; a < 3; ++a) j[a] += E27[i][a] * v;
+          }
+          const double un[3] = {j[0] / rho, j[1] / rho, j[2] / rho};
+          const double ub[3] = {side == 0 ? p.u0[0] : un[0], side == 0 ? p.u0[1] : un[1], side == 0 ? p.u0[2] : un[2]};
+          const double rb = side == 0 ? rho : p.rho0;
+          const double uun = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
+          const double uub = ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2];
+          for (int i = 0; i < Q; ++i) {
+            const double w = weight(Q, i);
+            const double eun = E27[i][0] * un[0] + E27[i][1] * un[1] + E27[i][2] * un[2];
+            const double eub = E27[i][0] * ub[0] + E27[i][1] * ub[1] + E27[i][2] * ub[2];
+            s->w_out[(int64_t)i * n + b] =
+                s->w_out[(int64_t)i * n + nn] + rb * feq2(w, eub, uub) - rho * feq2(w, eun, uun);
+          }
+          for (int a = 0; a < 3; ++a) s->vel[3 * b + a] = ub[a];
+        } else {
+          // phase field (no velocity in its equilibrium) and thermal lattice
+          double phn = 0, Tn = 0;
+          for (int i = 0; i < 7; ++i) {
+            phn += s->f_out[(int64_t)i * n + nn];
+            Tn += s->s_out[(int64_t)i * n + nn];
+          }
+          const double phb = side == 0 ? -1.0 : phn, Tb = side == 0 ? -p.delta : Tn;
+          const double* un = &s->vel[3 * nn];
+          const double* ub = &s->vel[3 * b];
+          for (int i = 0; i < 7; ++i) {
+            const double w = weight(7, i);
+            const double eun = E27[i][0] * un[0] + E27[i][1] * un[1] + E27[i][2] * un[2];
+            const double eub = E27[i][0] * ub[0] + E27[i][1] * ub[1] + E27[i][2] * ub[2];
+            s->f_out[(int64_t)i * n + b] = s->f_out[(int64_t)i * n + nn] + w * (phb - phn);
+            s->s_out[(int64_t)i * n + b] =
+                s->s_out[(int64_t)i * n + nn] + w * Tb * (1.0 + 4.0 * eub) - w * Tn * (1.0 + 4.0 * eun);
+          }
+          s->temp[b] = Tb;  // the face cell holds the boundary temperature
+        }
+      }
+  }
+}
+
+void flow_dendrite_step(orc_state* s) {
+  flow_dendrite_flow(s);       // uses phi of the previous loop
+  thermal_dendrite_step(s);    // phase field, then the advected thermal lattice
+  flow_dendrite_nee(s, false);
 }
 
 }  // namespace
@@ -708,7 +827,8 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) s->rot[9 * k + 3 * a + b] = R[a][b];
   }
-  if (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE) {
+  if (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
+      p->model == MK_MODEL_FLOW_DENDRITE) {
     for (int z = 0; z < s->nz; ++z)
       for (int y = 0; y < s->ny; ++y)
         for (int x = 0; x < s->nx; ++x) s->grain[cidx(s, x, y, z)] = nearest_seed(*p, x, y, z);
@@ -760,11 +880,39 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
     s->f_hlp.assign((size_t)7 * n, 0.0);
     s->s_out.assign((size_t)7 * n, 0.0);
     s->s_hlp.assign((size_t)7 * n, 0.0);
+    if (p->model == MK_MODEL_FLOW_DENDRITE && T0) std::memcpy(s->temp.data(), T0, n * sizeof(double));
     for (int64_t c = 0; c < n; ++c)
       for (int i = 0; i < 7; ++i) {
         s->f_out[(int64_t)i * n + c] = weight(7, i) * s->phi[c];
         s->s_out[(int64_t)i * n + c] = weight(7, i) * s->temp[c];
       }
+    if (p->model == MK_MODEL_FLOW_DENDRITE) {
+      // the flow starts at rho0 with u0 scaled by the liquid fraction, unless
+      // density / velocity fields are given
+      s->Qw = p->lattice;
+      const int Q = s->Qw;
+      s->w_out.assign((size_t)Q * n, 0.0);
+      s->w_hlp.assign((size_t)Q * n, 0.0);
+      s->vel.assign((size_t)3 * n, 0.0);
+      for (int64_t c = 0; c < n; ++c) {
+        const double ns = std::min(1.0, std::max(0.0, 0.5 * (1.0 + s->phi[c])));
+        const bool given = ux0 && uy0 && uz0;
+        const double u[3] = {given ? ux0[c] : (1.0 - ns) * p->u0[0], given ? uy0[c] : (1.0 - ns) * p->u0[1],
+                             given ? uz0[c] : (1.0 - ns) * p->u0[2]};
+        const double r = rho0 ? rho0[c] : p->rho0;
+        const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        for (int a = 0; a < 3; ++a) s->vel[3 * c + a] = u[a];
+        for (int i = 0; i < Q; ++i) {
+          const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+          s->w_out[(int64_t)i * n + c] = r * feq2(weight(Q, i), eu, uu);
+        }
+        // the thermal equilibrium carries the same velocity
+        for (int i = 0; i < 7; ++i) {
+          const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
+          s->s_out[(int64_t)i * n + c] = weight(7, i) * s->temp[c] * (1.0 + 4.0 * eu);
+        }
+      }
+    }
   }
   return s;
 }
@@ -785,6 +933,9 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
       case MK_MODEL_CONVECTION:
         convection_step(s);
         break;
+      case MK_MODEL_FLOW_DENDRITE:
+        flow_dendrite_step(s);
+        break;
       case MK_MODEL_THERMAL_DENDRITE:
       case MK_MODEL_SOLUTAL_DENDRITE:
         thermal_dendrite_step(s);  // the second lattice follows p.model
@@ -797,7 +948,7 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
 }
 
 extern "C" int orc_get_populations(const orc_state* s, int which, double* out) {
-  const std::vector<double>& v = which == 0 ? s->f_out : s->s_out;
+  const std::vector<double>& v = which == 0 ? s->f_out : (which == 1 ? s->s_out : s->w_out);
   if (v.empty()) return 1;
   std::memcpy(out, v.data(), v.size() * sizeof(double));
   return 0;
@@ -806,7 +957,7 @@ extern "C" int orc_get_populations(const orc_state* s, int which, double* out) {
 extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
   const int64_t n = s->n;
   const mk_params& p = s->p;
-  if (field == MK_FIELD_FLAG) {
+  if (field == MK_FIELD_FLAG && p.model != MK_MODEL_FLOW_DENDRITE) {
     for (int64_t c = 0; c < n; ++c) out[c] = s->flag[c];
     return 0;
   }
@@ -817,6 +968,31 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
   if (field == MK_FIELD_PHI) {
     std::memcpy(out, s->phi.data(), n * sizeof(double));
     return 0;
+  }
+  if (p.model == MK_MODEL_FLOW_DENDRITE) {
+    if (field == MK_FIELD_FLAG) {
+      // reset_flags (mkPhaseField.h:37): solid where phi > 0
+      for (int64_t c = 0; c < n; ++c) out[c] = s->flag[c] != MK_FLAG_FLUID ? s->flag[c]
+                                                 : (s->phi[c] > 0.0 ? MK_FLAG_SOLID : MK_FLAG_FLUID);
+      return 0;
+    }
+    if (field == MK_FIELD_RHO || field == MK_FIELD_UX || field == MK_FIELD_UY || field == MK_FIELD_UZ) {
+      const int Q = s->Qw;
+      for (int64_t c = 0; c < n; ++c) {
+        if (s->flag[c] != MK_FLAG_FLUID) {
+          out[c] = field == MK_FIELD_RHO ? p.rho0 : 0.0;
+          continue;
+        }
+        double rho = 0, j[3] = {0, 0, 0};
+        for (int i = 0; i < Q; ++i) {
+          const double f = s->w_out[(int64_t)i * n + c];
+          rho += f;
+          for (int a = 0; a < 3; ++a) j[a] += E27[i][a] * f;
+        }
+        out[c] = field == MK_FIELD_RHO ? rho : (j[field - MK_FIELD_UX] - 0.5 * p.force[field - MK_FIELD_UX]) / rho;
+      }
+      return 0;
+    }
   }
   if (p.model == MK_MODEL_CONVECTION && field == MK_FIELD_T) {
     std::memcpy(out, s->temp.data(), n * sizeof(double));
@@ -892,7 +1068,7 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
   }
   // dendrites
   if (field == MK_FIELD_T || field == MK_FIELD_C) {
-    if ((field == MK_FIELD_T) != (p.model == MK_MODEL_THERMAL_DENDRITE)) return 1;
+    if ((field == MK_FIELD_T) != (p.model != MK_MODEL_SOLUTAL_DENDRITE)) return 1;
     std::memcpy(out, s->temp.data(), n * sizeof(double));
     return 0;
   }

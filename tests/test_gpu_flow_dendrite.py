@@ -1,0 +1,100 @@
+"""Flow + dendrite model (run_flow_thermal_dendrite) on the GPU vs the FP64
+oracle, through the C ABI: porous bounce-back of the growing crystal, the
+thermal lattice advected by the flow, and the inflow/outflow faces.
+
+FP64 storage matches the oracle to 1e-10 relative L2 per field at loops 1, 2
+and 3 (both AA parities and the first boundary pass) and after 40 loops.
+"""
+import numpy as np
+import pytest
+
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params, initial_field
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
+from _oracle import Oracle, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FIELDS = ["phi", "T", "rho"]
+
+
+def _case(prec="fp64", coll="TRT", lat="D3Q19", inlet=True, **kw):
+    return cases.flow_dendrite(nx=24, ny=14, nz=12, radius=4.0, u_in=0.03, center=(8.0, 6.5, 5.5), precision=prec,
+                               collision=coll, lattice=lat, inlet=inlet, **kw)
+
+
+def _pair(casedir, name, text):
+    p = case_params(cases.write(text, f"{casedir}/{name}.xml"))
+    return p, Solver(params=p), Oracle(p, phi=initial_field(p, "phi"), T=initial_field(p, "T"))
+
+
+def _errs(s, o):
+    e = {f: rel_l2(s.field(f), o.field(f)) for f in FIELDS}
+    u = np.stack([s.field(f) for f in ("ux", "uy", "uz")])
+    v = np.stack([o.field(f) for f in ("ux", "uy", "uz")])
+    e["u"] = rel_l2(u, v)
+    return e
+
+
+@pytest.mark.parametrize("coll,lat,inlet", [("TRT", "D3Q19", True), ("MRT", "D3Q19", True), ("BGK", "D3Q27", True),
+                                            ("TRT", "D3Q19", False)])
+def test_flow_dendrite_fp64_steps(casedir, coll, lat, inlet):
+    p, s, o = _pair(casedir, f"fd_{coll}_{lat}_{int(inlet)}", _case(coll=coll, lat=lat, inlet=inlet))
+    for _ in range(3):
+        s.advance(1)
+        o.advance(1)
+        e = _errs(s, o)
+        assert max(e.values()) <= FP64_TOL, (s.step, e)
+    s.advance(37)
+    o.advance(37)
+    e = _errs(s, o)
+    assert max(e.values()) <= FP64_TOL, (s.step, e)
+    assert np.array_equal(s.field("flag"), o.field("flag"))
+    assert (s.field("flag") == A.MK_FLAG_SOLID).sum() > 100
+
+
+def test_flow_dendrite_fp32(casedir):
+    p, s, o = _pair(casedir, "fd32", _case("fp32"))
+    s.advance(60)
+    o.advance(60)
+    e = _errs(s, o)
+    assert max(e.values()) <= 1e-5, e
+
+
+@pytest.mark.parametrize("prec,tol", [("fp16", 2e-2), ("bf16", 5e-2)])
+def test_flow_dendrite_16bit(casedir, prec, tol):
+    p, s, o = _pair(casedir, f"fd_{prec}", _case(prec))
+    s.advance(60)
+    o.advance(60)
+    e = _errs(s, o)
+    assert max(e.values()) <= tol, e
+
+
+def test_flow_dendrite_launches_graph_and_checkpoint(casedir, tmp_path):
+    p = case_params(cases.write(_case("fp32"), f"{casedir}/fd_ck.xml"))
+    a, b = Solver(params=p), Solver(params=p)
+    assert a.launches_per_step() == 3
+    prof = a.profile(4, "boundary")
+    assert prof["kernel_ms"] > 0
+    b.advance(4)
+    a.advance(7, graph=True)
+    b.advance(7)
+    for f in ["phi", "T", "ux", "rho"]:
+        assert np.array_equal(a.field(f), b.field(f))
+    a.checkpoint(str(tmp_path / "fd.bin"))
+    a.advance(5)
+    c = Solver(params=p)
+    c.restore(str(tmp_path / "fd.bin"))
+    c.advance(5)
+    for f in ["phi", "T", "ux", "uz", "rho"]:
+        assert np.array_equal(a.field(f), c.field(f))
+    d = a.diagnostics()
+    assert d["n_bad"] == 0 and d["max_speed"] > 0.01
+
+
+def test_flow_dendrite_closed_faces_conserve_mass(casedir):
+    p = case_params(cases.write(_case("fp64", inlet=False), f"{casedir}/fd_mass.xml"))
+    s = Solver(params=p)
+    m0 = s.diagnostics()["mass"]
+    s.advance(50)
+    assert abs(s.diagnostics()["mass"] - m0) / m0 < 1e-12

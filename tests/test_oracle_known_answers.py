@@ -357,3 +357,71 @@ def test_rbc_above_onset_convects(casedir):
     o.advance(25000)
     nu = _nusselt(o, p)
     assert 2.6 < nu < 2.8, nu
+
+
+# ----------------------------------------------------- flow + dendrite (a1/a7/a8)
+def test_flow_dendrite_uniform_inflow_is_steady(casedir):
+    # All liquid at the far-field temperature: the inflow / outflow faces keep
+    # the uniform stream u0 and the uniform temperature to round-off.
+    p = _params(casedir, "fd_uniform", cases.flow_dendrite(nx=12, ny=6, nz=5, radius=3.0, u_in=0.03))
+    sh = (p.nz, p.ny, p.nx)
+    o = Oracle(p, phi=-np.ones(sh), T=np.full(sh, -p.delta))
+    o.advance(40)
+    assert np.abs(o.field("ux") - 0.03).max() < 1e-14
+    assert np.abs(o.field("uy")).max() < 1e-14 and np.abs(o.field("uz")).max() < 1e-14
+    assert np.abs(o.field("rho") - 1.0).max() < 1e-14
+    assert np.abs(o.field("T") + p.delta).max() < 1e-14
+    assert np.abs(o.field("phi") + 1.0).max() == 0.0
+
+
+def test_flow_dendrite_at_rest_is_the_thermal_dendrite(casedir):
+    # Closed faces and no inflow: the flow stays at rest (the porous
+    # bounce-back of an equilibrium at u = 0 is the identity) and the phase
+    # field and temperature are those of the thermal dendrite model.
+    p = _params(casedir, "fd_rest", cases.flow_dendrite(nx=20, ny=18, nz=16, radius=4.0, u_in=0.0, inlet=False))
+    q = A.MkParams.from_buffer_copy(p)
+    q.model = A.MK_MODEL_THERMAL_DENDRITE
+    phi, T = initial_field(p, "phi"), initial_field(p, "T")
+    o1, o2 = Oracle(p, phi=phi, T=T), Oracle(q, phi=phi, T=T)
+    o1.advance(60)
+    o2.advance(60)
+    assert (o1.field("phi") > 0).sum() > 500  # the seed grew
+    assert np.abs(o1.field("phi") - o2.field("phi")).max() < 1e-12
+    assert np.abs(o1.field("T") - o2.field("T")).max() < 1e-12
+    assert np.abs(o1.field("ux")).max() < 1e-15 and np.abs(o1.field("rho") - 1.0).max() < 1e-14
+
+
+def test_flow_dendrite_advects_heat_at_the_flow_speed(casedir):
+    # A temperature pulse in the uniform stream: its centroid moves at u0
+    # (first moment of w T (1 + 4 e.u) is T u) and the heat is conserved.
+    p = _params(casedir, "fd_adv", cases.flow_dendrite(nx=64, ny=4, nz=4, radius=3.0, u_in=0.05, D=0.02))
+    sh = (p.nz, p.ny, p.nx)
+    x = np.arange(p.nx)
+    T = np.broadcast_to(-p.delta + 0.1 * np.exp(-((x - 16.0) / 3.0) ** 2), sh).copy()
+    o = Oracle(p, phi=-np.ones(sh), T=T)
+
+    def moments():
+        e = o.field("T")[0, 0] + p.delta
+        return (e * x).sum() / e.sum(), e.sum()
+
+    c0, h0 = moments()
+    o.advance(300)
+    c1, h1 = moments()
+    assert abs((c1 - c0) - 0.05 * 300) < 1e-6
+    assert abs(h1 - h0) / h0 < 1e-10
+
+
+def test_flow_dendrite_solid_stops_the_flow(casedir):
+    # The porous bounce-back brings the velocity inside the crystal
+    # (phi > 0.99) to below 1 % of the stream around it.
+    p = _params(casedir, "fd_core", cases.flow_dendrite(nx=40, ny=24, nz=24, radius=6.0, u_in=0.02, delta=0.3))
+    o = Oracle(p, phi=initial_field(p, "phi"), T=initial_field(p, "T"))
+    o.advance(400)
+    phi = o.field("phi")
+    u = np.sqrt(o.field("ux") ** 2 + o.field("uy") ** 2 + o.field("uz") ** 2)
+    core = phi > 0.99
+    assert core.sum() > 50
+    assert u[core].max() < 0.01 * 0.02
+    assert u[phi < -0.99].mean() > 0.5 * 0.02
+    flag = o.field("flag")
+    assert np.array_equal(flag == A.MK_FLAG_SOLID, phi > 0)
