@@ -9,6 +9,9 @@ Workloads (--workload)
             thermal lattice, one centred seed)
   ensemble  48 seeded solutal dendrite domains (edges 48-128) packed into
             one lattice, BF16 storage, persistent launches + CUDA graph
+  flow_dendrite  thermal dendrite growing in a melt that flows in at x = 0
+            and out at x = n - 1, 128^3 (D3Q19 TRT flow with porous
+            bounce-back + phase field + advected D3Q7 thermal lattice)
 A "step" is one loop of the coupled step over every cell of the workload.
 MLUPS = lattice cells x steps / s / 1e6.
 
@@ -47,6 +50,12 @@ WORKLOADS = {
                  "metric": "MLUPS, %HBM roofline: thermal dendrite 128^3 (phase field + D3Q7 thermal)",
                  "size": 128, "precision": "fp32", "kernel": "k_dend_collide", "collision": "BGK(g) + BGK(T)",
                  "data": "synthetic (centred seed, eps4 0.05, undercooling 0.55)"},
+    "flow_dendrite": {"workload": "flow + thermal dendrite {n}^3, D3Q19 TRT flow (porous bounce-back, inflow 0.02) "
+                                  "+ phase field (D3Q7) + advected D3Q7 thermal, one seed",
+                      "metric": "MLUPS, %HBM roofline: flow + thermal dendrite 128^3 (D3Q19 + D3Q7 + D3Q7)",
+                      "size": 128, "precision": "fp32", "kernel": "k_fd_flow", "slot": "flow",
+                      "collision": "TRT(f, porous bounce-back) + BGK(g) + BGK(T)",
+                      "data": "synthetic (seed at x = n/3, eps4 0.05, undercooling 0.55, inflow u = 0.02)"},
     "ensemble": {"workload": "solutal dendrite ensemble: 48 domains, edges 48-128, 1-6 seeds each, seed 0xE45E",
                  "metric": "MLUPS aggregate, %HBM roofline: 48-domain solutal dendrite ensemble, BF16, "
                            "persistent + graph",
@@ -149,6 +158,9 @@ def _case_path(precision: str, n: int, workload: str = "bubbles") -> str:
     d = os.path.join(tempfile.gettempdir(), "mkb200_bench")
     if workload == "dendrite":
         text = cases.thermal_dendrite(n=n, precision=precision, loops=5000)
+    elif workload == "flow_dendrite":
+        text = cases.flow_dendrite(nx=n, ny=n, nz=n, precision=precision, loops=5000, radius=8.0, u_in=0.02,
+                                   center=(n / 3.0, (n - 1) / 2.0, (n - 1) / 2.0))
     else:
         text = cases.multiphase_bubbles(n=n, precision=precision, loops=10000)
     return cases.write(text, os.path.join(d, f"{workload}_{n}_{precision}.xml"))
@@ -162,11 +174,15 @@ def _collide_bytes(workload: str, prec: str, cells: int) -> int:
               16-bit storage.
     dendrite / ensemble: phase-field and T/U lattices (7 + 7) read and
               written, phi(t+1) and phi(t) read, T/U read and written.
+    flow_dendrite: the flow kernel: D3Q19 read and written, phi(t) read, the
+              velocity (3 values) written.
     """
     S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
     P = 8 if prec == "fp64" else 4
     if workload == "bubbles":
         return cells * (2 * 38 * S + P + (4 if S == 2 else 0))
+    if workload == "flow_dendrite":
+        return cells * (38 * S + 4 * P)
     return cells * (28 * S + 4 * P)
 
 
@@ -231,7 +247,7 @@ def run_ours(args):
         mlups = cells * K * ws / (ms * 1e-3) / 1e6
         bpc = s.bytes_per_cell()
         # dominant kernel, timed live with CUDA events on the library's stream
-        prof = s.profile(min(K, 50), "collide")
+        prof = s.profile(min(K, 50), wl.get("slot", "collide"))
         prof_phi = s.profile(min(K, 50), "phi")
         fluid = s.fluid_cells()
         launches = min(K, 50)
@@ -240,12 +256,22 @@ def run_ours(args):
         achieved = collide_bytes / t_launch / 1e9
         step_gbs = bpc * cells * K / (ms * 1e-3) / 1e9
         d = s.diagnostics(raise_on_divergence=False)
+        extra = {}
+        if wl.get("slot", "collide") != "collide":
+            # the phase-field / advected thermal kernel of the coupled model:
+            # g and T read and written, phi(t+1), phi(t) and the velocity read,
+            # T/U read and written
+            pd = s.profile(launches, "collide")
+            S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
+            Pb = 8 if prec == "fp64" else 4
+            t_d = pd["kernel_ms"] / launches
+            extra = {"dend_ms": t_d, "dend_frac": fluid * (28 * S + 7 * Pb) / (t_d * 1e-3) / 1e9 / peak}
         results[prec] = {
             "mlups": mlups, "ms_per_step": ms / K, "bytes_per_cell": bpc, "step_gbs": step_gbs,
             "step_frac": step_gbs / peak, "collide_ms": prof["kernel_ms"] / launches,
             "phi_ms": prof_phi["kernel_ms"] / launches, "collide_gbs": achieved, "collide_frac": achieved / peak,
             "collide_bytes_per_launch": collide_bytes, "clocks": clk.summary(), "n_bad": d["n_bad"],
-            "launches_per_step": s.launches_per_step(), "tune": tune,
+            "launches_per_step": s.launches_per_step(), "tune": tune, **extra,
         }
         if prec == args.precision:
             main = (params, s)
@@ -323,6 +349,8 @@ def run_ours(args):
                          "collide_frac": round(v["collide_frac"], 4), "step_frac": round(v["step_frac"], 4),
                          "bytes_per_cell": v["bytes_per_cell"], "n_bad": v["n_bad"],
                          "collide_ms": round(v["collide_ms"], 4), "phi_ms": round(v["phi_ms"], 4),
+                         **({"dend_ms": round(v["dend_ms"], 4), "dend_frac": round(v["dend_frac"], 4)}
+                            if "dend_ms" in v else {}),
                          "tuned": {"block": list(v["tune"]["block"]), "minb": v["tune"]["minb"]},
                          "speedup_vs_fp32": round(v["mlups"] / results["fp32"]["mlups"], 3)
                          if "fp32" in results else None}

@@ -218,6 +218,18 @@ typedef struct mk_diag {
   int32_t _pad;
 } mk_diag;
 
+/* Interface tip of one seed: the distance from the seed's centre to the
+ * outermost phi = iso crossing along +x, -x, +y, -y, +z, -z (phi sampled
+ * bilinearly across the line through the centre, linearly along it; 0 when
+ * the centre is outside, phi < iso), and its rate of change per loop since
+ * the previous mk_tip_track call on the handle for the same seed and iso
+ * (0 on the first call). */
+typedef struct mk_tip {
+  int64_t step;
+  double length[6];
+  double velocity[6];
+} mk_tip;
+
 typedef struct mk_handle mk_handle;
 
 /* Library / ABI. */
@@ -273,6 +285,23 @@ mk_status mk_set_state_f32(mk_handle* h, const float* phi, const float* temp, co
 /* Legacy VTK RECTILINEAR_GRID writer in the reference's format
  * (MaterKit/src/mkFluidsUser.cpp:714-947); file <dir>/fluid_t<loops>.vtk. */
 mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir);
+
+/* Points of the phi = iso surface, in place of the ParaView contour of the
+ * reference's post-processing (MaterKit/SaveContourBatch.py: Contour of
+ * order_parameter at 0 on each fluid_t<loops>.vtk).  One point per grid edge
+ * (no periodic wrap) whose end values straddle iso, placed by linear
+ * interpolation in the VTK coordinates (cell index + 0.5): the vertices of a
+ * marching-cubes contour.  Writes min(count, capacity) points: xyz gets 3
+ * doubles per point, scalar (nullable) the temperature or solute of the
+ * dendrite models interpolated the same way (0 for the others).  *count is
+ * the total; capacity 0 only counts.  Order: by cell index, then axis.
+ * MK_ERR_ARG for the models without an order parameter (flow, convection). */
+mk_status mk_interface_points(mk_handle* h, double iso, double* xyz, double* scalar, int64_t capacity,
+                              int64_t* count);
+
+/* Tip lengths and velocities of seed `seed` (mk_tip); MK_ERR_ARG without an
+ * order parameter or for a seed index out of range. */
+mk_status mk_tip_track(mk_handle* h, int32_t seed, double iso, mk_tip* out);
 
 /* FP64 conservation sums and the divergence watchdog. */
 mk_status mk_diagnostics(mk_handle* h, mk_diag* out);

@@ -85,6 +85,10 @@ class MkOptions(C.Structure):
         return cls(model, precision, collision, lattice, magic, device, block_x, block_y)
 
 
+class MkTip(C.Structure):
+    _fields_ = [("step", C.c_int64), ("length", C.c_double * 6), ("velocity", C.c_double * 6)]
+
+
 class MkDiag(C.Structure):
     _fields_ = [("step", C.c_int64), ("mass", C.c_double), ("momentum", C.c_double * 3), ("phi_sum", C.c_double),
                 ("solid_frac", C.c_double), ("heat", C.c_double), ("solute", C.c_double),
@@ -132,6 +136,8 @@ PROTOTYPES = {
     "mk_set_state_f32": (C.c_int, [H] + [P(C.c_float)] * 3),
     "mk_write_vtk": (C.c_int, [H, C.c_int64, C.c_char_p]),
     "mk_diagnostics": (C.c_int, [H, P(MkDiag)]),
+    "mk_interface_points": (C.c_int, [H, C.c_double, P(C.c_double), P(C.c_double), C.c_int64, P(C.c_int64)]),
+    "mk_tip_track": (C.c_int, [H, C.c_int32, C.c_double, P(MkTip)]),
     "mk_checkpoint": (C.c_int, [H, C.c_char_p]),
     "mk_restore": (C.c_int, [H, C.c_char_p]),
     "mk_profile_steps": (C.c_int, [H, C.c_int64, C.c_char_p, P(C.c_double), P(C.c_double), P(C.c_int64)]),

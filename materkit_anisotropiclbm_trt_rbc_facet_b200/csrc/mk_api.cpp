@@ -23,6 +23,11 @@ struct mk_handle {
   mke::Engine e;
   std::string err;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two loops captured, keyed by start parity
+  // last mk_tip_track result (velocity = change per loop since then)
+  int64_t tip_step = -1;
+  int32_t tip_seed = -1;
+  double tip_iso = 0.0;
+  double tip_len[6] = {0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -387,6 +392,41 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
     h->err = "write failed for " + fn.str();
     return MK_ERR_IO;
   }
+  return MK_OK;
+}
+
+mk_status mk_interface_points(mk_handle* h, double iso, double* xyz, double* scalar, int64_t capacity,
+                              int64_t* count) {
+  if (!h || !count || capacity < 0 || (capacity > 0 && !xyz)) return MK_ERR_ARG;
+  cudaError_t st = mke::engine_interface(h->e, iso, xyz, scalar, capacity, count);
+  if (st == cudaErrorInvalidValue) {
+    h->err = "this model has no order parameter";
+    return MK_ERR_ARG;
+  }
+  if (st != cudaSuccess) return cuda_fail(h, st, "interface_points");
+  return MK_OK;
+}
+
+mk_status mk_tip_track(mk_handle* h, int32_t seed, double iso, mk_tip* out) {
+  if (!h || !out) return MK_ERR_ARG;
+  double len[6];
+  cudaError_t st = mke::engine_tip(h->e, seed, iso, len);
+  if (st == cudaErrorInvalidValue) {
+    h->err = "no order parameter, or seed index out of range";
+    return MK_ERR_ARG;
+  }
+  if (st != cudaSuccess) return cuda_fail(h, st, "tip_track");
+  const int64_t step = h->e.step;
+  const bool prev = h->tip_step >= 0 && h->tip_seed == seed && h->tip_iso == iso && step > h->tip_step;
+  out->step = step;
+  for (int q = 0; q < 6; ++q) {
+    out->length[q] = len[q];
+    out->velocity[q] = prev ? (len[q] - h->tip_len[q]) / (double)(step - h->tip_step) : 0.0;
+    h->tip_len[q] = len[q];
+  }
+  h->tip_step = step;
+  h->tip_seed = seed;
+  h->tip_iso = iso;
   return MK_OK;
 }
 

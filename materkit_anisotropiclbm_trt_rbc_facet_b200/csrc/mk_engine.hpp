@@ -49,8 +49,8 @@ struct Engine {
   void* pop0;
   void* pop1;
   void* pop2;         // flow lattice of the flow + dendrite model (deviations f - w rho0)
-  void* face_u;       // flow + dendrite with inflow/outflow: collision velocity of the planes x = 1 and
-                      // x = nx - 2 (2 x 3 x ny nz values, phi type), read by the boundary kernel
+  void* vel;          // flow + dendrite: the loop's collision velocity, 3 planes of ncell (phi type), read by
+                      // the thermal lattice and the boundary kernel
   float* rest1;       // FP32 rest population of lattice 1 (multiphase h) with 16-bit storage, else null
   void* phi[2];
   void* temp;
@@ -114,6 +114,11 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out);
 size_t engine_pop_bytes(const Engine& e, int which);
 
 double engine_bytes_per_cell(const Engine& e);
+
+// phi = iso contour points (mk_interface_points) and tip lengths along the
+// six axis rays from a seed centre (mk_tip_track); mk_interface.cu.
+cudaError_t engine_interface(Engine& e, double iso, double* xyz, double* sc, int64_t capacity, int64_t* count);
+cudaError_t engine_tip(Engine& e, int seed, double iso, double out[6]);
 
 // Discrete adjoint of `steps` thermal dendrite loops from the current state
 // with checkpoints every `every` loops (<= 0: 100).  out = {loss, dL/deps4,

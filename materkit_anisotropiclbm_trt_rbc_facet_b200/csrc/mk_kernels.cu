@@ -491,80 +491,142 @@ struct FdK {
   int inlet;      // 1: inflow at x = 0, outflow at x = nx - 1
 };
 
-template <class S, class P, int Q, int COLL, int PARITY, bool GEN, class NB>
-__device__ __forceinline__ void fd_cell(S* __restrict__ W, S* __restrict__ G, S* __restrict__ Tp,
-                                        const P* __restrict__ phi_new, const P* __restrict__ phi_old,
-                                        P* __restrict__ temp, P* __restrict__ face_u,
-                                        const unsigned char* __restrict__ grain,
-                                        const typename Stor<S>::T* __restrict__ rot, const Geom& g, const NB& nb,
-                                        const int c, const int x, const int yz, const DendK<typename Stor<S>::T>& kd,
-                                        const FdK<typename Stor<S>::T>& k) {
-  typedef typename Stor<S>::T T;
-  T ux, uy, uz;
-  {
-    T f[Q], fc[Q];  // deviations f_i - w_i rho0 before and after the fluid collision
+// BGK / TRT collision with the porous bounce-back folded into the pair loop:
+// f* = f_coll + B (f_inv(i) - rho w_i P_i - f_coll), P_i = -3 e_i.u +
+// 4.5 (e_i.u)^2 - 1.5 u^2 (rho w_i - feq_inv(i)(rho, u) = -rho w_i P_i), the
+// Noble-Torczynski form with f_i cancelled.  Each output needs only the
+// cell's own pair, so no second copy of the populations stays live.
+template <class T, int Q, int COLL>
+__device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T ns, const T half, T& ux, T& uy,
+                                         T& uz) {
+  T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      f[i] = ld_in<S, Q>(W, g.stride, nb, PARITY, c, i);
-      fc[i] = f[i];
+  for (int i = 0; i < Q; ++i) {
+    drho += f[i];
+    if (ex(i)) jx += T(ex(i)) * f[i];
+    if (ey(i)) jy += T(ey(i)) * f[i];
+    if (ez(i)) jz += T(ez(i)) * f[i];
+  }
+  const T rho = k.ref + drho;
+  ux = (jx + T(0.5) * k.Fx) / rho;
+  uy = (jy + T(0.5) * k.Fy) / rho;
+  uz = (jz + T(0.5) * k.Fz) / rho;
+  const T uu = ux * ux + uy * uy + uz * uz;
+  const T uF = ux * k.Fx + uy * k.Fy + uz * k.Fz;
+  const T B = ns > T(0) ? ns * half / ((T(1) - ns) + half) : T(0);
+  T feq[Q], Fi[Q], P[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const T w = T(wq<Q>(i));
+    const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
+    const T eF = T(ex(i)) * k.Fx + T(ey(i)) * k.Fy + T(ez(i)) * k.Fz;
+    P[i] = T(-3) * eu + T(4.5) * eu * eu - T(1.5) * uu;
+    feq[i] = w * (drho + rho * (T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu));
+    Fi[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF);
+  }
+  T fo[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int j = inv(i);
+    T fc;
+    if constexpr (COLL == MK_COLL_TRT) {
+      const T fp = T(0.5) * (f[i] + f[j]), fm = T(0.5) * (f[i] - f[j]);
+      const T ep = T(0.5) * (feq[i] + feq[j]), em = T(0.5) * (feq[i] - feq[j]);
+      const T Fp = T(0.5) * (Fi[i] + Fi[j]), Fm = T(0.5) * (Fi[i] - Fi[j]);
+      fc = f[i] - k.om * (fp - ep) - k.om_m * (fm - em) + (T(1) - T(0.5) * k.om) * Fp + (T(1) - T(0.5) * k.om_m) * Fm;
+    } else {
+      fc = f[i] - k.om * (f[i] - feq[i]) + (T(1) - T(0.5) * k.om) * Fi[i];
     }
-    flow_relax<T, Q, COLL>(fc, k.f, k.f.Fx, k.f.Fy, k.f.Fz, ux, uy, uz);
-    const T ns = fmin(T(1), fmax(T(0), T(0.5) * (T(1) + T(phi_old[c]))));
+    fo[i] = fc + B * (f[j] - rho * T(wq<Q>(i)) * P[i] - fc);
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = fo[i];
+}
+
+// Flow lattice of one cell: collision with the porous bounce-back of the
+// crystal (solid fraction of the previous loop's phi).  MRT collides in
+// moment space and applies the porous term after it, reading the
+// pre-collision populations again (each slot is read and written by this
+// cell alone in the AA layout, and no store has happened yet).  The
+// collision velocity goes to vel[3][ncell] for the thermal lattice and the
+// boundary pass.
+template <class S, class P, int Q, int COLL, int PARITY, class NB>
+__device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restrict__ phi_old, P* __restrict__ vel,
+                                             const int64_t stride, const int64_t ncell, const NB& nb, const int c,
+                                             const FdK<typename Stor<S>::T>& k) {
+  typedef typename Stor<S>::T T;
+  T f[Q];  // deviations f_i - w_i rho0, post-collision after the relaxation
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(W, stride, nb, PARITY, c, i);
+  T ux, uy, uz;
+  const T ns = fmin(T(1), fmax(T(0), T(0.5) * (T(1) + T(phi_old[c]))));
+  if constexpr (COLL == MK_COLL_MRT && Q == 19) {
+    flow_relax<T, Q, COLL>(f, k.f, k.f.Fx, k.f.Fy, k.f.Fz, ux, uy, uz);
     if (ns > T(0)) {
       const T B = ns * k.half / ((T(1) - ns) + k.half);
       T drho = T(0);
 #pragma unroll
-      for (int i = 0; i < Q; ++i) drho += f[i];
+      for (int i = 0; i < Q; ++i) drho += ld_in<S, Q>(W, stride, nb, PARITY, c, i);
       const T rho = k.f.ref + drho;
       const T uu = ux * ux + uy * uy + uz * uz;
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
-        const T w = T(wq<Q>(i));
         const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
-        // rho w - feq_inv(i)(rho, u) with e_inv(i).u = -e_i.u
-        const T om_s = f[inv(i)] - f[i] - rho * w * (T(-3) * eu + T(4.5) * eu * eu - T(1.5) * uu);
-        fc[i] += B * (om_s - (fc[i] - f[i]));
+        const T fk = ld_in<S, Q>(W, stride, nb, PARITY, c, inv(i));
+        f[i] += B * (fk - rho * T(wq<Q>(i)) * (T(-3) * eu + T(4.5) * eu * eu - T(1.5) * uu) - f[i]);
       }
     }
+  } else {
+    fd_relax<T, Q, COLL>(f, k.f, ns, k.half, ux, uy, uz);
+  }
 #pragma unroll
-    for (int i = 0; i < Q; ++i) st_out<S, Q>(W, g.stride, nb, PARITY, c, i, fc[i]);
-  }
-  if (k.inlet) {
-    const int plane = g.ny * g.nz;
-    if (x == 1) {
-      face_u[yz] = P(ux);
-      face_u[plane + yz] = P(uy);
-      face_u[2 * plane + yz] = P(uz);
-    }
-    if (x == g.nx - 2) {
-      face_u[3 * plane + yz] = P(ux);
-      face_u[4 * plane + yz] = P(uy);
-      face_u[5 * plane + yz] = P(uz);
-    }
-  }
-  dend_cell<S, P, PARITY, false, GEN, NB, true>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, kd, ux,
-                                                uy, uz);
+  for (int i = 0; i < Q; ++i) st_out<S, Q>(W, stride, nb, PARITY, c, i, f[i]);
+  vel[c] = P(ux);
+  vel[ncell + c] = P(uy);
+  vel[2 * ncell + c] = P(uz);
 }
 
-template <class S, class P, int Q, int COLL, int PARITY, bool GEN>
+template <class S, class P, int Q, int COLL, int PARITY>
 __global__ void __launch_bounds__(256)
-    k_fd_collide(S* __restrict__ W, S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
-                 const P* __restrict__ phi_old, P* __restrict__ temp, P* __restrict__ face_u,
-                 const unsigned char* __restrict__ grain, const typename Stor<S>::T* __restrict__ rot, const Geom g,
-                 const DendK<typename Stor<S>::T> kd, const FdK<typename Stor<S>::T> k) {
+    k_fd_flow(S* __restrict__ W, const P* __restrict__ phi_old, P* __restrict__ vel, const Geom g,
+              const FdK<typename Stor<S>::T> k) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  const int yz = y + g.ny * z;
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
   if (fastw_cell(g, x, y, z)) {
     const FastW fa = make_fastw(g, x, y, z);
-    fd_cell<S, P, Q, COLL, PARITY, GEN>(W, G, Tp, phi_new, phi_old, temp, face_u, grain, rot, g, fa, fa.c, x, yz, kd,
-                                        k);
+    fd_flow_cell<S, P, Q, COLL, PARITY>(W, phi_old, vel, g.stride, ncell, fa, fa.c, k);
   } else {
     const Nbr nb(g, x, y, z);
-    fd_cell<S, P, Q, COLL, PARITY, GEN>(W, G, Tp, phi_new, phi_old, temp, face_u, grain, rot, g, nb, nb.idx(0, 0, 0),
-                                        x, yz, kd, k);
+    fd_flow_cell<S, P, Q, COLL, PARITY>(W, phi_old, vel, g.stride, ncell, nb, nb.idx(0, 0, 0), k);
+  }
+}
+
+// Phase field and thermal lattice with the equilibrium advected by the
+// loop's flow velocity.
+template <class S, class P, int PARITY, bool GEN>
+__global__ void __launch_bounds__(256)
+    k_fd_dend(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
+              P* __restrict__ temp, const P* __restrict__ vel, const unsigned char* __restrict__ grain,
+              const typename Stor<S>::T* __restrict__ rot, const Geom g, const DendK<typename Stor<S>::T> k) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+  if (fastw_cell(g, x, y, z)) {
+    const FastW fa = make_fastw(g, x, y, z);
+    const int c = fa.c;
+    dend_cell<S, P, PARITY, false, GEN, FastW, true>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, c, k,
+                                                     T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]));
+  } else {
+    const Nbr nb(g, x, y, z);
+    const int c = nb.idx(0, 0, 0);
+    dend_cell<S, P, PARITY, false, GEN, Nbr, true>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, k,
+                                                   T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]));
   }
 }
 
@@ -578,13 +640,13 @@ __global__ void __launch_bounds__(256)
 // outflow (x = nx - 1): rho_b = rho0, u_b = u_n, phi_b = phi_n, T_b = T_n;
 // the face cell's temperature becomes T_b.
 // rho_n, u_n, phi_n, T_n are moments of the post-collision populations of n,
-// except the thermal u_n, the collision velocity of n (face_u).  One thread
+// except the thermal u_n, the collision velocity of n (vel).  One thread
 // per face cell; each writes only its own cell's outgoing slots and reads only
 // those of x = 1 / x = nx - 2, so no two threads touch one slot.
 template <class S, class P, int Q>
 __global__ void __launch_bounds__(128)
     k_fd_nee(S* __restrict__ W, S* __restrict__ G, S* __restrict__ Tp, P* __restrict__ temp,
-             const P* __restrict__ face_u, const Geom g, int64_t steps_done, const FdK<typename Stor<S>::T> k) {
+             const P* __restrict__ vel, const Geom g, int64_t steps_done, const FdK<typename Stor<S>::T> k) {
   typedef typename Stor<S>::T T;
   const int plane = g.ny * g.nz;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -633,8 +695,8 @@ __global__ void __launch_bounds__(128)
   }
   const T phn = k.ref_g + sg, Tn = k.ref_t + st;
   const T phb = side == 0 ? T(-1) : phn, Tb = side == 0 ? k.ref_t : Tn;
-  const P* fu = face_u + 3 * side * plane;
-  const T vn[3] = {T(fu[yz]), T(fu[plane + yz]), T(fu[2 * plane + yz])};
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+  const T vn[3] = {T(vel[cn]), T(vel[ncell + cn]), T(vel[2 * ncell + cn])};
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
@@ -1308,33 +1370,17 @@ FdK<T> fd_coef(const mk_params& p, Refs r) {
   return k;
 }
 
-template <class S, int Q, int COLL, int PARITY>
-void launch_fd_collide(mke::Engine& e, dim3 grid, dim3 block, bool gen) {
+template <class S, int Q, int COLL>
+void launch_fd_flow(mke::Engine& e, int parity, dim3 grid, dim3 block) {
   typedef typename Stor<S>::T T;
   typedef typename PhiOf<S>::type P;
   const Geom g = make_geom(e);
-  const Refs r = refs_of(e.p);
-  const DendK<T> kd = dend_coef<T>(e.p, r);
-  const FdK<T> k = fd_coef<T>(e.p, r);
-  P* phi_old = (P*)e.phi[e.phi_cur];
-  P* phi_new = (P*)e.phi[1 - e.phi_cur];
-  if (gen)
-    k_fd_collide<S, P, Q, COLL, PARITY, true><<<grid, block, 0, e.stream>>>(
-        (S*)e.pop2, (S*)e.pop0, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, (P*)e.face_u, e.grain, (const T*)e.rot, g,
-        kd, k);
-  else
-    k_fd_collide<S, P, Q, COLL, PARITY, false><<<grid, block, 0, e.stream>>>(
-        (S*)e.pop2, (S*)e.pop0, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, (P*)e.face_u, e.grain, (const T*)e.rot, g,
-        kd, k);
-}
-
-template <class S, int Q, int COLL>
-void launch_fd_q(mke::Engine& e, int parity, dim3 grid, dim3 block) {
-  const bool gen = e.p.aniso != MK_ANISO_CUBIC;
+  const FdK<T> k = fd_coef<T>(e.p, refs_of(e.p));
+  const P* phi_old = (const P*)e.phi[e.phi_cur];
   if (parity == 0)
-    launch_fd_collide<S, Q, COLL, 0>(e, grid, block, gen);
+    k_fd_flow<S, P, Q, COLL, 0><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k);
   else
-    launch_fd_collide<S, Q, COLL, 1>(e, grid, block, gen);
+    k_fd_flow<S, P, Q, COLL, 1><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k);
 }
 
 // Flow + dendrite loop: phi of the streamed phase field, the fused flow /
@@ -1360,29 +1406,46 @@ void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   const int Q = e.p.lattice, C = e.p.collision;
   if (Q == 19) {
     if (C == MK_COLL_BGK)
-      launch_fd_q<S, 19, MK_COLL_BGK>(e, parity, grid, block);
+      launch_fd_flow<S, 19, MK_COLL_BGK>(e, parity, grid, block);
     else if (C == MK_COLL_TRT)
-      launch_fd_q<S, 19, MK_COLL_TRT>(e, parity, grid, block);
+      launch_fd_flow<S, 19, MK_COLL_TRT>(e, parity, grid, block);
     else
-      launch_fd_q<S, 19, MK_COLL_MRT>(e, parity, grid, block);
+      launch_fd_flow<S, 19, MK_COLL_MRT>(e, parity, grid, block);
   } else {
     if (C == MK_COLL_BGK)
-      launch_fd_q<S, 27, MK_COLL_BGK>(e, parity, grid, block);
+      launch_fd_flow<S, 27, MK_COLL_BGK>(e, parity, grid, block);
     else
-      launch_fd_q<S, 27, MK_COLL_TRT>(e, parity, grid, block);
+      launch_fd_flow<S, 27, MK_COLL_TRT>(e, parity, grid, block);
   }
-  if (ev) cudaEventRecord(ev[3], e.stream);
+  if (ev) {
+    cudaEventRecord(ev[3], e.stream);
+    cudaEventRecord(ev[4], e.stream);
+  }
+  {
+    const DendK<T> kd = dend_coef<T>(e.p, r);
+    const bool gen = e.p.aniso != MK_ANISO_CUBIC;
+    const P* vel = (const P*)e.vel;
+#define MK_FDD(PAR, GEN)                                                                                      \
+  k_fd_dend<S, P, PAR, GEN><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, vel, \
+                                                          e.grain, (const T*)e.rot, g, kd)
+    if (parity == 0)
+      gen ? MK_FDD(0, true) : MK_FDD(0, false);
+    else
+      gen ? MK_FDD(1, true) : MK_FDD(1, false);
+#undef MK_FDD
+  }
+  if (ev) cudaEventRecord(ev[5], e.stream);
   if (e.p.inlet) {
-    if (ev) cudaEventRecord(ev[4], e.stream);
+    if (ev) cudaEventRecord(ev[6], e.stream);
     const FdK<T> k = fd_coef<T>(e.p, r);
     const int nt = 2 * e.ny * e.nz;
     if (Q == 19)
-      k_fd_nee<S, P, 19><<<(nt + 127) / 128, 128, 0, e.stream>>>((S*)e.pop2, G, (S*)e.pop1, (P*)e.temp, (const P*)e.face_u, g,
+      k_fd_nee<S, P, 19><<<(nt + 127) / 128, 128, 0, e.stream>>>((S*)e.pop2, G, (S*)e.pop1, (P*)e.temp, (const P*)e.vel, g,
                                                                  e.step + 1, k);
     else
-      k_fd_nee<S, P, 27><<<(nt + 127) / 128, 128, 0, e.stream>>>((S*)e.pop2, G, (S*)e.pop1, (P*)e.temp, (const P*)e.face_u, g,
+      k_fd_nee<S, P, 27><<<(nt + 127) / 128, 128, 0, e.stream>>>((S*)e.pop2, G, (S*)e.pop1, (P*)e.temp, (const P*)e.vel, g,
                                                                  e.step + 1, k);
-    if (ev) cudaEventRecord(ev[5], e.stream);
+    if (ev) cudaEventRecord(ev[7], e.stream);
   }
 }
 
@@ -1414,7 +1477,7 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
     case MK_MODEL_FLOW_DENDRITE:
       launch_fd<S>(e, parity, grid, block, ev);
       e.phi_cur = 1 - e.phi_cur;
-      e.launches += e.p.inlet ? 3 : 2;
+      e.launches += e.p.inlet ? 4 : 3;
       break;
     default:
       launch_dend<S>(e, parity, grid, block, ev);
@@ -1637,8 +1700,8 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   if ((st = alloc(&e.pop0, (size_t)e.Q0 * e.stride * e.elem)) != cudaSuccess) return st;
   if ((st = alloc(&e.pop1, (size_t)e.Q1 * e.stride * e.elem)) != cudaSuccess) return st;
   if ((st = alloc(&e.pop2, (size_t)e.Q2 * e.stride * e.elem)) != cudaSuccess) return st;
-  const bool faces = p.model == MK_MODEL_FLOW_DENDRITE && p.inlet;
-  if ((st = alloc(&e.face_u, faces ? (size_t)6 * p.ny * p.nz * e.phi_elem : 0)) != cudaSuccess) return st;
+  const bool fd = p.model == MK_MODEL_FLOW_DENDRITE;
+  if ((st = alloc(&e.vel, fd ? (size_t)3 * e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (p.model == MK_MODEL_MULTIPHASE && e.elem == 2) {
     if ((st = alloc((void**)&e.rest1, (size_t)e.ncell * sizeof(float))) != cudaSuccess) return st;
   } else {
@@ -1699,7 +1762,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
-  void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.face_u, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
+  void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.vel, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
                   e.field32, e.stage32};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -1805,13 +1868,17 @@ cudaError_t engine_step(Engine& e, cudaEvent_t* ev) {
 static bool one_kernel(const Engine& e) { return e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION; }
 
 int engine_kernels_per_step(const Engine& e) {
-  if (e.p.model == MK_MODEL_FLOW_DENDRITE) return e.p.inlet ? 3 : 2;
+  if (e.p.model == MK_MODEL_FLOW_DENDRITE) return e.p.inlet ? 4 : 3;
   return one_kernel(e) ? 1 : 2;
 }
 
 const char* engine_kernel_name(const Engine& e, int k) {
   if (one_kernel(e)) return "collide";
-  return k == 0 ? "phi" : (k == 1 ? "collide" : "boundary");
+  if (e.p.model == MK_MODEL_FLOW_DENDRITE) {
+    static const char* const names[4] = {"phi", "flow", "collide", "boundary"};
+    return k >= 0 && k < 4 ? names[k] : "";
+  }
+  return k == 0 ? "phi" : "collide";
 }
 
 cudaError_t engine_field(Engine& e, int field) {

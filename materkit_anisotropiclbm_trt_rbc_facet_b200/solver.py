@@ -255,6 +255,47 @@ class Solver:
         _check(self._lib.mk_write_vtk(self._h, int(loops), os.fsencode(directory)), self._h)
         return os.path.join(directory, f"fluid_t{loops}.vtk")
 
+    def _iso(self, iso):
+        if iso is not None:
+            return float(iso)
+        return 0.5 if self.params.model == A.MK_MODEL_MULTIPHASE else 0.0
+
+    def interface_points(self, iso: float | None = None) -> dict:
+        """phi = iso contour points ((N, 3) VTK coordinates) and the scalar
+        (T or C of the dendrite models) interpolated at them; iso defaults to 0
+        (dendrites) or 1/2 (multiphase)."""
+        iso = self._iso(iso)
+        n = C.c_int64()
+        _check(self._lib.mk_interface_points(self._h, iso, None, None, 0, C.byref(n)), self._h)
+        xyz = np.zeros((max(n.value, 1), 3))
+        sc = np.zeros(max(n.value, 1))
+        dp = C.POINTER(C.c_double)
+        _check(self._lib.mk_interface_points(self._h, iso, xyz.ctypes.data_as(dp), sc.ctypes.data_as(dp), n.value,
+                                             C.byref(n)), self._h)
+        return {"xyz": xyz[:n.value], "scalar": sc[:n.value], "iso": iso}
+
+    def write_contour_csv(self, loops: int, directory: str, iso: float | None = None) -> str:
+        """loops<loops>.csv of the phi = iso contour points, in the column
+        layout of a ParaView contour export (order_parameter, temperature or
+        solute, Points:0..2), 8 significant digits."""
+        pts = self.interface_points(iso)
+        os.makedirs(directory, exist_ok=True)
+        path = os.path.join(directory, f"loops{loops}.csv")
+        name = "X0_solutes" if self.params.model == A.MK_MODEL_SOLUTAL_DENDRITE else "temperature"
+        with open(path, "w") as f:
+            f.write(f'"order_parameter","{name}","Points:0","Points:1","Points:2"\n')
+            for (x, y, z), v in zip(pts["xyz"], pts["scalar"]):
+                f.write(f"{pts['iso']:.8g},{v:.8g},{x:.8g},{y:.8g},{z:.8g}\n")
+        return path
+
+    def tip(self, seed: int = 0, iso: float | None = None) -> dict:
+        """Distances from the seed centre to the outermost interface crossing
+        along +x, -x, +y, -y, +z, -z, and their change per loop since the
+        previous call for the same seed."""
+        t = A.MkTip()
+        _check(self._lib.mk_tip_track(self._h, int(seed), self._iso(iso), C.byref(t)), self._h)
+        return {"step": t.step, "length": list(t.length), "velocity": list(t.velocity)}
+
     def diagnostics(self, raise_on_divergence: bool = True) -> dict:
         d = A.MkDiag()
         st = self._lib.mk_diagnostics(self._h, C.byref(d))

@@ -73,7 +73,7 @@ def test_flow_dendrite_16bit(casedir, prec, tol):
 def test_flow_dendrite_launches_graph_and_checkpoint(casedir, tmp_path):
     p = case_params(cases.write(_case("fp32"), f"{casedir}/fd_ck.xml"))
     a, b = Solver(params=p), Solver(params=p)
-    assert a.launches_per_step() == 3
+    assert a.launches_per_step() == 4  # phi, flow, phase field + thermal, boundary
     prof = a.profile(4, "boundary")
     assert prof["kernel_ms"] > 0
     b.advance(4)

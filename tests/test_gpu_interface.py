@@ -1,0 +1,106 @@
+"""phi = iso contour points and tip tracking on the device (the ParaView
+contour step of the reference's post-processing), checked against a numpy
+restatement on the same phi field downloaded from the device."""
+import numpy as np
+import pytest
+
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
+
+pytestmark = pytest.mark.gpu
+
+
+def contour_points(phi, sc, iso):
+    """Edge crossings of the grid (no wrap), ordered by cell index then axis."""
+    nz, ny, nx = phi.shape
+    keys, pts, vals = [], [], []
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cell = xx + nx * (yy + ny * zz)
+    for a, (dz, dy, dx) in enumerate([(0, 0, 1), (0, 1, 0), (1, 0, 0)]):
+        sl_a = (slice(0, nz - dz), slice(0, ny - dy), slice(0, nx - dx))
+        sl_b = (slice(dz, nz), slice(dy, ny), slice(dx, nx))
+        pa, pb = phi[sl_a], phi[sl_b]
+        m = (pa < iso) != (pb < iso)
+        t = (iso - pa[m]) / (pb[m] - pa[m])
+        p = np.stack([xx[sl_a][m] + 0.5 + dx * t, yy[sl_a][m] + 0.5 + dy * t, zz[sl_a][m] + 0.5 + dz * t], axis=1)
+        keys.append(cell[sl_a][m] * 3 + a)
+        pts.append(p)
+        vals.append(sc[sl_a][m] + t * (sc[sl_b][m] - sc[sl_a][m]))
+    k = np.concatenate(keys)
+    o = np.argsort(k, kind="stable")
+    return np.concatenate(pts)[o], np.concatenate(vals)[o]
+
+
+def _dend(casedir, prec="fp64", n=40):
+    p = case_params(cases.write(cases.thermal_dendrite(n=n, precision=prec, loops=100, radius=6.0),
+                                f"{casedir}/iface_{prec}_{n}.xml"))
+    return p, Solver(params=p)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_contour_points_match_numpy(casedir, prec):
+    p, s = _dend(casedir, prec)
+    s.advance(60)
+    r = s.interface_points()
+    xyz, sc = contour_points(s.field("phi"), s.field("T"), 0.0)
+    assert len(r["xyz"]) == len(xyz) > 100
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    assert np.abs(r["xyz"] - xyz).max() < tol
+    assert np.abs(r["scalar"] - sc).max() < tol
+    # every point lies on an edge: two integer (+0.5) coordinates
+    frac = np.abs(r["xyz"] - 0.5 - np.round(r["xyz"] - 0.5)) < 1e-9
+    assert (frac.sum(axis=1) >= 2).all()
+
+
+def test_contour_csv(casedir, tmp_path):
+    p, s = _dend(casedir)
+    path = s.write_contour_csv(0, str(tmp_path))
+    lines = open(path).read().splitlines()
+    assert lines[0] == '"order_parameter","temperature","Points:0","Points:1","Points:2"'
+    assert len(lines) - 1 == len(s.interface_points()["xyz"])
+
+
+def test_tip_of_initial_seed_and_growth(casedir):
+    p, s = _dend(casedir, n=40)
+    t0 = s.tip()
+    # phi = -tanh((r - R)/(sqrt2 W)) vanishes at r = R = 6; the lines through
+    # the half-integer centre pass 0.7 cells off it and linear sampling
+    # between cells puts the crossing within a tenth of R
+    assert np.allclose(t0["length"], 6.0, atol=0.1), t0
+    assert t0["velocity"] == [0.0] * 6
+    # centred seed with cubic anisotropy: the six arms stay equal
+    s.advance(200)
+    t1 = s.tip()
+    L = np.array(t1["length"])
+    assert np.abs(L - L[0]).max() < 1e-9 and L[0] > 6.5
+    assert np.allclose(t1["velocity"], (L - np.array(t0["length"])) / 200)
+
+
+def test_tip_matches_numpy_samples(casedir):
+    p, s = _dend(casedir, n=32)
+    s.advance(120)
+    phi = s.field("phi")
+    c = np.array(p.obj_center[0][:3])
+    L = s.tip()["length"]
+    # +x ray: phi along x at the bilinear mix of the four lines around (cy, cz)
+    y0, z0 = int(np.floor(c[1])), int(np.floor(c[2]))
+    wy, wz = c[1] - y0, c[2] - z0
+    line = ((1 - wy) * (1 - wz) * phi[z0, y0] + wy * (1 - wz) * phi[z0, y0 + 1] + (1 - wy) * wz * phi[z0 + 1, y0] +
+            wy * wz * phi[z0 + 1, y0 + 1])
+    k = int(np.ceil(c[0]))
+    while k + 1 < p.nx and line[k + 1] >= 0:
+        k += 1
+    expect = k + line[k] / (line[k] - line[k + 1]) - c[0]
+    assert abs(L[0] - expect) < 1e-12
+
+
+def test_multiphase_and_flow(casedir):
+    p = case_params(cases.write(cases.multiphase_bubbles(n=40, precision="fp32", loops=10, bubbles=2, rmin=4.0,
+                                                                 rmax=6.0), f"{casedir}/mpi.xml"))
+    s = Solver(params=p)
+    r = s.interface_points()
+    assert r["iso"] == 0.5 and len(r["xyz"]) > 100
+    q = case_params(cases.write(cases.poiseuille(nx=8, ny=6, nz=4, loops=1), f"{casedir}/fl.xml"))
+    f = Solver(params=q)
+    with pytest.raises(A.MkError):
+        f.interface_points()
