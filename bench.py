@@ -186,6 +186,31 @@ def _collide_bytes(workload: str, prec: str, cells: int) -> int:
     return cells * (28 * S + 4 * P)
 
 
+def _reducers(pg, device: str):
+    """Max and sum of a host scalar over the ranks of `pg` (None: one rank),
+    through a one-element FP64 tensor on `device` ("cuda" under NCCL, "cpu"
+    under gloo).  Every rank must call them in the same order."""
+    if pg is None:
+        return (lambda x: x), (lambda x: x)
+
+    def red(x, op):
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+        pg.all_reduce(t, op=op)
+        return float(t.item())
+
+    return (lambda x: red(x, pg.ReduceOp.MAX)), (lambda x: red(x, pg.ReduceOp.SUM))
+
+
+def job_mlups(cells_local: int, steps: int, seconds_local: float, reduce_max, reduce_sum):
+    """Whole-job MLUPS of a sharded or replicated run: the cells every rank
+    advanced, `steps` times, over the slowest rank's time.  Returns (MLUPS,
+    the max time)."""
+    t = reduce_max(seconds_local)
+    cells = reduce_sum(cells_local)
+    return cells * steps / t / 1e6, t
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -215,13 +240,7 @@ def run_ours(args):
         if pg is not None:
             pg.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks, sum_over_ranks = _reducers(pg, "cuda")
 
     n = args.size
     wl = WORKLOADS[args.workload]
@@ -242,9 +261,9 @@ def run_ours(args):
         clk = Clocks(local)
         with clk:
             ms = s.time_advance(K, graph=True)
-        ms = max_over_ranks(ms)
         cells = params.ncell()
-        mlups = cells * K * ws / (ms * 1e-3) / 1e6
+        mlups, ms_s = job_mlups(cells, K, ms * 1e-3, max_over_ranks, sum_over_ranks)
+        ms = ms_s * 1e3
         bpc = s.bytes_per_cell()
         # dominant kernel, timed live with CUDA events on the library's stream
         prof = s.profile(min(K, 50), wl.get("slot", "collide"))
@@ -299,10 +318,9 @@ def run_ours(args):
     stt |= lib.mk_advance_graph(s.handle, K)
     stt |= lib.mk_get_field(s.handle, A.MK_FIELD_PHI, A.MK_DTYPE_F32, hp_out, nbytes)
     e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s)
+    e2e_mlups, e2e_s = job_mlups(cells, K, e2e_s, max_over_ranks, sum_over_ranks)  # every rank, even on error
     if stt != 0:
         raise A.MkError(stt, lib.mk_last_error(s.handle).decode())
-    e2e_mlups = cells * K * ws / e2e_s / 1e6
     phi_ok = bool(np.isfinite(phi_out).all())
     lib.mk_host_free(hp_in)
     lib.mk_host_free(hp_out)
@@ -386,13 +404,7 @@ def run_ensemble(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
 
-    def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks, sum_over_ranks = _reducers(pg, "cuda")
 
     wl = WORKLOADS["ensemble"]
     K, W = args.steps, args.warmup
@@ -413,8 +425,9 @@ def run_ensemble(args):
         with clk:
             ms = e.time_advance(K)
         launches = e.launches - l0
-        ms = max_over_ranks(ms)
         cells = e.cells
+        mlups, ms_s = job_mlups(cells, K, ms * 1e-3, max_over_ranks, sum_over_ranks)
+        ms = ms_s * 1e3
         nprof = min(K, 50)
         prof = e.profile(nprof, "collide")
         prof_phi = e.profile(nprof, "phi")
@@ -426,7 +439,7 @@ def run_ensemble(args):
         bad = 0
         for d in range(nd):
             bad += int((~np.isfinite(e.field(d, "phi", np.float32))).sum())
-        results[prec] = {"mlups": cells * K * ws / (ms * 1e-3) / 1e6, "ms_per_step": ms / K, "cells": cells,
+        results[prec] = {"mlups": mlups, "ms_per_step": ms / K, "cells": cells,
                          "collide_ms": prof["kernel_ms"] / nprof, "phi_ms": prof_phi["kernel_ms"] / nprof,
                          "collide_gbs": cb / t_launch / 1e9, "collide_frac": cb / t_launch / 1e9 / peak,
                          "collide_bytes_per_launch": cb, "step_bytes_per_cell": step_bytes / cells,
@@ -446,7 +459,7 @@ def run_ensemble(args):
     e = Ensemble(ps)
     e.advance(K)
     phis = [e.field(d, "phi", np.float32) for d in range(nd)]
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_mlups, e2e_s = job_mlups(cells, K, time.perf_counter() - t0, max_over_ranks, sum_over_ranks)
     phi_ok = all(bool(np.isfinite(x).all()) for x in phis)
     e.close()
     cpu = None
@@ -479,7 +492,7 @@ def run_ensemble(args):
                          "collide_ms": round(v["collide_ms"], 4), "phi_ms": round(v["phi_ms"], 4),
                          "collide_frac": round(v["collide_frac"], 4), "step_frac": round(v["step_frac"], 4),
                          "n_bad": v["n_bad"]} for k, v in results.items()},
-        "e2e": {"value": round(cells * K * ws / e2e_s / 1e6, 1), "unit": "MLUPS",
+        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": cells * 16 / K, "d2h_bytes_per_step": cells * 4 / K,
                 "seconds": round(e2e_s, 4), "phi_finite": phi_ok,
                 "path": "mk_ensemble_create (host initial fields, FP64) + mk_ensemble_advance + "

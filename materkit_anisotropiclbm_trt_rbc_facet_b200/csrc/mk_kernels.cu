@@ -491,12 +491,16 @@ struct FdK {
   int inlet;      // 1: inflow at x = 0, outflow at x = nx - 1
 };
 
-// BGK / TRT collision with the porous bounce-back folded into the pair loop:
-// f* = f_coll + B (f_inv(i) - rho w_i P_i - f_coll), P_i = -3 e_i.u +
-// 4.5 (e_i.u)^2 - 1.5 u^2 (rho w_i - feq_inv(i)(rho, u) = -rho w_i P_i), the
-// Noble-Torczynski form with f_i cancelled.  Each output needs only the
-// cell's own pair, so no second copy of the populations stays live.
-template <class T, int Q, int COLL>
+// BGK / TRT collision with the porous bounce-back, over opposite pairs
+// (i, j = inv i; BGK is TRT with omega- = omega+).  With e_j = -e_i the pair's
+// symmetric and antisymmetric equilibrium parts are w (drho + rho (4.5 eu^2 -
+// 1.5 u^2)) and w rho 3 eu, the Guo force parts w (9 eu eF - 3 u.F) and w 3 eF.
+// The porous term f* = f_coll + B (f_inv(i) - rho w_i P_i - f_coll),
+// P_i = -3 e_i.u + 4.5 (e_i.u)^2 - 1.5 u^2 (rho w_i - feq_inv(i)(rho, u) =
+// -rho w_i P_i), is the Noble-Torczynski form with f_i cancelled; it is
+// evaluated only when a lane of the warp has B > 0.  FORCE = false drops the
+// force terms (a zero body force).
+template <class T, int Q, int COLL, bool FORCE>
 __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T ns, const T half, T& ux, T& uy,
                                          T& uz) {
   T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
@@ -508,39 +512,50 @@ __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T n
     if (ez(i)) jz += T(ez(i)) * f[i];
   }
   const T rho = k.ref + drho;
-  ux = (jx + T(0.5) * k.Fx) / rho;
-  uy = (jy + T(0.5) * k.Fy) / rho;
-  uz = (jz + T(0.5) * k.Fz) / rho;
+  const T irho = T(1) / rho;
+  ux = FORCE ? (jx + T(0.5) * k.Fx) * irho : jx * irho;
+  uy = FORCE ? (jy + T(0.5) * k.Fy) * irho : jy * irho;
+  uz = FORCE ? (jz + T(0.5) * k.Fz) * irho : jz * irho;
   const T uu = ux * ux + uy * uy + uz * uz;
-  const T uF = ux * k.Fx + uy * k.Fy + uz * k.Fz;
+  const T uF = FORCE ? ux * k.Fx + uy * k.Fy + uz * k.Fz : T(0);
+  const T om_p = k.om, om_m = COLL == MK_COLL_TRT ? k.om_m : k.om;
+  const T gp = T(1) - T(0.5) * om_p, gm = T(1) - T(0.5) * om_m;
   const T B = ns > T(0) ? ns * half / ((T(1) - ns) + half) : T(0);
-  T feq[Q], Fi[Q], P[Q];
+  // lanes past the row end or on walls have returned: vote among the active
+  // lanes only (a lane with B > 0 always votes itself in)
+  const bool psm = __any_sync(__activemask(), B > T(0));
+  const T base = drho - T(1.5) * rho * uu;  // symmetric equilibrium part / w, less the 4.5 eu^2 term
+  {
+    const T w = T(wq<Q>(0));
+    T fc = f[0] - om_p * (f[0] - w * base);
+    if (FORCE) fc += gp * w * T(-3) * uF;
+    if (psm) fc += B * (f[0] - rho * w * T(-1.5) * uu - fc);
+    f[0] = fc;
+  }
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
+  for (int i = 1; i < Q; i += 2) {
+    const int j = i + 1;
     const T w = T(wq<Q>(i));
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
-    const T eF = T(ex(i)) * k.Fx + T(ey(i)) * k.Fy + T(ez(i)) * k.Fz;
-    P[i] = T(-3) * eu + T(4.5) * eu * eu - T(1.5) * uu;
-    feq[i] = w * (drho + rho * (T(3) * eu + T(4.5) * eu * eu - T(1.5) * uu));
-    Fi[i] = w * (T(3) * eF + T(9) * eu * eF - T(3) * uF);
-  }
-  T fo[Q];
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const int j = inv(i);
-    T fc;
-    if constexpr (COLL == MK_COLL_TRT) {
-      const T fp = T(0.5) * (f[i] + f[j]), fm = T(0.5) * (f[i] - f[j]);
-      const T ep = T(0.5) * (feq[i] + feq[j]), em = T(0.5) * (feq[i] - feq[j]);
-      const T Fp = T(0.5) * (Fi[i] + Fi[j]), Fm = T(0.5) * (Fi[i] - Fi[j]);
-      fc = f[i] - k.om * (fp - ep) - k.om_m * (fm - em) + (T(1) - T(0.5) * k.om) * Fp + (T(1) - T(0.5) * k.om_m) * Fm;
-    } else {
-      fc = f[i] - k.om * (f[i] - feq[i]) + (T(1) - T(0.5) * k.om) * Fi[i];
+    const T fp = T(0.5) * (f[i] + f[j]), fm = T(0.5) * (f[i] - f[j]);
+    const T ep = w * (base + T(4.5) * rho * eu * eu), em = w * T(3) * rho * eu;
+    T dp = -om_p * (fp - ep), dm = -om_m * (fm - em);
+    if (FORCE) {
+      const T eF = T(ex(i)) * k.Fx + T(ey(i)) * k.Fy + T(ez(i)) * k.Fz;
+      dp += gp * w * (T(9) * eu * eF - T(3) * uF);
+      dm += gm * w * T(3) * eF;
     }
-    fo[i] = fc + B * (f[j] - rho * T(wq<Q>(i)) * P[i] - fc);
+    T ci = f[i] + dp + dm, cj = f[j] + dp - dm;
+    if (psm) {
+      const T q = T(4.5) * eu * eu - T(1.5) * uu;
+      const T gi = f[j] - rho * w * (q - T(3) * eu);
+      const T gj = f[i] - rho * w * (q + T(3) * eu);
+      ci += B * (gi - ci);
+      cj += B * (gj - cj);
+    }
+    f[i] = ci;
+    f[j] = cj;
   }
-#pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = fo[i];
 }
 
 // Flow lattice of one cell: collision with the porous bounce-back of the
@@ -550,7 +565,7 @@ __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T n
 // cell alone in the AA layout, and no store has happened yet).  The
 // collision velocity goes to vel[3][ncell] for the thermal lattice and the
 // boundary pass.
-template <class S, class P, int Q, int COLL, int PARITY, class NB>
+template <class S, class P, int Q, int COLL, int PARITY, bool FORCE, class NB>
 __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restrict__ phi_old, P* __restrict__ vel,
                                              const int64_t stride, const int64_t ncell, const NB& nb, const int c,
                                              const FdK<typename Stor<S>::T>& k) {
@@ -577,7 +592,7 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
       }
     }
   } else {
-    fd_relax<T, Q, COLL>(f, k.f, ns, k.half, ux, uy, uz);
+    fd_relax<T, Q, COLL, FORCE>(f, k.f, ns, k.half, ux, uy, uz);
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) st_out<S, Q>(W, stride, nb, PARITY, c, i, f[i]);
@@ -586,7 +601,7 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
   vel[2 * ncell + c] = P(uz);
 }
 
-template <class S, class P, int Q, int COLL, int PARITY>
+template <class S, class P, int Q, int COLL, int PARITY, bool FORCE>
 __global__ void __launch_bounds__(256)
     k_fd_flow(S* __restrict__ W, const P* __restrict__ phi_old, P* __restrict__ vel, const Geom g,
               const FdK<typename Stor<S>::T> k) {
@@ -597,10 +612,10 @@ __global__ void __launch_bounds__(256)
   const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
   if (fastw_cell(g, x, y, z)) {
     const FastW fa = make_fastw(g, x, y, z);
-    fd_flow_cell<S, P, Q, COLL, PARITY>(W, phi_old, vel, g.stride, ncell, fa, fa.c, k);
+    fd_flow_cell<S, P, Q, COLL, PARITY, FORCE>(W, phi_old, vel, g.stride, ncell, fa, fa.c, k);
   } else {
     const Nbr nb(g, x, y, z);
-    fd_flow_cell<S, P, Q, COLL, PARITY>(W, phi_old, vel, g.stride, ncell, nb, nb.idx(0, 0, 0), k);
+    fd_flow_cell<S, P, Q, COLL, PARITY, FORCE>(W, phi_old, vel, g.stride, ncell, nb, nb.idx(0, 0, 0), k);
   }
 }
 
@@ -1377,10 +1392,14 @@ void launch_fd_flow(mke::Engine& e, int parity, dim3 grid, dim3 block) {
   const Geom g = make_geom(e);
   const FdK<T> k = fd_coef<T>(e.p, refs_of(e.p));
   const P* phi_old = (const P*)e.phi[e.phi_cur];
+  const bool force = e.p.force[0] != 0.0 || e.p.force[1] != 0.0 || e.p.force[2] != 0.0;
+#define MK_FDF(PAR, FRC) \
+  k_fd_flow<S, P, Q, COLL, PAR, FRC><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k)
   if (parity == 0)
-    k_fd_flow<S, P, Q, COLL, 0><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k);
+    force ? MK_FDF(0, true) : MK_FDF(0, false);
   else
-    k_fd_flow<S, P, Q, COLL, 1><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k);
+    force ? MK_FDF(1, true) : MK_FDF(1, false);
+#undef MK_FDF
 }
 
 // Flow + dendrite loop: phi of the streamed phase field, the fused flow /
