@@ -156,14 +156,23 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T
 // the cell's domain, 9 values per grain.  ADV = true advects the thermal
 // equilibrium with the flow velocity (vx, vy, vz): t_eq = w T (1 + 4 e.u)
 // (mkThermalField::relaxation with a flow lattice, getTEquPDFs).
-template <class S, class P, int PARITY, bool SOL, bool GEN, class NB, bool ADV = false>
+// NEE = true (with ADV, thermal only) also applies the inflow / outflow faces
+// of the flow + dendrite model in registers: the cell at x = 0 (x = nx - 1)
+// takes the post-collision g, t of its inner neighbour — the next (previous)
+// lane of its warp, so nx % 32 != 1 and the row starts a warp — by shuffles:
+//   g(b) = g(n) + w (phi_b - phi_n),
+//   t(b) = t(n) + w T_b (1 + 4 e.u_b) - w T_n (1 + 4 e.u_n),
+// inflow phi_b = -1, T_b = ref_t; outflow phi_b = phi_n, T_b = T_n; u_b is
+// the face cell's own (vx, vy, vz), u_n the neighbour's; temp(b) = T_b.
+template <class S, class P, int PARITY, bool SOL, bool GEN, class NB, bool ADV = false, bool NEE = false>
 __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
                                           const P* __restrict__ phi_old, P* __restrict__ temp,
                                           const unsigned char* __restrict__ grain,
                                           const typename Stor<S>::T* __restrict__ rot, const int64_t stride,
                                           const NB& nb, const int c, const DendK<typename Stor<S>::T>& k,
                                           typename Stor<S>::T vx = 0, typename Stor<S>::T vy = 0,
-                                          typename Stor<S>::T vz = 0) {
+                                          typename Stor<S>::T vz = 0, int x = 0, int nx = 0) {
+  static_assert(!NEE || (ADV && !SOL), "the face pass belongs to the advected thermal lattice");
   typedef typename Stor<S>::T T;
   const T ph = T(phi_new[c]);
   T gx = T(0), gy = T(0), gz = T(0);
@@ -198,7 +207,10 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
     const T w = T(wq<7>(i));
     const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
     const T go = gv[i] - k.om_g * (gv[i] - w * dph) + fo * w * eB + w * src;
-    st_out<S, 7>(G, stride, nb, PARITY, c, i, go);
+    if constexpr (NEE)
+      gv[i] = go;  // stored after the face pass below
+    else
+      st_out<S, 7>(G, stride, nb, PARITY, c, i, go);
   }
   T t[7];
   T dT = T(0);
@@ -247,10 +259,50 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
         if (i > 0) eq += T(4) * (k.ref_t + dT) * eu;
       }
       const T to = t[i] - k.om_t * (t[i] - w * eq) + w * lat;
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
+      if constexpr (NEE)
+        t[i] = to;
+      else
+        st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
     }
   }
-  temp[c] = P(k.ref_t + dT);
+  T Tc = k.ref_t + dT;
+  if constexpr (NEE && !SOL) {
+    const unsigned act = __activemask();
+    const bool edge = x == 0 || x == nx - 1;
+    if (__any_sync(act, edge)) {
+      const int lane = threadIdx.x & 31;
+      const int src = x == 0 ? lane + 1 : lane - 1;
+      T sg = T(0), st = T(0);
+#pragma unroll
+      for (int i = 0; i < 7; ++i) {
+        sg += gv[i];
+        st += t[i];
+      }
+      sg = __shfl_sync(act, sg, src);
+      st = __shfl_sync(act, st, src);
+      const T un0 = __shfl_sync(act, vx, src), un1 = __shfl_sync(act, vy, src), un2 = __shfl_sync(act, vz, src);
+      const T phn = k.ref_g + sg, Tn = k.ref_t + st;
+      const T phb = x == 0 ? T(-1) : phn, Tb = x == 0 ? k.ref_t : Tn;
+#pragma unroll
+      for (int i = 0; i < 7; ++i) {
+        const T gn = __shfl_sync(act, gv[i], src), tn = __shfl_sync(act, t[i], src);
+        if (edge) {
+          const T w = T(wq<7>(i));
+          const T evn = T(ex(i)) * un0 + T(ey(i)) * un1 + T(ez(i)) * un2;
+          const T evb = T(ex(i)) * vx + T(ey(i)) * vy + T(ez(i)) * vz;
+          gv[i] = gn + w * (phb - phn);
+          t[i] = tn + w * (Tb * (T(1) + T(4) * evb) - Tn * (T(1) + T(4) * evn));
+        }
+      }
+      if (edge) Tc = Tb;
+    }
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      st_out<S, 7>(G, stride, nb, PARITY, c, i, gv[i]);
+      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, t[i]);
+    }
+  }
+  temp[c] = P(Tc);
 }
 
 template <class S, class P, int PARITY, bool SOL, bool GEN>

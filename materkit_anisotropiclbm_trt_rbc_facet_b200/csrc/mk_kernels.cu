@@ -565,10 +565,10 @@ __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T n
 // cell alone in the AA layout, and no store has happened yet).  The
 // collision velocity goes to vel[3][ncell] for the thermal lattice and the
 // boundary pass.
-template <class S, class P, int Q, int COLL, int PARITY, bool FORCE, class NB>
+template <class S, class P, int Q, int COLL, int PARITY, bool FORCE, bool NEE, class NB>
 __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restrict__ phi_old, P* __restrict__ vel,
                                              const int64_t stride, const int64_t ncell, const NB& nb, const int c,
-                                             const FdK<typename Stor<S>::T>& k) {
+                                             const int x, const int nx, const FdK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
   T f[Q];  // deviations f_i - w_i rho0, post-collision after the relaxation
 #pragma unroll
@@ -594,6 +594,56 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
   } else {
     fd_relax<T, Q, COLL, FORCE>(f, k.f, ns, k.half, ux, uy, uz);
   }
+  if constexpr (NEE) {
+    // inflow / outflow faces in registers: the cell at x = 0 (x = nx - 1)
+    // takes the post-collision populations of its inner neighbour, the next
+    // (previous) lane of its warp, f(b) = f(n) + feq(rho_b, u_b) - feq(rho_n, u_n),
+    // inflow u_b = u0, rho_b = rho_n; outflow rho_b = rho0, u_b = u_n; the face
+    // cell's velocity becomes u_b
+    const unsigned act = __activemask();
+    const bool edge = x == 0 || x == nx - 1;
+    if (__any_sync(act, edge)) {
+      const int lane = threadIdx.x & 31;
+      const int src = x == 0 ? lane + 1 : lane - 1;
+      // every lane sums its own post-collision moments; the face lanes take
+      // their neighbour's four sums, then its populations one by one
+      T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        drho += f[i];
+        if (ex(i)) jx += T(ex(i)) * f[i];
+        if (ey(i)) jy += T(ey(i)) * f[i];
+        if (ez(i)) jz += T(ez(i)) * f[i];
+      }
+      drho = __shfl_sync(act, drho, src);
+      jx = __shfl_sync(act, jx, src);
+      jy = __shfl_sync(act, jy, src);
+      jz = __shfl_sync(act, jz, src);
+      const T rn = k.f.ref + drho;
+      const T un[3] = {jx / rn, jy / rn, jz / rn};
+      const bool in = x == 0;
+      const T ub[3] = {in ? k.u0[0] : un[0], in ? k.u0[1] : un[1], in ? k.u0[2] : un[2]};
+      const T rb = in ? rn : k.f.ref;
+      const T uun = un[0] * un[0] + un[1] * un[1] + un[2] * un[2];
+      const T uub = ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        const T v = __shfl_sync(act, f[i], src);
+        if (edge) {
+          const T w = T(wq<Q>(i));
+          const T eun = T(ex(i)) * un[0] + T(ey(i)) * un[1] + T(ez(i)) * un[2];
+          const T eub = T(ex(i)) * ub[0] + T(ey(i)) * ub[1] + T(ez(i)) * ub[2];
+          f[i] = v + w * ((rb - rn) + rb * (T(3) * eub + T(4.5) * eub * eub - T(1.5) * uub) -
+                          rn * (T(3) * eun + T(4.5) * eun * eun - T(1.5) * uun));
+        }
+      }
+      if (edge) {
+        ux = ub[0];
+        uy = ub[1];
+        uz = ub[2];
+      }
+    }
+  }
 #pragma unroll
   for (int i = 0; i < Q; ++i) st_out<S, Q>(W, stride, nb, PARITY, c, i, f[i]);
   vel[c] = P(ux);
@@ -601,7 +651,7 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
   vel[2 * ncell + c] = P(uz);
 }
 
-template <class S, class P, int Q, int COLL, int PARITY, bool FORCE>
+template <class S, class P, int Q, int COLL, int PARITY, bool FORCE, bool NEE>
 __global__ void __launch_bounds__(256)
     k_fd_flow(S* __restrict__ W, const P* __restrict__ phi_old, P* __restrict__ vel, const Geom g,
               const FdK<typename Stor<S>::T> k) {
@@ -612,16 +662,17 @@ __global__ void __launch_bounds__(256)
   const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
   if (fastw_cell(g, x, y, z)) {
     const FastW fa = make_fastw(g, x, y, z);
-    fd_flow_cell<S, P, Q, COLL, PARITY, FORCE>(W, phi_old, vel, g.stride, ncell, fa, fa.c, k);
+    fd_flow_cell<S, P, Q, COLL, PARITY, FORCE, NEE>(W, phi_old, vel, g.stride, ncell, fa, fa.c, x, g.nx, k);
   } else {
     const Nbr nb(g, x, y, z);
-    fd_flow_cell<S, P, Q, COLL, PARITY, FORCE>(W, phi_old, vel, g.stride, ncell, nb, nb.idx(0, 0, 0), k);
+    fd_flow_cell<S, P, Q, COLL, PARITY, FORCE, NEE>(W, phi_old, vel, g.stride, ncell, nb, nb.idx(0, 0, 0), x, g.nx,
+                                                    k);
   }
 }
 
 // Phase field and thermal lattice with the equilibrium advected by the
 // loop's flow velocity.
-template <class S, class P, int PARITY, bool GEN>
+template <class S, class P, int PARITY, bool GEN, bool NEE>
 __global__ void __launch_bounds__(256)
     k_fd_dend(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
               P* __restrict__ temp, const P* __restrict__ vel, const unsigned char* __restrict__ grain,
@@ -635,13 +686,14 @@ __global__ void __launch_bounds__(256)
   if (fastw_cell(g, x, y, z)) {
     const FastW fa = make_fastw(g, x, y, z);
     const int c = fa.c;
-    dend_cell<S, P, PARITY, false, GEN, FastW, true>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, c, k,
-                                                     T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]));
+    dend_cell<S, P, PARITY, false, GEN, FastW, true, NEE>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, c,
+                                                          k, T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]), x,
+                                                          g.nx);
   } else {
     const Nbr nb(g, x, y, z);
     const int c = nb.idx(0, 0, 0);
-    dend_cell<S, P, PARITY, false, GEN, Nbr, true>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, k,
-                                                   T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]));
+    dend_cell<S, P, PARITY, false, GEN, Nbr, true, NEE>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, k,
+                                                        T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]), x, g.nx);
   }
 }
 
@@ -1385,6 +1437,12 @@ FdK<T> fd_coef(const mk_params& p, Refs r) {
   return k;
 }
 
+// Whether the inflow / outflow faces are applied in registers by the flow and
+// phase-field kernels (warp shuffles between a face cell and its inner
+// neighbour, which share a warp unless x = nx - 1 starts one) rather than by
+// the separate boundary kernel.
+bool fd_faces_in_warp(const mke::Engine& e) { return e.p.inlet && e.nx % 32 != 1; }
+
 template <class S, int Q, int COLL>
 void launch_fd_flow(mke::Engine& e, int parity, dim3 grid, dim3 block) {
   typedef typename Stor<S>::T T;
@@ -1393,17 +1451,22 @@ void launch_fd_flow(mke::Engine& e, int parity, dim3 grid, dim3 block) {
   const FdK<T> k = fd_coef<T>(e.p, refs_of(e.p));
   const P* phi_old = (const P*)e.phi[e.phi_cur];
   const bool force = e.p.force[0] != 0.0 || e.p.force[1] != 0.0 || e.p.force[2] != 0.0;
-#define MK_FDF(PAR, FRC) \
-  k_fd_flow<S, P, Q, COLL, PAR, FRC><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k)
+  const bool nee = fd_faces_in_warp(e);
+#define MK_FDF(PAR, FRC, NEE) \
+  k_fd_flow<S, P, Q, COLL, PAR, FRC, NEE><<<grid, block, 0, e.stream>>>((S*)e.pop2, phi_old, (P*)e.vel, g, k)
+#define MK_FDF2(PAR, FRC) nee ? MK_FDF(PAR, FRC, true) : MK_FDF(PAR, FRC, false)
   if (parity == 0)
-    force ? MK_FDF(0, true) : MK_FDF(0, false);
+    force ? MK_FDF2(0, true) : MK_FDF2(0, false);
   else
-    force ? MK_FDF(1, true) : MK_FDF(1, false);
+    force ? MK_FDF2(1, true) : MK_FDF2(1, false);
+#undef MK_FDF2
 #undef MK_FDF
 }
 
-// Flow + dendrite loop: phi of the streamed phase field, the fused flow /
-// phase-field / thermal collision, then the inflow/outflow faces.
+// Flow + dendrite loop: phi of the streamed phase field, the flow lattice,
+// the phase field with the advected thermal lattice, and the inflow/outflow
+// faces (in the two collision kernels, or a separate kernel when a face cell
+// and its inner neighbour can fall in different warps).
 template <class S>
 void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
   typedef typename Stor<S>::T T;
@@ -1444,17 +1507,20 @@ void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
     const DendK<T> kd = dend_coef<T>(e.p, r);
     const bool gen = e.p.aniso != MK_ANISO_CUBIC;
     const P* vel = (const P*)e.vel;
-#define MK_FDD(PAR, GEN)                                                                                      \
-  k_fd_dend<S, P, PAR, GEN><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, vel, \
-                                                          e.grain, (const T*)e.rot, g, kd)
+    const bool nee = fd_faces_in_warp(e);
+#define MK_FDD(PAR, GEN, NEE)                                                                                      \
+  k_fd_dend<S, P, PAR, GEN, NEE><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, vel, \
+                                                               e.grain, (const T*)e.rot, g, kd)
+#define MK_FDD2(PAR, GEN) nee ? MK_FDD(PAR, GEN, true) : MK_FDD(PAR, GEN, false)
     if (parity == 0)
-      gen ? MK_FDD(0, true) : MK_FDD(0, false);
+      gen ? MK_FDD2(0, true) : MK_FDD2(0, false);
     else
-      gen ? MK_FDD(1, true) : MK_FDD(1, false);
+      gen ? MK_FDD2(1, true) : MK_FDD2(1, false);
+#undef MK_FDD2
 #undef MK_FDD
   }
   if (ev) cudaEventRecord(ev[5], e.stream);
-  if (e.p.inlet) {
+  if (e.p.inlet && !fd_faces_in_warp(e)) {
     if (ev) cudaEventRecord(ev[6], e.stream);
     const FdK<T> k = fd_coef<T>(e.p, r);
     const int nt = 2 * e.ny * e.nz;
@@ -1496,7 +1562,7 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
     case MK_MODEL_FLOW_DENDRITE:
       launch_fd<S>(e, parity, grid, block, ev);
       e.phi_cur = 1 - e.phi_cur;
-      e.launches += e.p.inlet ? 4 : 3;
+      e.launches += (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
       break;
     default:
       launch_dend<S>(e, parity, grid, block, ev);
@@ -1887,7 +1953,7 @@ cudaError_t engine_step(Engine& e, cudaEvent_t* ev) {
 static bool one_kernel(const Engine& e) { return e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION; }
 
 int engine_kernels_per_step(const Engine& e) {
-  if (e.p.model == MK_MODEL_FLOW_DENDRITE) return e.p.inlet ? 4 : 3;
+  if (e.p.model == MK_MODEL_FLOW_DENDRITE) return (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
   return one_kernel(e) ? 1 : 2;
 }
 

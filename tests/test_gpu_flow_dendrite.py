@@ -53,6 +53,19 @@ def test_flow_dendrite_fp64_steps(casedir, coll, lat, inlet):
     assert (s.field("flag") == A.MK_FLAG_SOLID).sum() > 100
 
 
+def test_flow_dendrite_separate_boundary_kernel_fp64(casedir):
+    # nx = 33: the outflow face cell starts a warp, so the faces are applied by
+    # the separate boundary kernel instead of in the collision kernels
+    p, s, o = _pair(casedir, "fd_nx33", cases.flow_dendrite(nx=33, ny=10, nz=9, radius=3.0, u_in=0.03,
+                                                             center=(10.0, 4.5, 4.0), precision="fp64"))
+    assert s.launches_per_step() == 4
+    for n in (1, 1, 1, 20):
+        s.advance(n)
+        o.advance(n)
+        e = _errs(s, o)
+        assert max(e.values()) <= FP64_TOL, (s.step, e)
+
+
 def test_flow_dendrite_fp32(casedir):
     p, s, o = _pair(casedir, "fd32", _case("fp32"))
     s.advance(60)
@@ -73,8 +86,8 @@ def test_flow_dendrite_16bit(casedir, prec, tol):
 def test_flow_dendrite_launches_graph_and_checkpoint(casedir, tmp_path):
     p = case_params(cases.write(_case("fp32"), f"{casedir}/fd_ck.xml"))
     a, b = Solver(params=p), Solver(params=p)
-    assert a.launches_per_step() == 4  # phi, flow, phase field + thermal, boundary
-    prof = a.profile(4, "boundary")
+    assert a.launches_per_step() == 3  # phi, flow (+ faces), phase field + thermal (+ faces)
+    prof = a.profile(4, "collide")
     assert prof["kernel_ms"] > 0
     b.advance(4)
     a.advance(7, graph=True)
