@@ -119,24 +119,37 @@ class mkSolver {
 };
 
 // Flow and dendrite solver (MaterKit/inc/mkFluidsMRT.h).  The model comes from
-// initialize(xml, model): MK_MODEL_FLOW (run_flow_Poiseuille) or
-// MK_MODEL_THERMAL_DENDRITE (run_thermal_dendrite).
+// initialize(xml, model): MK_MODEL_FLOW (run_flow_Poiseuille),
+// MK_MODEL_THERMAL_DENDRITE (run_thermal_dendrite) or MK_MODEL_FLOW_DENDRITE
+// (run_flow_thermal_dendrite).
 class mkFluidsMRT : public mkSolver {
  public:
   explicit mkFluidsMRT(const mkSpace& s) : mkSolver(s, MK_MODEL_FLOW) {}
   void initialize_geometry_Poiseuille() { initialize_geometry(); }
   // mkFluidsLBM::propagate / relaxation (MaterKit.cpp:277-280)
-  void propagate() { call("propagate", {"propagate", "relaxation"}); }
-  void relaxation() { call("relaxation", {"propagate", "relaxation"}); }
+  void propagate() { call("propagate", seq()); }
+  void relaxation() { call("relaxation", seq()); }
   // mkPhaseField::propagate / relaxation_anisotropy_thermal, mkThermalField::propagate /
   // relaxation (MaterKit.cpp:775-781)
-  void phasefield_propagate() { call("pf_propagate", dendrite_seq()); }
-  void relaxation_anisotropy_thermal() { call("pf_relax", dendrite_seq()); }
-  void thermal_propagate() { call("t_propagate", dendrite_seq()); }
-  void thermal_relaxation() { call("t_relax", dendrite_seq()); }
+  void phasefield_propagate() { call("pf_propagate", seq()); }
+  void relaxation_anisotropy_thermal() { call("pf_relax", seq()); }
+  void thermal_propagate() { call("t_propagate", seq()); }
+  void thermal_relaxation() { call("t_relax", seq()); }
+  // mkFluidsMRT::propagate_PBB, bdyVelocity, mkThermalField::bdy_flowin
+  // (MaterKit.cpp:499-516)
+  void propagate_PBB() { call("propagate_PBB", seq()); }
+  void bdyVelocity() { call("bdyVelocity", seq()); }
+  void bdy_flowin() { call("bdy_flowin", seq()); }
 
  private:
-  static std::vector<std::string> dendrite_seq() { return {"pf_propagate", "pf_relax", "t_propagate", "t_relax"}; }
+  std::vector<std::string> seq() const {
+    if (model_ == MK_MODEL_FLOW_DENDRITE)
+      return {"propagate_PBB", "relaxation", "bdyVelocity", "pf_propagate", "pf_relax", "t_propagate", "t_relax",
+              "bdy_flowin"};
+    if (model_ == MK_MODEL_THERMAL_DENDRITE || model_ == MK_MODEL_SOLUTAL_DENDRITE)
+      return {"pf_propagate", "pf_relax", "t_propagate", "t_relax"};
+    return {"propagate", "relaxation"};
+  }
 };
 
 // Two-phase Allen-Cahn flow (MaterKit/inc/mkFluidsMultiphase.h), run_flow_multiphase

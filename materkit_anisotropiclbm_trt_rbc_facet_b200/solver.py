@@ -440,6 +440,10 @@ class mkFluidsMRT(_RefSolver):
         A.MK_MODEL_FLOW: ["propagate", "relaxation"],
         A.MK_MODEL_THERMAL_DENDRITE: ["phasefield_propagate", "relaxation_anisotropy_thermal",
                                       "thermal_propagate", "thermal_relaxation"],
+        # run_flow_thermal_dendrite (MaterKit.cpp:499-516)
+        A.MK_MODEL_FLOW_DENDRITE: ["propagate_PBB", "relaxation", "bdyVelocity", "phasefield_propagate",
+                                   "relaxation_anisotropy_thermal", "thermal_propagate", "thermal_relaxation",
+                                   "bdy_flowin"],
     }
 
     def initialize_geometry_Poiseuille(self) -> None:
@@ -450,6 +454,15 @@ class mkFluidsMRT(_RefSolver):
 
     def relaxation(self) -> None:
         self._call("relaxation")
+
+    def propagate_PBB(self) -> None:
+        self._call("propagate_PBB")
+
+    def bdyVelocity(self) -> None:
+        self._call("bdyVelocity")
+
+    def bdy_flowin(self) -> None:
+        self._call("bdy_flowin")
 
     # mkPhaseField / mkThermalField members, called as flow.mkPhaseField::propagate() in C++
     def phasefield_propagate(self) -> None:

@@ -111,3 +111,29 @@ def test_flow_dendrite_closed_faces_conserve_mass(casedir):
     m0 = s.diagnostics()["mass"]
     s.advance(50)
     assert abs(s.diagnostics()["mass"] - m0) / m0 < 1e-12
+
+
+def test_reference_call_sequence(casedir):
+    # run_flow_thermal_dendrite's per-loop calls (MaterKit.cpp:499-516) drive
+    # the same device loop as Solver.advance; a call out of order is refused
+    from materkit_anisotropiclbm_trt_rbc_facet_b200.solver import mkFluidsMRT, mkSpace
+    xml = cases.write(_case("fp32"), f"{casedir}/fd_seq.xml")
+    flow = mkFluidsMRT(mkSpace(xml), precision="fp32")
+    flow.initialize(xml, model=A.MK_MODEL_FLOW_DENDRITE)
+    flow.initialize_geometry()
+    for _ in range(3):
+        flow.propagate_PBB()
+        flow.relaxation()
+        flow.bdyVelocity()
+        flow.phasefield_propagate()
+        flow.relaxation_anisotropy_thermal()
+        flow.thermal_propagate()
+        flow.thermal_relaxation()
+        flow.bdy_flowin()
+    ref = Solver(params=case_params(xml, precision="fp32"))
+    ref.advance(3)
+    assert flow.solver.step == 3
+    for f in ["phi", "T", "ux", "rho"]:
+        assert np.array_equal(flow.solver.field(f), ref.field(f))
+    with pytest.raises(A.MkError):
+        flow.thermal_propagate()
