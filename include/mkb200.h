@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define MKB200_ABI_VERSION 1
+#define MKB200_ABI_VERSION 2
 
 /* Status codes.  Replace the exception family of
  * MaterKit/inc/mkRunTimeDiagnostics.h:59-117 (mkIOError, mkMemoryError, ...). */
@@ -63,9 +63,14 @@ typedef enum mk_model {
   MK_MODEL_CONVECTION = 4,       /* flow + advected D3Q7 scalar with Boussinesq buoyancy and
                                     Dirichlet plates: Rayleigh-Benard (bdy_RBC, Thermal_NusseltRBC,
                                     mkThermalField.h:33-40, mkFluidsLBM.h:59-68)                  */
-  MK_MODEL_FLOW_DENDRITE = 5     /* thermal dendrite growing in a flow: porous bounce-back of the
+  MK_MODEL_FLOW_DENDRITE = 5,    /* thermal dendrite growing in a flow: porous bounce-back of the
                                     flow by the solid fraction, thermal lattice advected, inflow /
                                     outflow faces, run_flow_thermal_dendrite (MaterKit.cpp:467-527) */
+  MK_MODEL_MULTIGRAIN = 6        /* one conservative Allen-Cahn order parameter per seed (grain) with
+                                    a pairwise overlap penalty, aggregate phi = (N - 1) + sum phi_j,
+                                    thermal ADE with latent heat: run_multiPhaseField
+                                    (MaterKit.cpp:529-571), mkFluidsUser::propagate/relaxation
+                                    (mkFluidsUser.cpp:68-299), mkMultiphaseField.h:24-60             */
 } mk_model;
 
 /* Population storage precision.  Collision arithmetic is FP64 for MK_PREC_FP64
@@ -190,6 +195,11 @@ typedef struct mk_params {
   double wall_u[2][3];  /* velocity of the low / high plate (flow) */
   double beta;          /* Boussinesq expansion coefficient: F = -rho0 beta (s - s_ref) g, g = force */
   double s_ref;         /* reference value of the scalar in the buoyancy */
+
+  /* multigrain: strength of the pairwise overlap penalty of grains 1..N-1
+   * (grain 0 has none, mkFluidsUser.cpp:233-251); the mobility is `mobility`,
+   * the interface width `W0` */
+  double grain_kappa;
 } mk_params;
 
 /* Optional overrides at creation; a negative value keeps the XML/default. */
@@ -274,6 +284,9 @@ mk_status mk_get_stream(mk_handle* h, void** stream);
 
 /* Copy a macroscopic field to host memory (synchronous). */
 mk_status mk_get_field(mk_handle* h, int32_t field, int32_t dtype, void* host_dst, size_t bytes);
+/* Multigrain: the order parameter of grain `grain` (phiVec[grain] of the
+ * reference's node, mkFluidsUser.cpp:147-160), as mk_get_field. */
+mk_status mk_get_grain_field(mk_handle* h, int32_t grain, int32_t dtype, void* host_dst, size_t bytes);
 /* Replace the state by the equilibrium of host-provided macroscopic fields
  * (phi, and rho/u/T/C where the model has them).  Any pointer may be NULL to
  * keep the case's initial field.  Resets the step counter to 0. */

@@ -120,8 +120,8 @@ class mkSolver {
 
 // Flow and dendrite solver (MaterKit/inc/mkFluidsMRT.h).  The model comes from
 // initialize(xml, model): MK_MODEL_FLOW (run_flow_Poiseuille),
-// MK_MODEL_THERMAL_DENDRITE (run_thermal_dendrite) or MK_MODEL_FLOW_DENDRITE
-// (run_flow_thermal_dendrite).
+// MK_MODEL_THERMAL_DENDRITE (run_thermal_dendrite), MK_MODEL_FLOW_DENDRITE
+// (run_flow_thermal_dendrite) or MK_MODEL_MULTIGRAIN (run_multiPhaseField).
 class mkFluidsMRT : public mkSolver {
  public:
   explicit mkFluidsMRT(const mkSpace& s) : mkSolver(s, MK_MODEL_FLOW) {}
@@ -148,6 +148,8 @@ class mkFluidsMRT : public mkSolver {
               "bdy_flowin"};
     if (model_ == MK_MODEL_THERMAL_DENDRITE || model_ == MK_MODEL_SOLUTAL_DENDRITE)
       return {"pf_propagate", "pf_relax", "t_propagate", "t_relax"};
+    if (model_ == MK_MODEL_MULTIGRAIN)  // run_multiPhaseField (MaterKit.cpp:563-567)
+      return {"propagate", "relaxation", "t_propagate", "t_relax"};
     return {"propagate", "relaxation"};
   }
 };

@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "MK_OK", 1: "MK_ERR_XML", 2: "MK_ERR_ARG", 3: "MK_ERR_CUDA", 
                 5: "MK_ERR_TIMEOUT", 6: "MK_ERR_OOM", 7: "MK_ERR_IO", 8: "MK_ERR_STATE", 9: "MK_ERR_NODEVICE"}
 
 (MK_MODEL_FLOW, MK_MODEL_MULTIPHASE, MK_MODEL_THERMAL_DENDRITE, MK_MODEL_SOLUTAL_DENDRITE, MK_MODEL_CONVECTION,
- MK_MODEL_FLOW_DENDRITE) = range(6)
+ MK_MODEL_FLOW_DENDRITE, MK_MODEL_MULTIGRAIN) = range(7)
 MK_PREC_FP64, MK_PREC_FP32, MK_PREC_FP16, MK_PREC_BF16 = range(4)
 MK_COLL_BGK, MK_COLL_TRT, MK_COLL_MRT = range(3)
 MK_D3Q7, MK_D3Q19, MK_D3Q27 = 7, 19, 27
@@ -34,7 +34,7 @@ MK_NOALLOC_MAX_CELLS = 2048 * 256 * 64
 PRECISIONS = {"fp64": MK_PREC_FP64, "fp32": MK_PREC_FP32, "fp16": MK_PREC_FP16, "bf16": MK_PREC_BF16}
 MODELS = {"flow": MK_MODEL_FLOW, "multiphase": MK_MODEL_MULTIPHASE, "thermal_dendrite": MK_MODEL_THERMAL_DENDRITE,
           "solutal_dendrite": MK_MODEL_SOLUTAL_DENDRITE, "convection": MK_MODEL_CONVECTION,
-          "flow_dendrite": MK_MODEL_FLOW_DENDRITE}
+          "flow_dendrite": MK_MODEL_FLOW_DENDRITE, "multigrain": MK_MODEL_MULTIGRAIN}
 FIELDS = {"rho": MK_FIELD_RHO, "ux": MK_FIELD_UX, "uy": MK_FIELD_UY, "uz": MK_FIELD_UZ, "T": MK_FIELD_T,
           "C": MK_FIELD_C, "phi": MK_FIELD_PHI, "flag": MK_FIELD_FLAG, "pressure": MK_FIELD_PRESSURE,
           "dphi": MK_FIELD_DPHI, "grain": MK_FIELD_GRAIN}
@@ -58,6 +58,7 @@ class MkParams(C.Structure):
         ("eps2", C.c_double),
         ("wall_axis", C.c_int32), ("inlet", C.c_int32), ("wall_value", C.c_double * 2),
         ("wall_u", (C.c_double * 3) * 2), ("beta", C.c_double), ("s_ref", C.c_double),
+        ("grain_kappa", C.c_double),
     ]
 
     def ncell(self) -> int:
@@ -132,6 +133,7 @@ PROTOTYPES = {
     "mk_sync": (C.c_int, [H]),
     "mk_get_stream": (C.c_int, [H, P(C.c_void_p)]),
     "mk_get_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),
+    "mk_get_grain_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),
     "mk_set_state": (C.c_int, [H] + [P(C.c_double)] * 7),
     "mk_set_state_f32": (C.c_int, [H] + [P(C.c_float)] * 3),
     "mk_write_vtk": (C.c_int, [H, C.c_int64, C.c_char_p]),

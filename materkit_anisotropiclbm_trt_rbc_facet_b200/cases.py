@@ -200,6 +200,37 @@ def flow_dendrite(nx=96, ny=64, nz=64, loops=3000, precision="fp32", u_in=0.02, 
 """
 
 
+def multigrain(n=48, loops=1000, precision="fp32", seeds=None, W0=1.5, mobility=1.0, kappa=1.0, delta=0.3,
+               D=0.1, nz=None, ny=None) -> str:
+    """Multiphase field of grains (run_multiPhaseField): one order parameter
+    per seed; `seeds` is a list of (x, y, z, radius), default two touching
+    grains along x.  Closed faces."""
+    nx = n
+    ny = ny or n
+    nz = nz or n
+    if seeds is None:
+        c = ((ny - 1) / 2.0, (nz - 1) / 2.0)
+        seeds = [(nx / 2.0 - 6.0, c[0], c[1], 7.0), (nx / 2.0 + 6.0, c[0], c[1], 7.0)]
+    centers = " ".join(f"{x} {y} {z}" for x, y, z, _ in seeds)
+    radii = " ".join(str(r) for *_, r in seeds)
+    angles = " ".join("0 0 0" for _ in seeds)
+    return _HEADER.format(dendrite="true", flow="false", loops=loops, frames=min(loops, 100), nx=nx, ny=ny, nz=nz) + f"""
+  <phasechange>
+    <d0> 0.138486 </d0> <lambda> 10.0 </lambda> <anisotropy> 0.0 </anisotropy> <W0> 1.0 </W0> <t0> 1.0 </t0>
+    <seed> <number> {len(seeds)} </number> <center> {centers} </center> <angle> {angles} </angle>
+      <radius> {radii} </radius> </seed>
+  </phasechange>
+  <temperature> <iniValue> {-delta} </iniValue> <undercooling> {delta} </undercooling>
+    <alphaFluid> {D} </alphaFluid> <alphaSolid> {D} </alphaSolid> <beta> 0.0 </beta> </temperature>
+  <b200>
+    <model> multigrain </model> <precision> {precision} </precision> <boundary> closed closed closed </boundary>
+    <W0> {W0} </W0> <mobility> {mobility} </mobility> <grainKappa> {kappa} </grainKappa> <delta> {delta} </delta>
+    <diffusivity> {D} </diffusivity>
+  </b200>
+</MaterKit>
+"""
+
+
 def write(text: str, path: str) -> str:
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
     with open(path, "w") as f:

@@ -144,7 +144,8 @@ mk_status mk_create(const mk_params* p, mk_handle** out) {
   const size_t n = (size_t)h->e.ncell;
   const bool flow = p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION;
   const bool scalar = p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
-                      p->model == MK_MODEL_CONVECTION || p->model == MK_MODEL_FLOW_DENDRITE;
+                      p->model == MK_MODEL_CONVECTION || p->model == MK_MODEL_FLOW_DENDRITE ||
+                      p->model == MK_MODEL_MULTIGRAIN;
   std::vector<double> phi(flow ? 0 : n), temp(scalar ? n : 0), rho(flow ? n : 0);
   if (!flow) mkc::initial_field(p, MK_FIELD_PHI, phi.data(), n, err);
   if (scalar) mkc::initial_field(p, MK_FIELD_T, temp.data(), n, err);
@@ -281,6 +282,39 @@ mk_status mk_get_field(mk_handle* h, int32_t field, int32_t dtype, void* host_ds
   return MK_OK;
 }
 
+mk_status mk_get_grain_field(mk_handle* h, int32_t grain, int32_t dtype, void* host_dst, size_t bytes) {
+  if (!h || !host_dst) return MK_ERR_ARG;
+  const size_t n = (size_t)h->e.ncell;
+  if (dtype != MK_DTYPE_F64 && dtype != MK_DTYPE_F32) {
+    h->err = "dtype must be MK_DTYPE_F64 or MK_DTYPE_F32";
+    return MK_ERR_ARG;
+  }
+  const size_t need = n * (dtype == MK_DTYPE_F64 ? 8 : 4);
+  if (bytes < need) {
+    h->err = "destination buffer too small";
+    return MK_ERR_ARG;
+  }
+  cudaError_t st = mke::engine_grain_field(h->e, grain);
+  if (st == cudaErrorInvalidValue) {
+    h->err = "not a multigrain case, or grain index out of range";
+    return MK_ERR_ARG;
+  }
+  if (st != cudaSuccess) return cuda_fail(h, st, "grain field");
+  if (dtype == MK_DTYPE_F32) {
+    std::vector<double> tmp(n);
+    st = cudaMemcpyAsync(tmp.data(), h->e.field, n * sizeof(double), cudaMemcpyDeviceToHost, h->e.stream);
+    if (st == cudaSuccess) st = cudaStreamSynchronize(h->e.stream);
+    if (st != cudaSuccess) return cuda_fail(h, st, "grain field copy");
+    float* out = (float*)host_dst;
+    for (size_t c = 0; c < n; ++c) out[c] = (float)tmp[c];
+    return MK_OK;
+  }
+  st = cudaMemcpyAsync(host_dst, h->e.field, need, cudaMemcpyDeviceToHost, h->e.stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(h->e.stream);
+  if (st != cudaSuccess) return cuda_fail(h, st, "grain field copy");
+  return MK_OK;
+}
+
 mk_status mk_set_state(mk_handle* h, const double* phi, const double* temp, const double* conc, const double* rho,
                        const double* ux, const double* uy, const double* uz) {
   if (!h) return MK_ERR_ARG;
@@ -340,7 +374,8 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   if ((s = copy_field(h, MK_FIELD_GRAIN, grain)) != MK_OK) return s;
   if ((s = copy_field(h, MK_FIELD_PHI, phi)) != MK_OK) return s;
   if (m == MK_MODEL_CONVECTION && (s = copy_field(h, MK_FIELD_T, temp)) != MK_OK) return s;
-  if (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE) {
+  if (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE ||
+      m == MK_MODEL_MULTIGRAIN) {
     const bool th = m != MK_MODEL_SOLUTAL_DENDRITE;
     if ((s = copy_field(h, MK_FIELD_DPHI, dphi)) != MK_OK) return s;
     if ((s = copy_field(h, th ? MK_FIELD_T : MK_FIELD_C, th ? temp : conc)) != MK_OK) return s;
@@ -519,6 +554,7 @@ mk_status mk_checkpoint(mk_handle* h, const char* path) {
   dump(e.temp, e.temp ? bp : 0);
   dump(e.rest1, e.rest1 ? (uint64_t)e.ncell * sizeof(float) : 0);
   dump(e.pop2, mke::engine_pop_bytes(e, 2));
+  dump(e.phij, e.phij ? (uint64_t)e.p.n_objects * bp : 0);
   fclose(f);
   if (!ok) {
     h->err = std::string("checkpoint write failed: ") + path;
@@ -571,6 +607,7 @@ mk_status mk_restore(mk_handle* h, const char* path) {
   load(e.temp, e.temp ? bp : 0);
   load(e.rest1, e.rest1 ? (uint64_t)e.ncell * sizeof(float) : 0);
   load(e.pop2, mke::engine_pop_bytes(e, 2));
+  load(e.phij, e.phij ? (uint64_t)e.p.n_objects * bp : 0);
   fclose(f);
   if (!ok) {
     h->err = "checkpoint truncated";

@@ -54,6 +54,7 @@ void default_params(mk_params* p) {
   p->eps2 = 0.0;
   p->wall_axis = -1;
   p->inlet = 0;
+  p->grain_kappa = 1.0;
 }
 
 void default_options(mk_options* o) {
@@ -223,7 +224,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model < 0 || p->model > 5) {
+  if (p->model < 0 || p->model > MK_MODEL_MULTIGRAIN) {
     err = "unknown model";
     return MK_ERR_ARG;
   }
@@ -295,6 +296,16 @@ mk_status validate_params(const mk_params* p, std::string& err) {
   } else if (p->model == MK_MODEL_MULTIPHASE) {
     if (!(p->tau_l > 0.5 && p->tau_g > 0.5 && p->rho_l > 0 && p->rho_g > 0 && p->width > 0 && p->mobility > 0)) {
       err = "multiphase parameters out of range (tau > 1/2, densities, W, M > 0)";
+      return MK_ERR_ARG;
+    }
+  }
+  if (p->model == MK_MODEL_MULTIGRAIN) {
+    if (p->n_objects < 1 || p->n_objects > MK_MAX_OBJECTS) {
+      err = "the multigrain model needs 1 to 64 seeds (one order parameter per grain)";
+      return MK_ERR_ARG;
+    }
+    if (!(p->W0 > 0 && p->mobility > 0 && p->D > 0)) {
+      err = "multigrain parameters out of range (W0, mobility, D > 0)";
       return MK_ERR_ARG;
     }
   }
@@ -377,6 +388,8 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       model = MK_MODEL_CONVECTION;
     else if (m == "flow_dendrite" || m == "flow_thermal_dendrite")
       model = MK_MODEL_FLOW_DENDRITE;
+    else if (m == "multigrain" || m == "multiphasefield" || m == "multi_phase_field")
+      model = MK_MODEL_MULTIGRAIN;
     else {
       err = "<b200><model>: unknown model '" + m + "'";
       return MK_ERR_XML;
@@ -480,7 +493,12 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       p.lambda = lam;
     else if (d0 > 0)
       p.lambda = 0.8839 * W0 / d0;
-    if (model == MK_MODEL_THERMAL_DENDRITE || model == MK_MODEL_FLOW_DENDRITE) {
+    if (model == MK_MODEL_MULTIGRAIN) {
+      // the grains' Allen-Cahn relaxation rate 1/(dt/dx^2/cs^2 + 1/2)
+      // (mkFluidsUser.cpp:282): mobility dt/dx^2, 1 in lattice units
+      p.mobility = 1.0;
+    }
+    if (model == MK_MODEL_THERMAL_DENDRITE || model == MK_MODEL_FLOW_DENDRITE || model == MK_MODEL_MULTIGRAIN) {
       if (!opt_d(r, "temperature/alphaFluid", alpha, err) || !opt_d(r, "temperature/undercooling", under, err) ||
           !opt_d(r, "temperature/iniValue", ini, err))
         return MK_ERR_XML;
@@ -607,7 +625,7 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
               opt_d(b, "eps4", p.eps4, err) && opt_d(b, "W0", p.W0, err) && opt_d(b, "lambda", p.lambda, err) &&
               opt_d(b, "delta", p.delta, err) && opt_d(b, "diffusivity", p.D, err) &&
               opt_d(b, "diffSolid", p.D_s, err) && opt_d(b, "partition", p.k_part, err) &&
-              opt_d(b, "antiTrapping", p.at_coef, err);
+              opt_d(b, "antiTrapping", p.at_coef, err) && opt_d(b, "grainKappa", p.grain_kappa, err);
     if (!ok) return MK_ERR_XML;
     // tau0 from the thin-interface relation unless given: tau0 = a2 lambda W0^2 / D
     double tau0 = -1;
@@ -710,6 +728,16 @@ static double bubble_phi(const mk_params* p, const double pos[3], const int n3[3
 
 // Solid seeds (phi = +1) in liquid (phi = -1): the largest of
 // -tanh((r_k - R_k)/(sqrt(2) W0)) over the seeds.
+// Order parameter of seed k alone: -tanh((r - R) / (sqrt 2 W0)).
+static double grain_phi(const mk_params* p, int k, const double pos[3]) {
+  double d2 = 0;
+  for (int a = 0; a < 3; ++a) {
+    const double d = pos[a] - p->obj_center[k][a];
+    d2 += d * d;
+  }
+  return -std::tanh((std::sqrt(d2) - p->obj_radius[k]) / (std::sqrt(2.0) * p->W0));
+}
+
 static double seed_phi(const mk_params* p, const double pos[3]) {
   double ph = -1.0;
   for (int k = 0; k < p->n_objects; ++k) {
@@ -796,6 +824,17 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
                  p->model == MK_MODEL_FLOW_DENDRITE)
                     ? best
                     : 0;
+            if (p->model == MK_MODEL_MULTIGRAIN) {
+              // the grain whose order parameter is largest (ties to the lower index)
+              double bp = -1e300;
+              for (int k = 0; k < p->n_objects; ++k) {
+                const double g = grain_phi(p, k, pos);
+                if (g > bp) {
+                  bp = g;
+                  v = k;
+                }
+              }
+            }
             break;
           }
           case MK_FIELD_PHI:
@@ -803,6 +842,10 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
               v = bubble_phi(p, pos, n3);
             } else if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION) {
               v = 0.0;
+            } else if (p->model == MK_MODEL_MULTIGRAIN) {
+              // aggregate phi = (N - 1) + sum_j phi_j (mkFluidsUser.cpp:162-168)
+              v = p->n_objects - 1.0;
+              for (int k = 0; k < p->n_objects; ++k) v += grain_phi(p, k, pos);
             } else {
               v = seed_phi(p, pos);
             }

@@ -51,6 +51,8 @@ struct Engine {
   void* pop2;         // flow lattice of the flow + dendrite model (deviations f - w rho0)
   void* vel;          // flow + dendrite: the loop's collision velocity, 3 planes of ncell (phi type), read by
                       // the thermal lattice and the boundary kernel
+  void* phij;         // multigrain: the grains' order parameters, N planes of ncell (phi type), else null
+  double* gseeds;     // multigrain: x, y, z, R per grain (initial state), else null
   float* rest1;       // FP32 rest population of lattice 1 (multiphase h) with 16-bit storage, else null
   void* phi[2];
   void* temp;
@@ -96,6 +98,8 @@ const char* engine_kernel_name(const Engine& e, int k);
 
 // Compute a macroscopic field of the current state into e.field (device).
 cudaError_t engine_field(Engine& e, int field);
+// Multigrain: grain j's order parameter into e.field (device).
+cudaError_t engine_grain_field(Engine& e, int grain);
 
 // FP64 diagnostics (two-pass reduction into e.dsum); host copy in out[DG_N].
 cudaError_t engine_diag(Engine& e, double* out);

@@ -776,6 +776,188 @@ __global__ void __launch_bounds__(128)
   temp[cb] = P(Tb);
 }
 
+// ====================================================== MULTIGRAIN (f-3)
+// run_multiPhaseField (MaterKit.cpp:529-571), mkFluidsUser::propagate /
+// relaxation (mkFluidsUser.cpp:68-299): one D3Q7 lattice per grain j (planes
+// 7j .. 7j+6 of lattice 0, held as g - w (-1)), phi_j = sum g_j (streamed),
+// the aggregate phi = (N - 1) + sum phi_j, and per grain
+//   g_j* = g_j - om (g_j - w phi_j) + w P_j + (1 - om/2) w lam_j (e.n_j),
+// P_j = -2 p_j kappa_j (sum_k p_k^2 - p_j^2), p = (1 + phi)/2, kappa_0 = 0;
+// n_j = grad phi_j / (|grad phi_j| + 1e-6) (D3Q19 gradient), lam_j =
+// (1 - phi_j^2)/(sqrt2 W0).
+// The thermal lattice relaxes with latent heat (1/2) dphi of the aggregate.
+template <class T>
+struct MgK {
+  T om, fo, inv_w, kappa, om_t, ref_t;
+  int ngr;
+};
+
+template <class S, class P, int PARITY, class NB>
+__device__ __forceinline__ void mg_phi_cell(const S* __restrict__ G, P* __restrict__ phij, P* __restrict__ phi_new,
+                                            const int64_t stride, const int64_t ncell, const NB& nb, const int c,
+                                            const int ngr) {
+  typedef typename Stor<S>::T T;
+  T agg = T(ngr - 1);
+  for (int j = 0; j < ngr; ++j) {
+    const S* Gj = G + (int64_t)j * 7 * stride;
+    T sum = T(-1);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) sum += ld_in<S, 7>(Gj, stride, nb, PARITY, c, i);
+    phij[(int64_t)j * ncell + c] = P(sum);
+    agg += sum;
+  }
+  phi_new[c] = P(agg);
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mg_phi(const S* __restrict__ G, P* __restrict__ phij,
+                                                const P* __restrict__ phi_old, P* __restrict__ phi_new, const Geom g,
+                                                int ngr) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+  if (!g.fluid(x, y, z)) {
+    const int64_t c = g.idx(x, y, z);
+    phi_new[c] = phi_old[c];
+    return;
+  }
+  if (fastw_cell(g, x, y, z)) {
+    const FastW fa = make_fastw(g, x, y, z);
+    mg_phi_cell<S, P, PARITY>(G, phij, phi_new, g.stride, ncell, fa, fa.c, ngr);
+  } else {
+    const Nbr nb(g, x, y, z);
+    mg_phi_cell<S, P, PARITY>(G, phij, phi_new, g.stride, ncell, nb, nb.idx(0, 0, 0), ngr);
+  }
+}
+
+template <class S, class P, int PARITY, class NB>
+__device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phij,
+                                        const P* __restrict__ phi_new, const P* __restrict__ phi_old,
+                                        P* __restrict__ temp, const int64_t stride, const int64_t ncell, const NB& nb,
+                                        const int c, const MgK<typename Stor<S>::T>& k) {
+  typedef typename Stor<S>::T T;
+  T S2 = T(0);
+  for (int j = 0; j < k.ngr; ++j) {
+    const T pk = T(0.5) * (T(1) + T(phij[(int64_t)j * ncell + c]));
+    S2 += pk * pk;
+  }
+  for (int j = 0; j < k.ngr; ++j) {
+    const P* f = phij + (int64_t)j * ncell;
+    const T ph = T(f[c]);
+    T gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll
+    for (int i = 1; i < 19; ++i) {
+      const T fn = nb_fluid(nb, ex(i), ey(i), ez(i)) ? T(__ldg(f + nb_idx(nb, ex(i), ey(i), ez(i)))) : ph;
+      const T w = T(wq<19>(i));
+      if (ex(i)) gx += (w * T(ex(i))) * fn;
+      if (ey(i)) gy += (w * T(ey(i))) * fn;
+      if (ez(i)) gz += (w * T(ez(i))) * fn;
+    }
+    gx *= T(3);
+    gy *= T(3);
+    gz *= T(3);
+    // regularised at 1e-6: where grad phi_j vanishes (a seed centre on a
+    // lattice point) its direction is rounding noise
+    const T inv = T(1) / (sqrt(gx * gx + gy * gy + gz * gz) + T(1e-6));
+    const T lam = (T(1) - ph * ph) * k.inv_w * k.fo;
+    const T pj = T(0.5) * (T(1) + ph);
+    const T Pj = j == 0 ? T(0) : T(-2) * pj * (S2 - pj * pj) * k.kappa;
+    const T dph = ph + T(1);  // phi_j - ref
+    S* Gj = G + (int64_t)j * 7 * stride;
+    T gv[7];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(Gj, stride, nb, PARITY, c, i);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      const T w = T(wq<7>(i));
+      const T en = (T(ex(i)) * gx + T(ey(i)) * gy + T(ez(i)) * gz) * inv;
+      st_out<S, 7>(Gj, stride, nb, PARITY, c, i, gv[i] - k.om * (gv[i] - w * dph) + w * Pj + w * lam * en);
+    }
+  }
+  // thermal lattice with latent heat (1/2) dphi of the aggregate
+  T t[7], dT = T(0);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
+    dT += t[i];
+  }
+  const T lat = T(0.5) * (T(phi_new[c]) - T(phi_old[c]));
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    const T w = T(wq<7>(i));
+    st_out<S, 7>(Tp, stride, nb, PARITY, c, i, t[i] - k.om_t * (t[i] - w * dT) + w * lat);
+  }
+  temp[c] = P(k.ref_t + dT);
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256)
+    k_mg_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phij, const P* __restrict__ phi_new,
+                 const P* __restrict__ phi_old, P* __restrict__ temp, const Geom g, const MgK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+  if (fastw_cell(g, x, y, z)) {
+    const FastW fa = make_fastw(g, x, y, z);
+    mg_cell<S, P, PARITY>(G, Tp, phij, phi_new, phi_old, temp, g.stride, ncell, fa, fa.c, k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    mg_cell<S, P, PARITY>(G, Tp, phij, phi_new, phi_old, temp, g.stride, ncell, nb, nb.idx(0, 0, 0), k);
+  }
+}
+
+// Initial state: grain j's order parameter -tanh((r_j - R_j)/(sqrt2 W0)) from
+// its seed (gseeds: x, y, z, R per grain), the aggregate, T, and the
+// equilibria of all lattices.
+template <class S, class InT>
+__global__ void k_mg_init(S* A0, S* A1, typename PhiOf<S>::type* phij, typename PhiOf<S>::type* phi0,
+                          typename PhiOf<S>::type* phi1, typename PhiOf<S>::type* temp, const InT* __restrict__ in_t,
+                          double d_t, const double* __restrict__ gseeds, int ngr, double W0, const Geom g,
+                          int64_t ncell, Refs refs) {
+  typedef typename PhiOf<S>::type P;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t c = g.idx(x, y, z);
+  const bool fl = g.fluid(x, y, z);
+  const Nbr nb(g, x, y, z);
+  double agg = ngr - 1.0;
+  for (int j = 0; j < ngr; ++j) {
+    const double dx = x - gseeds[4 * j], dy = y - gseeds[4 * j + 1], dz = z - gseeds[4 * j + 2];
+    const double ph = -tanh((sqrt(dx * dx + dy * dy + dz * dz) - gseeds[4 * j + 3]) / (sqrt(2.0) * W0));
+    phij[(int64_t)j * ncell + c] = P(ph);
+    agg += ph;
+    if (fl) put_eq<S, 7>(A0 + (int64_t)j * 7 * g.stride, g, nb, (int)c, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
+  }
+  phi0[c] = P(agg);
+  phi1[c] = P(agg);
+  const double tv = in_t ? double(in_t[c]) : d_t;
+  temp[c] = P(tv);
+  if (fl) put_eq<S, 7>(A1, g, nb, (int)c, tv, 0.0, 0.0, 0.0, 0.0, refs.r1);
+}
+
+// Grain field: the grain whose order parameter is largest (ties to the lower index).
+template <class P>
+__global__ void k_field_mg_grain(const P* __restrict__ phij, int ngr, int64_t n, double* __restrict__ out) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  int best = 0;
+  P bv = phij[c];
+  for (int j = 1; j < ngr; ++j) {
+    const P v = phij[(int64_t)j * n + c];
+    if (v > bv) {
+      bv = v;
+      best = j;
+    }
+  }
+  out[c] = best;
+}
+
 // ===================================================================== INIT
 template <class S, class InT>
 __global__ void k_init(int model, int Q0, S* A0, S* A1, S* A2, int Q2, float* H0, typename PhiOf<S>::type* phi0,
@@ -1534,6 +1716,46 @@ void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   }
 }
 
+template <class T>
+MgK<T> mg_coef(const mk_params& p, Refs r) {
+  MgK<T> k;
+  k.om = T(1.0 / (4.0 * p.mobility + 0.5));
+  k.fo = T(1.0 - 0.5 / (4.0 * p.mobility + 0.5));
+  k.inv_w = T(1.0 / (std::sqrt(2.0) * p.W0));
+  k.kappa = T(p.grain_kappa);
+  k.om_t = T(1.0 / (4.0 * p.D + 0.5));
+  k.ref_t = T(r.r1);
+  k.ngr = p.n_objects;
+  return k;
+}
+
+template <class S>
+void launch_mg(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  S* G = (S*)e.pop0;
+  P* phij = (P*)e.phij;
+  P* phi_old = (P*)e.phi[e.phi_cur];
+  P* phi_new = (P*)e.phi[1 - e.phi_cur];
+  if (ev) cudaEventRecord(ev[0], e.stream);
+  if (parity == 0)
+    k_mg_phi<S, P, 0><<<grid, block, 0, e.stream>>>(G, phij, phi_old, phi_new, g, e.p.n_objects);
+  else
+    k_mg_phi<S, P, 1><<<grid, block, 0, e.stream>>>(G, phij, phi_old, phi_new, g, e.p.n_objects);
+  if (ev) {
+    cudaEventRecord(ev[1], e.stream);
+    cudaEventRecord(ev[2], e.stream);
+  }
+  const MgK<T> k = mg_coef<T>(e.p, r);
+  if (parity == 0)
+    k_mg_collide<S, P, 0><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phij, phi_new, phi_old, (P*)e.temp, g, k);
+  else
+    k_mg_collide<S, P, 1><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phij, phi_new, phi_old, (P*)e.temp, g, k);
+  if (ev) cudaEventRecord(ev[3], e.stream);
+}
+
 template <class S>
 void step_t(mke::Engine& e, cudaEvent_t* ev) {
   dim3 grid, block;
@@ -1559,6 +1781,11 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
       launch_mp<S>(e, parity, grid, block, ev);
       e.launches += 2;
       break;
+    case MK_MODEL_MULTIGRAIN:
+      launch_mg<S>(e, parity, grid, block, ev);
+      e.phi_cur = 1 - e.phi_cur;
+      e.launches += 2;
+      break;
     case MK_MODEL_FLOW_DENDRITE:
       launch_fd<S>(e, parity, grid, block, ev);
       e.phi_cur = 1 - e.phi_cur;
@@ -1579,6 +1806,13 @@ cudaError_t set_state_t(mke::Engine& e, const InT* d_phi, const InT* d_t, const 
   dim3 grid, block;
   launch_dims(e, grid, block);
   const Geom g = make_geom(e);
+  if (e.p.model == MK_MODEL_MULTIGRAIN) {
+    // the grains' order parameters start from their seeds (phi is their aggregate)
+    k_mg_init<S, InT><<<grid, block, 0, e.stream>>>((S*)e.pop0, (S*)e.pop1, (P*)e.phij, (P*)e.phi[0], (P*)e.phi[1],
+                                                    (P*)e.temp, d_t, -e.p.delta, e.gseeds, e.p.n_objects, e.p.W0, g,
+                                                    e.ncell, refs_of(e.p));
+    return cudaGetLastError();
+  }
   k_init<S, InT><<<grid, block, 0, e.stream>>>(e.p.model, e.Q0, (S*)e.pop0, (S*)e.pop1, (S*)e.pop2, e.Q2, e.rest1,
                                                (P*)e.phi[0],
                                                (P*)e.phi[1],
@@ -1598,6 +1832,10 @@ cudaError_t field_t(mke::Engine& e, int field) {
   const Refs r = refs_of(e.p);
   const int m = e.p.model;
   const int nb = (int)((e.ncell + 255) / 256);
+  if (field == MK_FIELD_GRAIN && m == MK_MODEL_MULTIGRAIN) {
+    k_field_mg_grain<P><<<nb, 256, 0, e.stream>>>((const P*)e.phij, e.p.n_objects, e.ncell, e.field);
+    return cudaGetLastError();
+  }
   if (field == MK_FIELD_FLAG && m == MK_MODEL_FLOW_DENDRITE) {
     k_field_fdflag<P><<<grid, block, 0, e.stream>>>(g, (const P*)e.phi[e.phi_cur], e.field);
     return cudaGetLastError();
@@ -1647,7 +1885,8 @@ cudaError_t field_t(mke::Engine& e, int field) {
     return cudaGetLastError();
   }
   if (field == MK_FIELD_T || field == MK_FIELD_C) {
-    if ((field == MK_FIELD_T) != (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE))
+    if ((field == MK_FIELD_T) !=
+        (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE || m == MK_MODEL_MULTIGRAIN))
       return cudaErrorInvalidValue;
     k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.temp, nullptr, e.ncell, e.field);
     return cudaGetLastError();
@@ -1758,6 +1997,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     e.Q0 = 7;
     e.Q1 = 7;
   }
+  if (p.model == MK_MODEL_MULTIGRAIN) e.Q0 = 7 * p.n_objects;  // one D3Q7 lattice per grain
   e.Q2 = p.model == MK_MODEL_FLOW_DENDRITE ? p.lattice : 0;
   // Launch shape: a full warp row along x, rows stacked in y to 256 threads.
   int bx = block_x > 0 ? block_x : (p.nx >= 128 ? 128 : (p.nx >= 64 ? 64 : 32));
@@ -1794,7 +2034,19 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   }
   if ((st = alloc(&e.phi[0], (size_t)e.ncell * e.phi_elem)) != cudaSuccess) return st;
   const bool dend = p.model == MK_MODEL_THERMAL_DENDRITE || p.model == MK_MODEL_SOLUTAL_DENDRITE ||
-                    p.model == MK_MODEL_FLOW_DENDRITE;
+                    p.model == MK_MODEL_FLOW_DENDRITE || p.model == MK_MODEL_MULTIGRAIN;
+  const bool mg = p.model == MK_MODEL_MULTIGRAIN;
+  if ((st = alloc(&e.phij, mg ? (size_t)p.n_objects * e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
+  if (mg) {
+    std::vector<double> gs((size_t)4 * p.n_objects);
+    for (int k = 0; k < p.n_objects; ++k) {
+      for (int a = 0; a < 3; ++a) gs[4 * k + a] = p.obj_center[k][a];
+      gs[4 * k + 3] = p.obj_radius[k];
+    }
+    if ((st = cudaMalloc((void**)&e.gseeds, gs.size() * sizeof(double))) != cudaSuccess) return st;
+    if ((st = cudaMemcpy(e.gseeds, gs.data(), gs.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
+      return st;
+  }
   if ((st = alloc(&e.phi[1], dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (!dend) e.phi[1] = nullptr;
   if ((st = alloc(&e.temp, dend ? (size_t)e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
@@ -1847,7 +2099,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
-  void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.vel, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
+  void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.vel, e.phij, e.gseeds, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
                   e.field32, e.stage32};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -1979,6 +2231,18 @@ cudaError_t engine_field(Engine& e, int field) {
   }
 }
 
+cudaError_t engine_grain_field(Engine& e, int grain) {
+  if (e.p.model != MK_MODEL_MULTIGRAIN || grain < 0 || grain >= e.p.n_objects) return cudaErrorInvalidValue;
+  const int nb = (int)((e.ncell + 255) / 256);
+  if (e.phi_elem == 8)
+    k_field_copy<double><<<nb, 256, 0, e.stream>>>((const double*)e.phij + (int64_t)grain * e.ncell, nullptr, e.ncell,
+                                                   e.field);
+  else
+    k_field_copy<float><<<nb, 256, 0, e.stream>>>((const float*)e.phij + (int64_t)grain * e.ncell, nullptr, e.ncell,
+                                                  e.field);
+  return cudaGetLastError();
+}
+
 cudaError_t engine_diag(Engine& e, double* out) {
   cudaError_t st;
   switch (e.p.precision) {
@@ -2005,9 +2269,10 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   if (trial_steps < 1) trial_steps = 1;
   const size_t b0 = engine_pop_bytes(e, 0), b1 = engine_pop_bytes(e, 1), b2 = engine_pop_bytes(e, 2),
                bp = (size_t)e.ncell * e.phi_elem;
-  void* const bufs[7] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.rest1, e.pop2};
-  const size_t sizes[7] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0,
-                           e.rest1 ? (size_t)e.ncell * sizeof(float) : 0, b2};
+  void* const bufs[8] = {e.pop0, e.pop1, e.phi[0], e.phi[1], e.temp, e.rest1, e.pop2, e.phij};
+  const size_t sizes[8] = {b0, b1, bp, e.phi[1] ? bp : 0, e.temp ? bp : 0,
+                           e.rest1 ? (size_t)e.ncell * sizeof(float) : 0, b2,
+                           e.phij ? (size_t)e.p.n_objects * bp : 0};
   size_t total = 0;
   for (size_t s : sizes) total += s;
   char* save = nullptr;
@@ -2015,7 +2280,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   if (st != cudaSuccess) return st;
   auto copy = [&](bool to_save) -> cudaError_t {
     size_t off = 0;
-    for (int q = 0; q < 7; ++q) {
+    for (int q = 0; q < 8; ++q) {
       if (!sizes[q]) continue;
       cudaError_t s2 = to_save ? cudaMemcpyAsync(save + off, bufs[q], sizes[q], cudaMemcpyDeviceToDevice, e.stream)
                                : cudaMemcpyAsync(bufs[q], save + off, sizes[q], cudaMemcpyDeviceToDevice, e.stream);
@@ -2096,7 +2361,8 @@ double engine_bytes_per_cell(const Engine& e) {
   const double S = e.elem;
   const double phi = (e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION) ? 0.0 : 2.0 * e.phi_elem;
   const double rest = e.rest1 ? 2.0 * (4.0 - S) : 0.0;
-  return 2.0 * (e.Q0 + e.Q1 + e.Q2) * S + phi + rest;
+  const double grains = e.phij ? 2.0 * e.p.n_objects * e.phi_elem : 0.0;  // phi_j written, then read
+  return 2.0 * (e.Q0 + e.Q1 + e.Q2) * S + phi + rest + grains;
 }
 
 }  // namespace mke

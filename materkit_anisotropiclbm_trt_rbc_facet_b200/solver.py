@@ -223,6 +223,14 @@ class Solver:
         _check(self._lib.mk_get_field(self._h, A.FIELDS[name], code, out.ctypes.data, out.nbytes), self._h)
         return out.reshape(self.shape)
 
+    def grain_field(self, grain: int, dtype=np.float64) -> np.ndarray:
+        """Order parameter of one grain of a multigrain case, (nz, ny, nx)."""
+        out = np.empty(self.shape, dtype=dtype)
+        dt = A.MK_DTYPE_F64 if out.dtype == np.float64 else A.MK_DTYPE_F32
+        _check(self._lib.mk_get_grain_field(self._h, int(grain), dt, out.ctypes.data_as(C.c_void_p), out.nbytes),
+               self._h)
+        return out
+
     def set_state(self, phi=None, T=None, C_=None, rho=None, u=None) -> None:
         def ptr(a):
             if a is None:
@@ -444,6 +452,8 @@ class mkFluidsMRT(_RefSolver):
         A.MK_MODEL_FLOW_DENDRITE: ["propagate_PBB", "relaxation", "bdyVelocity", "phasefield_propagate",
                                    "relaxation_anisotropy_thermal", "thermal_propagate", "thermal_relaxation",
                                    "bdy_flowin"],
+        # run_multiPhaseField (MaterKit.cpp:563-567)
+        A.MK_MODEL_MULTIGRAIN: ["propagate", "relaxation", "thermal_propagate", "thermal_relaxation"],
     }
 
     def initialize_geometry_Poiseuille(self) -> None:

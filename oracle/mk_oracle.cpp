@@ -146,6 +146,9 @@ struct orc_state {
   int Qw = 0;                        // flow lattice of the flow + dendrite model, 0 if none
   std::vector<double> w_out, w_hlp;  // its populations
   std::vector<double> vel;           // its velocity, 3 per cell (advects the thermal lattice)
+  int Ng = 0;                                   // multigrain: number of grain order parameters
+  std::vector<std::vector<double>> gj_out, gj_hlp;  // their D3Q7 lattices, one [q][cell] array per grain
+  std::vector<double> phij;                     // their order parameters, [grain][cell]
   std::vector<int> grain;
   std::vector<double> rot;  // 9 per object (R, columns = crystal axes)
 };
@@ -549,6 +552,31 @@ void anisotropy(const double* R, int kind, double e4, double e2, const double g[
   *a_out = a;
 }
 
+// Thermal relaxation of the streamed D3Q7 lattice with latent heat (1/2)
+// dphi (mkThermalField::relaxation, mkThermalField.h:34); with a flow lattice
+// the equilibrium is advected, w T (1 + 4 e.u) (getTEquPDFs).
+void thermal_relax(orc_state* s) {
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  const double om_t = 1.0 / (4.0 * p.D + 0.5);
+  const bool adv = !s->vel.empty();
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) continue;
+    double T = 0;
+    for (int i = 0; i < 7; ++i) T += s->s_hlp[(int64_t)i * n + c];
+    const double lat = 0.5 * (s->phi[c] - s->phi_prev[c]);
+    for (int i = 0; i < 7; ++i) {
+      const double w = weight(7, i);
+      const double eu = adv ? E27[i][0] * s->vel[3 * c] + E27[i][1] * s->vel[3 * c + 1] + E27[i][2] * s->vel[3 * c + 2]
+                            : 0.0;
+      const double ti = s->s_hlp[(int64_t)i * n + c];
+      s->s_out[(int64_t)i * n + c] = ti - om_t * (ti - w * T * (1.0 + 4.0 * eu)) + w * lat;
+    }
+    s->temp[c] = T;
+  }
+}
+
 void thermal_dendrite_step(orc_state* s) {
   const int64_t n = s->n;
   const mk_params& p = s->p;
@@ -643,25 +671,7 @@ void thermal_dendrite_step(orc_state* s) {
         }
     return;
   }
-  // 3. thermal propagate + relaxation with latent heat (1/2) dphi; with a
-  // flow lattice the equilibrium is advected, w T (1 + 4 e.u) (getTEquPDFs).
-  const double om_t = 1.0 / (4.0 * p.D + 0.5);
-  const bool adv = !s->vel.empty();
-#pragma omp parallel for schedule(static)
-  for (int64_t c = 0; c < n; ++c) {
-    if (s->flag[c] != MK_FLAG_FLUID) continue;
-    double T = 0;
-    for (int i = 0; i < 7; ++i) T += s->s_hlp[(int64_t)i * n + c];
-    const double lat = 0.5 * (s->phi[c] - s->phi_prev[c]);
-    for (int i = 0; i < 7; ++i) {
-      const double w = weight(7, i);
-      const double eu = adv ? E27[i][0] * s->vel[3 * c] + E27[i][1] * s->vel[3 * c + 1] + E27[i][2] * s->vel[3 * c + 2]
-                            : 0.0;
-      const double ti = s->s_hlp[(int64_t)i * n + c];
-      s->s_out[(int64_t)i * n + c] = ti - om_t * (ti - w * T * (1.0 + 4.0 * eu)) + w * lat;
-    }
-    s->temp[c] = T;
-  }
+  thermal_relax(s);
 }
 
 // ------------------------------------------------ FLOW + DENDRITE model
@@ -768,6 +778,88 @@ void flow_dendrite_nee(orc_state* s, bool flow_lattice) {
         }
       }
   }
+}
+
+// ------------------------------------------------------- MULTIGRAIN model
+// run_multiPhaseField (MaterKit.cpp:529-571) with mkFluidsUser::propagate /
+// relaxation (mkFluidsUser.cpp:68-299, the multiphase field of "Programming
+// Phase-Field Modelling" p. 37 Eq. 4.35): one D3Q7 lattice per grain j,
+//   phi_j = sum_i g_j,i (streamed), phi = (N - 1) + sum_j phi_j,
+//   g_j* = g_j - om (g_j - w phi_j) + w P_j + (1 - om/2) w lam_j (e.n_j),
+// P_j = -2 p_j kappa_j sum_{k != j} p_k^2 with p = (1 + phi)/2 and kappa_0 = 0,
+// kappa_j = grain_kappa for j >= 1 (mkFluidsUser.cpp:233-251); the growth
+// source is off in the reference (Q_phi = 0 * ..., :255-263).  The Chai et al.
+// (IJHMT 122 (2018) 631) conservative Allen-Cahn flux with n_j = grad phi_j /
+// (|grad phi_j| + 1e-6) (D3Q19 isotropic gradient) and lam_j = (1 - phi_j^2)/(sqrt2 W0),
+// the flux that holds phi_j = tanh(x / (sqrt2 W0)), om = 1/(4 M + 1/2)
+// (:282, M = mobility).  Then the thermal lattice with latent heat (1/2) dphi of
+// the aggregate (mkThermalField::propagate / relaxation).  Left out: the
+// reference's aggregate g lattice (its density is overwritten by the sum of the
+// grains at :162-168 and never read) and its hard-coded test velocity of grain
+// 1 in the equilibrium (:220-226).
+void multigrain_step(orc_state* s) {
+  const int64_t n = s->n;
+  const mk_params& p = s->p;
+  const int N = s->Ng;
+  for (int j = 0; j < N; ++j) propagate(s, 7, s->gj_out[j], s->gj_hlp[j]);
+  std::swap(s->phi_prev, s->phi);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s->flag[c] != MK_FLAG_FLUID) {
+      s->phi[c] = s->phi_prev[c];
+      continue;
+    }
+    double agg = N - 1.0;
+    for (int j = 0; j < N; ++j) {
+      double ph = 0;
+      for (int i = 0; i < 7; ++i) ph += s->gj_hlp[j][(int64_t)i * n + c];
+      s->phij[(int64_t)j * n + c] = ph;
+      agg += ph;
+    }
+    s->phi[c] = agg;
+  }
+  const double om = 1.0 / (4.0 * p.mobility + 0.5);
+  const double fo = 1.0 - 0.5 * om;
+  const double inv_w = 1.0 / (std::sqrt(2.0) * p.W0);
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const int64_t c = cidx(s, x, y, z);
+        if (s->flag[c] != MK_FLAG_FLUID) continue;
+        double S2 = 0;
+        for (int k = 0; k < N; ++k) {
+          const double pk = 0.5 * (1.0 + s->phij[(int64_t)k * n + c]);
+          S2 += pk * pk;
+        }
+        for (int j = 0; j < N; ++j) {
+          const double* f = &s->phij[(int64_t)j * n];
+          const double ph = f[c];
+          double gr[3] = {0, 0, 0};
+          for (int i = 1; i < 19; ++i) {
+            const int64_t nb = nbr(s, x, y, z, E27[i][0], E27[i][1], E27[i][2]);
+            const double fn = nb >= 0 ? f[nb] : ph;
+            for (int a = 0; a < 3; ++a) gr[a] += weight(19, i) * E27[i][a] * fn;
+          }
+          for (int a = 0; a < 3; ++a) gr[a] *= 3.0;
+          const double gn = std::sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+          // regularised at 1e-6, not 1e-12: where grad phi_j vanishes (a seed
+          // centre on a lattice point) its direction is rounding noise, which
+          // the flux would carry at full strength lam
+          const double nv[3] = {gr[0] / (gn + 1e-6), gr[1] / (gn + 1e-6), gr[2] / (gn + 1e-6)};
+          const double lam = (1.0 - ph * ph) * inv_w;
+          const double pj = 0.5 * (1.0 + ph);
+          const double P = j == 0 ? 0.0 : -2.0 * pj * (S2 - pj * pj) * p.grain_kappa;
+          for (int i = 0; i < 7; ++i) {
+            const double w = weight(7, i);
+            const double en = E27[i][0] * nv[0] + E27[i][1] * nv[1] + E27[i][2] * nv[2];
+            const double g = s->gj_hlp[j][(int64_t)i * n + c];
+            s->gj_out[j][(int64_t)i * n + c] = g - om * (g - w * ph) + w * P + fo * w * lam * en;
+          }
+        }
+      }
+  propagate(s, 7, s->s_out, s->s_hlp);
+  thermal_relax(s);
 }
 
 void flow_dendrite_step(orc_state* s) {
@@ -880,12 +972,38 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
     s->f_hlp.assign((size_t)7 * n, 0.0);
     s->s_out.assign((size_t)7 * n, 0.0);
     s->s_hlp.assign((size_t)7 * n, 0.0);
-    if (p->model == MK_MODEL_FLOW_DENDRITE && T0) std::memcpy(s->temp.data(), T0, n * sizeof(double));
+    if ((p->model == MK_MODEL_FLOW_DENDRITE || p->model == MK_MODEL_MULTIGRAIN) && T0)
+      std::memcpy(s->temp.data(), T0, n * sizeof(double));
     for (int64_t c = 0; c < n; ++c)
       for (int i = 0; i < 7; ++i) {
         s->f_out[(int64_t)i * n + c] = weight(7, i) * s->phi[c];
         s->s_out[(int64_t)i * n + c] = weight(7, i) * s->temp[c];
       }
+    if (p->model == MK_MODEL_MULTIGRAIN) {
+      // one order parameter per seed, -tanh((r - R)/(sqrt2 W0)), and the
+      // aggregate (N - 1) + sum phi_j
+      const int N = p->n_objects;
+      s->Ng = N;
+      s->phij.assign((size_t)N * n, 0.0);
+      s->gj_out.assign(N, std::vector<double>((size_t)7 * n, 0.0));
+      s->gj_hlp.assign(N, std::vector<double>((size_t)7 * n, 0.0));
+      for (int z = 0; z < s->nz; ++z)
+        for (int y = 0; y < s->ny; ++y)
+          for (int x = 0; x < s->nx; ++x) {
+            const int64_t c = cidx(s, x, y, z);
+            double agg = N - 1.0;
+            for (int j = 0; j < N; ++j) {
+              const double dx = x - p->obj_center[j][0], dy = y - p->obj_center[j][1], dz = z - p->obj_center[j][2];
+              const double ph =
+                  -std::tanh((std::sqrt(dx * dx + dy * dy + dz * dz) - p->obj_radius[j]) / (std::sqrt(2.0) * p->W0));
+              s->phij[(int64_t)j * n + c] = ph;
+              agg += ph;
+              for (int i = 0; i < 7; ++i) s->gj_out[j][(int64_t)i * n + c] = weight(7, i) * ph;
+            }
+            s->phi[c] = agg;
+          }
+      s->phi_prev = s->phi;
+    }
     if (p->model == MK_MODEL_FLOW_DENDRITE) {
       // the flow starts at rho0 with u0 scaled by the liquid fraction, unless
       // density / velocity fields are given
@@ -936,6 +1054,9 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
       case MK_MODEL_FLOW_DENDRITE:
         flow_dendrite_step(s);
         break;
+      case MK_MODEL_MULTIGRAIN:
+        multigrain_step(s);
+        break;
       case MK_MODEL_THERMAL_DENDRITE:
       case MK_MODEL_SOLUTAL_DENDRITE:
         thermal_dendrite_step(s);  // the second lattice follows p.model
@@ -945,6 +1066,12 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
     }
     s->step++;
   }
+}
+
+extern "C" int orc_get_grain_phi(const orc_state* s, int grain, double* out) {
+  if (grain < 0 || grain >= s->Ng) return 1;
+  std::memcpy(out, &s->phij[(size_t)grain * s->n], s->n * sizeof(double));
+  return 0;
 }
 
 extern "C" int orc_get_populations(const orc_state* s, int which, double* out) {
@@ -962,6 +1089,16 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
     return 0;
   }
   if (field == MK_FIELD_GRAIN) {
+    if (p.model == MK_MODEL_MULTIGRAIN) {
+      // the grain whose order parameter is largest (ties to the lower index)
+      for (int64_t c = 0; c < n; ++c) {
+        int best = 0;
+        for (int j = 1; j < s->Ng; ++j)
+          if (s->phij[(int64_t)j * n + c] > s->phij[(int64_t)best * n + c]) best = j;
+        out[c] = best;
+      }
+      return 0;
+    }
     for (int64_t c = 0; c < n; ++c) out[c] = s->grain[c];
     return 0;
   }

@@ -108,6 +108,8 @@ int64_t orc_step(const orc_state* s);
 int orc_get_field(const orc_state* s, int field, double* out);
 // Raw post-collision populations of lattice `which` (0 flow/phase, 1 second lattice).
 int orc_get_populations(const orc_state* s, int which, double* out);
+// Multigrain: the order parameter of one grain (ncell doubles); 1 if out of range.
+int orc_get_grain_phi(const orc_state* s, int grain, double* out);
 void orc_set_threads(int n);
 // Discrete adjoint of the thermal dendrite loop: L = sum (phi - target)^2 after
 // `steps` loops from the current state; out = {L, dL/deps4, dL/dDelta,

@@ -41,6 +41,8 @@ def load() -> C.CDLL:
         lib.orc_step.argtypes = [C.c_void_p]
         lib.orc_get_field.restype = C.c_int
         lib.orc_get_field.argtypes = [C.c_void_p, C.c_int, D]
+        lib.orc_get_grain_phi.restype = C.c_int
+        lib.orc_get_grain_phi.argtypes = [C.c_void_p, C.c_int, D]
         lib.orc_get_populations.restype = C.c_int
         lib.orc_get_populations.argtypes = [C.c_void_p, C.c_int, D]
         lib.orc_set_threads.argtypes = [C.c_int]
@@ -101,6 +103,14 @@ class Oracle:
         rc = self.lib.orc_get_field(self.h, A.FIELDS[name], _ptr(out))
         if rc != 0:
             raise KeyError(name)
+        return out.reshape(p.nz, p.ny, p.nx)
+
+    def grain(self, j: int) -> np.ndarray:
+        """Order parameter of grain j (multigrain model)."""
+        p = self.params
+        out = np.empty(p.ncell(), dtype=np.float64)
+        if self.lib.orc_get_grain_phi(self.h, int(j), _ptr(out)) != 0:
+            raise KeyError(j)
         return out.reshape(p.nz, p.ny, p.nx)
 
     def close(self):
