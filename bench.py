@@ -9,6 +9,8 @@ Workloads (--workload)
             thermal lattice, one centred seed)
   ensemble  48 seeded solutal dendrite domains (edges 48-128) packed into
             one lattice, BF16 storage, persistent launches + CUDA graph
+  multigrain  eight grains (one Allen-Cahn order parameter each, pairwise
+            overlap penalty) + D3Q7 thermal lattice, 128^3
   flow_dendrite  thermal dendrite growing in a melt that flows in at x = 0
             and out at x = n - 1, 128^3 (D3Q19 TRT flow with porous
             bounce-back + phase field + advected D3Q7 thermal lattice)
@@ -56,6 +58,10 @@ WORKLOADS = {
                       "size": 128, "precision": "fp32", "kernel": "k_fd_flow", "slot": "flow",
                       "collision": "TRT(f, porous bounce-back) + BGK(g) + BGK(T)",
                       "data": "synthetic (seed at x = n/3, eps4 0.05, undercooling 0.55, inflow u = 0.02)"},
+    "multigrain": {"workload": "multigrain {n}^3: 8 grains (D3Q7 Allen-Cahn each, overlap penalty) + D3Q7 thermal",
+                   "metric": "MLUPS, %HBM roofline: multigrain 128^3, 8 grain lattices + thermal",
+                   "size": 128, "precision": "fp32", "kernel": "k_mg_collide", "collision": "BGK(g_j) + BGK(T)",
+                   "data": "synthetic (2 x 2 x 2 grains of radius n/5 at the quarter points)"},
     "ensemble": {"workload": "solutal dendrite ensemble: 48 domains, edges 48-128, 1-6 seeds each, seed 0xE45E",
                  "metric": "MLUPS aggregate, %HBM roofline: 48-domain solutal dendrite ensemble, BF16, "
                            "persistent + graph",
@@ -158,6 +164,10 @@ def _case_path(precision: str, n: int, workload: str = "bubbles") -> str:
     d = os.path.join(tempfile.gettempdir(), "mkb200_bench")
     if workload == "dendrite":
         text = cases.thermal_dendrite(n=n, precision=precision, loops=5000)
+    elif workload == "multigrain":
+        q = [n / 4.0, 3.0 * n / 4.0]
+        seeds = [(x, y, z, n / 5.0) for x in q for y in q for z in q]
+        text = cases.multigrain(n=n, precision=precision, loops=5000, seeds=seeds)
     elif workload == "flow_dendrite":
         text = cases.flow_dendrite(nx=n, ny=n, nz=n, precision=precision, loops=5000, radius=8.0, u_in=0.02,
                                    center=(n / 3.0, (n - 1) / 2.0, (n - 1) / 2.0))
@@ -183,6 +193,10 @@ def _collide_bytes(workload: str, prec: str, cells: int) -> int:
         return cells * (2 * 38 * S + P + (4 if S == 2 else 0))
     if workload == "flow_dendrite":
         return cells * (38 * S + 4 * P)
+    if workload == "multigrain":
+        # 8 grain lattices and the thermal lattice read and written, phi_j read
+        # (the stencil's halo counted once), phi(t+1), phi(t) read, T read and written
+        return cells * ((8 * 14 + 14) * S + (8 + 4) * P)
     return cells * (28 * S + 4 * P)
 
 
