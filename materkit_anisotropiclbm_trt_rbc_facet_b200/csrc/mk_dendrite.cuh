@@ -126,7 +126,7 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T
 #pragma unroll
   for (int q = 0; q < 9; ++q) R[q] = __ldg(Rm + q);
   const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
-  const T inv = T(1) / (gn + T(1e-12));
+  const T inv = div_fast(T(1), gn + T(1e-12));
   const T nl0 = gr[0] * inv, nl1 = gr[1] * inv, nl2 = gr[2] * inv;
   T nc[3];
 #pragma unroll
@@ -224,14 +224,17 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
     // anti-trapping current (first moment of the equilibrium) and the
     // rejection source; pair sums relax to equilibrium with rate 1, pair
     // differences with omega(phi)
+    // three divisions: su, then fj = -2 a_t W0 su / (|grad phi| + 1e-6) and
+    // om = 1 / (4 D + 1/2) = c / (4 c D + c/2) with c D the numerator of D
+    // (FP32: the fast division, well inside the single-precision tolerance)
     const T U = k.ref_t + dT;
     const T km = T(1) - k.k_part;
     const T cap = (T(1) + k.k_part - km * ph) * T(0.5);
     const T gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
-    const T fj = -k.at_w0 * (T(1) + km * U) * dphi / ((gn + T(1e-6)) * cap);
-    const T D = (k.D_l * (T(1) - ph) * T(0.5) + k.D_s * (T(1) + ph) * T(0.5)) / cap;
-    const T om = T(1) / (T(4) * D + T(0.5));
-    const T su = T(0.5) * (T(1) + km * U) * dphi / cap;
+    const T su = div_fast(T(0.5) * (T(1) + km * U) * dphi, cap);
+    const T fj = div_fast(T(-2) * k.at_w0 * su, gn + T(1e-6));
+    const T cD = k.D_l * (T(1) - ph) * T(0.5) + k.D_s * (T(1) + ph) * T(0.5);
+    const T om = div_fast(cap, T(4) * cD + T(0.5) * cap);
     {
       const T w0 = T(wq<7>(0));
       st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);

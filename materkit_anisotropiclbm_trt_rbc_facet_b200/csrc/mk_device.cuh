@@ -337,6 +337,15 @@ __host__ __device__ __forceinline__ void mrt19_collide(T (&f)[19], const T (&feq
 }
 
 // ------------------------------------------------- packed FP32 pairs (sm_100)
+// a / b: IEEE division in FP64, the fast approximate division in FP32 (about
+// two ulp, far inside the single-precision parity bounds; the denominators in
+// the kernels — densities, |grad phi| + eps, capacities, relaxation times —
+// are nowhere near its 2^126 limit).  An IEEE FP32 division is a
+// multi-instruction sequence with a slow path; the 16-bit kernels are
+// instruction-bound.
+__device__ __forceinline__ double div_fast(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_fast(float a, float b) { return __fdividef(a, b); }
+
 // Blackwell executes two FP32 lanes per FADD2 / FMUL2 / FFMA2 instruction
 // (round to nearest, no contraction beyond the written FMA).  Used where the
 // same arithmetic runs over two population pairs.

@@ -105,8 +105,9 @@ cudaError_t engine_grain_field(Engine& e, int grain);
 cudaError_t engine_diag(Engine& e, double* out);
 
 // Autotuner: times `trial_steps` loops of every candidate launch shape and
-// occupancy variant on a saved copy of the state, restores the state and
-// keeps the fastest.  Returns the chosen configuration and its ms per loop.
+// occupancy variant (two warm-up loops, then the faster of two timed repeats)
+// on a saved copy of the state, restores the state and keeps the fastest.
+// Returns the chosen configuration and its ms per loop.
 struct TuneResult {
   int block_x, block_y, minb;
   double ms_per_step;

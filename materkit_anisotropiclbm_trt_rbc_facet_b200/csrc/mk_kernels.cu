@@ -55,9 +55,10 @@ __device__ __forceinline__ void flow_relax(T (&f)[Q], const FlowK<T>& k, const T
     if (ez(i)) jz += T(ez(i)) * f[i];
   }
   const T rho = k.ref + drho;
-  ux = (jx + T(0.5) * Fx) / rho;
-  uy = (jy + T(0.5) * Fy) / rho;
-  uz = (jz + T(0.5) * Fz) / rho;
+  const T irho = div_fast(T(1), rho);
+  ux = (jx + T(0.5) * Fx) * irho;
+  uy = (jy + T(0.5) * Fy) * irho;
+  uz = (jz + T(0.5) * Fz) * irho;
   const T uu = ux * ux + uy * uy + uz * uz;
   if constexpr (COLL == MK_COLL_MRT && Q == 19) {
     MrtIn<T> q;  // equilibrium deviation: w [drho + rho (3eu + 4.5(eu)^2 - 1.5u^2)]
@@ -312,7 +313,7 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
   const T pstar = m[0], jx = m[3], jy = m[5], jz = m[7];
   T ph, rho, gphi[3], F[3];
   mp_force<T, P, NB>(phi, nb, c, k, pstar, ph, rho, gphi, F);
-  const T irho = T(1) / rho;
+  const T irho = div_fast(T(1), rho);
   const T ux = jx + T(0.5) * F[0] * irho;
   const T uy = jy + T(0.5) * F[1] * irho;
   const T uz = jz + T(0.5) * F[2] * irho;
@@ -337,13 +338,13 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
     q.uy = uy;
     q.uz = uz;
     q.sF = irho;
-    q.s_nu = T(1) / (k.tau_g + ph * (k.tau_l - k.tau_g));
+    q.s_nu = div_fast(T(1), k.tau_g + ph * (k.tau_l - k.tau_g));
     mrt19_relax_back<T>(gp_, m, q);
 #pragma unroll
     for (int i = 0; i < 19; ++i) st_out<S, 19>(G, stride, nb, PARITY, c, i, gp_[i]);
   }
   const T gn = sqrt(gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2]);
-  const T inv_gn = T(1) / (gn + T(1e-12));
+  const T inv_gn = div_fast(T(1), gn + T(1e-12));
   const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
   const T lam = k.inv_w4 * ph * (T(1) - ph);
   // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair, in the
@@ -512,7 +513,7 @@ __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T n
     if (ez(i)) jz += T(ez(i)) * f[i];
   }
   const T rho = k.ref + drho;
-  const T irho = T(1) / rho;
+  const T irho = div_fast(T(1), rho);
   ux = FORCE ? (jx + T(0.5) * k.Fx) * irho : jx * irho;
   uy = FORCE ? (jy + T(0.5) * k.Fy) * irho : jy * irho;
   uz = FORCE ? (jz + T(0.5) * k.Fz) * irho : jz * irho;
@@ -860,7 +861,10 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
     gz *= T(3);
     // regularised at 1e-6: where grad phi_j vanishes (a seed centre on a
     // lattice point) its direction is rounding noise
-    const T inv = T(1) / (sqrt(gx * gx + gy * gy + gz * gz) + T(1e-6));
+    // the fast division measured faster with 16-bit storage and slower with
+    // FP32 (0.38 -> 0.49 ms per 128^3 loop, 8 grains) in this kernel
+    const T gs = sqrt(gx * gx + gy * gy + gz * gz) + T(1e-6);
+    const T inv = Stor<S>::bytes == 2 ? div_fast(T(1), gs) : T(1) / gs;
     const T lam = (T(1) - ph * ph) * k.inv_w * k.fo;
     const T pj = T(0.5) * (T(1) + ph);
     const T Pj = j == 0 ? T(0) : T(-2) * pj * (S2 - pj * pj) * k.kappa;
@@ -2310,14 +2314,20 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
       e.block_x = bx;
       e.block_y = shapes[si][1];
       e.minb = nmb == 2 ? mb : mb0;
-      engine_step(e, nullptr);  // warm-up of this shape
-      cudaEventRecord(t0, e.stream);
-      for (int s = 0; s < trial_steps; ++s) engine_step(e, nullptr);
-      cudaEventRecord(t1, e.stream);
-      st = cudaEventSynchronize(t1);
-      if (st == cudaSuccess) st = cudaGetLastError();
-      float ms = 0;
-      if (st == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+      engine_step(e, nullptr);  // warm-up of this shape, both AA parities
+      engine_step(e, nullptr);
+      // the faster of two timed repeats (one slow repeat must not decide)
+      float ms = 1e30f;
+      for (int rep = 0; rep < 2 && st == cudaSuccess; ++rep) {
+        cudaEventRecord(t0, e.stream);
+        for (int s = 0; s < trial_steps; ++s) engine_step(e, nullptr);
+        cudaEventRecord(t1, e.stream);
+        st = cudaEventSynchronize(t1);
+        if (st == cudaSuccess) st = cudaGetLastError();
+        float m = 0;
+        if (st == cudaSuccess) cudaEventElapsedTime(&m, t0, t1);
+        ms = std::min(ms, m);
+      }
       ++ncand;
       if (st == cudaSuccess && ms / trial_steps < best) {
         best = ms / trial_steps;
