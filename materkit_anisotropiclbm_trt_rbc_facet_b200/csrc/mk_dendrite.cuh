@@ -174,6 +174,17 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
                                           typename Stor<S>::T vz = 0, int x = 0, int nx = 0) {
   static_assert(!NEE || (ADV && !SOL), "the face pass belongs to the advected thermal lattice");
   typedef typename Stor<S>::T T;
+  // FP32 / FP64: both lattices' slots go to L2 now, while the phi stencil
+  // and the anisotropy are computed (the kernel waits on load latency;
+  // measured 128^3 FP32 collide 58 -> 53 us).  With 16-bit storage the extra
+  // instructions cost more than they hide (ensemble BF16 0.98 -> 1.06 ms).
+  if constexpr (Stor<S>::bytes >= 4) {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      pf_in<S, 7>(G, stride, nb, PARITY, c, i);
+      pf_in<S, 7>(Tp, stride, nb, PARITY, c, i);
+    }
+  }
   const T ph = T(phi_new[c]);
   T gx = T(0), gy = T(0), gz = T(0);
 #pragma unroll
