@@ -839,6 +839,18 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
                                         P* __restrict__ temp, const int64_t stride, const int64_t ncell, const NB& nb,
                                         const int c, const MgK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
+  // FP32 / FP64: every grain's slots and the thermal slots go to L2 first;
+  // each grain's populations are loaded only after its stencil and penalty
+  // are computed (128^3, 8 grains: 0.39 -> 0.31 ms; no gain with 16-bit
+  // storage, where it is compiled out)
+  if constexpr (Stor<S>::bytes >= 4) {
+    for (int j = 0; j < k.ngr; ++j) {
+#pragma unroll
+      for (int i = 0; i < 7; ++i) pf_in<S, 7>(G + (int64_t)j * 7 * stride, stride, nb, PARITY, c, i);
+    }
+#pragma unroll
+    for (int i = 0; i < 7; ++i) pf_in<S, 7>(Tp, stride, nb, PARITY, c, i);
+  }
   T S2 = T(0);
   for (int j = 0; j < k.ngr; ++j) {
     const T pk = T(0.5) * (T(1) + T(phij[(int64_t)j * ncell + c]));
