@@ -300,11 +300,14 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
                                                 const P* __restrict__ phi, const int64_t stride, const NB& nb,
                                                 const int c, const MpK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
-  // the Allen-Cahn slots go to L2 now and are loaded once the pressure
-  // lattice is stored, so the two lattices' populations are never live
-  // together (register pressure sets the occupancy of this kernel)
+  // the Allen-Cahn slots go to L2 now (FP32 / FP64; with 16-bit storage the
+  // prefetch measured 2% slower) and are loaded once the pressure lattice is
+  // stored, so the two lattices' populations are never live together
+  // (register pressure sets the occupancy of this kernel)
+  if constexpr (Stor<S>::bytes >= 4) {
 #pragma unroll
-  for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
+    for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
+  }
   T gp_[19];  // g (rests at 0)
 #pragma unroll
   for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, stride, nb, PARITY, c, i);
