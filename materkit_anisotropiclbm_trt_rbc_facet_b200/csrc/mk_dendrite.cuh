@@ -319,8 +319,11 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
   temp[c] = P(Tc);
 }
 
+// 16-bit storage: five resident 256-thread blocks per SM (48 registers, a few
+// spilled bytes) for more loads in flight; measured 128^3 FP16 collide
+// 47.4 -> 46.4 us.
 template <class S, class P, int PARITY, bool SOL, bool GEN>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, Stor<S>::bytes == 2 ? 5 : 1)
     k_dend_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
                    P* __restrict__ temp, const unsigned char* __restrict__ grain,
                    const typename Stor<S>::T* __restrict__ rot, const Geom g, const DendK<typename Stor<S>::T> k) {
