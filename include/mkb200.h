@@ -74,8 +74,9 @@ typedef enum mk_model {
 } mk_model;
 
 /* Population storage precision.  Collision arithmetic is FP64 for MK_PREC_FP64
- * and FP32 otherwise.  FP16/BF16 store the deviation from the rest state
- * ("shifted storage"). */
+ * and FP32 otherwise (FP32 divisions by densities, gradient norms and
+ * capacities use the fast approximate division, about two ulp).  FP16/BF16
+ * store the deviation from the rest state ("shifted storage"). */
 typedef enum mk_precision {
   MK_PREC_FP64 = 0,
   MK_PREC_FP32 = 1,
