@@ -142,7 +142,7 @@ typedef enum mk_dtype {
 #define MK_MAX_OBJECTS 64
 
 /* Every resolved number of a case, in lattice units.  Filled from the
- * BoltzTechs XML (tags listed in DESIGN.md) plus the optional <b200> block. */
+ * BoltzTechs XML tags the reference's cases use plus the optional <b200> block. */
 typedef struct mk_params {
   int32_t model;      /* mk_model */
   int32_t lattice;    /* flow lattice (D3Q19/D3Q27); scalar lattices are D3Q7 */
