@@ -137,3 +137,17 @@ def test_reference_call_sequence(casedir):
         assert np.array_equal(flow.solver.field(f), ref.field(f))
     with pytest.raises(A.MkError):
         flow.thermal_propagate()
+
+
+def test_flow_dendrite_vtk_has_flow_and_flags(casedir, tmp_path):
+    p = case_params(cases.write(_case("fp32"), f"{casedir}/fd_vtk.xml"))
+    s = Solver(params=p)
+    s.advance(10)
+    text = open(s.write_vtk(10, str(tmp_path))).read()
+    assert "VECTORS velocity_vector float" in text and "SCALARS temperature float 1" in text
+    vel = text.split("VECTORS velocity_vector float\n")[1].split()
+    ux = np.array(vel[0::3], dtype=float).reshape(s.shape)
+    assert np.allclose(ux, s.field("ux"), rtol=1e-5, atol=1e-7)
+    flag = s.field("flag")
+    assert set(np.unique(flag)) <= {A.MK_FLAG_FLUID, A.MK_FLAG_SOLID}
+    assert np.array_equal(flag == A.MK_FLAG_SOLID, s.field("phi") > 0)

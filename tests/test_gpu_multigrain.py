@@ -91,3 +91,18 @@ def test_reference_call_sequence(casedir):
     for j in range(3):
         assert np.array_equal(flow.solver.grain_field(j), ref.grain_field(j))
     assert np.array_equal(flow.solver.field("T"), ref.field("T"))
+
+
+def test_multigrain_vtk_and_contour(casedir, tmp_path):
+    p = case_params(cases.write(_case("fp32"), f"{casedir}/mg_vtk.xml"))
+    s = Solver(params=p)
+    s.advance(4)
+    path = s.write_vtk(4, str(tmp_path))
+    text = open(path).read()
+    for name in ("order_parameter", "grain_id", "temperature", "delta_order_parameter"):
+        assert f"SCALARS {name} float 1" in text
+    # the grain ids written are those of the grain field
+    block = text.split("SCALARS grain_id float 1\nLOOKUP_TABLE default\n")[1].split("SCALARS")[0].split()
+    assert np.array_equal(np.array(block, dtype=float).reshape(s.shape), s.field("grain"))
+    pts = s.interface_points()
+    assert pts["iso"] == 0.0 and len(pts["xyz"]) > 100
