@@ -104,3 +104,18 @@ def test_multiphase_and_flow(casedir):
     f = Solver(params=q)
     with pytest.raises(A.MkError):
         f.interface_points()
+
+
+def test_contour_partial_capacity(casedir):
+    # a buffer smaller than the point count receives the first points and the
+    # full count comes back
+    import ctypes as C
+    p, s = _dend(casedir, "fp32", n=24)
+    s.advance(20)
+    full = s.interface_points()
+    n = C.c_int64()
+    xyz = np.zeros((10, 3))
+    dp = C.POINTER(C.c_double)
+    st = A.load().mk_interface_points(s.handle, 0.0, xyz.ctypes.data_as(dp), None, 10, C.byref(n))
+    assert st == A.MK_OK and n.value == len(full["xyz"]) > 10
+    assert np.array_equal(xyz, full["xyz"][:10])
