@@ -26,8 +26,17 @@ __device__ __forceinline__ void pf_phi_cell(const S* __restrict__ G, P* __restri
                                             const NB& nb, const int c, const typename Stor<S>::T ref_g) {
   typedef typename Stor<S>::T T;
   T s = T(0);
+  if constexpr (Stor<S>::scaled) {
+    // 16-bit storage holds f'/w: sum each weight class in stored units and
+    // scale once per class (2 multiplies instead of 7)
+    T sa = T(0);
 #pragma unroll
-  for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, stride, nb, PARITY, c, i);
+    for (int i = 1; i < 7; ++i) sa += ld_in_raw<S, 7>(G, stride, nb, PARITY, c, i);
+    s = T(wq<7>(0)) * ld_in_raw<S, 7>(G, stride, nb, PARITY, c, 0) + T(wq<7>(1)) * sa;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) s += ld_in<S, 7>(G, stride, nb, PARITY, c, i);
+  }
   phi_new[c] = P(ref_g + s);
 }
 

@@ -239,8 +239,19 @@ __device__ __forceinline__ void mp_phi_cell(const S* __restrict__ H, const float
                                             int64_t stride, const NB& nb, int c, typename Stor<S>::T ref_h) {
   typedef typename Stor<S>::T T;
   T s = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
+  if constexpr (Stor<S>::scaled) {
+    // 16-bit storage holds h'/w: sum the axis and the diagonal classes in
+    // stored units and scale once per class (2 multiplies instead of 18)
+    T sa = T(0), sd = T(0);
 #pragma unroll
-  for (int i = 1; i < 19; ++i) s += ld_in<S, 19>(H, stride, nb, PARITY, c, i);
+    for (int i = 1; i < 7; ++i) sa += ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
+#pragma unroll
+    for (int i = 7; i < 19; ++i) sd += ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
+    s += T(wq<19>(1)) * sa + T(wq<19>(7)) * sd;
+  } else {
+#pragma unroll
+    for (int i = 1; i < 19; ++i) s += ld_in<S, 19>(H, stride, nb, PARITY, c, i);
+  }
   phi[c] = P(ref_h + s);
 }
 
@@ -805,8 +816,15 @@ __device__ __forceinline__ void mg_phi_cell(const S* __restrict__ G, P* __restri
   for (int j = 0; j < ngr; ++j) {
     const S* Gj = G + (int64_t)j * 7 * stride;
     T sum = T(-1);
+    if constexpr (Stor<S>::scaled) {  // stored units, one multiply per weight class
+      T sa = T(0);
 #pragma unroll
-    for (int i = 0; i < 7; ++i) sum += ld_in<S, 7>(Gj, stride, nb, PARITY, c, i);
+      for (int i = 1; i < 7; ++i) sa += ld_in_raw<S, 7>(Gj, stride, nb, PARITY, c, i);
+      sum += T(wq<7>(0)) * ld_in_raw<S, 7>(Gj, stride, nb, PARITY, c, 0) + T(wq<7>(1)) * sa;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 7; ++i) sum += ld_in<S, 7>(Gj, stride, nb, PARITY, c, i);
+    }
     phij[(int64_t)j * ncell + c] = P(sum);
     agg += sum;
   }
