@@ -217,27 +217,45 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
   const T B1 = -cs2 * ((a * a - T(1)) * gr[1] + N[1]);
   const T B2 = -cs2 * ((a * a - T(1)) * gr[2] + N[2]);
   const T fo = (T(1) - T(0.5) * k.om_g) / cs2;
+  // SU: 16-bit storage holds f'/w; both lattices are then updated in those
+  // stored units (every term of the BGK/TRT updates below carries the factor
+  // w_i, so dividing by it leaves no weights to apply per population), and
+  // the weight enters only the class sum of T.  Off with the face pass.
+  constexpr bool SU = Stor<S>::scaled && !NEE;
   // phase-field lattice, all seven loaded before any store (in-place safety)
   T gv[7];
 #pragma unroll
-  for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(G, stride, nb, PARITY, c, i);
+  for (int i = 0; i < 7; ++i)
+    gv[i] = SU ? ld_in_raw<S, 7>(G, stride, nb, PARITY, c, i) : ld_in<S, 7>(G, stride, nb, PARITY, c, i);
   const T dph = ph - k.ref_g;
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
-    const T w = T(wq<7>(i));
+    const T w = SU ? T(1) : T(wq<7>(i));
     const T eB = T(ex(i)) * B0 + T(ey(i)) * B1 + T(ez(i)) * B2;
     const T go = gv[i] - k.om_g * (gv[i] - w * dph) + fo * w * eB + w * src;
     if constexpr (NEE)
       gv[i] = go;  // stored after the face pass below
+    else if constexpr (SU)
+      st_out_raw<S, 7>(G, stride, nb, PARITY, c, i, go);
     else
       st_out<S, 7>(G, stride, nb, PARITY, c, i, go);
   }
   T t[7];
   T dT = T(0);
+  if constexpr (SU) {
+    T sa = T(0);
 #pragma unroll
-  for (int i = 0; i < 7; ++i) {
-    t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
-    dT += t[i];
+    for (int i = 0; i < 7; ++i) {
+      t[i] = ld_in_raw<S, 7>(Tp, stride, nb, PARITY, c, i);
+      if (i > 0) sa += t[i];
+    }
+    dT = T(wq<7>(0)) * t[0] + T(wq<7>(1)) * sa;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
+      dT += t[i];
+    }
   }
   if constexpr (SOL) {
     // solutal lattice (TRT): capacity c(phi) applied to D(phi), the
@@ -256,26 +274,34 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
     const T cD = k.D_l * (T(1) - ph) * T(0.5) + k.D_s * (T(1) + ph) * T(0.5);
     const T om = div_fast(cap, T(4) * cD + T(0.5) * cap);
     {
-      const T w0 = T(wq<7>(0));
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
+      const T w0 = SU ? T(1) : T(wq<7>(0));
+      if constexpr (SU)
+        st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
+      else
+        st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
     }
 #pragma unroll
     for (int i = 1; i < 7; i += 2) {
       const int j = i + 1;
-      const T w = T(wq<7>(i));
+      const T w = SU ? T(1) : T(wq<7>(i));
       const T ej = fj * (T(ex(i)) * gr[0] + T(ey(i)) * gr[1] + T(ez(i)) * gr[2]);
       const T sym = w * dT;
       const T am = T(0.5) * (t[i] - t[j]);
       const T am_new = am - om * (am - w * T(4) * ej);
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
-      st_out<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
+      if constexpr (SU) {
+        st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
+        st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
+      } else {
+        st_out<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
+        st_out<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
+      }
     }
   } else {
     // thermal lattice: relaxation with latent heat (1/2) dphi
     const T lat = T(0.5) * dphi;
 #pragma unroll
     for (int i = 0; i < 7; ++i) {
-      const T w = T(wq<7>(i));
+      const T w = SU ? T(1) : T(wq<7>(i));
       T eq = dT;
       if constexpr (ADV) {
         const T eu = T(ex(i)) * vx + T(ey(i)) * vy + T(ez(i)) * vz;
@@ -284,6 +310,8 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
       const T to = t[i] - k.om_t * (t[i] - w * eq) + w * lat;
       if constexpr (NEE)
         t[i] = to;
+      else if constexpr (SU)
+        st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, i, to);
       else
         st_out<S, 7>(Tp, stride, nb, PARITY, c, i, to);
     }
