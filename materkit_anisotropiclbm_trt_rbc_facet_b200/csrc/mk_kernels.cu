@@ -515,17 +515,41 @@ struct FdK {
 // -rho w_i P_i), is the Noble-Torczynski form with f_i cancelled; it is
 // evaluated only when a lane of the warp has B > 0.  FORCE = false drops the
 // force terms (a zero body force).
-template <class T, int Q, int COLL, bool FORCE>
-__device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T ns, const T half, T& ux, T& uy,
-                                         T& uz) {
-  T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
+// Mass and momentum deviations of Q populations; SC: f holds f'/w (16-bit
+// stored units), summed per weight class and scaled once per class.
+__host__ __device__ constexpr int wclass_rep(int i) { return i == 0 ? 0 : (i <= 6 ? 1 : (i <= 18 ? 7 : 19)); }
+
+template <class T, int Q, bool SC>
+__device__ __forceinline__ void flow_moments(const T (&f)[Q], T& drho, T& jx, T& jy, T& jz) {
+  T d[4] = {T(0), T(0), T(0), T(0)}, x[4] = {T(0), T(0), T(0), T(0)}, y[4] = {T(0), T(0), T(0), T(0)},
+    z[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    drho += f[i];
-    if (ex(i)) jx += T(ex(i)) * f[i];
-    if (ey(i)) jy += T(ey(i)) * f[i];
-    if (ez(i)) jz += T(ez(i)) * f[i];
+    const int c = SC ? (i == 0 ? 0 : (i <= 6 ? 1 : (i <= 18 ? 2 : 3))) : 0;
+    d[c] += f[i];
+    if (ex(i)) x[c] += T(ex(i)) * f[i];
+    if (ey(i)) y[c] += T(ey(i)) * f[i];
+    if (ez(i)) z[c] += T(ez(i)) * f[i];
   }
+  if constexpr (SC) {
+    const T w0 = T(wq<Q>(0)), w1 = T(wq<Q>(1)), w2 = T(wq<Q>(7)), w3 = Q == 27 ? T(wq<Q>(19)) : T(0);
+    drho = w0 * d[0] + w1 * d[1] + w2 * d[2] + w3 * d[3];
+    jx = w1 * x[1] + w2 * x[2] + w3 * x[3];
+    jy = w1 * y[1] + w2 * y[2] + w3 * y[3];
+    jz = w1 * z[1] + w2 * z[2] + w3 * z[3];
+  } else {
+    drho = d[0];
+    jx = x[0];
+    jy = y[0];
+    jz = z[0];
+  }
+}
+
+template <class T, int Q, int COLL, bool FORCE, bool SC = false>
+__device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T ns, const T half, T& ux, T& uy,
+                                         T& uz) {
+  T drho, jx, jy, jz;
+  flow_moments<T, Q, SC>(f, drho, jx, jy, jz);
   const T rho = k.ref + drho;
   const T irho = div_fast(T(1), rho);
   ux = FORCE ? (jx + T(0.5) * k.Fx) * irho : jx * irho;
@@ -541,7 +565,7 @@ __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T n
   const bool psm = __any_sync(__activemask(), B > T(0));
   const T base = drho - T(1.5) * rho * uu;  // symmetric equilibrium part / w, less the 4.5 eu^2 term
   {
-    const T w = T(wq<Q>(0));
+    const T w = SC ? T(1) : T(wq<Q>(0));  // SC: every term below carries w, divided out
     T fc = f[0] - om_p * (f[0] - w * base);
     if (FORCE) fc += gp * w * T(-3) * uF;
     if (psm) fc += B * (f[0] - rho * w * T(-1.5) * uu - fc);
@@ -550,7 +574,7 @@ __device__ __forceinline__ void fd_relax(T (&f)[Q], const FlowK<T>& k, const T n
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
     const int j = i + 1;
-    const T w = T(wq<Q>(i));
+    const T w = SC ? T(1) : T(wq<Q>(i));
     const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
     const T fp = T(0.5) * (f[i] + f[j]), fm = T(0.5) * (f[i] - f[j]);
     const T ep = w * (base + T(4.5) * rho * eu * eu), em = w * T(3) * rho * eu;
@@ -585,9 +609,13 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
                                              const int64_t stride, const int64_t ncell, const NB& nb, const int c,
                                              const int x, const int nx, const FdK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
-  T f[Q];  // deviations f_i - w_i rho0, post-collision after the relaxation
+  // SC: 16-bit storage with BGK/TRT works in the stored units f'/w (the
+  // weights enter only the class sums of the moments)
+  constexpr bool SC = Stor<S>::scaled && COLL != MK_COLL_MRT;
+  T f[Q];  // deviations f_i - w_i rho0 (or f'/w), post-collision after the relaxation
 #pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = ld_in<S, Q>(W, stride, nb, PARITY, c, i);
+  for (int i = 0; i < Q; ++i)
+    f[i] = SC ? ld_in_raw<S, Q>(W, stride, nb, PARITY, c, i) : ld_in<S, Q>(W, stride, nb, PARITY, c, i);
   T ux, uy, uz;
   const T ns = fmin(T(1), fmax(T(0), T(0.5) * (T(1) + T(phi_old[c]))));
   if constexpr (COLL == MK_COLL_MRT && Q == 19) {
@@ -607,7 +635,7 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
       }
     }
   } else {
-    fd_relax<T, Q, COLL, FORCE>(f, k.f, ns, k.half, ux, uy, uz);
+    fd_relax<T, Q, COLL, FORCE, SC>(f, k.f, ns, k.half, ux, uy, uz);
   }
   if constexpr (NEE) {
     // inflow / outflow faces in registers: the cell at x = 0 (x = nx - 1)
@@ -622,14 +650,8 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
       const int src = x == 0 ? lane + 1 : lane - 1;
       // every lane sums its own post-collision moments; the face lanes take
       // their neighbour's four sums, then its populations one by one
-      T drho = T(0), jx = T(0), jy = T(0), jz = T(0);
-#pragma unroll
-      for (int i = 0; i < Q; ++i) {
-        drho += f[i];
-        if (ex(i)) jx += T(ex(i)) * f[i];
-        if (ey(i)) jy += T(ey(i)) * f[i];
-        if (ez(i)) jz += T(ez(i)) * f[i];
-      }
+      T drho, jx, jy, jz;
+      flow_moments<T, Q, SC>(f, drho, jx, jy, jz);
       drho = __shfl_sync(act, drho, src);
       jx = __shfl_sync(act, jx, src);
       jy = __shfl_sync(act, jy, src);
@@ -645,7 +667,7 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
       for (int i = 0; i < Q; ++i) {
         const T v = __shfl_sync(act, f[i], src);
         if (edge) {
-          const T w = T(wq<Q>(i));
+          const T w = SC ? T(1) : T(wq<Q>(i));
           const T eun = T(ex(i)) * un[0] + T(ey(i)) * un[1] + T(ez(i)) * un[2];
           const T eub = T(ex(i)) * ub[0] + T(ey(i)) * ub[1] + T(ez(i)) * ub[2];
           f[i] = v + w * ((rb - rn) + rb * (T(3) * eub + T(4.5) * eub * eub - T(1.5) * uub) -
@@ -660,7 +682,12 @@ __device__ __forceinline__ void fd_flow_cell(S* __restrict__ W, const P* __restr
     }
   }
 #pragma unroll
-  for (int i = 0; i < Q; ++i) st_out<S, Q>(W, stride, nb, PARITY, c, i, f[i]);
+  for (int i = 0; i < Q; ++i) {
+    if constexpr (SC)
+      st_out_raw<S, Q>(W, stride, nb, PARITY, c, i, f[i]);
+    else
+      st_out<S, Q>(W, stride, nb, PARITY, c, i, f[i]);
+  }
   vel[c] = P(ux);
   vel[ncell + c] = P(uy);
   vel[2 * ncell + c] = P(uz);
