@@ -520,18 +520,14 @@ def run_ensemble(args):
 
 def _oracle_case(workload: str, n: int):
     """FP64 parameters and initial fields of the workload's CPU sample (the
-    ensemble's sample is its first domain)."""
-    from materkit_anisotropiclbm_trt_rbc_facet_b200 import case_params, ensemble_params, initial_field
+    ensemble's sample is its first domain), from the oracle's own case layer:
+    the CPU arms never load the CUDA library."""
+    from oracle import case as ocase
     if workload == "ensemble":
-        params = ensemble_params(ENSEMBLE_SEED, 1, "fp64")[0]
+        params = ocase.ensemble(ENSEMBLE_SEED, 1, "fp64")[0]
     else:
-        params = case_params(_case_path("fp64", n, workload))
-    dend = workload != "bubbles"
-    fields = {"phi": initial_field(params, "phi")}
-    if dend:
-        fields["T"] = initial_field(params, "T")
-        fields["Cc"] = initial_field(params, "C")
-    return params, fields
+        params = ocase.resolve(_case_path("fp64", n, workload))
+    return params, ocase.oracle_fields(params)
 
 
 def _sample_name(workload: str, n: int) -> str:
@@ -542,8 +538,7 @@ def _sample_name(workload: str, n: int) -> str:
 
 def cpu_baseline(n: int, budget_s: float = 20.0, workload: str = "bubbles"):
     """Time the FP64 OpenMP oracle on the host cores on a bounded sample of the workload."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from _oracle import Oracle, load as load_oracle
+    from oracle.orc import Oracle, load as load_oracle
 
     lib = load_oracle()
     params, fields = _oracle_case(workload, n)
@@ -567,8 +562,7 @@ def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from _oracle import Oracle, load as load_oracle
+    from oracle.orc import Oracle, load as load_oracle
 
     lib = load_oracle()
     n = args.size
@@ -603,6 +597,50 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_accuracy(args):
+    """Reduced-precision accuracy of the bubble case at full size: the case
+    advanced `--accuracy-loops` loops (default 10,000) with FP64, FP32, FP16
+    and BF16 storage; each reduced precision against the FP64 run (which
+    equals the CPU oracle to 1e-10, tests/test_gpu_parity_at_size.py): phi
+    relative L2 error and largest absolute error over the fluid cells, and
+    the relative drift of the conserved phi sum.  Prints one JSON line."""
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, case_params
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
+
+    lib = A.load()
+    st = lib.mk_set_device(0)
+    if st != A.MK_OK:
+        raise A.MkError(st, lib.mk_last_global_error().decode())
+    n, loops = args.size, args.accuracy_loops
+    out, ref = {}, None
+    for prec in ("fp64", "fp32", "fp16", "bf16"):
+        params = case_params(_case_path(prec, n, "bubbles"))
+        s = Solver(params=params)
+        d0 = s.diagnostics()
+        t0 = time.perf_counter()
+        s.advance(loops, graph=True)
+        s.sync()
+        secs = time.perf_counter() - t0
+        d1 = s.diagnostics(raise_on_divergence=False)
+        phi = s.field("phi")
+        fluid = np.ones(phi.shape, dtype=bool)
+        fluid[0], fluid[-1] = False, False  # the z walls
+        drift = abs(d1["phi_sum"] - d0["phi_sum"]) / abs(d0["phi_sum"])
+        if ref is None:
+            ref = phi
+            out[prec] = {"phi_sum_drift": drift, "n_bad": d1["n_bad"], "seconds": round(secs, 2)}
+        else:
+            diff = (phi - ref)[fluid]
+            out[prec] = {"phi_rel_l2": float(np.linalg.norm(diff) / np.linalg.norm(ref[fluid])),
+                         "phi_max_abs_err": float(np.max(np.abs(diff))), "phi_sum_drift": drift,
+                         "n_bad": d1["n_bad"], "seconds": round(secs, 2)}
+        s.close()
+    line = {"metric": "reduced-precision accuracy vs FP64 storage", "workload":
+            WORKLOADS["bubbles"]["workload"].format(n=n), "loops": loops, "cells": n ** 3,
+            "reference": "FP64 storage on the device (equal to the CPU oracle to 1e-10)", "results": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -617,6 +655,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--accuracy", action="store_true",
+                    help="reduced-precision accuracy of the bubble case vs FP64 storage (not a timing run)")
+    ap.add_argument("--accuracy-loops", type=int, default=10000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -625,7 +666,9 @@ def main():
         args.precision = wl["precision"]
     if args.size is None:
         args.size = wl["size"]
-    if args.impl == "reference":
+    if args.accuracy:
+        run_accuracy(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble(args)

@@ -256,7 +256,10 @@ const char* mk_last_global_error(void);
 mk_status mk_read_parameters(const char* xml_path, int32_t* max_loops, int32_t* max_frames);
 
 /* Resolve a case to its parameters without touching a GPU
- * (= mkSpace(xml) + reset + read_parameters, MaterKit/inc/mkFluidsLBM.h:37,42). */
+ * (= mkSpace(xml) + reset + read_parameters, MaterKit/inc/mkFluidsLBM.h:37,42).
+ * A <seed> whose <center> holds fewer than 3 * <number> values places the
+ * seeds with a complete centre triple (n_objects = the count of full triples);
+ * a short <radius> list repeats its last value, a short <angle> list gives 0. */
 mk_status mk_case_params(const char* xml_path, const mk_options* opt, mk_params* out);
 
 /* Host-side initial state of a case (= initialize + initialize_geometry,

@@ -112,6 +112,9 @@ int parse_bc(const std::string& t) {
 
 // Seeds of <phasechange><seed> (BoltzTechs - thermal.xml:65-77): number,
 // center triples (lattice units), angle triples (degrees, ZYX), radius.
+// A centre list shorter than 3 * number places only the seeds whose centre
+// is complete (the shipped BoltzTechs - solutal.xml declares 2 seeds and
+// gives one centre): number is reduced to the count of full triples.
 bool read_seeds(const mkx::Element* seed, mk_params* p, std::string& err) {
   if (!seed) return true;
   int number = 0;
@@ -123,10 +126,7 @@ bool read_seeds(const mkx::Element* seed, mk_params* p, std::string& err) {
   }
   std::vector<double> c, a, r;
   if (!opt_v(seed, "center", c, err) || !opt_v(seed, "angle", a, err) || !opt_v(seed, "radius", r, err)) return false;
-  if ((int)c.size() < 3 * number) {
-    err = "seed/center has fewer than 3*number values";
-    return false;
-  }
+  number = std::min(number, (int)c.size() / 3);
   p->n_objects = number;
   for (int k = 0; k < number; ++k) {
     for (int d = 0; d < 3; ++d) {

@@ -11,7 +11,7 @@ relative agreement <= 1e-4.
 import numpy as np
 import pytest
 
-from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params, initial_field
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params
 from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
 from _oracle import Oracle
 
@@ -62,7 +62,7 @@ def test_device_adjoint_equals_oracle_adjoint(casedir, aniso, e2):
     p = _params(casedir, n, 0.05, 0.55, aniso=aniso, eps2=e2)
     s = Solver(params=p)
     g = s.backward(target, steps, checkpoint_every=6)  # 4 segments, the last one partial
-    o = Oracle(p, phi=initial_field(p, "phi"), T=initial_field(p, "T"))
+    o = Oracle.from_case(p)  # the oracle's own initial fields of the same parameters
     r = o.backward(target, steps)
     for k in ("loss", "d_eps4", "d_delta", "d_tau_t"):
         assert g[k] == pytest.approx(r[k], rel=1e-9, abs=1e-12), (k, g[k], r[k])

@@ -10,7 +10,7 @@ import pytest
 
 from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, cases, case_params, initial_field
 from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
-from _oracle import Oracle, rel_l2
+from _oracle import Oracle, ocase, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -18,14 +18,17 @@ FP64_TOL = 1e-10
 
 
 def _pair(casedir, name, text, **opt):
-    p = case_params(cases.write(text, f"{casedir}/{name}.xml"), **opt)
+    """The library and the oracle on one XML file, each through its own case
+    layer (parameters and initial fields resolved independently)."""
+    path = cases.write(text, f"{casedir}/{name}.xml")
+    p = case_params(path, **opt)
     s = Solver(params=p)
-    o = Oracle(p, phi=initial_field(p, "phi"), T=initial_field(p, "T"), Cc=initial_field(p, "C"))
+    o = Oracle.from_xml(path, **opt)
     return p, s, o
 
 
 def _fluid(p):
-    return initial_field(p, "flag") == 0
+    return ocase.flags(p) == 0
 
 
 # Per-cell magnitude below which a field counts as "still zero": the

@@ -2,14 +2,17 @@
 
 The FP64 device path equals the CPU oracle to 1e-10 (test_gpu_parity); over
 10,000 loops the oracle is too slow, so the reduced-precision runs are measured
-against the FP64 device run of the same case.  Each line states the phi
-relative L2 error and the drift of the conserved phi sum.
+against the FP64 device run of the same case.  Each precision states and
+bounds three numbers: the phi relative L2 error, the largest absolute phi
+error (phi is in [0, 1]) and the relative drift of the conserved phi sum.
+The headline-size figures (256^3, 10,000 loops) come from
+``python bench.py --accuracy``.
 """
 import numpy as np
 import pytest
 
-from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, case_params, cases, initial_field
-from _oracle import rel_l2
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, case_params, cases
+from _oracle import ocase, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -31,21 +34,32 @@ def fp64_run(tmp_path_factory):
     return p, s.field("phi"), d0, s.diagnostics(), str(d)
 
 
-# phi relative L2 bounds after 10k loops: 1e-3 is the goal for the shifted
-# 16-bit storage (measured FP32 2.5e-4, FP16 3.0e-4, BF16 6.7e-4 with the FP32
-# rest population carrying the rounding residual).
-@pytest.mark.parametrize("prec,bound", [("fp32", 6e-4), ("fp16", 1e-3), ("bf16", 1.5e-3)])
-def test_shifted_storage_accuracy_10k(fp64_run, prec, bound):
+# Goal: relative L2 <= 1e-3 after 10k loops for every storage.  The phi-sum
+# drift is bounded by the FP32 rounding of the sum's increments: the 16-bit
+# storage keeps the Allen-Cahn rest population in FP32, which absorbs the
+# rounding residual of the 18 moving populations.
+BOUNDS = {"fp32": (1e-3, 2e-2, 1e-5), "fp16": (1e-3, 2e-2, 1e-5), "bf16": (1e-3, 5e-2, 1e-5)}
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16", "bf16"])
+def test_shifted_storage_accuracy_10k(fp64_run, prec):
     p64, phi64, d0_64, d1_64, d = fp64_run
     p = case_params(cases.write(_case(prec), f"{d}/p_{prec}.xml"))
     s = Solver(params=p)
     d0 = s.diagnostics()
     s.advance(STEPS, graph=True)
     d1 = s.diagnostics()
-    fl = initial_field(p, "flag") == 0
-    err = rel_l2(s.field("phi"), phi64, fl)
+    fl = ocase.flags(p) == 0
+    phi = s.field("phi")
+    err = rel_l2(phi, phi64, fl)
+    emax = float(np.max(np.abs(phi - phi64)[fl]))
     drift = abs(d1["phi_sum"] - d0["phi_sum"]) / d0["phi_sum"]
-    print(f"{prec}: phi rel L2 vs FP64 after {STEPS} loops = {err:.3e}, phi-sum drift = {drift:.3e}, "
-          f"FP64 drift = {abs(d1_64['phi_sum'] - d0_64['phi_sum']) / d0_64['phi_sum']:.3e}")
+    drift64 = abs(d1_64["phi_sum"] - d0_64["phi_sum"]) / d0_64["phi_sum"]
+    print(f"{prec}: after {STEPS} loops phi rel L2 {err:.3e}, max |err| {emax:.3e}, phi-sum drift {drift:.3e} "
+          f"(FP64 drift {drift64:.3e})")
+    l2_bound, max_bound, drift_bound = BOUNDS[prec]
     assert d1["n_bad"] == 0
-    assert err <= bound, err
+    assert err <= l2_bound, err
+    assert emax <= max_bound, emax
+    assert drift <= drift_bound, drift
+    assert drift64 <= 1e-12, drift64

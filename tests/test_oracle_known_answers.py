@@ -6,7 +6,8 @@ pinned by analytic solutions and exact invariants of the method instead.
 import numpy as np
 import pytest
 
-from materkit_anisotropiclbm_trt_rbc_facet_b200 import cases, case_params, initial_field
+from materkit_anisotropiclbm_trt_rbc_facet_b200 import cases
+from oracle.case import initial_field, resolve as case_params
 from materkit_anisotropiclbm_trt_rbc_facet_b200 import _abi as A
 from _oracle import Oracle
 

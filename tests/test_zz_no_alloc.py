@@ -62,3 +62,29 @@ def test_noalloc_rejects_oversize_and_counts_nonfinite():
     torch.cuda.synchronize()
     got = out.cpu().numpy()
     assert got[0] == 2.5 and got[1] == 1.0 + 4.0 + 12.25 and got[2] == -2.0 and got[3] == 3.5 and got[4] == 2.0
+
+
+def test_noalloc_small_call_after_large_and_empty():
+    # a small call right after a large one must not read the block partials
+    # the large call left in the shared scratch; n = 0 gives the empty statistics
+    import torch
+
+    lib = A.load()
+    out = torch.zeros(5, dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(7)
+    big = rng.standard_normal(5_000_000).astype(np.float32)  # clamps to the full 2048 partial blocks
+    small = rng.standard_normal(1000).astype(np.float32) + 3.0  # 4 blocks
+    for host in (big, small, big[:257], small):
+        dev = torch.from_numpy(host).to("cuda")
+        torch.cuda.synchronize()
+        _stats(lib, dev, host.size, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        ref = host.astype(np.float64)
+        assert abs(got[0] - ref.sum()) <= 1e-12 * np.abs(ref).sum(), (host.size, got[0], ref.sum())
+        assert abs(got[1] - (ref * ref).sum()) <= 1e-12 * (ref * ref).sum()
+        assert got[2] == ref.min() and got[3] == ref.max() and got[4] == 0.0
+    _stats(lib, out, 0, out)  # the field pointer is not read when n = 0
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert got[0] == 0.0 and got[1] == 0.0 and got[2] == np.inf and got[3] == -np.inf and got[4] == 0.0
