@@ -278,11 +278,32 @@ mk_status mk_get_params(const mk_handle* h, mk_params* out);
 int64_t mk_get_step(const mk_handle* h);
 
 /* Advance n loops of the coupled step (propagate + relaxation of every field in
- * the reference's per-loop order).  Asynchronous on the handle's stream. */
+ * the reference's per-loop order).  Asynchronous on the handle's stream.
+ * A multiphase case runs each loop as one cooperative launch whose tiles
+ * exchange phi planes through flags with bounded waits, when the case admits
+ * it (x extent a multiple of 4, at least 8 planes in z), else as a phi kernel
+ * plus a collision kernel; the two forms give the same result. */
 mk_status mk_advance(mk_handle* h, int64_t nsteps);
 /* Capture the per-loop launches in a CUDA graph and replay it n times. */
 mk_status mk_advance_graph(mk_handle* h, int64_t nsteps);
+/* Wait for the handle's stream.  MK_ERR_TIMEOUT when a bounded device wait of
+ * the fused multiphase loop ran out since the last check (the loops since
+ * then are invalid; the handle stays usable). */
 mk_status mk_sync(mk_handle* h);
+/* Loop form of a multiphase case: 1 the fused one-launch loop with one
+ * producer warp per CTA (the default when the case admits it), 2 the fused
+ * loop in which every warp computes phi and collides, 0 the phi kernel plus
+ * the collision kernel.  MK_ERR_ARG when 1 or 2 is asked of a case that does
+ * not admit the fused loop.  The autotuner may change the form; mk_get_fused
+ * reports the current one. */
+mk_status mk_set_fused(mk_handle* h, int32_t fused);
+int32_t mk_get_fused(const mk_handle* h);
+/* Test hook of the failure detection, no counterpart in the reference.
+ * kind 1: in the next loop of a fused multiphase case one tile publishes none
+ * of its phi planes, so its neighbours' bounded waits run out (about a second)
+ * and the next mk_sync / mk_diagnostics returns MK_ERR_TIMEOUT.  Nothing
+ * faults or hangs.  MK_ERR_ARG for other kinds or cases without the fused loop. */
+mk_status mk_inject_fault(mk_handle* h, int32_t kind);
 /* The handle's cudaStream_t, for event timing by the caller. */
 mk_status mk_get_stream(mk_handle* h, void** stream);
 
@@ -344,9 +365,10 @@ mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel,
 mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, double* ms);
 
 /* Launch-shape autotuner: times `trial_steps` loops of each candidate block
- * shape and occupancy variant of the step's kernels on a saved copy of the
- * state (restored afterwards, so the simulation is unchanged) and keeps the
- * fastest.  Outputs may be NULL. */
+ * shape and occupancy variant of the step's kernels, and for a multiphase
+ * case also the fused one-launch loop, on a saved copy of the state (restored
+ * afterwards, so the simulation is unchanged) and keeps the fastest.  Outputs
+ * may be NULL; block_x = block_y = minb = 0 report that the fused loop won. */
 mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32_t* block_y, int32_t* minb,
                       double* ms_per_step);
 
@@ -419,7 +441,9 @@ int64_t mk_ensemble_step(const mk_ensemble* e);
  * mk_noalloc_last_error).  Every call on a device shares that array: calls
  * that overlap on the GPU race and must be serialised by the caller.  The
  * first call on a device looks up the array's address and should come before
- * any stream capture.  Calls no allocating routine. */
+ * any stream capture; the address is kept for the life of the process, so no
+ * call may follow a cudaDeviceReset of that device.  Calls no allocating
+ * routine. */
 #define MK_NOALLOC_MAX_BLOCKS 2048
 #define MK_NOALLOC_MAX_CELLS ((int64_t)MK_NOALLOC_MAX_BLOCKS * 256 * 64)
 mk_status mk_field_stats_noalloc(const float* d_field, int64_t n, double* d_out, void* stream);

@@ -131,6 +131,9 @@ PROTOTYPES = {
     "mk_advance": (C.c_int, [H, C.c_int64]),
     "mk_advance_graph": (C.c_int, [H, C.c_int64]),
     "mk_sync": (C.c_int, [H]),
+    "mk_inject_fault": (C.c_int, [H, C.c_int32]),
+    "mk_set_fused": (C.c_int, [H, C.c_int32]),
+    "mk_get_fused": (C.c_int32, [H]),
     "mk_get_stream": (C.c_int, [H, P(C.c_void_p)]),
     "mk_get_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),
     "mk_get_grain_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),

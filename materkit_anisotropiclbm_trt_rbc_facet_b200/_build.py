@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr",
                   "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
                   "-I", INCLUDE]
-SOURCES = ["mk_kernels.cu", "mk_ensemble.cu", "mk_adjoint.cu", "mk_noalloc.cu", "mk_interface.cu", "mk_api.cpp", "mk_case.cpp", "mk_xml.cpp"]
+SOURCES = ["mk_kernels.cu", "mk_multiphase.cu", "mk_ensemble.cu", "mk_adjoint.cu", "mk_noalloc.cu", "mk_interface.cu", "mk_api.cpp", "mk_case.cpp", "mk_xml.cpp"]
 
 
 def _nvcc() -> str:
@@ -42,11 +42,15 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def _compile(src: str, verbose: bool) -> str:
+def _compile(src: str, verbose: bool) -> tuple[str, bool]:
     obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
     path = os.path.join(CSRC, src)
-    if not _stale(obj, [path] + _headers()):
-        return obj
+    deps = [path] + _headers()
+    if not _stale(obj, deps):
+        return obj, False
+    # the object is stamped with its newest input's time as read before the
+    # compile starts, so a source edited while nvcc runs is seen as newer
+    stamp = max(os.path.getmtime(d) for d in deps)
     cmd = [_nvcc()] + NVFLAGS + ["-c", path, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [_nvcc(), "-x", "cu"] + NVFLAGS + ["-c", path, "-o", obj]
@@ -55,15 +59,17 @@ def _compile(src: str, verbose: bool) -> str:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
-    return obj
+    os.utime(obj, (stamp, stamp))
+    return obj, True
 
 
 def build(verbose: bool = False) -> str:
     """Build libmkb200.so if needed and return its path."""
     os.makedirs(OBJ, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
-    if _stale(LIB, objs):
+        done = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
+    objs = [o for o, _ in done]
+    if any(rebuilt for _, rebuilt in done) or _stale(LIB, objs):
         cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

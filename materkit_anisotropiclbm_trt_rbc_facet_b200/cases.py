@@ -96,16 +96,19 @@ def solutal_dendrite(n=64, ny=None, nz=None, loops=3000, precision="fp32", eps4=
 
 def multiphase_bubbles(n=256, nz=None, loops=10000, precision="fp32", bubbles=24, rmin=8.0, rmax=16.0,
                        seed=0xB200, width=4.0, sigma=1e-3, rho_ratio=10.0, nu_ratio=10.0, tau_l=0.8,
-                       mobility=0.05, gz=-1e-6, contact_angle=90.0) -> str:
+                       mobility=0.05, gz=-1e-6, contact_angle=90.0, ny=None,
+                       boundary="periodic periodic walls") -> str:
     """Config 3 (headline): 256^3 D3Q19 MRT + D3Q19 conservative Allen-Cahn, 24 bubbles.
 
     Liquid (phi = 1) density 1, gas density 1/rho_ratio; liquid kinematic
-    viscosity nu_l = (tau_l - 1/2)/3, gas nu_l / nu_ratio.
+    viscosity nu_l = (tau_l - 1/2)/3, gas nu_l / nu_ratio.  `ny` (default n)
+    and `boundary` (per axis x y z) reshape the box for tests.
     """
     nz = n if nz is None else nz
+    ny = n if ny is None else ny
     nu_l = (tau_l - 0.5) / 3.0
     tau_g = 3.0 * nu_l / nu_ratio + 0.5
-    return _HEADER.format(dendrite="false", flow="true", loops=loops, frames=min(loops, 100), nx=n, ny=n, nz=nz) + f"""
+    return _HEADER.format(dendrite="false", flow="true", loops=loops, frames=min(loops, 100), nx=n, ny=ny, nz=nz) + f"""
   <multiphases>
     <fluidDense> <kinematicViscosity> {nu_l} </kinematicViscosity> <density> 1.0 </density> </fluidDense>
     <fluidRare> <kinematicViscosity> {nu_l / nu_ratio} </kinematicViscosity> <density> {1.0 / rho_ratio} </density> </fluidRare>
@@ -114,7 +117,7 @@ def multiphase_bubbles(n=256, nz=None, loops=10000, precision="fp32", bubbles=24
   </multiphases>
   <b200>
     <model> multiphase </model> <collision> MRT </collision> <precision> {precision} </precision>
-    <boundary> periodic periodic walls </boundary>
+    <boundary> {boundary} </boundary>
     <rhoL> 1.0 </rhoL> <rhoG> {1.0 / rho_ratio} </rhoG> <tauL> {tau_l} </tauL> <tauG> {tau_g} </tauG>
     <sigma> {sigma} </sigma> <width> {width} </width> <mobility> {mobility} </mobility>
     <contactAngle> {contact_angle} </contactAngle> <force> 0.0 0.0 {gz} </force>

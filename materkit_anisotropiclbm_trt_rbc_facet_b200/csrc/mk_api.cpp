@@ -40,6 +40,9 @@ mk_status set_global(mk_status s, const std::string& m) {
 }
 
 mk_status cuda_fail(mk_handle* h, cudaError_t st, const char* where) {
+  // clear the runtime's last-error record (a failed allocation leaves it set,
+  // and a later launch check would report it again); sticky errors stay
+  cudaGetLastError();
   std::string m = std::string(where) + ": " + cudaGetErrorString(st);
   if (h) h->err = m;
   g_err = m;
@@ -214,12 +217,18 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
   if (!h || nsteps < 0) return MK_ERR_ARG;
   mke::Engine& e = h->e;
   int64_t left = nsteps;
+  if (left > 0 && e.wave_skip >= 0) {
+    // a pending test fault (mk_inject_fault) applies to one eager loop only
+    const mk_status s = mk_advance(h, 1);
+    if (s != MK_OK) return s;
+    --left;
+  }
   while (left >= 2) {
     const int par = (int)(e.step & 1);
-    if (!h->graph[par]) {
+    for (int attempt = 0; !h->graph[par]; ++attempt) {
       const int64_t step0 = e.step, l0 = e.launches;
       const int cur0 = e.phi_cur;
-      cudaGraph_t g;
+      cudaGraph_t g = nullptr;
       cudaError_t st = cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal);
       if (st != cudaSuccess) return cuda_fail(h, st, "capture begin");
       mke::engine_step(e, nullptr);
@@ -228,10 +237,25 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
       e.step = step0;
       e.launches = l0;
       e.phi_cur = cur0;
-      if (st != cudaSuccess) return cuda_fail(h, st, "capture end");
-      st = cudaGraphInstantiate(&h->graph[par], g, 0);
-      cudaGraphDestroy(g);
-      if (st != cudaSuccess) return cuda_fail(h, st, "graph instantiate");
+      if (st == cudaSuccess) {
+        st = cudaGraphInstantiate(&h->graph[par], g, 0);
+        cudaGraphDestroy(g);
+      }
+      if (st != cudaSuccess) {
+        if (attempt == 0 && e.wave) {
+          // the fused loop's cooperative launch could not be captured: the
+          // graph takes the two-kernel loop instead
+          cudaGetLastError();
+          e.wave = 0;
+          for (auto& gx : h->graph)
+            if (gx) {
+              cudaGraphExecDestroy(gx);
+              gx = nullptr;
+            }
+          continue;
+        }
+        return cuda_fail(h, st, "graph capture");
+      }
     }
     cudaError_t st = cudaGraphLaunch(h->graph[par], e.stream);
     if (st != cudaSuccess) return cuda_fail(h, st, "graph launch");
@@ -243,10 +267,66 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
   return MK_OK;
 }
 
+// After the stream is idle: report a bounded device wait of the fused
+// multiphase loop that ran out since the last check.
+mk_status check_waits(mk_handle* h) {
+  bool timed_out = false;
+  cudaError_t st = mke::engine_check_waits(h->e, &timed_out);
+  if (st != cudaSuccess) return cuda_fail(h, st, "wait check");
+  if (timed_out) {
+    h->err = "a bounded device wait of the fused multiphase loop ran out (a tile's phi planes were never "
+             "published); the loops since the last check are invalid";
+    return MK_ERR_TIMEOUT;
+  }
+  return MK_OK;
+}
+
 mk_status mk_sync(mk_handle* h) {
   if (!h) return MK_ERR_ARG;
   cudaError_t st = cudaStreamSynchronize(h->e.stream);
   if (st != cudaSuccess) return cuda_fail(h, st, "sync");
+  return check_waits(h);
+}
+
+mk_status mk_set_fused(mk_handle* h, int32_t fused) {
+  if (!h) return MK_ERR_ARG;
+  if (fused < 0 || fused > 2) {
+    h->err = "loop form must be 0, 1 or 2";
+    return MK_ERR_ARG;
+  }
+  if (fused && !h->e.wave_ok) {
+    h->err = "this case does not admit the fused multiphase loop (multiphase model, x extent a multiple of 4, "
+             "at least 8 planes in z)";
+    return MK_ERR_ARG;
+  }
+  const int form = fused == 1 ? 2 : (fused == 2 ? 1 : 0);
+  if (form != h->e.wave) {
+    h->e.wave = form;
+    for (auto& g : h->graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+  return MK_OK;
+}
+
+int32_t mk_get_fused(const mk_handle* h) {
+  if (!h || !h->e.wave_ok || !h->e.wave) return 0;
+  return h->e.wave == 2 ? 1 : 2;
+}
+
+mk_status mk_inject_fault(mk_handle* h, int32_t kind) {
+  if (!h) return MK_ERR_ARG;
+  if (kind != 1) {
+    h->err = "unknown fault kind";
+    return MK_ERR_ARG;
+  }
+  if (!(h->e.wave && h->e.wave_ok)) {
+    h->err = "fault kind 1 needs a case that runs the fused multiphase loop";
+    return MK_ERR_ARG;
+  }
+  h->e.wave_skip = 0;
   return MK_OK;
 }
 
@@ -470,6 +550,8 @@ mk_status mk_diagnostics(mk_handle* h, mk_diag* out) {
   double v[mke::DG_N];
   cudaError_t st = mke::engine_diag(h->e, v);
   if (st != cudaSuccess) return cuda_fail(h, st, "diagnostics");
+  const mk_status w = check_waits(h);
+  if (w != MK_OK) return w;
   std::memset(out, 0, sizeof(*out));
   out->step = h->e.step;
   out->mass = v[mke::DG_MASS];

@@ -67,6 +67,18 @@ struct Engine {
   float* stage32;     // 2 * ncell floats (FP32 state upload staging, allocated on first use)
   // launch counters
   int64_t launches;
+  // fused multiphase step: one cooperative launch per loop (k_mp_wave)
+  int wave;              // multiphase loop form: 0 phi kernel + collision kernel, 1 fused, 2 fused with a
+                         // producer warp per CTA (warp-specialised)
+  int wave_ok;           // the case admits the fused loop (x extent a multiple of 4, nz >= 8, grid co-resident)
+  int wave_sx, wave_sy;  // tiles: 32-cell x segments times y bands
+  int wave_rows;         // rows of the tallest band
+  int wave_threads;      // threads per CTA (form 1)
+  int wave_threads_ws;   // threads per CTA (form 2)
+  size_t wave_smem;      // dynamic shared memory (the phi ring)
+  unsigned* wave_flags;  // per-tile publication counters (zeroed before every launch)
+  int* wave_err;         // error word of the bounded waits (0 = none)
+  int wave_skip;         // test hook: tile that publishes nothing in the next fused launch (-1: none)
 };
 
 // Message returned by mk_last_global_error on this thread.
@@ -100,6 +112,16 @@ const char* engine_kernel_name(const Engine& e, int k);
 cudaError_t engine_field(Engine& e, int field);
 // Multigrain: grain j's order parameter into e.field (device).
 cudaError_t engine_grain_field(Engine& e, int grain);
+
+// Multiphase loop (mk_multiphase.cu): choose the fused loop's tiling for the
+// case (sets wave_ok and the wave_* fields), and launch one loop.
+void mp_configure(Engine& e);
+void mp_launch(Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev);
+
+// After a synchronisation: whether a bounded device wait of the fused loop
+// gave up since the last check (clears the record).  Returns the CUDA status
+// of the read; *timed_out is set when a wait ran out.
+cudaError_t engine_check_waits(Engine& e, bool* timed_out);
 
 // FP64 diagnostics (two-pass reduction into e.dsum); host copy in out[DG_N].
 cudaError_t engine_diag(Engine& e, double* out);

@@ -24,15 +24,12 @@
 
 #include "mk_device.cuh"
 #include "mk_engine.hpp"
+#include "mk_shared.cuh"
 
 using namespace mkd;
+using namespace mks;
 
 namespace {
-
-// Rest values of the two lattices: populations are held as f_i - w_i ref.
-struct Refs {
-  double r0, r1;
-};
 
 // ================================================================ FLOW (K1)
 template <class T>
@@ -213,271 +210,6 @@ __global__ void __launch_bounds__(256)
   } else {
     const Nbr nb(g, x, y, z);
     conv_cell<S, Q, COLL, PARITY, SCALAR, true>(F, Tp, g.stride, nb, nb.idx(0, 0, 0), coord, k);
-  }
-}
-
-// ========================================================= MULTIPHASE (K4)
-// The pressure lattice g rests at 0 (p* = 0, u = 0), so its deviation is g
-// itself; the Allen-Cahn lattice h rests at the liquid, h_i = w_i (phi = 1).
-template <class T>
-struct MpK {
-  T beta, kappa, om_h, coef_wet, inv_w4, rho_l, rho_g, tau_l, tau_g, gx, gy, gz;
-  T ref_h;  // 1
-};
-
-// With 16-bit storage the Allen-Cahn rest population h_0 (always stored at
-// its own cell, in both AA parities) lives in an FP32 plane H0 and absorbs the
-// rounding residual of the cell's 18 moving populations, so sum(h) — the
-// conserved phase volume — is kept to FP32 rounding.
-template <class S>
-struct Rest32 {
-  static constexpr bool on = Stor<S>::bytes == 2;
-};
-
-template <class S, class P, int PARITY, class NB>
-__device__ __forceinline__ void mp_phi_cell(const S* __restrict__ H, const float* __restrict__ H0, P* __restrict__ phi,
-                                            int64_t stride, const NB& nb, int c, typename Stor<S>::T ref_h) {
-  typedef typename Stor<S>::T T;
-  T s = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
-  if constexpr (Stor<S>::scaled) {
-    // 16-bit storage holds h'/w: sum the axis and the diagonal classes in
-    // stored units and scale once per class (2 multiplies instead of 18)
-    T sa = T(0), sd = T(0);
-#pragma unroll
-    for (int i = 1; i < 7; ++i) sa += ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
-#pragma unroll
-    for (int i = 7; i < 19; ++i) sd += ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
-    s += T(wq<19>(1)) * sa + T(wq<19>(7)) * sd;
-  } else {
-#pragma unroll
-    for (int i = 1; i < 19; ++i) s += ld_in<S, 19>(H, stride, nb, PARITY, c, i);
-  }
-  phi[c] = P(ref_h + s);
-}
-
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const float* __restrict__ H0,
-                                                P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  if (fast_cell(g, x, y, z)) {
-    const Fast fa = make_fast(g, x, y, z);
-    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, ref_h);
-  } else {
-    const Nbr nb(g, x, y, z);
-    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), ref_h);
-  }
-}
-
-// Density, phi gradient and total force of a fluid cell (shared by the
-// collision and by field output so both see identical values).
-template <class T, class P, class NB>
-__device__ __forceinline__ void mp_force(const P* __restrict__ phi, const NB& nb, int c, const MpK<T>& k, T pstar,
-                                         T& ph, T& rho, T (&gp)[3], T (&F)[3]) {
-  ph = T(phi[c]);
-  const T wall = ph + k.coef_wet * ph * (T(1) - ph);
-  T gx = T(0), gy = T(0), gz = T(0), l = T(0);
-#pragma unroll
-  for (int i = 1; i < 19; ++i) {
-    const T fn = nb_fluid(nb, ex(i), ey(i), ez(i)) ? T(__ldg(phi + nb_idx(nb, ex(i), ey(i), ez(i)))) : wall;
-    const T w = T(wq<19>(i));
-    if (ex(i)) gx += (w * T(ex(i))) * fn;
-    if (ey(i)) gy += (w * T(ey(i))) * fn;
-    if (ez(i)) gz += (w * T(ez(i))) * fn;
-    l += w * (fn - ph);
-  }
-  gp[0] = T(3) * gx;
-  gp[1] = T(3) * gy;
-  gp[2] = T(3) * gz;
-  const T lap = T(6) * l;
-  const T drho = k.rho_l - k.rho_g;
-  rho = k.rho_g + ph * drho;
-  const T mu = T(4) * k.beta * ph * (ph - T(1)) * (ph - T(0.5)) - k.kappa * lap;
-  const T pg = pstar * (T(1) / T(3)) * drho;
-  F[0] = mu * gp[0] + rho * k.gx - pg * gp[0];
-  F[1] = mu * gp[1] + rho * k.gy - pg * gp[1];
-  F[2] = mu * gp[2] + rho * k.gz - pg * gp[2];
-}
-
-// One loop of a fluid cell.  Every population load (19 g, 19 h) is issued
-// before any store: the loads are the latency the kernel must hide, and a
-// store into the same array in between would stop the compiler from hoisting
-// the later loads (in place, on odd loops a direction's result goes to the
-// slot its opposite direction is read from).
-template <class S, class P, int PARITY, class NB>
-__device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
-                                                const P* __restrict__ phi, const int64_t stride, const NB& nb,
-                                                const int c, const MpK<typename Stor<S>::T>& k) {
-  typedef typename Stor<S>::T T;
-  // the Allen-Cahn slots go to L2 now (FP32 / FP64; with 16-bit storage the
-  // prefetch measured 2% slower) and are loaded once the pressure lattice is
-  // stored, so the two lattices' populations are never live together
-  // (register pressure sets the occupancy of this kernel)
-  if constexpr (Stor<S>::bytes >= 4) {
-#pragma unroll
-    for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
-  }
-  T gp_[19];  // g (rests at 0)
-#pragma unroll
-  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, stride, nb, PARITY, c, i);
-  T m[19];  // MRT moments: m[0] = p*, (m[3], m[5], m[7]) = j
-  mrt19_moments<T>(gp_, m);
-  const T pstar = m[0], jx = m[3], jy = m[5], jz = m[7];
-  T ph, rho, gphi[3], F[3];
-  mp_force<T, P, NB>(phi, nb, c, k, pstar, ph, rho, gphi, F);
-  const T irho = div_fast(T(1), rho);
-  const T ux = jx + T(0.5) * F[0] * irho;
-  const T uy = jy + T(0.5) * F[1] * irho;
-  const T uz = jz + T(0.5) * F[2] * irho;
-  const T uu = ux * ux + uy * uy + uz * uz;
-  // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
-  {
-    MrtIn<T> q;
-    q.a0 = pstar - T(1.5) * uu;
-    q.bx = ux;
-    q.by = uy;
-    q.bz = uz;
-    q.qxx = ux * ux;
-    q.qyy = uy * uy;
-    q.qzz = uz * uz;
-    q.qxy = ux * uy;
-    q.qxz = ux * uz;
-    q.qyz = uy * uz;
-    q.Fx = F[0];
-    q.Fy = F[1];
-    q.Fz = F[2];
-    q.ux = ux;
-    q.uy = uy;
-    q.uz = uz;
-    q.sF = irho;
-    q.s_nu = div_fast(T(1), k.tau_g + ph * (k.tau_l - k.tau_g));
-    mrt19_relax_back<T>(gp_, m, q);
-#pragma unroll
-    for (int i = 0; i < 19; ++i) st_out<S, 19>(G, stride, nb, PARITY, c, i, gp_[i]);
-  }
-  const T gn = sqrt(gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2]);
-  const T inv_gn = div_fast(T(1), gn + T(1e-12));
-  const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
-  const T lam = k.inv_w4 * ph * (T(1) - ph);
-  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair, in the
-  // stored units (h' = h - w, or h'/w for 16-bit storage, sig = w or 1):
-  //   h*' = (1 - om) h' + sig [om (X_even +- X_odd) +- Y],
-  //   heq_i - w_i = w_i [X_even + X_odd], X_even = (phi - 1) + phi (4.5(eu)^2 - 1.5u^2),
-  //   X_odd = 3 phi eu, the sharpening flux w_i Y = w_i (1 - om/2) lam (e.n)
-  constexpr bool SC = Stor<S>::scaled;
-  T h[19];
-  h[0] = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
-#pragma unroll
-  for (int i = 1; i < 19; ++i) h[i] = ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
-  const T om_h = k.om_h;
-  const T one_om = T(1) - om_h;
-  const T src = (T(1) - T(0.5) * om_h) * lam;
-  const T dph = ph - k.ref_h;
-  T res_a = T(0), res_d = T(0);  // what the 16-bit stores rounded away, per weight class (Rest32 only)
-  if constexpr (std::is_same<T, float>::value) {
-    // FP32 arithmetic: two pairs per packed instruction, the pairs of equal
-    // weight grouped (+-x with +-y, then the four diagonal planes two by
-    // two); the +-z pair goes alone
-    auto store = [&](int i, float v, bool axis) {
-      if constexpr (Rest32<S>::on) {
-        const float r = v - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, i, v);
-        if (axis)
-          res_a += r;
-        else
-          res_d += r;
-      } else {
-        st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, v);
-      }
-    };
-    const float2 b_ph = bc2(ph), b_dph = bc2(dph), b_uu = bc2(-1.5f * uu), b_one_om = bc2(one_om);
-    const float2 b_om = bc2(om_h), b_3phom = bc2(3.0f * ph * om_h), b_src = bc2(src), b_m1 = bc2(-1.0f);
-    auto group = [&](int p, int q, float2 eu, float2 en, float sg) {
-      const float2 t = fma2(bc2(4.5f), mul2(eu, eu), b_uu);
-      const float2 E = mul2(b_om, fma2(b_ph, t, b_dph));          // om X_even
-      const float2 Pq = fma2(b_3phom, eu, mul2(b_src, en));       // om X_odd + Y
-      float2 a = add2(E, Pq), b = fma2(Pq, b_m1, E);
-      if (!SC) {
-        a = mul2(bc2(sg), a);
-        b = mul2(bc2(sg), b);
-      }
-      const float2 hi = make_float2(h[2 * p - 1], h[2 * q - 1]), hj = make_float2(h[2 * p], h[2 * q]);
-      const float2 vi = fma2(b_one_om, hi, a), vj = fma2(b_one_om, hj, b);
-      const bool ax = p <= 3;
-      store(2 * p - 1, vi.x, ax);
-      store(2 * p, vj.x, ax);
-      store(2 * q - 1, vi.y, ax);
-      store(2 * q, vj.y, ax);
-    };
-    const float wa = float(wq<19>(1)), wd = float(wq<19>(7));
-    group(1, 2, make_float2(ux, uy), make_float2(nx_, ny_), wa);
-    group(4, 5, make_float2(ux + uy, ux - uy), make_float2(nx_ + ny_, nx_ - ny_), wd);
-    group(6, 7, make_float2(ux + uz, ux - uz), make_float2(nx_ + nz_, nx_ - nz_), wd);
-    group(8, 9, make_float2(uy + uz, uy - uz), make_float2(ny_ + nz_, ny_ - nz_), wd);
-    {
-      // +-z alone
-      const float sg = SC ? 1.0f : wa;
-      const float eu = uz, en = nz_;
-      const float E = om_h * (dph + ph * (4.5f * eu * eu - 1.5f * uu));
-      const float Pq = 3.0f * ph * om_h * eu + src * en;
-      store(5, one_om * h[5] + sg * (E + Pq), true);
-      store(6, one_om * h[6] + sg * (E - Pq), true);
-    }
-  } else {
-#pragma unroll
-  for (int p = 1; p <= 9; ++p) {
-    const int i = 2 * p - 1, j = 2 * p;
-    const T sig = SC ? T(1) : T(wq<19>(i));
-    const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
-    const T en = T(ex(i)) * nx_ + T(ey(i)) * ny_ + T(ez(i)) * nz_;
-    const T xe = dph + ph * (T(4.5) * eu * eu - T(1.5) * uu);
-    const T xo = ph * (T(3) * eu);
-    const T y = src * en;
-    const T vi = one_om * h[i] + sig * (om_h * (xe + xo) + y);
-    const T vj = one_om * h[j] + sig * (om_h * (xe - xo) - y);
-    if constexpr (Rest32<S>::on) {
-      const T r = (vi - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, i, vi)) +
-                  (vj - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, j, vj));
-      if (p <= 3)
-        res_a += r;
-      else
-        res_d += r;
-    } else {
-      st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, vi);
-      st_out_raw<S, 19>(H, stride, nb, PARITY, c, j, vj);
-    }
-  }
-  }
-  {
-    const T w = T(wq<19>(0));
-    const T h0 = h[0];
-    const T heq = w * (dph - T(1.5) * ph * uu);
-    const T v0 = h0 - om_h * (h0 - heq);
-    if constexpr (Rest32<S>::on)
-      H0[c] = float(v0 + (T(wq<19>(1)) * res_a + T(wq<19>(7)) * res_d));
-    else
-      st_out<S, 19>(H, stride, nb, PARITY, c, 0, v0);
-  }
-}
-
-// MINB is the occupancy hint (resident 256-thread blocks per SM): 1 keeps
-// every value in registers, 2 doubles the warps per SM at the price of a few
-// spills; the autotuner picks.  Interior rows take the Fast addressing.
-template <class S, class P, int PARITY, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
-                                                          float* __restrict__ H0, const P* __restrict__ phi,
-                                                          const Geom g, const MpK<typename Stor<S>::T> k) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  if (fast_cell(g, x, y, z)) {
-    const Fast fa = make_fast(g, x, y, z);
-    mp_collide_cell<S, P, PARITY>(G, H, H0, phi, g.stride, fa, fa.c, k);
-  } else {
-    const Nbr nb(g, x, y, z);
-    mp_collide_cell<S, P, PARITY>(G, H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), k);
   }
 }
 
@@ -1446,41 +1178,6 @@ __global__ void k_diag_final(const double* __restrict__ partial, int nblocks, do
 }
 
 // ================================================================ launchers
-Geom make_geom(const mke::Engine& e) {
-  Geom g;
-  g.nx = e.nx;
-  g.ny = e.ny;
-  g.nz = e.nz;
-  g.bc0 = e.p.bc[0];
-  g.bc1 = e.p.bc[1];
-  g.bc2 = e.p.bc[2];
-  g.stride = e.stride;
-  return g;
-}
-
-void launch_dims(const mke::Engine& e, dim3& grid, dim3& block) {
-  block = dim3(e.block_x, e.block_y, 1);
-  grid = dim3((e.nx + e.block_x - 1) / e.block_x, (e.ny + e.block_y - 1) / e.block_y, e.nz);
-}
-
-// Rest values of the lattices (populations are held as f_i - w_i ref).
-Refs refs_of(const mk_params& p) {
-  Refs r{0.0, 0.0};
-  if (p.model == MK_MODEL_FLOW) {
-    r.r0 = p.rho0;
-  } else if (p.model == MK_MODEL_CONVECTION) {
-    r.r0 = p.rho0;
-    r.r1 = p.s_ref;  // t: the buoyancy reference value
-  } else if (p.model == MK_MODEL_MULTIPHASE) {
-    r.r0 = 0.0;  // g: rest state p* = 0, u = 0
-    r.r1 = 1.0;  // h: liquid phi = 1
-  } else {
-    r.r0 = -1.0;      // g: liquid phi = -1
-    r.r1 = -p.delta;  // t/U: far-field value
-  }
-  return r;
-}
-
 template <class T>
 FlowK<T> flow_coef(const mk_params& p, double ref) {
   FlowK<T> k;
@@ -1490,25 +1187,6 @@ FlowK<T> flow_coef(const mk_params& p, double ref) {
   k.Fy = T(p.force[1]);
   k.Fz = T(p.force[2]);
   k.ref = T(ref);
-  return k;
-}
-
-template <class T>
-MpK<T> mp_coef(const mk_params& p, Refs r) {
-  MpK<T> k;
-  k.beta = T(12.0 * p.sigma / p.width);
-  k.kappa = T(1.5 * p.sigma * p.width);
-  k.om_h = T(1.0 / (3.0 * p.mobility + 0.5));
-  k.coef_wet = T(4.0 * std::cos(p.contact_angle * M_PI / 180.0) / p.width);
-  k.inv_w4 = T(4.0 / p.width);
-  k.rho_l = T(p.rho_l);
-  k.rho_g = T(p.rho_g);
-  k.tau_l = T(p.tau_l);
-  k.tau_g = T(p.tau_g);
-  k.gx = T(p.force[0]);
-  k.gy = T(p.force[1]);
-  k.gz = T(p.force[2]);
-  k.ref_h = T(r.r1);
   return k;
 }
 
@@ -1600,39 +1278,6 @@ void launch_flow(mke::Engine& e, int parity, dim3 grid, dim3 block) {
     else
       launch_flow_t<S, 27, MK_COLL_TRT>(e, parity, grid, block);
   }
-}
-
-template <class S>
-void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
-  typedef typename Stor<S>::T T;
-  typedef typename PhiOf<S>::type P;
-  const Geom g = make_geom(e);
-  const Refs r = refs_of(e.p);
-  const MpK<T> k = mp_coef<T>(e.p, r);
-  S* G = (S*)e.pop0;
-  S* H = (S*)e.pop1;
-  P* phi = (P*)e.phi[0];
-  if (ev) cudaEventRecord(ev[0], e.stream);
-  if (parity == 0)
-    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
-  else
-    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
-  if (ev) {
-    cudaEventRecord(ev[1], e.stream);
-    cudaEventRecord(ev[2], e.stream);
-  }
-  if (e.minb == 1) {
-    if (parity == 0)
-      k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
-    else
-      k_mp_collide<S, P, 1, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
-  } else {
-    if (parity == 0)
-      k_mp_collide<S, P, 0, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
-    else
-      k_mp_collide<S, P, 1, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
-  }
-  if (ev) cudaEventRecord(ev[3], e.stream);
 }
 
 template <class S>
@@ -1847,8 +1492,8 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
       e.launches += 1;
       break;
     case MK_MODEL_MULTIPHASE:
-      launch_mp<S>(e, parity, grid, block, ev);
-      e.launches += 2;
+      mke::mp_launch(e, parity, grid, block, ev);
+      e.launches += (e.wave && e.wave_ok) ? 1 : 2;
       break;
     case MK_MODEL_MULTIGRAIN:
       launch_mg<S>(e, parity, grid, block, ev);
@@ -2161,6 +1806,15 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     return st;
   if ((st = cudaMalloc((void**)&e.dsum, DG_N * sizeof(double))) != cudaSuccess) return st;
   if ((st = cudaMalloc((void**)&e.field, (size_t)e.ncell * sizeof(double))) != cudaSuccess) return st;
+  e.wave_skip = -1;
+  if (p.model == MK_MODEL_MULTIPHASE) {
+    mp_configure(e);
+    if (e.wave_ok) {
+      if ((st = alloc((void**)&e.wave_flags, (size_t)e.wave_sx * e.wave_sy * sizeof(unsigned))) != cudaSuccess) return st;
+      if ((st = alloc((void**)&e.wave_err, sizeof(int))) != cudaSuccess) return st;
+      e.wave = 2;
+    }
+  }
   // host-side copy of sd must outlive the async copy
   st = cudaStreamSynchronize(e.stream);
   return st;
@@ -2169,7 +1823,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
   void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.vel, e.phij, e.gseeds, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
-                  e.field32, e.stage32};
+                  e.field32, e.stage32, e.wave_flags, e.wave_err};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (e.stream) cudaStreamDestroy(e.stream);
@@ -2273,13 +1927,15 @@ cudaError_t engine_step(Engine& e, cudaEvent_t* ev) {
 
 static bool one_kernel(const Engine& e) { return e.p.model == MK_MODEL_FLOW || e.p.model == MK_MODEL_CONVECTION; }
 
+static bool fused_mp(const Engine& e) { return e.p.model == MK_MODEL_MULTIPHASE && e.wave && e.wave_ok; }
+
 int engine_kernels_per_step(const Engine& e) {
   if (e.p.model == MK_MODEL_FLOW_DENDRITE) return (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
-  return one_kernel(e) ? 1 : 2;
+  return (one_kernel(e) || fused_mp(e)) ? 1 : 2;
 }
 
 const char* engine_kernel_name(const Engine& e, int k) {
-  if (one_kernel(e)) return "collide";
+  if (one_kernel(e) || fused_mp(e)) return "collide";
   if (e.p.model == MK_MODEL_FLOW_DENDRITE) {
     static const char* const names[4] = {"phi", "flow", "collide", "boundary"};
     return k >= 0 && k < 4 ? names[k] : "";
@@ -2310,6 +1966,21 @@ cudaError_t engine_grain_field(Engine& e, int grain) {
     k_field_copy<float><<<nb, 256, 0, e.stream>>>((const float*)e.phij + (int64_t)grain * e.ncell, nullptr, e.ncell,
                                                   e.field);
   return cudaGetLastError();
+}
+
+cudaError_t engine_check_waits(Engine& e, bool* timed_out) {
+  *timed_out = false;
+  if (!e.wave_err) return cudaSuccess;
+  int v = 0;
+  cudaError_t st = cudaMemcpyAsync(&v, e.wave_err, sizeof(int), cudaMemcpyDeviceToHost, e.stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e.stream);
+  if (st != cudaSuccess) return st;
+  if (v != 0) {
+    *timed_out = true;
+    st = cudaMemsetAsync(e.wave_err, 0, sizeof(int), e.stream);
+    if (st == cudaSuccess) st = cudaStreamSynchronize(e.stream);
+  }
+  return st;
 }
 
 cudaError_t engine_diag(Engine& e, double* out) {
@@ -2371,14 +2042,17 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   const int shapes[9][2] = {{32, 2}, {64, 1}, {32, 4}, {64, 2}, {128, 1}, {32, 8}, {64, 4}, {128, 2}, {256, 1}};
   const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 2 : 1;
   double best = 1e300;
-  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0;
-  for (int si = 0; si < 9 && st == cudaSuccess; ++si) {
-    const int bx = shapes[si][0];
-    if (bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
-    for (int mb = 1; mb <= nmb && st == cudaSuccess; ++mb) {
+  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0;
+  // candidates -2 and -1: the two forms of the fused multiphase loop (their
+  // tiling is fixed by the case)
+  for (int si = e.wave_ok ? -2 : 0; si < 9 && st == cudaSuccess; ++si) {
+    const int bx = si < 0 ? bx0 : shapes[si][0];
+    if (si >= 0 && bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
+    for (int mb = 1; mb <= (si < 0 ? 1 : nmb) && st == cudaSuccess; ++mb) {
+      e.wave = si == -2 ? 2 : (si == -1 ? 1 : 0);
       e.block_x = bx;
-      e.block_y = shapes[si][1];
-      e.minb = nmb == 2 ? mb : mb0;
+      e.block_y = si < 0 ? by0 : shapes[si][1];
+      e.minb = (nmb == 2 && si >= 0) ? mb : mb0;
       engine_step(e, nullptr);  // warm-up of this shape, both AA parities
       engine_step(e, nullptr);
       // the faster of two timed repeats (one slow repeat must not decide)
@@ -2399,6 +2073,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
         bbx = e.block_x;
         bby = e.block_y;
         bmb = e.minb;
+        bwave = e.wave;
       }
       e.step = step0;
       e.phi_cur = cur0;
@@ -2415,10 +2090,12 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   e.block_x = bbx;
   e.block_y = bby;
   e.minb = bmb;
+  e.wave = bwave;
   if (out) {
-    out->block_x = bbx;
-    out->block_y = bby;
-    out->minb = bmb;
+    // a fused multiphase loop has no block shape or occupancy variant: 0, 0, 0
+    out->block_x = bwave ? 0 : bbx;
+    out->block_y = bwave ? 0 : bby;
+    out->minb = bwave ? 0 : bmb;
     out->ms_per_step = best;
     out->candidates = ncand;
   }

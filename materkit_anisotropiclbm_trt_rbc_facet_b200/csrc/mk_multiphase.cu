@@ -1,0 +1,781 @@
+// mk_multiphase.cu — the two-phase Allen-Cahn loop (K4): the phi kernel and
+// the collision kernel, and the fused one-launch loop, with their launchers
+// (mkFluidsMultiphase::propagate/relaxation, mkFluidsMultiphase.h:52-57;
+// getEquPDFsLiang/PhiLiang, mkNode.h:38-40).
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+
+#include "mk_device.cuh"
+#include "mk_engine.hpp"
+#include "mk_shared.cuh"
+#include "mk_wave.cuh"
+
+using namespace mkd;
+using namespace mks;
+
+namespace {
+
+// One loop of a fluid cell.  Every population load (19 g, 19 h) is issued
+// before any store: the loads are the latency the kernel must hide, and a
+// store into the same array in between would stop the compiler from hoisting
+// the later loads (in place, on odd loops a direction's result goes to the
+// slot its opposite direction is read from).
+template <class S, class P, int PARITY, class NB, class PH>
+__device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                                const PH& phi_src, const int64_t stride, const NB& nb,
+                                                const int c, const MpK<typename Stor<S>::T>& k) {
+  typedef typename Stor<S>::T T;
+  // the Allen-Cahn slots go to L2 now (FP32 / FP64; with 16-bit storage the
+  // prefetch measured 2% slower) and are loaded once the pressure lattice is
+  // stored, so the two lattices' populations are never live together
+  // (register pressure sets the occupancy of this kernel)
+  if constexpr (Stor<S>::bytes >= 4) {
+#pragma unroll
+    for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
+  }
+  T gp_[19];  // g (rests at 0)
+#pragma unroll
+  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, stride, nb, PARITY, c, i);
+  T m[19];  // MRT moments: m[0] = p*, (m[3], m[5], m[7]) = j
+  mrt19_moments<T>(gp_, m);
+  const T pstar = m[0], jx = m[3], jy = m[5], jz = m[7];
+  T ph, rho, gphi[3], F[3];
+  mp_force_src<T, P, NB>(phi_src, nb, k, pstar, ph, rho, gphi, F);
+  const T irho = div_fast(T(1), rho);
+  const T ux = jx + T(0.5) * F[0] * irho;
+  const T uy = jy + T(0.5) * F[1] * irho;
+  const T uz = jz + T(0.5) * F[2] * irho;
+  const T uu = ux * ux + uy * uy + uz * uz;
+  // ---- pressure/velocity lattice: moment-space MRT with the Guo force / rho
+  {
+    MrtIn<T> q;
+    q.a0 = pstar - T(1.5) * uu;
+    q.bx = ux;
+    q.by = uy;
+    q.bz = uz;
+    q.qxx = ux * ux;
+    q.qyy = uy * uy;
+    q.qzz = uz * uz;
+    q.qxy = ux * uy;
+    q.qxz = ux * uz;
+    q.qyz = uy * uz;
+    q.Fx = F[0];
+    q.Fy = F[1];
+    q.Fz = F[2];
+    q.ux = ux;
+    q.uy = uy;
+    q.uz = uz;
+    q.sF = irho;
+    q.s_nu = div_fast(T(1), k.tau_g + ph * (k.tau_l - k.tau_g));
+    mrt19_relax_back<T>(gp_, m, q);
+#pragma unroll
+    for (int i = 0; i < 19; ++i) st_out<S, 19>(G, stride, nb, PARITY, c, i, gp_[i]);
+  }
+  const T gn = sqrt(gphi[0] * gphi[0] + gphi[1] * gphi[1] + gphi[2] * gphi[2]);
+  const T inv_gn = div_fast(T(1), gn + T(1e-12));
+  const T nx_ = gphi[0] * inv_gn, ny_ = gphi[1] * inv_gn, nz_ = gphi[2] * inv_gn;
+  const T lam = k.inv_w4 * ph * (T(1) - ph);
+  // ---- Allen-Cahn lattice (BGK + sharpening flux), pair by pair, in the
+  // stored units (h' = h - w, or h'/w for 16-bit storage, sig = w or 1):
+  //   h*' = (1 - om) h' + sig [om (X_even +- X_odd) +- Y],
+  //   heq_i - w_i = w_i [X_even + X_odd], X_even = (phi - 1) + phi (4.5(eu)^2 - 1.5u^2),
+  //   X_odd = 3 phi eu, the sharpening flux w_i Y = w_i (1 - om/2) lam (e.n)
+  constexpr bool SC = Stor<S>::scaled;
+  T h[19];
+  h[0] = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
+#pragma unroll
+  for (int i = 1; i < 19; ++i) h[i] = ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
+  const T om_h = k.om_h;
+  const T one_om = T(1) - om_h;
+  const T src = (T(1) - T(0.5) * om_h) * lam;
+  const T dph = ph - k.ref_h;
+  T res_a = T(0), res_d = T(0);  // what the 16-bit stores rounded away, per weight class (Rest32 only)
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32 arithmetic: two pairs per packed instruction, the pairs of equal
+    // weight grouped (+-x with +-y, then the four diagonal planes two by
+    // two); the +-z pair goes alone
+    auto store = [&](int i, float v, bool axis) {
+      if constexpr (Rest32<S>::on) {
+        const float r = v - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, i, v);
+        if (axis)
+          res_a += r;
+        else
+          res_d += r;
+      } else {
+        st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, v);
+      }
+    };
+    const float2 b_ph = bc2(ph), b_dph = bc2(dph), b_uu = bc2(-1.5f * uu), b_one_om = bc2(one_om);
+    const float2 b_om = bc2(om_h), b_3phom = bc2(3.0f * ph * om_h), b_src = bc2(src), b_m1 = bc2(-1.0f);
+    auto group = [&](int p, int q, float2 eu, float2 en, float sg) {
+      const float2 t = fma2(bc2(4.5f), mul2(eu, eu), b_uu);
+      const float2 E = mul2(b_om, fma2(b_ph, t, b_dph));          // om X_even
+      const float2 Pq = fma2(b_3phom, eu, mul2(b_src, en));       // om X_odd + Y
+      float2 a = add2(E, Pq), b = fma2(Pq, b_m1, E);
+      if (!SC) {
+        a = mul2(bc2(sg), a);
+        b = mul2(bc2(sg), b);
+      }
+      const float2 hi = make_float2(h[2 * p - 1], h[2 * q - 1]), hj = make_float2(h[2 * p], h[2 * q]);
+      const float2 vi = fma2(b_one_om, hi, a), vj = fma2(b_one_om, hj, b);
+      const bool ax = p <= 3;
+      store(2 * p - 1, vi.x, ax);
+      store(2 * p, vj.x, ax);
+      store(2 * q - 1, vi.y, ax);
+      store(2 * q, vj.y, ax);
+    };
+    const float wa = float(wq<19>(1)), wd = float(wq<19>(7));
+    group(1, 2, make_float2(ux, uy), make_float2(nx_, ny_), wa);
+    group(4, 5, make_float2(ux + uy, ux - uy), make_float2(nx_ + ny_, nx_ - ny_), wd);
+    group(6, 7, make_float2(ux + uz, ux - uz), make_float2(nx_ + nz_, nx_ - nz_), wd);
+    group(8, 9, make_float2(uy + uz, uy - uz), make_float2(ny_ + nz_, ny_ - nz_), wd);
+    {
+      // +-z alone
+      const float sg = SC ? 1.0f : wa;
+      const float eu = uz, en = nz_;
+      const float E = om_h * (dph + ph * (4.5f * eu * eu - 1.5f * uu));
+      const float Pq = 3.0f * ph * om_h * eu + src * en;
+      store(5, one_om * h[5] + sg * (E + Pq), true);
+      store(6, one_om * h[6] + sg * (E - Pq), true);
+    }
+  } else {
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    const int i = 2 * p - 1, j = 2 * p;
+    const T sig = SC ? T(1) : T(wq<19>(i));
+    const T eu = T(ex(i)) * ux + T(ey(i)) * uy + T(ez(i)) * uz;
+    const T en = T(ex(i)) * nx_ + T(ey(i)) * ny_ + T(ez(i)) * nz_;
+    const T xe = dph + ph * (T(4.5) * eu * eu - T(1.5) * uu);
+    const T xo = ph * (T(3) * eu);
+    const T y = src * en;
+    const T vi = one_om * h[i] + sig * (om_h * (xe + xo) + y);
+    const T vj = one_om * h[j] + sig * (om_h * (xe - xo) - y);
+    if constexpr (Rest32<S>::on) {
+      const T r = (vi - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, i, vi)) +
+                  (vj - st_out_raw_rt<S, 19>(H, stride, nb, PARITY, c, j, vj));
+      if (p <= 3)
+        res_a += r;
+      else
+        res_d += r;
+    } else {
+      st_out_raw<S, 19>(H, stride, nb, PARITY, c, i, vi);
+      st_out_raw<S, 19>(H, stride, nb, PARITY, c, j, vj);
+    }
+  }
+  }
+  {
+    const T w = T(wq<19>(0));
+    const T h0 = h[0];
+    const T heq = w * (dph - T(1.5) * ph * uu);
+    const T v0 = h0 - om_h * (h0 - heq);
+    if constexpr (Rest32<S>::on)
+      H0[c] = float(v0 + (T(wq<19>(1)) * res_a + T(wq<19>(7)) * res_d));
+    else
+      st_out<S, 19>(H, stride, nb, PARITY, c, 0, v0);
+  }
+}
+
+// MINB is the occupancy hint (resident 256-thread blocks per SM): 1 keeps
+// every value in registers, 2 doubles the warps per SM at the price of a few
+// spills; the autotuner picks.  Interior rows take the Fast addressing.
+template <class S, class P, int PARITY, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
+                                                          float* __restrict__ H0, const P* __restrict__ phi,
+                                                          const Geom g, const MpK<typename Stor<S>::T> k) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  if (fast_cell(g, x, y, z)) {
+    const Fast fa = make_fast(g, x, y, z);
+    mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Fast>{phi, fa, fa.c}, g.stride, fa, fa.c, k);
+  } else {
+    const Nbr nb(g, x, y, z);
+    const int c = nb.idx(0, 0, 0);
+    mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Nbr>{phi, nb, c}, g.stride, nb, c, k);
+  }
+}
+
+// ------------------------------------------------- fused multiphase step
+// One cooperative launch per loop.  Each CTA owns a tile column: a 32-cell x
+// segment times a band of rows, marching through z.  For its own cells it
+// computes phi = 1 + sum h' from exactly the slots the cell's collision reads
+// later (in both AA parities every slot is read and written by one cell
+// only), so computing phi ahead of the collision races with nothing.  A tile
+// publishes phi `look` planes ahead of its collision plane (a release store of
+// its count of finished planes), the bulk-copy engine stages the tile's phi
+// rows plus a one-cell halo (one row of each neighbour band, four columns of
+// each neighbour segment, periodic wrap resolved by the row addresses) into a
+// four-plane shared-memory ring two planes ahead, and the collision reads its
+// 19-point phi stencil from the ring.  h is read from HBM once per loop (the
+// phi pass's read is reused from L2 by the collision `look` planes later), so
+// the loop moves the compulsory 312 B/cell (FP32) instead of the 388 B/cell
+// of the separate phi kernel.
+//
+// Publication order of the planes: 0, 1, ..., nz-1, or nz-1, 0, ..., nz-2 with
+// a periodic z axis (the collision of plane 0 then needs plane nz-1 first).
+// The prologue publishes the first `look` planes (look + 1 when periodic).
+// Iteration z publishes the next one, stages sequence position z + 2 and
+// collides plane z; a neighbour published the planes staged at iteration z
+// one iteration earlier, so the waits are satisfied on arrival in steady
+// state.  The grid never exceeds the co-resident capacity (cooperative
+// launch), and every wait is bounded (mk_wave.cuh).
+struct Wave {
+  int sx, sy;        // x segments (32 cells) and y bands per segment: tile = band * sx + segment
+  int look;          // planes published ahead of the collision plane (>= 3)
+  int pz;            // 1: periodic z
+  int pitch;         // ring row pitch in phi elements
+  int rows_max;      // rows of the tallest band
+  unsigned* flags;   // per tile: planes published in this launch (zeroed before every launch)
+  int* err;          // error word (mkw::ERR_*), checked by the host
+  int skip_tile;     // test hook: this tile never publishes (-1: none)
+};
+
+template <class P>
+struct PhiRing {
+  const P* lo;   // plane z - 1
+  const P* mid;  // plane z
+  const P* hi;   // plane z + 1
+  int li, pitch;
+  __device__ __forceinline__ P center() const { return mid[li]; }
+  __device__ __forceinline__ P at(int dx, int dy, int dz) const {
+    const P* s = dz < 0 ? lo : (dz > 0 ? hi : mid);
+    return s[li + dy * pitch + dx];
+  }
+};
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256, 2) k_mp_wave(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                                    P* __restrict__ phi, const Geom g,
+                                                    const MpK<typename Stor<S>::T> k, const Wave w) {
+  extern __shared__ __align__(128) unsigned char wave_smem[];
+  __shared__ __align__(8) uint64_t bars[4];
+  __shared__ int nbr_tile[8];
+  P* const ring = reinterpret_cast<P*>(wave_smem);
+  const int tile = blockIdx.x;
+  const int seg = tile % w.sx, band = tile / w.sx;
+  const int x0 = seg * 32;
+  const int width = min(32, g.nx - x0);
+  const int y0 = (int)((int64_t)band * g.ny / w.sy), y1 = (int)((int64_t)(band + 1) * g.ny / w.sy);
+  const int rows = y1 - y0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int slot_elems = (w.rows_max + 2) * w.pitch;
+  const int nz = g.nz;
+  const bool publisher = tile != w.skip_tile;
+
+  if (threadIdx.x < 8) {
+    const int d = threadIdx.x < 4 ? threadIdx.x : threadIdx.x + 1;  // the 3 x 3 neighbourhood without its centre
+    int ns = seg + d % 3 - 1, nb = band + d / 3 - 1;
+    bool ok = true;
+    if (ns < 0 || ns >= w.sx) {
+      if (g.bc0 == 0)
+        ns = (ns + w.sx) % w.sx;
+      else
+        ok = false;
+    }
+    if (nb < 0 || nb >= w.sy) {
+      if (g.bc1 == 0)
+        nb = (nb + w.sy) % w.sy;
+      else
+        ok = false;
+    }
+    nbr_tile[threadIdx.x] = ok ? nb * w.sx + ns : -1;
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) mkw::mbar_init(&bars[s], 1);
+    mkw::fence_mbar_init();
+  }
+  __syncthreads();
+
+  const int P0 = w.look + w.pz;  // planes published by the prologue
+  auto pub_plane = [&](int kk) { return w.pz ? (kk == 0 ? nz - 1 : kk - 1) : kk; };
+  auto pub_index = [&](int q) { return w.pz ? (q == nz - 1 ? 0 : q + 1) : q; };
+
+  // phi of this tile's fluid cells in plane p (the phi kernel's arithmetic)
+  auto phi_plane = [&](int p) {
+    for (int r = warp; r < rows; r += nwarps) {
+      const int x = x0 + lane, y = y0 + r;
+      if (lane < width && g.fluid(x, y, p)) {
+        if (fast_cell(g, x, y, p)) {
+          const Fast fa = make_fast(g, x, y, p);
+          mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, k.ref_h);
+        } else {
+          const Nbr nb(g, x, y, p);
+          mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), k.ref_h);
+        }
+      }
+    }
+  };
+  // warp 0, lanes 0..7: wait until every neighbour tile has published `need` planes
+  auto wait_neighbours = [&](unsigned need) {
+    if (threadIdx.x < 8) {
+      const int t = nbr_tile[threadIdx.x];
+      if (t >= 0) mkw::wait_count(w.flags + t, need, w.err);
+    }
+  };
+  // thread 0: stage sequence position q (-1 <= q <= nz) of phi into its ring slot
+  auto stage = [&](int q) {
+    const int slot = (q + 1) & 3;
+    uint64_t* bar = &bars[slot];
+    P* dst0 = ring + (size_t)slot * slot_elems;
+    int plane = q;
+    if (w.pz) plane = (q + nz) % nz;
+    const bool have = plane >= 0 && plane < nz;
+    // bytes first (one arrival announcing them), then the copies
+    unsigned bytes = 0;
+    const int xl = x0 - 4, xr = x0 + width + 4;  // [xl, xr) with the halo
+    const int lo_mid = max(xl, 0), hi_mid = min(xr, g.nx);
+    const bool wrap_l = xl < 0 && g.bc0 == 0, wrap_r = xr > g.nx && g.bc0 == 0;
+    int nrows = 0;
+    if (have)
+      for (int lr = 0; lr < rows + 2; ++lr) {
+        const int y = y0 - 1 + lr;
+        if ((y < 0 || y >= g.ny) && g.bc1 != 0) continue;
+        ++nrows;
+      }
+    if (have)
+      bytes = (unsigned)(nrows * ((hi_mid - lo_mid) + (wrap_l ? 4 : 0) + (wrap_r ? 4 : 0)) * (int)sizeof(P));
+    mkw::mbar_arrive_expect(bar, bytes);
+    if (!have) return;
+    const int64_t pbase = (int64_t)plane * g.nx * g.ny;
+    for (int lr = 0; lr < rows + 2; ++lr) {
+      int y = y0 - 1 + lr;
+      if (y < 0 || y >= g.ny) {
+        if (g.bc1 != 0) continue;
+        y = (y + g.ny) % g.ny;
+      }
+      const P* src = phi + pbase + (int64_t)y * g.nx;
+      P* dst = dst0 + (size_t)lr * w.pitch;
+      mkw::bulk_g2s(dst + (lo_mid - xl), src + lo_mid, (unsigned)((hi_mid - lo_mid) * sizeof(P)), bar);
+      if (wrap_l) mkw::bulk_g2s(dst, src + (g.nx - 4), (unsigned)(4 * sizeof(P)), bar);
+      if (wrap_r) mkw::bulk_g2s(dst + 4 + width, src, (unsigned)(4 * sizeof(P)), bar);
+    }
+  };
+  auto parity_of = [](int q) { return (unsigned)(((q + 1) >> 2) & 1); };
+  auto slot_ptr = [&](int q) { return ring + (size_t)((q + 1) & 3) * slot_elems; };
+
+  // ---- prologue: publish the first P0 planes, stage positions -1, 0, 1
+  for (int kk = 0; kk < P0 && kk < nz; ++kk) phi_plane(pub_plane(kk));
+  __syncthreads();
+  if (threadIdx.x == 0 && publisher) {
+    __threadfence();
+    mkw::st_release(w.flags + tile, (unsigned)min(P0, nz));
+  }
+  wait_neighbours((unsigned)min(P0, nz));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mkw::fence_proxy_async_global();
+    stage(-1);
+    stage(0);
+    stage(1);
+  }
+  mkw::mbar_wait(&bars[0], parity_of(-1), w.err);
+  mkw::mbar_wait(&bars[1], parity_of(0), w.err);
+
+  for (int z = 0; z < nz; ++z) {
+    // neighbours' publication of the plane staged below (done one iteration ago)
+    const int q2 = z + 2;
+    const int plane2 = w.pz ? q2 % nz : q2;
+    const bool staged2 = q2 <= nz && plane2 < nz;
+    if (staged2) wait_neighbours((unsigned)(pub_index(plane2) + 1));
+    // publish the next plane
+    const int kk = P0 + z;
+    const bool pub = kk < nz;
+    if (pub) phi_plane(pub_plane(kk));
+    __syncthreads();  // also: every thread is done with collision z - 1 (ring slot of position z - 2)
+    if (threadIdx.x == 0) {
+      if (pub && publisher) {
+        __threadfence();
+        mkw::st_release(w.flags + tile, (unsigned)(kk + 1));
+      }
+      mkw::fence_proxy_async_global();
+      mkw::fence_proxy_async_shared();
+      if (q2 <= nz) stage(q2);
+    }
+    mkw::mbar_wait(&bars[(z + 2) & 3], parity_of(z + 1), w.err);
+    // collision of plane z from the ring (positions z - 1, z, z + 1)
+    const P* lo = slot_ptr(z - 1);
+    const P* mid = slot_ptr(z);
+    const P* hi = slot_ptr(z + 1);
+    for (int r = warp; r < rows; r += nwarps) {
+      const int x = x0 + lane, y = y0 + r;
+      if (lane < width && g.fluid(x, y, z)) {
+        const PhiRing<P> src{lo, mid, hi, (r + 1) * w.pitch + lane + 4, w.pitch};
+        if (fast_cell(g, x, y, z)) {
+          const Fast fa = make_fast(g, x, y, z);
+          mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, fa, fa.c, k);
+        } else {
+          const Nbr nb(g, x, y, z);
+          mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, nb, nb.idx(0, 0, 0), k);
+        }
+      }
+    }
+  }
+  // the last staged position (nz + 1 is never staged; nz was waited above)
+}
+
+// Warp-specialised form of the fused loop: warp 0 of a CTA is the producer,
+// the others are consumers.  The producer computes and publishes phi planes
+// (`look` ahead), waits for a ring slot to be released and for the
+// neighbours' publication, and stages the halo planes; the consumer warps
+// only collide rows, waiting on the ring's "full" barriers and releasing
+// slots through the "empty" barriers (one arrival per consumer warp).  There
+// is no CTA-wide barrier inside the plane loop, so the consumers stream like
+// the two-kernel collision while the producer's phi loads run beside them.
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256, 2) k_mp_wave_ws(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                                       P* __restrict__ phi, const Geom g,
+                                                       const MpK<typename Stor<S>::T> k, const Wave w) {
+  extern __shared__ __align__(128) unsigned char wave_smem[];
+  __shared__ __align__(8) uint64_t full[4];
+  __shared__ __align__(8) uint64_t empty[4];
+  __shared__ int nbr_tile[8];
+  P* const ring = reinterpret_cast<P*>(wave_smem);
+  const int tile = blockIdx.x;
+  const int seg = tile % w.sx, band = tile / w.sx;
+  const int x0 = seg * 32;
+  const int width = min(32, g.nx - x0);
+  const int y0 = (int)((int64_t)band * g.ny / w.sy), y1 = (int)((int64_t)(band + 1) * g.ny / w.sy);
+  const int rows = y1 - y0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nc = (blockDim.x >> 5) - 1;  // consumer warps
+  const int slot_elems = (w.rows_max + 2) * w.pitch;
+  const int nz = g.nz;
+
+  if (threadIdx.x < 8) {
+    const int d = threadIdx.x < 4 ? threadIdx.x : threadIdx.x + 1;
+    int ns = seg + d % 3 - 1, nb = band + d / 3 - 1;
+    bool ok = true;
+    if (ns < 0 || ns >= w.sx) {
+      if (g.bc0 == 0)
+        ns = (ns + w.sx) % w.sx;
+      else
+        ok = false;
+    }
+    if (nb < 0 || nb >= w.sy) {
+      if (g.bc1 == 0)
+        nb = (nb + w.sy) % w.sy;
+      else
+        ok = false;
+    }
+    nbr_tile[threadIdx.x] = ok ? nb * w.sx + ns : -1;
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      mkw::mbar_init(&full[s], 1);
+      mkw::mbar_init(&empty[s], nc);
+    }
+    mkw::fence_mbar_init();
+  }
+  __syncthreads();
+
+  const int P0 = w.look + w.pz;
+  auto parity_of = [](int q) { return (unsigned)(((q + 1) >> 2) & 1); };
+  auto slot_of = [](int q) { return (q + 1) & 3; };
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    const bool publisher = tile != w.skip_tile;
+    auto pub_plane = [&](int kk) { return w.pz ? (kk == 0 ? nz - 1 : kk - 1) : kk; };
+    auto pub_index = [&](int q) { return w.pz ? (q == nz - 1 ? 0 : q + 1) : q; };
+    // phi of column x0 + lane in every row of the tile, four rows in flight
+    auto phi_plane = [&](int p) {
+      const int x = x0 + lane;
+      if (lane >= width) return;
+      for (int r0 = 0; r0 < rows; r0 += 4) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int y = y0 + r0 + j;
+          if (r0 + j < rows && g.fluid(x, y, p)) {
+            if (fast_cell(g, x, y, p)) {
+              const Fast fa = make_fast(g, x, y, p);
+              mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, k.ref_h);
+            } else {
+              const Nbr nb(g, x, y, p);
+              mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), k.ref_h);
+            }
+          }
+        }
+      }
+    };
+    auto publish = [&](unsigned count) {
+      __syncwarp();
+      if (lane == 0 && publisher) {
+        __threadfence();
+        mkw::st_release(w.flags + tile, count);
+      }
+    };
+    auto wait_neighbours = [&](unsigned need) {
+      if (lane < 8) {
+        const int t = nbr_tile[lane];
+        if (t >= 0) mkw::wait_count(w.flags + t, need, w.err);
+      }
+      __syncwarp();
+    };
+    auto stage = [&](int q) {
+      const int slot = slot_of(q);
+      uint64_t* bar = &full[slot];
+      P* dst0 = ring + (size_t)slot * slot_elems;
+      const int plane = w.pz ? (q + nz) % nz : q;
+      const bool have = plane >= 0 && plane < nz;
+      const int xl = x0 - 4, xr = x0 + width + 4;
+      const int lo_mid = max(xl, 0), hi_mid = min(xr, g.nx);
+      const bool wrap_l = xl < 0 && g.bc0 == 0, wrap_r = xr > g.nx && g.bc0 == 0;
+      int nrows = 0;
+      if (have)
+        for (int lr = 0; lr < rows + 2; ++lr) {
+          const int y = y0 - 1 + lr;
+          if ((y < 0 || y >= g.ny) && g.bc1 != 0) continue;
+          ++nrows;
+        }
+      const unsigned bytes =
+          have ? (unsigned)(nrows * ((hi_mid - lo_mid) + (wrap_l ? 4 : 0) + (wrap_r ? 4 : 0)) * (int)sizeof(P)) : 0u;
+      mkw::mbar_arrive_expect(bar, bytes);
+      if (!have) return;
+      const int64_t pbase = (int64_t)plane * g.nx * g.ny;
+      for (int lr = 0; lr < rows + 2; ++lr) {
+        int y = y0 - 1 + lr;
+        if (y < 0 || y >= g.ny) {
+          if (g.bc1 != 0) continue;
+          y = (y + g.ny) % g.ny;
+        }
+        const P* src = phi + pbase + (int64_t)y * g.nx;
+        P* dst = dst0 + (size_t)lr * w.pitch;
+        mkw::bulk_g2s(dst + (lo_mid - xl), src + lo_mid, (unsigned)((hi_mid - lo_mid) * sizeof(P)), bar);
+        if (wrap_l) mkw::bulk_g2s(dst, src + (g.nx - 4), (unsigned)(4 * sizeof(P)), bar);
+        if (wrap_r) mkw::bulk_g2s(dst + 4 + width, src, (unsigned)(4 * sizeof(P)), bar);
+      }
+    };
+
+    for (int kk = 0; kk < P0 && kk < nz; ++kk) phi_plane(pub_plane(kk));
+    publish((unsigned)min(P0, nz));
+    wait_neighbours((unsigned)min(P0, nz));
+    if (lane == 0) {
+      mkw::fence_proxy_async_global();
+      stage(-1);
+      stage(0);
+      stage(1);
+    }
+    for (int z = 0; z < nz; ++z) {
+      const int kk = P0 + z;
+      if (kk < nz) {
+        phi_plane(pub_plane(kk));
+        publish((unsigned)(kk + 1));
+      }
+      const int q2 = z + 2;
+      if (q2 <= nz) {
+        // the slot's previous position (z - 2) is released after collision z - 1
+        if (z >= 1) mkw::mbar_wait(&empty[slot_of(q2)], parity_of(z - 2), w.err);
+        const int plane2 = w.pz ? q2 % nz : q2;
+        if (plane2 < nz) wait_neighbours((unsigned)(pub_index(plane2) + 1));
+        if (lane == 0) {
+          mkw::fence_proxy_async_global();
+          mkw::fence_proxy_async_shared();
+          stage(q2);
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ consumers
+    const int cw = warp - 1;
+    mkw::mbar_wait(&full[slot_of(-1)], parity_of(-1), w.err);
+    mkw::mbar_wait(&full[slot_of(0)], parity_of(0), w.err);
+    for (int z = 0; z < nz; ++z) {
+      mkw::mbar_wait(&full[slot_of(z + 1)], parity_of(z + 1), w.err);
+      const P* lo = ring + (size_t)slot_of(z - 1) * slot_elems;
+      const P* mid = ring + (size_t)slot_of(z) * slot_elems;
+      const P* hi = ring + (size_t)slot_of(z + 1) * slot_elems;
+      for (int r = cw; r < rows; r += nc) {
+        const int x = x0 + lane, y = y0 + r;
+        if (lane < width && g.fluid(x, y, z)) {
+          const PhiRing<P> src{lo, mid, hi, (r + 1) * w.pitch + lane + 4, w.pitch};
+          if (fast_cell(g, x, y, z)) {
+            const Fast fa = make_fast(g, x, y, z);
+            mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, fa, fa.c, k);
+          } else {
+            const Nbr nb(g, x, y, z);
+            mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, nb, nb.idx(0, 0, 0), k);
+          }
+        }
+      }
+      // position z - 1 is not read again: release its slot
+      __syncwarp();
+      if (lane == 0 && z - 1 <= nz - 2) mkw::mbar_arrive(&empty[slot_of(z - 1)]);
+    }
+  }
+}
+
+// The fused loop's tiling for this case (see k_mp_wave): 32-cell x segments
+// times y bands, with as many bands as the co-resident capacity of the
+// kernel allows, so every tile is one CTA and all CTAs are resident together.
+template <class S>
+void wave_config(mke::Engine& e) {
+  typedef typename PhiOf<S>::type P;
+  e.wave_ok = 0;
+  if (e.p.model != MK_MODEL_MULTIPHASE || e.nx % 4 != 0 || e.nz < 8) return;
+  int dev = e.device, sms = 0, coop = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (sms <= 0 || !coop) return;
+  const int sx = (e.nx + 31) / 32;
+  const int pitch = 40;
+  // occupancy of the larger launch (256 threads, 16 rows), both parities
+  size_t smem_max = (size_t)4 * (16 + 2) * pitch * sizeof(P);
+  const void* kerns[4] = {(const void*)k_mp_wave<S, P, 0>, (const void*)k_mp_wave<S, P, 1>,
+                          (const void*)k_mp_wave_ws<S, P, 0>, (const void*)k_mp_wave_ws<S, P, 1>};
+  int per_sm = 1 << 20;
+  for (const void* kern : kerns) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, smem_max) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    per_sm = std::min(per_sm, b);
+  }
+  const int cap = per_sm * sms;
+  if (per_sm < 1 || sx > cap) return;
+  const int sy = std::min(e.ny, cap / sx);
+  const int rows = (e.ny + sy - 1) / sy;
+  if (rows > 16) return;
+  e.wave_sx = sx;
+  e.wave_sy = sy;
+  e.wave_rows = rows;
+  e.wave_threads = 32 * std::min(rows, 8);         // one warp per row
+  e.wave_threads_ws = 32 * (1 + std::min(rows, 7));  // producer warp + one consumer warp per row
+  e.wave_smem = (size_t)4 * (rows + 2) * pitch * sizeof(P);
+  for (const void* kern : kerns)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.wave_smem) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+  e.wave_ok = 1;
+}
+
+template <class S>
+void launch_mp_wave(mke::Engine& e, int parity, cudaEvent_t* ev) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  const Geom g = make_geom(e);
+  const MpK<T> k = mp_coef<T>(e.p, refs_of(e.p));
+  Wave w;
+  w.sx = e.wave_sx;
+  w.sy = e.wave_sy;
+  w.look = 3;  // >= 3: a tile publishes before it waits within an iteration
+  w.pz = e.p.bc[2] == MK_BC_PERIODIC ? 1 : 0;
+  w.pitch = 40;
+  w.rows_max = e.wave_rows;
+  w.flags = e.wave_flags;
+  w.err = e.wave_err;
+  w.skip_tile = e.wave_skip;
+  e.wave_skip = -1;
+  const int tiles = w.sx * w.sy;
+  if (ev) cudaEventRecord(ev[0], e.stream);
+  cudaMemsetAsync(e.wave_flags, 0, (size_t)tiles * sizeof(unsigned), e.stream);
+  S* G = (S*)e.pop0;
+  S* H = (S*)e.pop1;
+  float* H0 = e.rest1;
+  P* phi = (P*)e.phi[0];
+  cudaLaunchConfig_t cfg = {};
+  const bool ws = e.wave == 2;
+  cfg.gridDim = dim3(tiles);
+  cfg.blockDim = dim3(ws ? e.wave_threads_ws : e.wave_threads);
+  cfg.dynamicSmemBytes = e.wave_smem;
+  cfg.stream = e.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (ws) {
+    if (parity == 0)
+      cudaLaunchKernelEx(&cfg, k_mp_wave_ws<S, P, 0>, G, H, H0, phi, g, k, w);
+    else
+      cudaLaunchKernelEx(&cfg, k_mp_wave_ws<S, P, 1>, G, H, H0, phi, g, k, w);
+  } else {
+    if (parity == 0)
+      cudaLaunchKernelEx(&cfg, k_mp_wave<S, P, 0>, G, H, H0, phi, g, k, w);
+    else
+      cudaLaunchKernelEx(&cfg, k_mp_wave<S, P, 1>, G, H, H0, phi, g, k, w);
+  }
+  if (ev) cudaEventRecord(ev[1], e.stream);
+}
+
+template <class S>
+void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  if (e.wave && e.wave_ok) {
+    launch_mp_wave<S>(e, parity, ev);
+    return;
+  }
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  const MpK<T> k = mp_coef<T>(e.p, r);
+  S* G = (S*)e.pop0;
+  S* H = (S*)e.pop1;
+  P* phi = (P*)e.phi[0];
+  if (ev) cudaEventRecord(ev[0], e.stream);
+  if (parity == 0)
+    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
+  else
+    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
+  if (ev) {
+    cudaEventRecord(ev[1], e.stream);
+    cudaEventRecord(ev[2], e.stream);
+  }
+  if (e.minb == 1) {
+    if (parity == 0)
+      k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
+    else
+      k_mp_collide<S, P, 1, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
+  } else {
+    if (parity == 0)
+      k_mp_collide<S, P, 0, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
+    else
+      k_mp_collide<S, P, 1, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
+  }
+  if (ev) cudaEventRecord(ev[3], e.stream);
+}
+
+}  // namespace
+
+namespace mke {
+
+void mp_configure(Engine& e) {
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      wave_config<double>(e);
+      break;
+    case MK_PREC_FP32:
+      wave_config<float>(e);
+      break;
+    case MK_PREC_FP16:
+      wave_config<__half>(e);
+      break;
+    default:
+      wave_config<__nv_bfloat16>(e);
+      break;
+  }
+}
+
+void mp_launch(Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      launch_mp<double>(e, parity, grid, block, ev);
+      break;
+    case MK_PREC_FP32:
+      launch_mp<float>(e, parity, grid, block, ev);
+      break;
+    case MK_PREC_FP16:
+      launch_mp<__half>(e, parity, grid, block, ev);
+      break;
+    default:
+      launch_mp<__nv_bfloat16>(e, parity, grid, block, ev);
+      break;
+  }
+}
+
+}  // namespace mke

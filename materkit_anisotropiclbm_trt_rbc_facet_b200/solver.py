@@ -357,6 +357,25 @@ class Solver:
                                      C.byref(ms)), self._h)
         return {"block": (bx.value, by.value), "minb": mb.value, "ms_per_step": ms.value}
 
+    @property
+    def fused(self) -> bool:
+        """Whether a multiphase loop runs as a fused one-launch form."""
+        return bool(self._lib.mk_get_fused(self._h))
+
+    @fused.setter
+    def fused(self, on: bool) -> None:
+        _check(self._lib.mk_set_fused(self._h, 1 if on else 0), self._h)
+
+    @property
+    def loop_form(self) -> int:
+        """Multiphase loop form (mk_set_fused): 0 two kernels, 1 fused with a
+        producer warp per CTA, 2 fused without warp specialisation."""
+        return int(self._lib.mk_get_fused(self._h))
+
+    @loop_form.setter
+    def loop_form(self, form: int) -> None:
+        _check(self._lib.mk_set_fused(self._h, int(form)), self._h)
+
     def bytes_per_cell(self) -> float:
         return float(self._lib.mk_bytes_per_cell(self._h))
 

@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _mp(casedir, prec="fp32"):
-    return case_params(cases.write(cases.multiphase_bubbles(n=24, nz=24, bubbles=1, rmin=4, rmax=5, width=3.0,
+    return case_params(cases.write(cases.multiphase_bubbles(n=32, nz=32, bubbles=1, rmin=4, rmax=5, width=2.0,
                                                             precision=prec, loops=10), f"{casedir}/f_mp_{prec}.xml"))
 
 
@@ -138,6 +138,7 @@ def test_allocation_failure_is_oom(casedir):
     assert lib.mk_create(A.C.byref(p), A.C.byref(h)) == A.MK_ERR_OOM
     assert not h.value
     assert b"allocate" in lib.mk_last_global_error()
+    # the failed allocation leaves nothing behind: the next handle creates and runs
     s = Solver(params=_mp(casedir))
     s.advance(2)
     assert s.diagnostics()["n_bad"] == 0
