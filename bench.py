@@ -260,7 +260,8 @@ def run_ours(args):
     wl = WORKLOADS[args.workload]
     K, W = args.steps, args.warmup
     results = {}
-    prec_list = [args.precision] + [p for p in ("fp32", "fp16", "bf16") if p != args.precision]
+    # FP64 storage too, so that the CPU arm (FP64) has a same-precision GPU line
+    prec_list = [args.precision] + [p for p in ("fp32", "fp16", "bf16", "fp64") if p != args.precision]
     if args.no_variants:
         prec_list = prec_list[:1]
     peak, peak_kind = _measured_peak()

@@ -66,11 +66,16 @@ typedef enum mk_model {
   MK_MODEL_FLOW_DENDRITE = 5,    /* thermal dendrite growing in a flow: porous bounce-back of the
                                     flow by the solid fraction, thermal lattice advected, inflow /
                                     outflow faces, run_flow_thermal_dendrite (MaterKit.cpp:467-527) */
-  MK_MODEL_MULTIGRAIN = 6        /* one conservative Allen-Cahn order parameter per seed (grain) with
+  MK_MODEL_MULTIGRAIN = 6,       /* one conservative Allen-Cahn order parameter per seed (grain) with
                                     a pairwise overlap penalty, aggregate phi = (N - 1) + sum phi_j,
                                     thermal ADE with latent heat: run_multiPhaseField
                                     (MaterKit.cpp:529-571), mkFluidsUser::propagate/relaxation
                                     (mkFluidsUser.cpp:68-299), mkMultiphaseField.h:24-60             */
+  MK_MODEL_FLOW_SOLUTAL = 7      /* solutal dendrite growing in a flow: the flow lattice of
+                                    MK_MODEL_FLOW_DENDRITE (porous bounce-back, inflow / outflow
+                                    faces), the solutal phase field, the U-lattice advected by the
+                                    flow with the solute inflow face: run_flow_solutal_dendrite
+                                    (MaterKit.cpp:399-465; bdy_LBflowin, mkSolutalField.h:53)       */
 } mk_model;
 
 /* Population storage precision.  Collision arithmetic is FP64 for MK_PREC_FP64
@@ -278,11 +283,10 @@ mk_status mk_get_params(const mk_handle* h, mk_params* out);
 int64_t mk_get_step(const mk_handle* h);
 
 /* Advance n loops of the coupled step (propagate + relaxation of every field in
- * the reference's per-loop order).  Asynchronous on the handle's stream.
- * A multiphase case runs each loop as one cooperative launch whose tiles
- * exchange phi planes through flags with bounded waits, when the case admits
- * it (x extent a multiple of 4, at least 8 planes in z), else as a phi kernel
- * plus a collision kernel; the two forms give the same result. */
+ * the reference's per-loop order).  Asynchronous on the handle's stream.  A
+ * multiphase loop runs as a phi kernel plus a collision kernel, or as one
+ * cooperative launch whose tiles exchange phi planes through flags with
+ * bounded waits (mk_set_fused); the two forms give the same result. */
 mk_status mk_advance(mk_handle* h, int64_t nsteps);
 /* Capture the per-loop launches in a CUDA graph and replay it n times. */
 mk_status mk_advance_graph(mk_handle* h, int64_t nsteps);
@@ -290,12 +294,12 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps);
  * the fused multiphase loop ran out since the last check (the loops since
  * then are invalid; the handle stays usable). */
 mk_status mk_sync(mk_handle* h);
-/* Loop form of a multiphase case: 1 the fused one-launch loop with one
- * producer warp per CTA (the default when the case admits it), 2 the fused
- * loop in which every warp computes phi and collides, 0 the phi kernel plus
- * the collision kernel.  MK_ERR_ARG when 1 or 2 is asked of a case that does
- * not admit the fused loop.  The autotuner may change the form; mk_get_fused
- * reports the current one. */
+/* Loop form of a multiphase case: 0 the phi kernel plus the collision kernel
+ * (the default), 1 the fused one-launch loop (cases with an x extent that is a
+ * multiple of 4 and at least 8 planes in z).  Both give bit-identical
+ * results; the autotuner keeps the faster (the two-kernel loop on B200 for
+ * the 256^3 bubble case).  MK_ERR_ARG when 1 is asked of a case that does not
+ * admit the fused loop.  mk_get_fused reports the current form. */
 mk_status mk_set_fused(mk_handle* h, int32_t fused);
 int32_t mk_get_fused(const mk_handle* h);
 /* Test hook of the failure detection, no counterpart in the reference.
@@ -448,6 +452,15 @@ int64_t mk_ensemble_step(const mk_ensemble* e);
 #define MK_NOALLOC_MAX_CELLS ((int64_t)MK_NOALLOC_MAX_BLOCKS * 256 * 64)
 mk_status mk_field_stats_noalloc(const float* d_field, int64_t n, double* d_out, void* stream);
 const char* mk_noalloc_last_error(void);
+
+/* JSON-lines metrics log, no counterpart in the reference (its only record is
+ * the write_document text file, MaterKit.cpp:126-184).  With a path set, every
+ * mk_time_advance appends {"event": "time_advance", model, precision, step,
+ * loops, ms, mlups, gbs (algorithmic bytes), launches_per_loop} and every
+ * mk_diagnostics {"event": "diagnostics", model, step, mass, phi_sum,
+ * mass_drift, phi_drift (relative to the handle's first diagnostics),
+ * solid_frac, max_speed, n_bad}.  NULL stops the log.  Process-wide. */
+mk_status mk_set_metrics_log(const char* path);
 
 /* Algorithmic bytes per cell per step of the handle's configuration. */
 double mk_bytes_per_cell(const mk_handle* h);

@@ -120,8 +120,10 @@ class mkSolver {
 
 // Flow and dendrite solver (MaterKit/inc/mkFluidsMRT.h).  The model comes from
 // initialize(xml, model): MK_MODEL_FLOW (run_flow_Poiseuille),
-// MK_MODEL_THERMAL_DENDRITE (run_thermal_dendrite), MK_MODEL_FLOW_DENDRITE
-// (run_flow_thermal_dendrite) or MK_MODEL_MULTIGRAIN (run_multiPhaseField).
+// MK_MODEL_THERMAL_DENDRITE (run_thermal_dendrite), MK_MODEL_SOLUTAL_DENDRITE
+// (run_solutal_dendrite), MK_MODEL_FLOW_DENDRITE (run_flow_thermal_dendrite),
+// MK_MODEL_FLOW_SOLUTAL (run_flow_solutal_dendrite) or MK_MODEL_MULTIGRAIN
+// (run_multiPhaseField).
 class mkFluidsMRT : public mkSolver {
  public:
   explicit mkFluidsMRT(const mkSpace& s) : mkSolver(s, MK_MODEL_FLOW) {}
@@ -140,13 +142,24 @@ class mkFluidsMRT : public mkSolver {
   void propagate_PBB() { call("propagate_PBB", seq()); }
   void bdyVelocity() { call("bdyVelocity", seq()); }
   void bdy_flowin() { call("bdy_flowin", seq()); }
+  // mkPhaseField::relaxation_anisotropy_solute(loops), mkSolutalField::propagate /
+  // relaxation / bdy_LBflowin (MaterKit.cpp:665-674, 448-456)
+  void relaxation_anisotropy_solute(int /*loops*/) { call("pf_relax_solute", seq()); }
+  void solutal_propagate() { call("c_propagate", seq()); }
+  void solutal_relaxation() { call("c_relax", seq()); }
+  void bdy_LBflowin() { call("bdy_LBflowin", seq()); }
 
  private:
   std::vector<std::string> seq() const {
     if (model_ == MK_MODEL_FLOW_DENDRITE)
       return {"propagate_PBB", "relaxation", "bdyVelocity", "pf_propagate", "pf_relax", "t_propagate", "t_relax",
               "bdy_flowin"};
-    if (model_ == MK_MODEL_THERMAL_DENDRITE || model_ == MK_MODEL_SOLUTAL_DENDRITE)
+    if (model_ == MK_MODEL_FLOW_SOLUTAL)  // run_flow_solutal_dendrite (MaterKit.cpp:430-456)
+      return {"propagate_PBB", "relaxation", "bdyVelocity", "pf_propagate", "pf_relax_solute", "c_propagate",
+              "c_relax", "bdy_LBflowin"};
+    if (model_ == MK_MODEL_SOLUTAL_DENDRITE)  // run_solutal_dendrite (MaterKit.cpp:665-674)
+      return {"pf_propagate", "pf_relax_solute", "c_propagate", "c_relax"};
+    if (model_ == MK_MODEL_THERMAL_DENDRITE)
       return {"pf_propagate", "pf_relax", "t_propagate", "t_relax"};
     if (model_ == MK_MODEL_MULTIGRAIN)  // run_multiPhaseField (MaterKit.cpp:563-567)
       return {"propagate", "relaxation", "t_propagate", "t_relax"};

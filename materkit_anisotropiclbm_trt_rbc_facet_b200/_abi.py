@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "MK_OK", 1: "MK_ERR_XML", 2: "MK_ERR_ARG", 3: "MK_ERR_CUDA", 
                 5: "MK_ERR_TIMEOUT", 6: "MK_ERR_OOM", 7: "MK_ERR_IO", 8: "MK_ERR_STATE", 9: "MK_ERR_NODEVICE"}
 
 (MK_MODEL_FLOW, MK_MODEL_MULTIPHASE, MK_MODEL_THERMAL_DENDRITE, MK_MODEL_SOLUTAL_DENDRITE, MK_MODEL_CONVECTION,
- MK_MODEL_FLOW_DENDRITE, MK_MODEL_MULTIGRAIN) = range(7)
+ MK_MODEL_FLOW_DENDRITE, MK_MODEL_MULTIGRAIN, MK_MODEL_FLOW_SOLUTAL) = range(8)
 MK_PREC_FP64, MK_PREC_FP32, MK_PREC_FP16, MK_PREC_BF16 = range(4)
 MK_COLL_BGK, MK_COLL_TRT, MK_COLL_MRT = range(3)
 MK_D3Q7, MK_D3Q19, MK_D3Q27 = 7, 19, 27
@@ -34,7 +34,8 @@ MK_NOALLOC_MAX_CELLS = 2048 * 256 * 64
 PRECISIONS = {"fp64": MK_PREC_FP64, "fp32": MK_PREC_FP32, "fp16": MK_PREC_FP16, "bf16": MK_PREC_BF16}
 MODELS = {"flow": MK_MODEL_FLOW, "multiphase": MK_MODEL_MULTIPHASE, "thermal_dendrite": MK_MODEL_THERMAL_DENDRITE,
           "solutal_dendrite": MK_MODEL_SOLUTAL_DENDRITE, "convection": MK_MODEL_CONVECTION,
-          "flow_dendrite": MK_MODEL_FLOW_DENDRITE, "multigrain": MK_MODEL_MULTIGRAIN}
+          "flow_dendrite": MK_MODEL_FLOW_DENDRITE, "multigrain": MK_MODEL_MULTIGRAIN,
+          "flow_solutal_dendrite": MK_MODEL_FLOW_SOLUTAL}
 FIELDS = {"rho": MK_FIELD_RHO, "ux": MK_FIELD_UX, "uy": MK_FIELD_UY, "uz": MK_FIELD_UZ, "T": MK_FIELD_T,
           "C": MK_FIELD_C, "phi": MK_FIELD_PHI, "flag": MK_FIELD_FLAG, "pressure": MK_FIELD_PRESSURE,
           "dphi": MK_FIELD_DPHI, "grain": MK_FIELD_GRAIN}
@@ -165,6 +166,7 @@ PROTOTYPES = {
     "mk_ensemble_step": (C.c_int64, [H]),
     "mk_field_stats_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "mk_noalloc_last_error": (C.c_char_p, []),
+    "mk_set_metrics_log": (C.c_int, [C.c_char_p]),
     "mk_bytes_per_cell": (C.c_double, [H]),
     "mk_fluid_cells": (C.c_int64, [H]),
     "mk_launches_per_step": (C.c_int32, [H]),

@@ -203,6 +203,35 @@ def flow_dendrite(nx=96, ny=64, nz=64, loops=3000, precision="fp32", u_in=0.02, 
 """
 
 
+def flow_solutal_dendrite(nx=96, ny=64, nz=64, loops=3000, precision="fp32", u_in=0.02, eps4=0.04, W0=1.5,
+                          lam=10.0, delta=0.55, D=0.1, D_s=1e-4, k=0.15, radius=6.0, center=None, tau=0.8,
+                          inlet=True, collision="TRT", lattice="D3Q19") -> str:
+    """Solutal dendrite in a melt flowing in at x = 0 with `u_in` and out at
+    x = nx - 1 (run_flow_solutal_dendrite); periodic across.  `inlet=False`
+    closes the x faces (the flow then stays at rest)."""
+    c = center if center is not None else (nx / 3.0, (ny - 1) / 2.0, (nz - 1) / 2.0)
+    bc = "closed periodic periodic" if inlet else "closed closed closed"
+    return _HEADER.format(dendrite="true", flow="true", loops=loops, frames=min(loops, 100), nx=nx, ny=ny, nz=nz) + f"""
+  <flow> <acceleration> 0.0 0.0 0.0 </acceleration> <velocityInlet> {u_in} 0.0 0.0 </velocityInlet> </flow>
+  <phasechange>
+    <d0> 0.2762 </d0> <lambda> {lam} </lambda> <anisotropy> {eps4} </anisotropy> <W0> 1.0 </W0> <t0> 1.0 </t0>
+    <seed> <number> 1 </number> <center> {c[0]} {c[1]} {c[2]} </center> <angle> 0 0 0 </angle>
+      <radius> {radius} </radius> </seed>
+  </phasechange>
+  <composition> <number> 1 </number> <diffFluid> {D} </diffFluid> <diffSolid> {D_s} </diffSolid>
+    <iniValue> {-delta} </iniValue> <partition> {k} </partition> </composition>
+  <b200>
+    <model> flow_solutal_dendrite </model> <precision> {precision} </precision> <boundary> {bc} </boundary>
+    <lattice> {lattice} </lattice> <collision> {collision} </collision>
+    <tau> {tau} </tau> <magic> 0.1875 </magic> <rho0> 1.0 </rho0> <velocity> {u_in} 0 0 </velocity>
+    <inlet> {1 if inlet else 0} </inlet>
+    <eps4> {eps4} </eps4> <W0> {W0} </W0> <lambda> {lam} </lambda> <delta> {delta} </delta>
+    <diffusivity> {D} </diffusivity> <diffSolid> {D_s} </diffSolid> <partition> {k} </partition>
+  </b200>
+</MaterKit>
+"""
+
+
 def multigrain(n=48, loops=1000, precision="fp32", seeds=None, W0=1.5, mobility=1.0, kappa=1.0, delta=0.3,
                D=0.1, nz=None, ny=None) -> str:
     """Multiphase field of grains (run_multiPhaseField): one order parameter

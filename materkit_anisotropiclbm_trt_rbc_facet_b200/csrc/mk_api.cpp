@@ -6,11 +6,13 @@
 // handle, in a thread-local slot (mk_last_global_error).  There is no CPU
 // fallback: without a CUDA device mk_create* returns MK_ERR_NODEVICE.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -18,6 +20,7 @@
 #include "../../include/mkb200.h"
 #include "mk_case.hpp"
 #include "mk_engine.hpp"
+#include "mk_models.hpp"
 
 struct mk_handle {
   mke::Engine e;
@@ -28,9 +31,41 @@ struct mk_handle {
   int32_t tip_seed = -1;
   double tip_iso = 0.0;
   double tip_len[6] = {0, 0, 0, 0, 0, 0};
+  // first diagnostics of the handle (reference of the drift in the metrics log)
+  bool have_d0 = false;
+  double d0_mass = 0.0, d0_phi = 0.0;
 };
 
 namespace {
+
+// NVTX range around an entry point (visible in Nsight Systems / ncu timelines;
+// without a tool attached the push / pop cost a few instructions).
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
+
+// JSON-lines metrics log (mk_set_metrics_log): one object per timed advance
+// and per diagnostics call, appended under a process-wide lock.
+std::mutex g_metrics_mu;
+std::string g_metrics_path;
+
+void metrics_line(const std::string& body) {
+  std::lock_guard<std::mutex> lock(g_metrics_mu);
+  if (g_metrics_path.empty()) return;
+  FILE* f = fopen(g_metrics_path.c_str(), "a");
+  if (!f) return;
+  fprintf(f, "{%s}\n", body.c_str());
+  fclose(f);
+}
+
+std::string fmt(const char* k, double v) {
+  char b[96];
+  snprintf(b, sizeof b, "\"%s\": %.17g", k, v);
+  return b;
+}
 
 thread_local std::string g_err;
 
@@ -98,6 +133,21 @@ const char* mk_version_string(void) { return "mkb200 1.0 (sm_100a)"; }
 
 const char* mk_last_global_error(void) { return g_err.c_str(); }
 
+mk_status mk_set_metrics_log(const char* path) {
+  std::lock_guard<std::mutex> lock(g_metrics_mu);
+  g_metrics_path = path ? path : "";
+  if (!g_metrics_path.empty()) {
+    FILE* f = fopen(g_metrics_path.c_str(), "a");
+    if (!f) {
+      g_err = std::string("cannot open metrics log ") + g_metrics_path;
+      g_metrics_path.clear();
+      return MK_ERR_IO;
+    }
+    fclose(f);
+  }
+  return MK_OK;
+}
+
 mk_status mk_read_parameters(const char* xml_path, int32_t* max_loops, int32_t* max_frames) {
   if (!xml_path || !max_loops || !max_frames) return set_global(MK_ERR_ARG, "null argument");
   std::string err;
@@ -127,6 +177,7 @@ mk_status mk_case_initial_field(const mk_params* p, int32_t field, double* out, 
 }
 
 mk_status mk_create(const mk_params* p, mk_handle** out) {
+  const Range nvtx_range("mk_create");
   if (!p || !out) return set_global(MK_ERR_ARG, "null argument");
   *out = nullptr;
   std::string err;
@@ -147,7 +198,7 @@ mk_status mk_create(const mk_params* p, mk_handle** out) {
   const size_t n = (size_t)h->e.ncell;
   const bool flow = p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION;
   const bool scalar = p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
-                      p->model == MK_MODEL_CONVECTION || p->model == MK_MODEL_FLOW_DENDRITE ||
+                      p->model == MK_MODEL_CONVECTION || mkm::flow_coupled(p->model) ||
                       p->model == MK_MODEL_MULTIGRAIN;
   std::vector<double> phi(flow ? 0 : n), temp(scalar ? n : 0), rho(flow ? n : 0);
   if (!flow) mkc::initial_field(p, MK_FIELD_PHI, phi.data(), n, err);
@@ -205,6 +256,7 @@ mk_status mk_get_params(const mk_handle* h, mk_params* out) {
 int64_t mk_get_step(const mk_handle* h) { return h ? h->e.step : -1; }
 
 mk_status mk_advance(mk_handle* h, int64_t nsteps) {
+  const Range nvtx_range("mk_advance");
   if (!h || nsteps < 0) return MK_ERR_ARG;
   for (int64_t t = 0; t < nsteps; ++t) {
     cudaError_t st = mke::engine_step(h->e, nullptr);
@@ -214,6 +266,7 @@ mk_status mk_advance(mk_handle* h, int64_t nsteps) {
 }
 
 mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
+  const Range nvtx_range("mk_advance_graph");
   if (!h || nsteps < 0) return MK_ERR_ARG;
   mke::Engine& e = h->e;
   int64_t left = nsteps;
@@ -290,8 +343,8 @@ mk_status mk_sync(mk_handle* h) {
 
 mk_status mk_set_fused(mk_handle* h, int32_t fused) {
   if (!h) return MK_ERR_ARG;
-  if (fused < 0 || fused > 2) {
-    h->err = "loop form must be 0, 1 or 2";
+  if (fused < 0 || fused > 1) {
+    h->err = "loop form must be 0 or 1";
     return MK_ERR_ARG;
   }
   if (fused && !h->e.wave_ok) {
@@ -299,9 +352,8 @@ mk_status mk_set_fused(mk_handle* h, int32_t fused) {
              "at least 8 planes in z)";
     return MK_ERR_ARG;
   }
-  const int form = fused == 1 ? 2 : (fused == 2 ? 1 : 0);
-  if (form != h->e.wave) {
-    h->e.wave = form;
+  if (fused != h->e.wave) {
+    h->e.wave = fused;
     for (auto& g : h->graph)
       if (g) {
         cudaGraphExecDestroy(g);
@@ -311,10 +363,7 @@ mk_status mk_set_fused(mk_handle* h, int32_t fused) {
   return MK_OK;
 }
 
-int32_t mk_get_fused(const mk_handle* h) {
-  if (!h || !h->e.wave_ok || !h->e.wave) return 0;
-  return h->e.wave == 2 ? 1 : 2;
-}
+int32_t mk_get_fused(const mk_handle* h) { return h && h->e.wave_ok && h->e.wave ? 1 : 0; }
 
 mk_status mk_inject_fault(mk_handle* h, int32_t kind) {
   if (!h) return MK_ERR_ARG;
@@ -337,6 +386,7 @@ mk_status mk_get_stream(mk_handle* h, void** stream) {
 }
 
 mk_status mk_get_field(mk_handle* h, int32_t field, int32_t dtype, void* host_dst, size_t bytes) {
+  const Range nvtx_range("mk_get_field");
   if (!h || !host_dst) return MK_ERR_ARG;
   const size_t n = (size_t)h->e.ncell;
   const size_t need = n * (dtype == MK_DTYPE_F64 ? 8 : 4);
@@ -407,7 +457,7 @@ mk_status mk_set_state(mk_handle* h, const double* phi, const double* temp, cons
     mkc::initial_field(&p, MK_FIELD_PHI, dphi.data(), n, err);
     phi = dphi.data();
   }
-  const double* tt = p.model == MK_MODEL_SOLUTAL_DENDRITE ? conc : temp;
+  const double* tt = mkm::solutal(p.model) ? conc : temp;
   if (!tt) {
     dt.resize(n);
     mkc::initial_field(&p, MK_FIELD_T, dt.data(), n, err);
@@ -430,7 +480,7 @@ mk_status mk_set_state_f32(mk_handle* h, const float* phi, const float* temp, co
     dphi.assign(tmp.begin(), tmp.end());
     phi = dphi.data();
   }
-  const float* tt = p.model == MK_MODEL_SOLUTAL_DENDRITE ? conc : temp;
+  const float* tt = mkm::solutal(p.model) ? conc : temp;
   cudaError_t st = mke::engine_set_state_f32(h->e, phi, tt);
   if (st == cudaSuccess) st = cudaStreamSynchronize(h->e.stream);
   if (st != cudaSuccess) return cuda_fail(h, st, "set_state_f32");
@@ -438,6 +488,7 @@ mk_status mk_set_state_f32(mk_handle* h, const float* phi, const float* temp, co
 }
 
 mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
+  const Range nvtx_range("mk_write_vtk");
   if (!h || !dir) return MK_ERR_ARG;
   const mk_params& p = h->e.p;
   const int64_t n = h->e.ncell;
@@ -445,7 +496,7 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   std::vector<double> rho(n, 1.0), grain(n, 0.0), phi(n, 0.0), dphi(n, 0.0), conc(n, 0.0), temp(n, 0.0), ux(n, 0.0),
       uy(n, 0.0), uz(n, 0.0);
   mk_status s;
-  if (m == MK_MODEL_FLOW || m == MK_MODEL_MULTIPHASE || m == MK_MODEL_CONVECTION || m == MK_MODEL_FLOW_DENDRITE) {
+  if (m == MK_MODEL_FLOW || m == MK_MODEL_MULTIPHASE || m == MK_MODEL_CONVECTION || mkm::flow_coupled(m)) {
     if ((s = copy_field(h, MK_FIELD_RHO, rho)) != MK_OK) return s;
     if ((s = copy_field(h, MK_FIELD_UX, ux)) != MK_OK) return s;
     if ((s = copy_field(h, MK_FIELD_UY, uy)) != MK_OK) return s;
@@ -454,9 +505,8 @@ mk_status mk_write_vtk(mk_handle* h, int64_t loops, const char* dir) {
   if ((s = copy_field(h, MK_FIELD_GRAIN, grain)) != MK_OK) return s;
   if ((s = copy_field(h, MK_FIELD_PHI, phi)) != MK_OK) return s;
   if (m == MK_MODEL_CONVECTION && (s = copy_field(h, MK_FIELD_T, temp)) != MK_OK) return s;
-  if (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE ||
-      m == MK_MODEL_MULTIGRAIN) {
-    const bool th = m != MK_MODEL_SOLUTAL_DENDRITE;
+  if (mkm::dendrite(m) || m == MK_MODEL_MULTIGRAIN) {
+    const bool th = !mkm::solutal(m);
     if ((s = copy_field(h, MK_FIELD_DPHI, dphi)) != MK_OK) return s;
     if ((s = copy_field(h, th ? MK_FIELD_T : MK_FIELD_C, th ? temp : conc)) != MK_OK) return s;
   }
@@ -546,6 +596,7 @@ mk_status mk_tip_track(mk_handle* h, int32_t seed, double iso, mk_tip* out) {
 }
 
 mk_status mk_diagnostics(mk_handle* h, mk_diag* out) {
+  const Range nvtx_range("mk_diagnostics");
   if (!h || !out) return MK_ERR_ARG;
   double v[mke::DG_N];
   cudaError_t st = mke::engine_diag(h->e, v);
@@ -564,6 +615,17 @@ mk_status mk_diagnostics(mk_handle* h, mk_diag* out) {
   out->solute = v[mke::DG_SOLUTE];
   out->max_speed = v[mke::DG_MAXU];
   out->n_bad = (int32_t)v[mke::DG_BAD];
+  if (!h->have_d0) {
+    h->have_d0 = true;
+    h->d0_mass = out->mass;
+    h->d0_phi = out->phi_sum;
+  }
+  metrics_line("\"event\": \"diagnostics\", " + fmt("model", h->e.p.model) + ", " + fmt("step", (double)out->step) +
+               ", " + fmt("mass", out->mass) + ", " + fmt("phi_sum", out->phi_sum) + ", " +
+               fmt("mass_drift", h->d0_mass != 0 ? (out->mass - h->d0_mass) / h->d0_mass : 0.0) + ", " +
+               fmt("phi_drift", h->d0_phi != 0 ? (out->phi_sum - h->d0_phi) / h->d0_phi : 0.0) + ", " +
+               fmt("solid_frac", out->solid_frac) + ", " + fmt("max_speed", out->max_speed) + ", " +
+               fmt("n_bad", out->n_bad));
   if (out->n_bad > 0) {
     h->err = "diverged: non-finite or non-positive state in " + std::to_string(out->n_bad) + " cells";
     return MK_ERR_DIVERGED;
@@ -602,6 +664,7 @@ mk_status mk_nusselt(mk_handle* h, double* nu) {
 static const char kMagic[8] = {'M', 'K', 'B', '2', '0', '0', 'C', 'K'};
 
 mk_status mk_checkpoint(mk_handle* h, const char* path) {
+  const Range nvtx_range("mk_checkpoint");
   if (!h || !path) return MK_ERR_ARG;
   mke::Engine& e = h->e;
   cudaError_t st = cudaStreamSynchronize(e.stream);
@@ -646,6 +709,7 @@ mk_status mk_checkpoint(mk_handle* h, const char* path) {
 }
 
 mk_status mk_restore(mk_handle* h, const char* path) {
+  const Range nvtx_range("mk_restore");
   if (!h || !path) return MK_ERR_ARG;
   mke::Engine& e = h->e;
   FILE* f = fopen(path, "rb");
@@ -743,6 +807,7 @@ mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel, dou
 }
 
 mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, double* ms) {
+  const Range nvtx_range("mk_time_advance");
   if (!h || nsteps < 0 || !ms) return MK_ERR_ARG;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
@@ -758,11 +823,21 @@ mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, doubl
   if (s != MK_OK) return s;
   if (st != cudaSuccess) return cuda_fail(h, st, "time_advance");
   *ms = f;
+  if (f > 0) {
+    const double cells = (double)h->e.ncell;
+    metrics_line("\"event\": \"time_advance\", " + fmt("model", h->e.p.model) + ", " +
+                 fmt("precision", h->e.p.precision) + ", " + fmt("step", (double)h->e.step) + ", " +
+                 fmt("loops", (double)nsteps) + ", " + fmt("ms", f) + ", " +
+                 fmt("mlups", cells * nsteps / (f * 1e-3) / 1e6) + ", " +
+                 fmt("gbs", mke::engine_bytes_per_cell(h->e) * cells * nsteps / (f * 1e-3) / 1e9) + ", " +
+                 fmt("launches_per_loop", mke::engine_kernels_per_step(h->e)));
+  }
   return MK_OK;
 }
 
 mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32_t* block_y, int32_t* minb,
                       double* ms_per_step) {
+  const Range nvtx_range("mk_autotune");
   if (!h || trial_steps < 1) return MK_ERR_ARG;
   mke::TuneResult r;
   cudaError_t st = mke::engine_autotune(h->e, trial_steps, &r);
@@ -781,6 +856,7 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
 }
 
 mk_status mk_backward(mk_handle* h, const mk_loss* loss, mk_grad* out) {
+  const Range nvtx_range("mk_backward");
   if (!h || !loss || !out || !loss->target_phi) return MK_ERR_ARG;
   std::string err;
   double r[5] = {0, 0, 0, 0, 0};

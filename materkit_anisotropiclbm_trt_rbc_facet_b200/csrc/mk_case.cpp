@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "mk_models.hpp"
 #include "mk_xml.hpp"
 
 namespace mkc {
@@ -224,7 +225,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model < 0 || p->model > MK_MODEL_MULTIGRAIN) {
+  if (p->model < 0 || p->model > MK_MODEL_FLOW_SOLUTAL) {
     err = "unknown model";
     return MK_ERR_ARG;
   }
@@ -255,7 +256,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
     }
   }
   if (p->inlet) {
-    if (p->model != MK_MODEL_FLOW && p->model != MK_MODEL_FLOW_DENDRITE) {
+    if (p->model != MK_MODEL_FLOW && !mkm::flow_coupled(p->model)) {
       err = "inflow / outflow faces apply to the flow and flow + dendrite models";
       return MK_ERR_ARG;
     }
@@ -268,7 +269,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION || p->model == MK_MODEL_FLOW_DENDRITE) {
+  if (p->model == MK_MODEL_FLOW || p->model == MK_MODEL_CONVECTION || mkm::flow_coupled(p->model)) {
     if (p->lattice != MK_D3Q19 && p->lattice != MK_D3Q27) {
       err = "flow lattice must be D3Q19 or D3Q27";
       return MK_ERR_ARG;
@@ -309,8 +310,7 @@ mk_status validate_params(const mk_params* p, std::string& err) {
       return MK_ERR_ARG;
     }
   }
-  if (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
-      p->model == MK_MODEL_FLOW_DENDRITE) {
+  if (mkm::dendrite(p->model)) {
     if (!(p->W0 > 0 && p->tau0 > 0 && p->D > 0)) {
       err = "phase-field parameters out of range (W0, tau0, D > 0)";
       return MK_ERR_ARG;
@@ -388,6 +388,8 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       model = MK_MODEL_CONVECTION;
     else if (m == "flow_dendrite" || m == "flow_thermal_dendrite")
       model = MK_MODEL_FLOW_DENDRITE;
+    else if (m == "flow_solutal_dendrite" || m == "flow_solutal")
+      model = MK_MODEL_FLOW_SOLUTAL;
     else if (m == "multigrain" || m == "multiphasefield" || m == "multi_phase_field")
       model = MK_MODEL_MULTIGRAIN;
     else {
@@ -515,7 +517,7 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
       if (iv < 1e299) p.delta = -iv;
     }
     p.bc[0] = p.bc[1] = p.bc[2] = MK_BC_CLOSED;
-    if (model == MK_MODEL_FLOW_DENDRITE) {
+    if (mkm::flow_coupled(model)) {
       // the melt flows in at x = 0 with flow/velocityInlet and out at
       // x = nx - 1 (boundary_vel, mkFluidsUser.cpp:455-617); periodic across
       double nu = -1;
@@ -777,7 +779,7 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
           case MK_FIELD_UX:
           case MK_FIELD_UY:
           case MK_FIELD_UZ:
-            if (p->model == MK_MODEL_FLOW_DENDRITE) {
+            if (mkm::flow_coupled(p->model)) {
               // u0 scaled by the liquid fraction of the seeded phi
               const double ns = std::min(1.0, std::max(0.0, 0.5 * (1.0 + seed_phi(p, pos))));
               v = (1.0 - ns) * p->u0[field - MK_FIELD_UX];
@@ -820,10 +822,7 @@ mk_status initial_field(const mk_params* p, int field, double* out, size_t ncell
                 best = k;
               }
             }
-            v = (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
-                 p->model == MK_MODEL_FLOW_DENDRITE)
-                    ? best
-                    : 0;
+            v = mkm::dendrite(p->model) ? best : 0;
             if (p->model == MK_MODEL_MULTIGRAIN) {
               // the grain whose order parameter is largest (ties to the lower index)
               double bp = -1e300;

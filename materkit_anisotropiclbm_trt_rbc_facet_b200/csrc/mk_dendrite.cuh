@@ -46,7 +46,10 @@ __global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P
   typedef typename Stor<S>::T T;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
+  // planes in descending order: the collision kernel that follows walks them
+  // ascending and starts on the planes whose populations this kernel read
+  // last (still in L2)
+  const int z = g.nz - 1 - (int)blockIdx.z;
   if (x >= g.nx || y >= g.ny) return;
   if (!g.fluid(x, y, z)) {
     const int64_t c = g.idx(x, y, z);
@@ -162,17 +165,21 @@ __device__ __forceinline__ void anisotropy(const T* __restrict__ Rm, int kind, T
 // One loop of a dendrite cell: the phase-field lattice, then the thermal
 // (SOL = false) or solutal (SOL = true) lattice.  `grain` is the per-cell
 // grain index (read only with more than one grain), `rot` the rotations of
-// the cell's domain, 9 values per grain.  ADV = true advects the thermal
+// the cell's domain, 9 values per grain.  ADV = true advects the scalar
 // equilibrium with the flow velocity (vx, vy, vz): t_eq = w T (1 + 4 e.u)
-// (mkThermalField::relaxation with a flow lattice, getTEquPDFs).
-// NEE = true (with ADV, thermal only) also applies the inflow / outflow faces
-// of the flow + dendrite model in registers: the cell at x = 0 (x = nx - 1)
-// takes the post-collision g, t of its inner neighbour — the next (previous)
-// lane of its warp, so nx % 32 != 1 and the row starts a warp — by shuffles:
+// (mkThermalField::relaxation with a flow lattice, getTEquPDFs); for the
+// solutal lattice the advective flux U u joins the anti-trapping current in
+// the equilibrium's first moment (the liquid's w U (1 + 4 e.u)).
+// NEE = true (with ADV) also applies the inflow / outflow faces of the flow
+// + dendrite models in registers: the cell at x = 0 (x = nx - 1) takes the
+// post-collision g, t of its inner neighbour — the next (previous) lane of
+// its warp, so nx % 32 != 1 and the row starts a warp — by shuffles:
 //   g(b) = g(n) + w (phi_b - phi_n),
 //   t(b) = t(n) + w T_b (1 + 4 e.u_b) - w T_n (1 + 4 e.u_n),
 // inflow phi_b = -1, T_b = ref_t; outflow phi_b = phi_n, T_b = T_n; u_b is
-// the face cell's own (vx, vy, vz), u_n the neighbour's; temp(b) = T_b.
+// the face cell's own (vx, vy, vz), u_n the neighbour's; temp(b) = T_b (T is
+// the supersaturation U for the solutal lattice: bdy_LBflowin,
+// mkSolutalField.h:53).
 template <class S, class P, int PARITY, bool SOL, bool GEN, class NB, bool ADV = false, bool NEE = false>
 __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new,
                                           const P* __restrict__ phi_old, P* __restrict__ temp,
@@ -181,7 +188,7 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
                                           const NB& nb, const int c, const DendK<typename Stor<S>::T>& k,
                                           typename Stor<S>::T vx = 0, typename Stor<S>::T vy = 0,
                                           typename Stor<S>::T vz = 0, int x = 0, int nx = 0) {
-  static_assert(!NEE || (ADV && !SOL), "the face pass belongs to the advected thermal lattice");
+  static_assert(!NEE || ADV, "the face pass belongs to the advected scalar lattice");
   typedef typename Stor<S>::T T;
   // FP32 / FP64: both lattices' slots go to L2 now, while the phi stencil
   // and the anisotropy are computed (the kernel waits on load latency;
@@ -275,7 +282,9 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
     const T om = div_fast(cap, T(4) * cD + T(0.5) * cap);
     {
       const T w0 = SU ? T(1) : T(wq<7>(0));
-      if constexpr (SU)
+      if constexpr (NEE)
+        t[0] = w0 * dT + w0 * su;  // stored after the face pass below
+      else if constexpr (SU)
         st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
       else
         st_out<S, 7>(Tp, stride, nb, PARITY, c, 0, w0 * dT + w0 * su);
@@ -284,11 +293,15 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
     for (int i = 1; i < 7; i += 2) {
       const int j = i + 1;
       const T w = SU ? T(1) : T(wq<7>(i));
-      const T ej = fj * (T(ex(i)) * gr[0] + T(ey(i)) * gr[1] + T(ez(i)) * gr[2]);
+      T ej = fj * (T(ex(i)) * gr[0] + T(ey(i)) * gr[1] + T(ez(i)) * gr[2]);
+      if constexpr (ADV) ej += U * (T(ex(i)) * vx + T(ey(i)) * vy + T(ez(i)) * vz);
       const T sym = w * dT;
       const T am = T(0.5) * (t[i] - t[j]);
       const T am_new = am - om * (am - w * T(4) * ej);
-      if constexpr (SU) {
+      if constexpr (NEE) {
+        t[i] = sym + am_new + w * su;
+        t[j] = sym - am_new + w * su;
+      } else if constexpr (SU) {
         st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, i, sym + am_new + w * su);
         st_out_raw<S, 7>(Tp, stride, nb, PARITY, c, j, sym - am_new + w * su);
       } else {
@@ -317,7 +330,7 @@ __device__ __forceinline__ void dend_cell(S* __restrict__ G, S* __restrict__ Tp,
     }
   }
   T Tc = k.ref_t + dT;
-  if constexpr (NEE && !SOL) {
+  if constexpr (NEE) {
     const unsigned act = __activemask();
     const bool edge = x == 0 || x == nx - 1;
     if (__any_sync(act, edge)) {

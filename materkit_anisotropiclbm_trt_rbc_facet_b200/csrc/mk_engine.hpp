@@ -68,13 +68,11 @@ struct Engine {
   // launch counters
   int64_t launches;
   // fused multiphase step: one cooperative launch per loop (k_mp_wave)
-  int wave;              // multiphase loop form: 0 phi kernel + collision kernel, 1 fused, 2 fused with a
-                         // producer warp per CTA (warp-specialised)
+  int wave;              // multiphase loop form: 0 phi kernel + collision kernel, 1 fused
   int wave_ok;           // the case admits the fused loop (x extent a multiple of 4, nz >= 8, grid co-resident)
   int wave_sx, wave_sy;  // tiles: 32-cell x segments times y bands
   int wave_rows;         // rows of the tallest band
-  int wave_threads;      // threads per CTA (form 1)
-  int wave_threads_ws;   // threads per CTA (form 2)
+  int wave_threads;      // threads per CTA
   size_t wave_smem;      // dynamic shared memory (the phi ring)
   unsigned* wave_flags;  // per-tile publication counters (zeroed before every launch)
   int* wave_err;         // error word of the bounded waits (0 = none)

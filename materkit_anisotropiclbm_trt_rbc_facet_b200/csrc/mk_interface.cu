@@ -156,7 +156,7 @@ namespace mke {
 static bool has_order_parameter(const Engine& e) {
   return e.p.model == MK_MODEL_MULTIPHASE || e.p.model == MK_MODEL_THERMAL_DENDRITE ||
          e.p.model == MK_MODEL_SOLUTAL_DENDRITE || e.p.model == MK_MODEL_FLOW_DENDRITE ||
-         e.p.model == MK_MODEL_MULTIGRAIN;
+         e.p.model == MK_MODEL_FLOW_SOLUTAL || e.p.model == MK_MODEL_MULTIGRAIN;
 }
 
 template <class P>

@@ -24,6 +24,7 @@
 
 #include "mk_device.cuh"
 #include "mk_engine.hpp"
+#include "mk_models.hpp"
 #include "mk_shared.cuh"
 
 using namespace mkd;
@@ -449,7 +450,7 @@ __global__ void __launch_bounds__(256)
 // With the face pass (NEE) the cell keeps both lattices' outputs until the
 // shuffles: four resident blocks per SM (64 registers, a few spilled bytes)
 // measured faster (128^3 FP32 81.5 -> 72.1 us) than the default allocation.
-template <class S, class P, int PARITY, bool GEN, bool NEE>
+template <class S, class P, int PARITY, bool GEN, bool NEE, bool SOL>
 __global__ void __launch_bounds__(256, NEE ? 4 : 1)
     k_fd_dend(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phi_new, const P* __restrict__ phi_old,
               P* __restrict__ temp, const P* __restrict__ vel, const unsigned char* __restrict__ grain,
@@ -463,13 +464,13 @@ __global__ void __launch_bounds__(256, NEE ? 4 : 1)
   if (fastw_cell(g, x, y, z)) {
     const FastW fa = make_fastw(g, x, y, z);
     const int c = fa.c;
-    dend_cell<S, P, PARITY, false, GEN, FastW, true, NEE>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, c,
+    dend_cell<S, P, PARITY, SOL, GEN, FastW, true, NEE>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, fa, c,
                                                           k, T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]), x,
                                                           g.nx);
   } else {
     const Nbr nb(g, x, y, z);
     const int c = nb.idx(0, 0, 0);
-    dend_cell<S, P, PARITY, false, GEN, Nbr, true, NEE>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, k,
+    dend_cell<S, P, PARITY, SOL, GEN, Nbr, true, NEE>(G, Tp, phi_new, phi_old, temp, grain, rot, g.stride, nb, c, k,
                                                         T(vel[c]), T(vel[ncell + c]), T(vel[2 * ncell + c]), x, g.nx);
   }
 }
@@ -801,7 +802,7 @@ __global__ void k_init(int model, int Q0, S* A0, S* A1, S* A2, int Q2, float* H0
     put_eq<S, 19>(A0, g, nb, ci, 1.0, ux, uy, uz, -1.0, refs.r0);
     put_eq<S, 19>(A1, g, nb, ci, ph, ux, uy, uz, 0.0, refs.r1);
     if (H0) H0[c] = float(wq<19>(0) * ((ph - refs.r1) - 1.5 * ph * (ux * ux + uy * uy + uz * uz)));
-  } else if (model == MK_MODEL_FLOW_DENDRITE) {
+  } else if (mkm::flow_coupled(model)) {
     // the flow starts at rho0 with u0 scaled by the liquid fraction (unless
     // given); the thermal equilibrium carries the same velocity
     const double ns = fmin(1.0, fmax(0.0, 0.5 * (1.0 + ph)));
@@ -1089,7 +1090,7 @@ template <class S, class P, int Q>
 __global__ void __launch_bounds__(256) k_diag_fd(const S* __restrict__ W, const P* __restrict__ phi,
                                                  const P* __restrict__ phi_prev, const P* __restrict__ temp,
                                                  const Geom g, int64_t steps_done, double Fx, double Fy, double Fz,
-                                                 double rho0, int64_t n, double* __restrict__ partial) {
+                                                 double rho0, int solutal, int64_t n, double* __restrict__ partial) {
   double v[mke::DG_N];
 #pragma unroll
   for (int q = 0; q < mke::DG_N; ++q) v[q] = 0.0;
@@ -1118,7 +1119,10 @@ __global__ void __launch_bounds__(256) k_diag_fd(const S* __restrict__ W, const 
     v[mke::DG_MZ] += mz;
     v[mke::DG_PHI] += p;
     v[mke::DG_SOLID] += p > 0.0 ? 1.0 : 0.0;
-    v[mke::DG_HEAT] += t - 0.5 * pp;
+    if (solutal)
+      v[mke::DG_SOLUTE] += t;
+    else
+      v[mke::DG_HEAT] += t - 0.5 * pp;
     v[mke::DG_FLUID] += 1.0;
     v[mke::DG_BAD] += bad ? 1.0 : 0.0;
     if (!bad) v[mke::DG_MAXU] = fmax(v[mke::DG_MAXU], sqrt(mx * mx + my * my + mz * mz) / rho);
@@ -1404,14 +1408,17 @@ void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
     const bool gen = e.p.aniso != MK_ANISO_CUBIC;
     const P* vel = (const P*)e.vel;
     const bool nee = fd_faces_in_warp(e);
-#define MK_FDD(PAR, GEN, NEE)                                                                                      \
-  k_fd_dend<S, P, PAR, GEN, NEE><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, vel, \
-                                                               e.grain, (const T*)e.rot, g, kd)
-#define MK_FDD2(PAR, GEN) nee ? MK_FDD(PAR, GEN, true) : MK_FDD(PAR, GEN, false)
+    const bool sol = mkm::solutal(e.p.model);
+#define MK_FDD(PAR, GEN, NEE, SOL)                                                                                 \
+  k_fd_dend<S, P, PAR, GEN, NEE, SOL><<<grid, block, 0, e.stream>>>(G, (S*)e.pop1, phi_new, phi_old, (P*)e.temp, \
+                                                                    vel, e.grain, (const T*)e.rot, g, kd)
+#define MK_FDD2(PAR, GEN, SOL) nee ? MK_FDD(PAR, GEN, true, SOL) : MK_FDD(PAR, GEN, false, SOL)
+#define MK_FDD3(PAR, SOL) gen ? MK_FDD2(PAR, true, SOL) : MK_FDD2(PAR, false, SOL)
     if (parity == 0)
-      gen ? MK_FDD2(0, true) : MK_FDD2(0, false);
+      sol ? MK_FDD3(0, true) : MK_FDD3(0, false);
     else
-      gen ? MK_FDD2(1, true) : MK_FDD2(1, false);
+      sol ? MK_FDD3(1, true) : MK_FDD3(1, false);
+#undef MK_FDD3
 #undef MK_FDD2
 #undef MK_FDD
   }
@@ -1501,6 +1508,7 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
       e.launches += 2;
       break;
     case MK_MODEL_FLOW_DENDRITE:
+    case MK_MODEL_FLOW_SOLUTAL:
       launch_fd<S>(e, parity, grid, block, ev);
       e.phi_cur = 1 - e.phi_cur;
       e.launches += (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
@@ -1550,13 +1558,12 @@ cudaError_t field_t(mke::Engine& e, int field) {
     k_field_mg_grain<P><<<nb, 256, 0, e.stream>>>((const P*)e.phij, e.p.n_objects, e.ncell, e.field);
     return cudaGetLastError();
   }
-  if (field == MK_FIELD_FLAG && m == MK_MODEL_FLOW_DENDRITE) {
+  if (field == MK_FIELD_FLAG && mkm::flow_coupled(m)) {
     k_field_fdflag<P><<<grid, block, 0, e.stream>>>(g, (const P*)e.phi[e.phi_cur], e.field);
     return cudaGetLastError();
   }
   if (field == MK_FIELD_FLAG || field == MK_FIELD_GRAIN) {
-    const int nobj = (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_SOLUTAL_DENDRITE ||
-                      m == MK_MODEL_FLOW_DENDRITE) ? e.p.n_objects : 0;
+    const int nobj = mkm::dendrite(m) ? e.p.n_objects : 0;
     k_field_geom<<<grid, block, 0, e.stream>>>(g, field, e.seeds, nobj, e.field);
     return cudaGetLastError();
   }
@@ -1579,7 +1586,7 @@ cudaError_t field_t(mke::Engine& e, int field) {
                                                         e.p.force[1], e.p.force[2], e.p.rho0, e.field);
     return cudaGetLastError();
   }
-  if (m == MK_MODEL_FLOW_DENDRITE &&
+  if (mkm::flow_coupled(m) &&
       (field == MK_FIELD_RHO || field == MK_FIELD_UX || field == MK_FIELD_UY || field == MK_FIELD_UZ)) {
     const Buoy bu = buoy_of(e.p);
     if (e.Q2 == 19)
@@ -1599,8 +1606,8 @@ cudaError_t field_t(mke::Engine& e, int field) {
     return cudaGetLastError();
   }
   if (field == MK_FIELD_T || field == MK_FIELD_C) {
-    if ((field == MK_FIELD_T) !=
-        (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE || m == MK_MODEL_MULTIGRAIN))
+    if ((field == MK_FIELD_T) != (m == MK_MODEL_THERMAL_DENDRITE || m == MK_MODEL_FLOW_DENDRITE ||
+                                  m == MK_MODEL_MULTIGRAIN))
       return cudaErrorInvalidValue;
     k_field_copy<P><<<nb, 256, 0, e.stream>>>((const P*)e.temp, nullptr, e.ncell, e.field);
     return cudaGetLastError();
@@ -1631,23 +1638,23 @@ cudaError_t diag_t(mke::Engine& e) {
     else
       k_diag_flow<S, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, Tp, bu, ax, g, e.step, e.p.force[0],
                                                    e.p.force[1], e.p.force[2], e.p.rho0, e.ncell, e.partial);
-  } else if (m == MK_MODEL_FLOW_DENDRITE) {
+  } else if (mkm::flow_coupled(m)) {
     const P* ph = (const P*)e.phi[e.phi_cur];
     const P* pp = (const P*)e.phi[1 - e.phi_cur];
     if (e.Q2 == 19)
       k_diag_fd<S, P, 19><<<nb, 256, 0, e.stream>>>((const S*)e.pop2, ph, pp, (const P*)e.temp, g, e.step,
-                                                    e.p.force[0], e.p.force[1], e.p.force[2], e.p.rho0, e.ncell,
-                                                    e.partial);
+                                                    e.p.force[0], e.p.force[1], e.p.force[2], e.p.rho0,
+                                                    mkm::solutal(m) ? 1 : 0, e.ncell, e.partial);
     else
       k_diag_fd<S, P, 27><<<nb, 256, 0, e.stream>>>((const S*)e.pop2, ph, pp, (const P*)e.temp, g, e.step,
-                                                    e.p.force[0], e.p.force[1], e.p.force[2], e.p.rho0, e.ncell,
-                                                    e.partial);
+                                                    e.p.force[0], e.p.force[1], e.p.force[2], e.p.rho0,
+                                                    mkm::solutal(m) ? 1 : 0, e.ncell, e.partial);
   } else if (m == MK_MODEL_MULTIPHASE) {
     k_diag_mp<S><<<nb, 256, 0, e.stream>>>((const S*)e.pop0, (const P*)e.phi[0], g, e.step, mp_coef<T>(e.p, r),
                                            e.ncell, e.partial);
   } else {
     k_diag_dend<P><<<nb, 256, 0, e.stream>>>((const P*)e.phi[e.phi_cur], (const P*)e.phi[1 - e.phi_cur],
-                                             (const P*)e.temp, g, m == MK_MODEL_SOLUTAL_DENDRITE ? 1 : 0, e.ncell,
+                                             (const P*)e.temp, g, mkm::solutal(m) ? 1 : 0, e.ncell,
                                              e.partial);
   }
   k_diag_final<<<1, 256, 0, e.stream>>>(e.partial, nb, e.dsum);
@@ -1712,7 +1719,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     e.Q1 = 7;
   }
   if (p.model == MK_MODEL_MULTIGRAIN) e.Q0 = 7 * p.n_objects;  // one D3Q7 lattice per grain
-  e.Q2 = p.model == MK_MODEL_FLOW_DENDRITE ? p.lattice : 0;
+  e.Q2 = mkm::flow_coupled(p.model) ? p.lattice : 0;
   // Launch shape: a full warp row along x, rows stacked in y to 256 threads.
   int bx = block_x > 0 ? block_x : (p.nx >= 128 ? 128 : (p.nx >= 64 ? 64 : 32));
   int by = block_y > 0 ? block_y : 256 / bx;
@@ -1739,7 +1746,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   if ((st = alloc(&e.pop0, (size_t)e.Q0 * e.stride * e.elem)) != cudaSuccess) return st;
   if ((st = alloc(&e.pop1, (size_t)e.Q1 * e.stride * e.elem)) != cudaSuccess) return st;
   if ((st = alloc(&e.pop2, (size_t)e.Q2 * e.stride * e.elem)) != cudaSuccess) return st;
-  const bool fd = p.model == MK_MODEL_FLOW_DENDRITE;
+  const bool fd = mkm::flow_coupled(p.model);
   if ((st = alloc(&e.vel, fd ? (size_t)3 * e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (p.model == MK_MODEL_MULTIPHASE && e.elem == 2) {
     if ((st = alloc((void**)&e.rest1, (size_t)e.ncell * sizeof(float))) != cudaSuccess) return st;
@@ -1747,8 +1754,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     e.rest1 = nullptr;
   }
   if ((st = alloc(&e.phi[0], (size_t)e.ncell * e.phi_elem)) != cudaSuccess) return st;
-  const bool dend = p.model == MK_MODEL_THERMAL_DENDRITE || p.model == MK_MODEL_SOLUTAL_DENDRITE ||
-                    p.model == MK_MODEL_FLOW_DENDRITE || p.model == MK_MODEL_MULTIGRAIN;
+  const bool dend = mkm::dendrite(p.model) || p.model == MK_MODEL_MULTIGRAIN;
   const bool mg = p.model == MK_MODEL_MULTIGRAIN;
   if ((st = alloc(&e.phij, mg ? (size_t)p.n_objects * e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (mg) {
@@ -1812,7 +1818,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     if (e.wave_ok) {
       if ((st = alloc((void**)&e.wave_flags, (size_t)e.wave_sx * e.wave_sy * sizeof(unsigned))) != cudaSuccess) return st;
       if ((st = alloc((void**)&e.wave_err, sizeof(int))) != cudaSuccess) return st;
-      e.wave = 2;
+      e.wave = 0;  // the two-kernel loop until mk_set_fused or the autotuner chooses the fused one
     }
   }
   // host-side copy of sd must outlive the async copy
@@ -1930,13 +1936,13 @@ static bool one_kernel(const Engine& e) { return e.p.model == MK_MODEL_FLOW || e
 static bool fused_mp(const Engine& e) { return e.p.model == MK_MODEL_MULTIPHASE && e.wave && e.wave_ok; }
 
 int engine_kernels_per_step(const Engine& e) {
-  if (e.p.model == MK_MODEL_FLOW_DENDRITE) return (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
+  if (mkm::flow_coupled(e.p.model)) return (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
   return (one_kernel(e) || fused_mp(e)) ? 1 : 2;
 }
 
 const char* engine_kernel_name(const Engine& e, int k) {
   if (one_kernel(e) || fused_mp(e)) return "collide";
-  if (e.p.model == MK_MODEL_FLOW_DENDRITE) {
+  if (mkm::flow_coupled(e.p.model)) {
     static const char* const names[4] = {"phi", "flow", "collide", "boundary"};
     return k >= 0 && k < 4 ? names[k] : "";
   }
@@ -2043,13 +2049,12 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 2 : 1;
   double best = 1e300;
   int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0;
-  // candidates -2 and -1: the two forms of the fused multiphase loop (their
-  // tiling is fixed by the case)
-  for (int si = e.wave_ok ? -2 : 0; si < 9 && st == cudaSuccess; ++si) {
+  // candidate -1: the fused multiphase loop (its tiling is fixed by the case)
+  for (int si = e.wave_ok ? -1 : 0; si < 9 && st == cudaSuccess; ++si) {
     const int bx = si < 0 ? bx0 : shapes[si][0];
     if (si >= 0 && bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
     for (int mb = 1; mb <= (si < 0 ? 1 : nmb) && st == cudaSuccess; ++mb) {
-      e.wave = si == -2 ? 2 : (si == -1 ? 1 : 0);
+      e.wave = si < 0 ? 1 : 0;
       e.block_x = bx;
       e.block_y = si < 0 ? by0 : shapes[si][1];
       e.minb = (nmb == 2 && si >= 0) ? mb : mb0;

@@ -16,6 +16,25 @@ using namespace mks;
 
 namespace {
 
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const float* __restrict__ H0,
+                                                P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  // planes in descending order: the collision kernel that follows walks them
+  // ascending, so it starts on the planes whose h this kernel read last
+  // (still in L2), and it ends where the next loop's phi kernel starts
+  const int z = g.nz - 1 - (int)blockIdx.z;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
+  if (fast_cell(g, x, y, z)) {
+    const Fast fa = make_fast(g, x, y, z);
+    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, ref_h);
+  } else {
+    const Nbr nb(g, x, y, z);
+    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), ref_h);
+  }
+}
+
 // One loop of a fluid cell.  Every population load (19 g, 19 h) is issued
 // before any store: the loads are the latency the kernel must hide, and a
 // store into the same array in between would stop the compiler from hoisting
@@ -359,10 +378,7 @@ __global__ void __launch_bounds__(256, 2) k_mp_wave(S* __restrict__ G, S* __rest
   // ---- prologue: publish the first P0 planes, stage positions -1, 0, 1
   for (int kk = 0; kk < P0 && kk < nz; ++kk) phi_plane(pub_plane(kk));
   __syncthreads();
-  if (threadIdx.x == 0 && publisher) {
-    __threadfence();
-    mkw::st_release(w.flags + tile, (unsigned)min(P0, nz));
-  }
+  if (threadIdx.x == 0 && publisher) mkw::st_release(w.flags + tile, (unsigned)min(P0, nz));
   wait_neighbours((unsigned)min(P0, nz));
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -386,10 +402,9 @@ __global__ void __launch_bounds__(256, 2) k_mp_wave(S* __restrict__ G, S* __rest
     if (pub) phi_plane(pub_plane(kk));
     __syncthreads();  // also: every thread is done with collision z - 1 (ring slot of position z - 2)
     if (threadIdx.x == 0) {
-      if (pub && publisher) {
-        __threadfence();
-        mkw::st_release(w.flags + tile, (unsigned)(kk + 1));
-      }
+      // the release store after the CTA barrier orders every thread's phi
+      // stores of the plane before the count (cumulativity of release)
+      if (pub && publisher) mkw::st_release(w.flags + tile, (unsigned)(kk + 1));
       mkw::fence_proxy_async_global();
       mkw::fence_proxy_async_shared();
       if (q2 <= nz) stage(q2);
@@ -416,198 +431,6 @@ __global__ void __launch_bounds__(256, 2) k_mp_wave(S* __restrict__ G, S* __rest
   // the last staged position (nz + 1 is never staged; nz was waited above)
 }
 
-// Warp-specialised form of the fused loop: warp 0 of a CTA is the producer,
-// the others are consumers.  The producer computes and publishes phi planes
-// (`look` ahead), waits for a ring slot to be released and for the
-// neighbours' publication, and stages the halo planes; the consumer warps
-// only collide rows, waiting on the ring's "full" barriers and releasing
-// slots through the "empty" barriers (one arrival per consumer warp).  There
-// is no CTA-wide barrier inside the plane loop, so the consumers stream like
-// the two-kernel collision while the producer's phi loads run beside them.
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256, 2) k_mp_wave_ws(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
-                                                       P* __restrict__ phi, const Geom g,
-                                                       const MpK<typename Stor<S>::T> k, const Wave w) {
-  extern __shared__ __align__(128) unsigned char wave_smem[];
-  __shared__ __align__(8) uint64_t full[4];
-  __shared__ __align__(8) uint64_t empty[4];
-  __shared__ int nbr_tile[8];
-  P* const ring = reinterpret_cast<P*>(wave_smem);
-  const int tile = blockIdx.x;
-  const int seg = tile % w.sx, band = tile / w.sx;
-  const int x0 = seg * 32;
-  const int width = min(32, g.nx - x0);
-  const int y0 = (int)((int64_t)band * g.ny / w.sy), y1 = (int)((int64_t)(band + 1) * g.ny / w.sy);
-  const int rows = y1 - y0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nc = (blockDim.x >> 5) - 1;  // consumer warps
-  const int slot_elems = (w.rows_max + 2) * w.pitch;
-  const int nz = g.nz;
-
-  if (threadIdx.x < 8) {
-    const int d = threadIdx.x < 4 ? threadIdx.x : threadIdx.x + 1;
-    int ns = seg + d % 3 - 1, nb = band + d / 3 - 1;
-    bool ok = true;
-    if (ns < 0 || ns >= w.sx) {
-      if (g.bc0 == 0)
-        ns = (ns + w.sx) % w.sx;
-      else
-        ok = false;
-    }
-    if (nb < 0 || nb >= w.sy) {
-      if (g.bc1 == 0)
-        nb = (nb + w.sy) % w.sy;
-      else
-        ok = false;
-    }
-    nbr_tile[threadIdx.x] = ok ? nb * w.sx + ns : -1;
-  }
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      mkw::mbar_init(&full[s], 1);
-      mkw::mbar_init(&empty[s], nc);
-    }
-    mkw::fence_mbar_init();
-  }
-  __syncthreads();
-
-  const int P0 = w.look + w.pz;
-  auto parity_of = [](int q) { return (unsigned)(((q + 1) >> 2) & 1); };
-  auto slot_of = [](int q) { return (q + 1) & 3; };
-
-  if (warp == 0) {
-    // ------------------------------------------------------------ producer
-    const bool publisher = tile != w.skip_tile;
-    auto pub_plane = [&](int kk) { return w.pz ? (kk == 0 ? nz - 1 : kk - 1) : kk; };
-    auto pub_index = [&](int q) { return w.pz ? (q == nz - 1 ? 0 : q + 1) : q; };
-    // phi of column x0 + lane in every row of the tile, four rows in flight
-    auto phi_plane = [&](int p) {
-      const int x = x0 + lane;
-      if (lane >= width) return;
-      for (int r0 = 0; r0 < rows; r0 += 4) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int y = y0 + r0 + j;
-          if (r0 + j < rows && g.fluid(x, y, p)) {
-            if (fast_cell(g, x, y, p)) {
-              const Fast fa = make_fast(g, x, y, p);
-              mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, k.ref_h);
-            } else {
-              const Nbr nb(g, x, y, p);
-              mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), k.ref_h);
-            }
-          }
-        }
-      }
-    };
-    auto publish = [&](unsigned count) {
-      __syncwarp();
-      if (lane == 0 && publisher) {
-        __threadfence();
-        mkw::st_release(w.flags + tile, count);
-      }
-    };
-    auto wait_neighbours = [&](unsigned need) {
-      if (lane < 8) {
-        const int t = nbr_tile[lane];
-        if (t >= 0) mkw::wait_count(w.flags + t, need, w.err);
-      }
-      __syncwarp();
-    };
-    auto stage = [&](int q) {
-      const int slot = slot_of(q);
-      uint64_t* bar = &full[slot];
-      P* dst0 = ring + (size_t)slot * slot_elems;
-      const int plane = w.pz ? (q + nz) % nz : q;
-      const bool have = plane >= 0 && plane < nz;
-      const int xl = x0 - 4, xr = x0 + width + 4;
-      const int lo_mid = max(xl, 0), hi_mid = min(xr, g.nx);
-      const bool wrap_l = xl < 0 && g.bc0 == 0, wrap_r = xr > g.nx && g.bc0 == 0;
-      int nrows = 0;
-      if (have)
-        for (int lr = 0; lr < rows + 2; ++lr) {
-          const int y = y0 - 1 + lr;
-          if ((y < 0 || y >= g.ny) && g.bc1 != 0) continue;
-          ++nrows;
-        }
-      const unsigned bytes =
-          have ? (unsigned)(nrows * ((hi_mid - lo_mid) + (wrap_l ? 4 : 0) + (wrap_r ? 4 : 0)) * (int)sizeof(P)) : 0u;
-      mkw::mbar_arrive_expect(bar, bytes);
-      if (!have) return;
-      const int64_t pbase = (int64_t)plane * g.nx * g.ny;
-      for (int lr = 0; lr < rows + 2; ++lr) {
-        int y = y0 - 1 + lr;
-        if (y < 0 || y >= g.ny) {
-          if (g.bc1 != 0) continue;
-          y = (y + g.ny) % g.ny;
-        }
-        const P* src = phi + pbase + (int64_t)y * g.nx;
-        P* dst = dst0 + (size_t)lr * w.pitch;
-        mkw::bulk_g2s(dst + (lo_mid - xl), src + lo_mid, (unsigned)((hi_mid - lo_mid) * sizeof(P)), bar);
-        if (wrap_l) mkw::bulk_g2s(dst, src + (g.nx - 4), (unsigned)(4 * sizeof(P)), bar);
-        if (wrap_r) mkw::bulk_g2s(dst + 4 + width, src, (unsigned)(4 * sizeof(P)), bar);
-      }
-    };
-
-    for (int kk = 0; kk < P0 && kk < nz; ++kk) phi_plane(pub_plane(kk));
-    publish((unsigned)min(P0, nz));
-    wait_neighbours((unsigned)min(P0, nz));
-    if (lane == 0) {
-      mkw::fence_proxy_async_global();
-      stage(-1);
-      stage(0);
-      stage(1);
-    }
-    for (int z = 0; z < nz; ++z) {
-      const int kk = P0 + z;
-      if (kk < nz) {
-        phi_plane(pub_plane(kk));
-        publish((unsigned)(kk + 1));
-      }
-      const int q2 = z + 2;
-      if (q2 <= nz) {
-        // the slot's previous position (z - 2) is released after collision z - 1
-        if (z >= 1) mkw::mbar_wait(&empty[slot_of(q2)], parity_of(z - 2), w.err);
-        const int plane2 = w.pz ? q2 % nz : q2;
-        if (plane2 < nz) wait_neighbours((unsigned)(pub_index(plane2) + 1));
-        if (lane == 0) {
-          mkw::fence_proxy_async_global();
-          mkw::fence_proxy_async_shared();
-          stage(q2);
-        }
-      }
-    }
-  } else {
-    // ------------------------------------------------------------ consumers
-    const int cw = warp - 1;
-    mkw::mbar_wait(&full[slot_of(-1)], parity_of(-1), w.err);
-    mkw::mbar_wait(&full[slot_of(0)], parity_of(0), w.err);
-    for (int z = 0; z < nz; ++z) {
-      mkw::mbar_wait(&full[slot_of(z + 1)], parity_of(z + 1), w.err);
-      const P* lo = ring + (size_t)slot_of(z - 1) * slot_elems;
-      const P* mid = ring + (size_t)slot_of(z) * slot_elems;
-      const P* hi = ring + (size_t)slot_of(z + 1) * slot_elems;
-      for (int r = cw; r < rows; r += nc) {
-        const int x = x0 + lane, y = y0 + r;
-        if (lane < width && g.fluid(x, y, z)) {
-          const PhiRing<P> src{lo, mid, hi, (r + 1) * w.pitch + lane + 4, w.pitch};
-          if (fast_cell(g, x, y, z)) {
-            const Fast fa = make_fast(g, x, y, z);
-            mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, fa, fa.c, k);
-          } else {
-            const Nbr nb(g, x, y, z);
-            mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, nb, nb.idx(0, 0, 0), k);
-          }
-        }
-      }
-      // position z - 1 is not read again: release its slot
-      __syncwarp();
-      if (lane == 0 && z - 1 <= nz - 2) mkw::mbar_arrive(&empty[slot_of(z - 1)]);
-    }
-  }
-}
-
 // The fused loop's tiling for this case (see k_mp_wave): 32-cell x segments
 // times y bands, with as many bands as the co-resident capacity of the
 // kernel allows, so every tile is one CTA and all CTAs are resident together.
@@ -624,8 +447,7 @@ void wave_config(mke::Engine& e) {
   const int pitch = 40;
   // occupancy of the larger launch (256 threads, 16 rows), both parities
   size_t smem_max = (size_t)4 * (16 + 2) * pitch * sizeof(P);
-  const void* kerns[4] = {(const void*)k_mp_wave<S, P, 0>, (const void*)k_mp_wave<S, P, 1>,
-                          (const void*)k_mp_wave_ws<S, P, 0>, (const void*)k_mp_wave_ws<S, P, 1>};
+  const void* kerns[2] = {(const void*)k_mp_wave<S, P, 0>, (const void*)k_mp_wave<S, P, 1>};
   int per_sm = 1 << 20;
   for (const void* kern : kerns) {
     int b = 0;
@@ -643,8 +465,7 @@ void wave_config(mke::Engine& e) {
   e.wave_sx = sx;
   e.wave_sy = sy;
   e.wave_rows = rows;
-  e.wave_threads = 32 * std::min(rows, 8);         // one warp per row
-  e.wave_threads_ws = 32 * (1 + std::min(rows, 7));  // producer warp + one consumer warp per row
+  e.wave_threads = 32 * std::min(rows, 8);  // one warp per row
   e.wave_smem = (size_t)4 * (rows + 2) * pitch * sizeof(P);
   for (const void* kern : kerns)
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.wave_smem) != cudaSuccess) {
@@ -679,9 +500,8 @@ void launch_mp_wave(mke::Engine& e, int parity, cudaEvent_t* ev) {
   float* H0 = e.rest1;
   P* phi = (P*)e.phi[0];
   cudaLaunchConfig_t cfg = {};
-  const bool ws = e.wave == 2;
   cfg.gridDim = dim3(tiles);
-  cfg.blockDim = dim3(ws ? e.wave_threads_ws : e.wave_threads);
+  cfg.blockDim = dim3(e.wave_threads);
   cfg.dynamicSmemBytes = e.wave_smem;
   cfg.stream = e.stream;
   cudaLaunchAttribute attr[1];
@@ -689,17 +509,10 @@ void launch_mp_wave(mke::Engine& e, int parity, cudaEvent_t* ev) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (ws) {
-    if (parity == 0)
-      cudaLaunchKernelEx(&cfg, k_mp_wave_ws<S, P, 0>, G, H, H0, phi, g, k, w);
-    else
-      cudaLaunchKernelEx(&cfg, k_mp_wave_ws<S, P, 1>, G, H, H0, phi, g, k, w);
-  } else {
-    if (parity == 0)
-      cudaLaunchKernelEx(&cfg, k_mp_wave<S, P, 0>, G, H, H0, phi, g, k, w);
-    else
-      cudaLaunchKernelEx(&cfg, k_mp_wave<S, P, 1>, G, H, H0, phi, g, k, w);
-  }
+  if (parity == 0)
+    cudaLaunchKernelEx(&cfg, k_mp_wave<S, P, 0>, G, H, H0, phi, g, k, w);
+  else
+    cudaLaunchKernelEx(&cfg, k_mp_wave<S, P, 1>, G, H, H0, phi, g, k, w);
   if (ev) cudaEventRecord(ev[1], e.stream);
 }
 

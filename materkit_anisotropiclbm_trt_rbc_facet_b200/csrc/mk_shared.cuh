@@ -93,21 +93,6 @@ __device__ __forceinline__ void mp_phi_cell(const S* __restrict__ H, const float
   phi[c] = P(ref_h + s);
 }
 
-template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const float* __restrict__ H0,
-                                                P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
-  if (fast_cell(g, x, y, z)) {
-    const Fast fa = make_fast(g, x, y, z);
-    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, ref_h);
-  } else {
-    const Nbr nb(g, x, y, z);
-    mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), ref_h);
-  }
-}
 
 // Where a collision reads phi: its own cell (center) and the neighbour
 // (dx, dy, dz) (at).  PhiGlobal reads the phi array, which no kernel writes

@@ -366,16 +366,6 @@ class Solver:
     def fused(self, on: bool) -> None:
         _check(self._lib.mk_set_fused(self._h, 1 if on else 0), self._h)
 
-    @property
-    def loop_form(self) -> int:
-        """Multiphase loop form (mk_set_fused): 0 two kernels, 1 fused with a
-        producer warp per CTA, 2 fused without warp specialisation."""
-        return int(self._lib.mk_get_fused(self._h))
-
-    @loop_form.setter
-    def loop_form(self, form: int) -> None:
-        _check(self._lib.mk_set_fused(self._h, int(form)), self._h)
-
     def bytes_per_cell(self) -> float:
         return float(self._lib.mk_bytes_per_cell(self._h))
 
@@ -473,6 +463,13 @@ class mkFluidsMRT(_RefSolver):
                                    "bdy_flowin"],
         # run_multiPhaseField (MaterKit.cpp:563-567)
         A.MK_MODEL_MULTIGRAIN: ["propagate", "relaxation", "thermal_propagate", "thermal_relaxation"],
+        # run_solutal_dendrite (MaterKit.cpp:665-674)
+        A.MK_MODEL_SOLUTAL_DENDRITE: ["phasefield_propagate", "relaxation_anisotropy_solute", "solutal_propagate",
+                                      "solutal_relaxation"],
+        # run_flow_solutal_dendrite (MaterKit.cpp:430-456)
+        A.MK_MODEL_FLOW_SOLUTAL: ["propagate_PBB", "relaxation", "bdyVelocity", "phasefield_propagate",
+                                  "relaxation_anisotropy_solute", "solutal_propagate", "solutal_relaxation",
+                                  "bdy_LBflowin"],
     }
 
     def initialize_geometry_Poiseuille(self) -> None:
@@ -505,6 +502,19 @@ class mkFluidsMRT(_RefSolver):
 
     def thermal_relaxation(self) -> None:
         self._call("thermal_relaxation")
+
+    # mkPhaseField / mkSolutalField members of the solutal drivers
+    def relaxation_anisotropy_solute(self, loops: int | None = None) -> None:
+        self._call("relaxation_anisotropy_solute")
+
+    def solutal_propagate(self) -> None:
+        self._call("solutal_propagate")
+
+    def solutal_relaxation(self) -> None:
+        self._call("solutal_relaxation")
+
+    def bdy_LBflowin(self) -> None:
+        self._call("bdy_LBflowin")
 
 
 class mkFluidsMultiphase(_RefSolver):

@@ -41,7 +41,9 @@ import numpy as np
 # ------------------------------------------------------------------ constants
 # Values of include/mkb200.h (the enums of the C ABI the oracle library shares).
 MODEL = {"flow": 0, "multiphase": 1, "thermal_dendrite": 2, "solutal_dendrite": 3, "convection": 4,
-         "flow_dendrite": 5, "multigrain": 6}
+         "flow_dendrite": 5, "multigrain": 6, "flow_solutal_dendrite": 7}
+FLOW_COUPLED = (MODEL["flow_dendrite"], MODEL["flow_solutal_dendrite"])
+DENDRITES = (MODEL["thermal_dendrite"], MODEL["solutal_dendrite"]) + FLOW_COUPLED
 PRECISION = {"fp64": 0, "fp32": 1, "fp16": 2, "bf16": 3}
 COLLISION = {"bgk": 0, "trt": 1, "mrt": 2}
 BC_PERIODIC, BC_WALLS, BC_CLOSED = 0, 1, 2
@@ -373,7 +375,7 @@ def validate(p: MkParams) -> None:
             bad("bad boundary kind")
         if p.bc[a] == BC_WALLS and n3[a] < 3:
             bad("a walled axis needs at least 3 cells")
-    if not 0 <= p.model <= MODEL["multigrain"]:
+    if not 0 <= p.model <= MODEL["flow_solutal_dendrite"]:
         bad("unknown model")
     if not 0 <= p.precision <= 3:
         bad("unknown precision")
@@ -387,11 +389,11 @@ def validate(p: MkParams) -> None:
     if p.model == MODEL["convection"] and (not p.D > 0 or p.wall_axis < 0):
         bad("convection needs a positive diffusivity and a plate axis")
     if p.inlet:
-        if p.model not in (MODEL["flow"], MODEL["flow_dendrite"]):
+        if p.model not in (MODEL["flow"],) + FLOW_COUPLED:
             bad("inflow / outflow faces apply to the flow and flow + dendrite models")
         if p.bc[0] != BC_CLOSED or p.nx < 3 or p.wall_axis == 0:
             bad("inflow / outflow faces need closed x faces, nx >= 3 and no x plates")
-    if p.model in (MODEL["flow"], MODEL["convection"], MODEL["flow_dendrite"]):
+    if p.model in (MODEL["flow"], MODEL["convection"]) + FLOW_COUPLED:
         if p.lattice not in (19, 27) or not 0 <= p.collision <= 2:
             bad("flow lattice / collision")
         if p.collision == COLLISION["mrt"] and p.lattice != 19:
@@ -404,7 +406,7 @@ def validate(p: MkParams) -> None:
     if p.model == MODEL["multigrain"]:
         if not 1 <= p.n_objects <= MAX_OBJECTS or not (p.W0 > 0 and p.mobility > 0 and p.D > 0):
             bad("multigrain parameters out of range")
-    if p.model in (MODEL["thermal_dendrite"], MODEL["solutal_dendrite"], MODEL["flow_dendrite"]):
+    if p.model in DENDRITES:
         if not (p.W0 > 0 and p.tau0 > 0 and p.D > 0):
             bad("phase-field parameters out of range")
         if not 0 <= p.n_objects <= MAX_OBJECTS or not 0 <= p.aniso <= 3:
@@ -418,7 +420,8 @@ _MODEL_WORDS = {
     "allen_cahn": "multiphase", "thermal_dendrite": "thermal_dendrite", "thermal": "thermal_dendrite",
     "solutal_dendrite": "solutal_dendrite", "solutal": "solutal_dendrite", "convection": "convection",
     "rbc": "convection", "rayleigh_benard": "convection", "flow_dendrite": "flow_dendrite",
-    "flow_thermal_dendrite": "flow_dendrite", "multigrain": "multigrain", "multiphasefield": "multigrain",
+    "flow_thermal_dendrite": "flow_dendrite", "flow_solutal_dendrite": "flow_solutal_dendrite",
+    "flow_solutal": "flow_solutal_dendrite", "multigrain": "multigrain", "multiphasefield": "multigrain",
     "multi_phase_field": "multigrain"}
 _BC_WORDS = {"periodic": BC_PERIODIC, "p": BC_PERIODIC, "walls": BC_WALLS, "wall": BC_WALLS, "w": BC_WALLS,
              "bounceback": BC_WALLS, "closed": BC_CLOSED, "noflux": BC_CLOSED, "zeroflux": BC_CLOSED,
@@ -554,7 +557,7 @@ def resolve(path: str, model=None, precision=None, collision=None, lattice=None,
             if iv is not None:
                 p.delta = -iv
         p.bc[:] = [BC_CLOSED] * 3
-        if name == "flow_dendrite":
+        if name in ("flow_dendrite", "flow_solutal_dendrite"):
             # inflow at x = 0 with flow/velocityInlet, outflow at x = nx - 1
             # (boundary_vel, mkFluidsUser.cpp:455-617), periodic across
             flow_tau()
@@ -725,7 +728,7 @@ def initial_field(p: MkParams, name: str) -> np.ndarray:
     """Initial macroscopic field (nz, ny, nx) float64 of the case."""
     xyz = _coords(p)
     shape = xyz[0].shape
-    dendrite = p.model in (MODEL["thermal_dendrite"], MODEL["solutal_dendrite"], MODEL["flow_dendrite"])
+    dendrite = p.model in DENDRITES
     if name == "flag":
         return flags(p)
     if name == "phi":
@@ -746,7 +749,7 @@ def initial_field(p: MkParams, name: str) -> np.ndarray:
         return np.full(shape, p.rho0)
     if name in ("ux", "uy", "uz"):
         a = "xyz".index(name[1])
-        if p.model == MODEL["flow_dendrite"]:
+        if p.model in FLOW_COUPLED:
             ns = np.clip(0.5 * (1.0 + seed_phi(p, xyz)), 0.0, 1.0)
             return (1.0 - ns) * p.u0[a]
         if p.model in (MODEL["flow"], MODEL["convection"]):

@@ -131,6 +131,11 @@ void rotation_zyx(const double ang_deg[3], double R[3][3]) {
 
 }  // namespace
 
+// Model families: the flow + dendrite models carry a flow lattice with porous
+// bounce-back and inflow / outflow faces; the solutal models a U-lattice.
+static bool flow_coupled(int model) { return model == MK_MODEL_FLOW_DENDRITE || model == MK_MODEL_FLOW_SOLUTAL; }
+static bool solutal(int model) { return model == MK_MODEL_SOLUTAL_DENDRITE || model == MK_MODEL_FLOW_SOLUTAL; }
+
 // ------------------------------------------------------------------ state
 struct orc_state {
   mk_params p;
@@ -622,10 +627,13 @@ void thermal_dendrite_step(orc_state* s) {
         }
       }
   propagate(s, 7, s->s_out, s->s_hlp);
-  if (p.model == MK_MODEL_SOLUTAL_DENDRITE) {
+  if (solutal(p.model)) {
     // 3'. solutal propagate + relaxation: variable diffusivity, anti-trapping
-    // current in the equilibrium's first moment, rejection and lagged capacity.
+    // current in the equilibrium's first moment, rejection and lagged capacity;
+    // with a flow lattice the first moment also carries the advective flux U u
+    // (the equilibrium w U (1 + 4 e.u) of the liquid).
     const double k = p.k_part;
+    const bool adv = !s->vel.empty();
 #pragma omp parallel for schedule(static)
     for (int z = 0; z < s->nz; ++z)
       for (int y = 0; y < s->ny; ++y)
@@ -660,7 +668,8 @@ void thermal_dendrite_step(orc_state* s) {
           for (int i = 1; i < 7; i += 2) {
             const int j = i + 1;
             const double w = weight(7, i);
-            const double ej = E27[i][0] * jat[0] + E27[i][1] * jat[1] + E27[i][2] * jat[2];
+            double ej = E27[i][0] * jat[0] + E27[i][1] * jat[1] + E27[i][2] * jat[2];
+            if (adv) ej += U * (E27[i][0] * s->vel[3 * c] + E27[i][1] * s->vel[3 * c + 1] + E27[i][2] * s->vel[3 * c + 2]);
             const double sym = w * U;             // (t_i + t_j)/2 after relaxation with rate 1
             const double am = 0.5 * (t[i] - t[j]);  // antisymmetric part
             const double am_new = am - om * (am - w * 4.0 * ej);
@@ -920,7 +929,7 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
       for (int b = 0; b < 3; ++b) s->rot[9 * k + 3 * a + b] = R[a][b];
   }
   if (p->model == MK_MODEL_THERMAL_DENDRITE || p->model == MK_MODEL_SOLUTAL_DENDRITE ||
-      p->model == MK_MODEL_FLOW_DENDRITE) {
+      flow_coupled(p->model)) {
     for (int z = 0; z < s->nz; ++z)
       for (int y = 0; y < s->ny; ++y)
         for (int x = 0; x < s->nx; ++x) s->grain[cidx(s, x, y, z)] = nearest_seed(*p, x, y, z);
@@ -967,7 +976,7 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
     s->Qs = 7;
     s->temp.assign(n, -p->delta);
     if (p->model == MK_MODEL_THERMAL_DENDRITE && T0) std::memcpy(s->temp.data(), T0, n * sizeof(double));
-    if (p->model == MK_MODEL_SOLUTAL_DENDRITE && C0) std::memcpy(s->temp.data(), C0, n * sizeof(double));
+    if (solutal(p->model) && C0) std::memcpy(s->temp.data(), C0, n * sizeof(double));
     s->f_out.assign((size_t)7 * n, 0.0);
     s->f_hlp.assign((size_t)7 * n, 0.0);
     s->s_out.assign((size_t)7 * n, 0.0);
@@ -1004,7 +1013,7 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
           }
       s->phi_prev = s->phi;
     }
-    if (p->model == MK_MODEL_FLOW_DENDRITE) {
+    if (flow_coupled(p->model)) {
       // the flow starts at rho0 with u0 scaled by the liquid fraction, unless
       // density / velocity fields are given
       s->Qw = p->lattice;
@@ -1052,6 +1061,7 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
         convection_step(s);
         break;
       case MK_MODEL_FLOW_DENDRITE:
+      case MK_MODEL_FLOW_SOLUTAL:
         flow_dendrite_step(s);
         break;
       case MK_MODEL_MULTIGRAIN:
@@ -1084,7 +1094,7 @@ extern "C" int orc_get_populations(const orc_state* s, int which, double* out) {
 extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
   const int64_t n = s->n;
   const mk_params& p = s->p;
-  if (field == MK_FIELD_FLAG && p.model != MK_MODEL_FLOW_DENDRITE) {
+  if (field == MK_FIELD_FLAG && !flow_coupled(p.model)) {
     for (int64_t c = 0; c < n; ++c) out[c] = s->flag[c];
     return 0;
   }
@@ -1106,7 +1116,7 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
     std::memcpy(out, s->phi.data(), n * sizeof(double));
     return 0;
   }
-  if (p.model == MK_MODEL_FLOW_DENDRITE) {
+  if (flow_coupled(p.model)) {
     if (field == MK_FIELD_FLAG) {
       // reset_flags (mkPhaseField.h:37): solid where phi > 0
       for (int64_t c = 0; c < n; ++c) out[c] = s->flag[c] != MK_FLAG_FLUID ? s->flag[c]
@@ -1205,7 +1215,7 @@ extern "C" int orc_get_field(const orc_state* s, int field, double* out) {
   }
   // dendrites
   if (field == MK_FIELD_T || field == MK_FIELD_C) {
-    if ((field == MK_FIELD_T) != (p.model != MK_MODEL_SOLUTAL_DENDRITE)) return 1;
+    if ((field == MK_FIELD_T) != !solutal(p.model)) return 1;
     std::memcpy(out, s->temp.data(), n * sizeof(double));
     return 0;
   }

@@ -84,6 +84,17 @@
 //   t0* = w0 U + w0 S,  t_i,j* = w U +- [a - omega (a - w 4 e_i.j_at/c)] + w S,
 //   a = (t_i - t_j)/2,  S = (1/2)(1 + (1-k)U) dphi / c(phi),
 //   U = sum t (post-stream), phi, dphi of this loop, n = grad phi/(|grad phi| + 1e-6).
+//
+// FLOW + DENDRITE (run_flow_thermal_dendrite, MaterKit.cpp:467-527) and FLOW +
+// SOLUTAL DENDRITE (run_flow_solutal_dendrite, MaterKit.cpp:399-465): per loop
+// the flow lattice with the partially saturated porous bounce-back
+// (propagate_PBB, relaxation) and the x faces (bdyVelocity), the phase field,
+// the scalar lattice advected by the flow's collision velocity u (thermal:
+// t_eq = w T (1 + 4 e.u); solutal: the advective flux U u joins the
+// anti-trapping current in the first moment, 4 w e.(j_at/c + U u)), then the
+// scalar faces (bdy_flowin / bdy_LBflowin): inflow T_b (U_b) = -Delta,
+// phi_b = -1, outflow copies the inner neighbour, by non-equilibrium
+// extrapolation of w T (1 + 4 e.u).
 // ---------------------------------------------------------------------------
 #ifndef MK_ORACLE_HPP
 #define MK_ORACLE_HPP

@@ -41,6 +41,7 @@ SMALL = {
     "convection": cases.convection(nx=20, ny=5, nz=12, Ra=2e4),
     "couette": cases.couette(nx=6, ny=12, nz=5, U=2e-2),
     "flow_dendrite": cases.flow_dendrite(nx=24, ny=14, nz=12, radius=4.0, u_in=0.03, center=(8.0, 6.5, 5.5)),
+    "flow_solutal": cases.flow_solutal_dendrite(nx=24, ny=14, nz=12, radius=4.0, u_in=0.03, center=(8.0, 6.5, 5.5)),
     "multigrain": cases.multigrain(n=20, ny=19, nz=18, seeds=[(7.0, 9.5, 9.0, 5.0), (13.0, 9.5, 9.0, 5.0),
                                                               (10.0, 14.0, 11.0, 3.0)]),
 }

@@ -4,9 +4,9 @@ memory by the bulk-copy engine) against the two-kernel loop (phi kernel, then
 collision kernel) and the oracle, and its bounded waits.
 
 Both forms run the same per-cell arithmetic on the same populations, so they
-must agree bit for bit in every storage precision; the FP64 form must match
-the oracle to 1e-10 (its default use is covered by every multiphase parity
-test, which now runs fused where the case admits it)."""
+must agree bit for bit in every storage precision; the FP64 fused form must
+match the oracle to 1e-10.  The two-kernel loop is the default (the autotuner
+keeps the faster form)."""
 import numpy as np
 import pytest
 
@@ -34,15 +34,14 @@ def _case(casedir, name, prec):
     return cases.write(text, f"{casedir}/fused_{name}_{prec}.xml")
 
 
-@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16", "bf16"])
 @pytest.mark.parametrize("name", sorted(SHAPES))
-def test_fused_equals_two_kernel(casedir, name, prec, form):
+def test_fused_equals_two_kernel(casedir, name, prec):
     p = case_params(_case(casedir, name, prec))
     a, b = Solver(params=p), Solver(params=p)
+    assert not a.fused, "the two-kernel loop is the default"
+    a.fused = True
     assert a.fused, "the case should admit the fused loop"
-    a.loop_form = form
-    b.fused = False
     for n in (1, 1, 5):
         a.advance(n)
         b.advance(n)
@@ -55,12 +54,11 @@ def test_fused_equals_two_kernel(casedir, name, prec, form):
     assert np.array_equal(a.field("phi"), b.field("phi"))
 
 
-@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("name", sorted(SHAPES))
-def test_fused_fp64_matches_oracle(casedir, name, form):
+def test_fused_fp64_matches_oracle(casedir, name):
     path = _case(casedir, name, "fp64")
     s = Solver(params=case_params(path))
-    s.loop_form = form
+    s.fused = True
     o = Oracle.from_xml(path)
     fl = ocase.flags(o.params) == 0
     for n in (1, 1, 1, 30):
@@ -83,19 +81,18 @@ def test_cases_without_fused_form(casedir):
         assert s.launches_per_step() == 2
 
 
-@pytest.mark.parametrize("form", [1, 2])
-def test_bounded_wait_times_out_and_recovers(casedir, tmp_path, form):
+def test_bounded_wait_times_out_and_recovers(casedir, tmp_path):
     # one tile never publishes its phi planes: its neighbours' waits run out
     # after their iteration limit, the launch ends, and the host reads
     # MK_ERR_TIMEOUT; the handle then runs normally again
     p = case_params(_case(casedir, "walls_z", "fp32"))
     s = Solver(params=p)
     ref = Solver(params=p)
-    s.loop_form = form
-    ref.loop_form = form
+    s.fused = True
+    ref.fused = True
     s.advance(2)
     ref.advance(2)
-    ck = str(tmp_path / f"before_{form}.bin")
+    ck = str(tmp_path / "before.bin")
     s.checkpoint(ck)
     assert s._lib.mk_inject_fault(s.handle, 1) == A.MK_OK
     s.advance(1)

@@ -428,6 +428,57 @@ def test_flow_dendrite_solid_stops_the_flow(casedir):
     assert np.array_equal(flag == A.MK_FLAG_SOLID, phi > 0)
 
 
+# ------------------------------------------------- flow + solutal dendrite (f-2)
+def test_flow_solutal_uniform_inflow_is_steady(casedir):
+    # All liquid at the far-field supersaturation: the faces keep the uniform
+    # stream and the uniform solute to round-off.
+    p = _params(casedir, "fs_uniform", cases.flow_solutal_dendrite(nx=12, ny=6, nz=5, radius=3.0, u_in=0.03))
+    sh = (p.nz, p.ny, p.nx)
+    o = Oracle(p, phi=-np.ones(sh), Cc=np.full(sh, -p.delta))
+    o.advance(40)
+    assert np.abs(o.field("ux") - 0.03).max() < 1e-14
+    assert np.abs(o.field("C") + p.delta).max() < 1e-14
+    assert np.abs(o.field("phi") + 1.0).max() == 0.0
+
+
+def test_flow_solutal_at_rest_is_the_solutal_dendrite(casedir):
+    # Closed faces and no inflow: the flow stays at rest and the phase field
+    # and the solute are those of the solutal dendrite model.
+    p = _params(casedir, "fs_rest", cases.flow_solutal_dendrite(nx=20, ny=18, nz=16, radius=4.0, u_in=0.0,
+                                                                inlet=False))
+    q = A.MkParams.from_buffer_copy(p)
+    q.model = A.MK_MODEL_SOLUTAL_DENDRITE
+    phi, U = initial_field(p, "phi"), initial_field(p, "C")
+    o1, o2 = Oracle(p, phi=phi, Cc=U), Oracle(q, phi=phi, Cc=U)
+    o1.advance(60)
+    o2.advance(60)
+    assert (o1.field("phi") > 0).sum() > 200  # the seed grew
+    assert np.abs(o1.field("phi") - o2.field("phi")).max() < 1e-12
+    assert np.abs(o1.field("C") - o2.field("C")).max() < 1e-12
+    assert np.abs(o1.field("ux")).max() < 1e-15
+
+
+def test_flow_solutal_advects_solute_at_the_flow_speed(casedir):
+    # A solute pulse in the uniform stream of liquid (capacity 1, no
+    # anti-trapping current): its centroid moves at u0 (first moment U u of
+    # the advected equilibrium) and the solute is conserved.
+    p = _params(casedir, "fs_adv", cases.flow_solutal_dendrite(nx=64, ny=4, nz=4, radius=3.0, u_in=0.05, D=0.02))
+    sh = (p.nz, p.ny, p.nx)
+    x = np.arange(p.nx)
+    U = np.broadcast_to(-p.delta + 0.1 * np.exp(-((x - 16.0) / 3.0) ** 2), sh).copy()
+    o = Oracle(p, phi=-np.ones(sh), Cc=U)
+
+    def moments():
+        e = o.field("C")[0, 0] + p.delta
+        return (e * x).sum() / e.sum(), e.sum()
+
+    c0, m0 = moments()
+    o.advance(300)
+    c1, m1 = moments()
+    assert abs((c1 - c0) - 0.05 * 300) < 1e-6
+    assert abs(m1 - m0) / m0 < 1e-10
+
+
 # ---------------------------------------------------------- multigrain (f-3)
 def test_multigrain_single_grain_conserves_phi_and_heat(casedir):
     # one grain: conservative Allen-Cahn (no penalty on grain 0), closed faces:
