@@ -51,3 +51,10 @@ def test_no_cpu_fallback_without_device(tmp_path):
     with pytest.raises(A.MkError) as e:
         Solver(xml)
     assert e.value.status == A.MK_ERR_NODEVICE
+
+
+def test_metrics_log_path_checked():
+    # host-only: an unwritable metrics log path is an MK_ERR_IO status
+    lib = A.load()
+    assert lib.mk_set_metrics_log(b"/nonexistent_dir/x/metrics.jsonl") == A.MK_ERR_IO
+    assert lib.mk_set_metrics_log(None) == A.MK_OK
