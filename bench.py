@@ -464,7 +464,7 @@ def run_ensemble(args):
                          "collide_gbs": cb / t_launch / 1e9, "collide_frac": cb / t_launch / 1e9 / peak,
                          "collide_bytes_per_launch": cb, "step_bytes_per_cell": step_bytes / cells,
                          "step_gbs": step_bytes * K / (ms * 1e-3) / 1e9, "clocks": clk.summary(),
-                         "launches": launches, "n_bad": bad}
+                         "launches": launches, "n_bad": bad, "kernel": wl["kernel"]}
         results[prec]["step_frac"] = results[prec]["step_gbs"] / peak
         e.close()
     r = results[args.precision]

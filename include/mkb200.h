@@ -462,8 +462,110 @@ const char* mk_noalloc_last_error(void);
  * solid_frac, max_speed, n_bad}.  NULL stops the log.  Process-wide. */
 mk_status mk_set_metrics_log(const char* path);
 
+/* ---- z-slab decomposition of one multiphase domain ----------------------
+ * No counterpart in the reference: its solver runs one domain in one process,
+ * its cell sweeps shared out by OpenMP (mkFluidsUser.cpp:70, 116, 147).  Here
+ * one domain of the multiphase model is split into contiguous runs of z
+ * planes, one per rank (one process per GPU, or several handles in one
+ * process), and the ranks exchange plane-sized runs between the two kernels
+ * of every loop.
+ *
+ * A slab handle holds its nz_own planes as the local planes 1 .. nz_own, plus
+ * two ghost planes (local 0 below, nz_own + 1 above) that receive copies of
+ * the neighbour slabs' boundary planes; its arrays have the layout of a
+ * domain of nz_own + 2 planes (mk_get_params reports that nz), and
+ * mk_get_field returns all nz_own + 2 planes.  Ghost cells are never updated.
+ *
+ * The in-place streaming (AA pattern) decides what crosses a slab face:
+ *   MK_SLAB_FILL   before an odd loop: the 5 populations with e_z = -1 of the
+ *                  top owned plane go up into the ghost 0 of the slab above,
+ *                  the 5 with e_z = +1 of plane 1 go down into the top ghost
+ *                  of the slab below (both lattices: 20 plane runs a slab);
+ *   MK_SLAB_PHI    every loop, after the phi kernel: the top owned phi plane
+ *                  up into ghost 0 above, plane 1 down into the top ghost
+ *                  below (the gradient and Laplacian stencil of phi);
+ *   MK_SLAB_RETURN after an odd loop, and once after mk_create_slab: the odd
+ *                  loop (and the initial state) wrote the same 5 + 5 slots of
+ *                  the ghost planes; they go back to the planes they belong
+ *                  to (ghost 0 down to the top owned plane below, the top
+ *                  ghost up to plane 1 above).  They land in the receiving
+ *                  slab's halo buffer, and mk_slab_done merges them into the
+ *                  owned plane on the handle's stream, except the slots whose
+ *                  source cell across the face is not fluid (next to an x or
+ *                  y wall or closed face, or a global wall plane): those the
+ *                  cell wrote itself by bounce-back.
+ * A loop is therefore [FILL if odd] RUN_PHI PHI RUN_COLLIDE [RETURN if odd];
+ * mk_slab_next reports the next action and the run / done calls refuse any
+ * other (MK_ERR_STATE).  Non-periodic global ends have no neighbour and
+ * exchange nothing; a periodic z axis wraps (with one rank, onto itself).
+ * Fused loops, graphs, the autotuner, checkpoints and the adjoint are not
+ * available on slab handles (MK_ERR_STATE). */
+enum {
+  MK_SLAB_FILL = 0,
+  MK_SLAB_PHI = 1,
+  MK_SLAB_RETURN = 2,
+  MK_SLAB_RUN_PHI = 3,
+  MK_SLAB_RUN_COLLIDE = 4
+};
+
+/* One plane-sized run of a slab exchange: `count` elements at element
+ * `offset` of an array of the slab (array 0: the pressure lattice g, whose
+ * element offset is population * stride + plane * nx * ny; 1: the Allen-Cahn
+ * lattice h, same; 2: phi, plane * nx * ny; 3: the halo buffer of a return
+ * exchange, ((face * 2 + lattice) * 5 + k) * nx * ny for the k-th population
+ * crossing the lower (face 0) or upper (face 1) face), sent to or received
+ * from `peer`.
+ * The two ends of one transfer carry the same `tag`; a rank's list is sorted
+ * by (peer, tag), so two ranks that post their sends and receives in list
+ * order match them pairwise. */
+typedef struct mk_slab_xfer {
+  int32_t peer;  /* the other rank (may be this rank, periodic z with one rank) */
+  int32_t send;  /* 1: this rank sends the run, 0: it receives into the run    */
+  int32_t tag;   /* 128 * (0 upward, 1 downward) + 32 * array + population    */
+  int32_t array; /* 0 g, 1 h, 2 phi, 3 return halo                             */
+  int64_t offset;
+  int64_t count;
+  int64_t bytes;
+  void* ptr;     /* device address of the run (mk_slab_transfers); NULL from mk_slab_plan */
+} mk_slab_xfer;
+
+/* The planes rank `rank` of `nranks` owns of a domain of nz planes: the first
+ * nz % nranks ranks own nz / nranks + 1, the others nz / nranks. */
+mk_status mk_slab_split(int32_t nz, int32_t rank, int32_t nranks, int32_t* z0, int32_t* nz_own);
+/* Host-only: the transfers of one exchange stage of rank `rank` for the global
+ * case `global` (ptr NULL).  At most MK_SLAB_MAX_XFER entries (a slab with a
+ * neighbour on both faces: 40 population runs, or 4 phi runs); `capacity`
+ * below what the stage needs is MK_ERR_ARG with *count set to the need. */
+#define MK_SLAB_MAX_XFER 40
+mk_status mk_slab_plan(const mk_params* global, int32_t rank, int32_t nranks, int32_t stage, mk_slab_xfer* out,
+                       int32_t capacity, int32_t* count);
+/* Create the slab of rank `rank` of the multiphase case `global` on the current
+ * device, from the global initial state (the same as mk_create's).  The first
+ * action is MK_SLAB_RETURN. */
+mk_status mk_create_slab(const mk_params* global, int32_t rank, int32_t nranks, mk_handle** out);
+/* Slab geometry of a handle (MK_ERR_STATE for a whole-domain handle). */
+mk_status mk_slab_info(const mk_handle* h, int32_t* rank, int32_t* nranks, int32_t* z0, int32_t* nz_own,
+                       int32_t* nz_global);
+/* Next action of the loop protocol (MK_SLAB_*), -1 for a whole-domain handle. */
+int32_t mk_slab_next(const mk_handle* h);
+/* mk_slab_plan of the handle's slab with device addresses filled in. */
+mk_status mk_slab_transfers(const mk_handle* h, int32_t stage, mk_slab_xfer* out, int32_t capacity, int32_t* count);
+/* The caller completed the exchange `stage` (every receive has landed and is
+ * ordered before the handle's next launch: done on the handle's stream, or
+ * synchronised).  For MK_SLAB_RETURN this launches the merge of the halo
+ * buffer into the owned planes. */
+mk_status mk_slab_done(mk_handle* h, int32_t stage);
+/* Launch the next kernel: MK_SLAB_RUN_PHI or MK_SLAB_RUN_COLLIDE (the latter
+ * completes the loop and advances mk_get_step). */
+mk_status mk_slab_run(mk_handle* h, int32_t action);
+/* In-process exchange among the n slabs of one decomposition (hs[r] is rank
+ * r, all of the same case and stage): stream-ordered device copies (peer
+ * copies across devices), then mk_slab_done on every handle. */
+mk_status mk_slab_exchange_local(mk_handle* const* hs, int32_t n, int32_t stage);
+
 /* Algorithmic bytes per cell per step of the handle's configuration. */
 double mk_bytes_per_cell(const mk_handle* h);
+/* Fluid cells the handle updates (a slab: its owned planes only). */
 int64_t mk_fluid_cells(const mk_handle* h);
 /* Number of kernel launches one step issues. */
 int32_t mk_launches_per_step(const mk_handle* h);

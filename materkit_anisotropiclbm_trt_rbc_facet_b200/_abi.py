@@ -111,6 +111,14 @@ class MkGrad(C.Structure):
                 ("forward_loops", C.c_int64)]
 
 
+class MkSlabXfer(C.Structure):
+    _fields_ = [("peer", C.c_int32), ("send", C.c_int32), ("tag", C.c_int32), ("array", C.c_int32),
+                ("offset", C.c_int64), ("count", C.c_int64), ("bytes", C.c_int64), ("ptr", C.c_void_p)]
+
+
+MK_SLAB_FILL, MK_SLAB_PHI, MK_SLAB_RETURN, MK_SLAB_RUN_PHI, MK_SLAB_RUN_COLLIDE = range(5)
+MK_SLAB_MAX_XFER = 40
+
 H = C.c_void_p
 P = C.POINTER
 
@@ -167,6 +175,16 @@ PROTOTYPES = {
     "mk_field_stats_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "mk_noalloc_last_error": (C.c_char_p, []),
     "mk_set_metrics_log": (C.c_int, [C.c_char_p]),
+    "mk_slab_split": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_int32)]),
+    "mk_slab_plan": (C.c_int, [P(MkParams), C.c_int32, C.c_int32, C.c_int32, P(MkSlabXfer), C.c_int32,
+                               P(C.c_int32)]),
+    "mk_create_slab": (C.c_int, [P(MkParams), C.c_int32, C.c_int32, P(H)]),
+    "mk_slab_info": (C.c_int, [H, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
+    "mk_slab_next": (C.c_int32, [H]),
+    "mk_slab_transfers": (C.c_int, [H, C.c_int32, P(MkSlabXfer), C.c_int32, P(C.c_int32)]),
+    "mk_slab_done": (C.c_int, [H, C.c_int32]),
+    "mk_slab_run": (C.c_int, [H, C.c_int32]),
+    "mk_slab_exchange_local": (C.c_int, [P(H), C.c_int32, C.c_int32]),
     "mk_bytes_per_cell": (C.c_double, [H]),
     "mk_fluid_cells": (C.c_int64, [H]),
     "mk_launches_per_step": (C.c_int32, [H]),

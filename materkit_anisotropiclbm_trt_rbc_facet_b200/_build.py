@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr",
                   "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
                   "-I", INCLUDE]
-SOURCES = ["mk_kernels.cu", "mk_multiphase.cu", "mk_ensemble.cu", "mk_adjoint.cu", "mk_noalloc.cu", "mk_interface.cu", "mk_api.cpp", "mk_case.cpp", "mk_xml.cpp"]
+SOURCES = ["mk_kernels.cu", "mk_multiphase.cu", "mk_ensemble.cu", "mk_adjoint.cu", "mk_noalloc.cu", "mk_interface.cu", "mk_api.cpp", "mk_slab.cpp", "mk_case.cpp", "mk_xml.cpp"]
 
 
 def _nvcc() -> str:

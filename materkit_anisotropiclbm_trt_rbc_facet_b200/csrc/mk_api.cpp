@@ -20,32 +20,11 @@
 #include "../../include/mkb200.h"
 #include "mk_case.hpp"
 #include "mk_engine.hpp"
+#include "mk_handle.hpp"
 #include "mk_models.hpp"
 
-struct mk_handle {
-  mke::Engine e;
-  std::string err;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two loops captured, keyed by start parity
-  // last mk_tip_track result (velocity = change per loop since then)
-  int64_t tip_step = -1;
-  int32_t tip_seed = -1;
-  double tip_iso = 0.0;
-  double tip_len[6] = {0, 0, 0, 0, 0, 0};
-  // first diagnostics of the handle (reference of the drift in the metrics log)
-  bool have_d0 = false;
-  double d0_mass = 0.0, d0_phi = 0.0;
-};
+namespace mka {
 
-namespace {
-
-// NVTX range around an entry point (visible in Nsight Systems / ncu timelines;
-// without a tool attached the push / pop cost a few instructions).
-struct Range {
-  explicit Range(const char* name) { nvtxRangePushA(name); }
-  ~Range() { nvtxRangePop(); }
-  Range(const Range&) = delete;
-  Range& operator=(const Range&) = delete;
-};
 
 // JSON-lines metrics log (mk_set_metrics_log): one object per timed advance
 // and per diagnostics call, appended under a process-wide lock.
@@ -85,6 +64,13 @@ mk_status cuda_fail(mk_handle* h, cudaError_t st, const char* where) {
   return MK_ERR_CUDA;
 }
 
+// Entry points a slab handle does not offer (its loop runs through the
+// slab protocol, with exchanges between the kernels).
+mk_status slab_refuse(mk_handle* h, const char* what) {
+  h->err = std::string(what) + ": not available on a slab handle (advance it with mk_slab_run and the exchanges)";
+  return MK_ERR_STATE;
+}
+
 bool have_device(std::string& why) {
   int n = 0;
   cudaError_t st = cudaGetDeviceCount(&n);
@@ -111,7 +97,9 @@ mk_status copy_field(mk_handle* h, int field, std::vector<double>& out) {
   return MK_OK;
 }
 
-}  // namespace
+}  // namespace mka
+
+using namespace mka;
 
 namespace mke {
 void set_global_error(const std::string& m) { g_err = m; }
@@ -258,6 +246,7 @@ int64_t mk_get_step(const mk_handle* h) { return h ? h->e.step : -1; }
 mk_status mk_advance(mk_handle* h, int64_t nsteps) {
   const Range nvtx_range("mk_advance");
   if (!h || nsteps < 0) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_advance");
   for (int64_t t = 0; t < nsteps; ++t) {
     cudaError_t st = mke::engine_step(h->e, nullptr);
     if (st != cudaSuccess) return cuda_fail(h, st, "advance");
@@ -268,6 +257,7 @@ mk_status mk_advance(mk_handle* h, int64_t nsteps) {
 mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
   const Range nvtx_range("mk_advance_graph");
   if (!h || nsteps < 0) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_advance_graph");
   mke::Engine& e = h->e;
   int64_t left = nsteps;
   if (left > 0 && e.wave_skip >= 0) {
@@ -343,6 +333,7 @@ mk_status mk_sync(mk_handle* h) {
 
 mk_status mk_set_fused(mk_handle* h, int32_t fused) {
   if (!h) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_set_fused");
   if (fused < 0 || fused > 1) {
     h->err = "loop form must be 0 or 1";
     return MK_ERR_ARG;
@@ -367,6 +358,7 @@ int32_t mk_get_fused(const mk_handle* h) { return h && h->e.wave_ok && h->e.wave
 
 mk_status mk_inject_fault(mk_handle* h, int32_t kind) {
   if (!h) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_inject_fault");
   if (kind != 1) {
     h->err = "unknown fault kind";
     return MK_ERR_ARG;
@@ -448,6 +440,7 @@ mk_status mk_get_grain_field(mk_handle* h, int32_t grain, int32_t dtype, void* h
 mk_status mk_set_state(mk_handle* h, const double* phi, const double* temp, const double* conc, const double* rho,
                        const double* ux, const double* uy, const double* uz) {
   if (!h) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_set_state");
   const mk_params& p = h->e.p;
   const size_t n = (size_t)h->e.ncell;
   std::string err;
@@ -470,6 +463,7 @@ mk_status mk_set_state(mk_handle* h, const double* phi, const double* temp, cons
 
 mk_status mk_set_state_f32(mk_handle* h, const float* phi, const float* temp, const float* conc) {
   if (!h) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_set_state_f32");
   const mk_params& p = h->e.p;
   const size_t n = (size_t)h->e.ncell;
   std::string err;
@@ -666,6 +660,7 @@ static const char kMagic[8] = {'M', 'K', 'B', '2', '0', '0', 'C', 'K'};
 mk_status mk_checkpoint(mk_handle* h, const char* path) {
   const Range nvtx_range("mk_checkpoint");
   if (!h || !path) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_checkpoint");
   mke::Engine& e = h->e;
   cudaError_t st = cudaStreamSynchronize(e.stream);
   if (st != cudaSuccess) return cuda_fail(h, st, "checkpoint sync");
@@ -711,6 +706,7 @@ mk_status mk_checkpoint(mk_handle* h, const char* path) {
 mk_status mk_restore(mk_handle* h, const char* path) {
   const Range nvtx_range("mk_restore");
   if (!h || !path) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_restore");
   mke::Engine& e = h->e;
   FILE* f = fopen(path, "rb");
   if (!f) {
@@ -767,6 +763,7 @@ mk_status mk_restore(mk_handle* h, const char* path) {
 mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel, double* kernel_ms, double* step_ms,
                            int64_t* kernel_launches) {
   if (!h || nsteps <= 0 || !kernel || !kernel_ms || !step_ms) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_profile_steps");
   mke::Engine& e = h->e;
   const int kps = mke::engine_kernels_per_step(e);
   int slot = -1;
@@ -809,6 +806,7 @@ mk_status mk_profile_steps(mk_handle* h, int64_t nsteps, const char* kernel, dou
 mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, double* ms) {
   const Range nvtx_range("mk_time_advance");
   if (!h || nsteps < 0 || !ms) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_time_advance");
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -839,6 +837,7 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
                       double* ms_per_step) {
   const Range nvtx_range("mk_autotune");
   if (!h || trial_steps < 1) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_autotune");
   mke::TuneResult r;
   cudaError_t st = mke::engine_autotune(h->e, trial_steps, &r);
   if (st != cudaSuccess) return cuda_fail(h, st, "autotune");
@@ -858,6 +857,7 @@ mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32
 mk_status mk_backward(mk_handle* h, const mk_loss* loss, mk_grad* out) {
   const Range nvtx_range("mk_backward");
   if (!h || !loss || !out || !loss->target_phi) return MK_ERR_ARG;
+  if (h->e.slab) return slab_refuse(h, "mk_backward");
   std::string err;
   double r[5] = {0, 0, 0, 0, 0};
   cudaError_t st = mke::engine_backward(h->e, loss->target_phi, loss->steps, loss->checkpoint_every, r, err);
@@ -899,6 +899,13 @@ int64_t mk_fluid_cells(const mk_handle* h) {
   int64_t f[3] = {p.nx, p.ny, p.nz};
   for (int a = 0; a < 3; ++a)
     if (p.bc[a] == MK_BC_WALLS) f[a] -= 2;
+  if (h->e.slab) {
+    // the owned planes, less the global wall planes among them
+    const mke::Engine& e = h->e;
+    f[2] = 0;
+    for (int z = e.zg0; z < e.zg0 + e.nz - 2; ++z)
+      if (p.bc[2] != MK_BC_WALLS || (z != 0 && z != e.nzg - 1)) ++f[2];
+  }
   return f[0] * f[1] * f[2];
 }
 

@@ -442,14 +442,33 @@ struct Stor<__nv_bfloat16> {
 // -------------------------------------------------------------- geometry
 // Boundary kinds per axis: 0 periodic, 1 walls (cells 0 and n-1 solid),
 // 2 closed faces (all cells fluid, the faces bounce back).
+//
+// z-slab of a larger domain (slab = 1): the local planes 1 .. nz - 2 are the
+// global planes zg0 .. zg0 + nz - 3 of a domain of nzg planes, and the local
+// planes 0 and nz - 1 are ghost copies of the neighbour slabs' boundary
+// planes.  Ghost cells are never updated (fluid() is false there), but a
+// neighbour link into a ghost plane is valid wherever the global domain has
+// that neighbour, so streaming reads and writes the ghost slots; the z wrap of
+// a periodic global axis goes through the ghosts, never through the index.
 struct Geom {
   int nx, ny, nz;
   int bc0, bc1, bc2;
   int64_t stride;  // population plane stride (cells)
+  int slab = 0, zg0 = 0, nzg = 0;
+
+  // global z of local plane z (slab), and whether a global plane is a cell of
+  // the domain that streams (not beyond a non-periodic face, not a wall)
+  __device__ __forceinline__ int gz(int z) const { return zg0 + z - 1; }
+  __device__ __forceinline__ bool gz_open(int q) const {
+    if (bc2 != 0 && (q < 0 || q >= nzg)) return false;
+    if (bc2 == 1 && (q == 0 || q == nzg - 1)) return false;
+    return true;
+  }
 
   __device__ __forceinline__ bool fluid(int x, int y, int z) const {
     if (bc0 == 1 && (x == 0 || x == nx - 1)) return false;
     if (bc1 == 1 && (y == 0 || y == ny - 1)) return false;
+    if (slab) return z >= 1 && z <= nz - 2 && gz_open(gz(z));
     if (bc2 == 1 && (z == 0 || z == nz - 1)) return false;
     return true;
   }
@@ -475,11 +494,15 @@ struct Geom {
       if (bc1 == 1 && (cy == 0 || cy == ny - 1)) return false;
     }
     if (dz != 0) {
-      if (cz < 0 || cz >= nz) {
-        if (bc2 != 0) return false;
-        cz = cz < 0 ? cz + nz : cz - nz;
+      if (slab) {
+        if (cz < 0 || cz >= nz || !gz_open(gz(cz))) return false;
+      } else {
+        if (cz < 0 || cz >= nz) {
+          if (bc2 != 0) return false;
+          cz = cz < 0 ? cz + nz : cz - nz;
+        }
+        if (bc2 == 1 && (cz == 0 || cz == nz - 1)) return false;
       }
-      if (bc2 == 1 && (cz == 0 || cz == nz - 1)) return false;
     }
     out = idx(cx, cy, cz);
     return true;
@@ -515,11 +538,26 @@ struct Nbr {
     }
   }
 
+  // z of a slab: no wrap (the ghosts hold the neighbours), validity from the
+  // global plane
+  __device__ __forceinline__ static void axis_slab(const Geom& g, int z, int (&o)[3], bool (&v)[3]) {
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      const int cc = z + d;
+      const bool in = cc >= 0 && cc < g.nz;
+      v[d + 1] = in && g.gz_open(g.gz(cc));
+      o[d + 1] = (in ? cc : z) * (g.nx * g.ny);
+    }
+  }
+
   __device__ __forceinline__ Nbr(const Geom& g, int x, int y, int z) {
     bool vx[3], vy[3], vz[3];
     axis(g.nx, g.bc0, x, 1, ox, vx);
     axis(g.ny, g.bc1, y, g.nx, oy, vy);
-    axis(g.nz, g.bc2, z, g.nx * g.ny, oz, vz);
+    if (g.slab)
+      axis_slab(g, z, oz, vz);
+    else
+      axis(g.nz, g.bc2, z, g.nx * g.ny, oz, vz);
     ok = 0u;
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz)
@@ -555,7 +593,9 @@ __device__ __forceinline__ bool fast_cell(const Geom& g, int x, int y, int z) {
     const int hi = bc == 1 ? n - 3 : n - 2;
     return c >= lo && c <= hi;
   };
-  return inside(y, g.ny, g.bc1) && inside(z, g.nz, g.bc2) && (g.bc0 == 0 ? g.nx >= 3 : inside(x, g.nx, g.bc0));
+  // a slab plane needs no z wrap; its z neighbours must all be open globally
+  const bool zin = g.slab ? (g.bc2 == 0 || inside(g.gz(z), g.nzg, g.bc2)) : inside(z, g.nz, g.bc2);
+  return inside(y, g.ny, g.bc1) && zin && (g.bc0 == 0 ? g.nx >= 3 : inside(x, g.nx, g.bc0));
 }
 
 __device__ __forceinline__ Fast make_fast(const Geom& g, int x, int y, int z) {
@@ -584,7 +624,8 @@ __device__ __forceinline__ bool fastw_cell(const Geom& g, int, int y, int z) {
     const int hi = bc == 1 ? n - 3 : n - 2;
     return c >= lo && c <= hi;
   };
-  return inside(y, g.ny, g.bc1) && inside(z, g.nz, g.bc2);
+  const bool zin = g.slab ? (g.bc2 == 0 || inside(g.gz(z), g.nzg, g.bc2)) : inside(z, g.nz, g.bc2);
+  return inside(y, g.ny, g.bc1) && zin;
 }
 
 __device__ __forceinline__ FastW make_fastw(const Geom& g, int x, int y, int z) {

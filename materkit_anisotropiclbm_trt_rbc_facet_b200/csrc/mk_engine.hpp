@@ -76,8 +76,26 @@ struct Engine {
   size_t wave_smem;      // dynamic shared memory (the phi ring)
   unsigned* wave_flags;  // per-tile publication counters (zeroed before every launch)
   int* wave_err;         // error word of the bounded waits (0 = none)
-  int wave_skip;         // test hook: tile that publishes nothing in the next fused launch (-1: none)
+  int wave_skip;         // test hook: tile that publishes nothing in the next fused loop (-1: none)
+  // z-slab of a larger multiphase domain (mk_create_slab): the local planes
+  // 1 .. nz - 2 are the global planes zg0 .. zg0 + nz - 3 of nzg planes; the
+  // planes 0 and nz - 1 are ghosts filled by the exchanges
+  int slab;              // 1 for a slab handle
+  int zg0, nzg;          // first owned global plane, global plane count
+  int rank, nranks;      // this slab and the slab count
+  int slab_next;         // next action of the loop protocol (MK_SLAB_*)
+  void* slab_halo;       // the runs a return exchange delivers: 2 faces x 2 lattices x 5 populations x nx ny,
+                         // merged into the owned boundary planes by mk_slab_done
 };
+
+// Population plane stride of a domain of ncell cells (a multiple of 64 cells).
+inline int64_t pop_stride(int64_t ncell) { return (ncell + 63) / 64 * 64; }
+
+// Bytes of one stored population / of one phi value for a storage precision.
+inline int pop_elem(int precision) {
+  return precision == MK_PREC_FP64 ? 8 : (precision == MK_PREC_FP32 ? 4 : 2);
+}
+inline int phi_elem_of(int precision) { return precision == MK_PREC_FP64 ? 8 : 4; }
 
 // Message returned by mk_last_global_error on this thread.
 void set_global_error(const std::string& m);
@@ -115,6 +133,10 @@ cudaError_t engine_grain_field(Engine& e, int grain);
 // case (sets wave_ok and the wave_* fields), and launch one loop.
 void mp_configure(Engine& e);
 void mp_launch(Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev);
+// One kernel of the two-kernel loop at the parity of e.step: part 0 the phi
+// kernel, part 1 the collision (slab handles run the loop in its parts, with
+// the exchanges between them).
+cudaError_t mp_launch_part(Engine& e, int part);
 
 // After a synchronisation: whether a bounded device wait of the fused loop
 // gave up since the last check (clears the record).  Returns the CUDA status

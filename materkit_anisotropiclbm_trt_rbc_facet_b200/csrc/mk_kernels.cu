@@ -1665,8 +1665,6 @@ cudaError_t diag_t(mke::Engine& e) {
 
 namespace mke {
 
-static int store_bytes(int prec) { return prec == MK_PREC_FP64 ? 8 : (prec == MK_PREC_FP32 ? 4 : 2); }
-
 // Grain table: centre + rotation per object (R = Rz Ry Rx of the ZYX angles in
 // degrees, as in the oracle); one identity entry when there are none.
 void seed_table(const mk_params& p, std::vector<double>& sd) {
@@ -1704,9 +1702,9 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   e.ny = p.ny;
   e.nz = p.nz;
   e.ncell = (int64_t)p.nx * p.ny * p.nz;
-  e.stride = (e.ncell + 63) / 64 * 64;
-  e.elem = store_bytes(p.precision);
-  e.phi_elem = p.precision == MK_PREC_FP64 ? 8 : 4;
+  e.stride = pop_stride(e.ncell);
+  e.elem = pop_elem(p.precision);
+  e.phi_elem = phi_elem_of(p.precision);
   e.device = device;
   if (p.model == MK_MODEL_FLOW || p.model == MK_MODEL_CONVECTION) {
     e.Q0 = p.lattice;
@@ -1829,7 +1827,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
   void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.vel, e.phij, e.gseeds, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
-                  e.field32, e.stage32, e.wave_flags, e.wave_err};
+                  e.field32, e.stage32, e.wave_flags, e.wave_err, e.slab_halo};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (e.stream) cudaStreamDestroy(e.stream);

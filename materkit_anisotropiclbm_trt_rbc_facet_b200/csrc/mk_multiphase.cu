@@ -516,11 +516,12 @@ void launch_mp_wave(mke::Engine& e, int parity, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[1], e.stream);
 }
 
+// parts: bit 0 the phi kernel, bit 1 the collision (3: the whole loop)
 template <class S>
-void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
+void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev, int parts = 3) {
   typedef typename Stor<S>::T T;
   typedef typename PhiOf<S>::type P;
-  if (e.wave && e.wave_ok) {
+  if (parts == 3 && e.wave && e.wave_ok) {
     launch_mp_wave<S>(e, parity, ev);
     return;
   }
@@ -531,13 +532,19 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   S* H = (S*)e.pop1;
   P* phi = (P*)e.phi[0];
   if (ev) cudaEventRecord(ev[0], e.stream);
-  if (parity == 0)
-    k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
-  else
-    k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
+  if (parts & 1) {
+    if (parity == 0)
+      k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
+    else
+      k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
+  }
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
+  }
+  if (!(parts & 2)) {
+    if (ev) cudaEventRecord(ev[3], e.stream);
+    return;
   }
   if (e.minb == 1) {
     if (parity == 0)
@@ -589,6 +596,31 @@ void mp_launch(Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev) {
       launch_mp<__nv_bfloat16>(e, parity, grid, block, ev);
       break;
   }
+}
+
+cudaError_t mp_launch_part(Engine& e, int part) {
+  if (part != 0 && part != 1) return cudaErrorInvalidValue;
+  dim3 grid, block;
+  launch_dims(e, grid, block);
+  const int parity = (int)(e.step & 1);
+  const int parts = part == 0 ? 1 : 2;
+  switch (e.p.precision) {
+    case MK_PREC_FP64:
+      launch_mp<double>(e, parity, grid, block, nullptr, parts);
+      break;
+    case MK_PREC_FP32:
+      launch_mp<float>(e, parity, grid, block, nullptr, parts);
+      break;
+    case MK_PREC_FP16:
+      launch_mp<__half>(e, parity, grid, block, nullptr, parts);
+      break;
+    default:
+      launch_mp<__nv_bfloat16>(e, parity, grid, block, nullptr, parts);
+      break;
+  }
+  e.launches += 1;
+  if (part == 1) e.step += 1;
+  return cudaGetLastError();
 }
 
 }  // namespace mke

@@ -28,6 +28,9 @@ inline Geom make_geom(const mke::Engine& e) {
   g.bc1 = e.p.bc[1];
   g.bc2 = e.p.bc[2];
   g.stride = e.stride;
+  g.slab = e.slab;
+  g.zg0 = e.zg0;
+  g.nzg = e.nzg;
   return g;
 }
 
