@@ -283,6 +283,7 @@ def run_ours(args):
         # dominant kernel, timed live with CUDA events on the library's stream
         prof = s.profile(min(K, 50), wl.get("slot", "collide"))
         fused = args.workload == "bubbles" and s.fused
+        rows = args.workload == "bubbles" and s.row_staged
         # the fused multiphase loop is one launch: no separate phi kernel
         prof_phi = {"kernel_ms": 0.0} if fused else s.profile(min(K, 50), "phi")
         fluid = s.fluid_cells()
@@ -308,8 +309,8 @@ def run_ours(args):
             "step_frac": step_gbs / peak, "collide_ms": prof["kernel_ms"] / launches,
             "phi_ms": prof_phi["kernel_ms"] / launches, "collide_gbs": achieved, "collide_frac": achieved / peak,
             "collide_bytes_per_launch": collide_bytes, "clocks": clk.summary(), "n_bad": d["n_bad"],
-            "launches_per_step": s.launches_per_step(), "tune": tune, "fused": fused,
-            "kernel": "k_mp_wave" if fused else wl["kernel"], **extra,
+            "launches_per_step": s.launches_per_step(), "tune": tune, "fused": fused, "row_staged": rows,
+            "kernel": "k_mp_wave" if fused else ("k_mp_rows" if rows else wl["kernel"]), **extra,
         }
         if prec == args.precision:
             main = (params, s)
@@ -389,7 +390,7 @@ def run_ours(args):
                          **({"dend_ms": round(v["dend_ms"], 4), "dend_frac": round(v["dend_frac"], 4)}
                             if "dend_ms" in v else {}),
                          "tuned": {"block": list(v["tune"]["block"]), "minb": v["tune"]["minb"],
-                                   "fused": v["fused"]}, "kernel": v["kernel"],
+                                   "fused": v["fused"], "row_staged": v["row_staged"]}, "kernel": v["kernel"],
                          "speedup_vs_fp32": round(v["mlups"] / results["fp32"]["mlups"], 3)
                          if "fp32" in results else None}
                      for k, v in results.items()},

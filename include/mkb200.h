@@ -302,6 +302,29 @@ mk_status mk_sync(mk_handle* h);
  * admit the fused loop.  mk_get_fused reports the current form. */
 mk_status mk_set_fused(mk_handle* h, int32_t fused);
 int32_t mk_get_fused(const mk_handle* h);
+/* Collision form of the two-kernel multiphase loop: 0 one thread per cell
+ * loading its populations from global memory, 1 row-staged (whole x rows of
+ * all 38 populations staged through shared memory by the bulk-copy engine,
+ * several rows in flight per CTA; cases whose x rows hold at most 256 cells
+ * and a multiple of 16 bytes).  Both give bit-identical results; the
+ * autotuner keeps the faster.  MK_ERR_ARG when 1 is asked of a case that does
+ * not admit it.  Also available on slab handles. */
+mk_status mk_set_row_staging(mk_handle* h, int32_t on);
+int32_t mk_get_row_staging(const mk_handle* h);
+
+/* The launch configuration of a handle's loop: what mk_autotune chooses, or a
+ * caller pins (a saved tuning reused for many runs of one case).  No
+ * counterpart in the reference.  Every configuration gives the same result
+ * (bit for bit with FP32, FP16 and BF16 storage). */
+typedef struct mk_tuning {
+  int32_t block_x, block_y;  /* block shape of the per-cell kernels (x a multiple of 32, at most 1024 threads) */
+  int32_t minb;              /* occupancy variant of the dominant kernel: 1 or 2 resident 256-thread blocks */
+  int32_t fused;             /* multiphase: the fused one-launch loop (mk_set_fused) */
+  int32_t row_staged;        /* multiphase: the row-staged collision (mk_set_row_staging) */
+} mk_tuning;
+mk_status mk_get_tuning(const mk_handle* h, mk_tuning* out);
+/* MK_ERR_ARG for a shape or a form the case does not admit (nothing changed). */
+mk_status mk_set_tuning(mk_handle* h, const mk_tuning* t);
 /* Test hook of the failure detection, no counterpart in the reference.
  * kind 1: in the next loop of a fused multiphase case one tile publishes none
  * of its phi planes, so its neighbours' bounded waits run out (about a second)
@@ -370,9 +393,12 @@ mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, doubl
 
 /* Launch-shape autotuner: times `trial_steps` loops of each candidate block
  * shape and occupancy variant of the step's kernels, and for a multiphase
- * case also the fused one-launch loop, on a saved copy of the state (restored
- * afterwards, so the simulation is unchanged) and keeps the fastest.  Outputs
- * may be NULL; block_x = block_y = minb = 0 report that the fused loop won. */
+ * case also the fused one-launch loop and the row-staged collision, on a
+ * saved copy of the state (restored afterwards, so the simulation is
+ * unchanged) and keeps the fastest.  Outputs may be NULL; block_x = block_y =
+ * minb = 0 report that the fused loop won, minb = 0 with a block shape that
+ * the row-staged collision won (the shape is the phi kernel's); mk_get_tuning
+ * gives the whole choice. */
 mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32_t* block_y, int32_t* minb,
                       double* ms_per_step);
 

@@ -116,6 +116,14 @@ class MkSlabXfer(C.Structure):
                 ("offset", C.c_int64), ("count", C.c_int64), ("bytes", C.c_int64), ("ptr", C.c_void_p)]
 
 
+class MkTuning(C.Structure):
+    _fields_ = [("block_x", C.c_int32), ("block_y", C.c_int32), ("minb", C.c_int32), ("fused", C.c_int32),
+                ("row_staged", C.c_int32)]
+
+    def to_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 MK_SLAB_FILL, MK_SLAB_PHI, MK_SLAB_RETURN, MK_SLAB_RUN_PHI, MK_SLAB_RUN_COLLIDE = range(5)
 MK_SLAB_MAX_XFER = 40
 
@@ -143,6 +151,10 @@ PROTOTYPES = {
     "mk_inject_fault": (C.c_int, [H, C.c_int32]),
     "mk_set_fused": (C.c_int, [H, C.c_int32]),
     "mk_get_fused": (C.c_int32, [H]),
+    "mk_set_row_staging": (C.c_int, [H, C.c_int32]),
+    "mk_get_tuning": (C.c_int, [H, P(MkTuning)]),
+    "mk_set_tuning": (C.c_int, [H, P(MkTuning)]),
+    "mk_get_row_staging": (C.c_int32, [H]),
     "mk_get_stream": (C.c_int, [H, P(C.c_void_p)]),
     "mk_get_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),
     "mk_get_grain_field": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t]),

@@ -356,6 +356,70 @@ mk_status mk_set_fused(mk_handle* h, int32_t fused) {
 
 int32_t mk_get_fused(const mk_handle* h) { return h && h->e.wave_ok && h->e.wave ? 1 : 0; }
 
+mk_status mk_set_row_staging(mk_handle* h, int32_t on) {
+  if (!h) return MK_ERR_ARG;
+  if (on < 0 || on > 1) {
+    h->err = "row staging must be 0 or 1";
+    return MK_ERR_ARG;
+  }
+  if (on && !h->e.rows_ok) {
+    h->err = "this case does not admit the row-staged collision (multiphase model, x rows of at most 256 cells "
+             "and a multiple of 16 bytes)";
+    return MK_ERR_ARG;
+  }
+  if (on != h->e.rows) {
+    h->e.rows = on;
+    for (auto& g : h->graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+  return MK_OK;
+}
+
+int32_t mk_get_row_staging(const mk_handle* h) { return h && h->e.rows_ok && h->e.rows ? 1 : 0; }
+
+mk_status mk_get_tuning(const mk_handle* h, mk_tuning* out) {
+  if (!h || !out) return MK_ERR_ARG;
+  const mke::Engine& e = h->e;
+  out->block_x = e.block_x;
+  out->block_y = e.block_y;
+  out->minb = e.minb;
+  out->fused = e.wave_ok && e.wave ? 1 : 0;
+  out->row_staged = e.rows_ok && e.rows ? 1 : 0;
+  return MK_OK;
+}
+
+mk_status mk_set_tuning(mk_handle* h, const mk_tuning* t) {
+  if (!h || !t) return MK_ERR_ARG;
+  mke::Engine& e = h->e;
+  auto bad = [&](const char* m) {
+    h->err = std::string("tuning: ") + m;
+    return MK_ERR_ARG;
+  };
+  if (t->block_x < 32 || t->block_x % 32 != 0 || t->block_y < 1 || t->block_x * t->block_y > 1024)
+    return bad("block shape must be a multiple of 32 in x and at most 1024 threads");
+  if ((t->fused != 0 && t->fused != 1) || (t->row_staged != 0 && t->row_staged != 1))
+    return bad("fused and row_staged are 0 or 1");
+  if (t->fused && t->row_staged) return bad("at most one of fused and row_staged");
+  if (t->minb != 1 && t->minb != 2) return bad("minb must be 1 or 2");
+  if (t->fused && !e.wave_ok) return bad("this case does not admit the fused multiphase loop");
+  if (t->row_staged && !e.rows_ok) return bad("this case does not admit the row-staged collision");
+  if (t->fused && e.slab) return slab_refuse(h, "mk_set_tuning (fused)");
+  e.block_x = t->block_x;
+  e.block_y = t->block_y;
+  e.minb = t->minb;
+  e.wave = t->fused;
+  e.rows = t->row_staged;
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  return MK_OK;
+}
+
 mk_status mk_inject_fault(mk_handle* h, int32_t kind) {
   if (!h) return MK_ERR_ARG;
   if (h->e.slab) return slab_refuse(h, "mk_inject_fault");

@@ -77,6 +77,13 @@ struct Engine {
   unsigned* wave_flags;  // per-tile publication counters (zeroed before every launch)
   int* wave_err;         // error word of the bounded waits (0 = none)
   int wave_skip;         // test hook: tile that publishes nothing in the next fused loop (-1: none)
+  // row-staged collision of the two-kernel multiphase loop (k_mp_rows): whole
+  // x rows of all 38 populations staged through shared memory by the
+  // bulk-copy engine, `rows_ns` rows in flight per CTA
+  int rows_ok;           // the case admits it (x rows of at most 256 cells, a multiple of 16 bytes)
+  int rows;              // 1: the collision runs row-staged
+  int rows_ns, rows_grid, rows_threads;
+  size_t rows_stage, rows_smem;
   // z-slab of a larger multiphase domain (mk_create_slab): the local planes
   // 1 .. nz - 2 are the global planes zg0 .. zg0 + nz - 3 of nzg planes; the
   // planes 0 and nz - 1 are ghosts filled by the exchanges

@@ -1815,9 +1815,12 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     mp_configure(e);
     if (e.wave_ok) {
       if ((st = alloc((void**)&e.wave_flags, (size_t)e.wave_sx * e.wave_sy * sizeof(unsigned))) != cudaSuccess) return st;
-      if ((st = alloc((void**)&e.wave_err, sizeof(int))) != cudaSuccess) return st;
       e.wave = 0;  // the two-kernel loop until mk_set_fused or the autotuner chooses the fused one
     }
+    // the error word of the bounded waits (fused loop, row-staged collision)
+    if (e.wave_ok || e.rows_ok)
+      if ((st = alloc((void**)&e.wave_err, sizeof(int))) != cudaSuccess) return st;
+    e.rows = 0;
   }
   // host-side copy of sd must outlive the async copy
   st = cudaStreamSynchronize(e.stream);
@@ -2046,13 +2049,16 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   const int shapes[9][2] = {{32, 2}, {64, 1}, {32, 4}, {64, 2}, {128, 1}, {32, 8}, {64, 4}, {128, 2}, {256, 1}};
   const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 2 : 1;
   double best = 1e300;
-  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0;
-  // candidate -1: the fused multiphase loop (its tiling is fixed by the case)
-  for (int si = e.wave_ok ? -1 : 0; si < 9 && st == cudaSuccess; ++si) {
+  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0, brows = 0;
+  // candidate -1: the fused multiphase loop (its tiling is fixed by the case);
+  // candidate -2: the row-staged collision (the block shape is the phi kernel's)
+  for (int si = -2; si < 9 && st == cudaSuccess; ++si) {
+    if ((si == -1 && !e.wave_ok) || (si == -2 && !e.rows_ok)) continue;
     const int bx = si < 0 ? bx0 : shapes[si][0];
     if (si >= 0 && bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
     for (int mb = 1; mb <= (si < 0 ? 1 : nmb) && st == cudaSuccess; ++mb) {
-      e.wave = si < 0 ? 1 : 0;
+      e.wave = si == -1 ? 1 : 0;
+      e.rows = si == -2 ? 1 : 0;
       e.block_x = bx;
       e.block_y = si < 0 ? by0 : shapes[si][1];
       e.minb = (nmb == 2 && si >= 0) ? mb : mb0;
@@ -2077,6 +2083,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
         bby = e.block_y;
         bmb = e.minb;
         bwave = e.wave;
+        brows = e.rows;
       }
       e.step = step0;
       e.phi_cur = cur0;
@@ -2094,11 +2101,13 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   e.block_y = bby;
   e.minb = bmb;
   e.wave = bwave;
+  e.rows = brows;
   if (out) {
-    // a fused multiphase loop has no block shape or occupancy variant: 0, 0, 0
+    // a fused multiphase loop has no block shape or occupancy variant: 0, 0, 0;
+    // the row-staged collision has no occupancy variant: minb 0
     out->block_x = bwave ? 0 : bbx;
     out->block_y = bwave ? 0 : bby;
-    out->minb = bwave ? 0 : bmb;
+    out->minb = (bwave || brows) ? 0 : bmb;
     out->ms_per_step = best;
     out->candidates = ncand;
   }

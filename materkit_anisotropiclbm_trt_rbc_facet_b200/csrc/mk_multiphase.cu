@@ -35,27 +35,50 @@ __global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const f
   }
 }
 
+// Where a collision reads its pre-collision populations: straight from the
+// lattices in global memory (GlobalLd), or from rows the bulk-copy engine
+// staged in shared memory (RowLd, below).  g(i) / h(0) return f'_i, hr(i)
+// the stored value (f'_i, or f'_i / w_i in 16-bit storage), h0() the FP32
+// rest population of 16-bit storage.
+template <class S, int PARITY, class NB>
+struct GlobalLd {
+  typedef typename Stor<S>::T T;
+  const S* __restrict__ G;
+  const S* __restrict__ H;
+  const float* __restrict__ H0;
+  int64_t stride;
+  const NB& nb;
+  int c;
+  // the Allen-Cahn slots go to L2 now (FP32 / FP64; with 16-bit storage the
+  // prefetch measured 2% slower) and are loaded once the pressure lattice is
+  // stored, so the two lattices' populations are never live together
+  // (register pressure sets the occupancy of this kernel)
+  __device__ __forceinline__ void prefetch() const {
+    if constexpr (Stor<S>::bytes >= 4) {
+#pragma unroll
+      for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
+    }
+  }
+  __device__ __forceinline__ T g(int i) const { return ld_in<S, 19>(G, stride, nb, PARITY, c, i); }
+  __device__ __forceinline__ T h(int i) const { return ld_in<S, 19>(H, stride, nb, PARITY, c, i); }
+  __device__ __forceinline__ T hr(int i) const { return ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i); }
+  __device__ __forceinline__ T h0() const { return T(H0[c]); }
+};
+
 // One loop of a fluid cell.  Every population load (19 g, 19 h) is issued
 // before any store: the loads are the latency the kernel must hide, and a
 // store into the same array in between would stop the compiler from hoisting
 // the later loads (in place, on odd loops a direction's result goes to the
 // slot its opposite direction is read from).
-template <class S, class P, int PARITY, class NB, class PH>
+template <class S, class P, int PARITY, class NB, class PH, class LD>
 __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
                                                 const PH& phi_src, const int64_t stride, const NB& nb,
-                                                const int c, const MpK<typename Stor<S>::T>& k) {
+                                                const int c, const MpK<typename Stor<S>::T>& k, const LD& ld) {
   typedef typename Stor<S>::T T;
-  // the Allen-Cahn slots go to L2 now (FP32 / FP64; with 16-bit storage the
-  // prefetch measured 2% slower) and are loaded once the pressure lattice is
-  // stored, so the two lattices' populations are never live together
-  // (register pressure sets the occupancy of this kernel)
-  if constexpr (Stor<S>::bytes >= 4) {
-#pragma unroll
-    for (int i = 1; i < 19; ++i) pf_in<S, 19>(H, stride, nb, PARITY, c, i);
-  }
+  ld.prefetch();
   T gp_[19];  // g (rests at 0)
 #pragma unroll
-  for (int i = 0; i < 19; ++i) gp_[i] = ld_in<S, 19>(G, stride, nb, PARITY, c, i);
+  for (int i = 0; i < 19; ++i) gp_[i] = ld.g(i);
   T m[19];  // MRT moments: m[0] = p*, (m[3], m[5], m[7]) = j
   mrt19_moments<T>(gp_, m);
   const T pstar = m[0], jx = m[3], jy = m[5], jz = m[7];
@@ -102,9 +125,9 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
   //   X_odd = 3 phi eu, the sharpening flux w_i Y = w_i (1 - om/2) lam (e.n)
   constexpr bool SC = Stor<S>::scaled;
   T h[19];
-  h[0] = Rest32<S>::on ? T(H0[c]) : ld_in<S, 19>(H, stride, nb, PARITY, c, 0);
+  h[0] = Rest32<S>::on ? ld.h0() : ld.h(0);
 #pragma unroll
-  for (int i = 1; i < 19; ++i) h[i] = ld_in_raw<S, 19>(H, stride, nb, PARITY, c, i);
+  for (int i = 1; i < 19; ++i) h[i] = ld.hr(i);
   const T om_h = k.om_h;
   const T one_om = T(1) - om_h;
   const T src = (T(1) - T(0.5) * om_h) * lam;
@@ -208,11 +231,180 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   if (fast_cell(g, x, y, z)) {
     const Fast fa = make_fast(g, x, y, z);
-    mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Fast>{phi, fa, fa.c}, g.stride, fa, fa.c, k);
+    mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Fast>{phi, fa, fa.c}, g.stride, fa, fa.c, k,
+                                  GlobalLd<S, PARITY, Fast>{G, H, H0, g.stride, fa, fa.c});
   } else {
     const Nbr nb(g, x, y, z);
     const int c = nb.idx(0, 0, 0);
-    mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Nbr>{phi, nb, c}, g.stride, nb, c, k);
+    mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Nbr>{phi, nb, c}, g.stride, nb, c, k,
+                                  GlobalLd<S, PARITY, Nbr>{G, H, H0, g.stride, nb, c});
+  }
+}
+
+// ------------------------------------------- row-staged collision (rows)
+// The two-kernel loop's collision with its population loads handed to the
+// bulk-copy engine.  A CTA owns whole x rows (one thread per cell) and keeps
+// `ns` rows in flight: for each row it stages the 19 g and 19 h source rows
+// (and the FP32 rest row of 16-bit storage) into shared memory with
+// cp.async.bulk, completing on the row's mbarrier, while it computes the row
+// staged before.  The bytes in flight no longer depend on how many warps the
+// collision's registers leave resident.
+//
+// The source row of direction i: on even loops the cell's own row of plane i;
+// on odd loops the row (y - e_y, z - e_z) of plane inv(i), or the own row of
+// plane i when that row link is closed (wall, closed face, slab end).  The x
+// shift of an odd loop is a column offset in shared memory (periodic x wraps
+// inside the staged row); a closed x link (walled or closed x, at the row
+// ends only) reads the own slot from global memory.  Every slot a row's
+// cells read is read and later written by that cell alone (AA ownership), so
+// staging ahead races with nothing.  The per-cell arithmetic is
+// mp_collide_cell's, on the same values: the result is bit-identical to
+// k_mp_collide.
+struct RowPlan {
+  int nrows;      // fluid rows (y, z)
+  int ylo, nyf;   // fluid y span
+  int zlo;        // first fluid plane
+  int xlo, xhi;   // fluid x span
+  int xper;       // x periodic
+  int xf;         // a fluid x (row link tests)
+  int ns;         // rows in flight per CTA
+  int stage;      // bytes of one staged row
+};
+
+template <class S, int PARITY>
+struct RowLd {
+  typedef typename Stor<S>::T T;
+  const S* sg;         // staged g rows [19][nx]
+  const S* sh;         // staged h rows [19][nx]
+  const float* sh0;    // staged FP32 rest row (16-bit storage)
+  int x, nx;
+  unsigned rowok;      // odd loops: bit i set when the row link of direction i is open
+  int xm, xp;          // column of the x - 1 / x + 1 source, -1 when that link is closed
+  const S* __restrict__ G;
+  const S* __restrict__ H;
+  int64_t stride;
+  int c;
+  __device__ __forceinline__ void prefetch() const {}
+  // shared-memory column of direction i's source, -1 for the cell's own slot in global memory
+  __device__ __forceinline__ int col(int i) const {
+    if (PARITY == 0 || ex(i) == 0 || !((rowok >> i) & 1u)) return x;
+    return ex(i) > 0 ? xm : xp;
+  }
+  __device__ __forceinline__ T g(int i) const {
+    const int q = col(i);
+    return Stor<S>::ld(q >= 0 ? sg + i * nx + q : G + i * stride + c, T(wq<19>(i)));
+  }
+  __device__ __forceinline__ T h(int i) const {
+    const int q = col(i);
+    return Stor<S>::ld(q >= 0 ? sh + i * nx + q : H + i * stride + c, T(wq<19>(i)));
+  }
+  __device__ __forceinline__ T hr(int i) const {
+    const int q = col(i);
+    return Stor<S>::ldr(q >= 0 ? sh + i * nx + q : H + i * stride + c);
+  }
+  __device__ __forceinline__ T h0() const { return T(sh0[x]); }
+};
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256, 2) k_mp_rows(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                                    const P* __restrict__ phi, const Geom g,
+                                                    const MpK<typename Stor<S>::T> k, const RowPlan rp,
+                                                    int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);        // ns <= 4 barriers
+  unsigned* s_rowok = reinterpret_cast<unsigned*>(smem + 64);  // per stage
+  unsigned char* stage0 = smem + 128;
+  const int nx = g.nx, tid = threadIdx.x;
+  const int nct = gridDim.x, b = blockIdx.x;
+  const int mine = b < rp.nrows ? (rp.nrows - b + nct - 1) / nct : 0;
+  if (mine == 0) return;  // the whole CTA, before any barrier
+  const int ns = rp.ns;
+  constexpr bool R32 = Rest32<S>::on;
+  const unsigned row_bytes = (unsigned)nx * sizeof(S);
+  if (tid == 0) {
+    for (int s = 0; s < ns; ++s) mkw::mbar_init(&bar[s], 1);
+    mkw::fence_mbar_init();
+  }
+  __syncthreads();
+  auto row_yz = [&](int kk, int& y, int& z) {
+    const int r = b + kk * nct;
+    y = rp.ylo + r % rp.nyf;
+    z = rp.zlo + r / rp.nyf;
+  };
+  // warp 0: stage the source rows of this CTA's kk-th row into stage kk % ns,
+  // lane i the two rows of direction i (lane 19 the FP32 rest row)
+  auto issue = [&](int kk) {
+    const int s = kk % ns, lane = tid & 31;
+    int y, z;
+    row_yz(kk, y, z);
+    unsigned char* st = stage0 + (size_t)s * rp.stage;
+    S* sg = reinterpret_cast<S*>(st);
+    S* sh = sg + 19 * nx;
+    const int64_t own = g.idx(0, y, z);
+    mkw::fence_proxy_async_shared();  // the stage's earlier reads before the engine's writes
+    if (lane == 0) {
+      const unsigned bytes = (R32 ? 37u : 38u) * row_bytes + (R32 ? (unsigned)nx * 4u : 0u);
+      mkw::mbar_arrive_expect(&bar[s], bytes);
+    }
+    __syncwarp();
+    bool open = false;
+    if (lane < 19) {
+      const int i = lane;
+      // element offset of the source row in the lattice arrays
+      int64_t nb = own, off = (int64_t)i * g.stride + own;
+      if (PARITY == 1 && g.nbr(rp.xf, y, z, 0, -ey(i), -ez(i), nb)) {
+        open = true;
+        off = (int64_t)inv(i) * g.stride + (nb - rp.xf);
+      }
+      mkw::bulk_g2s(sg + i * nx, G + off, row_bytes, &bar[s]);
+      if (!R32 || i > 0) mkw::bulk_g2s(sh + i * nx, H + off, row_bytes, &bar[s]);
+    } else if (R32 && lane == 19) {
+      mkw::bulk_g2s(sh + 19 * nx, H0 + own, (unsigned)nx * 4u, &bar[s]);
+    }
+    const unsigned ok = __ballot_sync(0xffffffffu, open);  // bit i: direction i's row link is open
+    if (lane == 0) s_rowok[s] = ok;
+  };
+  if (tid < 32)
+    for (int kk = 0; kk < ns && kk < mine; ++kk) issue(kk);
+  int kk = 0;
+  for (; kk < mine; ++kk) {
+    const int s = kk % ns;
+    const bool landed = mkw::mbar_wait(&bar[s], (unsigned)((kk / ns) & 1), err);
+    if (!__syncthreads_and(landed)) break;  // one decision for the CTA
+    int y, z;
+    row_yz(kk, y, z);
+    const int x = tid;
+    if (x < nx && x >= rp.xlo && x <= rp.xhi) {
+      const S* sg = reinterpret_cast<const S*>(stage0 + (size_t)s * rp.stage);
+      const S* sh = sg + 19 * nx;
+      const float* sh0 = reinterpret_cast<const float*>(sh + 19 * nx);
+      int xm = x - 1, xp = x + 1;
+      if (rp.xper) {
+        xm = x == 0 ? nx - 1 : xm;
+        xp = x == nx - 1 ? 0 : xp;
+      } else {
+        xm = xm >= rp.xlo ? xm : -1;
+        xp = xp <= rp.xhi ? xp : -1;
+      }
+      const unsigned rowok = s_rowok[s];
+      if (fast_cell(g, x, y, z)) {
+        const Fast fa = make_fast(g, x, y, z);
+        mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Fast>{phi, fa, fa.c}, g.stride, fa, fa.c, k,
+                                      RowLd<S, PARITY>{sg, sh, sh0, x, nx, rowok, xm, xp, G, H, g.stride, fa.c});
+      } else {
+        const Nbr nb(g, x, y, z);
+        const int c = nb.idx(0, 0, 0);
+        mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Nbr>{phi, nb, c}, g.stride, nb, c, k,
+                                      RowLd<S, PARITY>{sg, sh, sh0, x, nx, rowok, xm, xp, G, H, g.stride, c});
+      }
+    }
+    __syncthreads();  // every thread is done with stage s
+    if (tid < 32 && kk + ns < mine) issue(kk + ns);
+  }
+  // a wait gave up: let the copies already issued land before the CTA exits
+  if (kk < mine && tid == 0) {
+    const int issued = kk + ns < mine ? kk + ns : mine;
+    for (int q = kk; q < issued; ++q) mkw::mbar_wait(&bar[q % ns], (unsigned)((q / ns) & 1), err);
   }
 }
 
@@ -420,10 +612,13 @@ __global__ void __launch_bounds__(256, 2) k_mp_wave(S* __restrict__ G, S* __rest
         const PhiRing<P> src{lo, mid, hi, (r + 1) * w.pitch + lane + 4, w.pitch};
         if (fast_cell(g, x, y, z)) {
           const Fast fa = make_fast(g, x, y, z);
-          mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, fa, fa.c, k);
+          mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, fa, fa.c, k,
+                                        GlobalLd<S, PARITY, Fast>{G, H, H0, g.stride, fa, fa.c});
         } else {
           const Nbr nb(g, x, y, z);
-          mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, nb, nb.idx(0, 0, 0), k);
+          const int c = nb.idx(0, 0, 0);
+          mp_collide_cell<S, P, PARITY>(G, H, H0, src, g.stride, nb, c, k,
+                                        GlobalLd<S, PARITY, Nbr>{G, H, H0, g.stride, nb, c});
         }
       }
     }
@@ -473,6 +668,113 @@ void wave_config(mke::Engine& e) {
       return;
     }
   e.wave_ok = 1;
+}
+
+// Row-staged collision: eligibility, rows in flight and grid for the case.
+template <class S>
+void rows_config(mke::Engine& e) {
+  typedef typename PhiOf<S>::type P;
+  e.rows_ok = 0;
+  const int nx = e.nx;
+  if (e.p.model != MK_MODEL_MULTIPHASE || nx > 256 || ((size_t)nx * sizeof(S)) % 16 != 0 || nx < 3) return;
+  const bool r32 = Rest32<S>::on;
+  size_t stage = (size_t)38 * nx * sizeof(S) + (r32 ? (size_t)nx * 4 : 0);
+  stage = (stage + 127) / 128 * 128;
+  const int threads = (nx + 31) / 32 * 32;
+  int dev = e.device, sms = 0, smem_sm = 0, smem_blk = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (sms <= 0) return;
+  const void* kerns[2] = {(const void*)k_mp_rows<S, P, 0>, (const void*)k_mp_rows<S, P, 1>};
+  // CTAs per SM the registers allow, then as many rows in flight (2..4) as
+  // that many CTAs' shared memory holds
+  int per_sm = 1 << 20;
+  for (const void* kern : kerns) {
+    int bsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bsm, kern, threads, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    per_sm = std::min(per_sm, bsm);
+  }
+  if (per_sm < 1) return;
+  int ns = 0, cta = per_sm;
+  for (; cta >= 1 && ns < 2; --cta) {
+    const size_t budget = std::min<size_t>((size_t)smem_sm / cta - 1024, (size_t)smem_blk);
+    ns = (int)std::min<size_t>(4, (budget - 128) / stage);
+    if (ns >= 2) break;
+  }
+  if (ns < 2) return;
+  const size_t smem = 128 + (size_t)ns * stage;
+  for (const void* kern : kerns)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+  int resident = 1 << 20;
+  for (const void* kern : kerns) {
+    int bsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bsm, kern, threads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    resident = std::min(resident, bsm);
+  }
+  if (resident < 1) return;
+  e.rows_ns = ns;
+  e.rows_stage = stage;
+  e.rows_smem = smem;
+  e.rows_threads = threads;
+  e.rows_grid = resident * sms;
+  e.rows_ok = 1;
+}
+
+// The fluid rows of the case as the row-staged kernel enumerates them (the
+// spans Geom::fluid gives: walls drop the end cells of an axis, a slab its
+// ghost planes and any global wall plane it holds).
+inline RowPlan row_plan(const mke::Engine& e, const Geom& g) {
+  auto span = [](int n, int bc, int& lo, int& hi) {
+    lo = bc == MK_BC_WALLS ? 1 : 0;
+    hi = bc == MK_BC_WALLS ? n - 2 : n - 1;
+  };
+  RowPlan rp;
+  span(g.nx, g.bc0, rp.xlo, rp.xhi);
+  int yhi = 0, zlo = 0, zhi = 0;
+  span(g.ny, g.bc1, rp.ylo, yhi);
+  if (g.slab) {
+    zlo = 1;
+    zhi = g.nz - 2;
+    if (g.bc2 == MK_BC_WALLS) {
+      if (g.zg0 == 0) zlo = 2;
+      if (g.zg0 + g.nz - 3 == g.nzg - 1) zhi = g.nz - 3;
+    }
+  } else {
+    span(g.nz, g.bc2, zlo, zhi);
+  }
+  rp.nyf = std::max(0, yhi - rp.ylo + 1);
+  rp.zlo = zlo;
+  rp.nrows = rp.nyf * std::max(0, zhi - zlo + 1);
+  rp.xper = g.bc0 == MK_BC_PERIODIC;
+  rp.xf = rp.xlo;
+  rp.ns = e.rows_ns;
+  rp.stage = (int)e.rows_stage;
+  return rp;
+}
+
+template <class S>
+void launch_mp_rows(mke::Engine& e, int parity, const Geom& g, const MpK<typename Stor<S>::T>& k) {
+  typedef typename PhiOf<S>::type P;
+  const RowPlan rp = row_plan(e, g);
+  if (rp.nrows == 0 || rp.xhi < rp.xlo) return;
+  S* G = (S*)e.pop0;
+  S* H = (S*)e.pop1;
+  const P* phi = (const P*)e.phi[0];
+  const int grid = std::min(e.rows_grid, rp.nrows);
+  if (parity == 0)
+    k_mp_rows<S, P, 0><<<grid, e.rows_threads, e.rows_smem, e.stream>>>(G, H, e.rest1, phi, g, k, rp, e.wave_err);
+  else
+    k_mp_rows<S, P, 1><<<grid, e.rows_threads, e.rows_smem, e.stream>>>(G, H, e.rest1, phi, g, k, rp, e.wave_err);
 }
 
 template <class S>
@@ -546,7 +848,9 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
     if (ev) cudaEventRecord(ev[3], e.stream);
     return;
   }
-  if (e.minb == 1) {
+  if (e.rows && e.rows_ok) {
+    launch_mp_rows<S>(e, parity, g, k);
+  } else if (e.minb == 1) {
     if (parity == 0)
       k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
     else
@@ -568,15 +872,19 @@ void mp_configure(Engine& e) {
   switch (e.p.precision) {
     case MK_PREC_FP64:
       wave_config<double>(e);
+      rows_config<double>(e);
       break;
     case MK_PREC_FP32:
       wave_config<float>(e);
+      rows_config<float>(e);
       break;
     case MK_PREC_FP16:
       wave_config<__half>(e);
+      rows_config<__half>(e);
       break;
     default:
       wave_config<__nv_bfloat16>(e);
+      rows_config<__nv_bfloat16>(e);
       break;
   }
 }

@@ -1,7 +1,8 @@
-// mk_wave.cuh — inline PTX for the fused (one-launch) multiphase step:
-// inter-CTA publication flags with acquire/release at GPU scope, bounded
-// waits, mbarriers and the bulk-copy engine (cp.async.bulk, no multicast)
-// staging rows of the phi field into shared memory.
+// mk_wave.cuh — inline PTX for the staged multiphase kernels (the fused
+// one-launch loop and the row-staged collision): inter-CTA publication flags
+// with acquire/release at GPU scope, bounded waits, mbarriers and the
+// bulk-copy engine (cp.async.bulk, no multicast) staging rows into shared
+// memory.
 //
 // Every wait here has an iteration limit.  When it runs out the wait records
 // a code in the launch's error word and returns; later waits see the word and
@@ -80,12 +81,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 }
 
 // Wait for the completion of the barrier phase with the given parity.
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+// Returns false (and records the code) when the wait gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
   for (int it = 0; it < kSpinLimit; ++it) {
-    if (mbar_try_wait(bar, parity)) return;
+    if (mbar_try_wait(bar, parity)) return true;
     if (it >= 16) __nanosleep(64);
   }
   atomicCAS(err, ERR_NONE, ERR_MBAR_WAIT);
+  return false;
 }
 
 // Order this thread's earlier generic-proxy accesses (and what it observed

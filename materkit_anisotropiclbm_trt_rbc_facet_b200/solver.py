@@ -366,6 +366,31 @@ class Solver:
     def fused(self, on: bool) -> None:
         _check(self._lib.mk_set_fused(self._h, 1 if on else 0), self._h)
 
+    @property
+    def tuning(self) -> dict:
+        """The launch configuration (block shape, occupancy variant, loop and
+        collision forms) as a dict; assign a dict (or a subset) to pin it."""
+        t = A.MkTuning()
+        _check(self._lib.mk_get_tuning(self._h, C.byref(t)), self._h)
+        return t.to_dict()
+
+    @tuning.setter
+    def tuning(self, d: dict) -> None:
+        cur = self.tuning
+        cur.update(d)
+        t = A.MkTuning(**{k: int(v) for k, v in cur.items()})
+        _check(self._lib.mk_set_tuning(self._h, C.byref(t)), self._h)
+
+    @property
+    def row_staged(self) -> bool:
+        """Whether the multiphase collision stages whole x rows through shared
+        memory with the bulk-copy engine."""
+        return bool(self._lib.mk_get_row_staging(self._h))
+
+    @row_staged.setter
+    def row_staged(self, on: bool) -> None:
+        _check(self._lib.mk_set_row_staging(self._h, 1 if on else 0), self._h)
+
     def bytes_per_cell(self) -> float:
         return float(self._lib.mk_bytes_per_cell(self._h))
 
