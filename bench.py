@@ -62,6 +62,10 @@ WORKLOADS = {
                    "metric": "MLUPS, %HBM roofline: multigrain 128^3, 8 grain lattices + thermal",
                    "size": 128, "precision": "fp32", "kernel": "k_mg_collide", "collision": "BGK(g_j) + BGK(T)",
                    "data": "synthetic (2 x 2 x 2 grains of radius n/5 at the quarter points)"},
+    "poiseuille": {"workload": "Poiseuille channel {n}x{h}x{h}, D3Q19 TRT (magic 3/16), walls in y, body force 1e-6",
+                   "metric": "MLUPS: Poiseuille channel 64x32x32, D3Q19 TRT, FP64",
+                   "size": 64, "precision": "fp64", "kernel": "k_flow", "collision": "TRT(f)",
+                   "data": "synthetic (fluid at rest, constant body force)"},
     "ensemble": {"workload": "solutal dendrite ensemble: 48 domains, edges 48-128, 1-6 seeds each, seed 0xE45E",
                  "metric": "MLUPS aggregate, %HBM roofline: 48-domain solutal dendrite ensemble, BF16, "
                            "persistent + graph",
@@ -168,6 +172,8 @@ def _case_path(precision: str, n: int, workload: str = "bubbles") -> str:
         q = [n / 4.0, 3.0 * n / 4.0]
         seeds = [(x, y, z, n / 5.0) for x in q for y in q for z in q]
         text = cases.multigrain(n=n, precision=precision, loops=5000, seeds=seeds)
+    elif workload == "poiseuille":
+        text = cases.poiseuille(nx=n, ny=n // 2, nz=n // 2, precision=precision, loops=2000)
     elif workload == "flow_dendrite":
         text = cases.flow_dendrite(nx=n, ny=n, nz=n, precision=precision, loops=5000, radius=8.0, u_in=0.02,
                                    center=(n / 3.0, (n - 1) / 2.0, (n - 1) / 2.0))
@@ -186,6 +192,7 @@ def _collide_bytes(workload: str, prec: str, cells: int) -> int:
               written, phi(t+1) and phi(t) read, T/U read and written.
     flow_dendrite: the flow kernel: D3Q19 read and written, phi(t) read, the
               velocity (3 values) written.
+    poiseuille: the flow kernel: D3Q19 read and written.
     """
     S = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[prec]
     P = 8 if prec == "fp64" else 4
@@ -193,6 +200,8 @@ def _collide_bytes(workload: str, prec: str, cells: int) -> int:
         return cells * (2 * 38 * S + P + (4 if S == 2 else 0))
     if workload == "flow_dendrite":
         return cells * (38 * S + 4 * P)
+    if workload == "poiseuille":
+        return cells * 38 * S
     if workload == "multigrain":
         # 8 grain lattices and the thermal lattice read and written, phi_j read
         # (the stencil's halo counted once), phi(t+1), phi(t) read, T read and written
@@ -284,8 +293,8 @@ def run_ours(args):
         prof = s.profile(min(K, 50), wl.get("slot", "collide"))
         fused = args.workload == "bubbles" and s.fused
         rows = args.workload == "bubbles" and s.row_staged
-        # the fused multiphase loop is one launch: no separate phi kernel
-        prof_phi = {"kernel_ms": 0.0} if fused else s.profile(min(K, 50), "phi")
+        # the fused multiphase loop is one launch, the flow model has no phi kernel
+        prof_phi = {"kernel_ms": 0.0} if (fused or args.workload == "poiseuille") else s.profile(min(K, 50), "phi")
         fluid = s.fluid_cells()
         launches = min(K, 50)
         t_launch = prof["kernel_ms"] / launches * 1e-3
@@ -319,24 +328,40 @@ def run_ours(args):
     params, s = main
     r = results[args.precision]
 
-    # end to end through the C ABI: pinned host phi -> device, K loops, phi -> pinned host
+    # end to end through the C ABI: pinned host state -> device, K loops, a
+    # field -> pinned host (phi as FP32; the flow model: density as FP64 in,
+    # ux as FP32 out)
     cells = params.ncell()
+    flow = args.workload == "poiseuille"
     nbytes = cells * 4
+    nbytes_in = cells * (8 if flow else 4)
     hp_in, hp_out = A.C.c_void_p(), A.C.c_void_p()
-    lib.mk_host_alloc(nbytes, A.C.byref(hp_in))
+    lib.mk_host_alloc(nbytes_in, A.C.byref(hp_in))
     lib.mk_host_alloc(nbytes, A.C.byref(hp_out))
-    phi_in = np.ctypeslib.as_array((A.C.c_float * cells).from_address(hp_in.value))
     phi_out = np.ctypeslib.as_array((A.C.c_float * cells).from_address(hp_out.value))
-    phi_in[:] = initial_field(params, "phi").ravel().astype(np.float32)
-    fptr = phi_in.ctypes.data_as(A.C.POINTER(A.C.c_float))
+    out_field = A.MK_FIELD_UX if flow else A.MK_FIELD_PHI
+    if flow:
+        rho_in = np.ctypeslib.as_array((A.C.c_double * cells).from_address(hp_in.value))
+        rho_in[:] = initial_field(params, "rho").ravel()
+        dptr = rho_in.ctypes.data_as(A.C.POINTER(A.C.c_double))
+
+        def upload():
+            return lib.mk_set_state(s.handle, None, None, None, dptr, None, None, None)
+    else:
+        phi_in = np.ctypeslib.as_array((A.C.c_float * cells).from_address(hp_in.value))
+        phi_in[:] = initial_field(params, "phi").ravel().astype(np.float32)
+        fptr = phi_in.ctypes.data_as(A.C.POINTER(A.C.c_float))
+
+        def upload():
+            return lib.mk_set_state_f32(s.handle, fptr, None, None)
     # warm the staging buffers once
-    lib.mk_set_state_f32(s.handle, fptr, None, None)
-    lib.mk_get_field(s.handle, A.MK_FIELD_PHI, A.MK_DTYPE_F32, hp_out, nbytes)
+    upload()
+    lib.mk_get_field(s.handle, out_field, A.MK_DTYPE_F32, hp_out, nbytes)
     barrier()
     t0 = time.perf_counter()
-    stt = lib.mk_set_state_f32(s.handle, fptr, None, None)
+    stt = upload()
     stt |= lib.mk_advance_graph(s.handle, K)
-    stt |= lib.mk_get_field(s.handle, A.MK_FIELD_PHI, A.MK_DTYPE_F32, hp_out, nbytes)
+    stt |= lib.mk_get_field(s.handle, out_field, A.MK_DTYPE_F32, hp_out, nbytes)
     e2e_s = time.perf_counter() - t0
     e2e_mlups, e2e_s = job_mlups(cells, K, e2e_s, max_over_ranks, sum_over_ranks)  # every rank, even on error
     if stt != 0:
@@ -346,9 +371,10 @@ def run_ours(args):
     lib.mk_host_free(hp_out)
     s.close()
 
-    cpu = None
+    cpu = cpu_ref = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n, budget_s=args.cpu_budget, workload=args.workload)
+        cpu_ref = cpu_baseline_reference_structure(n, budget_s=args.cpu_budget, workload=args.workload)
 
     if pg is not None:
         pg.barrier()
@@ -369,12 +395,14 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "f64" if args.precision == "fp64" else "f32",
         "data": wl["data"],
-        "config": {"workload": wl["workload"].format(n=n), "cells": params.ncell(), "storage": args.precision,
-                   "collision": wl["collision"], "streaming": "AA in place",
-                   "l2": "inputs larger than L2 (%.2f GB resident populations)" % (
-                       r["bytes_per_cell"] * params.ncell() / 2 / 1e9),
+        "config": {"workload": wl["workload"].format(n=n, h=n // 2), "cells": params.ncell(),
+                   "storage": args.precision, "collision": wl["collision"], "streaming": "AA in place",
+                   "l2": ("inputs larger than L2 (%.2f GB resident populations)"
+                          if r["bytes_per_cell"] * params.ncell() / 2 > 126e6 else
+                          "inputs resident in L2 (%.3f GB resident populations: the rate is not an HBM figure)")
+                   % (r["bytes_per_cell"] * params.ncell() / 2 / 1e9),
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "kernel": r["kernel"], "achieved": round(r["collide_gbs"], 1),
                      "peak": peak, "unit": "GB/s", "frac": round(r["collide_frac"], 4),
@@ -394,13 +422,16 @@ def run_ours(args):
                          "speedup_vs_fp32": round(v["mlups"] / results["fp32"]["mlups"], 3)
                          if "fp32" in results else None}
                      for k, v in results.items()},
-        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": nbytes / K,
+        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": nbytes_in / K,
                 "d2h_bytes_per_step": nbytes / K, "seconds": round(e2e_s, 4), "phi_finite": phi_ok,
-                "path": "mk_set_state_f32 (pinned) + mk_advance_graph + mk_get_field f32 (pinned)"},
+                "path": ("mk_set_state rho f64 (pinned) + mk_advance_graph + mk_get_field ux f32 (pinned)" if flow
+                         else "mk_set_state_f32 (pinned) + mk_advance_graph + mk_get_field f32 (pinned)")},
         "gpu_launches": K * r["launches_per_step"],
         "clocks": r["clocks"],
         "cpu_baseline": cpu,
     }
+    if cpu_ref is not None:
+        line["cpu_baseline_reference_structure"] = cpu_ref
     print(json.dumps(line), flush=True)
 
 
@@ -540,7 +571,39 @@ def _oracle_case(workload: str, n: int):
 def _sample_name(workload: str, n: int) -> str:
     if workload == "ensemble":
         return "domain 0 of the ensemble"
+    if workload == "poiseuille":
+        return f"the {n}x{n // 2}x{n // 2} channel"
     return f"the {n}^3 case"
+
+
+def cpu_baseline_reference_structure(n: int, budget_s: float = 20.0, workload: str = "dendrite"):
+    """Time the method in the reference's node-object layout (mkNode, every
+    field of a node in one object, schedule(static, 16) node sweeps) on the
+    host cores, on a bounded sample; the flow model and the thermal dendrite
+    only (None for other workloads)."""
+    if workload not in ("dendrite", "poiseuille"):
+        return None
+    from oracle.orc import Oracle, ReferenceStructure, load as load_oracle
+
+    lib = load_oracle()
+    params, fields = _oracle_case(workload, n)
+    o = Oracle(params, **fields)
+    a = ReferenceStructure(o)
+    o.close()
+    t0 = time.perf_counter()
+    a.advance(1)
+    t1 = time.perf_counter() - t0
+    steps = max(1, min(2000, int(budget_s / max(t1, 1e-4))))
+    t0 = time.perf_counter()
+    a.advance(steps)
+    dt = time.perf_counter() - t0
+    a.close()
+    cells = params.ncell()
+    return {"value": round(cells * steps / dt / 1e6, 2), "unit": "MLUPS", "cores": int(lib.orc_get_threads()),
+            "kind": "reference-structure",
+            "sample": f"{steps} loops of {_sample_name(workload, n)} after 1 untimed loop (FP64, the reference's "
+                      f"node-object layout, {ReferenceStructure.node_bytes()} B per node, schedule(static, 16))",
+            "seconds": round(dt, 2)}
 
 
 def cpu_baseline(n: int, budget_s: float = 20.0, workload: str = "bubbles"):

@@ -318,7 +318,8 @@ int32_t mk_get_row_staging(const mk_handle* h);
  * (bit for bit with FP32, FP16 and BF16 storage). */
 typedef struct mk_tuning {
   int32_t block_x, block_y;  /* block shape of the per-cell kernels (x a multiple of 32, at most 1024 threads) */
-  int32_t minb;              /* occupancy variant of the dominant kernel: 1 or 2 resident 256-thread blocks */
+  int32_t minb;              /* occupancy variant of the dominant kernel: 1 or 2 resident 256-thread blocks;
+                                multiphase also 3, 4, 5: registers capped at 112, 96, 80 */
   int32_t fused;             /* multiphase: the fused one-launch loop (mk_set_fused) */
   int32_t row_staged;        /* multiphase: the row-staged collision (mk_set_row_staging) */
 } mk_tuning;

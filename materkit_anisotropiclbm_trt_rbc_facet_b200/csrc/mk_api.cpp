@@ -403,7 +403,8 @@ mk_status mk_set_tuning(mk_handle* h, const mk_tuning* t) {
   if ((t->fused != 0 && t->fused != 1) || (t->row_staged != 0 && t->row_staged != 1))
     return bad("fused and row_staged are 0 or 1");
   if (t->fused && t->row_staged) return bad("at most one of fused and row_staged");
-  if (t->minb != 1 && t->minb != 2) return bad("minb must be 1 or 2");
+  const int mb_max = e.p.model == MK_MODEL_MULTIPHASE ? 5 : 2;
+  if (t->minb < 1 || t->minb > mb_max) return bad("minb must be 1 or 2 (multiphase: 1 to 5)");
   if (t->fused && !e.wave_ok) return bad("this case does not admit the fused multiphase loop");
   if (t->row_staged && !e.rows_ok) return bad("this case does not admit the row-staged collision");
   if (t->fused && e.slab) return slab_refuse(h, "mk_set_tuning (fused)");

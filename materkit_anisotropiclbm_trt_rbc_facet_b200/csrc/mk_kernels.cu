@@ -1500,7 +1500,7 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
       break;
     case MK_MODEL_MULTIPHASE:
       mke::mp_launch(e, parity, grid, block, ev);
-      e.launches += (e.wave && e.wave_ok) ? 1 : 2;
+      e.launches += engine_kernels_per_step(e);
       break;
     case MK_MODEL_MULTIGRAIN:
       launch_mg<S>(e, parity, grid, block, ev);
@@ -2047,9 +2047,42 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   cudaEventCreate(&t1);
   // 64-, 128- and 256-thread blocks, a warp-multiple row along x
   const int shapes[9][2] = {{32, 2}, {64, 1}, {32, 4}, {64, 2}, {128, 1}, {32, 8}, {64, 4}, {128, 2}, {256, 1}};
-  const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 2 : 1;
+  // occupancy variants: 1, 2 (256-thread launch bounds), and for the
+  // multiphase collision 3, 4, 5 (registers capped at 112, 96, 80)
+  const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 5 : 1;
   double best = 1e300;
   int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0, brows = 0;
+  // time the configuration now in e (warm-up of both AA parities, then the
+  // faster of two timed repeats: one slow repeat must not decide), restore
+  // the state and keep the configuration if it is the fastest so far
+  auto trial = [&]() {
+    engine_step(e, nullptr);
+    engine_step(e, nullptr);
+    float ms = 1e30f;
+    for (int rep = 0; rep < 2 && st == cudaSuccess; ++rep) {
+      cudaEventRecord(t0, e.stream);
+      for (int s = 0; s < trial_steps; ++s) engine_step(e, nullptr);
+      cudaEventRecord(t1, e.stream);
+      st = cudaEventSynchronize(t1);
+      if (st == cudaSuccess) st = cudaGetLastError();
+      float m = 0;
+      if (st == cudaSuccess) cudaEventElapsedTime(&m, t0, t1);
+      ms = std::min(ms, m);
+    }
+    ++ncand;
+    if (st == cudaSuccess && ms / trial_steps < best) {
+      best = ms / trial_steps;
+      bbx = e.block_x;
+      bby = e.block_y;
+      bmb = e.minb;
+      bwave = e.wave;
+      brows = e.rows;
+    }
+    e.step = step0;
+    e.phi_cur = cur0;
+    e.launches = l0;
+    if (st == cudaSuccess) st = copy(false);
+  };
   // candidate -1: the fused multiphase loop (its tiling is fixed by the case);
   // candidate -2: the row-staged collision (the block shape is the phi kernel's)
   for (int si = -2; si < 9 && st == cudaSuccess; ++si) {
@@ -2061,34 +2094,8 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
       e.rows = si == -2 ? 1 : 0;
       e.block_x = bx;
       e.block_y = si < 0 ? by0 : shapes[si][1];
-      e.minb = (nmb == 2 && si >= 0) ? mb : mb0;
-      engine_step(e, nullptr);  // warm-up of this shape, both AA parities
-      engine_step(e, nullptr);
-      // the faster of two timed repeats (one slow repeat must not decide)
-      float ms = 1e30f;
-      for (int rep = 0; rep < 2 && st == cudaSuccess; ++rep) {
-        cudaEventRecord(t0, e.stream);
-        for (int s = 0; s < trial_steps; ++s) engine_step(e, nullptr);
-        cudaEventRecord(t1, e.stream);
-        st = cudaEventSynchronize(t1);
-        if (st == cudaSuccess) st = cudaGetLastError();
-        float m = 0;
-        if (st == cudaSuccess) cudaEventElapsedTime(&m, t0, t1);
-        ms = std::min(ms, m);
-      }
-      ++ncand;
-      if (st == cudaSuccess && ms / trial_steps < best) {
-        best = ms / trial_steps;
-        bbx = e.block_x;
-        bby = e.block_y;
-        bmb = e.minb;
-        bwave = e.wave;
-        brows = e.rows;
-      }
-      e.step = step0;
-      e.phi_cur = cur0;
-      e.launches = l0;
-      if (st == cudaSuccess) st = copy(false);
+      e.minb = (nmb > 1 && si >= 0) ? mb : mb0;
+      trial();
     }
   }
   cudaEventDestroy(t0);

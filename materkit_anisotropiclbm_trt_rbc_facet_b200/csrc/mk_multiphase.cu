@@ -16,15 +16,17 @@ using namespace mks;
 
 namespace {
 
+// The planes z_lo .. z_lo + gridDim.z - 1.
 template <class S, class P, int PARITY>
 __global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const float* __restrict__ H0,
-                                                P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h) {
+                                                P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h,
+                                                const int z_lo) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   // planes in descending order: the collision kernel that follows walks them
   // ascending, so it starts on the planes whose h this kernel read last
   // (still in L2), and it ends where the next loop's phi kernel starts
-  const int z = g.nz - 1 - (int)blockIdx.z;
+  const int z = z_lo + (int)(gridDim.z - 1 - blockIdx.z);
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   if (fast_cell(g, x, y, z)) {
     const Fast fa = make_fast(g, x, y, z);
@@ -218,16 +220,15 @@ __device__ __forceinline__ void mp_collide_cell(S* __restrict__ G, S* __restrict
   }
 }
 
-// MINB is the occupancy hint (resident 256-thread blocks per SM): 1 keeps
-// every value in registers, 2 doubles the warps per SM at the price of a few
-// spills; the autotuner picks.  Interior rows take the Fast addressing.
-template <class S, class P, int PARITY, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
-                                                          float* __restrict__ H0, const P* __restrict__ phi,
-                                                          const Geom g, const MpK<typename Stor<S>::T> k) {
+// One fluid cell of the thread-per-cell collision (planes z_lo ..
+// z_lo + gridDim.z - 1).  Interior rows take the Fast addressing.
+template <class S, class P, int PARITY>
+__device__ __forceinline__ void mp_collide_thread(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                                  const P* __restrict__ phi, const Geom& g,
+                                                  const MpK<typename Stor<S>::T>& k, int z_lo) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
+  const int z = z_lo + (int)blockIdx.z;
   if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   if (fast_cell(g, x, y, z)) {
     const Fast fa = make_fast(g, x, y, z);
@@ -239,6 +240,25 @@ __global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* 
     mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Nbr>{phi, nb, c}, g.stride, nb, c, k,
                                   GlobalLd<S, PARITY, Nbr>{G, H, H0, g.stride, nb, c});
   }
+}
+
+// Occupancy variants of the collision: MINB 1 or 2 resident 256-thread blocks
+// per SM (1 keeps every value in registers, 2 doubles the warps per SM at the
+// price of a few spills); k_mp_collide_r caps the registers at R (with
+// 64-thread blocks 112 gives 18 warps per SM, 96 gives 20, 80 gives 24).
+// The autotuner picks (minb 3, 4, 5 select R = 112, 96, 80).
+template <class S, class P, int PARITY, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mp_collide(S* __restrict__ G, S* __restrict__ H,
+                                                          float* __restrict__ H0, const P* __restrict__ phi,
+                                                          const Geom g, const MpK<typename Stor<S>::T> k,
+                                                          const int z_lo) {
+  mp_collide_thread<S, P, PARITY>(G, H, H0, phi, g, k, z_lo);
+}
+template <class S, class P, int PARITY, int R>
+__global__ void __maxnreg__(R) k_mp_collide_r(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0,
+                                              const P* __restrict__ phi, const Geom g,
+                                              const MpK<typename Stor<S>::T> k, const int z_lo) {
+  mp_collide_thread<S, P, PARITY>(G, H, H0, phi, g, k, z_lo);
 }
 
 // ------------------------------------------- row-staged collision (rows)
@@ -818,28 +838,74 @@ void launch_mp_wave(mke::Engine& e, int parity, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[1], e.stream);
 }
 
+// The phi kernel over planes z_lo .. z_lo + nzr - 1 on `st`.
+template <class S>
+void launch_phi_range(mke::Engine& e, int parity, dim3 grid, dim3 block, int z_lo, int nzr, cudaStream_t st) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  if (nzr <= 0) return;
+  const Geom g = make_geom(e);
+  const Refs r = refs_of(e.p);
+  grid.z = nzr;
+  S* H = (S*)e.pop1;
+  P* phi = (P*)e.phi[0];
+  if (parity == 0)
+    k_mp_phi<S, P, 0><<<grid, block, 0, st>>>(H, e.rest1, phi, g, T(r.r1), z_lo);
+  else
+    k_mp_phi<S, P, 1><<<grid, block, 0, st>>>(H, e.rest1, phi, g, T(r.r1), z_lo);
+}
+
+// The thread-per-cell collision over planes z_lo .. z_lo + nzr - 1 on `st`,
+// in the occupancy variant e.minb.
+template <class S>
+void launch_collide_range(mke::Engine& e, int parity, dim3 grid, dim3 block, int z_lo, int nzr, cudaStream_t st) {
+  typedef typename Stor<S>::T T;
+  typedef typename PhiOf<S>::type P;
+  if (nzr <= 0) return;
+  const Geom g = make_geom(e);
+  const MpK<T> k = mp_coef<T>(e.p, refs_of(e.p));
+  grid.z = nzr;
+  S* G = (S*)e.pop0;
+  S* H = (S*)e.pop1;
+  const P* phi = (const P*)e.phi[0];
+  if (e.minb == 1) {
+    if (parity == 0)
+      k_mp_collide<S, P, 0, 1><<<grid, block, 0, st>>>(G, H, e.rest1, phi, g, k, z_lo);
+    else
+      k_mp_collide<S, P, 1, 1><<<grid, block, 0, st>>>(G, H, e.rest1, phi, g, k, z_lo);
+  } else if (e.minb >= 3 && e.minb <= 5) {
+    // register-capped variants
+    auto go = [&](auto rr) {
+      constexpr int R = decltype(rr)::value;
+      if (parity == 0)
+        k_mp_collide_r<S, P, 0, R><<<grid, block, 0, st>>>(G, H, e.rest1, phi, g, k, z_lo);
+      else
+        k_mp_collide_r<S, P, 1, R><<<grid, block, 0, st>>>(G, H, e.rest1, phi, g, k, z_lo);
+    };
+    if (e.minb == 3)
+      go(std::integral_constant<int, 112>{});
+    else if (e.minb == 4)
+      go(std::integral_constant<int, 96>{});
+    else
+      go(std::integral_constant<int, 80>{});
+  } else {
+    if (parity == 0)
+      k_mp_collide<S, P, 0, 2><<<grid, block, 0, st>>>(G, H, e.rest1, phi, g, k, z_lo);
+    else
+      k_mp_collide<S, P, 1, 2><<<grid, block, 0, st>>>(G, H, e.rest1, phi, g, k, z_lo);
+  }
+}
+
 // parts: bit 0 the phi kernel, bit 1 the collision (3: the whole loop)
 template <class S>
 void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev, int parts = 3) {
   typedef typename Stor<S>::T T;
-  typedef typename PhiOf<S>::type P;
   if (parts == 3 && e.wave && e.wave_ok) {
     launch_mp_wave<S>(e, parity, ev);
     return;
   }
-  const Geom g = make_geom(e);
-  const Refs r = refs_of(e.p);
-  const MpK<T> k = mp_coef<T>(e.p, r);
-  S* G = (S*)e.pop0;
-  S* H = (S*)e.pop1;
-  P* phi = (P*)e.phi[0];
   if (ev) cudaEventRecord(ev[0], e.stream);
-  if (parts & 1) {
-    if (parity == 0)
-      k_mp_phi<S, P, 0><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
-    else
-      k_mp_phi<S, P, 1><<<grid, block, 0, e.stream>>>(H, e.rest1, phi, g, T(r.r1));
-  }
+  if (parts & 1) launch_phi_range<S>(e, parity, grid, block, 0, e.nz, e.stream);
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
@@ -849,17 +915,10 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
     return;
   }
   if (e.rows && e.rows_ok) {
-    launch_mp_rows<S>(e, parity, g, k);
-  } else if (e.minb == 1) {
-    if (parity == 0)
-      k_mp_collide<S, P, 0, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
-    else
-      k_mp_collide<S, P, 1, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
+    const Geom g = make_geom(e);
+    launch_mp_rows<S>(e, parity, g, mp_coef<T>(e.p, refs_of(e.p)));
   } else {
-    if (parity == 0)
-      k_mp_collide<S, P, 0, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
-    else
-      k_mp_collide<S, P, 1, 2><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k);
+    launch_collide_range<S>(e, parity, grid, block, 0, e.nz, e.stream);
   }
   if (ev) cudaEventRecord(ev[3], e.stream);
 }

@@ -1520,3 +1520,249 @@ extern "C" int orc_backward(orc_state* s, const double* target, int64_t steps, d
   out[3] = -om_t * om_t * omtb;
   return 0;
 }
+
+// ===================================================== reference-structure
+// The same method with the reference's data structure: every field of a node
+// in one object, mirroring the member list of mkNode (MaterKit/inc/mkNode.h:
+// 128-215: the f / g / h / x population vectors of 19 values each, the
+// equilibrium and neighbour vectors, velocity, density, phase and temperature
+// fields, the multigrain and solute vectors), an array of those objects, and
+// node sweeps `omp parallel for schedule(static, 16)` (MK_OMP_CHUNKSIZE,
+// MaterKit/src/mkFluidsUser.cpp:70).  Used as the CPU baseline closest to the
+// reference's own memory traffic (its solver bodies are in the closed DLL);
+// for the flow model and the thermal dendrite it reproduces orc_advance bit
+// for bit (the same per-cell arithmetic, in the same order).
+namespace {
+
+struct AosNode {
+  double f_out[19], f_hlp[19], f_equ[19];
+  double vel[3], vel_old[3];
+  double density, omega_f;
+  double g_out[19], g_hlp[19], g_nbr[19];
+  double phi, phi_old, d_phi;
+  std::vector<double> gVec_out, gVec_hlp, gVec_nbr;  // multigrain lattices (empty here)
+  std::vector<double> phiVec, phiVec_old, d_phiVec;
+  double N_v[3], D_p, A2s, phi_n[3], normal[3];
+  double h_out[19], h_hlp[19];
+  double temperature;
+  double index_nb[19];
+  double x_out[19], x_hlp[19];
+  std::vector<double> X_potents, X_solutes, X_DCs;  // solute vectors (empty here)
+  double ptl_mp, prs_mp, rho_mp, eta, k_d;
+  int flag, grain_id;
+};
+
+constexpr int kChunk = 16;
+
+}  // namespace
+
+struct orc_aos {
+  orc_state geo;  // parameters, flags, grains and rotations only
+  std::vector<AosNode> node;
+};
+
+namespace {
+
+// The streaming of mkFluidsUser.cpp:77-97 on one population vector member.
+template <double (AosNode::*OUT)[19], double (AosNode::*HLP)[19]>
+void aos_propagate(orc_aos* a, int Q) {
+  const orc_state* s = &a->geo;
+  const int64_t n = s->n;
+  AosNode* nd = a->node.data();
+#pragma omp parallel for schedule(static, kChunk)
+  for (int64_t c = 0; c < n; ++c) {
+    if (nd[c].flag != MK_FLAG_FLUID) continue;
+    const int x = (int)(c % s->nx), y = (int)((c / s->nx) % s->ny), z = (int)(c / ((int64_t)s->nx * s->ny));
+    for (int i = 0; i < Q; ++i) {
+      const int64_t src = nbr(s, x, y, z, -E27[i][0], -E27[i][1], -E27[i][2]);
+      (nd[c].*HLP)[i] = src >= 0 ? (nd[src].*OUT)[i] : (nd[c].*OUT)[inv_dir(i)];
+    }
+  }
+}
+
+// grad_lap on the nodes' phi (the same sums as grad_lap, in the same order).
+void aos_grad_lap(const orc_aos* a, int x, int y, int z, double g[3], double* lap) {
+  const orc_state* s = &a->geo;
+  const AosNode* nd = a->node.data();
+  const double f0 = nd[cidx(s, x, y, z)].phi;
+  g[0] = g[1] = g[2] = 0;
+  double l = 0;
+  for (int i = 1; i < 19; ++i) {
+    const int64_t j = nbr(s, x, y, z, E27[i][0], E27[i][1], E27[i][2]);
+    const double fn = j >= 0 ? nd[j].phi : f0;
+    const double w = weight(19, i);
+    g[0] += w * E27[i][0] * fn;
+    g[1] += w * E27[i][1] * fn;
+    g[2] += w * E27[i][2] * fn;
+    l += w * (fn - f0);
+  }
+  g[0] *= 3.0;
+  g[1] *= 3.0;
+  g[2] *= 3.0;
+  *lap = 6.0 * l;
+}
+
+void aos_flow_step(orc_aos* a) {
+  const orc_state* s = &a->geo;
+  const int Q = s->Qf;
+  aos_propagate<&AosNode::f_out, &AosNode::f_hlp>(a, Q);
+  double F[3];
+  flow_force(s, F);
+  const double tau = s->p.tau, om = 1.0 / tau;
+  const double om_m = 1.0 / (0.5 + s->p.magic / (tau - 0.5));
+  const int coll = s->p.collision;
+  AosNode* nd = a->node.data();
+#pragma omp parallel for schedule(static, kChunk)
+  for (int64_t c = 0; c < s->n; ++c) {
+    AosNode& q = nd[c];
+    if (q.flag != MK_FLAG_FLUID) continue;
+    double f[27], u[3];
+    for (int i = 0; i < Q; ++i) f[i] = q.f_hlp[i];
+    flow_collide(Q, coll, om, om_m, f, F, u);
+    for (int i = 0; i < Q; ++i) q.f_out[i] = f[i];
+    double rho = 0;
+    for (int i = 0; i < Q; ++i) rho += q.f_hlp[i];
+    q.density = rho;
+    for (int k = 0; k < 3; ++k) {
+      q.vel_old[k] = q.vel[k];
+      q.vel[k] = u[k];
+    }
+  }
+}
+
+void aos_thermal_dendrite_step(orc_aos* a) {
+  const orc_state* s = &a->geo;
+  const mk_params& p = s->p;
+  AosNode* nd = a->node.data();
+  aos_propagate<&AosNode::g_out, &AosNode::g_hlp>(a, 7);
+#pragma omp parallel for schedule(static, kChunk)
+  for (int64_t c = 0; c < s->n; ++c) {
+    AosNode& q = nd[c];
+    q.phi_old = q.phi;
+    if (q.flag != MK_FLAG_FLUID) continue;
+    double ph = 0;
+    for (int i = 0; i < 7; ++i) ph += q.g_hlp[i];
+    q.phi = ph;
+  }
+  const double D0 = p.W0 * p.W0 / p.tau0;
+  const double om_g = 1.0 / (4.0 * D0 + 0.5);
+  const double cs2 = 0.25;
+#pragma omp parallel for schedule(static, kChunk)
+  for (int64_t c = 0; c < s->n; ++c) {
+    AosNode& q = nd[c];
+    if (q.flag != MK_FLAG_FLUID) continue;
+    const int x = (int)(c % s->nx), y = (int)((c / s->nx) % s->ny), z = (int)(c / ((int64_t)s->nx * s->ny));
+    double gr[3], lap;
+    aos_grad_lap(a, x, y, z, gr, &lap);
+    double an, N[3];
+    anisotropy(&s->rot[9 * q.grain_id], p.aniso, p.eps4, p.eps2, gr, &an, N);
+    const double ph = q.phi;
+    const double dphi = ph - q.phi_old;
+    const double one_m = 1.0 - ph * ph;
+    const double src = (ph - ph * ph * ph - p.lambda * q.temperature * one_m * one_m) / p.tau0 + (1.0 - an * an) * dphi;
+    double B[3];
+    for (int k = 0; k < 3; ++k) B[k] = -cs2 * ((an * an - 1.0) * gr[k] + N[k]);
+    for (int k = 0; k < 3; ++k) {
+      q.phi_n[k] = gr[k];
+      q.normal[k] = N[k];
+    }
+    q.d_phi = dphi;
+    for (int i = 0; i < 7; ++i) {
+      const double w = weight(7, i);
+      const double eB = E27[i][0] * B[0] + E27[i][1] * B[1] + E27[i][2] * B[2];
+      const double gi = q.g_hlp[i];
+      q.g_out[i] = gi - om_g * (gi - w * ph) + (1.0 - 0.5 * om_g) * w * eB / cs2 + w * src;
+    }
+  }
+  aos_propagate<&AosNode::h_out, &AosNode::h_hlp>(a, 7);
+  const double om_t = 1.0 / (4.0 * p.D + 0.5);
+#pragma omp parallel for schedule(static, kChunk)
+  for (int64_t c = 0; c < s->n; ++c) {
+    AosNode& q = nd[c];
+    if (q.flag != MK_FLAG_FLUID) continue;
+    double T = 0;
+    for (int i = 0; i < 7; ++i) T += q.h_hlp[i];
+    const double lat = 0.5 * (q.phi - q.phi_old);
+    for (int i = 0; i < 7; ++i) {
+      const double w = weight(7, i);
+      const double ti = q.h_hlp[i];
+      q.h_out[i] = ti - om_t * (ti - w * T * (1.0 + 4.0 * 0.0)) + w * lat;
+    }
+    q.temperature = T;
+  }
+}
+
+}  // namespace
+
+extern "C" size_t orc_aos_node_bytes(void) { return sizeof(AosNode); }
+
+extern "C" orc_aos* orc_aos_create(const orc_state* s) {
+  const int m = s->p.model;
+  if (!((m == MK_MODEL_FLOW && s->Qf == 19 && s->p.wall_axis < 0) || m == MK_MODEL_THERMAL_DENDRITE)) return nullptr;
+  orc_aos* a = new orc_aos();
+  a->geo.p = s->p;
+  a->geo.nx = s->nx;
+  a->geo.ny = s->ny;
+  a->geo.nz = s->nz;
+  a->geo.n = s->n;
+  a->geo.step = s->step;
+  a->geo.Qf = s->Qf;
+  a->geo.Qs = s->Qs;
+  a->geo.flag = s->flag;
+  a->geo.grain = s->grain;
+  a->geo.rot = s->rot;
+  const int64_t n = s->n;
+  a->node.resize((size_t)n);
+  for (int64_t c = 0; c < n; ++c) {
+    AosNode& q = a->node[(size_t)c];  // value-initialised: every number starts at 0
+    q.flag = s->flag[c];
+    q.grain_id = s->grain.empty() ? 0 : s->grain[c];
+    if (m == MK_MODEL_FLOW) {
+      for (int i = 0; i < s->Qf; ++i) q.f_out[i] = s->f_out[(int64_t)i * n + c];
+    } else {
+      for (int i = 0; i < 7; ++i) {
+        q.g_out[i] = s->f_out[(int64_t)i * n + c];
+        q.h_out[i] = s->s_out[(int64_t)i * n + c];
+      }
+      q.phi = s->phi[c];
+      q.phi_old = s->phi_prev[c];
+      q.temperature = s->temp[c];
+    }
+  }
+  return a;
+}
+
+extern "C" void orc_aos_destroy(orc_aos* a) { delete a; }
+
+extern "C" void orc_aos_advance(orc_aos* a, int64_t nsteps) {
+  for (int64_t t = 0; t < nsteps; ++t) {
+    if (a->geo.p.model == MK_MODEL_FLOW)
+      aos_flow_step(a);
+    else
+      aos_thermal_dendrite_step(a);
+    a->geo.step += 1;
+  }
+}
+
+// Post-collision populations in the layout of orc_get_populations ([q][cell];
+// which 0: the flow lattice or the phase-field lattice, 1: the thermal one),
+// or the phase field / temperature (field MK_FIELD_PHI / MK_FIELD_T).
+extern "C" int orc_aos_get_populations(const orc_aos* a, int which, double* out) {
+  const int64_t n = a->geo.n;
+  const bool flow = a->geo.p.model == MK_MODEL_FLOW;
+  if (which < 0 || which > 1 || (flow && which == 1)) return -1;
+  const int Q = flow ? a->geo.Qf : 7;
+  for (int64_t c = 0; c < n; ++c) {
+    const AosNode& q = a->node[(size_t)c];
+    const double* v = flow ? q.f_out : (which == 0 ? q.g_out : q.h_out);
+    for (int i = 0; i < Q; ++i) out[(int64_t)i * n + c] = v[i];
+  }
+  return 0;
+}
+
+extern "C" int orc_aos_get_field(const orc_aos* a, int field, double* out) {
+  if (field != MK_FIELD_PHI && field != MK_FIELD_T) return -1;
+  for (int64_t c = 0; c < a->geo.n; ++c)
+    out[c] = field == MK_FIELD_PHI ? a->node[(size_t)c].phi : a->node[(size_t)c].temperature;
+  return 0;
+}

@@ -130,6 +130,18 @@ int orc_backward(orc_state* s, const double* target, int64_t steps, double* out)
 void orc_anisotropy(int kind, double e4, double e2, const double* n, double* a, double* g);
 int orc_get_threads(void);
 
+// Reference-structure variant (the reference's node-object layout and its
+// schedule(static, 16) sweeps) of the flow model (D3Q19, no moving plates)
+// and the thermal dendrite, created from an oracle state and bit-identical
+// to orc_advance; NULL for other models.
+typedef struct orc_aos orc_aos;
+orc_aos* orc_aos_create(const orc_state* s);
+void orc_aos_destroy(orc_aos* a);
+void orc_aos_advance(orc_aos* a, int64_t nsteps);
+int orc_aos_get_populations(const orc_aos* a, int which, double* out);
+int orc_aos_get_field(const orc_aos* a, int field, double* out);
+size_t orc_aos_node_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,15 @@ def load() -> C.CDLL:
         lib.orc_anisotropy.argtypes = [C.c_int, C.c_double, C.c_double, D, D, D]
         lib.orc_backward.restype = C.c_int
         lib.orc_backward.argtypes = [C.c_void_p, D, C.c_int64, D]
+        lib.orc_aos_create.restype = C.c_void_p
+        lib.orc_aos_create.argtypes = [C.c_void_p]
+        lib.orc_aos_destroy.argtypes = [C.c_void_p]
+        lib.orc_aos_advance.argtypes = [C.c_void_p, C.c_int64]
+        lib.orc_aos_get_populations.restype = C.c_int
+        lib.orc_aos_get_populations.argtypes = [C.c_void_p, C.c_int, D]
+        lib.orc_aos_get_field.restype = C.c_int
+        lib.orc_aos_get_field.argtypes = [C.c_void_p, C.c_int, D]
+        lib.orc_aos_node_bytes.restype = C.c_size_t
         _lib = lib
     return _lib
 
@@ -138,9 +147,66 @@ class Oracle:
             raise KeyError(j)
         return out.reshape(p.nz, p.ny, p.nx)
 
+    def populations(self, which: int = 0) -> np.ndarray:
+        """Post-collision populations of lattice `which`, (Q, ncell)."""
+        p = self.params
+        q = {0: p.lattice if p.model in (0, 4) else 7}.get(which, 7)
+        out = np.empty(q * p.ncell(), dtype=np.float64)
+        if self.lib.orc_get_populations(self.h, int(which), _ptr(out)) != 0:
+            raise KeyError(which)
+        return out.reshape(q, p.ncell())
+
     def close(self):
         if self.h:
             self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ReferenceStructure:
+    """The oracle's method in the reference's data structure: one object per
+    node with every field of mkNode (MaterKit/inc/mkNode.h:128-215), node
+    sweeps with schedule(static, 16) (MaterKit/src/mkFluidsUser.cpp:70).
+    Started from an oracle state; the flow model (D3Q19) and the thermal
+    dendrite; bit-identical to the oracle.  The CPU baseline of that layout."""
+
+    def __init__(self, oracle: Oracle):
+        self.lib = load()
+        self.params = oracle.params
+        self.h = self.lib.orc_aos_create(oracle.h)
+        if not self.h:
+            raise ValueError("the reference-structure variant covers the flow model (D3Q19) and the thermal dendrite")
+
+    @staticmethod
+    def node_bytes() -> int:
+        return int(load().orc_aos_node_bytes())
+
+    def advance(self, n: int) -> None:
+        self.lib.orc_aos_advance(self.h, int(n))
+
+    def populations(self, which: int = 0) -> np.ndarray:
+        p = self.params
+        q = p.lattice if p.model == 0 else 7
+        out = np.empty(q * p.ncell(), dtype=np.float64)
+        if self.lib.orc_aos_get_populations(self.h, int(which), _ptr(out)) != 0:
+            raise KeyError(which)
+        return out.reshape(q, p.ncell())
+
+    def field(self, name: str) -> np.ndarray:
+        p = self.params
+        out = np.empty(p.ncell(), dtype=np.float64)
+        if self.lib.orc_aos_get_field(self.h, K.FIELD[name], _ptr(out)) != 0:
+            raise KeyError(name)
+        return out.reshape(p.nz, p.ny, p.nx)
+
+    def close(self):
+        if self.h:
+            self.lib.orc_aos_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -176,7 +176,8 @@ def test_autotune_keeps_state(casedir, prec):
     a.advance(3)
     b.advance(3)
     r = a.autotune(2)
-    assert r["ms_per_step"] > 0 and r["minb"] in (1, 2)
+    # minb: 1, 2 or the register-capped 3-5; 0 for a fused or row-staged choice
+    assert r["ms_per_step"] > 0 and r["minb"] in (0, 1, 2, 3, 4, 5)
     assert a.step == 3
     a.advance(6, graph=True)
     b.advance(6)

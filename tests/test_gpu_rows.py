@@ -123,7 +123,7 @@ def test_tuning_roundtrip_and_checks(casedir):
     assert set(t) == {"block_x", "block_y", "minb", "fused", "row_staged"}
     s.tuning = {"block_x": 32, "block_y": 4, "minb": 1, "row_staged": 1}
     assert s.tuning == dict(t, block_x=32, block_y=4, minb=1, row_staged=1)
-    for bad in ({"block_x": 48}, {"block_x": 64, "block_y": 32}, {"minb": 3}, {"row_staged": 2}):
+    for bad in ({"block_x": 48}, {"block_x": 64, "block_y": 32}, {"minb": 6}, {"minb": 0}, {"row_staged": 2}):
         with pytest.raises(A.MkError) as e:
             s.tuning = bad
         assert e.value.status == A.MK_ERR_ARG, bad
@@ -139,3 +139,23 @@ def test_tuning_roundtrip_and_checks(casedir):
     s2.advance(4)
     ref.advance(4)
     assert np.array_equal(s2.field("phi"), ref.field("phi"))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "bf16"])
+@pytest.mark.parametrize("minb", [1, 3, 4, 5])
+def test_occupancy_variants_agree(casedir, prec, minb):
+    # the register-capped variants (minb 3, 4, 5: 112, 96, 80 registers) run
+    # the same source as the 256-thread launch-bound ones
+    p = case_params(_case(casedir, "walls_x_closed_z", prec))
+    a, b = Solver(params=p), Solver(params=p)
+    a.tuning = {"block_x": 64, "block_y": 1, "minb": minb}
+    b.tuning = {"block_x": 64, "block_y": 1, "minb": 2}
+    for n in (1, 1, 5):
+        a.advance(n)
+        b.advance(n)
+    for f in FIELDS:
+        x, y = a.field(f), b.field(f)
+        if prec == "fp64":
+            assert float(np.max(np.abs(x - y))) <= 1e-13 * max(float(np.max(np.abs(y))), 1e-30), f
+        else:
+            assert np.array_equal(x, y), (prec, minb, f)
