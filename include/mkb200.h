@@ -489,6 +489,33 @@ const char* mk_noalloc_last_error(void);
  * solid_frac, max_speed, n_bad}.  NULL stops the log.  Process-wide. */
 mk_status mk_set_metrics_log(const char* path);
 
+/* ---- A dendrite growing in a two-phase flow ------------------------------
+ * run_flow_multiphase_dendrite (MaterKit/MaterKit.cpp:377-397) couples two
+ * solver objects per loop: the dendrite's phase field, its thermal lattice
+ * advected by the flow (update_velocity, mkThermalField.h:36), then the
+ * multiphase flow with the dendrite's solid as geometry (update_geometry,
+ * mkFluidsMultiphase.h:37).  Here the two objects are two handles of the same
+ * grid on the same device, and a loop is
+ *   mk_update_velocity(dendrite, flow); mk_advance(dendrite, 1);
+ *   mk_update_geometry(flow, dendrite); mk_advance(flow, 1);
+ * (the reference's bodies are in its closed DLL; these are the semantics
+ * defined here). */
+
+/* The multiphase flow's cells where the dendrite's phase field is positive
+ * become solid (cumulative: a solid cell stays solid): a solid cell is not
+ * updated, links into it bounce back (half-way), and the Allen-Cahn stencil
+ * sees the wetting value there, as at a wall.  The change takes effect at the
+ * flow's next even loop count, where the in-place streaming holds every
+ * population in its own cell (the liquid of a cell that solidifies leaves the
+ * flow).  The fused and row-staged forms are turned off for the flow.
+ * MK_ERR_ARG unless flow is a multiphase and dendrite a thermal or solutal
+ * dendrite handle of the same grid and device (no slab handles). */
+mk_status mk_update_geometry(mk_handle* flow, mk_handle* dendrite);
+/* The dendrite's scalar lattice is advected by the flow's current velocity
+ * (its equilibrium w T (1 + 4 e.u), as in the flow + dendrite models); the
+ * phase field is not.  Synchronous.  MK_ERR_ARG as for mk_update_geometry. */
+mk_status mk_update_velocity(mk_handle* dendrite, mk_handle* flow);
+
 /* ---- z-slab decomposition of one multiphase domain ----------------------
  * No counterpart in the reference: its solver runs one domain in one process,
  * its cell sweeps shared out by OpenMP (mkFluidsUser.cpp:70, 116, 147).  Here

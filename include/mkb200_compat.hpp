@@ -145,6 +145,13 @@ class mkFluidsMRT : public mkSolver {
   // mkPhaseField::relaxation_anisotropy_solute(loops), mkSolutalField::propagate /
   // relaxation / bdy_LBflowin (MaterKit.cpp:665-674, 448-456)
   void relaxation_anisotropy_solute(int /*loops*/) { call("pf_relax_solute", seq()); }
+  // run_flow_multiphase_dendrite (MaterKit.cpp:377-397): the dendrite's
+  // calls that take the two-phase flow.  update_velocity copies the flow's
+  // velocity for the thermal relaxation (mkThermalField::update_velocity,
+  // mkThermalField.h:36); the phase field does not read the flow.
+  void relaxation_anisotropy_thermal(mkSolver& /*flow*/) { relaxation_anisotropy_thermal(); }
+  void update_velocity(mkSolver& flow) { check(mk_update_velocity(h_, flow.handle()), h_); }
+  void thermal_relaxation(mkSolver& /*flow*/) { thermal_relaxation(); }
   void solutal_propagate() { call("c_propagate", seq()); }
   void solutal_relaxation() { call("c_relax", seq()); }
   void bdy_LBflowin() { call("bdy_LBflowin", seq()); }
@@ -174,6 +181,9 @@ class mkFluidsMultiphase : public mkSolver {
   explicit mkFluidsMultiphase(const mkSpace& s) : mkSolver(s, MK_MODEL_MULTIPHASE) {}
   void propagate() { call("propagate", {"propagate", "relaxation"}); }
   void relaxation() { call("relaxation", {"propagate", "relaxation"}); }
+  // The dendrite's solid (phi > 0) becomes this flow's geometry from its next
+  // even loop count (mkFluidsMultiphase::update_geometry, mkFluidsMultiphase.h:37).
+  void update_geometry(mkSolver& dendrite) { check(mk_update_geometry(h_, dendrite.handle()), h_); }
 };
 
 }  // namespace mkb200

@@ -152,6 +152,8 @@ PROTOTYPES = {
     "mk_set_fused": (C.c_int, [H, C.c_int32]),
     "mk_get_fused": (C.c_int32, [H]),
     "mk_set_row_staging": (C.c_int, [H, C.c_int32]),
+    "mk_update_geometry": (C.c_int, [H, H]),
+    "mk_update_velocity": (C.c_int, [H, H]),
     "mk_get_tuning": (C.c_int, [H, P(MkTuning)]),
     "mk_set_tuning": (C.c_int, [H, P(MkTuning)]),
     "mk_get_row_staging": (C.c_int32, [H]),

@@ -266,6 +266,16 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
     if (s != MK_OK) return s;
     --left;
   }
+  if (left > 0 && e.mpending_set) {
+    // dynamic solids change at an even loop count: reach one eagerly
+    if (e.step & 1) {
+      const mk_status s = mk_advance(h, 1);
+      if (s != MK_OK) return s;
+      --left;
+    }
+    cudaError_t st = mke::mp_apply_solids(e);
+    if (st != cudaSuccess) return cuda_fail(h, st, "dynamic solids");
+  }
   while (left >= 2) {
     const int par = (int)(e.step & 1);
     for (int attempt = 0; !h->graph[par]; ++attempt) {
@@ -274,8 +284,10 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
       cudaGraph_t g = nullptr;
       cudaError_t st = cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal);
       if (st != cudaSuccess) return cuda_fail(h, st, "capture begin");
+      e.capturing = 1;
       mke::engine_step(e, nullptr);
       mke::engine_step(e, nullptr);
+      e.capturing = 0;
       st = cudaStreamEndCapture(e.stream, &g);
       e.step = step0;
       e.launches = l0;
@@ -379,6 +391,58 @@ mk_status mk_set_row_staging(mk_handle* h, int32_t on) {
 }
 
 int32_t mk_get_row_staging(const mk_handle* h) { return h && h->e.rows_ok && h->e.rows ? 1 : 0; }
+
+namespace {
+
+bool couple_ok(const mke::Engine& f, const mke::Engine& d) {
+  const int dm = d.p.model;
+  return f.p.model == MK_MODEL_MULTIPHASE && (dm == MK_MODEL_THERMAL_DENDRITE || dm == MK_MODEL_SOLUTAL_DENDRITE) &&
+         f.nx == d.nx && f.ny == d.ny && f.nz == d.nz && f.device == d.device && !f.slab && !d.slab;
+}
+
+void drop_graphs(mk_handle* h) {
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+}  // namespace
+
+mk_status mk_update_geometry(mk_handle* flow, mk_handle* dendrite) {
+  const Range nvtx_range("mk_update_geometry");
+  if (!flow || !dendrite) return MK_ERR_ARG;
+  if (!couple_ok(flow->e, dendrite->e)) {
+    flow->err = "update_geometry: a multiphase handle and a thermal or solutal dendrite handle of one grid and device";
+    return MK_ERR_ARG;
+  }
+  mke::Engine& f = flow->e;
+  const bool fresh = !f.msolid;
+  // the dendrite's current phi, ordered before the flow's next work
+  cudaError_t st = cudaStreamSynchronize(dendrite->e.stream);
+  if (st != cudaSuccess) return cuda_fail(dendrite, st, "update_geometry");
+  const mke::Engine& d = dendrite->e;
+  st = mke::mp_solid_from_phi(f, d.phi[d.phi_cur], d.phi_elem == 8 ? 1 : 0);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(f.stream);  // done with the dendrite's phi
+  if (st != cudaSuccess) return cuda_fail(flow, st, "update_geometry");
+  if (fresh) drop_graphs(flow);  // the captured geometry had no solids
+  return MK_OK;
+}
+
+mk_status mk_update_velocity(mk_handle* dendrite, mk_handle* flow) {
+  const Range nvtx_range("mk_update_velocity");
+  if (!flow || !dendrite) return MK_ERR_ARG;
+  if (!couple_ok(flow->e, dendrite->e)) {
+    dendrite->err = "update_velocity: a thermal or solutal dendrite handle and a multiphase handle of one grid and device";
+    return MK_ERR_ARG;
+  }
+  const bool fresh = !dendrite->e.vel;
+  cudaError_t st = mke::engine_set_velocity(dendrite->e, flow->e);
+  if (st != cudaSuccess) return cuda_fail(dendrite, st, "update_velocity");
+  if (fresh) drop_graphs(dendrite);  // the captured loop had no advection
+  return MK_OK;
+}
 
 mk_status mk_get_tuning(const mk_handle* h, mk_tuning* out) {
   if (!h || !out) return MK_ERR_ARG;

@@ -450,11 +450,19 @@ struct Stor<__nv_bfloat16> {
 // neighbour link into a ghost plane is valid wherever the global domain has
 // that neighbour, so streaming reads and writes the ghost slots; the z wrap of
 // a periodic global axis goes through the ghosts, never through the index.
+//
+// Dynamic solids (a multiphase flow coupled to a growing dendrite): `solid`
+// flags cells that left the fluid (1), and `near` the fluid cells with a
+// solid neighbour; both NULL when the domain has none.  A solid cell is not
+// fluid, a link into it bounces back, and a cell next to one takes the
+// general neighbourhood (Nbr) instead of the interior-row addressing.
 struct Geom {
   int nx, ny, nz;
   int bc0, bc1, bc2;
   int64_t stride;  // population plane stride (cells)
   int slab = 0, zg0 = 0, nzg = 0;
+  const unsigned char* solid = nullptr;
+  const unsigned char* near = nullptr;
 
   // global z of local plane z (slab), and whether a global plane is a cell of
   // the domain that streams (not beyond a non-periodic face, not a wall)
@@ -466,6 +474,7 @@ struct Geom {
   }
 
   __device__ __forceinline__ bool fluid(int x, int y, int z) const {
+    if (solid && solid[idx(x, y, z)]) return false;
     if (bc0 == 1 && (x == 0 || x == nx - 1)) return false;
     if (bc1 == 1 && (y == 0 || y == ny - 1)) return false;
     if (slab) return z >= 1 && z <= nz - 2 && gz_open(gz(z));
@@ -505,7 +514,7 @@ struct Geom {
       }
     }
     out = idx(cx, cy, cz);
-    return true;
+    return !(solid && solid[out]);
   }
 };
 
@@ -566,6 +575,12 @@ struct Nbr {
 #pragma unroll
         for (int dx = 0; dx < 3; ++dx)
           if (vx[dx] && vy[dy] && vz[dz]) ok |= 1u << (dx + 3 * dy + 9 * dz);
+    if (g.solid) {
+      // links into dynamic solids close
+#pragma unroll
+      for (int b = 0; b < 27; ++b)
+        if (((ok >> b) & 1u) && g.solid[ox[b % 3] + oy[(b / 3) % 3] + oz[b / 9]]) ok &= ~(1u << b);
+    }
   }
   __device__ __forceinline__ int idx(int dx, int dy, int dz) const {
     return base + ox[dx + 1] + oy[dy + 1] + oz[dz + 1];
@@ -588,6 +603,7 @@ struct Fast {
 // Whether (x,y,z) may use Fast: y, z strictly inside the fluid span of their
 // axis, x inside it or on a periodic axis.
 __device__ __forceinline__ bool fast_cell(const Geom& g, int x, int y, int z) {
+  if (g.near && g.near[g.idx(x, y, z)]) return false;
   auto inside = [](int c, int n, int bc) {
     const int lo = bc == 1 ? 2 : 1;
     const int hi = bc == 1 ? n - 3 : n - 2;
@@ -618,7 +634,8 @@ struct FastW : Fast {
 
 // Whether (x,y,z) may use FastW: y and z strictly inside the fluid span of
 // their axis (x is free).
-__device__ __forceinline__ bool fastw_cell(const Geom& g, int, int y, int z) {
+__device__ __forceinline__ bool fastw_cell(const Geom& g, int x, int y, int z) {
+  if (g.near && g.near[g.idx(x, y, z)]) return false;
   auto inside = [](int c, int n, int bc) {
     const int lo = bc == 1 ? 2 : 1;
     const int hi = bc == 1 ? n - 3 : n - 2;

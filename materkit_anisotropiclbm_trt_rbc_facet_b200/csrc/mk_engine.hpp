@@ -84,6 +84,14 @@ struct Engine {
   int rows;              // 1: the collision runs row-staged
   int rows_ns, rows_grid, rows_threads;
   size_t rows_stage, rows_smem;
+  // dynamic solids of a multiphase flow coupled to a dendrite
+  // (mk_update_geometry): the solid flags, the fluid cells next to a solid,
+  // and the flags of the next update, applied at the next even loop count
+  unsigned char* msolid;
+  unsigned char* mnear;
+  unsigned char* mpending;
+  int mpending_set;
+  int capturing;         // a loop is being captured into a graph (no host-side state changes)
   // z-slab of a larger multiphase domain (mk_create_slab): the local planes
   // 1 .. nz - 2 are the global planes zg0 .. zg0 + nz - 3 of nzg planes; the
   // planes 0 and nz - 1 are ghosts filled by the exchanges
@@ -133,6 +141,10 @@ const char* engine_kernel_name(const Engine& e, int k);
 
 // Compute a macroscopic field of the current state into e.field (device).
 cudaError_t engine_field(Engine& e, int field);
+// A thermal or solutal dendrite advected by a multiphase flow of the same
+// grid: the flow's velocity into d.vel (allocated on first use), after which
+// the dendrite's scalar lattice carries it.  Synchronous.
+cudaError_t engine_set_velocity(Engine& d, Engine& f);
 // Multigrain: grain j's order parameter into e.field (device).
 cudaError_t engine_grain_field(Engine& e, int grain);
 
@@ -140,6 +152,13 @@ cudaError_t engine_grain_field(Engine& e, int grain);
 // case (sets wave_ok and the wave_* fields), and launch one loop.
 void mp_configure(Engine& e);
 void mp_launch(Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* ev);
+// Dynamic solids: set the pending flags from a dendrite's phi (solid where
+// phi > 0, cumulative), on the handle's stream; and apply pending flags
+// (solid, near) when the loop count is even.  The dendrite's phi is FP64
+// (phi_double) or FP32.
+cudaError_t mp_solid_from_phi(Engine& e, const void* dend_phi, int phi_double);
+cudaError_t mp_apply_solids(Engine& e);
+
 // One kernel of the two-kernel loop at the parity of e.step: part 0 the phi
 // kernel, part 1 the collision (slab handles run the loop in its parts, with
 // the exchanges between them).

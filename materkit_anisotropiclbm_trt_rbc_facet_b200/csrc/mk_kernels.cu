@@ -924,6 +924,12 @@ __global__ void k_field_copy(const P* __restrict__ a, const P* __restrict__ b, i
   out[i] = b ? double(a[i]) - double(b[i]) : double(a[i]);
 }
 
+template <class P>
+__global__ void k_double_to_plane(const double* __restrict__ a, P* __restrict__ out, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = P(a[i]);
+}
+
 __global__ void k_to_f32(const double* __restrict__ a, int64_t n, float* __restrict__ out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (float)a[i];
@@ -937,7 +943,7 @@ __global__ void k_field_geom(const Geom g, int field, const double* __restrict__
   if (x >= g.nx || y >= g.ny) return;
   const int64_t c = g.idx(x, y, z);
   if (field == MK_FIELD_FLAG)
-    out[c] = g.fluid(x, y, z) ? MK_FLAG_FLUID : MK_FLAG_WALLS;
+    out[c] = g.fluid(x, y, z) ? MK_FLAG_FLUID : ((g.solid && g.solid[c]) ? MK_FLAG_SOLID : MK_FLAG_WALLS);
   else
     out[c] = nobj > 0 ? nearest_seed(seeds, nobj, x, y, z) : 0;
 }
@@ -1307,6 +1313,28 @@ void launch_dend(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t*
   }
   const bool sol = e.p.model == MK_MODEL_SOLUTAL_DENDRITE;
   const bool gen = e.p.aniso != MK_ANISO_CUBIC;
+  if (e.vel) {
+    // an external velocity (mk_update_velocity): the scalar lattice advected
+    // as in the flow + dendrite models, no inflow faces
+    const P* vel = (const P*)e.vel;
+#define MK_DENDV(PAR, GEN, SOL)                                                                                 \
+  k_fd_dend<S, P, PAR, GEN, false, SOL><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, vel, e.grain, \
+                                                                      (const T*)e.rot, g, k)
+    if (parity == 0) {
+      if (sol)
+        gen ? MK_DENDV(0, true, true) : MK_DENDV(0, false, true);
+      else
+        gen ? MK_DENDV(0, true, false) : MK_DENDV(0, false, false);
+    } else {
+      if (sol)
+        gen ? MK_DENDV(1, true, true) : MK_DENDV(1, false, true);
+      else
+        gen ? MK_DENDV(1, true, false) : MK_DENDV(1, false, false);
+    }
+#undef MK_DENDV
+    if (ev) cudaEventRecord(ev[3], e.stream);
+    return;
+  }
 #define MK_DEND(PAR, SOL, GEN)                                                                              \
   k_dend_collide<S, P, PAR, SOL, GEN><<<grid, block, 0, e.stream>>>(G, Tp, phi_new, phi_old, temp, e.grain, \
                                                                     (const T*)e.rot, g, k)
@@ -1499,6 +1527,7 @@ void step_t(mke::Engine& e, cudaEvent_t* ev) {
       e.launches += 1;
       break;
     case MK_MODEL_MULTIPHASE:
+      if (e.mpending_set && !e.capturing) mke::mp_apply_solids(e);
       mke::mp_launch(e, parity, grid, block, ev);
       e.launches += engine_kernels_per_step(e);
       break;
@@ -1830,7 +1859,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
 void engine_free(Engine& e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
   void* ptrs[] = {e.pop0, e.pop1, e.pop2, e.vel, e.phij, e.gseeds, e.rest1, e.phi[0], e.phi[1], e.temp, e.seeds, e.rot, e.grain, e.partial, e.dsum, e.field,
-                  e.field32, e.stage32, e.wave_flags, e.wave_err, e.slab_halo};
+                  e.field32, e.stage32, e.wave_flags, e.wave_err, e.slab_halo, e.msolid, e.mnear, e.mpending};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (e.stream) cudaStreamDestroy(e.stream);
@@ -1950,6 +1979,31 @@ const char* engine_kernel_name(const Engine& e, int k) {
   return k == 0 ? "phi" : "collide";
 }
 
+cudaError_t engine_set_velocity(Engine& d, Engine& f) {
+  const int dm = d.p.model;
+  if (!(dm == MK_MODEL_THERMAL_DENDRITE || dm == MK_MODEL_SOLUTAL_DENDRITE) || f.p.model != MK_MODEL_MULTIPHASE ||
+      d.nx != f.nx || d.ny != f.ny || d.nz != f.nz || d.device != f.device || d.slab || f.slab)
+    return cudaErrorInvalidValue;
+  const int64_t n = d.ncell;
+  cudaError_t st = cudaSuccess;
+  if (!d.vel) {
+    if ((st = cudaMalloc(&d.vel, (size_t)3 * n * d.phi_elem)) != cudaSuccess) return st;
+    if ((st = cudaMemsetAsync(d.vel, 0, (size_t)3 * n * d.phi_elem, d.stream)) != cudaSuccess) return st;
+  }
+  const int blocks = (int)((n + 255) / 256);
+  for (int a = 0; a < 3; ++a) {
+    if ((st = engine_field(f, MK_FIELD_UX + a)) != cudaSuccess) return st;
+    if ((st = cudaStreamSynchronize(f.stream)) != cudaSuccess) return st;
+    if (d.phi_elem == 8)
+      k_double_to_plane<double><<<blocks, 256, 0, d.stream>>>(f.field, (double*)d.vel + a * n, n);
+    else
+      k_double_to_plane<float><<<blocks, 256, 0, d.stream>>>(f.field, (float*)d.vel + a * n, n);
+    if ((st = cudaGetLastError()) != cudaSuccess) return st;
+    if ((st = cudaStreamSynchronize(d.stream)) != cudaSuccess) return st;  // f.field is reused
+  }
+  return cudaSuccess;
+}
+
 cudaError_t engine_field(Engine& e, int field) {
   switch (e.p.precision) {
     case MK_PREC_FP64:
@@ -2038,7 +2092,11 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   };
   const int64_t step0 = e.step, l0 = e.launches;
   const int cur0 = e.phi_cur, bx0 = e.block_x, by0 = e.block_y, mb0 = e.minb;
+  // pending dynamic solids are not applied by the trial loops
+  const int pend0 = e.mpending_set;
+  e.capturing = 1;
   if ((st = copy(true)) != cudaSuccess) {
+    e.capturing = 0;
     cudaFree(save);
     return st;
   }
@@ -2100,6 +2158,8 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  e.capturing = 0;
+  e.mpending_set = pend0;
   cudaError_t s3 = cudaStreamSynchronize(e.stream);
   cudaFree(save);
   if (st != cudaSuccess) return st;

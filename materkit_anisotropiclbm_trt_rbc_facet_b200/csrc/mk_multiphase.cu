@@ -923,9 +923,121 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   if (ev) cudaEventRecord(ev[3], e.stream);
 }
 
+// Dynamic solids: pending |= (a fluid cell of the static geometry with the
+// dendrite's phi > 0).
+template <class P>
+__global__ void k_solid_from_phi(const P* __restrict__ dphi, const Geom g, unsigned char* __restrict__ pending,
+                                 int64_t n) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(c % g.nx), y = (int)((c / g.nx) % g.ny), z = (int)(c / ((int64_t)g.nx * g.ny));
+    if (g.fluid(x, y, z) && double(dphi[c]) > 0.0) pending[c] = 1;
+  }
+}
+
+// near = a fluid cell with a D3Q19 neighbour that is solid (g carries the
+// static geometry; `solid` the new flags).
+__global__ void k_near_solid(const Geom g, const unsigned char* __restrict__ solid, unsigned char* __restrict__ near,
+                             int64_t n) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(c % g.nx), y = (int)((c / g.nx) % g.ny), z = (int)(c / ((int64_t)g.nx * g.ny));
+    unsigned char v = 0;
+    if (!solid[c] && g.fluid(x, y, z)) {
+#pragma unroll
+      for (int i = 1; i < 19; ++i) {
+        int64_t j;
+        if (g.nbr(x, y, z, ex(i), ey(i), ez(i), j) && solid[j]) v = 1;
+      }
+    }
+    near[c] = v;
+  }
+}
+
+// Re-streams the links that the cells turning solid close.  At an even loop
+// count the in-place layout holds each fluid cell's streamed (pre-collision)
+// populations in its own slots, streamed with the geometry of the last loop:
+// slot i of a cell c whose upwind neighbour c - e_i turns solid now holds
+// that neighbour's outgoing population.  With the new geometry that link
+// bounces back: it must hold c's own outgoing population in direction
+// inv(i), which the last odd loop wrote into the neighbour's slot inv(i)
+// (the link was open then).  The new solids' slots are only read and the
+// fluid cells' only written, so the copy is race-free; a raw element copy is
+// exact in every storage format (w_i = w_inv(i)).  `g` carries the solids
+// of the last loop, `pending` the new set (a superset).
+template <class W>
+__global__ void k_solid_restream(W* __restrict__ G, W* __restrict__ H, const Geom g,
+                                 const unsigned char* __restrict__ pending, int64_t n) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(c % g.nx), y = (int)((c / g.nx) % g.ny), z = (int)(c / ((int64_t)g.nx * g.ny));
+    if (pending[c] || !g.fluid(x, y, z)) continue;
+#pragma unroll
+    for (int i = 1; i < 19; ++i) {
+      int64_t j;
+      if (g.nbr(x, y, z, -ex(i), -ey(i), -ez(i), j) && pending[j]) {
+        G[(int64_t)i * g.stride + c] = G[(int64_t)inv(i) * g.stride + j];
+        H[(int64_t)i * g.stride + c] = H[(int64_t)inv(i) * g.stride + j];
+      }
+    }
+  }
+}
+
 }  // namespace
 
 namespace mke {
+
+cudaError_t mp_solid_from_phi(Engine& e, const void* dend_phi, int phi_double) {
+  if (e.p.model != MK_MODEL_MULTIPHASE || e.slab) return cudaErrorInvalidValue;
+  const size_t n = (size_t)e.ncell;
+  cudaError_t st = cudaSuccess;
+  for (unsigned char** a : {&e.msolid, &e.mnear, &e.mpending})
+    if (!*a) {
+      if ((st = cudaMalloc((void**)a, n)) != cudaSuccess) return st;
+      if ((st = cudaMemsetAsync(*a, 0, n, e.stream)) != cudaSuccess) return st;
+    }
+  Geom g = make_geom(e);
+  g.solid = nullptr;  // the static geometry
+  g.near = nullptr;
+  const int blocks = (int)std::min<int64_t>((e.ncell + 255) / 256, 4096);
+  if (phi_double)
+    k_solid_from_phi<double><<<blocks, 256, 0, e.stream>>>((const double*)dend_phi, g, e.mpending, e.ncell);
+  else
+    k_solid_from_phi<float><<<blocks, 256, 0, e.stream>>>((const float*)dend_phi, g, e.mpending, e.ncell);
+  if ((st = cudaGetLastError()) != cudaSuccess) return st;
+  e.mpending_set = 1;
+  // the staged and fused forms assume a static geometry
+  e.wave = e.wave_ok = 0;
+  e.rows = e.rows_ok = 0;
+  return mp_apply_solids(e);
+}
+
+cudaError_t mp_apply_solids(Engine& e) {
+  if (!e.mpending_set || (e.step & 1)) return cudaSuccess;
+  const int blocks = (int)std::min<int64_t>((e.ncell + 255) / 256, 4096);
+  Geom g = make_geom(e);  // the solids of the last loop
+  g.near = nullptr;
+  switch (pop_elem(e.p.precision)) {
+    case 8:
+      k_solid_restream<uint64_t><<<blocks, 256, 0, e.stream>>>((uint64_t*)e.pop0, (uint64_t*)e.pop1, g, e.mpending,
+                                                               e.ncell);
+      break;
+    case 4:
+      k_solid_restream<uint32_t><<<blocks, 256, 0, e.stream>>>((uint32_t*)e.pop0, (uint32_t*)e.pop1, g, e.mpending,
+                                                               e.ncell);
+      break;
+    default:
+      k_solid_restream<uint16_t><<<blocks, 256, 0, e.stream>>>((uint16_t*)e.pop0, (uint16_t*)e.pop1, g, e.mpending,
+                                                               e.ncell);
+      break;
+  }
+  cudaError_t st = cudaGetLastError();
+  if (st != cudaSuccess) return st;
+  if ((st = cudaMemcpyAsync(e.msolid, e.mpending, (size_t)e.ncell, cudaMemcpyDeviceToDevice, e.stream)) !=
+      cudaSuccess)
+    return st;
+  g.solid = nullptr;
+  k_near_solid<<<blocks, 256, 0, e.stream>>>(g, e.msolid, e.mnear, e.ncell);
+  e.mpending_set = 0;
+  return cudaGetLastError();
+}
 
 void mp_configure(Engine& e) {
   switch (e.p.precision) {

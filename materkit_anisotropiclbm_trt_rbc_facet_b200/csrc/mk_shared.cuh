@@ -31,6 +31,8 @@ inline Geom make_geom(const mke::Engine& e) {
   g.slab = e.slab;
   g.zg0 = e.zg0;
   g.nzg = e.nzg;
+  g.solid = e.msolid;
+  g.near = e.mnear;
   return g;
 }
 

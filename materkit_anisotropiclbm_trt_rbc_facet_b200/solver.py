@@ -366,6 +366,17 @@ class Solver:
     def fused(self, on: bool) -> None:
         _check(self._lib.mk_set_fused(self._h, 1 if on else 0), self._h)
 
+    # -- coupling of a dendrite and a two-phase flow (run_flow_multiphase_dendrite)
+    def update_geometry(self, dendrite: "Solver") -> None:
+        """This multiphase flow takes the dendrite's solid (phi > 0) as geometry
+        from its next even loop count (mkFluidsMultiphase::update_geometry)."""
+        _check(self._lib.mk_update_geometry(self._h, dendrite.handle), self._h)
+
+    def update_velocity(self, flow: "Solver") -> None:
+        """This dendrite's scalar lattice is advected by the flow's velocity
+        (mkThermalField::update_velocity)."""
+        _check(self._lib.mk_update_velocity(self._h, flow.handle), self._h)
+
     @property
     def tuning(self) -> dict:
         """The launch configuration (block shape, occupancy variant, loop and

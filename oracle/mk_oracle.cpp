@@ -156,6 +156,8 @@ struct orc_state {
   std::vector<double> phij;                     // their order parameters, [grain][cell]
   std::vector<int> grain;
   std::vector<double> rot;  // 9 per object (R, columns = crystal axes)
+  std::vector<uint8_t> pend;  // multiphase: cells to turn solid (orc_update_geometry)
+  int pend_set = 0;
 };
 
 namespace {
@@ -1048,6 +1050,39 @@ extern "C" void orc_destroy(orc_state* s) { delete s; }
 
 extern "C" int64_t orc_step(const orc_state* s) { return s->step; }
 
+// Coupling of a dendrite and a multiphase flow of one grid (the semantics of
+// mk_update_geometry / mk_update_velocity): the flow's fluid cells where the
+// dendrite's phi > 0 become solid at the flow's next even loop count
+// (cumulative), and the dendrite's scalar lattice takes the flow's velocity.
+static void apply_pending_solids(orc_state* s) {
+  if (!s->pend_set || (s->step & 1)) return;
+  for (int64_t c = 0; c < s->n; ++c)
+    if (s->pend[c]) s->flag[c] = MK_FLAG_SOLID;
+  s->pend_set = 0;
+}
+
+extern "C" int orc_update_geometry(orc_state* flow, const orc_state* dend) {
+  if (flow->p.model != MK_MODEL_MULTIPHASE || flow->n != dend->n || flow->nx != dend->nx || flow->ny != dend->ny)
+    return 1;
+  if (flow->pend.empty()) flow->pend.assign(flow->n, 0);
+  for (int64_t c = 0; c < flow->n; ++c)
+    if (flow->flag[c] == MK_FLAG_FLUID && dend->phi[c] > 0.0) flow->pend[c] = 1;
+  flow->pend_set = 1;
+  apply_pending_solids(flow);
+  return 0;
+}
+
+extern "C" int orc_update_velocity(orc_state* dend, const orc_state* flow) {
+  if (flow->p.model != MK_MODEL_MULTIPHASE || flow->n != dend->n) return 1;
+  std::vector<double> u((size_t)flow->n);
+  dend->vel.assign((size_t)3 * flow->n, 0.0);
+  for (int a = 0; a < 3; ++a) {
+    orc_get_field(flow, MK_FIELD_UX + a, u.data());
+    for (int64_t c = 0; c < flow->n; ++c) dend->vel[(size_t)(3 * c + a)] = u[(size_t)c];
+  }
+  return 0;
+}
+
 extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
   for (int64_t t = 0; t < nsteps; ++t) {
     switch (s->p.model) {
@@ -1055,6 +1090,7 @@ extern "C" void orc_advance(orc_state* s, int64_t nsteps) {
         flow_step(s);
         break;
       case MK_MODEL_MULTIPHASE:
+        apply_pending_solids(s);
         mp_step(s);
         break;
       case MK_MODEL_CONVECTION:

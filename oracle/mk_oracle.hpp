@@ -134,6 +134,12 @@ int orc_get_threads(void);
 // schedule(static, 16) sweeps) of the flow model (D3Q19, no moving plates)
 // and the thermal dendrite, created from an oracle state and bit-identical
 // to orc_advance; NULL for other models.
+// Coupling of a dendrite and a multiphase flow of one grid: the flow's fluid
+// cells with dendrite phi > 0 turn solid at its next even loop count; the
+// dendrite's scalar lattice takes the flow's velocity.  1 for a mismatch.
+int orc_update_geometry(orc_state* flow, const orc_state* dendrite);
+int orc_update_velocity(orc_state* dendrite, const orc_state* flow);
+
 typedef struct orc_aos orc_aos;
 orc_aos* orc_aos_create(const orc_state* s);
 void orc_aos_destroy(orc_aos* a);

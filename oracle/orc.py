@@ -52,6 +52,10 @@ def load() -> C.CDLL:
         lib.orc_anisotropy.argtypes = [C.c_int, C.c_double, C.c_double, D, D, D]
         lib.orc_backward.restype = C.c_int
         lib.orc_backward.argtypes = [C.c_void_p, D, C.c_int64, D]
+        lib.orc_update_geometry.restype = C.c_int
+        lib.orc_update_geometry.argtypes = [C.c_void_p, C.c_void_p]
+        lib.orc_update_velocity.restype = C.c_int
+        lib.orc_update_velocity.argtypes = [C.c_void_p, C.c_void_p]
         lib.orc_aos_create.restype = C.c_void_p
         lib.orc_aos_create.argtypes = [C.c_void_p]
         lib.orc_aos_destroy.argtypes = [C.c_void_p]
@@ -146,6 +150,17 @@ class Oracle:
         if self.lib.orc_get_grain_phi(self.h, int(j), _ptr(out)) != 0:
             raise KeyError(j)
         return out.reshape(p.nz, p.ny, p.nx)
+
+    def update_geometry(self, dendrite: "Oracle") -> None:
+        """This multiphase flow takes the dendrite's solid (phi > 0) as geometry
+        from its next even loop count."""
+        if self.lib.orc_update_geometry(self.h, dendrite.h) != 0:
+            raise ValueError("update_geometry: a multiphase flow and a dendrite of one grid")
+
+    def update_velocity(self, flow: "Oracle") -> None:
+        """This dendrite's scalar lattice takes the flow's velocity."""
+        if self.lib.orc_update_velocity(self.h, flow.h) != 0:
+            raise ValueError("update_velocity: a dendrite and a multiphase flow of one grid")
 
     def populations(self, which: int = 0) -> np.ndarray:
         """Post-collision populations of lattice `which`, (Q, ncell)."""
