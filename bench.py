@@ -9,8 +9,8 @@ Workloads (--workload)
             thermal lattice, one centred seed)
   ensemble  48 seeded solutal dendrite domains (edges 48-128) packed into
             one lattice, BF16 storage, persistent launches + CUDA graph
-  multigrain  eight grains (one Allen-Cahn order parameter each, pairwise
-            overlap penalty) + D3Q7 thermal lattice, 128^3
+  multigrain  eight grains (one D3Q19 Allen-Cahn order parameter each,
+            pairwise overlap penalty) + D3Q7 thermal lattice, 128^3
   flow_dendrite  thermal dendrite growing in a melt that flows in at x = 0
             and out at x = n - 1, 128^3 (D3Q19 TRT flow with porous
             bounce-back + phase field + advected D3Q7 thermal lattice)
@@ -58,7 +58,7 @@ WORKLOADS = {
                       "size": 128, "precision": "fp32", "kernel": "k_fd_flow", "slot": "flow",
                       "collision": "TRT(f, porous bounce-back) + BGK(g) + BGK(T)",
                       "data": "synthetic (seed at x = n/3, eps4 0.05, undercooling 0.55, inflow u = 0.02)"},
-    "multigrain": {"workload": "multigrain {n}^3: 8 grains (D3Q7 Allen-Cahn each, overlap penalty) + D3Q7 thermal",
+    "multigrain": {"workload": "multigrain {n}^3: 8 grains (D3Q19 Allen-Cahn each, overlap penalty) + D3Q7 thermal",
                    "metric": "MLUPS, %HBM roofline: multigrain 128^3, 8 grain lattices + thermal",
                    "size": 128, "precision": "fp32", "kernel": "k_mg_collide", "collision": "BGK(g_j) + BGK(T)",
                    "data": "synthetic (2 x 2 x 2 grains of radius n/5 at the quarter points)"},
@@ -203,9 +203,10 @@ def _collide_bytes(workload: str, prec: str, cells: int) -> int:
     if workload == "poiseuille":
         return cells * 38 * S
     if workload == "multigrain":
-        # 8 grain lattices and the thermal lattice read and written, phi_j read
-        # (the stencil's halo counted once), phi(t+1), phi(t) read, T read and written
-        return cells * ((8 * 14 + 14) * S + (8 + 4) * P)
+        # 8 D3Q19 grain lattices and the D3Q7 thermal lattice read and written,
+        # phi_j read (the stencil's halo counted once), phi(t+1), phi(t) read,
+        # T read and written
+        return cells * ((8 * 38 + 14) * S + (8 + 4) * P)
     return cells * (28 * S + 4 * P)
 
 

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define MKB200_ABI_VERSION 2
+#define MKB200_ABI_VERSION 3
 
 /* Status codes.  Replace the exception family of
  * MaterKit/inc/mkRunTimeDiagnostics.h:59-117 (mkIOError, mkMemoryError, ...). */
@@ -206,6 +206,10 @@ typedef struct mk_params {
    * (grain 0 has none, mkFluidsUser.cpp:233-251); the mobility is `mobility`,
    * the interface width `W0` */
   double grain_kappa;
+  /* multigrain: velocity in the equilibrium of grain 1 (the reference
+   * relaxes grain 1 towards a moving equilibrium with u = (0.02, 0, 0),
+   * mkFluidsUser.cpp:220-226, the default; every other grain is at rest) */
+  double grain_u[3];
 } mk_params;
 
 /* Optional overrides at creation; a negative value keeps the XML/default. */

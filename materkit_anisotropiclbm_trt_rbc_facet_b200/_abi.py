@@ -59,7 +59,7 @@ class MkParams(C.Structure):
         ("eps2", C.c_double),
         ("wall_axis", C.c_int32), ("inlet", C.c_int32), ("wall_value", C.c_double * 2),
         ("wall_u", (C.c_double * 3) * 2), ("beta", C.c_double), ("s_ref", C.c_double),
-        ("grain_kappa", C.c_double),
+        ("grain_kappa", C.c_double), ("grain_u", C.c_double * 3),
     ]
 
     def ncell(self) -> int:

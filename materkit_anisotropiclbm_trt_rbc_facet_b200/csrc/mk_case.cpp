@@ -56,6 +56,10 @@ void default_params(mk_params* p) {
   p->wall_axis = -1;
   p->inlet = 0;
   p->grain_kappa = 1.0;
+  // grain 1 relaxes towards an equilibrium moving at (0.02, 0, 0) in the
+  // reference's multigrain relaxation (mkFluidsUser.cpp:220-226)
+  p->grain_u[0] = 0.02;
+  p->grain_u[1] = p->grain_u[2] = 0.0;
 }
 
 void default_options(mk_options* o) {
@@ -641,6 +645,10 @@ mk_status resolve_case(const std::string& xml, const mk_options* opt, mk_params*
     if (b->child("velocity")) {
       if (!opt_v(b, "velocity", v, err)) return MK_ERR_XML;
       for (int a = 0; a < 3; ++a) p.u0[a] = a < (int)v.size() ? v[a] : 0.0;
+    }
+    if (b->child("grainVelocity")) {
+      if (!opt_v(b, "grainVelocity", v, err)) return MK_ERR_XML;
+      for (int a = 0; a < 3; ++a) p.grain_u[a] = a < (int)v.size() ? v[a] : 0.0;
     }
     if (const mkx::Element* e = b->child("wallAxis")) {
       const std::string t = lower(mkx::trimmed(e->text));

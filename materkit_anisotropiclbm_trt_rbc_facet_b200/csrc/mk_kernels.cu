@@ -555,18 +555,22 @@ __global__ void __launch_bounds__(128)
 }
 
 // ====================================================== MULTIGRAIN (f-3)
-// run_multiPhaseField (MaterKit.cpp:529-571), mkFluidsUser::propagate /
-// relaxation (mkFluidsUser.cpp:68-299): one D3Q7 lattice per grain j (planes
-// 7j .. 7j+6 of lattice 0, held as g - w (-1)), phi_j = sum g_j (streamed),
-// the aggregate phi = (N - 1) + sum phi_j, and per grain
-//   g_j* = g_j - om (g_j - w phi_j) + w P_j + (1 - om/2) w lam_j (e.n_j),
-// P_j = -2 p_j kappa_j (sum_k p_k^2 - p_j^2), p = (1 + phi)/2, kappa_0 = 0;
-// n_j = grad phi_j / (|grad phi_j| + 1e-6) (D3Q19 gradient), lam_j =
-// (1 - phi_j^2)/(sqrt2 W0).
+// run_multiPhaseField with mkFluidsUser::propagate / relaxation
+// (mkFluidsUser.cpp:68-299): one D3Q19 lattice per grain (pop0 planes
+// 19j .. 19j+18, held as g - w (-1); on a one-cell periodic z axis D3Q19
+// reduces exactly to the D2Q9 set the reference ships), phi_j = sum g_j
+// (streamed), the aggregate phi = (N - 1) + sum phi_j, and per grain
+//   g_j* = g_j - om (g_j - geq_j) + w P_j + (1 - om/2) w lam_j (e.n_j),
+// geq_j = w phi_j (1 + 3 e.u + 4.5 (e.u)^2 - 1.5 u^2) with u = grain_u for
+// j = 1 and 0 otherwise (mkFluidsUser.cpp:220-226), P_j = -2 p_j kappa_j
+// (sum_k p_k^2 - p_j^2), p = (1 + phi)/2, kappa_0 = 0; n_j = s_j / (|s_j| +
+// 1e-6) with s_j = sum_i w_i e_i phi_j(x + e_i) (:201-208); lam_j = (1 -
+// phi_j^2)/(sqrt2 W0); om = 1/(3 M + 1/2) (:282).
 // The thermal lattice relaxes with latent heat (1/2) dphi of the aggregate.
 template <class T>
 struct MgK {
   T om, fo, inv_w, kappa, om_t, ref_t;
+  T ux, uy, uz, uu;  // grain 1's equilibrium velocity and its square
   int ngr;
 };
 
@@ -577,16 +581,19 @@ __device__ __forceinline__ void mg_phi_cell(const S* __restrict__ G, P* __restri
   typedef typename Stor<S>::T T;
   T agg = T(ngr - 1);
   for (int j = 0; j < ngr; ++j) {
-    const S* Gj = G + (int64_t)j * 7 * stride;
+    const S* Gj = G + (int64_t)j * 19 * stride;
     T sum = T(-1);
     if constexpr (Stor<S>::scaled) {  // stored units, one multiply per weight class
-      T sa = T(0);
+      T sa = T(0), sd = T(0);
 #pragma unroll
-      for (int i = 1; i < 7; ++i) sa += ld_in_raw<S, 7>(Gj, stride, nb, PARITY, c, i);
-      sum += T(wq<7>(0)) * ld_in_raw<S, 7>(Gj, stride, nb, PARITY, c, 0) + T(wq<7>(1)) * sa;
+      for (int i = 1; i < 7; ++i) sa += ld_in_raw<S, 19>(Gj, stride, nb, PARITY, c, i);
+#pragma unroll
+      for (int i = 7; i < 19; ++i) sd += ld_in_raw<S, 19>(Gj, stride, nb, PARITY, c, i);
+      sum += T(wq<19>(0)) * ld_in_raw<S, 19>(Gj, stride, nb, PARITY, c, 0) + T(wq<19>(1)) * sa +
+             T(wq<19>(7)) * sd;
     } else {
 #pragma unroll
-      for (int i = 0; i < 7; ++i) sum += ld_in<S, 7>(Gj, stride, nb, PARITY, c, i);
+      for (int i = 0; i < 19; ++i) sum += ld_in<S, 19>(Gj, stride, nb, PARITY, c, i);
     }
     phij[(int64_t)j * ncell + c] = P(sum);
     agg += sum;
@@ -625,12 +632,11 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
   typedef typename Stor<S>::T T;
   // FP32 / FP64: every grain's slots and the thermal slots go to L2 first;
   // each grain's populations are loaded only after its stencil and penalty
-  // are computed (128^3, 8 grains: 0.39 -> 0.31 ms; no gain with 16-bit
-  // storage, where it is compiled out)
+  // are computed (no gain with 16-bit storage, where it is compiled out)
   if constexpr (Stor<S>::bytes >= 4) {
     for (int j = 0; j < k.ngr; ++j) {
 #pragma unroll
-      for (int i = 0; i < 7; ++i) pf_in<S, 7>(G + (int64_t)j * 7 * stride, stride, nb, PARITY, c, i);
+      for (int i = 0; i < 19; ++i) pf_in<S, 19>(G + (int64_t)j * 19 * stride, stride, nb, PARITY, c, i);
     }
 #pragma unroll
     for (int i = 0; i < 7; ++i) pf_in<S, 7>(Tp, stride, nb, PARITY, c, i);
@@ -652,28 +658,29 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
       if (ey(i)) gy += (w * T(ey(i))) * fn;
       if (ez(i)) gz += (w * T(ez(i))) * fn;
     }
-    gx *= T(3);
-    gy *= T(3);
-    gz *= T(3);
     // regularised at 1e-6: where grad phi_j vanishes (a seed centre on a
     // lattice point) its direction is rounding noise
-    // the fast division measured faster with 16-bit storage and slower with
-    // FP32 (0.38 -> 0.49 ms per 128^3 loop, 8 grains) in this kernel
     const T gs = sqrt(gx * gx + gy * gy + gz * gz) + T(1e-6);
     const T inv = Stor<S>::bytes == 2 ? div_fast(T(1), gs) : T(1) / gs;
     const T lam = (T(1) - ph * ph) * k.inv_w * k.fo;
     const T pj = T(0.5) * (T(1) + ph);
     const T Pj = j == 0 ? T(0) : T(-2) * pj * (S2 - pj * pj) * k.kappa;
     const T dph = ph + T(1);  // phi_j - ref
-    S* Gj = G + (int64_t)j * 7 * stride;
-    T gv[7];
+    const bool moving = j == 1;
+    S* Gj = G + (int64_t)j * 19 * stride;
+    T gv[19];
 #pragma unroll
-    for (int i = 0; i < 7; ++i) gv[i] = ld_in<S, 7>(Gj, stride, nb, PARITY, c, i);
+    for (int i = 0; i < 19; ++i) gv[i] = ld_in<S, 19>(Gj, stride, nb, PARITY, c, i);
 #pragma unroll
-    for (int i = 0; i < 7; ++i) {
-      const T w = T(wq<7>(i));
+    for (int i = 0; i < 19; ++i) {
+      const T w = T(wq<19>(i));
       const T en = (T(ex(i)) * gx + T(ey(i)) * gy + T(ez(i)) * gz) * inv;
-      st_out<S, 7>(Gj, stride, nb, PARITY, c, i, gv[i] - k.om * (gv[i] - w * dph) + w * Pj + w * lam * en);
+      T eq = dph;  // geq - w ref, over w
+      if (moving) {
+        const T eu = T(ex(i)) * k.ux + T(ey(i)) * k.uy + T(ez(i)) * k.uz;
+        eq += ph * (T(3) * eu + T(4.5) * eu * eu - T(1.5) * k.uu);
+      }
+      st_out<S, 19>(Gj, stride, nb, PARITY, c, i, gv[i] - k.om * (gv[i] - w * eq) + w * Pj + w * lam * en);
     }
   }
   // thermal lattice with latent heat (1/2) dphi of the aggregate
@@ -692,10 +699,8 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
   temp[c] = P(k.ref_t + dT);
 }
 
-// Three resident blocks per SM (80 registers; the odd loop spills a little in
-// FP32): 128^3, 8 grains, 0.31 -> 0.28 ms FP32 and 0.28 -> 0.25 ms FP16.
 template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256)
     k_mg_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phij, const P* __restrict__ phi_new,
                  const P* __restrict__ phi_old, P* __restrict__ temp, const Geom g, const MgK<typename Stor<S>::T> k) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -734,7 +739,7 @@ __global__ void k_mg_init(S* A0, S* A1, typename PhiOf<S>::type* phij, typename 
     const double ph = -tanh((sqrt(dx * dx + dy * dy + dz * dz) - gseeds[4 * j + 3]) / (sqrt(2.0) * W0));
     phij[(int64_t)j * ncell + c] = P(ph);
     agg += ph;
-    if (fl) put_eq<S, 7>(A0 + (int64_t)j * 7 * g.stride, g, nb, (int)c, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
+    if (fl) put_eq<S, 19>(A0 + (int64_t)j * 19 * g.stride, g, nb, (int)c, ph, 0.0, 0.0, 0.0, 0.0, refs.r0);
   }
   phi0[c] = P(agg);
   phi1[c] = P(agg);
@@ -1468,8 +1473,13 @@ void launch_fd(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
 template <class T>
 MgK<T> mg_coef(const mk_params& p, Refs r) {
   MgK<T> k;
-  k.om = T(1.0 / (4.0 * p.mobility + 0.5));
-  k.fo = T(1.0 - 0.5 / (4.0 * p.mobility + 0.5));
+  // omega_g = 1/(dt/dx^2/cs^2 + 1/2), cs^2 = 1/3 (mkFluidsUser.cpp:282; M = dt/dx^2)
+  k.om = T(1.0 / (3.0 * p.mobility + 0.5));
+  k.fo = T(1.0 - 0.5 / (3.0 * p.mobility + 0.5));
+  k.ux = T(p.grain_u[0]);
+  k.uy = T(p.grain_u[1]);
+  k.uz = T(p.grain_u[2]);
+  k.uu = T(p.grain_u[0] * p.grain_u[0] + p.grain_u[1] * p.grain_u[1] + p.grain_u[2] * p.grain_u[2]);
   k.inv_w = T(1.0 / (std::sqrt(2.0) * p.W0));
   k.kappa = T(p.grain_kappa);
   k.om_t = T(1.0 / (4.0 * p.D + 0.5));
@@ -1745,7 +1755,7 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
     e.Q0 = 7;
     e.Q1 = 7;
   }
-  if (p.model == MK_MODEL_MULTIGRAIN) e.Q0 = 7 * p.n_objects;  // one D3Q7 lattice per grain
+  if (p.model == MK_MODEL_MULTIGRAIN) e.Q0 = 19 * p.n_objects;  // one D3Q19 lattice per grain
   e.Q2 = mkm::flow_coupled(p.model) ? p.lattice : 0;
   // Launch shape: a full warp row along x, rows stacked in y to 256 threads.
   int bx = block_x > 0 ? block_x : (p.nx >= 128 ? 128 : (p.nx >= 64 ? 64 : 32));

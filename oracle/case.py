@@ -84,7 +84,7 @@ class MkParams(C.Structure):
         ("eps2", C.c_double),
         ("wall_axis", C.c_int32), ("inlet", C.c_int32), ("wall_value", C.c_double * 2),
         ("wall_u", (C.c_double * 3) * 2), ("beta", C.c_double), ("s_ref", C.c_double),
-        ("grain_kappa", C.c_double),
+        ("grain_kappa", C.c_double), ("grain_u", C.c_double * 3),
     ]
 
     def ncell(self) -> int:
@@ -126,6 +126,7 @@ def defaults() -> MkParams:
     p.aniso = ANISO["cubic"]
     p.wall_axis = -1
     p.grain_kappa = 1.0
+    p.grain_u[:] = [0.02, 0.0, 0.0]  # grain 1's equilibrium velocity (mkFluidsUser.cpp:220-226)
     return p
 
 
@@ -617,7 +618,7 @@ def _b200(b: Node, p: MkParams) -> None:
     tau0 = number(b.child("tau0")) if b.child("tau0") is not None else -1.0
     if any(b.child(t) is not None for t in ("W0", "lambda", "diffusivity")) or tau0 > 0:
         p.tau0 = tau0 if tau0 > 0 else 0.6267 * p.lambda_ * p.W0 ** 2 / p.D
-    for tag, field in (("force", "force"), ("velocity", "u0")):
+    for tag, field in (("force", "force"), ("velocity", "u0"), ("grainVelocity", "grain_u")):
         if b.child(tag) is not None:
             v = numbers(b.child(tag))
             getattr(p, field)[:] = [v[a] if a < len(v) else 0.0 for a in range(3)]

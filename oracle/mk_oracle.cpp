@@ -152,7 +152,7 @@ struct orc_state {
   std::vector<double> w_out, w_hlp;  // its populations
   std::vector<double> vel;           // its velocity, 3 per cell (advects the thermal lattice)
   int Ng = 0;                                   // multigrain: number of grain order parameters
-  std::vector<std::vector<double>> gj_out, gj_hlp;  // their D3Q7 lattices, one [q][cell] array per grain
+  std::vector<std::vector<double>> gj_out, gj_hlp;  // their D3Q19 lattices, one [q][cell] array per grain
   std::vector<double> phij;                     // their order parameters, [grain][cell]
   std::vector<int> grain;
   std::vector<double> rot;  // 9 per object (R, columns = crystal axes)
@@ -794,25 +794,28 @@ void flow_dendrite_nee(orc_state* s, bool flow_lattice) {
 // ------------------------------------------------------- MULTIGRAIN model
 // run_multiPhaseField (MaterKit.cpp:529-571) with mkFluidsUser::propagate /
 // relaxation (mkFluidsUser.cpp:68-299, the multiphase field of "Programming
-// Phase-Field Modelling" p. 37 Eq. 4.35): one D3Q7 lattice per grain j,
-//   phi_j = sum_i g_j,i (streamed), phi = (N - 1) + sum_j phi_j,
-//   g_j* = g_j - om (g_j - w phi_j) + w P_j + (1 - om/2) w lam_j (e.n_j),
-// P_j = -2 p_j kappa_j sum_{k != j} p_k^2 with p = (1 + phi)/2 and kappa_0 = 0,
-// kappa_j = grain_kappa for j >= 1 (mkFluidsUser.cpp:233-251); the growth
-// source is off in the reference (Q_phi = 0 * ..., :255-263).  The Chai et al.
-// (IJHMT 122 (2018) 631) conservative Allen-Cahn flux with n_j = grad phi_j /
-// (|grad phi_j| + 1e-6) (D3Q19 isotropic gradient) and lam_j = (1 - phi_j^2)/(sqrt2 W0),
-// the flux that holds phi_j = tanh(x / (sqrt2 W0)), om = 1/(4 M + 1/2)
-// (:282, M = mobility).  Then the thermal lattice with latent heat (1/2) dphi of
-// the aggregate (mkThermalField::propagate / relaxation).  Left out: the
-// reference's aggregate g lattice (its density is overwritten by the sum of the
-// grains at :162-168 and never read) and its hard-coded test velocity of grain
-// 1 in the equilibrium (:220-226).
+// Phase-Field Modelling" p. 37 Eq. 4.35), whose arithmetic is readable: one
+// lattice per grain j on the reference's flow/phase velocity set (D3Q19 here;
+// on a one-cell periodic z axis it reduces exactly to the D2Q9 the reference
+// ships with QF = 9, mkGlobalDefs.h:134),
+//   phi_j = sum_i g_j,i (streamed, :156-160), phi = (N - 1) + sum_j phi_j (:162-168),
+//   n_j = s_j / (|s_j| + eps), s_j = sum_i w_i e_i phi_j(x + e_i) (:201-208),
+//   g_j* = g_j - om (g_j - geq_j) + w P_j + (1 - om/2) w lam_j (e.n_j) (:283-297),
+// geq_j = w phi_j (1 + 3 e.u + 4.5 (e.u)^2 - 1.5 u^2) with u = grain_u for
+// j = 1 and 0 otherwise (:220-226), P_j = -2 p_j kappa_j sum_{k != j} p_k^2,
+// p = (1 + phi)/2, kappa_0 = 0, kappa_j = grain_kappa (:231-252), om =
+// 1/(M/cs^2 + 1/2) with cs^2 = 1/3 (:282, M = dt/dx^2 = mobility); the growth
+// source is off (Q_phi = 0 * ..., :255-263).  The library's source term
+// (getAddedPhasePDFs) is the Chai et al. (IJHMT 122 (2018) 631) conservative
+// flux with lam_j = (1 - phi_j^2)/(sqrt2 W0), eps = 1e-6.  Then the thermal
+// lattice with latent heat (1/2) dphi of the aggregate (mkThermalField::
+// propagate / relaxation).  Left out: the aggregate g lattice (its density is
+// overwritten by the sum of the grains, :162-168, and never read).
 void multigrain_step(orc_state* s) {
   const int64_t n = s->n;
   const mk_params& p = s->p;
   const int N = s->Ng;
-  for (int j = 0; j < N; ++j) propagate(s, 7, s->gj_out[j], s->gj_hlp[j]);
+  for (int j = 0; j < N; ++j) propagate(s, 19, s->gj_out[j], s->gj_hlp[j]);
   std::swap(s->phi_prev, s->phi);
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < n; ++c) {
@@ -823,13 +826,13 @@ void multigrain_step(orc_state* s) {
     double agg = N - 1.0;
     for (int j = 0; j < N; ++j) {
       double ph = 0;
-      for (int i = 0; i < 7; ++i) ph += s->gj_hlp[j][(int64_t)i * n + c];
+      for (int i = 0; i < 19; ++i) ph += s->gj_hlp[j][(int64_t)i * n + c];
       s->phij[(int64_t)j * n + c] = ph;
       agg += ph;
     }
     s->phi[c] = agg;
   }
-  const double om = 1.0 / (4.0 * p.mobility + 0.5);
+  const double om = 1.0 / (3.0 * p.mobility + 0.5);
   const double fo = 1.0 - 0.5 * om;
   const double inv_w = 1.0 / (std::sqrt(2.0) * p.W0);
 #pragma omp parallel for schedule(static)
@@ -838,34 +841,37 @@ void multigrain_step(orc_state* s) {
       for (int x = 0; x < s->nx; ++x) {
         const int64_t c = cidx(s, x, y, z);
         if (s->flag[c] != MK_FLAG_FLUID) continue;
-        double S2 = 0;
-        for (int k = 0; k < N; ++k) {
-          const double pk = 0.5 * (1.0 + s->phij[(int64_t)k * n + c]);
-          S2 += pk * pk;
-        }
         for (int j = 0; j < N; ++j) {
           const double* f = &s->phij[(int64_t)j * n];
           const double ph = f[c];
-          double gr[3] = {0, 0, 0};
+          double sv[3] = {0, 0, 0};
           for (int i = 1; i < 19; ++i) {
             const int64_t nb = nbr(s, x, y, z, E27[i][0], E27[i][1], E27[i][2]);
             const double fn = nb >= 0 ? f[nb] : ph;
-            for (int a = 0; a < 3; ++a) gr[a] += weight(19, i) * E27[i][a] * fn;
+            for (int a = 0; a < 3; ++a) sv[a] += weight(19, i) * E27[i][a] * fn;
           }
-          for (int a = 0; a < 3; ++a) gr[a] *= 3.0;
-          const double gn = std::sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
-          // regularised at 1e-6, not 1e-12: where grad phi_j vanishes (a seed
-          // centre on a lattice point) its direction is rounding noise, which
-          // the flux would carry at full strength lam
-          const double nv[3] = {gr[0] / (gn + 1e-6), gr[1] / (gn + 1e-6), gr[2] / (gn + 1e-6)};
+          // regularised at 1e-6: where grad phi_j vanishes (a seed centre on
+          // a lattice point) its direction is rounding noise, which the flux
+          // would carry at full strength lam
+          const double sn = std::sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]) + 1e-6;
+          const double nv[3] = {sv[0] / sn, sv[1] / sn, sv[2] / sn};
           const double lam = (1.0 - ph * ph) * inv_w;
-          const double pj = 0.5 * (1.0 + ph);
-          const double P = j == 0 ? 0.0 : -2.0 * pj * (S2 - pj * pj) * p.grain_kappa;
-          for (int i = 0; i < 7; ++i) {
-            const double w = weight(7, i);
+          double others = 0;
+          for (int k = 0; k < N; ++k)
+            if (k != j) {
+              const double pk = 0.5 * (1.0 + s->phij[(int64_t)k * n + c]);
+              others += pk * pk;
+            }
+          const double P = j == 0 ? 0.0 : -2.0 * (0.5 * (1.0 + ph)) * others * p.grain_kappa;
+          const double u[3] = {j == 1 ? p.grain_u[0] : 0.0, j == 1 ? p.grain_u[1] : 0.0, j == 1 ? p.grain_u[2] : 0.0};
+          const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+          for (int i = 0; i < 19; ++i) {
+            const double w = weight(19, i);
+            const double eu = E27[i][0] * u[0] + E27[i][1] * u[1] + E27[i][2] * u[2];
             const double en = E27[i][0] * nv[0] + E27[i][1] * nv[1] + E27[i][2] * nv[2];
+            const double geq = w * ph * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
             const double g = s->gj_hlp[j][(int64_t)i * n + c];
-            s->gj_out[j][(int64_t)i * n + c] = g - om * (g - w * ph) + w * P + fo * w * lam * en;
+            s->gj_out[j][(int64_t)i * n + c] = g - om * (g - geq) + w * P + fo * w * lam * en;
           }
         }
       }
@@ -996,8 +1002,8 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
       const int N = p->n_objects;
       s->Ng = N;
       s->phij.assign((size_t)N * n, 0.0);
-      s->gj_out.assign(N, std::vector<double>((size_t)7 * n, 0.0));
-      s->gj_hlp.assign(N, std::vector<double>((size_t)7 * n, 0.0));
+      s->gj_out.assign(N, std::vector<double>((size_t)19 * n, 0.0));
+      s->gj_hlp.assign(N, std::vector<double>((size_t)19 * n, 0.0));
       for (int z = 0; z < s->nz; ++z)
         for (int y = 0; y < s->ny; ++y)
           for (int x = 0; x < s->nx; ++x) {
@@ -1009,7 +1015,7 @@ extern "C" orc_state* orc_create(const mk_params* p, const double* phi0, const d
                   -std::tanh((std::sqrt(dx * dx + dy * dy + dz * dz) - p->obj_radius[j]) / (std::sqrt(2.0) * p->W0));
               s->phij[(int64_t)j * n + c] = ph;
               agg += ph;
-              for (int i = 0; i < 7; ++i) s->gj_out[j][(int64_t)i * n + c] = weight(7, i) * ph;
+              for (int i = 0; i < 19; ++i) s->gj_out[j][(int64_t)i * n + c] = weight(19, i) * ph;
             }
             s->phi[c] = agg;
           }

@@ -37,8 +37,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_struct_sizes():
     lib = A.load()
-    assert lib.mk_abi_version() == 2
-    assert A.C.sizeof(A.MkParams) == 3960
+    assert lib.mk_abi_version() == 3
+    assert A.C.sizeof(A.MkParams) == 3984
     assert A.C.sizeof(A.MkDiag) == 88
 
 

@@ -47,12 +47,17 @@ def test_multigrain_fp64_steps(casedir):
 
 
 def test_multigrain_fp32_and_16bit(casedir):
-    for prec, tol in (("fp32", 1e-5), ("fp16", 5e-3), ("bf16", 3e-2)):
+    # grain 1 relaxes towards a moving equilibrium (u = 0.02): its field keeps
+    # changing, so storage rounding accumulates over the loops instead of
+    # settling with the field, as it does for the grains at rest
+    tols = {"fp32": 5e-5, "fp16": 5e-3, "bf16": 3e-2}
+    errs = {}
+    for prec in tols:
         p, s, o = _pair(casedir, f"mg_{prec}", _case(prec))
         s.advance(60)
         o.advance(60)
-        e = _errs(p, s, o, dphi=False)
-        assert max(e.values()) <= tol, (prec, e)
+        errs[prec] = _errs(p, s, o, dphi=False)
+    assert all(max(errs[k].values()) <= tols[k] for k in tols), errs
 
 
 def test_multigrain_checkpoint_graph_and_grain_errors(casedir, tmp_path):
@@ -108,3 +113,24 @@ def test_multigrain_vtk_and_contour(casedir, tmp_path):
     assert np.array_equal(np.array(block, dtype=float).reshape(s.shape), s.field("grain"))
     pts = s.interface_points()
     assert pts["iso"] == 0.0 and len(pts["xyz"]) > 100
+
+
+@pytest.mark.parametrize("name", ["multigrain_ref_d2q9.npz", "multigrain_ref_d3q19.npz"])
+def test_multigrain_fp64_matches_the_reference_solver(tmp_path, name):
+    # the reference's own mkFluidsUser::propagate / relaxation, compiled with
+    # stand-ins for its closed library (fixtures in tests/golden/); the D2Q9
+    # fixture runs on the device's D3Q19 grain lattices with nz = 1
+    from test_oracle_multigrain_ref import compare, load
+    xml, _, phi, _ = load(name)
+    path = tmp_path / "case.xml"
+    path.write_text(xml)
+    s = Solver(params=case_params(str(path)))
+    assert s.params.grain_u[0] == 0.02  # the reference's moving grain 1
+    state = {"done": 0}
+
+    def run(n):
+        s.advance(n - state["done"])
+        state["done"] = n
+        return [s.grain_field(j).reshape(phi.shape[2:]) for j in range(phi.shape[1])]
+
+    compare(run, name, tol=1e-11)
