@@ -315,7 +315,7 @@ mk_status mk_advance_graph(mk_handle* h, int64_t nsteps) {
     cudaError_t st = cudaGraphLaunch(h->graph[par], e.stream);
     if (st != cudaSuccess) return cuda_fail(h, st, "graph launch");
     e.step += 2;
-    e.launches += 2 * mke::engine_kernels_per_step(e);
+    e.launches += 2 * mke::engine_launches_per_step(e);
     left -= 2;
   }
   if (left) return mk_advance(h, left);
@@ -1038,6 +1038,6 @@ int64_t mk_fluid_cells(const mk_handle* h) {
   return f[0] * f[1] * f[2];
 }
 
-int32_t mk_launches_per_step(const mk_handle* h) { return h ? mke::engine_kernels_per_step(h->e) : 0; }
+int32_t mk_launches_per_step(const mk_handle* h) { return h ? mke::engine_launches_per_step(h->e) : 0; }
 
 }  // extern "C"

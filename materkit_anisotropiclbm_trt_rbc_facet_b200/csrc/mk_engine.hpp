@@ -136,7 +136,9 @@ cudaError_t engine_field_f32(Engine& e, int field);
 
 // One loop.  When `ev` is non-null, ev[2k], ev[2k+1] bracket the k-th kernel.
 cudaError_t engine_step(Engine& e, cudaEvent_t* ev);
+// Kernel phases of one loop (the profiler's slots) and the launches they take.
 int engine_kernels_per_step(const Engine& e);
+int engine_launches_per_step(const Engine& e);
 const char* engine_kernel_name(const Engine& e, int k);
 
 // Compute a macroscopic field of the current state into e.field (device).
