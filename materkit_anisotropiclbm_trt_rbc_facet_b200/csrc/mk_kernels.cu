@@ -597,23 +597,15 @@ __device__ __forceinline__ void mg_phi_cell(const S* __restrict__ Gj, P* __restr
   phij[c] = P(sum);
 }
 
-// phi_j of every fluid cell; a solid cell keeps its aggregate (grain 0's
-// thread copies it).
+// phi_j of every fluid cell.
 template <class S, class P, int PARITY>
-__global__ void __launch_bounds__(256) k_mg_phi(const S* __restrict__ G, P* __restrict__ phij,
-                                                const P* __restrict__ phi_old, P* __restrict__ phi_new, const Geom g,
-                                                int j0) {
+__global__ void __launch_bounds__(256) k_mg_phi(const S* __restrict__ G, P* __restrict__ phij, const Geom g, int j0) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = (int)(blockIdx.z % (unsigned)g.nz);
   const int j = j0 + (int)(blockIdx.z / (unsigned)g.nz);
-  if (x >= g.nx || y >= g.ny) return;
+  if (x >= g.nx || y >= g.ny || !g.fluid(x, y, z)) return;
   const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
-  if (!g.fluid(x, y, z)) {
-    const int64_t c = g.idx(x, y, z);
-    if (j == 0) phi_new[c] = phi_old[c];
-    return;
-  }
   const S* Gj = G + (int64_t)j * 19 * g.stride;
   P* pj = phij + (int64_t)j * ncell;
   if (fastw_cell(g, x, y, z)) {
@@ -625,12 +617,41 @@ __global__ void __launch_bounds__(256) k_mg_phi(const S* __restrict__ G, P* __re
   }
 }
 
+// Per cell, once: the aggregate phi = (N - 1) + sum phi_j into phi_new and
+// S2 = sum_k p_k^2, p = (1 + phi)/2, into plane N of phij (the grains'
+// threads of the collision read it instead of all N order parameters each).
+// A solid cell keeps its aggregate.
+template <class S, class P>
+__global__ void __launch_bounds__(256) k_mg_sums(P* __restrict__ phij, const P* __restrict__ phi_old,
+                                                 P* __restrict__ phi_new, const Geom g, int ngr) {
+  typedef typename Stor<S>::T T;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+  const int64_t c = g.idx(x, y, z);
+  if (!g.fluid(x, y, z)) {
+    phi_new[c] = phi_old[c];
+    return;
+  }
+  T S2 = T(0), agg = T(ngr - 1);
+  for (int q = 0; q < ngr; ++q) {
+    const T fq = T(phij[(int64_t)q * ncell + c]);
+    const T pk = T(0.5) * (T(1) + fq);
+    S2 += pk * pk;
+    agg += fq;
+  }
+  phi_new[c] = P(agg);
+  phij[(int64_t)ngr * ncell + c] = P(S2);
+}
+
 // Grain j of one cell: its D3Q19 gradient, overlap penalty and relaxation.
-// Grain 0's thread also forms the aggregate phi and relaxes the thermal
-// lattice with its latent heat (1/2) dphi.
+// Grain 0's thread also relaxes the thermal lattice with the latent heat
+// (1/2) dphi of the aggregate.
 template <class S, class P, int PARITY, class NB>
 __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phij,
-                                        P* __restrict__ phi_new, const P* __restrict__ phi_old,
+                                        const P* __restrict__ phi_new, const P* __restrict__ phi_old,
                                         P* __restrict__ temp, const int64_t stride, const int64_t ncell, const NB& nb,
                                         const int c, const int j, const MgK<typename Stor<S>::T>& k) {
   typedef typename Stor<S>::T T;
@@ -646,13 +667,7 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
       for (int i = 0; i < 7; ++i) pf_in<S, 7>(Tp, stride, nb, PARITY, c, i);
     }
   }
-  T S2 = T(0), agg = T(k.ngr - 1);
-  for (int q = 0; q < k.ngr; ++q) {
-    const T fq = T(phij[(int64_t)q * ncell + c]);
-    const T pk = T(0.5) * (T(1) + fq);
-    S2 += pk * pk;
-    agg += fq;
-  }
+  const T S2 = T(phij[(int64_t)k.ngr * ncell + c]);
   const P* f = phij + (int64_t)j * ncell;
   const T ph = T(f[c]);
   T gx = T(0), gy = T(0), gz = T(0);
@@ -688,7 +703,6 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
     st_out<S, 19>(Gj, stride, nb, PARITY, c, i, gv[i] - k.om * (gv[i] - w * eq) + w * Pj + w * lam * en);
   }
   if (j != 0) return;
-  phi_new[c] = P(agg);
   // thermal lattice with latent heat (1/2) dphi of the aggregate
   T t[7], dT = T(0);
 #pragma unroll
@@ -696,7 +710,7 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
     t[i] = ld_in<S, 7>(Tp, stride, nb, PARITY, c, i);
     dT += t[i];
   }
-  const T lat = T(0.5) * (T(P(agg)) - T(phi_old[c]));
+  const T lat = T(0.5) * (T(phi_new[c]) - T(phi_old[c]));
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const T w = T(wq<7>(i));
@@ -707,7 +721,7 @@ __device__ __forceinline__ void mg_cell(S* __restrict__ G, S* __restrict__ Tp, c
 
 template <class S, class P, int PARITY>
 __global__ void __launch_bounds__(256)
-    k_mg_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phij, P* __restrict__ phi_new,
+    k_mg_collide(S* __restrict__ G, S* __restrict__ Tp, const P* __restrict__ phij, const P* __restrict__ phi_new,
                  const P* __restrict__ phi_old, P* __restrict__ temp, const Geom g, const MgK<typename Stor<S>::T> k,
                  int j0) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1516,13 +1530,18 @@ void launch_mg(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   for (int j0 = 0; j0 < ngr; j0 += ppl) {
     const dim3 gz(grid.x, grid.y, (unsigned)(e.nz * std::min(ppl, ngr - j0)));
     if (parity == 0)
-      k_mg_phi<S, P, 0><<<gz, block, 0, e.stream>>>(G, phij, phi_old, phi_new, g, j0);
+      k_mg_phi<S, P, 0><<<gz, block, 0, e.stream>>>(G, phij, g, j0);
     else
-      k_mg_phi<S, P, 1><<<gz, block, 0, e.stream>>>(G, phij, phi_old, phi_new, g, j0);
+      k_mg_phi<S, P, 1><<<gz, block, 0, e.stream>>>(G, phij, g, j0);
   }
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
+  }
+  k_mg_sums<S, P><<<grid, block, 0, e.stream>>>(phij, phi_old, phi_new, g, ngr);
+  if (ev) {
+    cudaEventRecord(ev[3], e.stream);
+    cudaEventRecord(ev[4], e.stream);
   }
   for (int j0 = 0; j0 < ngr; j0 += ppl) {
     const dim3 gz(grid.x, grid.y, (unsigned)(e.nz * std::min(ppl, ngr - j0)));
@@ -1531,7 +1550,7 @@ void launch_mg(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
     else
       k_mg_collide<S, P, 1><<<gz, block, 0, e.stream>>>(G, (S*)e.pop1, phij, phi_new, phi_old, (P*)e.temp, g, k, j0);
   }
-  if (ev) cudaEventRecord(ev[3], e.stream);
+  if (ev) cudaEventRecord(ev[5], e.stream);
 }
 
 template <class S>
@@ -1812,7 +1831,8 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
   if ((st = alloc(&e.phi[0], (size_t)e.ncell * e.phi_elem)) != cudaSuccess) return st;
   const bool dend = mkm::dendrite(p.model) || p.model == MK_MODEL_MULTIGRAIN;
   const bool mg = p.model == MK_MODEL_MULTIGRAIN;
-  if ((st = alloc(&e.phij, mg ? (size_t)p.n_objects * e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
+  // N order parameters and the per-cell sum of p_k^2 (plane N)
+  if ((st = alloc(&e.phij, mg ? (size_t)(p.n_objects + 1) * e.ncell * e.phi_elem : 0)) != cudaSuccess) return st;
   if (mg) {
     std::vector<double> gs((size_t)4 * p.n_objects);
     for (int k = 0; k < p.n_objects; ++k) {
@@ -1996,13 +2016,14 @@ static bool fused_mp(const Engine& e) { return e.p.model == MK_MODEL_MULTIPHASE 
 
 int engine_kernels_per_step(const Engine& e) {
   if (mkm::flow_coupled(e.p.model)) return (e.p.inlet && !fd_faces_in_warp(e)) ? 4 : 3;
+  if (e.p.model == MK_MODEL_MULTIGRAIN) return 3;
   return (one_kernel(e) || fused_mp(e)) ? 1 : 2;
 }
 
 int engine_launches_per_step(const Engine& e) {
   if (e.p.model == MK_MODEL_MULTIGRAIN) {
     const int ppl = mg_grains_per_launch(e);
-    return 2 * ((e.p.n_objects + ppl - 1) / ppl);
+    return 2 * ((e.p.n_objects + ppl - 1) / ppl) + 1;
   }
   return engine_kernels_per_step(e);
 }
@@ -2012,6 +2033,10 @@ const char* engine_kernel_name(const Engine& e, int k) {
   if (mkm::flow_coupled(e.p.model)) {
     static const char* const names[4] = {"phi", "flow", "collide", "boundary"};
     return k >= 0 && k < 4 ? names[k] : "";
+  }
+  if (e.p.model == MK_MODEL_MULTIGRAIN) {
+    static const char* const names[3] = {"phi", "sums", "collide"};
+    return k >= 0 && k < 3 ? names[k] : "";
   }
   return k == 0 ? "phi" : "collide";
 }
