@@ -372,10 +372,11 @@ def run_ours(args):
     lib.mk_host_free(hp_out)
     s.close()
 
-    cpu = cpu_ref = None
+    cpu = cpu_ref = cpu_code = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n, budget_s=args.cpu_budget, workload=args.workload)
         cpu_ref = cpu_baseline_reference_structure(n, budget_s=args.cpu_budget, workload=args.workload)
+        cpu_code = cpu_baseline_reference_code(budget_s=args.cpu_budget, workload=args.workload)
 
     if pg is not None:
         pg.barrier()
@@ -433,6 +434,8 @@ def run_ours(args):
     }
     if cpu_ref is not None:
         line["cpu_baseline_reference_structure"] = cpu_ref
+    if cpu_code:
+        line["cpu_baseline_reference_code"] = cpu_code
     print(json.dumps(line), flush=True)
 
 
@@ -607,6 +610,65 @@ def cpu_baseline_reference_structure(n: int, budget_s: float = 20.0, workload: s
             "seconds": round(dt, 2)}
 
 
+def _grain_fields(params) -> np.ndarray:
+    """-tanh((r - R)/(sqrt2 W0)) per grain, x fastest (both case layers' initial order parameters)."""
+    nx, ny, nz = params.nx, params.ny, params.nz
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    out = []
+    for j in range(params.n_objects):
+        cx, cy, cz = params.obj_center[j][0], params.obj_center[j][1], params.obj_center[j][2]
+        r = np.sqrt((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2)
+        out.append(-np.tanh((r - params.obj_radius[j]) / (np.sqrt(2.0) * params.W0)))
+    return np.ascontiguousarray(np.stack(out), dtype=np.float64)
+
+
+REF_CODE_SAMPLE = 64  # edge of the multigrain sample: the reference's nodes take ~4.5 KB each
+
+
+def cpu_baseline_reference_code(budget_s: float = 20.0, workload: str = "multigrain"):
+    """Time the reference's own multigrain solver source (mkFluidsUser::propagate /
+    relaxation, MaterKit/src/mkFluidsUser.cpp:68-299, built into oracle/_ref
+    against stand-ins for its closed library) on the host cores, on the
+    workload's case at 64^3 with periodic faces (the stand-in neighbour
+    wraps).  None for other workloads or where oracle/_ref is not built."""
+    if workload != "multigrain":
+        return None
+    path = os.path.join(ROOT, "oracle", "_ref", "libmgref_q19.so")
+    if not os.path.exists(path):
+        return None
+    import ctypes as C
+    from oracle.orc import load as load_oracle
+
+    lib = C.CDLL(path)
+    lib.mgref_run.argtypes = [C.c_int] * 4 + [C.c_double, C.c_void_p, C.c_int, C.c_void_p]
+    lib.mgref_loop_seconds.restype = C.c_double
+    lib.mgref_set_threads.argtypes = [C.c_int]
+    cores = int(load_oracle().orc_get_threads())
+    lib.mgref_set_threads(cores)
+    n = REF_CODE_SAMPLE
+    params, _ = _oracle_case(workload, n)
+    phi0 = _grain_fields(params)
+    out = np.empty_like(phi0)
+
+    def run(k):
+        if lib.mgref_run(params.nx, params.ny, params.nz, params.n_objects, params.W0, phi0.ctypes.data, k,
+                         out.ctypes.data) != 0:
+            raise RuntimeError("mgref_run refused the case")
+        return lib.mgref_loop_seconds()
+
+    # the reference allocates per-node vectors in every relaxation, so a loop's
+    # time is estimated from two
+    t1 = run(2) / 2.0
+    steps = max(1, min(50, int(budget_s / max(t1, 1e-4))))
+    dt = run(steps)
+    cells = params.ncell()
+    return {"value": round(cells * steps / dt / 1e6, 2), "unit": "MLUPS", "cores": cores, "kind": "reference",
+            "sample": f"{steps} loops of the {n}^3 case with periodic faces (the reference's mkFluidsUser.cpp "
+                      f"multigrain propagate / relaxation compiled with stand-ins for its closed library; node "
+                      f"objects of the reference's layout; set-up not timed)",
+            "seconds": round(dt, 2)}
+
+
 def cpu_baseline(n: int, budget_s: float = 20.0, workload: str = "bubbles"):
     """Time the FP64 OpenMP oracle on the host cores on a bounded sample of the workload."""
     from oracle.orc import Oracle, load as load_oracle
@@ -638,20 +700,31 @@ def run_reference(args):
     lib = load_oracle()
     n = args.size
     wl = WORKLOADS[args.workload]
-    params, fields = _oracle_case(args.workload, n)
-    o = Oracle(params, **fields)
-    t0 = time.perf_counter()
-    o.advance(1)  # one untimed warm-up loop
-    t1 = time.perf_counter() - t0
-    # each step is one full loop; the number of timed loops is capped so the
-    # whole run stays within the budget
-    steps = max(1, min(args.steps, int(args.ref_budget / max(t1, 1e-3))))
-    t0 = time.perf_counter()
-    o.advance(steps)
-    dt = time.perf_counter() - t0
-    cells = params.ncell()
-    mlups = cells * steps / dt / 1e6
-    cores = int(lib.orc_get_threads())
+    code = cpu_baseline_reference_code(budget_s=args.ref_budget, workload=args.workload)
+    if code is not None:
+        # the reference's own multigrain source on its bounded sample (see there)
+        mlups, dt, cores = code["value"], code["seconds"], code["cores"]
+        steps = max(1, int(round(mlups * 1e6 * dt / REF_CODE_SAMPLE ** 3)))
+        cells = n ** 3
+        kind, sample = "reference", code["sample"]
+    else:
+        params, fields = _oracle_case(args.workload, n)
+        o = Oracle(params, **fields)
+        t0 = time.perf_counter()
+        o.advance(1)  # one untimed warm-up loop
+        t1 = time.perf_counter() - t0
+        # each step is one full loop; the number of timed loops is capped so the
+        # whole run stays within the budget
+        steps = max(1, min(args.steps, int(args.ref_budget / max(t1, 1e-3))))
+        t0 = time.perf_counter()
+        o.advance(steps)
+        dt = time.perf_counter() - t0
+        cells = params.ncell()
+        mlups = cells * steps / dt / 1e6
+        cores = int(lib.orc_get_threads())
+        kind = "port"
+        sample = (f"{steps} loops of {_sample_name(args.workload, n)} (requested {args.steps}); the reference's own "
+                  f"solver is a closed Windows DLL, so this is the FP64 OpenMP restatement")
     line = {
         "metric": wl["metric"], "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws, "steps": steps, "warmup": 1,
         "ms_per_step": round(dt / steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
@@ -659,10 +732,8 @@ def run_reference(args):
         "config": {"workload": wl["workload"].format(n=n), "cells": cells, "storage": "fp64",
                    "parallelism": f"{cores} host threads"},
         "impl": "reference",
-        "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": cores, "kind": "port",
-                         "sample": f"{steps} loops of {_sample_name(args.workload, n)} (requested {args.steps}); "
-                                   f"the reference's own "
-                                   f"solver is a closed Windows DLL, so this is the FP64 OpenMP restatement"},
+        "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": cores, "kind": kind,
+                         "sample": sample},
         "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

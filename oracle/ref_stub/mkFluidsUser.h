@@ -2,9 +2,10 @@
 // solver, MaterKit/src/mkFluidsUser.cpp, outside its closed library.
 //
 // Test infrastructure: this header and ref_stub.cpp build oracle/_ref only
-// (the fixture generator of tests/golden/make_multigrain_ref.py); nothing in
-// the product includes them.  The reference's mkFluidsUser.cpp is compiled
-// where it lies and includes "mkFluidsUser.h" by name, so this file carries
+// (the fixture generator tests/golden/make_multigrain_ref.py and bench.py's
+// CPU baseline legs load it); nothing in the product includes them.  The
+// reference's mkFluidsUser.cpp is compiled where it lies and includes
+// "mkFluidsUser.h" by name, so this file carries
 // exactly the names that source uses (classes, members and functions of
 // MaterKit/inc/mkFluidsLBM.h, mkNode.h, mkLattice.h, mkPhaseField.h and
 // mkFluidsUser.h) and nothing of the library itself: the bodies of the

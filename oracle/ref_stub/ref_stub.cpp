@@ -3,8 +3,9 @@
 // calls, restated from the published forms, and a C entry point that runs
 // that solver on given initial order parameters.  Test infrastructure: built
 // into oracle/_ref by oracle/Makefile (target `ref`) together with the
-// reference's mkFluidsUser.cpp, compiled where it lies; only the fixture
-// generator tests/golden/make_multigrain_ref.py loads the result.
+// reference's mkFluidsUser.cpp, compiled where it lies; the fixture generator
+// tests/golden/make_multigrain_ref.py and bench.py's CPU baseline legs load
+// the result.
 //
 // Restated here (not readable in the reference):
 //   lattice        D2Q9 (QF 9) or D3Q19 (QF 19) velocities and weights, cs^2 = 1/3
@@ -15,10 +16,11 @@
 //   neighbor       periodic wrap on every axis
 //   reset_flags    leaves every node fluid (the multigrain case has no solid)
 //   epsilon        1e-6, the regularisation of the grain normal
-// The harness runs one OpenMP thread: relaxation() keeps omega_g firstprivate
-// and sets it after its first use, so the first node each thread relaxes sees
-// omega_g = 1 in its source term (thread-count dependent in the reference);
-// the fixtures keep that node in pure melt, where the source vanishes.
+// The harness runs one OpenMP thread unless mgref_set_threads says otherwise:
+// relaxation() keeps omega_g firstprivate and sets it after its first use, so
+// the first node each thread relaxes sees omega_g = 1 in its source term
+// (thread-count dependent in the reference); the fixtures exclude the light
+// cone of that node.  Timing runs may use every host thread.
 #include <omp.h>
 
 #include <cstring>
@@ -28,6 +30,8 @@
 namespace {
 double g_W0 = 1.0;
 const mkLattice* g_lat = nullptr;
+int g_threads = 1;
+double g_loop_seconds = 0.0;
 }  // namespace
 
 mkReal mkPDFs::density() const {
@@ -130,9 +134,15 @@ void mkFluidsLBM::reset_flags() {}
 // lattice cannot run (QF 9 needs nz = 1).
 extern "C" int mgref_lattice(void) { return QF; }
 
+// OpenMP threads of the next runs (1 by default: the fixtures' setting).
+extern "C" void mgref_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+
+// Wall time of the propagate + relaxation loops of the last run, seconds.
+extern "C" double mgref_loop_seconds(void) { return g_loop_seconds; }
+
 extern "C" int mgref_run(int nx, int ny, int nz, int ngr, double W0, const double* phi0, int loops, double* out) {
   if (nx < 1 || ny < 1 || nz < 1 || ngr < 1 || (QF == 9 && nz != 1)) return 1;
-  omp_set_num_threads(1);
+  omp_set_num_threads(g_threads);
   g_W0 = W0;
   const int64_t n = (int64_t)nx * ny * nz;
   std::vector<mkNode> nodes((size_t)n);
@@ -162,10 +172,12 @@ extern "C" int mgref_run(int nx, int ny, int nz, int ngr, double W0, const doubl
         q.phi = agg;
         q.g_out = q.getEquPDFs(agg, rest);
       }
+  const double t0 = omp_get_wtime();
   for (int t = 0; t < loops; ++t) {
     u.propagate();
     u.relaxation();
   }
+  g_loop_seconds = omp_get_wtime() - t0;
   for (int x = 0; x < nx; ++x)
     for (int y = 0; y < ny; ++y)
       for (int z = 0; z < nz; ++z) {
