@@ -122,7 +122,7 @@ def defaults() -> MkParams:
     p.eps4, p.W0, p.lambda_, p.delta = 0.05, 1.5, 10.0, 0.55
     p.D, p.D_s, p.k_part = 0.1, 1e-4, 0.15
     p.at_coef = 1.0 / (2.0 * math.sqrt(2.0))
-    p.tau0 = 0.6267 * p.lambda_ * p.W0 ** 2 / p.D
+    p.tau0 = 0.6267 * p.lambda_ * p.W0 * p.W0 / p.D
     p.aniso = ANISO["cubic"]
     p.wall_axis = -1
     p.grain_kappa = 1.0
@@ -617,7 +617,7 @@ def _b200(b: Node, p: MkParams) -> None:
     # tau0 from the thin-interface relation tau0 = 0.6267 lambda W0^2 / D unless given
     tau0 = number(b.child("tau0")) if b.child("tau0") is not None else -1.0
     if any(b.child(t) is not None for t in ("W0", "lambda", "diffusivity")) or tau0 > 0:
-        p.tau0 = tau0 if tau0 > 0 else 0.6267 * p.lambda_ * p.W0 ** 2 / p.D
+        p.tau0 = tau0 if tau0 > 0 else 0.6267 * p.lambda_ * p.W0 * p.W0 / p.D
     for tag, field in (("force", "force"), ("velocity", "u0"), ("grainVelocity", "grain_u")):
         if b.child(tag) is not None:
             v = numbers(b.child(tag))
