@@ -739,6 +739,43 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_slabs(args):
+    """Cost of the z-slab decomposition of one multiphase domain, measured in
+    one process on one GPU: the bubble case advanced whole and as 2 and 4
+    slabs (ghost planes, the FILL / PHI / RETURN exchanges as in-library
+    copies, the masked return merge), milliseconds per loop from the host
+    clock with the device synchronised on both sides (the exchange protocol is
+    host-driven).  The slabs share this GPU's compute, so the figure bounds
+    the protocol's cost; it is not a multi-GPU scaling number.  Prints one
+    JSON line."""
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import Solver, case_params
+    from materkit_anisotropiclbm_trt_rbc_facet_b200 import slab as S
+
+    n, K = args.size, args.steps
+    params = case_params(_case_path(args.precision, n, "bubbles"))
+
+    def timed(step):
+        step(args.warmup)
+        t0 = time.perf_counter()
+        step(K)
+        return (time.perf_counter() - t0) / K * 1e3
+
+    whole = Solver(params=params)
+    out = {"whole": round(timed(lambda k: (whole.advance(k), whole.sync())), 4)}
+    whole.close()
+    for nr in (2, 4):
+        slabs = [S.Slab(params, r, nr) for r in range(nr)]
+        out[f"slabs_{nr}"] = round(timed(lambda k: (S.advance_local(slabs, k), [s.sync() for s in slabs])), 4)
+        for s in slabs:
+            s.close()
+    line = {"metric": "ms per loop, z-slab decomposition of one domain in one process", "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "steps": K, "warmup": args.warmup, "dtype": args.precision,
+            "data": "synthetic", "config": {"workload": f"multiphase Allen-Cahn bubbles {n}^3", "cells": n ** 3},
+            "ms_per_loop": out,
+            "overhead": {k: round(v / out["whole"] - 1.0, 4) for k, v in out.items() if k != "whole"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_accuracy(args):
     """Reduced-precision accuracy of the bubble case at full size: the case
     advanced `--accuracy-loops` loops (default 10,000) with FP64, FP32, FP16
@@ -800,6 +837,8 @@ def main():
     ap.add_argument("--accuracy", action="store_true",
                     help="reduced-precision accuracy of the bubble case vs FP64 storage (not a timing run)")
     ap.add_argument("--accuracy-loops", type=int, default=10000)
+    ap.add_argument("--slabs", action="store_true",
+                    help="cost of the z-slab decomposition in one process on one GPU (not a timing run of the step)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -810,6 +849,8 @@ def main():
         args.size = wl["size"]
     if args.accuracy:
         run_accuracy(args)
+    elif args.slabs:
+        run_slabs(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble":
