@@ -95,6 +95,27 @@ def test_multiphase_flat_interface_stays_tanh(casedir):
     assert np.max(np.abs(o.field("uz"))) < 1e-5
 
 
+def test_multiphase_static_drop_obeys_laplace(casedir):
+    # A gas drop at rest in liquid (no gravity, periodic box).  The model's
+    # momentum balance is rho du/dt = -grad(cs^2 rho p*) + mu grad(phi) + rho g,
+    # so the hydrodynamic pressure is p = cs^2 rho p*; its jump across the
+    # interface is 2 sigma / R (Laplace), within the diffuse-interface error
+    # that shrinks as W / R does (R the radius of the drop's gas volume).
+    ratio = {}
+    for R in (7.0, 10.0):
+        p = _mp(casedir, f"mp_laplace_{int(R)}", n=32, bubbles=1, rmin=R, rmax=R, width=3.0, gz=0.0, loops=1,
+                boundary="periodic periodic periodic")
+        o = Oracle(p, phi=initial_field(p, "phi"))
+        o.advance(1200)
+        phi, rho, ps = o.field("phi"), o.field("rho"), o.field("pressure")
+        pres = rho * ps / 3.0
+        r_eff = (3.0 * (1.0 - phi).sum() / (4.0 * np.pi)) ** (1.0 / 3.0)
+        jump = pres[phi < 0.01].mean() - pres[phi > 0.99].mean()
+        ratio[R] = jump * r_eff / (2.0 * p.sigma)
+    assert all(abs(v - 1.0) < 0.12 for v in ratio.values()), ratio
+    assert abs(ratio[10.0] - 1.0) < abs(ratio[7.0] - 1.0), ratio
+
+
 def test_thermal_diffusion_variance_rate(casedir):
     # No seed: phi = -1 everywhere, so T obeys pure D3Q7 diffusion; the
     # variance of a Gaussian grows by 2 D per step along each axis.
