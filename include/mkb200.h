@@ -134,7 +134,8 @@ typedef enum mk_field {
   MK_FIELD_C = 5,        /* solute: supersaturation U of the dilute alloy    */
   MK_FIELD_PHI = 6,      /* order parameter                                  */
   MK_FIELD_FLAG = 7,     /* node flag (as double)                            */
-  MK_FIELD_PRESSURE = 8, /* normalised pressure p* (multiphase)              */
+  MK_FIELD_PRESSURE = 8, /* normalised pressure p* (multiphase); the         *
+                          * hydrodynamic pressure is rho p* / 3             */
   MK_FIELD_DPHI = 9,     /* phi(n) - phi(n-1), the latent-heat driver        */
   MK_FIELD_GRAIN = 10    /* grain id (seed index)                            */
 } mk_field;
