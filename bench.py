@@ -294,6 +294,7 @@ def run_ours(args):
         prof = s.profile(min(K, 50), wl.get("slot", "collide"))
         fused = args.workload == "bubbles" and s.fused
         rows = args.workload == "bubbles" and s.row_staged
+        tile = args.workload == "bubbles" and bool(s.tuning.get("phi_tile", 0))
         # the fused multiphase loop is one launch, the flow model has no phi kernel
         prof_phi = {"kernel_ms": 0.0} if (fused or args.workload == "poiseuille") else s.profile(min(K, 50), "phi")
         fluid = s.fluid_cells()
@@ -320,7 +321,9 @@ def run_ours(args):
             "phi_ms": prof_phi["kernel_ms"] / launches, "collide_gbs": achieved, "collide_frac": achieved / peak,
             "collide_bytes_per_launch": collide_bytes, "clocks": clk.summary(), "n_bad": d["n_bad"],
             "launches_per_step": s.launches_per_step(), "tune": tune, "fused": fused, "row_staged": rows,
-            "kernel": "k_mp_wave" if fused else ("k_mp_rows" if rows else wl["kernel"]), **extra,
+            "phi_tile": tile,
+            "kernel": "k_mp_wave" if fused else ("k_mp_rows" if rows else ("k_mp_collide_tma" if tile else wl["kernel"])),
+            **extra,
         }
         if prec == args.precision:
             main = (params, s)
@@ -420,7 +423,8 @@ def run_ours(args):
                          **({"dend_ms": round(v["dend_ms"], 4), "dend_frac": round(v["dend_frac"], 4)}
                             if "dend_ms" in v else {}),
                          "tuned": {"block": list(v["tune"]["block"]), "minb": v["tune"]["minb"],
-                                   "fused": v["fused"], "row_staged": v["row_staged"]}, "kernel": v["kernel"],
+                                   "fused": v["fused"], "row_staged": v["row_staged"], "phi_tile": v["phi_tile"]},
+                         "kernel": v["kernel"],
                          "speedup_vs_fp32": round(v["mlups"] / results["fp32"]["mlups"], 3)
                          if "fp32" in results else None}
                      for k, v in results.items()},

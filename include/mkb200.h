@@ -327,6 +327,9 @@ typedef struct mk_tuning {
                                 multiphase also 3, 4, 5: registers capped at 112, 96, 80 */
   int32_t fused;             /* multiphase: the fused one-launch loop (mk_set_fused) */
   int32_t row_staged;        /* multiphase: the row-staged collision (mk_set_row_staging) */
+  int32_t phi_tile;          /* multiphase: the collision stages each block's phi tile and its one-cell
+                                halo into shared memory with one TMA tensor load (64 x 4 blocks; needs
+                                nx a multiple of 4); at most one of fused, row_staged, phi_tile */
 } mk_tuning;
 mk_status mk_get_tuning(const mk_handle* h, mk_tuning* out);
 /* MK_ERR_ARG for a shape or a form the case does not admit (nothing changed). */

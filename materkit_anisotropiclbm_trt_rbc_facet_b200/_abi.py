@@ -118,7 +118,7 @@ class MkSlabXfer(C.Structure):
 
 class MkTuning(C.Structure):
     _fields_ = [("block_x", C.c_int32), ("block_y", C.c_int32), ("minb", C.c_int32), ("fused", C.c_int32),
-                ("row_staged", C.c_int32)]
+                ("row_staged", C.c_int32), ("phi_tile", C.c_int32)]
 
     def to_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

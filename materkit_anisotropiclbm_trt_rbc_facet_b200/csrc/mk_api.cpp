@@ -452,6 +452,7 @@ mk_status mk_get_tuning(const mk_handle* h, mk_tuning* out) {
   out->minb = e.minb;
   out->fused = e.wave_ok && e.wave ? 1 : 0;
   out->row_staged = e.rows_ok && e.rows ? 1 : 0;
+  out->phi_tile = e.tma_ok && e.tma ? 1 : 0;
   return MK_OK;
 }
 
@@ -464,19 +465,22 @@ mk_status mk_set_tuning(mk_handle* h, const mk_tuning* t) {
   };
   if (t->block_x < 32 || t->block_x % 32 != 0 || t->block_y < 1 || t->block_x * t->block_y > 1024)
     return bad("block shape must be a multiple of 32 in x and at most 1024 threads");
-  if ((t->fused != 0 && t->fused != 1) || (t->row_staged != 0 && t->row_staged != 1))
-    return bad("fused and row_staged are 0 or 1");
-  if (t->fused && t->row_staged) return bad("at most one of fused and row_staged");
+  if ((t->fused != 0 && t->fused != 1) || (t->row_staged != 0 && t->row_staged != 1) ||
+      (t->phi_tile != 0 && t->phi_tile != 1))
+    return bad("fused, row_staged and phi_tile are 0 or 1");
+  if (t->fused + t->row_staged + t->phi_tile > 1) return bad("at most one of fused, row_staged and phi_tile");
   const int mb_max = e.p.model == MK_MODEL_MULTIPHASE ? 5 : 2;
   if (t->minb < 1 || t->minb > mb_max) return bad("minb must be 1 or 2 (multiphase: 1 to 5)");
   if (t->fused && !e.wave_ok) return bad("this case does not admit the fused multiphase loop");
   if (t->row_staged && !e.rows_ok) return bad("this case does not admit the row-staged collision");
+  if (t->phi_tile && !e.tma_ok) return bad("this case does not admit the TMA phi tile (nx a multiple of 4, no slab)");
   if (t->fused && e.slab) return slab_refuse(h, "mk_set_tuning (fused)");
   e.block_x = t->block_x;
   e.block_y = t->block_y;
   e.minb = t->minb;
   e.wave = t->fused;
   e.rows = t->row_staged;
+  e.tma = t->phi_tile;
   for (auto& g : h->graph)
     if (g) {
       cudaGraphExecDestroy(g);

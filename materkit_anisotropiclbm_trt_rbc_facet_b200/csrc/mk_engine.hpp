@@ -84,6 +84,13 @@ struct Engine {
   int rows;              // 1: the collision runs row-staged
   int rows_ns, rows_grid, rows_threads;
   size_t rows_stage, rows_smem;
+  // collision with its phi tile (and halo) staged by one TMA tensor load per
+  // block: the case admits it (the map encoded: nx a multiple of 4, no
+  // slab), the form is chosen, and the 3-D tensor map over phi (the driver's
+  // 128-byte CUtensorMap)
+  int tma_ok;
+  int tma;
+  alignas(64) unsigned char tma_map[128];
   // dynamic solids of a multiphase flow coupled to a dendrite
   // (mk_update_geometry): the solid flags, the fluid cells next to a solid,
   // and the flags of the next update, applied at the next even loop count

@@ -1895,8 +1895,9 @@ cudaError_t engine_alloc(Engine& e, const mk_params& p, int device, int block_x,
       if ((st = alloc((void**)&e.wave_flags, (size_t)e.wave_sx * e.wave_sy * sizeof(unsigned))) != cudaSuccess) return st;
       e.wave = 0;  // the two-kernel loop until mk_set_fused or the autotuner chooses the fused one
     }
-    // the error word of the bounded waits (fused loop, row-staged collision)
-    if (e.wave_ok || e.rows_ok)
+    // the error word of the bounded waits (fused loop, row-staged collision,
+    // TMA phi tile)
+    if (e.wave_ok || e.rows_ok || e.tma_ok)
       if ((st = alloc((void**)&e.wave_err, sizeof(int))) != cudaSuccess) return st;
     e.rows = 0;
   }
@@ -2171,7 +2172,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   // multiphase collision 3, 4, 5 (registers capped at 112, 96, 80)
   const int nmb = e.p.model == MK_MODEL_MULTIPHASE ? 5 : 1;
   double best = 1e300;
-  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0, brows = 0;
+  int bbx = bx0, bby = by0, bmb = mb0, ncand = 0, bwave = 0, brows = 0, btma = 0;
   // time the configuration now in e (warm-up of both AA parities, then the
   // faster of two timed repeats: one slow repeat must not decide), restore
   // the state and keep the configuration if it is the fastest so far
@@ -2197,6 +2198,7 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
       bmb = e.minb;
       bwave = e.wave;
       brows = e.rows;
+      btma = e.tma;
     }
     e.step = step0;
     e.phi_cur = cur0;
@@ -2204,14 +2206,16 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
     if (st == cudaSuccess) st = copy(false);
   };
   // candidate -1: the fused multiphase loop (its tiling is fixed by the case);
-  // candidate -2: the row-staged collision (the block shape is the phi kernel's)
-  for (int si = -2; si < 9 && st == cudaSuccess; ++si) {
-    if ((si == -1 && !e.wave_ok) || (si == -2 && !e.rows_ok)) continue;
+  // candidate -2: the row-staged collision, -3: the TMA phi tile (the block
+  // shape given is the phi kernel's)
+  for (int si = -3; si < 9 && st == cudaSuccess; ++si) {
+    if ((si == -1 && !e.wave_ok) || (si == -2 && !e.rows_ok) || (si == -3 && !e.tma_ok)) continue;
     const int bx = si < 0 ? bx0 : shapes[si][0];
     if (si >= 0 && bx > 32 && bx / 2 >= e.nx) continue;  // no wider than the row
     for (int mb = 1; mb <= (si < 0 ? 1 : nmb) && st == cudaSuccess; ++mb) {
       e.wave = si == -1 ? 1 : 0;
       e.rows = si == -2 ? 1 : 0;
+      e.tma = si == -3 ? 1 : 0;
       e.block_x = bx;
       e.block_y = si < 0 ? by0 : shapes[si][1];
       e.minb = (nmb > 1 && si >= 0) ? mb : mb0;
@@ -2231,12 +2235,13 @@ cudaError_t engine_autotune(Engine& e, int trial_steps, TuneResult* out) {
   e.minb = bmb;
   e.wave = bwave;
   e.rows = brows;
+  e.tma = btma;
   if (out) {
     // a fused multiphase loop has no block shape or occupancy variant: 0, 0, 0;
     // the row-staged collision has no occupancy variant: minb 0
     out->block_x = bwave ? 0 : bbx;
     out->block_y = bwave ? 0 : bby;
-    out->minb = (bwave || brows) ? 0 : bmb;
+    out->minb = (bwave || brows || btma) ? 0 : bmb;
     out->ms_per_step = best;
     out->candidates = ncand;
   }

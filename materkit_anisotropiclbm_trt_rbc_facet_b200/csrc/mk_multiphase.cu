@@ -2,6 +2,8 @@
 // the collision kernel, and the fused one-launch loop, with their launchers
 // (mkFluidsMultiphase::propagate/relaxation, mkFluidsMultiphase.h:52-57;
 // getEquPDFsLiang/PhiLiang, mkNode.h:38-40).
+#include <cuda.h>  // CUtensorMap and its encoding enums (resolved through the runtime)
+
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
@@ -818,6 +820,126 @@ inline RowPlan row_plan(const mke::Engine& e, const Geom& g) {
   return rp;
 }
 
+// ------------------------------------------- TMA-staged phi tile (phi_tile)
+// The two-kernel loop's collision with the phi stencil read from shared
+// memory: one 3-D TMA tensor load per block stages the block's phi tile and
+// its one-cell halo (x rounded out to 16 bytes, y +-1, z +-1) for a 64 x 4
+// block in one plane.  Interior cells (the Fast path, no periodic wrap along
+// x) read their 19 phi values from the tile; every other cell reads global
+// memory as in k_mp_collide.  The values are the same, so the result is
+// bit-identical.  The tensor map covers this GPU's own phi buffer; no
+// multicast.
+constexpr int kTileX = 64, kTileY = 4, kTileHX = 4;
+constexpr int kTileW = kTileX + 2 * kTileHX, kTileH = kTileY + 2;
+
+// The stencil's first access (center) waits for the tile, so the cell's
+// population loads, issued before it, overlap the tile's transfer; a wait
+// that gives up (recorded in *err) falls back to global memory.
+template <class P>
+struct PhiTile {
+  const P* t;
+  uint64_t* bar;
+  int* err;
+  const P* phi;  // global phi, the fallback
+  const Fast& fa;
+  int lx, ly;  // the cell's column and row in the tile
+  mutable bool tile_ok;
+  __device__ __forceinline__ P center() const {
+    tile_ok = mkw::mbar_wait(bar, 0, err);
+    return tile_ok ? t[(kTileH + ly) * kTileW + lx] : phi[fa.c];
+  }
+  __device__ __forceinline__ P at(int dx, int dy, int dz) const {
+    return tile_ok ? t[((1 + dz) * kTileH + ly + dy) * kTileW + lx + dx] : __ldg(phi + fa.idx(dx, dy, dz));
+  }
+};
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(kTileX* kTileY, 2)
+    k_mp_collide_tma(S* __restrict__ G, S* __restrict__ H, float* __restrict__ H0, const P* __restrict__ phi,
+                     const Geom g, const MpK<typename Stor<S>::T> k, const __grid_constant__ CUtensorMap tmap,
+                     int* err) {
+  __shared__ alignas(128) P tile[3 * kTileH * kTileW];
+  __shared__ alignas(8) uint64_t bar;
+  const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY, z = blockIdx.z;
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  if (lead) {
+    mkw::mbar_init(&bar, 1);
+    mkw::fence_mbar_init();
+  }
+  __syncthreads();
+  if (lead) {
+    mkw::mbar_arrive_expect(&bar, (unsigned)sizeof(tile));
+    mkw::tma_load_3d(tile, &tmap, x0 - kTileHX, y0 - 1, z - 1, &bar);
+  }
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x < g.nx && y < g.ny && g.fluid(x, y, z)) {
+    if (fast_cell(g, x, y, z)) {
+      const Fast fa = make_fast(g, x, y, z);
+      if (x >= 1 && x <= g.nx - 2)
+        mp_collide_cell<S, P, PARITY>(
+            G, H, H0, PhiTile<P>{tile, &bar, err, phi, fa, (int)threadIdx.x + kTileHX, (int)threadIdx.y + 1, false},
+            g.stride, fa, fa.c, k, GlobalLd<S, PARITY, Fast>{G, H, H0, g.stride, fa, fa.c});
+      else
+        mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Fast>{phi, fa, fa.c}, g.stride, fa, fa.c, k,
+                                      GlobalLd<S, PARITY, Fast>{G, H, H0, g.stride, fa, fa.c});
+    } else {
+      const Nbr nb(g, x, y, z);
+      const int c = nb.idx(0, 0, 0);
+      mp_collide_cell<S, P, PARITY>(G, H, H0, PhiGlobal<P, Nbr>{phi, nb, c}, g.stride, nb, c, k,
+                                    GlobalLd<S, PARITY, Nbr>{G, H, H0, g.stride, nb, c});
+    }
+  }
+  // the block's shared memory must outlive the tile's transfer, whether or
+  // not any of its cells read the tile (bounded)
+  if (lead) mkw::mbar_wait(&bar, 0, err);
+}
+
+// The tensor map over phi (nx x ny x nz, x fastest): admitted when the row
+// stride is a multiple of 16 bytes (nx a multiple of 4) and the driver
+// encodes the map; slabs are not admitted.
+template <class P>
+void tma_config(mke::Engine& e) {
+  e.tma_ok = 0;
+  e.tma = 0;
+  if (e.slab || e.nx % 4 != 0 || e.nx < 4) return;
+  typedef CUresult (*Encode)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                             const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                             CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static const Encode encode = []() -> Encode {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return (Encode)fn;
+  }();
+  if (!encode) return;
+  const cuuint64_t dims[3] = {(cuuint64_t)e.nx, (cuuint64_t)e.ny, (cuuint64_t)e.nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)e.nx * sizeof(P), (cuuint64_t)e.nx * e.ny * sizeof(P)};
+  const cuuint32_t box[3] = {(cuuint32_t)kTileW, (cuuint32_t)kTileH, 3u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r =
+      encode(reinterpret_cast<CUtensorMap*>(e.tma_map),
+             sizeof(P) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, e.phi[0], dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  e.tma_ok = r == CUDA_SUCCESS ? 1 : 0;
+}
+
+template <class S>
+void launch_mp_tma(mke::Engine& e, int parity, const Geom& g, const MpK<typename Stor<S>::T>& k) {
+  typedef typename PhiOf<S>::type P;
+  const dim3 grid((e.nx + kTileX - 1) / kTileX, (e.ny + kTileY - 1) / kTileY, e.nz), block(kTileX, kTileY);
+  const CUtensorMap& m = *reinterpret_cast<const CUtensorMap*>(e.tma_map);
+  S* G = (S*)e.pop0;
+  S* H = (S*)e.pop1;
+  const P* phi = (const P*)e.phi[0];
+  if (parity == 0)
+    k_mp_collide_tma<S, P, 0><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k, m, e.wave_err);
+  else
+    k_mp_collide_tma<S, P, 1><<<grid, block, 0, e.stream>>>(G, H, e.rest1, phi, g, k, m, e.wave_err);
+}
+
 template <class S>
 void launch_mp_rows(mke::Engine& e, int parity, const Geom& g, const MpK<typename Stor<S>::T>& k) {
   typedef typename PhiOf<S>::type P;
@@ -953,6 +1075,9 @@ void launch_mp(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   if (e.rows && e.rows_ok) {
     const Geom g = make_geom(e);
     launch_mp_rows<S>(e, parity, g, mp_coef<T>(e.p, refs_of(e.p)));
+  } else if (e.tma && e.tma_ok) {
+    const Geom g = make_geom(e);
+    launch_mp_tma<S>(e, parity, g, mp_coef<T>(e.p, refs_of(e.p)));
   } else {
     launch_collide_range<S>(e, parity, grid, block, 0, e.nz, e.stream);
   }
@@ -1080,18 +1205,22 @@ void mp_configure(Engine& e) {
     case MK_PREC_FP64:
       wave_config<double>(e);
       rows_config<double>(e);
+      tma_config<double>(e);
       break;
     case MK_PREC_FP32:
       wave_config<float>(e);
       rows_config<float>(e);
+      tma_config<float>(e);
       break;
     case MK_PREC_FP16:
       wave_config<__half>(e);
       rows_config<__half>(e);
+      tma_config<float>(e);
       break;
     default:
       wave_config<__nv_bfloat16>(e);
       rows_config<__nv_bfloat16>(e);
+      tma_config<float>(e);
       break;
   }
 }

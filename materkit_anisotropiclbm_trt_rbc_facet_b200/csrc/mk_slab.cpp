@@ -338,6 +338,8 @@ mk_status mk_create_slab(const mk_params* global, int32_t rank, int32_t nranks, 
   e.nranks = nranks;
   e.wave = 0;
   e.wave_ok = 0;  // the fused loop has no exchange points
+  e.tma_ok = 0;   // the TMA phi tile is validated on whole domains only
+  e.tma = 0;
   const size_t halo_bytes = (size_t)20 * global->nx * global->ny * e.elem;
   if ((st = cudaMalloc(&e.slab_halo, halo_bytes)) != cudaSuccess ||
       (st = cudaMemsetAsync(e.slab_halo, 0, halo_bytes, e.stream)) != cudaSuccess) {

@@ -105,6 +105,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// One 3-D tile of a tensor map (global) into this CTA's shared memory,
+// completing on `bar`; coordinates (x, y, z) of the tile's first element,
+// x times the element size a multiple of 16 bytes; elements outside the
+// tensor read as zero.  `tmap` is the address of a __grid_constant__ kernel
+// parameter.  No multicast.
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
 }  // namespace mkw
 
 #endif

@@ -120,7 +120,7 @@ def test_tuning_roundtrip_and_checks(casedir):
     p = case_params(_case(casedir, "walls_z", "fp32"))
     s = Solver(params=p)
     t = s.tuning
-    assert set(t) == {"block_x", "block_y", "minb", "fused", "row_staged"}
+    assert set(t) == {"block_x", "block_y", "minb", "fused", "row_staged", "phi_tile"}
     s.tuning = {"block_x": 32, "block_y": 4, "minb": 1, "row_staged": 1}
     assert s.tuning == dict(t, block_x=32, block_y=4, minb=1, row_staged=1)
     for bad in ({"block_x": 48}, {"block_x": 64, "block_y": 32}, {"minb": 6}, {"minb": 0}, {"row_staged": 2}):
