@@ -402,12 +402,12 @@ mk_status mk_time_advance(mk_handle* h, int64_t nsteps, int32_t use_graph, doubl
 
 /* Launch-shape autotuner: times `trial_steps` loops of each candidate block
  * shape and occupancy variant of the step's kernels, and for a multiphase
- * case also the fused one-launch loop and the row-staged collision, on a
- * saved copy of the state (restored afterwards, so the simulation is
- * unchanged) and keeps the fastest.  Outputs may be NULL; block_x = block_y =
- * minb = 0 report that the fused loop won, minb = 0 with a block shape that
- * the row-staged collision won (the shape is the phi kernel's); mk_get_tuning
- * gives the whole choice. */
+ * case also the fused one-launch loop, the row-staged collision and the TMA
+ * phi-tile collision, on a saved copy of the state (restored afterwards, so
+ * the simulation is unchanged) and keeps the fastest.  Outputs may be NULL;
+ * block_x = block_y = minb = 0 report that the fused loop won, minb = 0 with a
+ * block shape that the row-staged or the phi-tile collision won (the shape is
+ * the phi kernel's); mk_get_tuning gives the whole choice. */
 mk_status mk_autotune(mk_handle* h, int32_t trial_steps, int32_t* block_x, int32_t* block_y, int32_t* minb,
                       double* ms_per_step);
 
