@@ -66,7 +66,8 @@ typedef enum mk_model {
   MK_MODEL_FLOW_DENDRITE = 5,    /* thermal dendrite growing in a flow: porous bounce-back of the
                                     flow by the solid fraction, thermal lattice advected, inflow /
                                     outflow faces, run_flow_thermal_dendrite (MaterKit.cpp:467-527) */
-  MK_MODEL_MULTIGRAIN = 6,       /* one conservative Allen-Cahn order parameter per seed (grain) with
+  MK_MODEL_MULTIGRAIN = 6,       /* one conservative Allen-Cahn order parameter per seed (grain) on
+                                    a D3Q19 lattice (the reference's D2Q9 on a one-cell periodic z) with
                                     a pairwise overlap penalty, aggregate phi = (N - 1) + sum phi_j,
                                     thermal ADE with latent heat: run_multiPhaseField
                                     (MaterKit.cpp:529-571), mkFluidsUser::propagate/relaxation
