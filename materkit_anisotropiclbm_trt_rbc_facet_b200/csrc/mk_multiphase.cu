@@ -62,6 +62,72 @@ __global__ void __launch_bounds__(256) k_mp_phi(const S* __restrict__ H, const f
   }
 }
 
+// Two stored 16-bit values at p (p 4-byte aligned) as floats.
+__device__ __forceinline__ float2 ldr2(const __half* p) { return __half22float2(*reinterpret_cast<const __half2*>(p)); }
+__device__ __forceinline__ float2 ldr2(const __nv_bfloat16* p) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+}
+
+// The phi kernel with 16-bit storage, two cells per thread (x even, nx
+// even): a 16-bit load per slot moves half the bytes of an FP32 one, so
+// each slot pair that is 4-byte aligned (every slot of the even loop, the
+// odd loop's directions without an x component) is one 32-bit load; the odd
+// loop's x-shifted slots stay 16-bit loads per cell.  Each cell's sums run
+// in mp_phi_cell's order, so phi is bit-identical.  Pairs with a cell off
+// the interior path or not fluid take mp_phi_cell per cell.
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mp_phi2(const S* __restrict__ H, const float* __restrict__ H0,
+                                                 P* __restrict__ phi, const Geom g, typename Stor<S>::T ref_h,
+                                                 const int z_lo) {
+  const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = z_lo + (int)(gridDim.z - 1 - blockIdx.z);
+  if (x >= g.nx || y >= g.ny) return;
+  const bool f0 = g.fluid(x, y, z), f1 = g.fluid(x + 1, y, z);
+  if (f0 && f1 && fast_cell(g, x, y, z) && fast_cell(g, x + 1, y, z)) {
+    const Fast a = make_fast(g, x, y, z), b = make_fast(g, x + 1, y, z);
+    const int64_t st = g.stride;
+    const float2 r0 = *reinterpret_cast<const float2*>(H0 + a.c);
+    float sa0 = 0.f, sa1 = 0.f, sd0 = 0.f, sd1 = 0.f;
+#pragma unroll
+    for (int i = 1; i < 19; ++i) {
+      float v0, v1;
+      if (PARITY == 0 || ex(i) == 0) {
+        const int64_t o = PARITY == 0 ? (int64_t)i * st + a.c : (int64_t)inv(i) * st + a.idx(0, -ey(i), -ez(i));
+        const float2 v = ldr2(H + o);
+        v0 = v.x;
+        v1 = v.y;
+      } else {
+        v0 = Stor<S>::ldr(H + (int64_t)inv(i) * st + a.idx(-ex(i), -ey(i), -ez(i)));
+        v1 = Stor<S>::ldr(H + (int64_t)inv(i) * st + b.idx(-ex(i), -ey(i), -ez(i)));
+      }
+      if (i < 7) {
+        sa0 += v0;
+        sa1 += v1;
+      } else {
+        sd0 += v0;
+        sd1 += v1;
+      }
+    }
+    float s0 = r0.x, s1 = r0.y;
+    s0 += float(wq<19>(1)) * sa0 + float(wq<19>(7)) * sd0;
+    s1 += float(wq<19>(1)) * sa1 + float(wq<19>(7)) * sd1;
+    *reinterpret_cast<float2*>(phi + a.c) = make_float2(ref_h + s0, ref_h + s1);
+    return;
+  }
+  for (int k = 0; k < 2; ++k) {
+    const int xx = x + k;
+    if (!(k == 0 ? f0 : f1)) continue;
+    if (fast_cell(g, xx, y, z)) {
+      const Fast fa = make_fast(g, xx, y, z);
+      mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, fa, fa.c, ref_h);
+    } else {
+      const Nbr nb(g, xx, y, z);
+      mp_phi_cell<S, P, PARITY>(H, H0, phi, g.stride, nb, nb.idx(0, 0, 0), ref_h);
+    }
+  }
+}
+
 // Where a collision reads its pre-collision populations: straight from the
 // lattices in global memory (GlobalLd), or from rows the bulk-copy engine
 // staged in shared memory (RowLd, below).  g(i) / h(0) return f'_i, hr(i)
@@ -1007,6 +1073,17 @@ void launch_phi_range(mke::Engine& e, int parity, dim3 grid, dim3 block, int z_l
   grid.z = nzr;
   S* H = (S*)e.pop1;
   P* phi = (P*)e.phi[0];
+  if constexpr (Stor<S>::bytes == 2) {
+    if (e.nx % 2 == 0) {  // two cells per thread
+      dim3 g2 = grid;
+      g2.x = (unsigned)((e.nx / 2 + block.x - 1) / block.x);
+      if (parity == 0)
+        k_mp_phi2<S, P, 0><<<g2, block, 0, st>>>(H, e.rest1, phi, g, T(r.r1), z_lo);
+      else
+        k_mp_phi2<S, P, 1><<<g2, block, 0, st>>>(H, e.rest1, phi, g, T(r.r1), z_lo);
+      return;
+    }
+  }
   if (parity == 0)
     k_mp_phi<S, P, 0><<<grid, block, 0, st>>>(H, e.rest1, phi, g, T(r.r1), z_lo);
   else
