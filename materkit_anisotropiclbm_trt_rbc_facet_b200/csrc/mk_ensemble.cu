@@ -97,6 +97,83 @@ __global__ void __launch_bounds__(TILE)
   }
 }
 
+// The phi pass with 16-bit storage, two cells per thread (TILE / 2 threads
+// per tile, cells x and x + 1 of one row; every domain's nx even): each
+// 4-byte-aligned slot pair (every slot of the even loop, the odd loop's
+// slots without an x shift) is one 32-bit load, and phi is stored as a
+// float2.  Each cell's sums keep pf_phi_cell's order (bit-identical); pairs
+// with a cell off the interior path or not fluid take pf_phi_cell per cell.
+__device__ __forceinline__ float2 ens_ldr2(const __half* p) {
+  return __half22float2(*reinterpret_cast<const __half2*>(p));
+}
+__device__ __forceinline__ float2 ens_ldr2(const __nv_bfloat16* p) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+}
+
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(TILE / 2)
+    k_ens_phi2(const S* __restrict__ G, const P* __restrict__ phi_old, P* __restrict__ phi_new,
+               const DomInfo* __restrict__ dom, const int* __restrict__ tile_dom, const int ntiles,
+               const typename Stor<S>::T ref_g) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const DomInfo di = dom[__ldg(tile_dom + t)];
+    const int c0 = t * TILE + 2 * (int)threadIdx.x;
+    const int local = c0 - di.off;
+    int r, x, y;
+    const int z = div_small(local, di.g.nx * di.g.ny, di.inv_nxy, r);
+    y = div_small(r, di.g.nx, di.inv_nx, x);
+    const bool f0 = di.g.fluid(x, y, z), f1 = di.g.fluid(x + 1, y, z);
+    if (f0 && f1 && fastw_cell(di.g, x, y, z) && fastw_cell(di.g, x + 1, y, z)) {
+      FastW a = make_fastw(di.g, x, y, z), b = make_fastw(di.g, x + 1, y, z);
+      a.c += di.off;
+      b.c += di.off;
+      const int64_t st = di.g.stride;
+      float r0a, r0b, sa0 = 0.f, sa1 = 0.f;
+      {
+        const int64_t o = PARITY == 0 ? (int64_t)a.c : (int64_t)a.idx(0, 0, 0);
+        const float2 v = ens_ldr2(G + o);
+        r0a = v.x;
+        r0b = v.y;
+      }
+#pragma unroll
+      for (int i = 1; i < 7; ++i) {
+        float v0, v1;
+        if (PARITY == 0 || ex(i) == 0) {
+          const int64_t o = PARITY == 0 ? (int64_t)i * st + a.c : (int64_t)inv(i) * st + a.idx(0, -ey(i), -ez(i));
+          const float2 v = ens_ldr2(G + o);
+          v0 = v.x;
+          v1 = v.y;
+        } else {
+          v0 = ld_in_raw<S, 7>(G, st, a, PARITY, a.c, i);
+          v1 = ld_in_raw<S, 7>(G, st, b, PARITY, b.c, i);
+        }
+        sa0 += v0;
+        sa1 += v1;
+      }
+      const float s0 = float(wq<7>(0)) * r0a + float(wq<7>(1)) * sa0;
+      const float s1 = float(wq<7>(0)) * r0b + float(wq<7>(1)) * sa1;
+      *reinterpret_cast<float2*>(phi_new + a.c) = make_float2(ref_g + s0, ref_g + s1);
+      continue;
+    }
+    for (int k = 0; k < 2; ++k) {
+      const int xx = x + k, c = c0 + k;
+      if (!(k == 0 ? f0 : f1)) {
+        phi_new[c] = phi_old[c];
+        continue;
+      }
+      if (fastw_cell(di.g, xx, y, z)) {
+        FastW fa = make_fastw(di.g, xx, y, z);
+        fa.c += di.off;
+        pf_phi_cell<S, P, PARITY>(G, phi_new, di.g.stride, fa, fa.c, ref_g);
+      } else {
+        Nbr nb(di.g, xx, y, z);
+        nb.base = di.off;
+        pf_phi_cell<S, P, PARITY>(G, phi_new, di.g.stride, nb, nb.idx(0, 0, 0), ref_g);
+      }
+    }
+  }
+}
+
 // Four resident 256-thread blocks per SM (64 registers) for the 32-bit and
 // 16-bit variants; the FP64 one keeps its registers.
 template <class S, class P, int PARITY, bool SOL, bool GEN>
@@ -187,6 +264,7 @@ struct mk_ensemble {
   int device = 0, sms = 148;
   int grid_phi[2] = {1, 1}, grid_col[2] = {1, 1};  // persistent launch sizes per parity
   bool gen_aniso = false;  // some domain has a non-cubic anisotropy kind
+  bool pair = false;       // 16-bit storage and every domain's nx even: k_ens_phi2
   cudaStream_t stream = nullptr;
   void* pop0 = nullptr;
   void* pop1 = nullptr;
@@ -223,9 +301,9 @@ mk_status ens_arg(mk_ensemble* e, const std::string& m) {
 
 // Blocks of a persistent launch: resident blocks per SM x SMs, at most one per tile.
 template <class K>
-int persistent_grid(const mk_ensemble& e, K kernel) {
+int persistent_grid(const mk_ensemble& e, K kernel, int threads = TILE) {
   int per_sm = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE, 0) != cudaSuccess || per_sm < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1) {
     cudaGetLastError();
     per_sm = 1;
   }
@@ -246,12 +324,26 @@ void loop_t(mk_ensemble& e, cudaEvent_t* ev) {
   const DendK<T>* kd = (const DendK<T>*)e.kd;
   const T ref_g = T(-1.0);
   if (ev) cudaEventRecord(ev[0], e.stream);
-  if (parity == 0)
-    k_ens_phi<S, P, 0><<<e.grid_phi[0], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
-                                                             ref_g);
-  else
-    k_ens_phi<S, P, 1><<<e.grid_phi[1], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
-                                                             ref_g);
+  bool paired = false;
+  if constexpr (Stor<S>::bytes == 2) {
+    if (e.pair) {
+      if (parity == 0)
+        k_ens_phi2<S, P, 0><<<e.grid_phi[0], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
+                                                                      e.ntiles, ref_g);
+      else
+        k_ens_phi2<S, P, 1><<<e.grid_phi[1], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
+                                                                      e.ntiles, ref_g);
+      paired = true;
+    }
+  }
+  if (!paired) {
+    if (parity == 0)
+      k_ens_phi<S, P, 0><<<e.grid_phi[0], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
+                                                               ref_g);
+    else
+      k_ens_phi<S, P, 1><<<e.grid_phi[1], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
+                                                               ref_g);
+  }
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
     cudaEventRecord(ev[2], e.stream);
@@ -310,6 +402,12 @@ void size_grids(mk_ensemble& e) {
   // each parity has its own register footprint, hence its own resident count
   e.grid_phi[0] = persistent_grid(e, k_ens_phi<S, P, 0>);
   e.grid_phi[1] = persistent_grid(e, k_ens_phi<S, P, 1>);
+  if constexpr (Stor<S>::bytes == 2) {
+    if (e.pair) {
+      e.grid_phi[0] = persistent_grid(e, k_ens_phi2<S, P, 0>, TILE / 2);
+      e.grid_phi[1] = persistent_grid(e, k_ens_phi2<S, P, 1>, TILE / 2);
+    }
+  }
   for (int par = 0; par < 2; ++par) {
     int g;
     if (e.gen_aniso)
@@ -509,7 +607,11 @@ mk_status mk_ensemble_create(const mk_params* params, int32_t n_domains, mk_ense
   e->model = params[0].model;
   e->precision = params[0].precision;
   e->elem = store_bytes(e->precision);
-  for (int d = 0; d < n_domains; ++d) e->gen_aniso = e->gen_aniso || params[d].aniso != MK_ANISO_CUBIC;
+  e->pair = e->elem == 2;
+  for (int d = 0; d < n_domains; ++d) {
+    e->gen_aniso = e->gen_aniso || params[d].aniso != MK_ANISO_CUBIC;
+    e->pair = e->pair && params[d].nx % 2 == 0;
+  }
   e->phi_elem = e->precision == MK_PREC_FP64 ? 8 : 4;
   cudaGetDevice(&e->device);
   cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device);

@@ -68,6 +68,40 @@ def test_ensemble_matches_single_domains(precision, model):
         s.close()
 
 
+def _shaped(precision, model, shapes):
+    """Box-shaped domains (nx, ny, nz), each cell count a multiple of 256."""
+    ps = _small(precision, model, edges=tuple(max(sh) for sh in shapes))
+    rng = np.random.default_rng(11)
+    for p, sh in zip(ps, shapes):
+        p.nx, p.ny, p.nz = sh
+        for s in range(p.n_objects):
+            for a in range(3):
+                p.obj_center[s][a] = 3.0 + (sh[a] - 6.0) * rng.random() + 0.137
+    return ps
+
+
+# every nx even (16-bit storage takes the two-cells-per-thread phi pass) and
+# one odd nx (every domain on the one-cell pass)
+SHAPES = {"even": [(18, 16, 16), (32, 8, 24), (16, 32, 8)],
+          "odd": [(18, 16, 16), (17, 16, 16), (16, 32, 8)]}
+
+
+@pytest.mark.parametrize("precision,model", [("fp16", "thermal_dendrite"), ("bf16", "solutal_dendrite")])
+@pytest.mark.parametrize("shapes", sorted(SHAPES))
+def test_ensemble_box_domains_match_single_domains(precision, model, shapes):
+    ps = _shaped(precision, model, SHAPES[shapes])
+    ens = Ensemble(ps)
+    singles = [Solver(params=p) for p in ps]
+    for n in (13, 8):
+        ens.advance(n)
+        for s in singles:
+            s.advance(n)
+        _check_equal(ens, singles, _fields(model), f"{shapes} shapes after {ens.step} loops")
+    ens.close()
+    for s in singles:
+        s.close()
+
+
 def test_generated_ensemble_runs():
     ps = ensemble_params(0xE45E, 6, "bf16")
     ens = Ensemble(ps)
