@@ -40,6 +40,45 @@ __device__ __forceinline__ void pf_phi_cell(const S* __restrict__ G, P* __restri
   phi_new[c] = P(ref_g + s);
 }
 
+// phi of the two cells a and b (b = a + 1 in x, a.c even, both fluid and on
+// the FastW path): each slot pair of the even loop and each of the odd loop's
+// slots without an x shift is one aligned pair load (the slot planes' stride
+// is even); each cell's sum keeps pf_phi_cell's order, so both values are
+// bit-identical to it.
+template <class S, class P, int PARITY>
+__device__ __forceinline__ void pf_phi_pair(const S* __restrict__ G, P* __restrict__ phi_new, const int64_t stride,
+                                            const FastW& a, const FastW& b, const typename Stor<S>::T ref_g) {
+  typedef typename Stor<S>::T T;
+  T v0[7], v1[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    if (PARITY == 0 || ex(i) == 0) {
+      ldr_pair(G + off_in<7>(stride, a, PARITY, a.c, i), v0[i], v1[i]);
+    } else {
+      v0[i] = ld_in_raw<S, 7>(G, stride, a, PARITY, a.c, i);
+      v1[i] = ld_in_raw<S, 7>(G, stride, b, PARITY, b.c, i);
+    }
+  }
+  T s0 = T(0), s1 = T(0);
+  if constexpr (Stor<S>::scaled) {
+    T sa0 = T(0), sa1 = T(0);
+#pragma unroll
+    for (int i = 1; i < 7; ++i) {
+      sa0 += v0[i];
+      sa1 += v1[i];
+    }
+    s0 = T(wq<7>(0)) * v0[0] + T(wq<7>(1)) * sa0;
+    s1 = T(wq<7>(0)) * v1[0] + T(wq<7>(1)) * sa1;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      s0 += v0[i];
+      s1 += v1[i];
+    }
+  }
+  st_pair(phi_new + a.c, P(ref_g + s0), P(ref_g + s1));
+}
+
 template <class S, class P, int PARITY>
 __global__ void __launch_bounds__(256) k_pf_phi(const S* __restrict__ G, const P* __restrict__ phi_old,
                                                 P* __restrict__ phi_new, const Geom g, typename Stor<S>::T ref_g) {

@@ -730,6 +730,31 @@ __device__ __forceinline__ void pf_in(const S* __restrict__ A, int64_t stride, c
 
 // The stored value itself: f'_i, or f'_i / w_i for the 16-bit formats
 // (Stor<S>::scaled), for arithmetic that works in the stored units.
+// Two adjacent stored values at p as ldr reads them (p aligned to twice the
+// element size): one 16-, 8- or 4-byte load.
+__device__ __forceinline__ void ldr_pair(const double* p, double& a, double& b) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ldr_pair(const float* p, float& a, float& b) {
+  const float2 v = *reinterpret_cast<const float2*>(p);
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ldr_pair(const __half* p, float& a, float& b) {
+  const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ldr_pair(const __nv_bfloat16* p, float& a, float& b) {
+  const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void st_pair(double* p, double a, double b) { *reinterpret_cast<double2*>(p) = make_double2(a, b); }
+__device__ __forceinline__ void st_pair(float* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+
 template <class S, int Q, class NB>
 __device__ __forceinline__ typename Stor<S>::T ld_in_raw(const S* __restrict__ A, int64_t stride, const NB& nb,
                                                           int parity, int c, int i) {

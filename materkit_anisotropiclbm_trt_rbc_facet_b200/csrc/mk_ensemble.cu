@@ -97,19 +97,10 @@ __global__ void __launch_bounds__(TILE)
   }
 }
 
-// The phi pass with 16-bit storage, two cells per thread (TILE / 2 threads
-// per tile, cells x and x + 1 of one row; every domain's nx even): each
-// 4-byte-aligned slot pair (every slot of the even loop, the odd loop's
-// slots without an x shift) is one 32-bit load, and phi is stored as a
-// float2.  Each cell's sums keep pf_phi_cell's order (bit-identical); pairs
-// with a cell off the interior path or not fluid take pf_phi_cell per cell.
-__device__ __forceinline__ float2 ens_ldr2(const __half* p) {
-  return __half22float2(*reinterpret_cast<const __half2*>(p));
-}
-__device__ __forceinline__ float2 ens_ldr2(const __nv_bfloat16* p) {
-  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
-}
-
+// The phi pass with two cells per thread (TILE / 2 threads per tile, cells x
+// and x + 1 of one row; every domain's nx even): pf_phi_pair where both cells
+// are fluid and on the interior path, else pf_phi_cell per cell; phi is
+// bit-identical to k_ens_phi.
 template <class S, class P, int PARITY>
 __global__ void __launch_bounds__(TILE / 2)
     k_ens_phi2(const S* __restrict__ G, const P* __restrict__ phi_old, P* __restrict__ phi_new,
@@ -127,32 +118,7 @@ __global__ void __launch_bounds__(TILE / 2)
       FastW a = make_fastw(di.g, x, y, z), b = make_fastw(di.g, x + 1, y, z);
       a.c += di.off;
       b.c += di.off;
-      const int64_t st = di.g.stride;
-      float r0a, r0b, sa0 = 0.f, sa1 = 0.f;
-      {
-        const int64_t o = PARITY == 0 ? (int64_t)a.c : (int64_t)a.idx(0, 0, 0);
-        const float2 v = ens_ldr2(G + o);
-        r0a = v.x;
-        r0b = v.y;
-      }
-#pragma unroll
-      for (int i = 1; i < 7; ++i) {
-        float v0, v1;
-        if (PARITY == 0 || ex(i) == 0) {
-          const int64_t o = PARITY == 0 ? (int64_t)i * st + a.c : (int64_t)inv(i) * st + a.idx(0, -ey(i), -ez(i));
-          const float2 v = ens_ldr2(G + o);
-          v0 = v.x;
-          v1 = v.y;
-        } else {
-          v0 = ld_in_raw<S, 7>(G, st, a, PARITY, a.c, i);
-          v1 = ld_in_raw<S, 7>(G, st, b, PARITY, b.c, i);
-        }
-        sa0 += v0;
-        sa1 += v1;
-      }
-      const float s0 = float(wq<7>(0)) * r0a + float(wq<7>(1)) * sa0;
-      const float s1 = float(wq<7>(0)) * r0b + float(wq<7>(1)) * sa1;
-      *reinterpret_cast<float2*>(phi_new + a.c) = make_float2(ref_g + s0, ref_g + s1);
+      pf_phi_pair<S, P, PARITY>(G, phi_new, di.g.stride, a, b, ref_g);
       continue;
     }
     for (int k = 0; k < 2; ++k) {
@@ -264,7 +230,7 @@ struct mk_ensemble {
   int device = 0, sms = 148;
   int grid_phi[2] = {1, 1}, grid_col[2] = {1, 1};  // persistent launch sizes per parity
   bool gen_aniso = false;  // some domain has a non-cubic anisotropy kind
-  bool pair = false;       // 16-bit storage and every domain's nx even: k_ens_phi2
+  bool pair = false;       // every domain's nx even: the phi pass is k_ens_phi2
   cudaStream_t stream = nullptr;
   void* pop0 = nullptr;
   void* pop1 = nullptr;
@@ -324,25 +290,19 @@ void loop_t(mk_ensemble& e, cudaEvent_t* ev) {
   const DendK<T>* kd = (const DendK<T>*)e.kd;
   const T ref_g = T(-1.0);
   if (ev) cudaEventRecord(ev[0], e.stream);
-  bool paired = false;
-  if constexpr (Stor<S>::bytes == 2) {
-    if (e.pair) {
-      if (parity == 0)
-        k_ens_phi2<S, P, 0><<<e.grid_phi[0], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
-                                                                      e.ntiles, ref_g);
-      else
-        k_ens_phi2<S, P, 1><<<e.grid_phi[1], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
-                                                                      e.ntiles, ref_g);
-      paired = true;
-    }
-  }
-  if (!paired) {
+  if (e.pair) {
     if (parity == 0)
-      k_ens_phi<S, P, 0><<<e.grid_phi[0], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
-                                                               ref_g);
+      k_ens_phi2<S, P, 0><<<e.grid_phi[0], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
+                                                                    e.ntiles, ref_g);
     else
-      k_ens_phi<S, P, 1><<<e.grid_phi[1], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
-                                                               ref_g);
+      k_ens_phi2<S, P, 1><<<e.grid_phi[1], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
+                                                                    e.ntiles, ref_g);
+  } else if (parity == 0) {
+    k_ens_phi<S, P, 0><<<e.grid_phi[0], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
+                                                             ref_g);
+  } else {
+    k_ens_phi<S, P, 1><<<e.grid_phi[1], TILE, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom, e.ntiles,
+                                                             ref_g);
   }
   if (ev) {
     cudaEventRecord(ev[1], e.stream);
@@ -400,13 +360,12 @@ void size_grids(mk_ensemble& e) {
   typedef typename PhiOf<S>::type P;
   const bool sol = e.model == MK_MODEL_SOLUTAL_DENDRITE;
   // each parity has its own register footprint, hence its own resident count
-  e.grid_phi[0] = persistent_grid(e, k_ens_phi<S, P, 0>);
-  e.grid_phi[1] = persistent_grid(e, k_ens_phi<S, P, 1>);
-  if constexpr (Stor<S>::bytes == 2) {
-    if (e.pair) {
-      e.grid_phi[0] = persistent_grid(e, k_ens_phi2<S, P, 0>, TILE / 2);
-      e.grid_phi[1] = persistent_grid(e, k_ens_phi2<S, P, 1>, TILE / 2);
-    }
+  if (e.pair) {
+    e.grid_phi[0] = persistent_grid(e, k_ens_phi2<S, P, 0>, TILE / 2);
+    e.grid_phi[1] = persistent_grid(e, k_ens_phi2<S, P, 1>, TILE / 2);
+  } else {
+    e.grid_phi[0] = persistent_grid(e, k_ens_phi<S, P, 0>);
+    e.grid_phi[1] = persistent_grid(e, k_ens_phi<S, P, 1>);
   }
   for (int par = 0; par < 2; ++par) {
     int g;
@@ -607,7 +566,7 @@ mk_status mk_ensemble_create(const mk_params* params, int32_t n_domains, mk_ense
   e->model = params[0].model;
   e->precision = params[0].precision;
   e->elem = store_bytes(e->precision);
-  e->pair = e->elem == 2;
+  e->pair = true;
   for (int d = 0; d < n_domains; ++d) {
     e->gen_aniso = e->gen_aniso || params[d].aniso != MK_ANISO_CUBIC;
     e->pair = e->pair && params[d].nx % 2 == 0;

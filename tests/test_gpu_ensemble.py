@@ -80,13 +80,15 @@ def _shaped(precision, model, shapes):
     return ps
 
 
-# every nx even (16-bit storage takes the two-cells-per-thread phi pass) and
-# one odd nx (every domain on the one-cell pass)
+# every nx even (the ensemble's phi pass takes two cells per thread, the
+# domains run alone one) and one odd nx (the one-cell pass everywhere): both
+# passes give the same bits
 SHAPES = {"even": [(18, 16, 16), (32, 8, 24), (16, 32, 8)],
           "odd": [(18, 16, 16), (17, 16, 16), (16, 32, 8)]}
 
 
-@pytest.mark.parametrize("precision,model", [("fp16", "thermal_dendrite"), ("bf16", "solutal_dendrite")])
+@pytest.mark.parametrize("precision,model", [("fp64", "solutal_dendrite"), ("fp32", "thermal_dendrite"),
+                                             ("fp16", "thermal_dendrite"), ("bf16", "solutal_dendrite")])
 @pytest.mark.parametrize("shapes", sorted(SHAPES))
 def test_ensemble_box_domains_match_single_domains(precision, model, shapes):
     ps = _shaped(precision, model, SHAPES[shapes])
