@@ -140,6 +140,23 @@ __global__ void __launch_bounds__(TILE / 2)
   }
 }
 
+// The even loop's phi pass when every cell of every domain is fluid (no wall
+// axis; ensemble domains carry no solid mask): an even loop reads only a
+// cell's own slots, so phi is a flat sum over the packed index, two cells per
+// thread, with no domain lookup or coordinates (pf_phi_pair at parity 0 uses
+// the cell index alone; bit-identical to k_ens_phi).
+template <class S, class P>
+__global__ void __launch_bounds__(TILE)
+    k_ens_phi_flat(const S* __restrict__ G, P* __restrict__ phi_new, const int64_t stride, const int ncell,
+                   const typename Stor<S>::T ref_g) {
+  for (int64_t c = 2 * (int64_t)(blockIdx.x * blockDim.x + threadIdx.x); c < ncell;
+       c += 2 * (int64_t)gridDim.x * blockDim.x) {
+    FastW a{};
+    a.c = (int)c;
+    pf_phi_pair<S, P, 0>(G, phi_new, stride, a, a, ref_g);
+  }
+}
+
 // Four resident 256-thread blocks per SM (64 registers) for the 32-bit and
 // 16-bit variants; the FP64 one keeps its registers.
 template <class S, class P, int PARITY, bool SOL, bool GEN>
@@ -229,8 +246,10 @@ struct mk_ensemble {
   int ntiles = 0;
   int device = 0, sms = 148;
   int grid_phi[2] = {1, 1}, grid_col[2] = {1, 1};  // persistent launch sizes per parity
+  int grid_flat = 1;
   bool gen_aniso = false;  // some domain has a non-cubic anisotropy kind
   bool pair = false;       // every domain's nx even: the phi pass is k_ens_phi2
+  bool flat_even = false;  // no domain has a wall axis: the even loop's phi pass is k_ens_phi_flat
   cudaStream_t stream = nullptr;
   void* pop0 = nullptr;
   void* pop1 = nullptr;
@@ -290,7 +309,9 @@ void loop_t(mk_ensemble& e, cudaEvent_t* ev) {
   const DendK<T>* kd = (const DendK<T>*)e.kd;
   const T ref_g = T(-1.0);
   if (ev) cudaEventRecord(ev[0], e.stream);
-  if (e.pair) {
+  if (parity == 0 && e.flat_even) {
+    k_ens_phi_flat<S, P><<<e.grid_flat, TILE, 0, e.stream>>>(G, phi_new, e.stride, (int)e.ncell, ref_g);
+  } else if (e.pair) {
     if (parity == 0)
       k_ens_phi2<S, P, 0><<<e.grid_phi[0], TILE / 2, 0, e.stream>>>(G, phi_old, phi_new, e.dom, e.tile_dom,
                                                                     e.ntiles, ref_g);
@@ -360,6 +381,7 @@ void size_grids(mk_ensemble& e) {
   typedef typename PhiOf<S>::type P;
   const bool sol = e.model == MK_MODEL_SOLUTAL_DENDRITE;
   // each parity has its own register footprint, hence its own resident count
+  e.grid_flat = persistent_grid(e, k_ens_phi_flat<S, P>);
   if (e.pair) {
     e.grid_phi[0] = persistent_grid(e, k_ens_phi2<S, P, 0>, TILE / 2);
     e.grid_phi[1] = persistent_grid(e, k_ens_phi2<S, P, 1>, TILE / 2);
@@ -567,9 +589,11 @@ mk_status mk_ensemble_create(const mk_params* params, int32_t n_domains, mk_ense
   e->precision = params[0].precision;
   e->elem = store_bytes(e->precision);
   e->pair = true;
+  e->flat_even = true;
   for (int d = 0; d < n_domains; ++d) {
     e->gen_aniso = e->gen_aniso || params[d].aniso != MK_ANISO_CUBIC;
     e->pair = e->pair && params[d].nx % 2 == 0;
+    for (int a = 0; a < 3; ++a) e->flat_even = e->flat_even && params[d].bc[a] != MK_BC_WALLS;
   }
   e->phi_elem = e->precision == MK_PREC_FP64 ? 8 : 4;
   cudaGetDevice(&e->device);

@@ -104,6 +104,24 @@ def test_ensemble_box_domains_match_single_domains(precision, model, shapes):
         s.close()
 
 
+@pytest.mark.parametrize("precision,model", [("fp32", "thermal_dendrite"), ("bf16", "solutal_dendrite")])
+def test_ensemble_with_walls_matches_single_domains(precision, model):
+    """Walls in y on one domain: the even loop's phi pass leaves the flat
+    all-fluid form for the per-tile one (wall cells keep their phi)."""
+    ps = _shaped(precision, model, SHAPES["even"])
+    ps[1].bc[1] = A.MK_BC_WALLS
+    ens = Ensemble(ps)
+    singles = [Solver(params=p) for p in ps]
+    for n in (13, 8):
+        ens.advance(n)
+        for s in singles:
+            s.advance(n)
+        _check_equal(ens, singles, _fields(model), f"walls after {ens.step} loops")
+    ens.close()
+    for s in singles:
+        s.close()
+
+
 def test_generated_ensemble_runs():
     ps = ensemble_params(0xE45E, 6, "bf16")
     ens = Ensemble(ps)
