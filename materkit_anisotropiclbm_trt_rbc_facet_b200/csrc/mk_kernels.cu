@@ -617,6 +617,67 @@ __global__ void __launch_bounds__(256) k_mg_phi(const S* __restrict__ G, P* __re
   }
 }
 
+// k_mg_phi with 16-bit storage, two cells of a row per thread (nx even):
+// each slot pair of the even loop and each of the odd loop's slots without an
+// x shift is one 32-bit load, phi_j is stored as a float2; each cell's sums
+// keep mg_phi_cell's order (bit-identical).  A pair with a cell off the
+// interior path or not fluid takes mg_phi_cell per cell.
+template <class S, class P, int PARITY>
+__global__ void __launch_bounds__(256) k_mg_phi2(const S* __restrict__ G, P* __restrict__ phij, const Geom g, int j0) {
+  typedef typename Stor<S>::T T;
+  static_assert(Stor<S>::scaled, "the pair form is the 16-bit one");
+  const int x = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = (int)(blockIdx.z % (unsigned)g.nz);
+  const int j = j0 + (int)(blockIdx.z / (unsigned)g.nz);
+  if (x >= g.nx || y >= g.ny) return;
+  const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+  const S* Gj = G + (int64_t)j * 19 * g.stride;
+  P* pj = phij + (int64_t)j * ncell;
+  const bool f0 = g.fluid(x, y, z), f1 = g.fluid(x + 1, y, z);
+  if (f0 && f1 && fastw_cell(g, x, y, z) && fastw_cell(g, x + 1, y, z)) {
+    const FastW a = make_fastw(g, x, y, z), b = make_fastw(g, x + 1, y, z);
+    T v0[19], v1[19];
+#pragma unroll
+    for (int i = 0; i < 19; ++i) {
+      if (PARITY == 0 || ex(i) == 0) {
+        ldr_pair(Gj + off_in<19>(g.stride, a, PARITY, a.c, i), v0[i], v1[i]);
+      } else {
+        v0[i] = ld_in_raw<S, 19>(Gj, g.stride, a, PARITY, a.c, i);
+        v1[i] = ld_in_raw<S, 19>(Gj, g.stride, b, PARITY, b.c, i);
+      }
+    }
+    T sa0 = T(0), sd0 = T(0), sa1 = T(0), sd1 = T(0);
+#pragma unroll
+    for (int i = 1; i < 7; ++i) {
+      sa0 += v0[i];
+      sa1 += v1[i];
+    }
+#pragma unroll
+    for (int i = 7; i < 19; ++i) {
+      sd0 += v0[i];
+      sd1 += v1[i];
+    }
+    T sum0 = T(-1), sum1 = T(-1);
+    sum0 += T(wq<19>(0)) * v0[0] + T(wq<19>(1)) * sa0 + T(wq<19>(7)) * sd0;
+    sum1 += T(wq<19>(0)) * v1[0] + T(wq<19>(1)) * sa1 + T(wq<19>(7)) * sd1;
+    st_pair(pj + a.c, P(sum0), P(sum1));
+    return;
+  }
+#pragma unroll 1
+  for (int k = 0; k < 2; ++k) {
+    const int xx = x + k;
+    if (!(k == 0 ? f0 : f1)) continue;
+    if (fastw_cell(g, xx, y, z)) {
+      const FastW fa = make_fastw(g, xx, y, z);
+      mg_phi_cell<S, P, PARITY>(Gj, pj, g.stride, fa, fa.c);
+    } else {
+      const Nbr nb(g, xx, y, z);
+      mg_phi_cell<S, P, PARITY>(Gj, pj, g.stride, nb, nb.idx(0, 0, 0));
+    }
+  }
+}
+
 // Per cell, once: the aggregate phi = (N - 1) + sum phi_j into phi_new and
 // S2 = sum_k p_k^2, p = (1 + phi)/2, into plane N of phij (the grains'
 // threads of the collision read it instead of all N order parameters each).
@@ -1529,6 +1590,18 @@ void launch_mg(mke::Engine& e, int parity, dim3 grid, dim3 block, cudaEvent_t* e
   if (ev) cudaEventRecord(ev[0], e.stream);
   for (int j0 = 0; j0 < ngr; j0 += ppl) {
     const dim3 gz(grid.x, grid.y, (unsigned)(e.nz * std::min(ppl, ngr - j0)));
+    bool paired = false;
+    if constexpr (Stor<S>::bytes == 2) {
+      if (e.nx % 2 == 0) {
+        const dim3 g2((unsigned)((e.nx / 2 + (int)block.x - 1) / (int)block.x), gz.y, gz.z);
+        if (parity == 0)
+          k_mg_phi2<S, P, 0><<<g2, block, 0, e.stream>>>(G, phij, g, j0);
+        else
+          k_mg_phi2<S, P, 1><<<g2, block, 0, e.stream>>>(G, phij, g, j0);
+        paired = true;
+      }
+    }
+    if (paired) continue;
     if (parity == 0)
       k_mg_phi<S, P, 0><<<gz, block, 0, e.stream>>>(G, phij, g, j0);
     else
