@@ -66,8 +66,8 @@ WORKLOADS = {
                    "metric": "MLUPS: Poiseuille channel 64x32x32, D3Q19 TRT, FP64",
                    "size": 64, "precision": "fp64", "kernel": "k_flow", "collision": "TRT(f)",
                    "data": "synthetic (fluid at rest, constant body force)"},
-    "ensemble": {"workload": "solutal dendrite ensemble: 48 domains, edges 48-128, 1-6 seeds each, seed 0xE45E",
-                 "metric": "MLUPS aggregate, %HBM roofline: 48-domain solutal dendrite ensemble, BF16, "
+    "ensemble": {"workload": "solutal dendrite ensemble: {nd} domains, edges 48-128, 1-6 seeds each, seed 0xE45E",
+                 "metric": "MLUPS aggregate, %HBM roofline: {nd}-domain solutal dendrite ensemble, BF16, "
                            "persistent + graph",
                  "size": 0, "precision": "bf16", "kernel": "k_ens_collide", "collision": "BGK(g) + TRT(U)",
                  "data": "synthetic (splitmix64 ensemble generator, seed 0xE45E)"},
@@ -390,7 +390,7 @@ def run_ours(args):
     tkey = f"{args.workload}_collide_{args.precision}_bytes_per_cell"
     traffic_launch = traffic[tkey] * params.ncell() if tkey in traffic else None
     line = {
-        "metric": wl["metric"],
+        "metric": wl["metric"].format(nd=args.domains),
         "value": round(r["mlups"], 1),
         "unit": "MLUPS",
         "n_gpus": ws,
@@ -402,7 +402,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32",
         "data": wl["data"],
-        "config": {"workload": wl["workload"].format(n=n, h=n // 2), "cells": params.ncell(),
+        "config": {"workload": wl["workload"].format(n=n, h=n // 2, nd=args.domains), "cells": params.ncell(),
                    "storage": args.precision, "collision": wl["collision"], "streaming": "AA in place",
                    "l2": ("inputs larger than L2 (%.2f GB resident populations)"
                           if r["bytes_per_cell"] * params.ncell() / 2 > 126e6 else
@@ -533,11 +533,12 @@ def run_ensemble(args):
     traffic = _ncu_traffic()
     tkey = f"ensemble_collide_{args.precision}_bytes_per_cell"
     line = {
-        "metric": wl["metric"], "value": round(r["mlups"], 1), "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": W,
+        "metric": wl["metric"].format(nd=nd), "value": round(r["mlups"], 1), "unit": "MLUPS", "n_gpus": ws, "steps": K,
+        "warmup": W,
         "ms_per_step": round(r["ms_per_step"], 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32"}.get(args.precision, "f32"),
         "data": wl["data"],
-        "config": {"workload": wl["workload"], "domains": nd, "cells": r["cells"], "storage": args.precision,
+        "config": {"workload": wl["workload"].format(nd=nd), "domains": nd, "cells": r["cells"], "storage": args.precision,
                    "collision": wl["collision"], "streaming": "AA in place",
                    "l2": "inputs larger than L2 (%.2f GB resident state)" % (
                        r["step_bytes_per_cell"] * r["cells"] / 2 / 1e9),
@@ -730,10 +731,11 @@ def run_reference(args):
         sample = (f"{steps} loops of {_sample_name(args.workload, n)} (requested {args.steps}); the reference's own "
                   f"solver is a closed Windows DLL, so this is the FP64 OpenMP restatement")
     line = {
-        "metric": wl["metric"], "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws, "steps": steps, "warmup": 1,
+        "metric": wl["metric"].format(nd=args.domains), "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": ws,
+        "steps": steps, "warmup": 1,
         "ms_per_step": round(dt / steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": wl["data"],
-        "config": {"workload": wl["workload"].format(n=n), "cells": cells, "storage": "fp64",
+        "config": {"workload": wl["workload"].format(n=n, nd=args.domains), "cells": cells, "storage": "fp64",
                    "parallelism": f"{cores} host threads"},
         "impl": "reference",
         "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": cores, "kind": kind,
